@@ -1,0 +1,309 @@
+"""Benchmark of the per-level LBM step on B200 (one JSON line on rank 0).
+
+Workload (the throughput roofline configuration): periodic 256^3 uniform box,
+16.8M cells, one level, D3Q19 BGK, Taylor-Green vortex u0 = 0.05, tau = 0.55.
+A step is one TimeLoop::advance_one (one fused pull-stream + collide launch).
+`value` is whole-job MLUPS (all ranks) with the state resident in HBM; the
+lattice (2 x 1.27 GB FP32) is larger than L2 (126 MB), so no L2 flush is
+needed between steps.  `e2e` runs the same job through the C ABI from host
+memory: FP64 initial populations uploaded, K steps, fields read back.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision fp32|fp16] [--n 256]
+
+N > 1 (torchrun) runs N independent replicas (weak scaling, no collective in
+the data path), timed as the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def committed_traffic(kernel_key):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary
+    (profiles/ncu_traffic.txt lines: '<key> <bytes_per_launch>'), or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == kernel_key:
+                try:
+                    return float(parts[1])
+                except ValueError:
+                    return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 7:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx = float(p[1])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[3 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("gloo", timeout=timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, v):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def cpu_reference_mlups(n, steps_budget_s=12.0, threads=None):
+    """The reference's own BlockLattice<double> collide / fill_periodic_halo /
+    stream (oracle/_ref; the C restatement when it is absent) on the host
+    cores: `threads` independent periodic z-slabs covering the n^3 box."""
+    from oracle import oracle
+    import ctypes
+    threads = threads or os.cpu_count() or 1
+    L = oracle.load("ref")
+    kind = "reference"
+    if L is None:
+        L = oracle.load("orc")
+        kind = "port"
+    slabs = max(1, min(threads, n // 4))
+    nzs = n // slabs
+    blocks = [oracle.Block(L, n, n, nzs) for _ in range(slabs)]
+    for b in blocks:
+        b.initialize(1.0, (0.01, 0.0, 0.0))
+    omega = 1.0 / 0.55
+    # calibrate: one step on one slab
+    t0 = time.perf_counter()
+    blocks[0].run_periodic(omega, 1)
+    t_one = time.perf_counter() - t0
+    per_step_par = t_one * slabs / min(threads, slabs)
+    steps = max(1, int(steps_budget_s / max(per_step_par, 1e-6)))
+    ths = [threading.Thread(target=b.run_periodic, args=(omega, steps)) for b in blocks]
+    t0 = time.perf_counter()
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    sec = time.perf_counter() - t0
+    mlups = n * n * nzs * slabs * steps / sec / 1e6
+    return {"value": mlups, "unit": "MLUPS", "cores": min(threads, slabs), "kind": kind,
+            "sample": f"{steps} steps of {n}^3 as {slabs} periodic {n}x{n}x{nzs} slabs, FP64, "
+                      f"{min(threads, slabs)} threads ({sec:.1f} s)"}
+
+
+def run_reference_arm(args, world, rank, pg):
+    if rank != 0:
+        return
+    lines = []
+    vals = []
+    # each step is a bounded sample so K + W samples end within a few minutes
+    per = min(args.ref_seconds, 150.0 / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        cpu_reference_mlups(args.n, steps_budget_s=min(per, 1.0))
+    for _ in range(args.steps):
+        r = cpu_reference_mlups(args.n, steps_budget_s=per)
+        vals.append(r["value"])
+        lines.append(r)
+    v = statistics.median(vals)
+    r = lines[0]
+    out = {"metric": "MLUPS", "value": v, "unit": "MLUPS", "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"tgv_periodic_{args.n}^3", "cells": args.n ** 3, "tau": 0.55, "u0": 0.05},
+           "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": r["cores"], "kind": r["kind"], "sample": r["sample"]},
+           "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--ref-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local, pg = dist_setup(args)
+
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    import octlb_b200 as ob
+    from octlb_b200 import cases
+
+    n = args.n
+    results = {}
+    for prec_name in (["fp32", "fp16"] if args.precision == "fp32" else ["fp16", "fp32"]):
+        prec = ob.FP32 if prec_name == "fp32" else ob.FP16_SHIFTED
+        mesh, init, info = cases.tgv_periodic(n, u0=0.05, tau=0.55)
+        lat = ob.GpuLattice(mesh, info["omega"], precision=prec, init_pops=init)
+        stream = torch.cuda.current_stream()
+        lat.set_stream(stream.cuda_stream)
+        launches, lups = lat.step_stats()
+        lat.advance(args.warmup)
+        torch.cuda.synchronize()
+        barrier(pg)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as cs:
+            e0.record(stream)
+            lat.advance(args.steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        barrier(pg)
+        ms = e0.elapsed_time(e1)
+        ms_max = max_over_ranks(pg, ms)
+        ms_step = ms_max / args.steps
+        mlups = world * lups * args.steps / (ms_max * 1e-3) / 1e6
+        bytes_per_lu = 152 if prec == ob.FP32 else 76
+        results[prec_name] = {"mlups": mlups, "ms_step": ms_step, "launches": launches,
+                              "bytes_per_lu": bytes_per_lu, "clocks": cs.summary(), "lups": lups}
+        # e2e: the same job through the C ABI from host memory
+        if prec_name == args.precision:
+            pinned = torch.from_numpy(np.ascontiguousarray(init.reshape(-1))).pin_memory()
+            init_host = pinned.numpy()
+            e2e_steps = args.steps
+            torch.cuda.synchronize()
+            barrier(pg)
+            t0 = time.perf_counter()
+            lat.set_populations(init_host)
+            lat.advance(e2e_steps)
+            rho, u = lat.get_fields()
+            t1 = time.perf_counter()
+            e2e_s = max_over_ranks(pg, t1 - t0)
+            results["e2e"] = {"value": world * lups * e2e_steps / e2e_s / 1e6, "unit": "MLUPS",
+                              "h2d_bytes_per_step": int(init_host.nbytes / e2e_steps),
+                              "d2h_bytes_per_step": int((rho.nbytes + u.nbytes) / e2e_steps),
+                              "steps": e2e_steps, "seconds": e2e_s}
+        lat.close()
+        del lat
+        torch.cuda.empty_cache()
+
+    main_r = results[args.precision]
+    peak, peak_kind = measured_peak()
+    # algorithmic bytes of one launch (per GPU) / average launch time
+    achieved = main_r["bytes_per_lu"] * main_r["lups"] / (main_r["ms_step"] * 1e-3) / 1e9
+    key = f"k_step_periodic_{args.precision}_{n}"
+    traffic = committed_traffic(key)
+    out = {
+        "metric": "MLUPS", "value": main_r["mlups"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": main_r["ms_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"tgv_periodic_{n}^3", "cells": n ** 3, "tau": 0.55, "u0": 0.05,
+                   "storage": args.precision, "parallelism": f"replicas{world}",
+                   "l2": "lattice 2x{:.2f} GB > L2, no flush".format(n ** 3 * 19 * (4 if args.precision == 'fp32' else 2) / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "bytes_per_lu": main_r["bytes_per_lu"], "peak_kind": peak_kind},
+        "gpu_launches": int(main_r["launches"] * args.steps),
+        "clocks": main_r["clocks"],
+        "e2e": {k: v for k, v in results["e2e"].items() if k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step")},
+        "fp16_shifted": {"mlups": results["fp16"]["mlups"], "ms_per_step": results["fp16"]["ms_step"],
+                         "bytes_per_lu": 76, "speedup_vs_fp32": results["fp16"]["mlups"] / results["fp32"]["mlups"]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_reference_mlups(n, steps_budget_s=args.ref_seconds)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,141 @@
+/* octlb_gpu.h -- C ABI of the B200 (sm_100a) per-level LBM time step.
+ *
+ * This is the drop-in boundary for OctLB's per-level time step: one context
+ * holds, on one GPU, every octree level's blocks (SoA populations in HBM), the
+ * flattened topology the reference keeps in FacePairList / GhostSchedule /
+ * LevelCoupler, and the TimeLoop recursion.  Plain C99: no C++ or torch types,
+ * no exceptions across the boundary.  0 = OK, negative = error; the message of
+ * the last error is available from octlb_gpu_last_error().
+ *
+ * Reference interfaces each entry point replaces (paths in gezengran/octlb):
+ *   octlb_gpu_create    TimeLoop ctor + BlockCollection factory + GhostSchedule
+ *                       ctor + LevelCoupler ctor + BouzidiLinkData
+ *                       (src/solver/lbm/time_loop/time_loop.h:49-54,123-164;
+ *                        src/solver/field/ghost_schedule.h:23-119;
+ *                        src/solver/lbm/level_coupler.cpp:216-307;
+ *                        src/solver/lbm/bouzidi_link_data.cpp:107-137)
+ *   octlb_gpu_advance   TimeLoop::advance_one (time_loop.h:242-246), n times
+ *   octlb_gpu_force     MomentumExchangeDrag::force_on_fluid_if summed over
+ *                       blocks (src/solver/lbm/drag_postprocessor.h:67-115,
+ *                        examples/cylinder3d/cylinder3d_case.h:473-517)
+ *   octlb_gpu_audit     Cylinder3dCase::total_mass (cylinder3d_case.h:601-622)
+ *                       plus total momentum
+ *   octlb_gpu_get_fields / _get_populations / _set_populations
+ *                       BlockLattice::get(...).computeRhoU and direct
+ *                       population access (block_lattice.h:113-125,226-256)
+ *   octlb_gpu_counters  TimeLoop::counters (time_loop.h:30-34,76)
+ */
+#ifndef OCTLB_GPU_H_
+#define OCTLB_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OCTLB_OK 0
+#define OCTLB_EINVAL (-1)   /* table / argument validation failed */
+#define OCTLB_ENOMEM (-2)   /* device allocation failed */
+#define OCTLB_ECUDA (-3)    /* CUDA runtime error */
+#define OCTLB_ENAN (-4)     /* non-finite populations detected (audit) */
+#define OCTLB_ESTATE (-6)   /* call not valid in the context's state */
+
+/* Population storage.  FP32 stores the shifted populations f - w as float;
+ * FP16_SHIFTED stores (f - w) * scale[level] as IEEE half.  Arithmetic is
+ * FP32 in both; audits and forces accumulate in FP64. */
+#define OCTLB_FP32 0
+#define OCTLB_FP16_SHIFTED 1
+
+/* Stream rule (reference BlockLattice::stream, block_lattice.cpp:554-557):
+ * ROTATE = no link table attached (every padded slot is torus-pulled);
+ * LINKS = a BouzidiLinkData is attached (per-cell pull with half-way
+ * bounce-back / Bouzidi on solid sources, default q = 1). */
+#define OCTLB_STREAM_ROTATE 0
+#define OCTLB_STREAM_LINKS 1
+
+/* Tree-boundary face conditions (restated; applied as halo fills before the
+ * same-level exchange, i.e. at DomainBoundaryHandler::apply()). */
+#define OCTLB_TB_NONE 0
+#define OCTLB_TB_WALL 1     /* half-way bounce-back wall, optionally moving */
+#define OCTLB_TB_OUTFLOW 2  /* zero-gradient ghost copy (outflow_bc.h:15-21) */
+
+/* Flattened mesh + per-cell data.  All arrays are host memory owned by the
+ * caller and copied at create.  Cell order inside a block is the reference's
+ * (ix * n + iy) * n + iz (block_lattice.h:290-296). */
+typedef struct octlb_tables {
+  int n;                          /* cells per block edge (even) */
+  int n_blocks;                   /* leaves (OctantId 0..n_blocks-1) */
+  const int* levels;              /* [n_blocks] quadrant level */
+  const double* bounds;           /* [n_blocks][6] xmin,ymin,zmin,xmax,ymax,zmax */
+  const uint8_t* kinds;           /* [n_blocks][n^3] BcKind (bc_kind.h:14-23) */
+  int n_same_level;               /* FacePairList::same_level_faces() */
+  const int* same_level;          /* [n][3] local_id, dir, remote_id */
+  int n_coarse_fine;              /* FacePairList::coarse_fine_faces() */
+  const int* coarse_fine;         /* [n][8] coarse, fine0..3, normal, clevel, flevel */
+  const double* coarse_fine_bounds; /* [n][30] coarse box, then 4 fine boxes */
+  int n_tree_boundary;            /* FacePairList::tree_boundary_faces() */
+  const int* tree_boundary;       /* [n][2] octant_id, face_dir */
+  const double* tree_boundary_spec; /* [n][8] type, u[3], prof_axis, lo, hi, 0 */
+  int n_links;                    /* Bouzidi cut links (q in (0,1)) */
+  const int* link_cells;          /* [n][5] octant, ix, iy, iz, pop */
+  const double* link_q;           /* [n] fractional link length q */
+  const uint8_t* moving;          /* [n_blocks][n^3] moving solid cells or NULL */
+  const double* wall_u;           /* [n_blocks][n^3][3] their velocity or NULL */
+  const uint8_t* obstacle;        /* [n_blocks][n^3] MEM obstacle mask or NULL */
+  int periodic;                   /* 1: single block, periodic in x, y, z */
+} octlb_tables;
+
+typedef struct octlb_params {
+  double omega;                   /* one global BGK rate (time_loop.h:183-187) */
+  int precision;                  /* OCTLB_FP32 or OCTLB_FP16_SHIFTED */
+  int stream_mode;                /* OCTLB_STREAM_ROTATE or OCTLB_STREAM_LINKS */
+  int drag;                       /* 1: MEM force every coarse step */
+  double fp16_scale[32];          /* per-level scale; 0 = default 2^16 */
+} octlb_params;
+
+typedef struct octlb_ctx octlb_ctx;
+
+/* init_pops: [n_blocks][n^3][19] shifted populations (the reference state
+ * before a step), or NULL for equilibrium at rho = 1, u = 0. */
+int octlb_gpu_create(const octlb_tables* tables, const octlb_params* params,
+                     const double* init_pops, octlb_ctx** out);
+void octlb_gpu_destroy(octlb_ctx* ctx);
+const char* octlb_gpu_last_error(const octlb_ctx* ctx);
+
+/* Bind the context to a caller's cudaStream_t (NULL = the context's own). */
+int octlb_gpu_set_stream(octlb_ctx* ctx, void* cuda_stream);
+
+/* n_coarse_steps x TimeLoop::advance_one(), asynchronously on the stream. */
+int octlb_gpu_advance(octlb_ctx* ctx, int n_coarse_steps);
+int octlb_gpu_synchronize(octlb_ctx* ctx);
+
+/* Reference state f (post-stream, pre-collision) -> context; the next step
+ * starts by colliding it. */
+int octlb_gpu_set_populations(octlb_ctx* ctx, const double* pops);
+/* Post-collision populations the next stream reads (what the reference's
+ * take_post_collide_snapshot holds after the next collide), core cells. */
+int octlb_gpu_get_populations(octlb_ctx* ctx, double* pops);
+/* rho [n_blocks][n^3] and u [n_blocks][n^3][3] of every core cell. */
+int octlb_gpu_get_fields(octlb_ctx* ctx, double* rho, double* u);
+
+/* MEM force on the fluid after the last coarse step, FP64. */
+int octlb_gpu_force(octlb_ctx* ctx, double out[3]);
+/* Sum of that force over every coarse step since create / reset, and count. */
+int octlb_gpu_force_sum(octlb_ctx* ctx, double out[3], long long* steps);
+int octlb_gpu_force_reset(octlb_ctx* ctx);
+/* out[0] = sum rho, out[1..3] = sum rho u over kBulk core cells (FP64);
+ * returns OCTLB_ENAN if any population is not finite. */
+int octlb_gpu_audit(octlb_ctx* ctx, double out[4]);
+
+/* Per-level collide / stream counts and max level (TimeLoop::counters). */
+int octlb_gpu_counters(const octlb_ctx* ctx, int* collide, int* stream, int max_levels);
+int octlb_gpu_max_level(const octlb_ctx* ctx);
+/* Kernel launches one coarse step issues, and lattice updates it performs. */
+int octlb_gpu_step_stats(const octlb_ctx* ctx, long long* launches, long long* lattice_updates);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

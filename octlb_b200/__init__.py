@@ -1,0 +1,299 @@
+"""octlb_b200 -- B200 (sm_100a) per-level time step of OctLB.
+
+Host mirror of the reference's solver entry points for this path:
+
+* ``Forest``        -- OctreeForest + FacePairList (p4est in the reference):
+                       brick of trees, refine, 2:1 balance, flattened faces.
+* ``Mesh``          -- the flattened tables octlb_gpu_create consumes
+                       (leaves, BcKind per cell, faces, Bouzidi links, ...).
+* ``GpuLattice``    -- one GPU context: every level's SoA populations plus the
+                       flattened GhostSchedule / LevelCoupler tables.
+* ``GpuTimeLoop``   -- the reference TimeLoop's method names
+                       (src/solver/lbm/time_loop/time_loop.h:47-121) over a
+                       GpuLattice.
+
+All compute runs in the in-tree CUDA library liboctlb_b200.so; importing this
+package without it raises ImportError.
+"""
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .capi import (BULK, SOLID, BOUNCE_BACK, MOVING_BOUNCE_BACK, BOUZIDI, VELOCITY_DIRICHLET,
+                   PRESSURE_DIRICHLET, OUTFLOW, FP32, FP16_SHIFTED, STREAM_ROTATE, STREAM_LINKS,
+                   TB_NONE, TB_WALL, TB_OUTFLOW, OctlbError)
+
+capi.lib()  # fail loudly at import when the library is missing
+
+Q = 19
+# D3Q19 in the reference's population order (descriptor/definition/common.h:165-197)
+C = np.array([[0, 0, 0], [-1, 0, 0], [0, -1, 0], [0, 0, -1], [-1, -1, 0], [-1, 1, 0], [-1, 0, -1],
+              [-1, 0, 1], [0, -1, -1], [0, -1, 1], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 0],
+              [1, -1, 0], [1, 0, 1], [1, 0, -1], [0, 1, 1], [0, 1, -1]], dtype=np.int64)
+OPP = np.array([0, 10, 11, 12, 13, 14, 15, 16, 17, 18, 1, 2, 3, 4, 5, 6, 7, 8, 9])
+W = np.array([1 / 3] + [1 / 18] * 3 + [1 / 36] * 6 + [1 / 18] * 3 + [1 / 36] * 6)
+
+
+def feq(rho, u):
+    """Shifted second-order equilibrium f_eq - w (dynamics/lbm.h:50-64).
+
+    rho: (...), u: (..., 3) -> (..., 19)."""
+    rho = np.asarray(rho, dtype=np.float64)
+    u = np.asarray(u, dtype=np.float64)
+    cu = np.einsum("...d,qd->...q", u, C.astype(np.float64))
+    usq = np.sum(u * u, axis=-1)[..., None]
+    return rho[..., None] * W * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq) - W
+
+
+class Forest:
+    """Brick of octrees with refinement and 2:1 balance (include/octlb_forest.h)."""
+
+    def __init__(self, bricks=(1, 1, 1), periodic=(0, 0, 0), domain=(0, 0, 0, 1, 1, 1)):
+        self._L = capi.lib()
+        dom = np.asarray(domain, dtype=np.float64)
+        self._h = self._L.octlb_forest_new(*[int(b) for b in bricks], *[int(p) for p in periodic],
+                                           capi.ptr(dom, ctypes.c_double))
+        if not self._h:
+            raise ValueError("invalid brick")
+        self.bricks, self.periodic, self.domain = tuple(bricks), tuple(periodic), tuple(domain)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._L.octlb_forest_free(self._h)
+            self._h = None
+
+    def refine_uniform(self, level):
+        self._L.octlb_forest_refine_uniform(self._h, int(level))
+        return self
+
+    def refine_box(self, box, level):
+        b = np.asarray(box, dtype=np.float64)
+        self._L.octlb_forest_refine_box(self._h, capi.ptr(b, ctypes.c_double), int(level))
+        return self
+
+    def balance(self):
+        self._L.octlb_forest_balance(self._h)
+        return self
+
+    def build(self):
+        L, h = self._L, self._h
+        n = L.octlb_forest_build(h)
+        self.levels = np.zeros(n, np.int32)
+        self.bounds = np.zeros((n, 6), np.float64)
+        L.octlb_forest_leaves(h, capi.ptr(self.levels, ctypes.c_int), capi.ptr(self.bounds, ctypes.c_double))
+        ns = L.octlb_forest_num_same_level(h)
+        self.same_level = np.zeros((ns, 3), np.int32)
+        L.octlb_forest_same_level(h, capi.ptr(self.same_level, ctypes.c_int))
+        nc = L.octlb_forest_num_coarse_fine(h)
+        self.coarse_fine = np.zeros((nc, 8), np.int32)
+        self.coarse_fine_bounds = np.zeros((nc, 30), np.float64)
+        L.octlb_forest_coarse_fine(h, capi.ptr(self.coarse_fine, ctypes.c_int),
+                                   capi.ptr(self.coarse_fine_bounds, ctypes.c_double))
+        nt = L.octlb_forest_num_tree_boundary(h)
+        self.tree_boundary = np.zeros((nt, 2), np.int32)
+        L.octlb_forest_tree_boundary(h, capi.ptr(self.tree_boundary, ctypes.c_int))
+        return self
+
+    @property
+    def num_leaves(self):
+        return len(self.levels)
+
+
+class Mesh:
+    """Flattened tables for octlb_gpu_create (octlb_tables).
+
+    Cell arrays are [block][ix][iy][iz] (the reference's block order)."""
+
+    def __init__(self, n, levels, bounds, kinds=None, same_level=None, coarse_fine=None,
+                 coarse_fine_bounds=None, tree_boundary=None, tree_boundary_spec=None,
+                 link_cells=None, link_q=None, moving=None, wall_u=None, obstacle=None, periodic=0):
+        self.n = int(n)
+        self.levels = np.ascontiguousarray(levels, dtype=np.int32)
+        nb = len(self.levels)
+        self.bounds = np.ascontiguousarray(bounds, dtype=np.float64).reshape(nb, 6)
+        shape = (nb, self.n, self.n, self.n)
+        self.kinds = np.zeros(shape, np.uint8) if kinds is None else np.ascontiguousarray(kinds, np.uint8).reshape(shape)
+        self.same_level = np.zeros((0, 3), np.int32) if same_level is None else np.ascontiguousarray(same_level, np.int32).reshape(-1, 3)
+        self.coarse_fine = np.zeros((0, 8), np.int32) if coarse_fine is None else np.ascontiguousarray(coarse_fine, np.int32).reshape(-1, 8)
+        self.coarse_fine_bounds = (np.zeros((len(self.coarse_fine), 30)) if coarse_fine_bounds is None
+                                   else np.ascontiguousarray(coarse_fine_bounds, np.float64).reshape(-1, 30))
+        self.tree_boundary = np.zeros((0, 2), np.int32) if tree_boundary is None else np.ascontiguousarray(tree_boundary, np.int32).reshape(-1, 2)
+        self.tree_boundary_spec = (np.zeros((len(self.tree_boundary), 8)) if tree_boundary_spec is None
+                                   else np.ascontiguousarray(tree_boundary_spec, np.float64).reshape(-1, 8))
+        self.link_cells = np.zeros((0, 5), np.int32) if link_cells is None else np.ascontiguousarray(link_cells, np.int32).reshape(-1, 5)
+        self.link_q = np.zeros(0) if link_q is None else np.ascontiguousarray(link_q, np.float64).reshape(-1)
+        self.moving = None if moving is None else np.ascontiguousarray(moving, np.uint8).reshape(shape)
+        self.wall_u = None if wall_u is None else np.ascontiguousarray(wall_u, np.float64).reshape(shape + (3,))
+        self.obstacle = None if obstacle is None else np.ascontiguousarray(obstacle, np.uint8).reshape(shape)
+        self.periodic = int(periodic)
+
+    @classmethod
+    def from_forest(cls, forest, n, **kw):
+        return cls(n, forest.levels, forest.bounds, same_level=forest.same_level,
+                   coarse_fine=forest.coarse_fine, coarse_fine_bounds=forest.coarse_fine_bounds,
+                   tree_boundary=forest.tree_boundary, **kw)
+
+    @property
+    def n_blocks(self):
+        return len(self.levels)
+
+    def cells_per_level(self):
+        out = {}
+        for l in self.levels:
+            out[int(l)] = out.get(int(l), 0) + self.n ** 3
+        return out
+
+    def lattice_updates_per_coarse_step(self):
+        """sum over levels of cells x 2^level (TimeLoop recursion from level 0)."""
+        return sum(c << l for l, c in self.cells_per_level().items())
+
+    def c_tables(self):
+        t = capi.Tables()
+        t.n, t.n_blocks = self.n, self.n_blocks
+        t.levels = capi.ptr(self.levels, ctypes.c_int)
+        t.bounds = capi.ptr(self.bounds, ctypes.c_double)
+        t.kinds = capi.ptr(self.kinds, ctypes.c_uint8)
+        t.n_same_level, t.same_level = len(self.same_level), capi.ptr(self.same_level, ctypes.c_int)
+        t.n_coarse_fine = len(self.coarse_fine)
+        t.coarse_fine = capi.ptr(self.coarse_fine, ctypes.c_int)
+        t.coarse_fine_bounds = capi.ptr(self.coarse_fine_bounds, ctypes.c_double)
+        t.n_tree_boundary = len(self.tree_boundary)
+        t.tree_boundary = capi.ptr(self.tree_boundary, ctypes.c_int)
+        t.tree_boundary_spec = capi.ptr(self.tree_boundary_spec, ctypes.c_double)
+        t.n_links = len(self.link_q)
+        t.link_cells = capi.ptr(self.link_cells, ctypes.c_int)
+        t.link_q = capi.ptr(self.link_q, ctypes.c_double)
+        t.moving = capi.ptr(self.moving, ctypes.c_uint8)
+        t.wall_u = capi.ptr(self.wall_u, ctypes.c_double)
+        t.obstacle = capi.ptr(self.obstacle, ctypes.c_uint8)
+        t.periodic = self.periodic
+        return t
+
+
+class GpuLattice:
+    """One octlb_gpu context (include/octlb_gpu.h)."""
+
+    def __init__(self, mesh, omega, precision=FP32, stream_mode=STREAM_ROTATE, drag=False,
+                 init_pops=None, fp16_scale=None):
+        self._L = capi.lib()
+        self.mesh = mesh
+        self.omega = float(omega)
+        self.precision = precision
+        p = capi.Params()
+        p.omega, p.precision, p.stream_mode, p.drag = float(omega), int(precision), int(stream_mode), int(bool(drag))
+        if fp16_scale is not None:
+            sc = np.broadcast_to(np.asarray(fp16_scale, dtype=np.float64), (32,))
+            for i in range(32):
+                p.fp16_scale[i] = float(sc[i])
+        self._init = None if init_pops is None else np.ascontiguousarray(init_pops, np.float64)
+        if self._init is not None:
+            assert self._init.size == mesh.n_blocks * mesh.n ** 3 * Q
+        h = capi.P()
+        rc = self._L.octlb_gpu_create(ctypes.byref(mesh.c_tables()), ctypes.byref(p),
+                                      capi.ptr(self._init, ctypes.c_double), ctypes.byref(h))
+        self._h = h
+        if rc != 0:
+            msg = self._L.octlb_gpu_last_error(h).decode() if h else "create failed"
+            self.close()
+            raise OctlbError(rc, msg)
+
+    def _check(self, rc):
+        if rc != 0:
+            raise OctlbError(rc, self._L.octlb_gpu_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.octlb_gpu_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def set_stream(self, cuda_stream_ptr):
+        self._check(self._L.octlb_gpu_set_stream(self._h, capi.P(cuda_stream_ptr) if cuda_stream_ptr else None))
+
+    def advance(self, n=1):
+        self._check(self._L.octlb_gpu_advance(self._h, int(n)))
+
+    def synchronize(self):
+        self._check(self._L.octlb_gpu_synchronize(self._h))
+
+    def _cells(self):
+        return self.mesh.n_blocks * self.mesh.n ** 3
+
+    def get_populations(self):
+        out = np.zeros((self._cells(), Q))
+        self._check(self._L.octlb_gpu_get_populations(self._h, capi.ptr(out, ctypes.c_double)))
+        n = self.mesh.n
+        return out.reshape(self.mesh.n_blocks, n, n, n, Q)
+
+    def set_populations(self, pops):
+        a = np.ascontiguousarray(pops, np.float64)
+        assert a.size == self._cells() * Q
+        self._check(self._L.octlb_gpu_set_populations(self._h, capi.ptr(a, ctypes.c_double)))
+
+    def get_fields(self):
+        rho = np.zeros(self._cells())
+        u = np.zeros((self._cells(), 3))
+        self._check(self._L.octlb_gpu_get_fields(self._h, capi.ptr(rho, ctypes.c_double), capi.ptr(u, ctypes.c_double)))
+        n = self.mesh.n
+        return rho.reshape(self.mesh.n_blocks, n, n, n), u.reshape(self.mesh.n_blocks, n, n, n, 3)
+
+    def force(self):
+        out = np.zeros(3)
+        self._check(self._L.octlb_gpu_force(self._h, capi.ptr(out, ctypes.c_double)))
+        return out
+
+    def force_sum(self):
+        out = np.zeros(3)
+        steps = ctypes.c_longlong(0)
+        self._check(self._L.octlb_gpu_force_sum(self._h, capi.ptr(out, ctypes.c_double), ctypes.byref(steps)))
+        return out, steps.value
+
+    def force_reset(self):
+        self._check(self._L.octlb_gpu_force_reset(self._h))
+
+    def audit(self):
+        out = np.zeros(4)
+        self._check(self._L.octlb_gpu_audit(self._h, capi.ptr(out, ctypes.c_double)))
+        return out
+
+    def counters(self):
+        c = np.zeros(32, np.int32)
+        s = np.zeros(32, np.int32)
+        nl = self._L.octlb_gpu_counters(self._h, capi.ptr(c, ctypes.c_int), capi.ptr(s, ctypes.c_int), 32)
+        return c[:nl].tolist(), s[:nl].tolist()
+
+    def max_level(self):
+        return self._L.octlb_gpu_max_level(self._h)
+
+    def step_stats(self):
+        a, b = ctypes.c_longlong(0), ctypes.c_longlong(0)
+        self._check(self._L.octlb_gpu_step_stats(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+
+class GpuTimeLoop:
+    """Reference TimeLoop interface (time_loop.h:47-121) over a GpuLattice."""
+
+    def __init__(self, lattice):
+        self.lattice = lattice
+        self._snapshot = False
+
+    def advance_one(self):
+        self.lattice.advance(1)
+
+    def max_level(self):
+        return self.lattice.max_level()
+
+    def counters(self):
+        c, s = self.lattice.counters()
+        return {"collide": c, "stream": s}
+
+    def set_snapshot_post_collide(self, on):
+        # The momentum-exchange force always reads the post-collide state the
+        # step consumed; nothing extra is copied.
+        self._snapshot = bool(on)
+
+    def snapshot_post_collide(self):
+        return self._snapshot

@@ -1,0 +1,179 @@
+"""Case builders: the callers of the per-level step (the reference's
+examples/cavity3d and examples/cylinder3d drivers play this role).
+
+Each builder returns (mesh, init_pops, info) with synthetic, seeded inputs of
+the shapes the benchmark configurations name:
+
+* ``tgv_periodic``   periodic box, Taylor-Green vortex initial condition
+* ``cavity_shell``   lid-driven cavity as one block with a solid shell and a
+                     moving top layer (half-way bounce-back + moving-wall term)
+* ``cavity_forest``  lid-driven cavity on an octree forest with tree-boundary
+                     walls (optionally a refined band under the lid)
+* ``cylinder_forest`` channel flow past a cylinder: exact-circle Bouzidi q,
+                     parabolic inlet, zero-gradient outlet, refinement near the
+                     cylinder
+"""
+import math
+
+import numpy as np
+
+from . import (Forest, Mesh, Q, C, feq, BULK, SOLID, BOUZIDI, TB_WALL, TB_OUTFLOW)
+
+
+def tgv_fields(nx, ny, nz, u0):
+    """Taylor-Green vortex on an nx*ny*nz periodic box, k = 2 pi / n per axis."""
+    x = (np.arange(nx) + 0.5) * 2 * math.pi / nx
+    y = (np.arange(ny) + 0.5) * 2 * math.pi / ny
+    z = (np.arange(nz) + 0.5) * 2 * math.pi / nz
+    X, Y, Z = np.meshgrid(x, y, z, indexing="ij")
+    u = np.stack([u0 * np.sin(X) * np.cos(Y) * np.cos(Z),
+                  -u0 * np.cos(X) * np.sin(Y) * np.cos(Z),
+                  np.zeros_like(X)], axis=-1)
+    p = u0 * u0 / 16.0 * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0)
+    rho = 1.0 + 3.0 * p
+    return rho, u
+
+
+def tgv_periodic(n, u0=0.05, tau=0.55):
+    rho, u = tgv_fields(n, n, n, u0)
+    mesh = Mesh(n, [0], [0, 0, 0, 1, 1, 1], periodic=1)
+    init = feq(rho, u).reshape(1, n, n, n, Q)
+    return mesh, init, {"omega": 1.0 / tau, "tau": tau}
+
+
+def cavity_shell(n=32, lid=0.1, tau=0.6):
+    """(n+2)^3 block: solid shell, fluid n^3, top (+y) shell layer moves with
+    (lid, 0, 0).  Links stream rule with q = 1 everywhere (half-way
+    bounce-back), the moving-wall term on links pulled from the lid."""
+    m = n + 2
+    kinds = np.full((m, m, m), SOLID, np.uint8)
+    kinds[1:-1, 1:-1, 1:-1] = BULK
+    moving = np.zeros((m, m, m), np.uint8)
+    moving[:, -1, :] = 1
+    wall_u = np.zeros((m, m, m, 3))
+    wall_u[:, -1, :, 0] = lid
+    mesh = Mesh(m, [0], [0, 0, 0, 1, 1, 1], kinds=kinds[None], moving=moving[None], wall_u=wall_u[None])
+    init = np.zeros((1, m, m, m, Q))
+    return mesh, init, {"omega": 1.0 / tau, "tau": tau}
+
+
+def _tb_spec(forest, fn):
+    spec = np.zeros((len(forest.tree_boundary), 8))
+    for k, (b, d) in enumerate(forest.tree_boundary):
+        spec[k] = fn(int(b), int(d))
+    return spec
+
+
+def cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=0):
+    """Cavity of cells^3 base cells in blocks of n^3, walls on every tree
+    boundary, +y wall moving with (lid,0,0).  band_cells > 0 refines the top
+    band of that many base cells one level (2:1)."""
+    assert cells % n == 0
+    base = int(round(math.log2(cells // n)))
+    f = Forest((1, 1, 1), (0, 0, 0), (0, 0, 0, 1, 1, 1)).refine_uniform(base)
+    if band_cells:
+        h = band_cells / cells
+        f.refine_box((0, 1 - h, 0, 1, 1, 1), base + 1)
+    f.balance().build()
+
+    def spec(b, d):
+        if d == 3:
+            return [TB_WALL, lid, 0, 0, -1, 0, 0, 0]
+        return [TB_WALL, 0, 0, 0, -1, 0, 0, 0]
+
+    mesh = Mesh.from_forest(f, n, tree_boundary_spec=_tb_spec(f, spec))
+    init = np.zeros((mesh.n_blocks, n, n, n, Q))
+    return mesh, init, {"omega": 1.0 / tau, "tau": tau, "forest": f}
+
+
+def circle_links(mesh, center, radius, axis_free=2):
+    """Exact-circle Bouzidi q for every fluid cell whose D3Q19 source x - c_i
+    lies inside the circle (cylinder along `axis_free`): q solves
+    |x - t c_i - center| = R for the first t in (0, 1] (host FP64), in units
+    of the block's cell width.  Marks cells inside as SOLID in mesh.kinds."""
+    n = mesh.n
+    ax = [a for a in range(3) if a != axis_free]
+    cells, qs = [], []
+    for b in range(mesh.n_blocks):
+        bd = mesh.bounds[b]
+        dx = (bd[3] - bd[0]) / n
+        idx = np.arange(n)
+        ctr = [bd[a] + (idx + 0.5) * dx for a in range(3)]
+        X = np.meshgrid(*ctr, indexing="ij")
+        r2 = (X[ax[0]] - center[0]) ** 2 + (X[ax[1]] - center[1]) ** 2
+        inside = r2 < radius * radius
+        mesh.kinds[b][inside] = SOLID
+    for b in range(mesh.n_blocks):
+        bd = mesh.bounds[b]
+        dx = (bd[3] - bd[0]) / n
+        kinds = mesh.kinds[b]
+        fluid = np.argwhere(kinds != SOLID)
+        for (x, y, z) in fluid:
+            p = np.array([bd[0] + (x + 0.5) * dx, bd[1] + (y + 0.5) * dx, bd[2] + (z + 0.5) * dx])
+            for i in range(1, Q):
+                s = np.array([x, y, z]) - C[i]
+                if np.any(s < 0) or np.any(s >= n):
+                    continue
+                if kinds[s[0], s[1], s[2]] != SOLID:
+                    continue
+                # segment p -> p - c_i dx crosses the circle: solve |p - t d - c| = R
+                d = -C[i].astype(float) * dx
+                px, py = p[ax[0]] - center[0], p[ax[1]] - center[1]
+                dx_, dy_ = d[ax[0]], d[ax[1]]
+                a2 = dx_ * dx_ + dy_ * dy_
+                if a2 == 0.0:
+                    continue
+                b2 = 2 * (px * dx_ + py * dy_)
+                c2 = px * px + py * py - radius * radius
+                disc = b2 * b2 - 4 * a2 * c2
+                if disc < 0:
+                    continue
+                t = (-b2 - math.sqrt(disc)) / (2 * a2)
+                if 0.0 < t <= 1.0:
+                    cells.append((b, x, y, z, i))
+                    qs.append(t)
+    mesh.link_cells = np.asarray(cells, np.int32).reshape(-1, 5)
+    mesh.link_q = np.asarray(qs, np.float64)
+    return mesh
+
+
+def cylinder_forest(length=256, height=64, n=8, diameter=16.0, center=(64.0, 32.0), levels=3,
+                    refine_dist=None, u_max=0.05, re=100.0, periodic_z=True):
+    """Channel length x height x height finest cells, cylinder along z.
+
+    Level L-1 (finest) covers the box within refine_dist (default 2D) of the
+    cylinder surface; coarser levels elsewhere, 2:1 balanced.  Inlet -x:
+    moving wall with a parabolic profile in y (u_max at mid-height);
+    outlet +x: zero-gradient ghost copy; y walls: half-way bounce-back;
+    z periodic.  Returns mesh, initial state (rest), info with omega of the
+    finest level for Re = u_max D / nu."""
+    fine = 2 ** (levels - 1)
+    base_cells = height // fine            # coarsest cells across the height
+    assert base_cells % n == 0 and length % height == 0
+    bx = length // height
+    tree_cells = height                    # finest cells per tree edge
+    base_level = int(round(math.log2(base_cells // n)))
+    f = Forest((bx, 1, 1), (0, 0, 1 if periodic_z else 0), (0, 0, 0, float(length), float(height), float(height)))
+    f.refine_uniform(base_level)
+    rd = 2.0 * diameter if refine_dist is None else refine_dist
+    for k in range(1, levels):
+        dist = rd * (levels - k) / (levels - 1) + 0.0
+        r = diameter / 2 + dist
+        f.refine_box((center[0] - r, center[1] - r, -1, center[0] + r, center[1] + r, height + 1), base_level + k)
+    f.balance().build()
+
+    def spec(b, d):
+        if d == 0:
+            return [TB_WALL, u_max, 0, 0, 1, 0.0, float(height), 0]
+        if d == 1:
+            return [TB_OUTFLOW, 0, 0, 0, -1, 0, 0, 0]
+        return [TB_WALL, 0, 0, 0, -1, 0, 0, 0]
+
+    mesh = Mesh.from_forest(f, n, tree_boundary_spec=_tb_spec(f, spec))
+    circle_links(mesh, center, diameter / 2.0)
+    # obstacle mask for the momentum exchange: the cylinder's solid cells
+    mesh.obstacle = (mesh.kinds == SOLID).astype(np.uint8)
+    nu = u_max * diameter / re                  # finest-level lattice units
+    tau = 3.0 * nu + 0.5
+    init = np.zeros((mesh.n_blocks, n, n, n, Q))
+    return mesh, init, {"omega": 1.0 / tau, "tau": tau, "forest": f, "tree_cells": tree_cells}

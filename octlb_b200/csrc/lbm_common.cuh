@@ -1,0 +1,144 @@
+// Shared device/host definitions of the sm_100a per-level LBM step.
+//
+// D3Q19 lattice in the reference's population order
+// (src/solver/lbm/descriptor/definition/common.h:165-197): rest, the nine
+// "negative" velocities, then their opposites, opposite(i) = i +- 9.
+#pragma once
+
+#include <cstdint>
+#include <cuda_fp16.h>
+
+namespace octlb_gpu {
+
+constexpr int kQ = 19;
+
+__host__ __device__ constexpr int cx(int i) {
+  constexpr int t[kQ] = {0, -1, 0, 0, -1, -1, -1, -1, 0, 0, 1, 0, 0, 1, 1, 1, 1, 0, 0};
+  return t[i];
+}
+__host__ __device__ constexpr int cy(int i) {
+  constexpr int t[kQ] = {0, 0, -1, 0, -1, 1, 0, 0, -1, -1, 0, 1, 0, 1, -1, 0, 0, 1, 1};
+  return t[i];
+}
+__host__ __device__ constexpr int cz(int i) {
+  constexpr int t[kQ] = {0, 0, 0, -1, 0, 0, -1, 1, -1, 1, 0, 0, 1, 0, 0, 1, -1, 1, -1};
+  return t[i];
+}
+__host__ __device__ constexpr int opp(int i) { return i == 0 ? 0 : (i <= 9 ? i + 9 : i - 9); }
+// Weights t_i: 1/3 rest, 1/18 axis, 1/36 diagonal.
+__host__ __device__ constexpr float wf(int i) {
+  return i == 0 ? 1.0f / 3.0f : ((cx(i) != 0) + (cy(i) != 0) + (cz(i) != 0) == 1 ? 1.0f / 18.0f : 1.0f / 36.0f);
+}
+__host__ __device__ constexpr double wd(int i) {
+  return i == 0 ? 1.0 / 3.0 : ((cx(i) != 0) + (cy(i) != 0) + (cz(i) != 0) == 1 ? 1.0 / 18.0 : 1.0 / 36.0);
+}
+
+// BcKind codes (src/solver/lbm/bc_kind.h:14-23).
+enum : uint8_t {
+  kBulk = 0, kSolid = 1, kBounceBack = 2, kMovingBounceBack = 3,
+  kBouzidi = 4, kVelocityDirichlet = 5, kPressureDirichlet = 6, kOutflow = 7
+};
+// Per-slot flag byte on the device: bits 0-2 kind, then role bits.
+enum : uint8_t {
+  kKindMask = 0x07,
+  kFlagHalo = 0x08,     // padded halo slot (kind reads as kBulk)
+  kFlagLink = 0x10,     // core cell with a link record (q / moving-wall term)
+  kFlagSave = 0x20,     // save pre-collision populations (coupler source)
+};
+
+__host__ __device__ inline bool reflects_on_pull(int k) {
+  // BcKindReflectsOnPull (bc_kind.h:30-33)
+  return k == kVelocityDirichlet || k == kPressureDirichlet || k == kBouzidi;
+}
+
+// Unsigned 32-bit division by a runtime-invariant divisor via multiply-high
+// (round-up method of Granlund & Montgomery 1994).
+struct FastDiv {
+  uint32_t d, m, s;
+  FastDiv() : d(1), m(0), s(0) {}
+  explicit FastDiv(uint32_t div) : d(div) {
+    s = 0;
+    while ((1ull << s) < div) ++s;
+    m = static_cast<uint32_t>((((1ull << 32) * ((1ull << s) - div)) / div) + 1);
+  }
+  __host__ __device__ inline uint32_t div(uint32_t n) const {
+#ifdef __CUDA_ARCH__
+    const uint32_t t = __umulhi(n, m);
+#else
+    const uint32_t t = static_cast<uint32_t>((static_cast<uint64_t>(n) * m) >> 32);
+#endif
+    return static_cast<uint32_t>((static_cast<uint64_t>(t) + n) >> s);
+  }
+};
+
+// Population element access for the two storage types.
+template <typename T> struct Store;
+template <> struct Store<float> {
+  __device__ static inline float ld(const float* p, float) { return *p; }
+  __device__ static inline void st(float* p, float v, float) { *p = v; }
+};
+template <> struct Store<__half> {
+  __device__ static inline float ld(const __half* p, float inv_scale) {
+    return __half2float(*p) * inv_scale;
+  }
+  __device__ static inline void st(__half* p, float v, float scale) {
+    *p = __float2half_rn(v * scale);
+  }
+};
+
+// Shifted second-order equilibrium minus t_i, in the cancellation-free form
+// t_i (drho + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u^2)) with drho = rho - 1; equal to
+// rho t_i (1 + 3cu + 4.5cu^2 - 1.5u^2) - t_i (src/solver/lbm/dynamics/lbm.h:50-64).
+template <int I>
+__device__ __forceinline__ float feq_shifted(float drho, float rho, float ux, float uy, float uz,
+                                             float usq15) {
+  const float cu = cx(I) * ux + cy(I) * uy + cz(I) * uz;
+  return wf(I) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - usq15));
+}
+
+// In-register BGK (block_lattice.cpp:328-341): moments of the shifted
+// populations, rho = 1 + sum f, u = sum f c / rho, then f += omega (feq - f).
+template <int I = 0>
+__device__ __forceinline__ void bgk_apply(float (&f)[kQ], float omega, float drho, float rho,
+                                          float ux, float uy, float uz, float usq15) {
+  if constexpr (I < kQ) {
+    f[I] += omega * (feq_shifted<I>(drho, rho, ux, uy, uz, usq15) - f[I]);
+    bgk_apply<I + 1>(f, omega, drho, rho, ux, uy, uz, usq15);
+  }
+}
+__device__ __forceinline__ void moments(const float (&f)[kQ], float& drho, float& jx, float& jy,
+                                        float& jz) {
+  // Pairwise grouping of opposite directions keeps the sums short.
+  drho = f[0];
+  jx = 0.f; jy = 0.f; jz = 0.f;
+#pragma unroll
+  for (int i = 1; i < kQ; ++i) {
+    drho += f[i];
+    if (cx(i)) jx += cx(i) * f[i];
+    if (cy(i)) jy += cy(i) * f[i];
+    if (cz(i)) jz += cz(i) * f[i];
+  }
+}
+__device__ __forceinline__ void bgk(float (&f)[kQ], float omega) {
+  float drho, jx, jy, jz;
+  moments(f, drho, jx, jy, jz);
+  const float rho = 1.0f + drho;
+  const float inv = 1.0f / rho;
+  const float ux = jx * inv, uy = jy * inv, uz = jz * inv;
+  const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
+  bgk_apply(f, omega, drho, rho, ux, uy, uz, usq15);
+}
+
+// Bouzidi interpolated bounce-back with the reference's argument roles
+// (src/solver/lbm/boundary/bouzidi_pull.h:8-26); q in (0,1) guaranteed by the
+// caller (q = 1 means plain half-way bounce-back).
+__device__ __forceinline__ float bouzidi(float f_bb, float f_q, float f_same, float q) {
+  if (q >= 1.0f) return f_bb;
+  if (q >= 0.5f) {
+    const float inv2q = 0.5f / q;
+    return inv2q * f_bb + (1.0f - inv2q) * f_q;
+  }
+  return 2.0f * q * f_bb + (1.0f - 2.0f * q) * f_same;
+}
+
+}  // namespace octlb_gpu

@@ -1,0 +1,541 @@
+// sm_100a kernels of the per-level LBM time step.
+//
+//   k_step      fused pull-stream + BGK collide over one level (K1), with the
+//               reference's two stream rules (torus rotate / per-cell links
+//               with half-way bounce-back and Bouzidi, K2), moving-wall term,
+//               halo torus-stream of open blocks, and pre-collision save of
+//               coupler source cells.
+//   k_ghost     device ghost fill (K3): same-level face / edge exchange and
+//               tree-boundary halo fills, from flattened tables.
+//   k_prolong   Lagrava prolongation (K4), k_restrict Lagrava restriction (K5).
+//   k_drag      momentum-exchange force (K6), FP64 with warp shuffles.
+//   k_audit     FP64 mass / momentum audit and non-finite check.
+//
+// Storage is the shifted population g = f - w after collision ("post-collide"
+// state): one launch of k_step reads g_n, pulls f_{n+1} = S(g_n), and writes
+// g_{n+1} = C(f_{n+1}).  The reference's per-step order collide -> exchange ->
+// stream (time_loop.h:201-217) is therefore a ghost fill followed by k_step.
+#include <cstdio>
+
+#include "octlb_internal.h"
+
+namespace octlb_gpu {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ float LD(const T* base, long long qs, int i, long long slot, float inv) {
+  return Store<T>::ld(base + i * qs + slot, inv);
+}
+
+// Pull of direction i into core cell `slot` under the per-cell link rule
+// (block_lattice.cpp:613-672).  `fl` is the cell's flag byte, `li` its link
+// record or -1.  Called inside unrolled loops, so i folds to a constant.
+template <typename T>
+__device__ __forceinline__ float pull_link(const StepArgs& a, const T* src, long long slot,
+                                           uint8_t fl, int li, int i) {
+  const int kind = fl & kKindMask;
+  const long long s = slot - a.off[i];
+  const uint8_t sf = a.flags[s];
+  if (reflects_on_pull(kind) && (sf & kFlagHalo)) return LD(src, a.qs, opp(i), slot, a.inv_scale);
+  const int sk = (sf & kFlagHalo) ? kBulk : (sf & kKindMask);
+  if (sk == kSolid || sk == kBouzidi) {
+    float v;
+    const float q = li >= 0 ? a.link_rec[li * 38 + i] : 1.0f;
+    const float f_bb = LD(src, a.qs, opp(i), slot, a.inv_scale);
+    if (q < 1.0f) {
+      const float f_same = LD(src, a.qs, i, slot, a.inv_scale);
+      const long long nb = slot + a.off[i];
+      const uint8_t nf = a.flags[nb];
+      const int nk = (nf & kFlagHalo) ? kBulk : (nf & kKindMask);
+      const float f_q = nk == kBulk ? LD(src, a.qs, i, nb, a.inv_scale) : f_same;
+      v = bouzidi(f_bb, f_q, f_same, q);
+    } else {
+      v = f_bb;
+    }
+    if (li >= 0) v += a.link_rec[li * 38 + kQ + i];
+    return v;
+  }
+  return LD(src, a.qs, i, s, a.inv_scale);
+}
+
+template <typename T, bool PERIODIC, bool LINKS, bool FLAGS>
+__global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= a.nitems) return;
+  const T* src = static_cast<const T*>(a.src);
+  T* dst = static_cast<T*>(a.dst);
+  const uint32_t n = a.n;
+  float f[kQ];
+  if (t < a.ncore) {
+    const uint32_t b = a.div_n3.div(t);
+    uint32_t r = t - b * n * n * n;
+    const uint32_t x = a.div_n2.div(r);
+    r -= x * n * n;
+    const uint32_t y = a.div_n.div(r);
+    const uint32_t z = r - y * n;
+    long long slot;
+    uint8_t fl = 0;
+    if constexpr (PERIODIC) {
+      // One periodic block without halo: fill_periodic_halo + stream of the
+      // reference (block_lattice.cpp:918-964) is a wrapped pull.
+      slot = (static_cast<long long>(x) * n + y) * n + z;
+      if constexpr (FLAGS) fl = a.flags[slot];
+      const uint32_t xm = x == 0 ? n - 1 : x - 1, xp = x == n - 1 ? 0 : x + 1;
+      const uint32_t ym = y == 0 ? n - 1 : y - 1, yp = y == n - 1 ? 0 : y + 1;
+      const uint32_t zm = z == 0 ? n - 1 : z - 1, zp = z == n - 1 ? 0 : z + 1;
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) {
+        const uint32_t sx = cx(i) == 1 ? xm : (cx(i) == -1 ? xp : x);
+        const uint32_t sy = cy(i) == 1 ? ym : (cy(i) == -1 ? yp : y);
+        const uint32_t sz = cz(i) == 1 ? zm : (cz(i) == -1 ? zp : z);
+        f[i] = LD(src, a.qs, i, (static_cast<long long>(sx) * n + sy) * n + sz, a.inv_scale);
+      }
+    } else {
+      slot = b * a.bstride + ((x + 1) * a.np + (y + 1)) * a.np + (z + 1);
+      if constexpr (FLAGS) fl = a.flags[slot];
+      if constexpr (LINKS) {
+        if ((fl & kKindMask) == kSolid) {
+          // Solid cells are neither streamed nor collided (block_lattice.cpp:581-583).
+#pragma unroll
+          for (int i = 0; i < kQ; ++i) dst[i * a.qs + slot] = src[i * a.qs + slot];
+          return;
+        }
+        const int li = (fl & kFlagLink) ? a.link_idx[slot] : -1;
+#pragma unroll
+        for (int i = 0; i < kQ; ++i) f[i] = pull_link<T>(a, src, slot, fl, li, i);
+      } else {
+#pragma unroll
+        for (int i = 0; i < kQ; ++i) f[i] = LD(src, a.qs, i, slot - a.off[i], a.inv_scale);
+      }
+    }
+    if constexpr (FLAGS) {
+      if (fl & kFlagSave) {
+        float* sv = a.save_buf + static_cast<long long>(a.save_idx[slot]) * kQ;
+#pragma unroll
+        for (int i = 0; i < kQ; ++i) sv[i] = f[i];
+      }
+      if ((fl & kKindMask) == kBulk) bgk(f, a.omega);
+    } else {
+      bgk(f, a.omega);
+    }
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + slot, f[i], a.scale);
+  } else {
+    // Halo slot of an open block: torus pull over the padded block's linear
+    // index (block_lattice.h:70-89), no collision.
+    const uint32_t k = t - a.ncore;
+    const uint32_t ob = a.div_halo.div(k);
+    const uint32_t h = k - ob * a.n_halo;
+    const long long base = static_cast<long long>(a.open_blocks[ob]) * a.bstride;
+    const int loc = a.halo_map[h];
+    const int cells = static_cast<int>(a.bstride);
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      int s = loc - a.off[i];
+      s = s < 0 ? s + cells : (s >= cells ? s - cells : s);
+      dst[i * a.qs + base + loc] = src[i * a.qs + base + s];
+    }
+  }
+}
+
+// Ghost fill: copy descriptors first (one thread per cell of a region, all 19
+// populations), then single-population bounce-back writes.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_ghost(T* pops, long long qs, const CopyDesc* cd, const uint32_t* cd_start, int ncd,
+        uint32_t ncopy, const BBOp* bb, uint32_t nbb, float scale, float inv_scale) {
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  if (t < ncopy) {
+    int lo = 0, hi = ncd - 1;
+    while (lo < hi) {  // last descriptor whose start <= t
+      const int mid = (lo + hi + 1) >> 1;
+      if (cd_start[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const CopyDesc d = cd[lo];
+    const uint32_t k = t - cd_start[lo];
+    const int a0 = static_cast<int>(k / d.n1), a1 = static_cast<int>(k % d.n1);
+    const long long s = d.src + static_cast<long long>(a0) * d.s0 + static_cast<long long>(a1) * d.s1;
+    const long long o = d.dst + static_cast<long long>(a0) * d.d0 + static_cast<long long>(a1) * d.d1;
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) pops[i * qs + o] = pops[i * qs + s];
+    return;
+  }
+  const uint32_t u = t - ncopy;
+  if (u >= nbb) return;
+  const BBOp op = bb[u];
+  const float v = Store<T>::ld(pops + op.src_pop * qs + op.src, inv_scale) + op.add;
+  Store<T>::st(pops + op.pop * qs + op.dst, v, scale);
+}
+
+// Macro state (rho - 1, u, f_neq) of saved pre-collision populations
+// (LevelCoupler::ReadMacro, level_coupler.cpp:183-189).
+struct Macro {
+  float drho, ux, uy, uz;
+  float fneq[kQ];
+};
+__device__ inline void read_macro(const float* f, Macro& m) {
+  float fr[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) fr[i] = f[i];
+  float drho, jx, jy, jz;
+  moments(fr, drho, jx, jy, jz);
+  const float rho = 1.0f + drho, inv = 1.0f / rho;
+  m.drho = drho; m.ux = jx * inv; m.uy = jy * inv; m.uz = jz * inv;
+  const float usq15 = 1.5f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const float cu = cx(i) * m.ux + cy(i) * m.uy + cz(i) * m.uz;
+    m.fneq[i] = fr[i] - wf(i) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - usq15));
+  }
+}
+// feq(rho,u) + scale * f_neq (WriteProlongation, level_coupler.cpp:191-201),
+// then BGK if the target cell is kBulk: the written state is collided by the
+// next step of its level before it is streamed.
+__device__ inline void write_macro_cell(const Macro& m, float s, int kind, float omega, float (&f)[kQ]) {
+  const float rho = 1.0f + m.drho;
+  const float usq15 = 1.5f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const float cu = cx(i) * m.ux + cy(i) * m.uy + cz(i) * m.uz;
+    f[i] = wf(i) * (m.drho + rho * (3.0f * cu + 4.5f * cu * cu - usq15)) + s * m.fneq[i];
+  }
+  if (kind == kBulk) bgk(f, omega);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_prolong(const ProlongItem* items, int nitems, const float* coarse_save, float* prev, int half,
+          T* fine, long long fine_qs, float scale, float omega, float fscale) {
+  const int t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= nitems) return;
+  const ProlongItem it = items[t];
+  Macro m;
+  read_macro(coarse_save + static_cast<long long>(it.coarse_save) * kQ, m);
+  float* pv = prev + static_cast<long long>(it.prev) * 23;
+  Macro w = m;
+  if (half) {
+    // Half-time: average of previous and current coarse macros
+    // (level_coupler.cpp:455-465).
+    w.drho = 0.5f * (pv[0] + m.drho);
+    w.ux = 0.5f * (pv[1] + m.ux); w.uy = 0.5f * (pv[2] + m.uy); w.uz = 0.5f * (pv[3] + m.uz);
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) w.fneq[i] = 0.5f * (pv[4 + i] + m.fneq[i]);
+  } else {
+    // Full-time: prev <- current (level_coupler.cpp:470-476).
+    pv[0] = m.drho; pv[1] = m.ux; pv[2] = m.uy; pv[3] = m.uz;
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) pv[4 + i] = m.fneq[i];
+  }
+  float f[kQ];
+  write_macro_cell(w, scale, it.fine_kind, omega, f);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) Store<T>::st(fine + i * fine_qs + it.fine_slot, f[i], fscale);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_restrict(const RestrictItem* items, int nitems, const float* fine_save, T* coarse,
+           long long coarse_qs, float scale, float omega, float cscale) {
+  const int t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= nitems) return;
+  const RestrictItem& it = items[t];
+  Macro m;
+  read_macro(fine_save + static_cast<long long>(it.fine_save) * kQ, m);
+  float sum[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) sum[i] = 0.f;
+  for (int k = 0; k < it.nnb; ++k) {
+    Macro nm;
+    read_macro(fine_save + static_cast<long long>(it.nb_save[k]) * kQ, nm);
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) sum[i] += nm.fneq[i];
+  }
+  const float inv = 1.0f / static_cast<float>(it.nnb + 1);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) m.fneq[i] = (m.fneq[i] + sum[i]) * inv;
+  float f[kQ];
+  write_macro_cell(m, scale, it.coarse_kind, omega, f);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) Store<T>::st(coarse + i * coarse_qs + it.coarse_slot, f[i], cscale);
+}
+
+// FP64 block reduction of N doubles: warp shuffles, then one warp over the
+// per-warp partials; thread 0 returns the totals.
+template <int N>
+__device__ inline void block_reduce(double (&v)[N]) {
+  __shared__ double sm[kThreads / 32][N];
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < N; ++k) sm[wid][k] = v[k];
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      v[k] = lane < kThreads / 32 ? sm[lane][k] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    }
+  }
+}
+
+// Momentum-exchange force (drag_postprocessor.h:67-115) from the buffer the
+// last step read: f_out = g_i(x) is the post-collide snapshot, and the bounced
+// f_opp(x) is re-pulled from the same buffer with the step's own rule.
+template <typename T, bool LINKS>
+__global__ void __launch_bounds__(kThreads)
+k_drag(const StepArgs a, const DragItem* items, int nitems, double* partial) {
+  const int t = blockIdx.x * kThreads + threadIdx.x;
+  double acc[3] = {0.0, 0.0, 0.0};
+  if (t < nitems) {
+    const DragItem it = items[t];
+    const T* src = static_cast<const T*>(a.src);
+    const uint8_t fl = a.flags[it.slot];
+    const int li = (LINKS && (fl & kFlagLink)) ? a.link_idx[it.slot] : -1;
+#pragma unroll
+    for (int i = 1; i < kQ; ++i) {
+      if (!(it.mask & (1u << i))) continue;
+      const float f_out = LD(src, a.qs, i, it.slot, a.inv_scale);
+      float f_bar;
+      if constexpr (LINKS) {
+        f_bar = pull_link<T>(a, src, it.slot, fl, li, opp(i));
+      } else {
+        f_bar = LD(src, a.qs, opp(i), it.slot + a.off[i], a.inv_scale);
+      }
+      const double s = static_cast<double>(f_out) + static_cast<double>(f_bar);
+      acc[0] += s * cx(i); acc[1] += s * cy(i); acc[2] += s * cz(i);
+    }
+  }
+  block_reduce<3>(acc);
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x * 3 + 0] = -acc[0];
+    partial[blockIdx.x * 3 + 1] = -acc[1];
+    partial[blockIdx.x * 3 + 2] = -acc[2];
+  }
+}
+
+// Sum of per-CTA partials, `width` doubles each, by one CTA: fixed strided
+// per-thread sums then a fixed shuffle tree (deterministic).
+__global__ void __launch_bounds__(kThreads)
+k_sum_partials(const double* partial, int nparts, int width, double* out, double* accum) {
+  for (int k = 0; k < width; ++k) {
+    double v[1] = {0.0};
+    for (int p = threadIdx.x; p < nparts; p += kThreads) v[0] += partial[p * width + k];
+    block_reduce<1>(v);
+    if (threadIdx.x == 0) {
+      out[k] = v[0];
+      if (accum) accum[k] += v[0];
+    }
+    __syncthreads();
+  }
+}
+
+// Mass / momentum audit over kBulk core cells (total_mass,
+// cylinder3d_case.h:601-622) with a non-finite check over every core cell.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_audit(const StepArgs a, double* partial) {
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (t < a.ncore) {
+    const uint32_t n = a.n;
+    const uint32_t b = a.div_n3.div(t);
+    uint32_t r = t - b * n * n * n;
+    const uint32_t x = a.div_n2.div(r);
+    r -= x * n * n;
+    const uint32_t y = a.div_n.div(r);
+    const uint32_t z = r - y * n;
+    const long long slot = a.np == static_cast<int>(n)
+                               ? (static_cast<long long>(x) * n + y) * n + z
+                               : b * a.bstride + ((x + 1) * a.np + (y + 1)) * a.np + (z + 1);
+    const T* src = static_cast<const T*>(a.src);
+    float f[kQ];
+    bool finite = true;
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      f[i] = LD(src, a.qs, i, slot, a.inv_scale);
+      finite = finite && isfinite(f[i]);
+    }
+    const int kind = a.flags ? (a.flags[slot] & kKindMask) : kBulk;
+    if (!finite) acc[4] = 1.0;
+    if (kind == kBulk) {
+      double drho = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) {
+        drho += f[i]; jx += cx(i) * static_cast<double>(f[i]);
+        jy += cy(i) * static_cast<double>(f[i]); jz += cz(i) * static_cast<double>(f[i]);
+      }
+      acc[0] = 1.0 + drho; acc[1] = jx; acc[2] = jy; acc[3] = jz;
+    }
+  }
+  block_reduce<5>(acc);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 5; ++k) partial[blockIdx.x * 5 + k] = acc[k];
+}
+
+// Core cells <-> dense FP64 host order [block][ix][iy][iz][19].
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_gather(const StepArgs a, double* out, int mode /*0 pops, 1 fields*/) {
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= a.ncore) return;
+  const uint32_t n = a.n;
+  const uint32_t b = a.div_n3.div(t);
+  uint32_t r = t - b * n * n * n;
+  const uint32_t x = a.div_n2.div(r);
+  r -= x * n * n;
+  const uint32_t y = a.div_n.div(r);
+  const uint32_t z = r - y * n;
+  const long long slot = a.np == static_cast<int>(n)
+                             ? (static_cast<long long>(x) * n + y) * n + z
+                             : b * a.bstride + ((x + 1) * a.np + (y + 1)) * a.np + (z + 1);
+  const T* src = static_cast<const T*>(a.src);
+  if (mode == 0) {
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) out[static_cast<long long>(t) * kQ + i] = LD(src, a.qs, i, slot, a.inv_scale);
+  } else {
+    double drho = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      const double v = LD(src, a.qs, i, slot, a.inv_scale);
+      drho += v; jx += cx(i) * v; jy += cy(i) * v; jz += cz(i) * v;
+    }
+    const double rho = 1.0 + drho;
+    out[static_cast<long long>(t) * 4 + 0] = rho;
+    out[static_cast<long long>(t) * 4 + 1] = jx / rho;
+    out[static_cast<long long>(t) * 4 + 2] = jy / rho;
+    out[static_cast<long long>(t) * 4 + 3] = jz / rho;
+  }
+}
+
+// Reference state f (pre-collision, FP64) -> stored g = C(f) for kBulk cells.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_scatter(const StepArgs a, const double* in) {
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= a.ncore) return;
+  const uint32_t n = a.n;
+  const uint32_t b = a.div_n3.div(t);
+  uint32_t r = t - b * n * n * n;
+  const uint32_t x = a.div_n2.div(r);
+  r -= x * n * n;
+  const uint32_t y = a.div_n.div(r);
+  const uint32_t z = r - y * n;
+  const long long slot = a.np == static_cast<int>(n)
+                             ? (static_cast<long long>(x) * n + y) * n + z
+                             : b * a.bstride + ((x + 1) * a.np + (y + 1)) * a.np + (z + 1);
+  float f[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) f[i] = static_cast<float>(in[static_cast<long long>(t) * kQ + i]);
+  const int kind = a.flags ? (a.flags[slot] & kKindMask) : kBulk;
+  if (kind == kBulk) bgk(f, a.omega);
+  T* dst = static_cast<T*>(a.dst);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + slot, f[i], a.scale);
+}
+
+inline uint32_t grid_for(uint32_t items) { return (items + kThreads - 1) / kThreads; }
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers
+template <typename T>
+cudaError_t launch_step(const StepArgs& a, bool periodic, bool links, bool flags, cudaStream_t s) {
+  if (a.nitems == 0) return cudaSuccess;
+  const dim3 g(grid_for(a.nitems));
+  if (periodic) {
+    if (flags) k_step<T, true, false, true><<<g, kThreads, 0, s>>>(a);
+    else k_step<T, true, false, false><<<g, kThreads, 0, s>>>(a);
+  } else if (links) {
+    k_step<T, false, true, true><<<g, kThreads, 0, s>>>(a);
+  } else {
+    k_step<T, false, false, true><<<g, kThreads, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_ghost(T* pops, long long qs, const CopyDesc* cd, const uint32_t* cd_start, int ncd,
+                         uint32_t ncopy, const BBOp* bb, uint32_t nbb, float scale, float inv_scale,
+                         cudaStream_t s) {
+  const uint32_t total = ncopy + nbb;
+  if (total == 0) return cudaSuccess;
+  k_ghost<T><<<grid_for(total), kThreads, 0, s>>>(pops, qs, cd, cd_start, ncd, ncopy, bb, nbb, scale,
+                                                  inv_scale);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_prolong(const ProlongItem* items, int n, const float* coarse_save, float* prev,
+                           int half, T* fine, long long fine_qs, float scale, float omega,
+                           float fscale, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_prolong<T><<<grid_for(n), kThreads, 0, s>>>(items, n, coarse_save, prev, half, fine, fine_qs,
+                                                scale, omega, fscale);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_restrict(const RestrictItem* items, int n, const float* fine_save, T* coarse,
+                            long long coarse_qs, float scale, float omega, float cscale,
+                            cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_restrict<T><<<grid_for(n), kThreads, 0, s>>>(items, n, fine_save, coarse, coarse_qs, scale,
+                                                 omega, cscale);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_drag(const StepArgs& a, bool links, const DragItem* items, int n, double* partial,
+                        double* out, double* accum, cudaStream_t s) {
+  const uint32_t g = grid_for(static_cast<uint32_t>(n > 0 ? n : 1));
+  if (links) k_drag<T, true><<<g, kThreads, 0, s>>>(a, items, n, partial);
+  else k_drag<T, false><<<g, kThreads, 0, s>>>(a, items, n, partial);
+  k_sum_partials<<<1, kThreads, 0, s>>>(partial, static_cast<int>(g), 3, out, accum);
+  return cudaGetLastError();
+}
+uint32_t drag_partials(int n) { return grid_for(static_cast<uint32_t>(n > 0 ? n : 1)); }
+
+template <typename T>
+cudaError_t launch_audit(const StepArgs& a, double* partial, double* out, cudaStream_t s) {
+  const uint32_t g = grid_for(a.ncore);
+  k_audit<T><<<g, kThreads, 0, s>>>(a, partial);
+  k_sum_partials<<<1, kThreads, 0, s>>>(partial, static_cast<int>(g), 5, out, nullptr);
+  return cudaGetLastError();
+}
+uint32_t audit_partials(const StepArgs& a) { return grid_for(a.ncore); }
+
+template <typename T>
+cudaError_t launch_gather(const StepArgs& a, double* out, int mode, cudaStream_t s) {
+  k_gather<T><<<grid_for(a.ncore), kThreads, 0, s>>>(a, out, mode);
+  return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) {
+  k_scatter<T><<<grid_for(a.ncore), kThreads, 0, s>>>(a, in);
+  return cudaGetLastError();
+}
+
+#define OCTLB_INST(T)                                                                              \
+  template cudaError_t launch_step<T>(const StepArgs&, bool, bool, bool, cudaStream_t);            \
+  template cudaError_t launch_ghost<T>(T*, long long, const CopyDesc*, const uint32_t*, int,       \
+                                       uint32_t, const BBOp*, uint32_t, float, float, cudaStream_t); \
+  template cudaError_t launch_prolong<T>(const ProlongItem*, int, const float*, float*, int, T*,   \
+                                         long long, float, float, float, cudaStream_t);            \
+  template cudaError_t launch_restrict<T>(const RestrictItem*, int, const float*, T*, long long,   \
+                                          float, float, float, cudaStream_t);                      \
+  template cudaError_t launch_drag<T>(const StepArgs&, bool, const DragItem*, int, double*,        \
+                                      double*, double*, cudaStream_t);                             \
+  template cudaError_t launch_audit<T>(const StepArgs&, double*, double*, cudaStream_t);           \
+  template cudaError_t launch_gather<T>(const StepArgs&, double*, int, cudaStream_t);              \
+  template cudaError_t launch_scatter<T>(const StepArgs&, const double*, cudaStream_t);
+
+OCTLB_INST(float)
+OCTLB_INST(__half)
+
+}  // namespace octlb_gpu

@@ -1,0 +1,1080 @@
+// Host side of the C ABI (include/octlb_gpu.h): flattens the forest tables
+// into per-level device tables, owns every device allocation, and drives the
+// reference's recursive subcycling (TimeLoop::advance, time_loop.h:201-240) as
+// a sequence of kernel launches on one stream.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "octlb_internal.h"
+#include "../../include/octlb_gpu.h"
+
+namespace octlb_gpu {
+
+template <typename T> cudaError_t launch_step(const StepArgs&, bool, bool, bool, cudaStream_t);
+template <typename T>
+cudaError_t launch_ghost(T*, long long, const CopyDesc*, const uint32_t*, int, uint32_t, const BBOp*,
+                         uint32_t, float, float, cudaStream_t);
+template <typename T>
+cudaError_t launch_prolong(const ProlongItem*, int, const float*, float*, int, T*, long long, float,
+                           float, float, cudaStream_t);
+template <typename T>
+cudaError_t launch_restrict(const RestrictItem*, int, const float*, T*, long long, float, float,
+                            float, cudaStream_t);
+template <typename T>
+cudaError_t launch_drag(const StepArgs&, bool, const DragItem*, int, double*, double*, double*,
+                        cudaStream_t);
+template <typename T> cudaError_t launch_audit(const StepArgs&, double*, double*, cudaStream_t);
+template <typename T> cudaError_t launch_gather(const StepArgs&, double*, int, cudaStream_t);
+template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*, cudaStream_t);
+uint32_t drag_partials(int n);
+uint32_t audit_partials(const StepArgs& a);
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+  ~DevBuf() { if (p) cudaFree(p); }
+  cudaError_t alloc(size_t b) {
+    if (p) { cudaFree(p); p = nullptr; }
+    bytes = b;
+    if (b == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) e = cudaMemset(p, 0, b);
+    return e;
+  }
+  template <typename U> U* as() const { return static_cast<U*>(p); }
+};
+
+template <typename U>
+cudaError_t upload(DevBuf& d, const std::vector<U>& h) {
+  cudaError_t e = d.alloc(h.size() * sizeof(U));
+  if (e != cudaSuccess || h.empty()) return e;
+  return cudaMemcpy(d.p, h.data(), h.size() * sizeof(U), cudaMemcpyHostToDevice);
+}
+
+struct PlanPoint {  // CouplingPoint (level_coupler.h:18-30)
+  int coarse_id, ci, cj, ck, fine_id, fi, fj, fk, normal, coarse_level, fine_level, slot;
+};
+
+struct Level {
+  int lvl = 0;
+  std::vector<int> blocks;          // global block ids, level-local order
+  int nblk = 0, n = 0, np = 0;
+  long long bstride = 0, nslots = 0;
+  DevBuf buf[2];
+  int cur = 0;
+  DevBuf flags, link_idx, link_rec, save_idx, save_buf, open_blocks, halo_map;
+  int n_open = 0, n_halo = 0, n_save = 0, n_links = 0;
+  bool has_flags = false;
+  // ghost fill
+  DevBuf copy_desc, copy_start, bb_ops;
+  int n_copy_desc = 0;
+  uint32_t n_copy_cells = 0, n_bb = 0;
+  // coupler: this level as coarse (prolong) and as fine (restrict)
+  DevBuf prolong_items, prev, restrict_items;
+  int n_prolong = 0, n_restrict = 0;
+  // drag
+  DevBuf drag_items, drag_partial;
+  int n_drag = 0;
+  float scale = 1.f, inv_scale = 1.f;
+  StepArgs args{};
+};
+
+}  // namespace
+}  // namespace octlb_gpu
+
+using namespace octlb_gpu;
+
+struct octlb_ctx {
+  std::string err;
+  int n = 0, n_blocks = 0, precision = 0, stream_mode = 0, periodic = 0, drag = 0;
+  double omega = 1.0;
+  int max_level = 0;
+  std::vector<Level> levels;
+  std::vector<int> blk_level, blk_local;
+  std::vector<uint8_t> kinds;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  DevBuf force_lvl, force, force_sum, audit_out, audit_partial, host_tmp;
+  long long force_steps = 0;
+  std::vector<int> counters_collide, counters_stream;
+  long long launches_per_step = 0, lups_per_step = 0;
+  float prolong_scale = 0.f, restrict_scale = 0.f;
+};
+
+namespace octlb_host {
+
+int fail(octlb_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+int cuda_fail(octlb_ctx* c, cudaError_t e, const char* where) {
+  return fail(c, OCTLB_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);       \
+  } while (0)
+
+inline long long slot_of(const Level& L, int local_blk, int hx, int hy, int hz) {
+  return local_blk * L.bstride + (static_cast<long long>(hx) * L.np + hy) * L.np + hz;
+}
+
+// Coupling plan of the reference (AppendFaceCouplingPoints,
+// level_coupler.cpp:70-139): for each hanging face and fine slot, the fine
+// block's quadrant of the coarse face decides which (n/2)^2 coarse face cells
+// pair 1:1 with the fine block's first (n/2)^2 interface cells.
+std::vector<PlanPoint> build_plan(const octlb_tables* t) {
+  std::vector<PlanPoint> plan;
+  const int n = t->n, half = n / 2;
+  for (int f = 0; f < t->n_coarse_fine; ++f) {
+    const int* r = t->coarse_fine + 8 * f;
+    const double* bd = t->coarse_fine_bounds + 30 * f;
+    const int normal = r[5], ax = normal / 2, tan0 = (ax + 1) % 3, tan1 = (ax + 2) % 3;
+    const bool is_max = (normal & 1) != 0;
+    const double cc[3] = {0.5 * (bd[0] + bd[3]), 0.5 * (bd[1] + bd[4]), 0.5 * (bd[2] + bd[5])};
+    for (int s = 0; s < 4; ++s) {
+      const double* fb = bd + 6 + 6 * s;
+      const double fc[3] = {0.5 * (fb[0] + fb[3]), 0.5 * (fb[1] + fb[4]), 0.5 * (fb[2] + fb[5])};
+      const int q0 = fc[tan0] < cc[tan0] ? 0 : 1, q1 = fc[tan1] < cc[tan1] ? 0 : 1;
+      for (int a = q0 * half; a < q0 * half + half; ++a)
+        for (int b = q1 * half; b < q1 * half + half; ++b) {
+          int ci[3], fi[3];
+          ci[ax] = is_max ? n - 1 : 0;
+          fi[ax] = is_max ? 0 : n - 1;
+          ci[tan0] = a; ci[tan1] = b;
+          fi[tan0] = a - q0 * half; fi[tan1] = b - q1 * half;
+          plan.push_back({r[0], ci[0], ci[1], ci[2], r[1 + s], fi[0], fi[1], fi[2], normal, r[6], r[7], s});
+        }
+    }
+  }
+  return plan;
+}
+
+// ReadMacro of a double-precision cell (level_coupler.cpp:183-189), as floats
+// (rho - 1, u, f_neq).
+void host_macro(const double* f, float out[23]) {
+  double drho = 0, j[3] = {0, 0, 0};
+  for (int i = 0; i < kQ; ++i) {
+    drho += f[i]; j[0] += cx(i) * f[i]; j[1] += cy(i) * f[i]; j[2] += cz(i) * f[i];
+  }
+  const double rho = 1.0 + drho, u[3] = {j[0] / rho, j[1] / rho, j[2] / rho};
+  const double usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  out[0] = static_cast<float>(drho);
+  for (int d = 0; d < 3; ++d) out[1 + d] = static_cast<float>(u[d]);
+  for (int i = 0; i < kQ; ++i) {
+    const double cu = cx(i) * u[0] + cy(i) * u[1] + cz(i) * u[2];
+    const double feq = rho * wd(i) * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq) - wd(i);
+    out[4 + i] = static_cast<float>(f[i] - feq);
+  }
+}
+
+template <typename T>
+int do_advance_level(octlb_ctx* ctx, int l);
+
+template <typename T>
+int launch_level_step(octlb_ctx* ctx, Level& L) {
+  if (L.nblk == 0) return OCTLB_OK;
+  // Ghost fill into the buffer the step reads (reference: apply() then
+  // exchange() after collide, time_loop.h:207-211).
+  CK(launch_ghost<T>(L.buf[L.cur].as<T>(), L.nslots, L.copy_desc.as<CopyDesc>(),
+                     L.copy_start.as<uint32_t>(), L.n_copy_desc, L.n_copy_cells,
+                     L.bb_ops.as<BBOp>(), L.n_bb, L.scale, L.inv_scale, ctx->stream));
+  StepArgs a = L.args;
+  a.src = L.buf[L.cur].p;
+  a.dst = L.buf[1 - L.cur].p;
+  CK(launch_step<T>(a, ctx->periodic != 0, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags,
+                    ctx->stream));
+  if (ctx->drag && L.n_drag > 0) {
+    CK(launch_drag<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.drag_items.as<DragItem>(), L.n_drag,
+                      L.drag_partial.as<double>(), ctx->force_lvl.as<double>() + 3 * L.lvl, nullptr,
+                      ctx->stream));
+  }
+  L.cur = 1 - L.cur;
+  return OCTLB_OK;
+}
+
+template <typename T>
+int do_advance_level(octlb_ctx* ctx, int l) {
+  Level& L = ctx->levels[l];
+  int rc = launch_level_step<T>(ctx, L);
+  if (rc) return rc;
+  ++ctx->counters_collide[l];
+  ++ctx->counters_stream[l];
+  if (l >= ctx->max_level) return OCTLB_OK;
+  Level& F = ctx->levels[l + 1];
+  // apply_half_time(l) -> advance(l+1) -> apply_full_time(l) -> advance(l+1)
+  // -> restrict(l+1)  (time_loop.h:228-239)
+  for (int phase = 0; phase < 2; ++phase) {
+    if (L.n_prolong > 0) {
+      CK(launch_prolong<T>(L.prolong_items.as<ProlongItem>(), L.n_prolong, L.save_buf.as<float>(),
+                           L.prev.as<float>(), phase == 0 ? 1 : 0, F.buf[F.cur].as<T>(), F.nslots,
+                           ctx->prolong_scale, static_cast<float>(ctx->omega), F.scale, ctx->stream));
+    }
+    rc = do_advance_level<T>(ctx, l + 1);
+    if (rc) return rc;
+  }
+  if (F.n_restrict > 0) {
+    CK(launch_restrict<T>(F.restrict_items.as<RestrictItem>(), F.n_restrict, F.save_buf.as<float>(),
+                          L.buf[L.cur].as<T>(), L.nslots, ctx->restrict_scale,
+                          static_cast<float>(ctx->omega), L.scale, ctx->stream));
+  }
+  return OCTLB_OK;
+}
+
+// Sum of the per-level MEM forces into the step force and its running sum.
+__global__ void k_force_total(const double* lvl, int nlvl, double* out, double* sum) {
+  if (threadIdx.x < 3) {
+    double s = 0.0;
+    for (int l = 0; l < nlvl; ++l) s += lvl[3 * l + threadIdx.x];
+    out[threadIdx.x] = s;
+    sum[threadIdx.x] += s;
+  }
+}
+
+int validate(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p) {
+  if (!t || !p) return fail(ctx, OCTLB_EINVAL, "null tables or params");
+  if (t->n < 2 || (t->n % 2) != 0) return fail(ctx, OCTLB_EINVAL, "block edge n must be even and >= 2");
+  if (t->n_blocks < 1 || !t->levels || !t->kinds) return fail(ctx, OCTLB_EINVAL, "no blocks / levels / kinds");
+  if (p->precision != OCTLB_FP32 && p->precision != OCTLB_FP16_SHIFTED)
+    return fail(ctx, OCTLB_EINVAL, "unknown precision");
+  if (p->stream_mode != OCTLB_STREAM_ROTATE && p->stream_mode != OCTLB_STREAM_LINKS)
+    return fail(ctx, OCTLB_EINVAL, "unknown stream mode");
+  if (!(p->omega > 0.0 && p->omega < 2.0)) return fail(ctx, OCTLB_EINVAL, "omega must lie in (0, 2)");
+  for (int b = 0; b < t->n_blocks; ++b)
+    if (t->levels[b] < 0 || t->levels[b] > 30) return fail(ctx, OCTLB_EINVAL, "block level out of range");
+  const long long n3 = static_cast<long long>(t->n) * t->n * t->n;
+  for (long long k = 0; k < n3 * t->n_blocks; ++k)
+    if (t->kinds[k] > kOutflow) return fail(ctx, OCTLB_EINVAL, "BcKind out of range");
+  if (t->periodic) {
+    if (t->n_blocks != 1) return fail(ctx, OCTLB_EINVAL, "periodic mode needs exactly one block");
+    if (p->stream_mode != OCTLB_STREAM_ROTATE)
+      return fail(ctx, OCTLB_EINVAL, "periodic mode uses the rotate stream rule");
+    if (t->n_same_level || t->n_coarse_fine || t->n_tree_boundary)
+      return fail(ctx, OCTLB_EINVAL, "periodic mode takes no face lists");
+  }
+  for (int k = 0; k < t->n_same_level; ++k) {
+    const int* r = t->same_level + 3 * k;
+    if (r[0] < 0 || r[0] >= t->n_blocks || r[2] < 0 || r[2] >= t->n_blocks || r[1] < 0 || r[1] > 5)
+      return fail(ctx, OCTLB_EINVAL, "same-level face entry out of range");
+    if (t->levels[r[0]] != t->levels[r[2]]) return fail(ctx, OCTLB_EINVAL, "same-level face joins two levels");
+  }
+  for (int k = 0; k < t->n_coarse_fine; ++k) {
+    const int* r = t->coarse_fine + 8 * k;
+    if (r[0] < 0 || r[0] >= t->n_blocks || r[5] < 0 || r[5] > 5)
+      return fail(ctx, OCTLB_EINVAL, "coarse-fine face entry out of range");
+    for (int s = 0; s < 4; ++s)
+      if (r[1 + s] < 0 || r[1 + s] >= t->n_blocks || t->levels[r[1 + s]] != t->levels[r[0]] + 1)
+        return fail(ctx, OCTLB_EINVAL, "coarse-fine face: fine block must be one level finer");
+    if (r[6] != t->levels[r[0]] || r[7] != r[6] + 1)
+      return fail(ctx, OCTLB_EINVAL, "coarse-fine face levels disagree with the block levels");
+  }
+  for (int k = 0; k < t->n_tree_boundary; ++k) {
+    const int* r = t->tree_boundary + 2 * k;
+    if (r[0] < 0 || r[0] >= t->n_blocks || r[1] < 0 || r[1] > 5)
+      return fail(ctx, OCTLB_EINVAL, "tree-boundary entry out of range");
+    if (t->tree_boundary_spec) {
+      const double ty = t->tree_boundary_spec[8 * k];
+      if (ty != OCTLB_TB_NONE && ty != OCTLB_TB_WALL && ty != OCTLB_TB_OUTFLOW)
+        return fail(ctx, OCTLB_EINVAL, "unknown tree-boundary condition");
+    }
+  }
+  for (int k = 0; k < t->n_links; ++k) {
+    const int* c = t->link_cells + 5 * k;
+    if (c[0] < 0 || c[0] >= t->n_blocks || c[1] < 0 || c[2] < 0 || c[3] < 0 || c[1] >= t->n ||
+        c[2] >= t->n || c[3] >= t->n || c[4] < 0 || c[4] >= kQ)
+      return fail(ctx, OCTLB_EINVAL, "link cell out of range");
+  }
+  if (t->n_links && p->stream_mode != OCTLB_STREAM_LINKS)
+    return fail(ctx, OCTLB_EINVAL, "Bouzidi links need the links stream rule");
+  return OCTLB_OK;
+}
+
+template <typename T>
+int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, const double* init) {
+  const int n = t->n, nb = t->n_blocks;
+  const long long n3 = static_cast<long long>(n) * n * n;
+  const bool links = p->stream_mode == OCTLB_STREAM_LINKS;
+  ctx->kinds.assign(t->kinds, t->kinds + n3 * nb);
+  for (int b = 0; b < nb; ++b) ctx->max_level = std::max(ctx->max_level, t->levels[b]);
+  const int nlev = ctx->max_level + 1;
+  ctx->levels.resize(nlev);
+  ctx->blk_level.resize(nb);
+  ctx->blk_local.resize(nb);
+  ctx->counters_collide.assign(nlev, 0);
+  ctx->counters_stream.assign(nlev, 0);
+  const double tau = 1.0 / p->omega;
+  ctx->prolong_scale = static_cast<float>((tau - 0.25) / tau);   // level_coupler.cpp:226-228
+  ctx->restrict_scale = static_cast<float>(tau / (tau - 0.25));
+  for (int l = 0; l < nlev; ++l) ctx->levels[l].lvl = l;
+  for (int b = 0; b < nb; ++b) {
+    Level& L = ctx->levels[t->levels[b]];
+    ctx->blk_level[b] = t->levels[b];
+    ctx->blk_local[b] = static_cast<int>(L.blocks.size());
+    L.blocks.push_back(b);
+  }
+  // Equilibrium at rest when no initial state is given (block_lattice.cpp:272-285).
+  std::vector<double> init_pops;
+  if (!init) {
+    init_pops.assign(static_cast<size_t>(n3 * nb * kQ), 0.0);
+    init = init_pops.data();
+  }
+
+  // ---- per-level storage and flags
+  for (int l = 0; l < nlev; ++l) {
+    Level& L = ctx->levels[l];
+    L.nblk = static_cast<int>(L.blocks.size());
+    L.n = n;
+    L.np = ctx->periodic ? n : n + 2;
+    L.bstride = static_cast<long long>(L.np) * L.np * L.np;
+    L.nslots = L.bstride * L.nblk;
+    double sc = p->fp16_scale[l < 32 ? l : 31];
+    if (!(sc > 0)) sc = 65536.0;
+    L.scale = p->precision == OCTLB_FP16_SHIFTED ? static_cast<float>(sc) : 1.f;
+    L.inv_scale = 1.f / L.scale;
+    if (L.nblk == 0) continue;
+    if (L.nslots * static_cast<long long>(kQ) >= (1LL << 40))
+      return fail(ctx, OCTLB_EINVAL, "level too large");
+    if (static_cast<long long>(L.nblk) * n3 >= (1LL << 31))
+      return fail(ctx, OCTLB_EINVAL, "level has more than 2^31 cells");
+    for (int k = 0; k < 2; ++k) CK(L.buf[k].alloc(static_cast<size_t>(L.nslots) * kQ * sizeof(T)));
+  }
+
+  // Link records: q per direction (1 = half-way bounce-back) and the moving-wall
+  // term per direction, for core cells with a cut link or a moving neighbour.
+  std::map<long long, std::vector<float>> recs;  // global cell -> 38 floats
+  auto rec_for = [&](long long gcell) -> std::vector<float>& {
+    auto it = recs.find(gcell);
+    if (it == recs.end()) {
+      std::vector<float> r(38, 0.f);
+      for (int i = 0; i < kQ; ++i) r[i] = 1.f;
+      it = recs.emplace(gcell, std::move(r)).first;
+    }
+    return it->second;
+  };
+  if (links) {
+    for (int k = 0; k < t->n_links; ++k) {
+      const int* c = t->link_cells + 5 * k;
+      const double q = t->link_q[k];
+      // Reference thresholds (block_lattice.cpp:652, bouzidi_pull.h:11-16):
+      // q outside (1e-10, 1-1e-10) or within 1e-14 of 0 / 1 is plain bounce-back.
+      float qf = 1.f;
+      if (q > 1.0e-10 && q < 1.0 - 1.0e-10 && q > 1.0e-14 && q < 1.0 - 1.0e-14) {
+        qf = static_cast<float>(q);
+        if (qf >= 1.f) qf = std::nextafter(1.f, 0.f);
+        if (q >= 0.5 - 1.0e-14 && qf < 0.5f) qf = 0.5f;
+      }
+      rec_for(c[0] * n3 + (static_cast<long long>(c[1]) * n + c[2]) * n + c[3])[c[4]] = qf;
+    }
+    if (t->moving && t->wall_u) {
+      for (int b = 0; b < nb; ++b)
+        for (int x = 0; x < n; ++x)
+          for (int y = 0; y < n; ++y)
+            for (int z = 0; z < n; ++z) {
+              const long long g = b * n3 + (static_cast<long long>(x) * n + y) * n + z;
+              if (t->kinds[g] == kSolid) continue;
+              for (int i = 1; i < kQ; ++i) {
+                const int sx = x - cx(i), sy = y - cy(i), sz = z - cz(i);
+                if (sx < 0 || sy < 0 || sz < 0 || sx >= n || sy >= n || sz >= n) continue;
+                const long long s = b * n3 + (static_cast<long long>(sx) * n + sy) * n + sz;
+                if ((t->kinds[s] != kSolid && t->kinds[s] != kBouzidi) || !t->moving[s]) continue;
+                const double cu = cx(i) * t->wall_u[3 * s] + cy(i) * t->wall_u[3 * s + 1] +
+                                  cz(i) * t->wall_u[3 * s + 2];
+                if (cu == 0.0) continue;
+                rec_for(g)[kQ + i] += static_cast<float>(6.0 * wd(i) * cu);
+              }
+            }
+    }
+  }
+  // ---- coupler plan (reference order) and level ranges
+  const std::vector<PlanPoint> plan = build_plan(t);
+  {
+    // LevelRangeBegin/End take min/max plan index per coarse level
+    // (level_coupler.cpp:238-250); the flattened path requires the ranges not
+    // to interleave, which holds when hanging faces are listed level by level.
+    std::vector<int> lo(nlev, 1 << 30), hi(nlev, -1);
+    for (size_t k = 0; k < plan.size(); ++k) {
+      lo[plan[k].coarse_level] = std::min(lo[plan[k].coarse_level], static_cast<int>(k));
+      hi[plan[k].coarse_level] = std::max(hi[plan[k].coarse_level], static_cast<int>(k));
+    }
+    for (size_t k = 0; k < plan.size(); ++k)
+      for (int l = 0; l < nlev; ++l)
+        if (l != plan[k].coarse_level && static_cast<int>(k) >= lo[l] && static_cast<int>(k) <= hi[l])
+          return fail(ctx, OCTLB_EINVAL, "coarse-fine faces must be grouped by coarse level");
+  }
+  // save rows: level -> (local slot -> row)
+  std::vector<std::map<long long, int>> save_rows(nlev);
+  auto save_row = [&](int l, long long slot) {
+    auto& m = save_rows[l];
+    auto it = m.find(slot);
+    if (it != m.end()) return it->second;
+    const int r = static_cast<int>(m.size());
+    m.emplace(slot, r);
+    return r;
+  };
+  auto core_slot = [&](int gblk, int x, int y, int z) {
+    const Level& L = ctx->levels[ctx->blk_level[gblk]];
+    return slot_of(L, ctx->blk_local[gblk], x + 1, y + 1, z + 1);
+  };
+  auto gcell = [&](int gblk, int x, int y, int z) {
+    return gblk * n3 + (static_cast<long long>(x) * n + y) * n + z;
+  };
+  std::vector<std::vector<ProlongItem>> prolong(nlev);
+  std::vector<std::vector<RestrictItem>> restrict_items(nlev);
+  std::vector<float> prev(plan.size() * 23, 0.f);
+  for (size_t k = 0; k < plan.size(); ++k)
+    host_macro(init + gcell(plan[k].coarse_id, plan[k].ci, plan[k].cj, plan[k].ck) * kQ, &prev[k * 23]);
+  {
+    // Prolongation writes a fine cell per point; a later point writing the
+    // same cell wins (plan order, level_coupler.cpp:440-477).
+    std::vector<std::map<long long, size_t>> last(nlev);
+    for (size_t k = 0; k < plan.size(); ++k)
+      last[plan[k].coarse_level][gcell(plan[k].fine_id, plan[k].fi, plan[k].fj, plan[k].fk)] = k;
+    for (size_t k = 0; k < plan.size(); ++k) {
+      const PlanPoint& pt = plan[k];
+      if (last[pt.coarse_level][gcell(pt.fine_id, pt.fi, pt.fj, pt.fk)] != k) continue;
+      ProlongItem it{};
+      it.fine_slot = core_slot(pt.fine_id, pt.fi, pt.fj, pt.fk);
+      it.coarse_save = save_row(pt.coarse_level, core_slot(pt.coarse_id, pt.ci, pt.cj, pt.ck));
+      it.prev = static_cast<int>(k);
+      it.fine_kind = t->kinds[gcell(pt.fine_id, pt.fi, pt.fj, pt.fk)];
+      prolong[pt.coarse_level].push_back(it);
+    }
+    // Restriction writes a coarse cell per point from the fine cell and its
+    // in-block D3Q19 neighbours (level_coupler.cpp:613-654).
+    std::vector<std::map<long long, size_t>> lastc(nlev);
+    for (size_t k = 0; k < plan.size(); ++k)
+      lastc[plan[k].fine_level][gcell(plan[k].coarse_id, plan[k].ci, plan[k].cj, plan[k].ck)] = k;
+    for (size_t k = 0; k < plan.size(); ++k) {
+      const PlanPoint& pt = plan[k];
+      if (lastc[pt.fine_level][gcell(pt.coarse_id, pt.ci, pt.cj, pt.ck)] != k) continue;
+      RestrictItem it{};
+      it.coarse_slot = core_slot(pt.coarse_id, pt.ci, pt.cj, pt.ck);
+      it.coarse_kind = t->kinds[gcell(pt.coarse_id, pt.ci, pt.cj, pt.ck)];
+      it.fine_save = save_row(pt.fine_level, core_slot(pt.fine_id, pt.fi, pt.fj, pt.fk));
+      it.nnb = 0;
+      for (int j = 1; j < kQ; ++j) {
+        const int x = pt.fi + cx(j), y = pt.fj + cy(j), z = pt.fk + cz(j);
+        if (x < 0 || y < 0 || z < 0 || x >= n || y >= n || z >= n) continue;
+        it.nb_save[it.nnb++] = save_row(pt.fine_level, core_slot(pt.fine_id, x, y, z));
+      }
+      restrict_items[pt.fine_level].push_back(it);
+    }
+  }
+
+  // ---- per-level flags, links, ghost ops, open blocks, drag items
+  std::vector<int> face_nbr(static_cast<size_t>(nb) * 6, -1);
+  for (int k = 0; k < t->n_same_level; ++k) {
+    const int* r = t->same_level + 3 * k;
+    face_nbr[static_cast<size_t>(r[0]) * 6 + r[1]] = r[2];
+  }
+  for (int l = 0; l < nlev; ++l) {
+    Level& L = ctx->levels[l];
+    if (L.nblk == 0) continue;
+    const int np = L.np;
+    L.has_flags = !ctx->periodic || !save_rows[l].empty();
+    if (ctx->periodic) {
+      for (long long k = 0; k < n3; ++k) if (t->kinds[k] != kBulk) L.has_flags = true;
+    }
+    std::vector<uint8_t> flags(static_cast<size_t>(L.nslots), 0);
+    std::vector<int> lidx;
+    std::vector<float> lrec;
+    std::vector<int> sidx;
+    if (!ctx->periodic)
+      for (int lb = 0; lb < L.nblk; ++lb)
+        for (int hx = 0; hx < np; ++hx)
+          for (int hy = 0; hy < np; ++hy)
+            for (int hz = 0; hz < np; ++hz) {
+              const bool core = hx >= 1 && hy >= 1 && hz >= 1 && hx <= n && hy <= n && hz <= n;
+              if (!core) flags[slot_of(L, lb, hx, hy, hz)] = kFlagHalo;
+            }
+    for (int lb = 0; lb < L.nblk; ++lb) {
+      const int gb = L.blocks[lb];
+      for (int x = 0; x < n; ++x)
+        for (int y = 0; y < n; ++y)
+          for (int z = 0; z < n; ++z) {
+            const long long s = ctx->periodic ? (static_cast<long long>(x) * n + y) * n + z
+                                              : slot_of(L, lb, x + 1, y + 1, z + 1);
+            flags[s] = t->kinds[gcell(gb, x, y, z)];
+          }
+    }
+    // link records of this level
+    for (const auto& kv : recs) {
+      const int gb = static_cast<int>(kv.first / n3);
+      if (ctx->blk_level[gb] != l) continue;
+      const long long c = kv.first % n3;
+      const int x = static_cast<int>(c / (n * n)), y = static_cast<int>((c / n) % n), z = static_cast<int>(c % n);
+      const long long s = slot_of(L, ctx->blk_local[gb], x + 1, y + 1, z + 1);
+      if (lidx.empty()) lidx.assign(static_cast<size_t>(L.nslots), -1);
+      lidx[s] = static_cast<int>(lrec.size() / 38);
+      lrec.insert(lrec.end(), kv.second.begin(), kv.second.end());
+      flags[s] |= kFlagLink;
+    }
+    L.n_links = static_cast<int>(lrec.size() / 38);
+    if (!save_rows[l].empty()) {
+      sidx.assign(static_cast<size_t>(L.nslots), -1);
+      for (const auto& kv : save_rows[l]) {
+        sidx[kv.first] = kv.second;
+        flags[kv.first] |= kFlagSave;
+      }
+      L.n_save = static_cast<int>(save_rows[l].size());
+    }
+
+    // Ghost ops.  Tree-boundary fills first (apply(), in list order, later
+    // writes of the same halo population win), then same-level faces and
+    // edges (GhostSchedule::exchange, ghost_schedule.h:148-254).
+    std::map<std::pair<long long, int>, BBOp> bbmap;
+    std::vector<std::pair<long long, int>> bborder;
+    auto put_bb = [&](long long dst, int pop, long long src, int src_pop, float add) {
+      const auto key = std::make_pair(dst, pop);
+      if (!bbmap.count(key)) bborder.push_back(key);
+      bbmap[key] = BBOp{dst, src, pop, src_pop, add, 0};
+    };
+    std::vector<CopyDesc> copies;
+    const long long sx_ = static_cast<long long>(np) * np, sy_ = np, sz_ = 1;
+    const long long astride[3] = {sx_, sy_, sz_};
+    for (int k = 0; k < t->n_tree_boundary; ++k) {
+      const int gb = t->tree_boundary[2 * k], dir = t->tree_boundary[2 * k + 1];
+      if (ctx->blk_level[gb] != l || !t->tree_boundary_spec) continue;
+      const double* sp = t->tree_boundary_spec + 8 * k;
+      const int type = static_cast<int>(sp[0]);
+      if (type == OCTLB_TB_NONE) continue;
+      const int lb = ctx->blk_local[gb];
+      const double* bd = t->bounds + 6 * gb;
+      const double dx = (bd[3] - bd[0]) / n;
+      const int ax = dir / 2, t0 = (ax + 1) % 3, t1 = (ax + 2) % 3;
+      const bool is_max = (dir & 1) != 0;
+      const int hl = is_max ? n + 1 : 0, nin = is_max ? -1 : 1;
+      for (int a = 0; a < n + 2; ++a)
+        for (int b2 = 0; b2 < n + 2; ++b2) {
+          int h[3];
+          h[ax] = hl; h[t0] = a; h[t1] = b2;
+          const long long hs = slot_of(L, lb, h[0], h[1], h[2]);
+          if (type == OCTLB_TB_WALL) {
+            double shape = 1.0;
+            const int pax = static_cast<int>(sp[4]);
+            if (pax >= 0) {
+              const double pc = bd[pax] + (h[pax] - 1 + 0.5) * dx;
+              const double tt = (pc - sp[5]) / (sp[6] - sp[5]);
+              shape = (tt <= 0.0 || tt >= 1.0) ? 0.0 : 4.0 * tt * (1.0 - tt);
+            }
+            for (int i = 1; i < kQ; ++i) {
+              const int ci[3] = {cx(i), cy(i), cz(i)};
+              if (ci[ax] != nin) continue;
+              const int xx = h[0] + ci[0], yy = h[1] + ci[1], zz = h[2] + ci[2];
+              if (xx < 1 || yy < 1 || zz < 1 || xx > n || yy > n || zz > n) continue;
+              const double cu = (ci[0] * sp[1] + ci[1] * sp[2] + ci[2] * sp[3]) * shape;
+              put_bb(hs, i, slot_of(L, lb, xx, yy, zz), opp(i), static_cast<float>(6.0 * wd(i) * cu));
+            }
+          } else {  // outflow: copy the adjacent interior cell, tangentially clamped
+            int src[3];
+            src[ax] = hl + nin;
+            src[t0] = std::min(std::max(a, 1), n);
+            src[t1] = std::min(std::max(b2, 1), n);
+            const long long ss = slot_of(L, lb, src[0], src[1], src[2]);
+            for (int i = 0; i < kQ; ++i) put_bb(hs, i, ss, i, 0.f);
+          }
+        }
+    }
+    // Same-level faces.
+    std::set<std::pair<long long, long long>> seen_copy;
+    for (int k = 0; k < t->n_same_level; ++k) {
+      const int* r = t->same_level + 3 * k;
+      if (ctx->blk_level[r[0]] != l) continue;
+      const int dir = r[1], ax = dir / 2, t0 = std::min((ax + 1) % 3, (ax + 2) % 3),
+                t1 = std::max((ax + 1) % 3, (ax + 2) % 3);
+      const bool is_max = (dir & 1) != 0;
+      int hs[3] = {1, 1, 1}, hd[3] = {1, 1, 1};
+      hs[ax] = is_max ? n : 1;
+      hd[ax] = is_max ? 0 : n + 1;
+      CopyDesc d{};
+      d.src = slot_of(L, ctx->blk_local[r[0]], hs[0], hs[1], hs[2]);
+      d.dst = slot_of(L, ctx->blk_local[r[2]], hd[0], hd[1], hd[2]);
+      d.n0 = n; d.n1 = n;
+      d.s0 = d.d0 = static_cast<int>(astride[t0]);
+      d.s1 = d.d1 = static_cast<int>(astride[t1]);
+      copies.push_back(d);
+    }
+    // Same-level edges by composing face neighbours (ghost_schedule.h:56-95).
+    for (int a = 0; a < nb; ++a) {
+      if (ctx->blk_level[a] != l) continue;
+      for (int d1 = 0; d1 < 6; ++d1)
+        for (int d2 = 0; d2 < 6; ++d2) {
+          if (d1 / 2 == d2 / 2) continue;
+          const int bb = face_nbr[static_cast<size_t>(a) * 6 + d1];
+          if (bb < 0) continue;
+          const int dd = face_nbr[static_cast<size_t>(bb) * 6 + d2];
+          if (dd < 0) continue;
+          const int a1 = d1 / 2, a2 = d2 / 2, a3 = 3 - a1 - a2;
+          int hs[3], hd[3];
+          hs[a1] = (d1 & 1) ? n : 1; hs[a2] = (d2 & 1) ? n : 1; hs[a3] = 1;
+          hd[a1] = (d1 & 1) ? 0 : n + 1; hd[a2] = (d2 & 1) ? 0 : n + 1; hd[a3] = 1;
+          CopyDesc d{};
+          d.src = slot_of(L, ctx->blk_local[a], hs[0], hs[1], hs[2]);
+          d.dst = slot_of(L, ctx->blk_local[dd], hd[0], hd[1], hd[2]);
+          if (!seen_copy.insert({d.dst, d.src}).second) continue;
+          d.n0 = 1; d.n1 = n;
+          d.s0 = d.d0 = 0;
+          d.s1 = d.d1 = static_cast<int>(astride[a3]);
+          copies.push_back(d);
+        }
+    }
+    std::vector<uint32_t> cstart;
+    uint32_t ncells = 0;
+    for (const CopyDesc& d : copies) { cstart.push_back(ncells); ncells += static_cast<uint32_t>(d.n0 * d.n1); }
+    std::vector<BBOp> bbv;
+    for (const auto& key : bborder) bbv.push_back(bbmap[key]);
+    L.n_copy_desc = static_cast<int>(copies.size());
+    L.n_copy_cells = ncells;
+    L.n_bb = static_cast<uint32_t>(bbv.size());
+
+    // Open blocks: some halo population a core read depends on is not
+    // rewritten by the ghost fill, so the halo carries the reference's torus
+    // stream from step to step.
+    std::vector<int> open;
+    std::vector<int> halo_map;
+    if (!ctx->periodic) {
+      std::set<std::pair<long long, int>> covered;
+      for (const CopyDesc& d : copies)
+        for (int a0 = 0; a0 < d.n0; ++a0)
+          for (int a1 = 0; a1 < d.n1; ++a1)
+            for (int i = 0; i < kQ; ++i) covered.insert({d.dst + static_cast<long long>(a0) * d.d0 + static_cast<long long>(a1) * d.d1, i});
+      for (const BBOp& op : bbv) covered.insert({op.dst, op.pop});
+      for (int lb = 0; lb < L.nblk; ++lb) {
+        bool is_open = false;
+        for (int x = 1; x <= n && !is_open; ++x)
+          for (int y = 1; y <= n && !is_open; ++y)
+            for (int z = 1; z <= n && !is_open; ++z) {
+              if (x > 1 && y > 1 && z > 1 && x < n && y < n && z < n) continue;
+              const long long s = slot_of(L, lb, x, y, z);
+              const int kind = flags[s] & kKindMask;
+              for (int i = 1; i < kQ && !is_open; ++i) {
+                const int hx = x - cx(i), hy = y - cy(i), hz = z - cz(i);
+                const bool halo = hx < 1 || hy < 1 || hz < 1 || hx > n || hy > n || hz > n;
+                if (halo) {
+                  const bool reads = !links || !(kind == kSolid || reflects_on_pull(kind));
+                  if (reads && !covered.count({slot_of(L, lb, hx, hy, hz), i})) is_open = true;
+                }
+                if (links && (flags[s] & kFlagLink)) {
+                  const int nx_ = x + cx(i), ny_ = y + cy(i), nz_ = z + cz(i);
+                  const bool nhalo = nx_ < 1 || ny_ < 1 || nz_ < 1 || nx_ > n || ny_ > n || nz_ > n;
+                  if (nhalo && !covered.count({slot_of(L, lb, nx_, ny_, nz_), i})) is_open = true;
+                }
+              }
+            }
+        if (is_open) open.push_back(lb);
+      }
+      for (int hx = 0; hx < np; ++hx)
+        for (int hy = 0; hy < np; ++hy)
+          for (int hz = 0; hz < np; ++hz) {
+            const bool core = hx >= 1 && hy >= 1 && hz >= 1 && hx <= n && hy <= n && hz <= n;
+            if (!core) halo_map.push_back((hx * np + hy) * np + hz);
+          }
+    }
+    L.n_open = static_cast<int>(open.size());
+    L.n_halo = static_cast<int>(halo_map.size());
+
+    // Drag cells (drag_postprocessor.h:73-110).
+    std::vector<DragItem> drag;
+    if (ctx->drag) {
+      for (int lb = 0; lb < L.nblk; ++lb) {
+        const int gb = L.blocks[lb];
+        for (int x = 0; x < n; ++x)
+          for (int y = 0; y < n; ++y)
+            for (int z = 0; z < n; ++z) {
+              if (t->kinds[gcell(gb, x, y, z)] != kBulk) continue;
+              uint32_t mask = 0;
+              for (int i = 1; i < kQ; ++i) {
+                const int xx = x + cx(i), yy = y + cy(i), zz = z + cz(i);
+                if (xx < 0 || yy < 0 || zz < 0 || xx >= n || yy >= n || zz >= n) continue;
+                const long long g = gcell(gb, xx, yy, zz);
+                if (t->kinds[g] != kSolid && t->kinds[g] != kBouzidi) continue;
+                if (t->obstacle && !t->obstacle[g]) continue;
+                mask |= 1u << i;
+              }
+              if (!mask) continue;
+              DragItem it{};
+              it.slot = ctx->periodic ? (static_cast<long long>(x) * n + y) * n + z
+                                      : slot_of(L, lb, x + 1, y + 1, z + 1);
+              it.mask = mask;
+              drag.push_back(it);
+            }
+      }
+    }
+    L.n_drag = static_cast<int>(drag.size());
+
+    // Bounds of every index a kernel derives from these tables, checked on the
+    // host before anything runs on the device.
+    {
+      const long long ns = L.nslots;
+      auto in = [&](long long v, long long hi) { return v >= 0 && v < hi; };
+      for (const CopyDesc& d : copies) {
+        const long long ls = d.src + static_cast<long long>(d.n0 - 1) * d.s0 + static_cast<long long>(d.n1 - 1) * d.s1;
+        const long long ld = d.dst + static_cast<long long>(d.n0 - 1) * d.d0 + static_cast<long long>(d.n1 - 1) * d.d1;
+        if (!in(d.src, ns) || !in(d.dst, ns) || !in(ls, ns) || !in(ld, ns) || d.s0 < 0 || d.s1 < 0 ||
+            d.d0 < 0 || d.d1 < 0 || d.n0 < 1 || d.n1 < 1)
+          return fail(ctx, OCTLB_EINVAL, "internal: ghost copy out of range");
+      }
+      for (const BBOp& op : bbv)
+        if (!in(op.dst, ns) || !in(op.src, ns) || !in(op.pop, kQ) || !in(op.src_pop, kQ))
+          return fail(ctx, OCTLB_EINVAL, "internal: ghost write out of range");
+      for (int v : lidx) if (v < -1 || v >= L.n_links) return fail(ctx, OCTLB_EINVAL, "internal: link index");
+      for (int v : sidx) if (v < -1 || v >= L.n_save) return fail(ctx, OCTLB_EINVAL, "internal: save index");
+      for (int v : open) if (!in(v, L.nblk)) return fail(ctx, OCTLB_EINVAL, "internal: open block");
+      for (int v : halo_map) if (!in(v, L.bstride)) return fail(ctx, OCTLB_EINVAL, "internal: halo map");
+      for (const DragItem& it : drag) if (!in(it.slot, ns)) return fail(ctx, OCTLB_EINVAL, "internal: drag slot");
+      for (const RestrictItem& it : restrict_items[l]) {
+        if (!in(it.fine_save, L.n_save) || it.nnb < 0 || it.nnb > 18)
+          return fail(ctx, OCTLB_EINVAL, "internal: restriction source");
+        for (int k = 0; k < it.nnb; ++k)
+          if (!in(it.nb_save[k], L.n_save)) return fail(ctx, OCTLB_EINVAL, "internal: restriction source");
+      }
+      if (static_cast<long long>(L.n_open) * L.n_halo + static_cast<long long>(L.nblk) * n3 >= (1LL << 32))
+        return fail(ctx, OCTLB_EINVAL, "level work exceeds 2^32 items");
+      if (!L.has_flags && (L.n_save > 0 || !ctx->periodic))
+        return fail(ctx, OCTLB_EINVAL, "internal: flags required");
+    }
+
+    // uploads
+    if (L.has_flags) CK(upload(L.flags, flags));
+    CK(upload(L.link_idx, lidx));
+    CK(upload(L.link_rec, lrec));
+    CK(upload(L.save_idx, sidx));
+    CK(L.save_buf.alloc(static_cast<size_t>(L.n_save) * kQ * sizeof(float)));
+    CK(upload(L.open_blocks, open));
+    CK(upload(L.halo_map, halo_map));
+    CK(upload(L.copy_desc, copies));
+    CK(upload(L.copy_start, cstart));
+    CK(upload(L.bb_ops, bbv));
+    CK(upload(L.prolong_items, prolong[l]));
+    CK(upload(L.restrict_items, restrict_items[l]));
+    L.n_prolong = static_cast<int>(prolong[l].size());
+    L.n_restrict = static_cast<int>(restrict_items[l].size());
+    CK(upload(L.drag_items, drag));
+    CK(L.drag_partial.alloc(drag_partials(L.n_drag) * 3 * sizeof(double)));
+
+    StepArgs& A = L.args;
+    A = StepArgs{};
+    A.qs = L.nslots;
+    A.flags = L.has_flags ? L.flags.as<uint8_t>() : nullptr;
+    A.link_idx = L.link_idx.as<int>();
+    A.link_rec = L.link_rec.as<float>();
+    A.save_idx = L.save_idx.as<int>();
+    A.save_buf = L.save_buf.as<float>();
+    A.open_blocks = L.open_blocks.as<int>();
+    A.halo_map = L.halo_map.as<int>();
+    A.n_open = L.n_open;
+    A.n_halo = L.n_halo;
+    A.nblk = L.nblk; A.n = n; A.np = np;
+    A.bstride = L.bstride;
+    A.plane = static_cast<long long>(np) * np;
+    A.ncore = static_cast<uint32_t>(L.nblk * n3);
+    A.nitems = A.ncore + static_cast<uint32_t>(L.n_open) * static_cast<uint32_t>(L.n_halo);
+    A.div_n = FastDiv(n);
+    A.div_n2 = FastDiv(n * n);
+    A.div_n3 = FastDiv(static_cast<uint32_t>(n3));
+    A.div_halo = FastDiv(L.n_halo > 0 ? L.n_halo : 1);
+    A.omega = static_cast<float>(p->omega);
+    A.scale = L.scale;
+    A.inv_scale = L.inv_scale;
+    for (int i = 0; i < kQ; ++i) A.off[i] = static_cast<int>(cx(i) * A.plane + cy(i) * np + cz(i));
+  }
+  // Cross-level coupler indices: prolongation targets live on level l+1,
+  // restriction targets on level l-1.
+  for (int l = 0; l < nlev; ++l) {
+    for (const ProlongItem& it : prolong[l]) {
+      if (l + 1 >= nlev || it.fine_slot < 0 || it.fine_slot >= ctx->levels[l + 1].nslots ||
+          it.coarse_save < 0 || it.coarse_save >= ctx->levels[l].n_save || it.prev < 0 ||
+          it.prev >= static_cast<int>(plan.size()))
+        return fail(ctx, OCTLB_EINVAL, "internal: prolongation item out of range");
+    }
+    for (const RestrictItem& it : restrict_items[l]) {
+      if (l < 1 || it.coarse_slot < 0 || it.coarse_slot >= ctx->levels[l - 1].nslots)
+        return fail(ctx, OCTLB_EINVAL, "internal: restriction target out of range");
+    }
+  }
+  // prev macros live with the coarse level
+  for (int l = 0; l < nlev; ++l) {
+    if (ctx->levels[l].n_prolong == 0) continue;
+    CK(upload(ctx->levels[l].prev, prev));
+  }
+  CK(ctx->force_lvl.alloc(static_cast<size_t>(nlev) * 3 * sizeof(double)));
+  CK(ctx->force.alloc(3 * sizeof(double)));
+  CK(ctx->force_sum.alloc(3 * sizeof(double)));
+  CK(ctx->audit_out.alloc(5 * sizeof(double)));
+
+  // ---- initial state: g = C(f0) on kBulk cells
+  for (int l = 0; l < nlev; ++l) {
+    Level& L = ctx->levels[l];
+    if (L.nblk == 0) continue;
+    std::vector<double> dense(static_cast<size_t>(L.nblk * n3 * kQ));
+    for (int lb = 0; lb < L.nblk; ++lb)
+      std::memcpy(&dense[static_cast<size_t>(lb * n3 * kQ)], init + static_cast<size_t>(L.blocks[lb] * n3 * kQ),
+                  sizeof(double) * n3 * kQ);
+    DevBuf d;
+    CK(upload(d, dense));
+    StepArgs a = L.args;
+    a.dst = L.buf[L.cur].p;
+    CK(launch_scatter<T>(a, d.as<double>(), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  long long lups = 0;
+  for (int l = 0; l < nlev; ++l) lups += static_cast<long long>(ctx->levels[l].nblk) * n3 << l;
+  ctx->lups_per_step = lups;
+  return OCTLB_OK;
+}
+
+template <typename T>
+int advance_impl(octlb_ctx* ctx, int steps) {
+  for (int s = 0; s < steps; ++s) {
+    int rc = do_advance_level<T>(ctx, 0);
+    if (rc) return rc;
+    if (ctx->drag) {
+      k_force_total<<<1, 32, 0, ctx->stream>>>(ctx->force_lvl.as<double>(), ctx->max_level + 1,
+                                               ctx->force.as<double>(), ctx->force_sum.as<double>());
+      CK(cudaGetLastError());
+      ++ctx->force_steps;
+    }
+  }
+  return OCTLB_OK;
+}
+
+template <typename T>
+int gather_impl(octlb_ctx* ctx, double* out, int mode) {
+  const int n = ctx->n;
+  const long long n3 = static_cast<long long>(n) * n * n;
+  const int width = mode == 0 ? kQ : 4;
+  std::vector<double> host;
+  for (auto& L : ctx->levels) {
+    if (L.nblk == 0) continue;
+    DevBuf d;
+    CK(d.alloc(static_cast<size_t>(L.nblk * n3 * width) * sizeof(double)));
+    StepArgs a = L.args;
+    a.src = L.buf[L.cur].p;
+    CK(launch_gather<T>(a, d.as<double>(), mode, ctx->stream));
+    host.resize(static_cast<size_t>(L.nblk * n3 * width));
+    CK(cudaMemcpyAsync(host.data(), d.p, host.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int lb = 0; lb < L.nblk; ++lb)
+      std::memcpy(out + static_cast<size_t>(L.blocks[lb] * n3 * width), &host[static_cast<size_t>(lb * n3 * width)],
+                  sizeof(double) * n3 * width);
+  }
+  return OCTLB_OK;
+}
+
+template <typename T>
+int scatter_impl(octlb_ctx* ctx, const double* in) {
+  const int n = ctx->n;
+  const long long n3 = static_cast<long long>(n) * n * n;
+  for (auto& L : ctx->levels) {
+    if (L.nblk == 0) continue;
+    std::vector<double> dense(static_cast<size_t>(L.nblk * n3 * kQ));
+    for (int lb = 0; lb < L.nblk; ++lb)
+      std::memcpy(&dense[static_cast<size_t>(lb * n3 * kQ)], in + static_cast<size_t>(L.blocks[lb] * n3 * kQ),
+                  sizeof(double) * n3 * kQ);
+    DevBuf d;
+    CK(upload(d, dense));
+    StepArgs a = L.args;
+    a.dst = L.buf[L.cur].p;
+    CK(launch_scatter<T>(a, d.as<double>(), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  return OCTLB_OK;
+}
+
+template <typename T>
+int audit_impl(octlb_ctx* ctx, double out[4]) {
+  double tot[5] = {0, 0, 0, 0, 0};
+  for (auto& L : ctx->levels) {
+    if (L.nblk == 0) continue;
+    StepArgs a = L.args;
+    a.src = L.buf[L.cur].p;
+    DevBuf part;
+    CK(part.alloc(audit_partials(a) * 5 * sizeof(double)));
+    CK(launch_audit<T>(a, part.as<double>(), ctx->audit_out.as<double>(), ctx->stream));
+    double h[5];
+    CK(cudaMemcpyAsync(h, ctx->audit_out.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < 5; ++k) tot[k] += h[k];
+  }
+  for (int k = 0; k < 4; ++k) out[k] = tot[k];
+  if (tot[4] != 0.0) return fail(ctx, OCTLB_ENAN, "non-finite populations");
+  return OCTLB_OK;
+}
+
+}  // namespace octlb_host
+
+using namespace octlb_host;
+
+// ====================================================================== C ABI
+extern "C" {
+
+int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double* init, octlb_ctx** out) {
+  if (!out) return OCTLB_EINVAL;
+  *out = nullptr;
+  auto ctx = std::make_unique<octlb_ctx>();
+  int rc = validate(ctx.get(), t, p);
+  if (rc) { *out = ctx.release(); return rc; }
+  ctx->n = t->n;
+  ctx->n_blocks = t->n_blocks;
+  ctx->precision = p->precision;
+  ctx->stream_mode = p->stream_mode;
+  ctx->periodic = t->periodic;
+  ctx->drag = p->drag;
+  ctx->omega = p->omega;
+  cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "cudaStreamCreate"); *out = ctx.release(); return rc; }
+  ctx->own_stream = true;
+  rc = p->precision == OCTLB_FP32 ? create_impl<float>(ctx.get(), t, p, init)
+                                  : create_impl<__half>(ctx.get(), t, p, init);
+  *out = ctx.release();
+  return rc;
+}
+
+void octlb_gpu_destroy(octlb_ctx* ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  cudaStream_t s = ctx->own_stream ? ctx->stream : nullptr;
+  ctx->levels.clear();
+  if (s) cudaStreamDestroy(s);
+  delete ctx;
+}
+
+const char* octlb_gpu_last_error(const octlb_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int octlb_gpu_set_stream(octlb_ctx* ctx, void* s) {
+  if (!ctx) return OCTLB_EINVAL;
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  if (s) {
+    ctx->stream = static_cast<cudaStream_t>(s);
+    ctx->own_stream = false;
+  } else {
+    cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    ctx->own_stream = true;
+  }
+  return OCTLB_OK;
+}
+
+int octlb_gpu_advance(octlb_ctx* ctx, int steps) {
+  if (!ctx || steps < 0) return OCTLB_EINVAL;
+  if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
+  return ctx->precision == OCTLB_FP32 ? advance_impl<float>(ctx, steps) : advance_impl<__half>(ctx, steps);
+}
+
+int octlb_gpu_synchronize(octlb_ctx* ctx) {
+  if (!ctx) return OCTLB_EINVAL;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OCTLB_OK;
+}
+
+int octlb_gpu_set_populations(octlb_ctx* ctx, const double* pops) {
+  if (!ctx || !pops) return OCTLB_EINVAL;
+  return ctx->precision == OCTLB_FP32 ? scatter_impl<float>(ctx, pops) : scatter_impl<__half>(ctx, pops);
+}
+
+int octlb_gpu_get_populations(octlb_ctx* ctx, double* pops) {
+  if (!ctx || !pops) return OCTLB_EINVAL;
+  return ctx->precision == OCTLB_FP32 ? gather_impl<float>(ctx, pops, 0) : gather_impl<__half>(ctx, pops, 0);
+}
+
+int octlb_gpu_get_fields(octlb_ctx* ctx, double* rho, double* u) {
+  if (!ctx || !rho || !u) return OCTLB_EINVAL;
+  const long long cells = static_cast<long long>(ctx->n) * ctx->n * ctx->n * ctx->n_blocks;
+  std::vector<double> tmp(static_cast<size_t>(cells * 4));
+  const int rc = ctx->precision == OCTLB_FP32 ? gather_impl<float>(ctx, tmp.data(), 1)
+                                              : gather_impl<__half>(ctx, tmp.data(), 1);
+  if (rc) return rc;
+  for (long long k = 0; k < cells; ++k) {
+    rho[k] = tmp[4 * k];
+    u[3 * k] = tmp[4 * k + 1]; u[3 * k + 1] = tmp[4 * k + 2]; u[3 * k + 2] = tmp[4 * k + 3];
+  }
+  return OCTLB_OK;
+}
+
+int octlb_gpu_force(octlb_ctx* ctx, double out[3]) {
+  if (!ctx || !out) return OCTLB_EINVAL;
+  if (!ctx->drag) return fail(ctx, OCTLB_ESTATE, "context created without drag");
+  CK(cudaMemcpyAsync(out, ctx->force.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OCTLB_OK;
+}
+
+int octlb_gpu_force_sum(octlb_ctx* ctx, double out[3], long long* steps) {
+  if (!ctx || !out) return OCTLB_EINVAL;
+  if (!ctx->drag) return fail(ctx, OCTLB_ESTATE, "context created without drag");
+  CK(cudaMemcpyAsync(out, ctx->force_sum.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (steps) *steps = ctx->force_steps;
+  return OCTLB_OK;
+}
+
+int octlb_gpu_force_reset(octlb_ctx* ctx) {
+  if (!ctx) return OCTLB_EINVAL;
+  if (ctx->force_sum.p) CK(cudaMemsetAsync(ctx->force_sum.p, 0, 3 * sizeof(double), ctx->stream));
+  ctx->force_steps = 0;
+  return OCTLB_OK;
+}
+
+int octlb_gpu_audit(octlb_ctx* ctx, double out[4]) {
+  if (!ctx || !out) return OCTLB_EINVAL;
+  return ctx->precision == OCTLB_FP32 ? audit_impl<float>(ctx, out) : audit_impl<__half>(ctx, out);
+}
+
+int octlb_gpu_counters(const octlb_ctx* ctx, int* collide, int* stream, int max_levels) {
+  if (!ctx) return OCTLB_EINVAL;
+  const int nl = static_cast<int>(ctx->counters_collide.size());
+  for (int l = 0; l < nl && l < max_levels; ++l) {
+    if (collide) collide[l] = ctx->counters_collide[l];
+    if (stream) stream[l] = ctx->counters_stream[l];
+  }
+  return nl;
+}
+
+int octlb_gpu_max_level(const octlb_ctx* ctx) { return ctx ? ctx->max_level : OCTLB_EINVAL; }
+
+// Host-only check of the multiply-high divider the kernels use for index
+// decomposition (no device work).
+unsigned octlb_gpu_debug_fastdiv(unsigned d, unsigned n) { return FastDiv(d).div(n); }
+
+int octlb_gpu_step_stats(const octlb_ctx* ctx, long long* launches, long long* lups) {
+  if (!ctx) return OCTLB_EINVAL;
+  long long total = 0;
+  // Per level advance: ghost fill (if any ops) + step (+ drag + partial sum);
+  // per coarse level: two prolongations, per fine level: one restriction.
+  std::vector<long long> per(ctx->levels.size(), 0);
+  for (size_t l = 0; l < ctx->levels.size(); ++l) {
+    const Level& L = ctx->levels[l];
+    if (L.nblk == 0) continue;
+    per[l] = (L.n_copy_cells + L.n_bb > 0 ? 1 : 0) + (L.args.nitems > 0 ? 1 : 0) +
+             (ctx->drag && L.n_drag > 0 ? 2 : 0);
+  }
+  for (size_t l = 0; l < ctx->levels.size(); ++l) {
+    const Level& L = ctx->levels[l];
+    long long mult = 1LL << l;
+    total += per[l] * mult;
+    if (l + 1 < ctx->levels.size()) {
+      total += (L.n_prolong > 0 ? 2 : 0) * mult;
+      total += (ctx->levels[l + 1].n_restrict > 0 ? 1 : 0) * mult;
+    }
+  }
+  if (ctx->drag) total += 1;
+  if (launches) *launches = total;
+  if (lups) *lups = ctx->lups_per_step;
+  return OCTLB_OK;
+}
+
+}  // extern "C"

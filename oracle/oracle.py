@@ -1,0 +1,204 @@
+"""Python handles on the two CPU oracles.  TEST INFRASTRUCTURE ONLY: used by
+tests/, __graft_entry__.smoke() and bench.py's CPU legs as the checker, never
+by the product.
+
+* ``liboctlb_oracle.so``  -- plain-C restatement (octlb_oracle.c), always built.
+* ``_ref/liboctlb_ref.so`` -- the reference's own BlockLattice / LevelCoupler /
+  GhostSchedule / TimeLoop / MomentumExchangeDrag, compiled from its sources by
+  `make -C oracle ref` where the reference tree is available; prebuilt files
+  travel with the repository.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORC_PATH = os.path.join(HERE, "liboctlb_oracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "liboctlb_ref.so")
+Q = 19
+P = ctypes.c_void_p
+
+
+def _p(a, t=ctypes.c_double):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def build(ref=True):
+    """make -C oracle (and the reference build when its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    src = os.environ.get("OCTLB_REFERENCE", "/root/reference")
+    if ref and os.path.isdir(os.path.join(src, "src", "solver", "lbm")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={src}"], check=True)
+
+
+def load(which):
+    path = ORC_PATH if which == "orc" else REF_PATH
+    if not os.path.exists(path):
+        return None
+    L = ctypes.CDLL(path)
+    pre = "orc_" if which == "orc" else "ref_"
+    for fn in ("block_new", "sim_new"):
+        if hasattr(L, pre + fn):
+            getattr(L, pre + fn).restype = P
+    for fn in ("feq", "bouzidi_pull"):
+        getattr(L, pre + fn).restype = ctypes.c_double
+        getattr(L, pre + fn).argtypes = ([ctypes.c_int] + [ctypes.c_double] * 4 if fn == "feq"
+                                         else [ctypes.c_double] * 4)
+    if which == "orc":
+        L.orc_periodic_slabs_mlups.restype = ctypes.c_double
+        L.orc_periodic_slabs_mlups.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double, ctypes.c_int]
+    L._pre = pre
+    return L
+
+
+class Block:
+    """One BlockLattice<double> (reference layout, halo 1) in either oracle."""
+
+    def __init__(self, L, nx, ny=None, nz=None):
+        ny = nx if ny is None else ny
+        nz = nx if nz is None else nz
+        self.L, self.pre, self.shape = L, L._pre, (nx, ny, nz)
+        self.h = P(getattr(L, self.pre + "block_new")(nx, ny, nz))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            getattr(self.L, self.pre + "block_free")(self.h)
+            self.h = None
+
+    def _f(self, name):
+        return getattr(self.L, self.pre + name)
+
+    def initialize(self, rho, u):
+        self._f("block_initialize")(self.h, ctypes.c_double(rho), *[ctypes.c_double(v) for v in u])
+
+    def set_kinds(self, kinds):
+        k = np.ascontiguousarray(kinds, np.uint8)
+        self._f("block_set_kinds")(self.h, _p(k, ctypes.c_uint8))
+
+    def padded(self):
+        nx, ny, nz = self.shape
+        out = np.zeros((nx + 2, ny + 2, nz + 2, Q))
+        self._f("block_get_padded")(self.h, _p(out))
+        return out
+
+    def set_padded(self, pad):
+        a = np.ascontiguousarray(pad, np.float64)
+        self._f("block_set_padded")(self.h, _p(a))
+
+    def core(self):
+        return self.padded()[1:-1, 1:-1, 1:-1]
+
+    def set_core(self, core):
+        pad = self.padded()
+        pad[1:-1, 1:-1, 1:-1] = core
+        self.set_padded(pad)
+
+    def collide(self, omega):
+        self._f("block_collide")(self.h, ctypes.c_double(omega))
+
+    def fill_periodic(self):
+        self._f("block_fill_periodic")(self.h)
+
+    def stream(self):
+        self._f("block_stream")(self.h)
+
+    def snapshot(self):
+        self._f("block_snapshot")(self.h)
+
+    def set_links(self, cell_pop, q):
+        cp = np.ascontiguousarray(cell_pop, np.int32).reshape(-1, 4)
+        qq = np.ascontiguousarray(q, np.float64).reshape(-1)
+        self._f("block_set_links")(self.h, ctypes.c_int(len(qq)), _p(cp, ctypes.c_int), _p(qq))
+
+    def add_moving_wall(self, moving, wall_u):
+        m = np.ascontiguousarray(moving, np.uint8)
+        w = np.ascontiguousarray(wall_u, np.float64)
+        self._f("block_add_moving_wall")(self.h, _p(m, ctypes.c_uint8), _p(w))
+
+    def run_periodic(self, omega, steps):
+        self._f("block_run_periodic")(self.h, ctypes.c_double(omega), ctypes.c_int(steps))
+
+    def run_walls(self, omega, steps, moving=None, wall_u=None):
+        m = None if moving is None else np.ascontiguousarray(moving, np.uint8)
+        w = None if wall_u is None else np.ascontiguousarray(wall_u, np.float64)
+        self._f("block_run_walls")(self.h, ctypes.c_double(omega), ctypes.c_int(steps),
+                                   _p(m, ctypes.c_uint8), _p(w))
+
+    def drag(self, mask=None):
+        out = np.zeros(3)
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        self._f("block_drag")(self.h, _p(m, ctypes.c_uint8), _p(out))
+        return out
+
+
+def rho_u(pops):
+    """rho = 1 + sum f, u = sum f c / rho (block_lattice.h:113-125)."""
+    from octlb_b200 import C
+    rho = 1.0 + pops.sum(-1)
+    u = np.einsum("...q,qd->...d", pops, C.astype(np.float64)) / rho[..., None]
+    return rho, u
+
+
+class Sim:
+    """TimeLoop over a forest (reference oracle only: ref_sim_*)."""
+
+    def __init__(self, L, mesh, omega, init_pops=None, link_mode=False):
+        self.L, self.mesh = L, mesh
+        n = mesh.n
+        self._keep = [mesh]
+        init = None if init_pops is None else np.ascontiguousarray(init_pops, np.float64)
+        self._keep.append(init)
+        lc = mesh.link_cells if len(mesh.link_q) else np.zeros((0, 5), np.int32)
+        self.h = P(L.ref_sim_new(
+            ctypes.c_int(mesh.n_blocks), _p(mesh.levels, ctypes.c_int), _p(mesh.bounds),
+            ctypes.c_int(len(mesh.same_level)), _p(mesh.same_level, ctypes.c_int),
+            ctypes.c_int(len(mesh.coarse_fine)), _p(mesh.coarse_fine, ctypes.c_int), _p(mesh.coarse_fine_bounds),
+            ctypes.c_int(len(mesh.tree_boundary)), _p(mesh.tree_boundary, ctypes.c_int), _p(mesh.tree_boundary_spec),
+            ctypes.c_int(n), ctypes.c_double(omega), _p(mesh.kinds, ctypes.c_uint8), _p(init),
+            ctypes.c_int(len(mesh.link_q)), _p(np.ascontiguousarray(lc, np.int32), ctypes.c_int), _p(mesh.link_q),
+            ctypes.c_int(1 if link_mode else 0)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.ref_sim_free(self.h)
+            self.h = None
+
+    def advance(self, steps=1):
+        self.L.ref_sim_advance(self.h, ctypes.c_int(steps))
+
+    def core(self):
+        n = self.mesh.n
+        out = np.zeros((self.mesh.n_blocks, n, n, n, Q))
+        self.L.ref_sim_get_core(self.h, _p(out))
+        return out
+
+    def drag(self, mask=None):
+        out = np.zeros(3)
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        self.L.ref_sim_drag(self.h, _p(m, ctypes.c_uint8), _p(out))
+        return out
+
+    def counters(self):
+        c = np.zeros(32, np.int32)
+        s = np.zeros(32, np.int32)
+        calls = np.zeros(2 * 4096, np.int32)
+        ncalls = self.L.ref_sim_counters(self.h, _p(c, ctypes.c_int), _p(s, ctypes.c_int),
+                                         _p(calls, ctypes.c_int), ctypes.c_int(4096))
+        ml = self.L.ref_sim_max_level(self.h)
+        return c[:ml + 1].tolist(), s[:ml + 1].tolist(), calls[:2 * min(ncalls, 4096)].reshape(-1, 2).tolist()
+
+    def plan(self):
+        out = np.zeros((65536, 10), np.int32)
+        n = self.L.ref_sim_plan(self.h, _p(out, ctypes.c_int), ctypes.c_int(65536))
+        return out[:n]
+
+    def coupler_full(self, level):
+        self.L.ref_sim_coupler_full(self.h, ctypes.c_int(level))
+
+    def coupler_half(self, level):
+        self.L.ref_sim_coupler_half(self.h, ctypes.c_int(level))
+
+    def coupler_restrict(self, level):
+        self.L.ref_sim_coupler_restrict(self.h, ctypes.c_int(level))
