@@ -210,7 +210,11 @@ class GpuLattice:
     __del__ = close
 
     def set_stream(self, cuda_stream_ptr):
-        self._check(self._L.octlb_gpu_set_stream(self._h, capi.P(cuda_stream_ptr) if cuda_stream_ptr else None))
+        """Run on the caller's cudaStream_t (an integer handle); 0 / None
+        gives the context a private non-blocking stream again."""
+        if not cuda_stream_ptr:
+            raise ValueError("pass a non-default stream handle (the legacy default stream is not used)")
+        self._check(self._L.octlb_gpu_set_stream(self._h, capi.P(cuda_stream_ptr)))
 
     def advance(self, n=1):
         self._check(self._L.octlb_gpu_advance(self._h, int(n)))
@@ -232,9 +236,13 @@ class GpuLattice:
         assert a.size == self._cells() * Q
         self._check(self._L.octlb_gpu_set_populations(self._h, capi.ptr(a, ctypes.c_double)))
 
-    def get_fields(self):
-        rho = np.zeros(self._cells())
-        u = np.zeros((self._cells(), 3))
+    def get_fields(self, rho=None, u=None):
+        """rho, u of every core cell; pass preallocated (ideally pinned)
+        float64 arrays of n_blocks*n^3 and n_blocks*n^3*3 to fill in place."""
+        rho = np.zeros(self._cells()) if rho is None else rho
+        u = np.zeros((self._cells(), 3)) if u is None else u
+        assert rho.dtype == np.float64 and u.dtype == np.float64 and rho.size == self._cells() and u.size == 3 * self._cells()
+        assert rho.flags.c_contiguous and u.flags.c_contiguous
         self._check(self._L.octlb_gpu_get_fields(self._h, capi.ptr(rho, ctypes.c_double), capi.ptr(u, ctypes.c_double)))
         n = self.mesh.n
         return rho.reshape(self.mesh.n_blocks, n, n, n), u.reshape(self.mesh.n_blocks, n, n, n, 3)

@@ -381,7 +381,7 @@ k_audit(const StepArgs a, double* partial) {
 // Core cells <-> dense FP64 host order [block][ix][iy][iz][19].
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_gather(const StepArgs a, double* out, int mode /*0 pops, 1 fields*/) {
+k_gather(const StepArgs a, double* out, double* out_u, int mode /*0 pops, 1 fields*/) {
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   if (t >= a.ncore) return;
   const uint32_t n = a.n;
@@ -406,10 +406,10 @@ k_gather(const StepArgs a, double* out, int mode /*0 pops, 1 fields*/) {
       drho += v; jx += cx(i) * v; jy += cy(i) * v; jz += cz(i) * v;
     }
     const double rho = 1.0 + drho;
-    out[static_cast<long long>(t) * 4 + 0] = rho;
-    out[static_cast<long long>(t) * 4 + 1] = jx / rho;
-    out[static_cast<long long>(t) * 4 + 2] = jy / rho;
-    out[static_cast<long long>(t) * 4 + 3] = jz / rho;
+    out[t] = rho;
+    out_u[static_cast<long long>(t) * 3 + 0] = jx / rho;
+    out_u[static_cast<long long>(t) * 3 + 1] = jy / rho;
+    out_u[static_cast<long long>(t) * 3 + 2] = jz / rho;
   }
 }
 
@@ -511,8 +511,8 @@ cudaError_t launch_audit(const StepArgs& a, double* partial, double* out, cudaSt
 uint32_t audit_partials(const StepArgs& a) { return grid_for(a.ncore); }
 
 template <typename T>
-cudaError_t launch_gather(const StepArgs& a, double* out, int mode, cudaStream_t s) {
-  k_gather<T><<<grid_for(a.ncore), kThreads, 0, s>>>(a, out, mode);
+cudaError_t launch_gather(const StepArgs& a, double* out, double* out_u, int mode, cudaStream_t s) {
+  k_gather<T><<<grid_for(a.ncore), kThreads, 0, s>>>(a, out, out_u, mode);
   return cudaGetLastError();
 }
 template <typename T>
@@ -532,7 +532,7 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
   template cudaError_t launch_drag<T>(const StepArgs&, bool, const DragItem*, int, double*,        \
                                       double*, double*, cudaStream_t);                             \
   template cudaError_t launch_audit<T>(const StepArgs&, double*, double*, cudaStream_t);           \
-  template cudaError_t launch_gather<T>(const StepArgs&, double*, int, cudaStream_t);              \
+  template cudaError_t launch_gather<T>(const StepArgs&, double*, double*, int, cudaStream_t);              \
   template cudaError_t launch_scatter<T>(const StepArgs&, const double*, cudaStream_t);
 
 OCTLB_INST(float)

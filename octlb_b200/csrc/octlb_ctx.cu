@@ -31,7 +31,7 @@ template <typename T>
 cudaError_t launch_drag(const StepArgs&, bool, const DragItem*, int, double*, double*, double*,
                         cudaStream_t);
 template <typename T> cudaError_t launch_audit(const StepArgs&, double*, double*, cudaStream_t);
-template <typename T> cudaError_t launch_gather(const StepArgs&, double*, int, cudaStream_t);
+template <typename T> cudaError_t launch_gather(const StepArgs&, double*, double*, int, cudaStream_t);
 template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*, cudaStream_t);
 uint32_t drag_partials(int n);
 uint32_t audit_partials(const StepArgs& a);
@@ -852,41 +852,71 @@ int advance_impl(octlb_ctx* ctx, int steps) {
   return OCTLB_OK;
 }
 
+// Level-local block order equals a contiguous run of global ids: host
+// arrays can be copied without reordering.
+bool contiguous(const Level& L) {
+  for (int k = 1; k < L.nblk; ++k)
+    if (L.blocks[k] != L.blocks[0] + k) return false;
+  return true;
+}
+
 template <typename T>
-int gather_impl(octlb_ctx* ctx, double* out, int mode) {
-  const int n = ctx->n;
-  const long long n3 = static_cast<long long>(n) * n * n;
-  const int width = mode == 0 ? kQ : 4;
-  std::vector<double> host;
+int gather_impl(octlb_ctx* ctx, double* pops, double* rho, double* u) {
+  const long long n3 = static_cast<long long>(ctx->n) * ctx->n * ctx->n;
   for (auto& L : ctx->levels) {
     if (L.nblk == 0) continue;
-    DevBuf d;
-    CK(d.alloc(static_cast<size_t>(L.nblk * n3 * width) * sizeof(double)));
+    const long long cells = L.nblk * n3;
+    const int mode = pops ? 0 : 1;
+    DevBuf d, du;
+    CK(d.alloc(static_cast<size_t>(cells * (mode == 0 ? kQ : 1)) * sizeof(double)));
+    if (mode == 1) CK(du.alloc(static_cast<size_t>(cells * 3) * sizeof(double)));
     StepArgs a = L.args;
     a.src = L.buf[L.cur].p;
-    CK(launch_gather<T>(a, d.as<double>(), mode, ctx->stream));
-    host.resize(static_cast<size_t>(L.nblk * n3 * width));
-    CK(cudaMemcpyAsync(host.data(), d.p, host.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(launch_gather<T>(a, d.as<double>(), du.as<double>(), mode, ctx->stream));
+    const bool direct = contiguous(L);
+    const long long off = static_cast<long long>(L.blocks[0]) * n3;
+    std::vector<double> h0, h1;
+    double* o0 = mode == 0 ? pops + off * kQ : rho + off;
+    double* o1 = mode == 0 ? nullptr : u + off * 3;
+    if (!direct) {
+      h0.resize(static_cast<size_t>(cells * (mode == 0 ? kQ : 1)));
+      o0 = h0.data();
+      if (mode == 1) { h1.resize(static_cast<size_t>(cells * 3)); o1 = h1.data(); }
+    }
+    CK(cudaMemcpyAsync(o0, d.p, d.bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    if (mode == 1) CK(cudaMemcpyAsync(o1, du.p, du.bytes, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    for (int lb = 0; lb < L.nblk; ++lb)
-      std::memcpy(out + static_cast<size_t>(L.blocks[lb] * n3 * width), &host[static_cast<size_t>(lb * n3 * width)],
-                  sizeof(double) * n3 * width);
+    if (!direct) {
+      for (int lb = 0; lb < L.nblk; ++lb) {
+        const long long g = static_cast<long long>(L.blocks[lb]) * n3, l0 = lb * n3;
+        if (mode == 0) {
+          std::memcpy(pops + g * kQ, &h0[static_cast<size_t>(l0 * kQ)], sizeof(double) * n3 * kQ);
+        } else {
+          std::memcpy(rho + g, &h0[static_cast<size_t>(l0)], sizeof(double) * n3);
+          std::memcpy(u + g * 3, &h1[static_cast<size_t>(l0 * 3)], sizeof(double) * n3 * 3);
+        }
+      }
+    }
   }
   return OCTLB_OK;
 }
 
 template <typename T>
 int scatter_impl(octlb_ctx* ctx, const double* in) {
-  const int n = ctx->n;
-  const long long n3 = static_cast<long long>(n) * n * n;
+  const long long n3 = static_cast<long long>(ctx->n) * ctx->n * ctx->n;
   for (auto& L : ctx->levels) {
     if (L.nblk == 0) continue;
-    std::vector<double> dense(static_cast<size_t>(L.nblk * n3 * kQ));
-    for (int lb = 0; lb < L.nblk; ++lb)
-      std::memcpy(&dense[static_cast<size_t>(lb * n3 * kQ)], in + static_cast<size_t>(L.blocks[lb] * n3 * kQ),
-                  sizeof(double) * n3 * kQ);
+    const long long cells = L.nblk * n3;
     DevBuf d;
-    CK(upload(d, dense));
+    CK(d.alloc(static_cast<size_t>(cells * kQ) * sizeof(double)));
+    if (contiguous(L)) {
+      CK(cudaMemcpyAsync(d.p, in + static_cast<long long>(L.blocks[0]) * n3 * kQ, d.bytes,
+                         cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+      for (int lb = 0; lb < L.nblk; ++lb)
+        CK(cudaMemcpyAsync(d.as<double>() + lb * n3 * kQ, in + static_cast<long long>(L.blocks[lb]) * n3 * kQ,
+                           sizeof(double) * n3 * kQ, cudaMemcpyHostToDevice, ctx->stream));
+    }
     StepArgs a = L.args;
     a.dst = L.buf[L.cur].p;
     CK(launch_scatter<T>(a, d.as<double>(), ctx->stream));
@@ -988,21 +1018,14 @@ int octlb_gpu_set_populations(octlb_ctx* ctx, const double* pops) {
 
 int octlb_gpu_get_populations(octlb_ctx* ctx, double* pops) {
   if (!ctx || !pops) return OCTLB_EINVAL;
-  return ctx->precision == OCTLB_FP32 ? gather_impl<float>(ctx, pops, 0) : gather_impl<__half>(ctx, pops, 0);
+  return ctx->precision == OCTLB_FP32 ? gather_impl<float>(ctx, pops, nullptr, nullptr)
+                                      : gather_impl<__half>(ctx, pops, nullptr, nullptr);
 }
 
 int octlb_gpu_get_fields(octlb_ctx* ctx, double* rho, double* u) {
   if (!ctx || !rho || !u) return OCTLB_EINVAL;
-  const long long cells = static_cast<long long>(ctx->n) * ctx->n * ctx->n * ctx->n_blocks;
-  std::vector<double> tmp(static_cast<size_t>(cells * 4));
-  const int rc = ctx->precision == OCTLB_FP32 ? gather_impl<float>(ctx, tmp.data(), 1)
-                                              : gather_impl<__half>(ctx, tmp.data(), 1);
-  if (rc) return rc;
-  for (long long k = 0; k < cells; ++k) {
-    rho[k] = tmp[4 * k];
-    u[3 * k] = tmp[4 * k + 1]; u[3 * k + 1] = tmp[4 * k + 2]; u[3 * k + 2] = tmp[4 * k + 3];
-  }
-  return OCTLB_OK;
+  return ctx->precision == OCTLB_FP32 ? gather_impl<float>(ctx, nullptr, rho, u)
+                                      : gather_impl<__half>(ctx, nullptr, rho, u);
 }
 
 int octlb_gpu_force(octlb_ctx* ctx, double out[3]) {
