@@ -40,6 +40,7 @@ extern "C" {
 #define OCTLB_ENOMEM (-2)   /* device allocation failed */
 #define OCTLB_ECUDA (-3)    /* CUDA runtime error */
 #define OCTLB_ENAN (-4)     /* non-finite populations detected (audit) */
+#define OCTLB_ETIMEOUT (-5) /* a bounded device wait gave up (no hang) */
 #define OCTLB_ESTATE (-6)   /* call not valid in the context's state */
 
 /* Population storage.  FP32 stores the shifted populations f - w as float;

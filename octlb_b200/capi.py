@@ -18,6 +18,7 @@ OCTLB_EINVAL = -1
 OCTLB_ENOMEM = -2
 OCTLB_ECUDA = -3
 OCTLB_ENAN = -4
+OCTLB_ETIMEOUT = -5
 OCTLB_ESTATE = -6
 
 FP32 = 0

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -33,6 +34,9 @@ cudaError_t launch_drag(const StepArgs&, bool, const DragItem*, int, double*, do
 template <typename T> cudaError_t launch_audit(const StepArgs&, double*, double*, cudaStream_t);
 template <typename T> cudaError_t launch_gather(const StepArgs&, double*, double*, int, cudaStream_t);
 template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*, cudaStream_t);
+template <typename T> cudaError_t launch_step_bulk(const StepArgs&, int, cudaStream_t);
+template <typename T> int bulk_prepare(int n);
+bool bulk_step_eligible(int n, int elem_bytes);
 uint32_t drag_partials(int n);
 uint32_t audit_partials(const StepArgs& a);
 
@@ -89,6 +93,8 @@ struct Level {
   DevBuf drag_items, drag_partial;
   int n_drag = 0;
   float scale = 1.f, inv_scale = 1.f;
+  bool use_bulk = false;            // pipelined bulk-copy step (periodic block)
+  int bulk_grid = 0;
   StepArgs args{};
 };
 
@@ -107,10 +113,11 @@ struct octlb_ctx {
   std::vector<uint8_t> kinds;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  DevBuf force_lvl, force, force_sum, audit_out, audit_partial, host_tmp;
+  DevBuf force_lvl, force, force_sum, audit_out, audit_partial, host_tmp, dev_err;
   long long force_steps = 0;
   std::vector<int> counters_collide, counters_stream;
   long long launches_per_step = 0, lups_per_step = 0;
+  bool no_bulk = false;             // OCTLB_NO_BULK=1 forces the plain step kernel
   float prolong_scale = 0.f, restrict_scale = 0.f;
 };
 
@@ -196,8 +203,12 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
   StepArgs a = L.args;
   a.src = L.buf[L.cur].p;
   a.dst = L.buf[1 - L.cur].p;
-  CK(launch_step<T>(a, ctx->periodic != 0, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags,
-                    ctx->stream));
+  if (L.use_bulk) {
+    CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
+  } else {
+    CK(launch_step<T>(a, ctx->periodic != 0, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags,
+                      ctx->stream));
+  }
   if (ctx->drag && L.n_drag > 0) {
     CK(launch_drag<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.drag_items.as<DragItem>(), L.n_drag,
                       L.drag_partial.as<double>(), ctx->force_lvl.as<double>() + 3 * L.lvl, nullptr,
@@ -309,6 +320,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
   const long long n3 = static_cast<long long>(n) * n * n;
   const bool links = p->stream_mode == OCTLB_STREAM_LINKS;
   ctx->kinds.assign(t->kinds, t->kinds + n3 * nb);
+  CK(ctx->dev_err.alloc(sizeof(int)));
   for (int b = 0; b < nb; ++b) ctx->max_level = std::max(ctx->max_level, t->levels[b]);
   const int nlev = ctx->max_level + 1;
   ctx->levels.resize(nlev);
@@ -791,6 +803,18 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     A.scale = L.scale;
     A.inv_scale = L.inv_scale;
     for (int i = 0; i < kQ; ++i) A.off[i] = static_cast<int>(cx(i) * A.plane + cy(i) * np + cz(i));
+    A.err = ctx->dev_err.as<int>();
+    // One all-kBulk periodic block: the pipelined bulk-copy step.
+    if (ctx->periodic && !L.has_flags && !ctx->no_bulk && bulk_step_eligible(n, sizeof(T))) {
+      const int per_sm = bulk_prepare<T>(n);
+      int dev = 0, sms = 0;
+      CK(cudaGetDevice(&dev));
+      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      if (per_sm > 0) {
+        L.use_bulk = true;
+        L.bulk_grid = std::min(per_sm * sms, n * n);
+      }
+    }
   }
   // Cross-level coupler indices: prolongation targets live on level l+1,
   // restriction targets on level l-1.
@@ -834,6 +858,16 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
   long long lups = 0;
   for (int l = 0; l < nlev; ++l) lups += static_cast<long long>(ctx->levels[l].nblk) * n3 << l;
   ctx->lups_per_step = lups;
+  return OCTLB_OK;
+}
+
+// Reads the device error word (after the stream has drained).
+int check_device_error(octlb_ctx* ctx) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, ctx->dev_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (h == kErrBulkTimeout) return fail(ctx, OCTLB_ETIMEOUT, "bulk-copy wait gave up after 1 s");
+  if (h != 0) return fail(ctx, OCTLB_ECUDA, "device error word set");
   return OCTLB_OK;
 }
 
@@ -965,6 +999,7 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
   ctx->periodic = t->periodic;
   ctx->drag = p->drag;
   ctx->omega = p->omega;
+  if (const char* nb = std::getenv("OCTLB_NO_BULK")) ctx->no_bulk = nb[0] == '1';
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "cudaStreamCreate"); *out = ctx.release(); return rc; }
   ctx->own_stream = true;
@@ -1008,7 +1043,7 @@ int octlb_gpu_advance(octlb_ctx* ctx, int steps) {
 int octlb_gpu_synchronize(octlb_ctx* ctx) {
   if (!ctx) return OCTLB_EINVAL;
   CK(cudaStreamSynchronize(ctx->stream));
-  return OCTLB_OK;
+  return check_device_error(ctx);
 }
 
 int octlb_gpu_set_populations(octlb_ctx* ctx, const double* pops) {
@@ -1018,12 +1053,14 @@ int octlb_gpu_set_populations(octlb_ctx* ctx, const double* pops) {
 
 int octlb_gpu_get_populations(octlb_ctx* ctx, double* pops) {
   if (!ctx || !pops) return OCTLB_EINVAL;
+  if (int rc = check_device_error(ctx)) return rc;
   return ctx->precision == OCTLB_FP32 ? gather_impl<float>(ctx, pops, nullptr, nullptr)
                                       : gather_impl<__half>(ctx, pops, nullptr, nullptr);
 }
 
 int octlb_gpu_get_fields(octlb_ctx* ctx, double* rho, double* u) {
   if (!ctx || !rho || !u) return OCTLB_EINVAL;
+  if (int rc = check_device_error(ctx)) return rc;
   return ctx->precision == OCTLB_FP32 ? gather_impl<float>(ctx, nullptr, rho, u)
                                       : gather_impl<__half>(ctx, nullptr, rho, u);
 }
@@ -1054,6 +1091,7 @@ int octlb_gpu_force_reset(octlb_ctx* ctx) {
 
 int octlb_gpu_audit(octlb_ctx* ctx, double out[4]) {
   if (!ctx || !out) return OCTLB_EINVAL;
+  if (int rc = check_device_error(ctx)) return rc;
   return ctx->precision == OCTLB_FP32 ? audit_impl<float>(ctx, out) : audit_impl<__half>(ctx, out);
 }
 

@@ -33,7 +33,11 @@ struct StepArgs {
   FastDiv div_n, div_n2, div_n3, div_halo;
   float omega, scale, inv_scale;
   int off[kQ];              // slot offset of c_i: cx*plane + cy*np + cz
+  int* err;                 // device error word (bounded waits that gave up)
 };
+
+// Device error codes written to StepArgs::err.
+enum : int { kErrNone = 0, kErrBulkTimeout = 1 };
 
 // Rectangular halo copy (same-level face / edge exchange, outflow ghost copy):
 // dst(a,b) <- src(a,b) for all 19 populations.
