@@ -141,6 +141,72 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
   }
 }
 
+// Two-element vector access for the paired periodic kernel.
+template <typename T> struct Pair;
+template <> struct Pair<float> {
+  using V = float2;
+  __device__ static inline void ld(const float* p, float inv, float& a, float& b) {
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    a = v.x; b = v.y;
+  }
+  __device__ static inline void st(float* p, float a, float b, float) {
+    *reinterpret_cast<float2*>(p) = make_float2(a, b);
+  }
+};
+template <> struct Pair<__half> {
+  __device__ static inline void ld(const __half* p, float inv, float& a, float& b) {
+    const float2 v = __half22float2(*reinterpret_cast<const __half2*>(p));
+    a = v.x * inv; b = v.y * inv;
+  }
+  __device__ static inline void st(__half* p, float a, float b, float scale) {
+    *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a * scale, b * scale);
+  }
+};
+
+// One periodic all-kBulk block, two consecutive z cells per thread: every
+// population row is read and written with 2-element vector accesses; a z-shift
+// of +-1 takes the two aligned pairs around it.  Same arithmetic as k_step.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_step_pair(const StepArgs a) {
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  const uint32_t n = a.n, half = n >> 1;
+  if (t >= a.ncore / 2) return;
+  const uint32_t row = a.div_n.div(2 * t);  // = t / (n / 2)
+  const uint32_t z = (t - row * half) * 2;
+  const uint32_t x = a.div_n.div(row), y = row - x * n;
+  const uint32_t xm = x == 0 ? n - 1 : x - 1, xp = x == n - 1 ? 0 : x + 1;
+  const uint32_t ym = y == 0 ? n - 1 : y - 1, yp = y == n - 1 ? 0 : y + 1;
+  const uint32_t zm2 = z == 0 ? n - 2 : z - 2, zp2 = z + 2 == n ? 0 : z + 2;
+  const T* src = static_cast<const T*>(a.src);
+  T* dst = static_cast<T*>(a.dst);
+  float f0[kQ], f1[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const uint32_t sx = cx(i) == 1 ? xm : (cx(i) == -1 ? xp : x);
+    const uint32_t sy = cy(i) == 1 ? ym : (cy(i) == -1 ? yp : y);
+    const T* r = src + i * a.qs + (static_cast<long long>(sx) * n + sy) * n;
+    if (cz(i) == 0) {
+      Pair<T>::ld(r + z, a.inv_scale, f0[i], f1[i]);
+    } else if (cz(i) == 1) {  // cells z, z+1 pull z-1, z
+      float u, v, w;
+      Pair<T>::ld(r + zm2, a.inv_scale, u, v);
+      Pair<T>::ld(r + z, a.inv_scale, f1[i], w);
+      f0[i] = v;
+    } else {                  // cells z, z+1 pull z+1, z+2
+      float u, v, w;
+      Pair<T>::ld(r + z, a.inv_scale, u, f0[i]);
+      Pair<T>::ld(r + zp2, a.inv_scale, f1[i], w);
+      (void)u;
+      (void)v;
+    }
+  }
+  bgk(f0, a.omega);
+  bgk(f1, a.omega);
+  T* o = dst + static_cast<long long>(row) * n + z;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) Pair<T>::st(o + i * a.qs, f0[i], f1[i], a.scale);
+}
+
 // Ghost fill: copy descriptors first (one thread per cell of a region, all 19
 // populations), then single-population bounce-back writes.
 template <typename T>
@@ -460,6 +526,14 @@ cudaError_t launch_step(const StepArgs& a, bool periodic, bool links, bool flags
 }
 
 template <typename T>
+cudaError_t launch_step_pair(const StepArgs& a, cudaStream_t s) {
+  k_step_pair<T><<<grid_for(a.ncore / 2), kThreads, 0, s>>>(a);
+  return cudaGetLastError();
+}
+// Paired kernel: even n (aligned pairs), n^3 < 2^31.
+bool pair_step_eligible(int n) { return n >= 4 && (n % 2) == 0 && n <= 1024; }
+
+template <typename T>
 cudaError_t launch_ghost(T* pops, long long qs, const CopyDesc* cd, const uint32_t* cd_start, int ncd,
                          uint32_t ncopy, const BBOp* bb, uint32_t nbb, float scale, float inv_scale,
                          cudaStream_t s) {
@@ -523,6 +597,7 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
 
 #define OCTLB_INST(T)                                                                              \
   template cudaError_t launch_step<T>(const StepArgs&, bool, bool, bool, cudaStream_t);            \
+  template cudaError_t launch_step_pair<T>(const StepArgs&, cudaStream_t);                         \
   template cudaError_t launch_ghost<T>(T*, long long, const CopyDesc*, const uint32_t*, int,       \
                                        uint32_t, const BBOp*, uint32_t, float, float, cudaStream_t); \
   template cudaError_t launch_prolong<T>(const ProlongItem*, int, const float*, float*, int, T*,   \

@@ -36,6 +36,8 @@ template <typename T> cudaError_t launch_gather(const StepArgs&, double*, double
 template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*, cudaStream_t);
 template <typename T> cudaError_t launch_step_bulk(const StepArgs&, int, cudaStream_t);
 template <typename T> int bulk_prepare(int n);
+template <typename T> cudaError_t launch_step_pair(const StepArgs&, cudaStream_t);
+bool pair_step_eligible(int n);
 bool bulk_step_eligible(int n, int elem_bytes);
 uint32_t drag_partials(int n);
 uint32_t audit_partials(const StepArgs& a);
@@ -94,6 +96,7 @@ struct Level {
   int n_drag = 0;
   float scale = 1.f, inv_scale = 1.f;
   bool use_bulk = false;            // pipelined bulk-copy step (periodic block)
+  bool use_pair = false;            // two-cells-per-thread step (periodic block)
   int bulk_grid = 0;
   StepArgs args{};
 };
@@ -117,7 +120,7 @@ struct octlb_ctx {
   long long force_steps = 0;
   std::vector<int> counters_collide, counters_stream;
   long long launches_per_step = 0, lups_per_step = 0;
-  bool no_bulk = false;             // OCTLB_NO_BULK=1 forces the plain step kernel
+  int step_kernel = 0;              // OCTLB_STEP_KERNEL: 0 pair (default), 1 bulk, 2 plain
   float prolong_scale = 0.f, restrict_scale = 0.f;
 };
 
@@ -205,6 +208,8 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
   a.dst = L.buf[1 - L.cur].p;
   if (L.use_bulk) {
     CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
+  } else if (L.use_pair) {
+    CK(launch_step_pair<T>(a, ctx->stream));
   } else {
     CK(launch_step<T>(a, ctx->periodic != 0, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags,
                       ctx->stream));
@@ -804,8 +809,12 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     A.inv_scale = L.inv_scale;
     for (int i = 0; i < kQ; ++i) A.off[i] = static_cast<int>(cx(i) * A.plane + cy(i) * np + cz(i));
     A.err = ctx->dev_err.as<int>();
-    // One all-kBulk periodic block: the pipelined bulk-copy step.
-    if (ctx->periodic && !L.has_flags && !ctx->no_bulk && bulk_step_eligible(n, sizeof(T))) {
+    // One all-kBulk periodic block: paired vector step by default, the
+    // pipelined bulk-copy step on request (OCTLB_STEP_KERNEL=bulk), the plain
+    // one-cell-per-thread step with OCTLB_STEP_KERNEL=plain.
+    const bool uniform = ctx->periodic && !L.has_flags;
+    if (uniform && ctx->step_kernel == 0 && pair_step_eligible(n)) L.use_pair = true;
+    if (uniform && ctx->step_kernel == 1 && bulk_step_eligible(n, sizeof(T))) {
       const int per_sm = bulk_prepare<T>(n);
       int dev = 0, sms = 0;
       CK(cudaGetDevice(&dev));
@@ -999,7 +1008,10 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
   ctx->periodic = t->periodic;
   ctx->drag = p->drag;
   ctx->omega = p->omega;
-  if (const char* nb = std::getenv("OCTLB_NO_BULK")) ctx->no_bulk = nb[0] == '1';
+  if (const char* sk = std::getenv("OCTLB_STEP_KERNEL")) {
+    const std::string v(sk);
+    ctx->step_kernel = v == "bulk" ? 1 : (v == "plain" ? 2 : 0);
+  }
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "cudaStreamCreate"); *out = ctx.release(); return rc; }
   ctx->own_stream = true;

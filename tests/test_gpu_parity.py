@@ -148,17 +148,18 @@ def test_audit_mass_conserved_periodic(ob):
 
 
 @pytest.mark.parametrize("prec", ["fp32", "fp16"])
-def test_bulk_pipeline_bitwise_equals_plain_kernel(ob, prec, monkeypatch):
-    """The pipelined bulk-copy step and the plain step kernel compute the same
-    arithmetic on the same pulled values: identical populations."""
+def test_step_kernel_variants_bitwise_equal(ob, prec, monkeypatch):
+    """The paired vector step, the pipelined bulk-copy step and the plain step
+    kernel compute the same arithmetic on the same pulled values: identical
+    populations."""
     from octlb_b200 import cases
     p = ob.FP32 if prec == "fp32" else ob.FP16_SHIFTED
     mesh, init, info = cases.tgv_periodic(64, u0=0.05, tau=0.55)
     outs = []
-    for no_bulk in ("0", "1"):
-        monkeypatch.setenv("OCTLB_NO_BULK", no_bulk)
+    for variant in ("pair", "bulk", "plain"):
+        monkeypatch.setenv("OCTLB_STEP_KERNEL", variant)
         lat = ob.GpuLattice(mesh, info["omega"], precision=p, init_pops=init)
         lat.advance(25)
         outs.append(lat.get_populations())
         lat.close()
-    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
