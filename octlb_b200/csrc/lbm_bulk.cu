@@ -132,13 +132,13 @@ __global__ void __launch_bounds__(1024) k_step_bulk(const StepArgs a) {
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
       const uint32_t zs = cz(i) == 1 ? zm : (cz(i) == -1 ? zp : z);
-      f[i] = Store<T>::ld(S + i * n + zs, a.inv_scale);
+      f[i] = Store<T>::ld(S + i * n + zs, 1.0f);
     }
-    bgk(f, a.omega);
+    bgk(f, a.omega, a.scale, a.inv_scale);  // storage units h = s (f - w)
     const uint32_t row = blockIdx.x + k * gridDim.x;
     T* o = dst + static_cast<long long>(row) * n + z;
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) Store<T>::st(o + i * a.qs, f[i], a.scale);
+    for (int i = 0; i < kQ; ++i) Store<T>::st(o + i * a.qs, f[i], 1.0f);
   }
 }
 

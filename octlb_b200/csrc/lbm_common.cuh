@@ -86,29 +86,8 @@ template <> struct Store<__half> {
   }
 };
 
-// Shifted second-order equilibrium minus t_i, in the cancellation-free form
-// t_i (drho + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u^2)) with drho = rho - 1; equal to
-// rho t_i (1 + 3cu + 4.5cu^2 - 1.5u^2) - t_i (src/solver/lbm/dynamics/lbm.h:50-64).
-template <int I>
-__device__ __forceinline__ float feq_shifted(float drho, float rho, float ux, float uy, float uz,
-                                             float usq15) {
-  const float cu = cx(I) * ux + cy(I) * uy + cz(I) * uz;
-  return wf(I) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - usq15));
-}
-
-// In-register BGK (block_lattice.cpp:328-341): moments of the shifted
-// populations, rho = 1 + sum f, u = sum f c / rho, then f += omega (feq - f).
-template <int I = 0>
-__device__ __forceinline__ void bgk_apply(float (&f)[kQ], float omega, float drho, float rho,
-                                          float ux, float uy, float uz, float usq15) {
-  if constexpr (I < kQ) {
-    f[I] += omega * (feq_shifted<I>(drho, rho, ux, uy, uz, usq15) - f[I]);
-    bgk_apply<I + 1>(f, omega, drho, rho, ux, uy, uz, usq15);
-  }
-}
 __device__ __forceinline__ void moments(const float (&f)[kQ], float& drho, float& jx, float& jy,
                                         float& jz) {
-  // Pairwise grouping of opposite directions keeps the sums short.
   drho = f[0];
   jx = 0.f; jy = 0.f; jz = 0.f;
 #pragma unroll
@@ -119,14 +98,32 @@ __device__ __forceinline__ void moments(const float (&f)[kQ], float& drho, float
     if (cz(i)) jz += cz(i) * f[i];
   }
 }
-__device__ __forceinline__ void bgk(float (&f)[kQ], float omega) {
-  float drho, jx, jy, jz;
-  moments(f, drho, jx, jy, jz);
-  const float rho = 1.0f + drho;
-  const float inv = 1.0f / rho;
-  const float ux = jx * inv, uy = jy * inv, uz = jz * inv;
-  const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
-  bgk_apply(f, omega, drho, rho, ux, uy, uz, usq15);
+
+// In-register BGK on populations stored as h = s (f - w) (s = 1 for FP32
+// storage): the moments of the shifted populations (rho = 1 + sum f,
+// u = sum f c / rho, block_lattice.h:113-125), then f += omega (feq - f) with
+// the shifted second-order equilibrium (dynamics/lbm.h:50-64,
+// block_lattice.cpp:328-341) rewritten per direction as
+//   s (feq_i - w_i) = w_i (c0 + cu (3 A + 4.5 A cu)),  A = s rho,
+//   c0 = s (rho - 1) - 1.5 A |u|^2,
+// which has no cancellation against w_i and keeps the scale out of the
+// per-population work.  Arithmetic is FP32.
+__device__ __forceinline__ void bgk(float (&f)[kQ], float omega, float s = 1.0f, float inv_s = 1.0f) {
+  float dh, jx, jy, jz;
+  moments(f, dh, jx, jy, jz);
+  const float rho = 1.0f + dh * inv_s;
+  const float k = inv_s / rho;
+  const float ux = jx * k, uy = jy * k, uz = jz * k;
+  const float A = s * rho;
+  const float a3 = 3.0f * A, b45 = 4.5f * A;
+  const float c0 = dh - 1.5f * A * (ux * ux + uy * uy + uz * uz);
+  const float om1 = 1.0f - omega;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const float cu = (cx(i) ? cx(i) * ux : 0.f) + (cy(i) ? cy(i) * uy : 0.f) + (cz(i) ? cz(i) * uz : 0.f);
+    const float t = i == 0 ? c0 : fmaf(cu, fmaf(b45, cu, a3), c0);
+    f[i] = fmaf(omega * wf(i), t, om1 * f[i]);
+  }
 }
 
 // Bouzidi interpolated bounce-back with the reference's argument roles

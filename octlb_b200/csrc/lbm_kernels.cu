@@ -91,8 +91,17 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
         const uint32_t sx = cx(i) == 1 ? xm : (cx(i) == -1 ? xp : x);
         const uint32_t sy = cy(i) == 1 ? ym : (cy(i) == -1 ? yp : y);
         const uint32_t sz = cz(i) == 1 ? zm : (cz(i) == -1 ? zp : z);
-        f[i] = LD(src, a.qs, i, (static_cast<long long>(sx) * n + sy) * n + sz, a.inv_scale);
+        f[i] = Store<T>::ld(src + i * a.qs + (static_cast<long long>(sx) * n + sy) * n + sz, 1.0f);
       }
+      // scaled units throughout (h = s (f - w))
+      if constexpr (FLAGS) {
+        if ((fl & kKindMask) == kBulk) bgk(f, a.omega, a.scale, a.inv_scale);
+      } else {
+        bgk(f, a.omega, a.scale, a.inv_scale);
+      }
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + slot, f[i], 1.0f);
+      return;
     } else {
       slot = b * a.bstride + ((x + 1) * a.np + (y + 1)) * a.np + (z + 1);
       if constexpr (FLAGS) fl = a.flags[slot];
@@ -154,12 +163,12 @@ template <> struct Pair<float> {
   }
 };
 template <> struct Pair<__half> {
-  __device__ static inline void ld(const __half* p, float inv, float& a, float& b) {
+  __device__ static inline void ld(const __half* p, float, float& a, float& b) {
     const float2 v = __half22float2(*reinterpret_cast<const __half2*>(p));
-    a = v.x * inv; b = v.y * inv;
+    a = v.x; b = v.y;
   }
-  __device__ static inline void st(__half* p, float a, float b, float scale) {
-    *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a * scale, b * scale);
+  __device__ static inline void st(__half* p, float a, float b, float) {
+    *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a, b);
   }
 };
 
@@ -200,8 +209,9 @@ __global__ void __launch_bounds__(kThreads) k_step_pair(const StepArgs a) {
       (void)v;
     }
   }
-  bgk(f0, a.omega);
-  bgk(f1, a.omega);
+  // populations stay in storage units h = s (f - w); the scale lives in bgk
+  bgk(f0, a.omega, a.scale, a.inv_scale);
+  bgk(f1, a.omega, a.scale, a.inv_scale);
   T* o = dst + static_cast<long long>(row) * n + z;
 #pragma unroll
   for (int i = 0; i < kQ; ++i) Pair<T>::st(o + i * a.qs, f0[i], f1[i], a.scale);
