@@ -86,17 +86,24 @@ template <> struct Store<__half> {
   }
 };
 
+// Moments from opposite pairs: d_i = f_i - f_opp(i) for the nine positive
+// directions is nearly exact (the two are close), so the momentum sums carry
+// far less rounding than a running sum of mixed-sign terms.
 __device__ __forceinline__ void moments(const float (&f)[kQ], float& drho, float& jx, float& jy,
                                         float& jz) {
-  drho = f[0];
-  jx = 0.f; jy = 0.f; jz = 0.f;
-#pragma unroll
-  for (int i = 1; i < kQ; ++i) {
-    drho += f[i];
-    if (cx(i)) jx += cx(i) * f[i];
-    if (cy(i)) jy += cy(i) * f[i];
-    if (cz(i)) jz += cz(i) * f[i];
-  }
+  // positive directions 10..18 and their opposites 1..9
+  const float d10 = f[10] - f[1], d11 = f[11] - f[2], d12 = f[12] - f[3];
+  const float d13 = f[13] - f[4], d14 = f[14] - f[5], d15 = f[15] - f[6];
+  const float d16 = f[16] - f[7], d17 = f[17] - f[8], d18 = f[18] - f[9];
+  // c_10 = +x, c_11 = +y, c_12 = +z, c_13 = (1,1,0), c_14 = (1,-1,0),
+  // c_15 = (1,0,1), c_16 = (1,0,-1), c_17 = (0,1,1), c_18 = (0,1,-1)
+  jx = ((d10 + d13) + (d14 + d15)) + d16;
+  jy = ((d11 + d13) - d14) + ((d17 + d18));
+  jz = ((d12 + d15) - d16) + (d17 - d18);
+  const float s1 = (f[1] + f[10]) + (f[2] + f[11]) + (f[3] + f[12]);
+  const float s2 = ((f[4] + f[13]) + (f[5] + f[14])) + ((f[6] + f[15]) + (f[7] + f[16]));
+  const float s3 = (f[8] + f[17]) + (f[9] + f[18]);
+  drho = f[0] + (s1 + (s2 + s3));
 }
 
 // In-register BGK on populations stored as h = s (f - w) (s = 1 for FP32

@@ -163,3 +163,59 @@ def test_step_kernel_variants_bitwise_equal(ob, prec, monkeypatch):
         outs.append(lat.get_populations())
         lat.close()
     assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+
+
+def small_cylinder(ob):
+    from octlb_b200 import cases
+    return cases.cylinder_forest(length=128, height=32, n=8, diameter=8.0, center=(32.0, 16.0),
+                                 levels=2, u_max=0.05, re=40.0)
+
+
+def test_cylinder_two_levels_matches_reference_with_drag(ob, ref):
+    """Two-level channel with an exact-circle Bouzidi cylinder, parabolic
+    inlet, zero-gradient outlet, periodic z: fields and the momentum-exchange
+    force per coarse step against the reference TimeLoop + MomentumExchangeDrag."""
+    mesh, init, info = small_cylinder(ob)
+    assert len(mesh.link_q) > 0 and len(mesh.coarse_fine) > 0
+    lat = ob.GpuLattice(mesh, info["omega"], stream_mode=ob.STREAM_LINKS, drag=True, init_pops=init)
+    sim = oracle.Sim(ref, mesh, info["omega"], init, link_mode=True)
+    for step in range(12):
+        lat.advance(1)
+        sim.advance(1)
+        fg, fr = lat.force(), sim.drag(mesh.obstacle)
+        assert np.max(np.abs(fg - fr)) <= 1e-5 * max(np.max(np.abs(fr)), 1e-6), (step, fg, fr)
+    rho_g, u_g = lat.get_fields()
+    rho_r, u_r = fields_of(sim.core())
+    fl = mesh.kinds == ob.BULK
+    assert rel(rho_g[fl], rho_r[fl]) <= TOL32
+    assert rel(u_g[fl], u_r[fl]) <= TOL32
+    fs, n = lat.force_sum()
+    assert n == 12 and np.all(np.isfinite(fs))
+
+
+def test_cylinder_fp16_drag_close_to_fp32(ob):
+    mesh, init, info = small_cylinder(ob)
+    forces = {}
+    for p in (ob.FP32, ob.FP16_SHIFTED):
+        lat = ob.GpuLattice(mesh, info["omega"], precision=p, stream_mode=ob.STREAM_LINKS, drag=True,
+                            init_pops=init)
+        lat.advance(200)
+        lat.force_reset()
+        lat.advance(100)
+        forces[p] = lat.force_sum()[0] / 100.0
+        lat.close()
+    f32, f16 = forces[ob.FP32], forces[ob.FP16_SHIFTED]
+    assert abs(f16[0] - f32[0]) <= 1e-2 * abs(f32[0])
+
+
+def test_amr_cavity_fp16_fields(ob, ref):
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=8)
+    lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP16_SHIFTED, init_pops=init)
+    lat.advance(10)
+    rho_g, u_g = lat.get_fields()
+    sim = oracle.Sim(ref, mesh, info["omega"], init)
+    sim.advance(10)
+    rho_r, u_r = fields_of(sim.core())
+    assert rel(u_g, u_r) <= 5e-3
+    assert rel(rho_g, rho_r) <= 5e-3
