@@ -114,7 +114,9 @@ __device__ __forceinline__ void moments(const float (&f)[kQ], float& drho, float
 //   s (feq_i - w_i) = w_i (c0 + cu (3 A + 4.5 A cu)),  A = s rho,
 //   c0 = s (rho - 1) - 1.5 A |u|^2,
 // which has no cancellation against w_i and keeps the scale out of the
-// per-population work.  Arithmetic is FP32.
+// per-population work.  The relaxation is applied to the small difference,
+// f + omega fma(w_i, t, -f), never as (1 - omega) f + omega feq, whose two
+// large terms cancel.  Arithmetic is FP32.
 __device__ __forceinline__ void bgk(float (&f)[kQ], float omega, float s = 1.0f, float inv_s = 1.0f) {
   float dh, jx, jy, jz;
   moments(f, dh, jx, jy, jz);
@@ -124,12 +126,11 @@ __device__ __forceinline__ void bgk(float (&f)[kQ], float omega, float s = 1.0f,
   const float A = s * rho;
   const float a3 = 3.0f * A, b45 = 4.5f * A;
   const float c0 = dh - 1.5f * A * (ux * ux + uy * uy + uz * uz);
-  const float om1 = 1.0f - omega;
 #pragma unroll
   for (int i = 0; i < kQ; ++i) {
     const float cu = (cx(i) ? cx(i) * ux : 0.f) + (cy(i) ? cy(i) * uy : 0.f) + (cz(i) ? cz(i) * uz : 0.f);
     const float t = i == 0 ? c0 : fmaf(cu, fmaf(b45, cu, a3), c0);
-    f[i] = fmaf(omega * wf(i), t, om1 * f[i]);
+    f[i] = fmaf(omega, fmaf(wf(i), t, -f[i]), f[i]);
   }
 }
 
