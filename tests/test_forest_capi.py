@@ -155,3 +155,37 @@ def test_lattice_updates_per_coarse_step(ob):
     # TimeLoop recursion from level 0: a level-l leaf is stepped 2^l times
     exp = sum((8 ** 3) << int(l) for l in mesh.levels)
     assert mesh.lattice_updates_per_coarse_step() == exp
+
+
+def test_cpp_adapter_compiles_links_and_reports_errors(ob, tmp_path):
+    """include/octlb_gpu_time_loop.hpp (TimeLoop method names over the C ABI)
+    compiles against the library; invalid tables raise std::runtime_error
+    before any device work."""
+    import subprocess
+    src = tmp_path / "adapter.cpp"
+    src.write_text(r'''
+#include "octlb_gpu_time_loop.hpp"
+#include <cstdio>
+int main() {
+  octlb_tables t{};
+  octlb_params p{};
+  t.n = 3;  // odd block edge: rejected by validation
+  t.n_blocks = 1;
+  int lv = 0; double bd[6] = {0,0,0,1,1,1}; unsigned char k[27] = {0};
+  t.levels = &lv; t.bounds = bd; t.kinds = k;
+  p.omega = 1.5;
+  try {
+    octlb::GpuTimeLoop loop(t, p);
+    return 2;
+  } catch (const std::runtime_error& e) {
+    std::printf("%s\n", e.what());
+    return 0;
+  }
+}
+''')
+    exe = tmp_path / "adapter"
+    lib_dir = os.path.join(ROOT, "octlb_b200")
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", lib_dir, "-loctlb_b200", f"-Wl,-rpath,{lib_dir}"], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0 and "even" in r.stdout
