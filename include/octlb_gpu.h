@@ -130,6 +130,20 @@ int octlb_gpu_force_reset(octlb_ctx* ctx);
  * returns OCTLB_ENAN if any population is not finite. */
 int octlb_gpu_audit(octlb_ctx* ctx, double out[4]);
 
+/* Mass / momentum audit that allocates nothing on the device: same result as
+ * octlb_gpu_audit, for callers that must not call cudaMalloc / cudaFree (an
+ * application whose device memory is owned by another allocator, or a
+ * per-step monitoring loop that cannot afford their implicit device
+ * synchronisation).  It has no counterpart in the reference (whose audit is
+ * a host loop).  Its partial sums live in one fixed file-scope device array of
+ * 16,385 x 5 doubles (~640 KB), held by every GPU that loads the library until
+ * the process exits; levels of more than 33,554,432 cells are rejected with
+ * OCTLB_EINVAL.  The first call made on a device looks up that array's device
+ * address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture; call with the context's device current.  All calls share the
+ * array: calls that overlap on the GPU race. */
+int octlb_gpu_audit_noalloc(octlb_ctx* ctx, double out[4]);
+
 /* Per-level collide / stream counts and max level (TimeLoop::counters). */
 int octlb_gpu_counters(const octlb_ctx* ctx, int* collide, int* stream, int max_levels);
 int octlb_gpu_max_level(const octlb_ctx* ctx);

@@ -83,6 +83,7 @@ def lib():
         "octlb_gpu_force_sum": (ctypes.c_int, [P, F64P, ctypes.POINTER(ctypes.c_longlong)]),
         "octlb_gpu_force_reset": (ctypes.c_int, [P]),
         "octlb_gpu_audit": (ctypes.c_int, [P, F64P]),
+        "octlb_gpu_audit_noalloc": (ctypes.c_int, [P, F64P]),
         "octlb_gpu_counters": (ctypes.c_int, [P, I32P, I32P, ctypes.c_int]),
         "octlb_gpu_max_level": (ctypes.c_int, [P]),
         "octlb_gpu_step_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),

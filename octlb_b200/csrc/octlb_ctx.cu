@@ -1151,3 +1151,144 @@ int octlb_gpu_step_stats(const octlb_ctx* ctx, long long* launches, long long* l
 }
 
 }  // extern "C"
+
+// ==================================================== allocation-free audit
+// octlb_gpu_audit_noalloc: the mass / momentum audit with its per-CTA
+// partial sums in a fixed, file-scope device array instead of a cudaMalloc'd
+// buffer, for callers that must not allocate device memory.  The array holds
+// kNoAllocRows partial rows (one per CTA of 256 threads x 8 cells) plus one
+// result row; every GPU that loads this library keeps it until exit.  Its
+// device address is looked up with cudaGetSymbolAddress once per device, on
+// the first call made with that device current.  Every call overwrites the
+// whole array (no state carries over), so calls that overlap on the GPU race.
+namespace octlb_host {
+
+constexpr int kNoAllocRows = 16384;                 // partial rows (640 KB)
+constexpr int kNoAllocCellsPerCta = 256 * 8;
+constexpr long long kNoAllocMaxCells = static_cast<long long>(kNoAllocRows) * kNoAllocCellsPerCta;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_scratch[(kNoAllocRows + 1) * 5];
+static double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_audit_noalloc(const StepArgs a, double* rows) {
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  const uint32_t n = a.n;
+  for (int k = 0; k < 8; ++k) {
+    const uint32_t t = blockIdx.x * kNoAllocCellsPerCta + k * 256 + threadIdx.x;
+    if (t >= a.ncore) break;
+    const uint32_t b = a.div_n3.div(t);
+    uint32_t r = t - b * n * n * n;
+    const uint32_t x = a.div_n2.div(r);
+    r -= x * n * n;
+    const uint32_t y = a.div_n.div(r);
+    const uint32_t z = r - y * n;
+    const long long slot = a.np == static_cast<int>(n)
+                               ? (static_cast<long long>(x) * n + y) * n + z
+                               : b * a.bstride + ((x + 1) * a.np + (y + 1)) * a.np + (z + 1);
+    const T* src = static_cast<const T*>(a.src);
+    double drho = 0, jx = 0, jy = 0, jz = 0;
+    bool finite = true;
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      const float v = Store<T>::ld(src + i * a.qs + slot, a.inv_scale);
+      finite = finite && isfinite(v);
+      drho += v; jx += cx(i) * static_cast<double>(v);
+      jy += cy(i) * static_cast<double>(v); jz += cz(i) * static_cast<double>(v);
+    }
+    if (!finite) acc[4] = 1.0;
+    const int kind = a.flags ? (a.flags[slot] & kKindMask) : kBulk;
+    if (kind == kBulk) {
+      acc[0] += 1.0 + drho; acc[1] += jx; acc[2] += jy; acc[3] += jz;
+    }
+  }
+  __shared__ double sm[8][5];
+  for (int c = 0; c < 5; ++c)
+    for (int o = 16; o > 0; o >>= 1) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o);
+  if ((threadIdx.x & 31) == 0)
+    for (int c = 0; c < 5; ++c) sm[threadIdx.x >> 5][c] = acc[c];
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += sm[w][threadIdx.x];
+    rows[blockIdx.x * 5 + threadIdx.x] = s;
+  }
+}
+
+// Fixed-order sum of the partial rows into the result row: strided
+// per-thread sums, then a fixed shuffle tree (deterministic).
+__global__ void __launch_bounds__(256) k_audit_noalloc_sum(double* rows, int nrows) {
+  __shared__ double sm[8];
+  for (int c = 0; c < 5; ++c) {
+    double v = 0.0;
+    for (int r = threadIdx.x; r < nrows; r += 256) v += rows[r * 5 + c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < 8; ++w) s += sm[w];
+      rows[kNoAllocRows * 5 + c] = s;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+int audit_noalloc_impl(octlb_ctx* ctx, double* scratch, double out[4]) {
+  double tot[5] = {0, 0, 0, 0, 0};
+  for (auto& L : ctx->levels) {
+    if (L.nblk == 0) continue;
+    StepArgs a = L.args;
+    a.src = L.buf[L.cur].p;
+    const int nrows = static_cast<int>((a.ncore + kNoAllocCellsPerCta - 1) / kNoAllocCellsPerCta);
+    k_audit_noalloc<T><<<nrows, 256, 0, ctx->stream>>>(a, scratch);
+    CK(cudaGetLastError());
+    k_audit_noalloc_sum<<<1, 256, 0, ctx->stream>>>(scratch, nrows);
+    CK(cudaGetLastError());
+    double h[5];
+    CK(cudaMemcpyAsync(h, scratch + kNoAllocRows * 5, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < 5; ++k) tot[k] += h[k];
+  }
+  for (int k = 0; k < 4; ++k) out[k] = tot[k];
+  if (tot[4] != 0.0) return fail(ctx, OCTLB_ENAN, "non-finite populations");
+  return OCTLB_OK;
+}
+
+}  // namespace octlb_host
+
+extern "C" int octlb_gpu_audit_noalloc(octlb_ctx* ctx, double out[4]) {
+  if (!ctx || !out) return OCTLB_EINVAL;
+  if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
+  for (const auto& L : ctx->levels) {
+    if (static_cast<long long>(L.args.ncore) > kNoAllocMaxCells)
+      return fail(ctx, OCTLB_EINVAL,
+                  "octlb_gpu_audit_noalloc: a level has " + std::to_string(L.args.ncore) +
+                      " cells, more than the " + std::to_string(kNoAllocMaxCells) +
+                      " its fixed device scratch covers");
+  }
+  // The context's buffers must live on the current device.
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  for (const auto& L : ctx->levels) {
+    if (!L.buf[0].p) continue;
+    cudaPointerAttributes attr{};
+    CK(cudaPointerGetAttributes(&attr, L.buf[0].p));
+    if (attr.device != dev)
+      return fail(ctx, OCTLB_EINVAL, "octlb_gpu_audit_noalloc: make the context's device current first");
+    break;
+  }
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(ctx, OCTLB_EINVAL, "device ordinal out of range");
+  // One-time set-up on this device: the scratch array's device address.  In
+  // host code the array's name is only a host-side stand-in, never a device
+  // address, so the kernels receive this pointer.
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  return ctx->precision == OCTLB_FP32 ? audit_noalloc_impl<float>(ctx, g_noalloc_ptr[dev], out)
+                                      : audit_noalloc_impl<__half>(ctx, g_noalloc_ptr[dev], out);
+}
