@@ -87,51 +87,54 @@ def cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=0):
 
 
 def circle_links(mesh, center, radius, axis_free=2):
-    """Exact-circle Bouzidi q for every fluid cell whose D3Q19 source x - c_i
-    lies inside the circle (cylinder along `axis_free`): q solves
-    |x - t c_i - center| = R for the first t in (0, 1] (host FP64), in units
-    of the block's cell width.  Marks cells inside as SOLID in mesh.kinds."""
+    """Exact-circle Bouzidi q for every non-solid cell x and D3Q19 direction i
+    whose source x - c_i is an in-block cell inside the circle (cylinder along
+    `axis_free`): q is the first root t in (0, 1] of |x - t c_i dx - center| = R
+    (host FP64), the fraction of the link from x to the wall.  Marks the cells
+    inside as SOLID in mesh.kinds."""
     n = mesh.n
     ax = [a for a in range(3) if a != axis_free]
     cells, qs = [], []
+    idx = np.arange(n)
     for b in range(mesh.n_blocks):
         bd = mesh.bounds[b]
         dx = (bd[3] - bd[0]) / n
-        idx = np.arange(n)
         ctr = [bd[a] + (idx + 0.5) * dx for a in range(3)]
         X = np.meshgrid(*ctr, indexing="ij")
-        r2 = (X[ax[0]] - center[0]) ** 2 + (X[ax[1]] - center[1]) ** 2
-        inside = r2 < radius * radius
-        mesh.kinds[b][inside] = SOLID
-    for b in range(mesh.n_blocks):
-        bd = mesh.bounds[b]
-        dx = (bd[3] - bd[0]) / n
+        px, py = X[ax[0]] - center[0], X[ax[1]] - center[1]
+        inside = px * px + py * py < radius * radius
+        if not inside.any():
+            continue
         kinds = mesh.kinds[b]
-        fluid = np.argwhere(kinds != SOLID)
-        for (x, y, z) in fluid:
-            p = np.array([bd[0] + (x + 0.5) * dx, bd[1] + (y + 0.5) * dx, bd[2] + (z + 0.5) * dx])
-            for i in range(1, Q):
-                s = np.array([x, y, z]) - C[i]
-                if np.any(s < 0) or np.any(s >= n):
-                    continue
-                if kinds[s[0], s[1], s[2]] != SOLID:
-                    continue
-                # segment p -> p - c_i dx crosses the circle: solve |p - t d - c| = R
-                d = -C[i].astype(float) * dx
-                px, py = p[ax[0]] - center[0], p[ax[1]] - center[1]
-                dx_, dy_ = d[ax[0]], d[ax[1]]
-                a2 = dx_ * dx_ + dy_ * dy_
-                if a2 == 0.0:
-                    continue
-                b2 = 2 * (px * dx_ + py * dy_)
-                c2 = px * px + py * py - radius * radius
-                disc = b2 * b2 - 4 * a2 * c2
-                if disc < 0:
-                    continue
-                t = (-b2 - math.sqrt(disc)) / (2 * a2)
-                if 0.0 < t <= 1.0:
-                    cells.append((b, x, y, z, i))
-                    qs.append(t)
+        kinds[inside] = SOLID
+        solid = kinds == SOLID
+        for i in range(1, Q):
+            c = C[i]
+            # x - c_i in block and solid, x itself not solid
+            src = np.zeros((n, n, n), bool)
+            sl_dst = tuple(slice(max(0, c[a]), n + min(0, c[a])) for a in range(3))
+            sl_src = tuple(slice(max(0, -c[a]), n - max(0, c[a])) for a in range(3))
+            src[sl_dst] = solid[sl_src]
+            cand = src & ~solid
+            if not cand.any():
+                continue
+            d = -c.astype(float) * dx
+            dx_, dy_ = d[ax[0]], d[ax[1]]
+            a2 = dx_ * dx_ + dy_ * dy_
+            if a2 == 0.0:
+                continue
+            qx, qy = px[cand], py[cand]
+            b2 = 2 * (qx * dx_ + qy * dy_)
+            c2 = qx * qx + qy * qy - radius * radius
+            disc = b2 * b2 - 4 * a2 * c2
+            ok = disc >= 0
+            t = np.full(qx.shape, -1.0)
+            t[ok] = (-b2[ok] - np.sqrt(disc[ok])) / (2 * a2)
+            good = (t > 0.0) & (t <= 1.0)
+            xyz = np.argwhere(cand)[good]
+            for (x, y, z), tt in zip(xyz, t[good]):
+                cells.append((b, x, y, z, i))
+                qs.append(tt)
     mesh.link_cells = np.asarray(cells, np.int32).reshape(-1, 5)
     mesh.link_q = np.asarray(qs, np.float64)
     return mesh
@@ -157,8 +160,8 @@ def cylinder_forest(length=256, height=64, n=8, diameter=16.0, center=(64.0, 32.
     f.refine_uniform(base_level)
     rd = 2.0 * diameter if refine_dist is None else refine_dist
     for k in range(1, levels):
-        dist = rd * (levels - k) / (levels - 1) + 0.0
-        r = diameter / 2 + dist
+        # finest level within rd of the surface, each coarser level twice as far
+        r = diameter / 2 + rd * 2 ** (levels - 1 - k)
         f.refine_box((center[0] - r, center[1] - r, -1, center[0] + r, center[1] + r, height + 1), base_level + k)
     f.balance().build()
 

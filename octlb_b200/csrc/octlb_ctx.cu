@@ -121,6 +121,15 @@ struct octlb_ctx {
   std::vector<int> counters_collide, counters_stream;
   long long launches_per_step = 0, lups_per_step = 0;
   int step_kernel = 0;              // OCTLB_STEP_KERNEL: 0 pair (default), 1 bulk, 2 plain
+  // advance_one captured as CUDA graphs, keyed by the A/B parity of every
+  // level's buffers (the launch arguments depend on it)
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t out_mask = 0;
+    std::vector<int> dcollide;
+  };
+  std::map<uint64_t, GraphEntry> graphs;
+  bool use_graphs = true;           // OCTLB_NO_GRAPH=1 launches kernel by kernel
   float prolong_scale = 0.f, restrict_scale = 0.f;
 };
 
@@ -880,17 +889,64 @@ int check_device_error(octlb_ctx* ctx) {
   return OCTLB_OK;
 }
 
+// One advance_one: the TimeLoop recursion from level 0, then the force total.
+template <typename T>
+int advance_one_launches(octlb_ctx* ctx) {
+  int rc = do_advance_level<T>(ctx, 0);
+  if (rc) return rc;
+  if (ctx->drag) {
+    k_force_total<<<1, 32, 0, ctx->stream>>>(ctx->force_lvl.as<double>(), ctx->max_level + 1,
+                                             ctx->force.as<double>(), ctx->force_sum.as<double>());
+    CK(cudaGetLastError());
+  }
+  return OCTLB_OK;
+}
+
+uint64_t parity_mask(const octlb_ctx* ctx) {
+  uint64_t m = 0;
+  for (size_t l = 0; l < ctx->levels.size(); ++l)
+    if (ctx->levels[l].cur) m |= 1ull << l;
+  return m;
+}
+
 template <typename T>
 int advance_impl(octlb_ctx* ctx, int steps) {
   for (int s = 0; s < steps; ++s) {
-    int rc = do_advance_level<T>(ctx, 0);
-    if (rc) return rc;
-    if (ctx->drag) {
-      k_force_total<<<1, 32, 0, ctx->stream>>>(ctx->force_lvl.as<double>(), ctx->max_level + 1,
-                                               ctx->force.as<double>(), ctx->force_sum.as<double>());
-      CK(cudaGetLastError());
-      ++ctx->force_steps;
+    if (!ctx->use_graphs) {
+      int rc = advance_one_launches<T>(ctx);
+      if (rc) return rc;
+    } else {
+      const uint64_t mask = parity_mask(ctx);
+      auto it = ctx->graphs.find(mask);
+      if (it == ctx->graphs.end()) {
+        // Capture this parity's advance_one (the host bookkeeping runs once
+        // during capture), then launch it.
+        const std::vector<int> c0 = ctx->counters_collide;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = advance_one_launches<T>(ctx);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (ee != cudaSuccess) return cuda_fail(ctx, ee, "cudaStreamEndCapture");
+        octlb_ctx::GraphEntry e;
+        const cudaError_t ei = cudaGraphInstantiate(&e.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return cuda_fail(ctx, ei, "cudaGraphInstantiate");
+        e.out_mask = parity_mask(ctx);
+        e.dcollide.resize(ctx->counters_collide.size());
+        for (size_t l = 0; l < e.dcollide.size(); ++l) e.dcollide[l] = ctx->counters_collide[l] - c0[l];
+        it = ctx->graphs.emplace(mask, e).first;
+        CK(cudaGraphLaunch(it->second.exec, ctx->stream));
+      } else {
+        CK(cudaGraphLaunch(it->second.exec, ctx->stream));
+        for (size_t l = 0; l < ctx->levels.size(); ++l) ctx->levels[l].cur = (it->second.out_mask >> l) & 1;
+        for (size_t l = 0; l < it->second.dcollide.size(); ++l) {
+          ctx->counters_collide[l] += it->second.dcollide[l];
+          ctx->counters_stream[l] += it->second.dcollide[l];
+        }
+      }
     }
+    if (ctx->drag) ++ctx->force_steps;
   }
   return OCTLB_OK;
 }
@@ -1008,6 +1064,7 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
   ctx->periodic = t->periodic;
   ctx->drag = p->drag;
   ctx->omega = p->omega;
+  if (const char* ng = std::getenv("OCTLB_NO_GRAPH")) ctx->use_graphs = ng[0] != '1';
   if (const char* sk = std::getenv("OCTLB_STEP_KERNEL")) {
     const std::string v(sk);
     ctx->step_kernel = v == "bulk" ? 1 : (v == "plain" ? 2 : 0);
@@ -1024,6 +1081,9 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
 void octlb_gpu_destroy(octlb_ctx* ctx) {
   if (!ctx) return;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  ctx->graphs.clear();
   cudaStream_t s = ctx->own_stream ? ctx->stream : nullptr;
   ctx->levels.clear();
   if (s) cudaStreamDestroy(s);
