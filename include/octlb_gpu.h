@@ -144,6 +144,14 @@ int octlb_gpu_audit(octlb_ctx* ctx, double out[4]);
  * array: calls that overlap on the GPU race. */
 int octlb_gpu_audit_noalloc(octlb_ctx* ctx, double out[4]);
 
+/* Host-only dry run of octlb_gpu_create: validates and flattens the tables
+ * (every index the kernels derive is bounds-checked) without touching a
+ * device, and reports the plan: stats[0] = levels, then per level 10 values
+ * (blocks, halo pages, open blocks, boundary-fill writes, prolongation items,
+ * restriction items, saved cells, link records, drag cells, slots).  Returns
+ * the number of values, or a negative error code. */
+int octlb_gpu_plan(const octlb_tables* tables, const octlb_params* params, long long* stats, int max_stats);
+
 /* Per-level collide / stream counts and max level (TimeLoop::counters). */
 int octlb_gpu_counters(const octlb_ctx* ctx, int* collide, int* stream, int max_levels);
 int octlb_gpu_max_level(const octlb_ctx* ctx);

@@ -171,6 +171,22 @@ class Mesh:
         return t
 
 
+def plan(mesh, omega, precision=FP32, stream_mode=STREAM_ROTATE, drag=False):
+    """Host-only dry run of the context build (octlb_gpu_plan): per level a
+    dict of blocks, halo pages, open blocks, boundary-fill writes, coupler
+    items, saved cells, link records, drag cells and slots."""
+    L = capi.lib()
+    p = capi.Params()
+    p.omega, p.precision, p.stream_mode, p.drag = float(omega), int(precision), int(stream_mode), int(bool(drag))
+    buf = (ctypes.c_longlong * 4096)()
+    n = L.octlb_gpu_plan(ctypes.byref(mesh.c_tables()), ctypes.byref(p), buf, 4096)
+    if n < 0:
+        raise OctlbError(n, "plan failed")
+    keys = ["blocks", "pages", "open", "fills", "prolong", "restrict", "saved", "links", "drag", "slots"]
+    nl = buf[0]
+    return [dict(zip(keys, [buf[1 + 10 * l + k] for k in range(10)])) for l in range(nl)]
+
+
 class GpuLattice:
     """One octlb_gpu context (include/octlb_gpu.h)."""
 

@@ -88,6 +88,8 @@ def lib():
         "octlb_gpu_max_level": (ctypes.c_int, [P]),
         "octlb_gpu_step_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
         "octlb_gpu_debug_fastdiv": (ctypes.c_uint, [ctypes.c_uint, ctypes.c_uint]),
+        "octlb_gpu_plan": (ctypes.c_int, [ctypes.POINTER(Tables), ctypes.POINTER(Params),
+                                           ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
         "octlb_forest_new": (P, [ctypes.c_int] * 6 + [F64P]),
         "octlb_forest_free": (None, [P]),
         "octlb_forest_refine_uniform": (ctypes.c_int, [P, ctypes.c_int]),

@@ -30,26 +30,83 @@ __device__ __forceinline__ float LD(const T* base, long long qs, int i, long lon
   return Store<T>::ld(base + i * qs + slot, inv);
 }
 
-// Pull of direction i into core cell `slot` under the per-cell link rule
+// Core coordinates of core work item t (slot t).
+struct Cell {
+  uint32_t b, x, y, z;
+};
+__device__ __forceinline__ Cell cell_of(const StepArgs& a, uint32_t t) {
+  const uint32_t n = a.n;
+  Cell c;
+  c.b = a.div_n3.div(t);
+  uint32_t r = t - c.b * n * n * n;
+  c.x = a.div_n2.div(r);
+  r -= c.x * n * n;
+  c.y = a.div_n.div(r);
+  c.z = r - c.y * n;
+  return c;
+}
+
+// Slot holding padded position (X, Y, Z) in [0, n+1]^3 of block b: the own
+// core, the same-level neighbour's core cell the reference's exchange copies
+// into that halo position, or the block's own halo page.  in_halo reports a
+// position outside the core (the reference sees such sources as kBulk halo
+// cells, block_lattice.cpp:510-518).
+__device__ __forceinline__ long long resolve(const StepArgs& a, uint32_t b, int X, int Y, int Z,
+                                             bool& in_halo) {
+  const int n = a.n;
+  const int ox = X == 0 ? -1 : (X == n + 1 ? 1 : 0);
+  const int oy = Y == 0 ? -1 : (Y == n + 1 ? 1 : 0);
+  const int oz = Z == 0 ? -1 : (Z == n + 1 ? 1 : 0);
+  const long long lin = (static_cast<long long>(X - 1) * n + (Y - 1)) * n + (Z - 1);
+  in_halo = (ox | oy | oz) != 0;
+  if (!in_halo) return static_cast<long long>(b) * n * n * n + lin;
+  const long long base = a.nbase[b * 27 + (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1)];
+  if (base != kOwnPage) return base + lin;
+  const int pg = a.page_of[b];
+  const int h = a.hmap[(X * a.np + Y) * a.np + Z];
+  if (pg < 0 || h < 0) {  // excluded by construction; keep the access in bounds
+    atomicExch(a.err, kErrHalo);
+    return static_cast<long long>(b) * n * n * n;
+  }
+  return a.halo_base + static_cast<long long>(pg) * a.n_halo + h;
+}
+
+// Source slot of direction i for core cell c at slot `slot`; `interior` means
+// every D3Q19 source stays in the own core.
+__device__ __forceinline__ long long src_slot(const StepArgs& a, const Cell& c, long long slot, bool interior,
+                                              int i, bool& in_halo) {
+  if (interior) {
+    in_halo = false;
+    return slot - a.off[i];
+  }
+  return resolve(a, c.b, static_cast<int>(c.x) + 1 - cx(i), static_cast<int>(c.y) + 1 - cy(i),
+                 static_cast<int>(c.z) + 1 - cz(i), in_halo);
+}
+
+// Pull of direction i into core cell c under the per-cell link rule
 // (block_lattice.cpp:613-672).  `fl` is the cell's flag byte, `li` its link
 // record or -1.  Called inside unrolled loops, so i folds to a constant.
 template <typename T>
-__device__ __forceinline__ float pull_link(const StepArgs& a, const T* src, long long slot,
-                                           uint8_t fl, int li, int i) {
+__device__ __forceinline__ float pull_link(const StepArgs& a, const T* src, const Cell& c, long long slot,
+                                           bool interior, uint8_t fl, int li, int i) {
   const int kind = fl & kKindMask;
-  const long long s = slot - a.off[i];
-  const uint8_t sf = a.flags[s];
-  if (reflects_on_pull(kind) && (sf & kFlagHalo)) return LD(src, a.qs, opp(i), slot, a.inv_scale);
-  const int sk = (sf & kFlagHalo) ? kBulk : (sf & kKindMask);
+  bool halo;
+  const long long s = src_slot(a, c, slot, interior, i, halo);
+  if (reflects_on_pull(kind) && halo) return LD(src, a.qs, opp(i), slot, a.inv_scale);
+  const int sk = halo ? kBulk : (a.flags[s] & kKindMask);
   if (sk == kSolid || sk == kBouzidi) {
     float v;
     const float q = li >= 0 ? a.link_rec[li * 38 + i] : 1.0f;
     const float f_bb = LD(src, a.qs, opp(i), slot, a.inv_scale);
     if (q < 1.0f) {
       const float f_same = LD(src, a.qs, i, slot, a.inv_scale);
-      const long long nb = slot + a.off[i];
-      const uint8_t nf = a.flags[nb];
-      const int nk = (nf & kFlagHalo) ? kBulk : (nf & kKindMask);
+      bool nhalo;
+      const long long nb = interior ? slot + a.off[i]
+                                    : resolve(a, c.b, static_cast<int>(c.x) + 1 + cx(i),
+                                              static_cast<int>(c.y) + 1 + cy(i),
+                                              static_cast<int>(c.z) + 1 + cz(i), nhalo);
+      if (interior) nhalo = false;
+      const int nk = nhalo ? kBulk : (a.flags[nb] & kKindMask);
       const float f_q = nk == kBulk ? LD(src, a.qs, i, nb, a.inv_scale) : f_same;
       v = bouzidi(f_bb, f_q, f_same, q);
     } else {
@@ -61,63 +118,38 @@ __device__ __forceinline__ float pull_link(const StepArgs& a, const T* src, long
   return LD(src, a.qs, i, s, a.inv_scale);
 }
 
-template <typename T, bool PERIODIC, bool LINKS, bool FLAGS>
+__device__ __forceinline__ bool is_interior(const StepArgs& a, const Cell& c) {
+  const uint32_t m = a.n - 2;  // 1 <= x <= n-2  <=>  x - 1 < n - 2 (unsigned)
+  return (c.x - 1 < m) && (c.y - 1 < m) && (c.z - 1 < m);
+}
+
+template <typename T, bool LINKS, bool FLAGS>
 __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   if (t >= a.nitems) return;
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
-  const uint32_t n = a.n;
-  float f[kQ];
   if (t < a.ncore) {
-    const uint32_t b = a.div_n3.div(t);
-    uint32_t r = t - b * n * n * n;
-    const uint32_t x = a.div_n2.div(r);
-    r -= x * n * n;
-    const uint32_t y = a.div_n.div(r);
-    const uint32_t z = r - y * n;
-    long long slot;
-    uint8_t fl = 0;
-    if constexpr (PERIODIC) {
-      // One periodic block without halo: fill_periodic_halo + stream of the
-      // reference (block_lattice.cpp:918-964) is a wrapped pull.
-      slot = (static_cast<long long>(x) * n + y) * n + z;
-      if constexpr (FLAGS) fl = a.flags[slot];
-      const uint32_t xm = x == 0 ? n - 1 : x - 1, xp = x == n - 1 ? 0 : x + 1;
-      const uint32_t ym = y == 0 ? n - 1 : y - 1, yp = y == n - 1 ? 0 : y + 1;
-      const uint32_t zm = z == 0 ? n - 1 : z - 1, zp = z == n - 1 ? 0 : z + 1;
+    const Cell c = cell_of(a, t);
+    const long long slot = t;
+    const bool interior = is_interior(a, c);
+    const uint8_t fl = FLAGS ? a.flags[slot] : 0;
+    float f[kQ];
+    if constexpr (LINKS) {
+      if ((fl & kKindMask) == kSolid) {
+        // Solid cells are neither streamed nor collided (block_lattice.cpp:581-583).
+#pragma unroll
+        for (int i = 0; i < kQ; ++i) dst[i * a.qs + slot] = src[i * a.qs + slot];
+        return;
+      }
+      const int li = (fl & kFlagLink) ? a.link_idx[slot] : -1;
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) f[i] = pull_link<T>(a, src, c, slot, interior, fl, li, i);
+    } else {
 #pragma unroll
       for (int i = 0; i < kQ; ++i) {
-        const uint32_t sx = cx(i) == 1 ? xm : (cx(i) == -1 ? xp : x);
-        const uint32_t sy = cy(i) == 1 ? ym : (cy(i) == -1 ? yp : y);
-        const uint32_t sz = cz(i) == 1 ? zm : (cz(i) == -1 ? zp : z);
-        f[i] = Store<T>::ld(src + i * a.qs + (static_cast<long long>(sx) * n + sy) * n + sz, 1.0f);
-      }
-      // scaled units throughout (h = s (f - w))
-      if constexpr (FLAGS) {
-        if ((fl & kKindMask) == kBulk) bgk(f, a.omega, a.scale, a.inv_scale);
-      } else {
-        bgk(f, a.omega, a.scale, a.inv_scale);
-      }
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + slot, f[i], 1.0f);
-      return;
-    } else {
-      slot = b * a.bstride + ((x + 1) * a.np + (y + 1)) * a.np + (z + 1);
-      if constexpr (FLAGS) fl = a.flags[slot];
-      if constexpr (LINKS) {
-        if ((fl & kKindMask) == kSolid) {
-          // Solid cells are neither streamed nor collided (block_lattice.cpp:581-583).
-#pragma unroll
-          for (int i = 0; i < kQ; ++i) dst[i * a.qs + slot] = src[i * a.qs + slot];
-          return;
-        }
-        const int li = (fl & kFlagLink) ? a.link_idx[slot] : -1;
-#pragma unroll
-        for (int i = 0; i < kQ; ++i) f[i] = pull_link<T>(a, src, slot, fl, li, i);
-      } else {
-#pragma unroll
-        for (int i = 0; i < kQ; ++i) f[i] = LD(src, a.qs, i, slot - a.off[i], a.inv_scale);
+        bool halo;
+        f[i] = LD(src, a.qs, i, src_slot(a, c, slot, interior, i, halo), a.inv_scale);
       }
     }
     if constexpr (FLAGS) {
@@ -133,20 +165,23 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
 #pragma unroll
     for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + slot, f[i], a.scale);
   } else {
-    // Halo slot of an open block: torus pull over the padded block's linear
-    // index (block_lattice.h:70-89), no collision.
+    // Torus-streamed halo population of an open block (block_lattice.h:70-89):
+    // item (page, block, halo index, population); no collision; the source
+    // resolves like a core pull (own core, the neighbour core the exchange
+    // copies, or the own halo page).
     const uint32_t k = t - a.ncore;
-    const uint32_t ob = a.div_halo.div(k);
-    const uint32_t h = k - ob * a.n_halo;
-    const long long base = static_cast<long long>(a.open_blocks[ob]) * a.bstride;
-    const int loc = a.halo_map[h];
-    const int cells = static_cast<int>(a.bstride);
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) {
-      int s = loc - a.off[i];
-      s = s < 0 ? s + cells : (s >= cells ? s - cells : s);
-      dst[i * a.qs + base + loc] = src[i * a.qs + base + s];
-    }
+    const int4 it = reinterpret_cast<const int4*>(a.open_pages)[k];
+    const int i = it.w;
+    const int cells = a.np * a.np * a.np;
+    int s = a.hpos[it.z] - a.off_pad[i];
+    s = s < 0 ? s + cells : (s >= cells ? s - cells : s);
+    const int X = static_cast<int>(a.div_np2.div(static_cast<uint32_t>(s)));
+    const int rem = s - X * a.np * a.np;
+    const int Y = static_cast<int>(a.div_np.div(static_cast<uint32_t>(rem)));
+    const int Z = rem - Y * a.np;
+    bool halo;
+    const long long sslot = resolve(a, static_cast<uint32_t>(it.y), X, Y, Z, halo);
+    dst[i * a.qs + a.halo_base + static_cast<long long>(it.x) * a.n_halo + it.z] = src[i * a.qs + sslot];
   }
 }
 
@@ -371,6 +406,8 @@ k_drag(const StepArgs a, const DragItem* items, int nitems, double* partial) {
   if (t < nitems) {
     const DragItem it = items[t];
     const T* src = static_cast<const T*>(a.src);
+    const Cell c = cell_of(a, static_cast<uint32_t>(it.slot));
+    const bool interior = is_interior(a, c);
     const uint8_t fl = a.flags[it.slot];
     const int li = (LINKS && (fl & kFlagLink)) ? a.link_idx[it.slot] : -1;
 #pragma unroll
@@ -379,9 +416,9 @@ k_drag(const StepArgs a, const DragItem* items, int nitems, double* partial) {
       const float f_out = LD(src, a.qs, i, it.slot, a.inv_scale);
       float f_bar;
       if constexpr (LINKS) {
-        f_bar = pull_link<T>(a, src, it.slot, fl, li, opp(i));
+        f_bar = pull_link<T>(a, src, c, it.slot, interior, fl, li, opp(i));
       } else {
-        f_bar = LD(src, a.qs, opp(i), it.slot + a.off[i], a.inv_scale);
+        f_bar = LD(src, a.qs, opp(i), it.slot + a.off[i], a.inv_scale);  // x + c_i is in-block core
       }
       const double s = static_cast<double>(f_out) + static_cast<double>(f_bar);
       acc[0] += s * cx(i); acc[1] += s * cy(i); acc[2] += s * cz(i);
@@ -419,16 +456,7 @@ k_audit(const StepArgs a, double* partial) {
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   if (t < a.ncore) {
-    const uint32_t n = a.n;
-    const uint32_t b = a.div_n3.div(t);
-    uint32_t r = t - b * n * n * n;
-    const uint32_t x = a.div_n2.div(r);
-    r -= x * n * n;
-    const uint32_t y = a.div_n.div(r);
-    const uint32_t z = r - y * n;
-    const long long slot = a.np == static_cast<int>(n)
-                               ? (static_cast<long long>(x) * n + y) * n + z
-                               : b * a.bstride + ((x + 1) * a.np + (y + 1)) * a.np + (z + 1);
+    const long long slot = t;  // compact core slot
     const T* src = static_cast<const T*>(a.src);
     float f[kQ];
     bool finite = true;
@@ -460,16 +488,7 @@ __global__ void __launch_bounds__(kThreads)
 k_gather(const StepArgs a, double* out, double* out_u, int mode /*0 pops, 1 fields*/) {
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   if (t >= a.ncore) return;
-  const uint32_t n = a.n;
-  const uint32_t b = a.div_n3.div(t);
-  uint32_t r = t - b * n * n * n;
-  const uint32_t x = a.div_n2.div(r);
-  r -= x * n * n;
-  const uint32_t y = a.div_n.div(r);
-  const uint32_t z = r - y * n;
-  const long long slot = a.np == static_cast<int>(n)
-                             ? (static_cast<long long>(x) * n + y) * n + z
-                             : b * a.bstride + ((x + 1) * a.np + (y + 1)) * a.np + (z + 1);
+  const long long slot = t;  // compact core slot
   const T* src = static_cast<const T*>(a.src);
   if (mode == 0) {
 #pragma unroll
@@ -495,16 +514,7 @@ __global__ void __launch_bounds__(kThreads)
 k_scatter(const StepArgs a, const double* in) {
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   if (t >= a.ncore) return;
-  const uint32_t n = a.n;
-  const uint32_t b = a.div_n3.div(t);
-  uint32_t r = t - b * n * n * n;
-  const uint32_t x = a.div_n2.div(r);
-  r -= x * n * n;
-  const uint32_t y = a.div_n.div(r);
-  const uint32_t z = r - y * n;
-  const long long slot = a.np == static_cast<int>(n)
-                             ? (static_cast<long long>(x) * n + y) * n + z
-                             : b * a.bstride + ((x + 1) * a.np + (y + 1)) * a.np + (z + 1);
+  const long long slot = t;  // compact core slot
   float f[kQ];
 #pragma unroll
   for (int i = 0; i < kQ; ++i) f[i] = static_cast<float>(in[static_cast<long long>(t) * kQ + i]);
@@ -522,15 +532,15 @@ inline uint32_t grid_for(uint32_t items) { return (items + kThreads - 1) / kThre
 // ---------------------------------------------------------------- launchers
 template <typename T>
 cudaError_t launch_step(const StepArgs& a, bool periodic, bool links, bool flags, cudaStream_t s) {
+  (void)periodic;
   if (a.nitems == 0) return cudaSuccess;
   const dim3 g(grid_for(a.nitems));
-  if (periodic) {
-    if (flags) k_step<T, true, false, true><<<g, kThreads, 0, s>>>(a);
-    else k_step<T, true, false, false><<<g, kThreads, 0, s>>>(a);
-  } else if (links) {
-    k_step<T, false, true, true><<<g, kThreads, 0, s>>>(a);
+  if (links) {
+    k_step<T, true, true><<<g, kThreads, 0, s>>>(a);
+  } else if (flags) {
+    k_step<T, false, true><<<g, kThreads, 0, s>>>(a);
   } else {
-    k_step<T, false, false, true><<<g, kThreads, 0, s>>>(a);
+    k_step<T, false, false><<<g, kThreads, 0, s>>>(a);
   }
   return cudaGetLastError();
 }

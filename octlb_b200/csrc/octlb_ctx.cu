@@ -44,6 +44,10 @@ uint32_t audit_partials(const StepArgs& a);
 
 namespace {
 
+// Host-only planning (octlb_gpu_plan): every allocation, upload and launch is
+// skipped while the tables are flattened and checked.
+thread_local bool g_dry_run = false;
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
@@ -55,6 +59,7 @@ struct DevBuf {
   cudaError_t alloc(size_t b) {
     if (p) { cudaFree(p); p = nullptr; }
     bytes = b;
+    if (g_dry_run) return cudaSuccess;
     if (b == 0) return cudaSuccess;
     cudaError_t e = cudaMalloc(&p, b);
     if (e == cudaSuccess) e = cudaMemset(p, 0, b);
@@ -66,7 +71,7 @@ struct DevBuf {
 template <typename U>
 cudaError_t upload(DevBuf& d, const std::vector<U>& h) {
   cudaError_t e = d.alloc(h.size() * sizeof(U));
-  if (e != cudaSuccess || h.empty()) return e;
+  if (e != cudaSuccess || h.empty() || g_dry_run) return e;
   return cudaMemcpy(d.p, h.data(), h.size() * sizeof(U), cudaMemcpyHostToDevice);
 }
 
@@ -77,17 +82,17 @@ struct PlanPoint {  // CouplingPoint (level_coupler.h:18-30)
 struct Level {
   int lvl = 0;
   std::vector<int> blocks;          // global block ids, level-local order
-  int nblk = 0, n = 0, np = 0;
-  long long bstride = 0, nslots = 0;
+  int nblk = 0, n = 0;
+  long long ncore = 0, nslots = 0;  // core slots, core + halo-page slots
   DevBuf buf[2];
   int cur = 0;
-  DevBuf flags, link_idx, link_rec, save_idx, save_buf, open_blocks, halo_map;
-  int n_open = 0, n_halo = 0, n_save = 0, n_links = 0;
+  DevBuf flags, link_idx, link_rec, save_idx, save_buf;
+  DevBuf nbase, page_of, hmap, hpos, open_pages;
+  int n_open = 0, n_halo = 0, n_pages = 0, n_save = 0, n_links = 0;
   bool has_flags = false;
-  // ghost fill
-  DevBuf copy_desc, copy_start, bb_ops;
-  int n_copy_desc = 0;
-  uint32_t n_copy_cells = 0, n_bb = 0;
+  // tree-boundary halo fills
+  DevBuf bb_ops;
+  uint32_t n_bb = 0;
   // coupler: this level as coarse (prolong) and as fine (restrict)
   DevBuf prolong_items, prev, restrict_items;
   int n_prolong = 0, n_restrict = 0;
@@ -148,8 +153,9 @@ int cuda_fail(octlb_ctx* c, cudaError_t e, const char* where) {
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);       \
   } while (0)
 
-inline long long slot_of(const Level& L, int local_blk, int hx, int hy, int hz) {
-  return local_blk * L.bstride + (static_cast<long long>(hx) * L.np + hy) * L.np + hz;
+inline long long core_slot_of(int n, int local_blk, int x, int y, int z) {
+  const long long n3 = static_cast<long long>(n) * n * n;
+  return local_blk * n3 + (static_cast<long long>(x) * n + y) * n + z;
 }
 
 // Coupling plan of the reference (AppendFaceCouplingPoints,
@@ -209,9 +215,8 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
   if (L.nblk == 0) return OCTLB_OK;
   // Ghost fill into the buffer the step reads (reference: apply() then
   // exchange() after collide, time_loop.h:207-211).
-  CK(launch_ghost<T>(L.buf[L.cur].as<T>(), L.nslots, L.copy_desc.as<CopyDesc>(),
-                     L.copy_start.as<uint32_t>(), L.n_copy_desc, L.n_copy_cells,
-                     L.bb_ops.as<BBOp>(), L.n_bb, L.scale, L.inv_scale, ctx->stream));
+  CK(launch_ghost<T>(L.buf[L.cur].as<T>(), L.nslots, nullptr, nullptr, 0, 0, L.bb_ops.as<BBOp>(), L.n_bb,
+                     L.scale, L.inv_scale, ctx->stream));
   StepArgs a = L.args;
   a.src = L.buf[L.cur].p;
   a.dst = L.buf[1 - L.cur].p;
@@ -364,19 +369,13 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     Level& L = ctx->levels[l];
     L.nblk = static_cast<int>(L.blocks.size());
     L.n = n;
-    L.np = ctx->periodic ? n : n + 2;
-    L.bstride = static_cast<long long>(L.np) * L.np * L.np;
-    L.nslots = L.bstride * L.nblk;
+    L.ncore = L.nblk * n3;
     double sc = p->fp16_scale[l < 32 ? l : 31];
     if (!(sc > 0)) sc = 65536.0;
     L.scale = p->precision == OCTLB_FP16_SHIFTED ? static_cast<float>(sc) : 1.f;
     L.inv_scale = 1.f / L.scale;
     if (L.nblk == 0) continue;
-    if (L.nslots * static_cast<long long>(kQ) >= (1LL << 40))
-      return fail(ctx, OCTLB_EINVAL, "level too large");
-    if (static_cast<long long>(L.nblk) * n3 >= (1LL << 31))
-      return fail(ctx, OCTLB_EINVAL, "level has more than 2^31 cells");
-    for (int k = 0; k < 2; ++k) CK(L.buf[k].alloc(static_cast<size_t>(L.nslots) * kQ * sizeof(T)));
+    if (L.ncore >= (1LL << 31)) return fail(ctx, OCTLB_EINVAL, "level has more than 2^31 cells");
   }
 
   // Link records: q per direction (1 = half-way bounce-back) and the moving-wall
@@ -451,10 +450,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     m.emplace(slot, r);
     return r;
   };
-  auto core_slot = [&](int gblk, int x, int y, int z) {
-    const Level& L = ctx->levels[ctx->blk_level[gblk]];
-    return slot_of(L, ctx->blk_local[gblk], x + 1, y + 1, z + 1);
-  };
+  auto core_slot = [&](int gblk, int x, int y, int z) { return core_slot_of(n, ctx->blk_local[gblk], x, y, z); };
   auto gcell = [&](int gblk, int x, int y, int z) {
     return gblk * n3 + (static_cast<long long>(x) * n + y) * n + z;
   };
@@ -501,57 +497,67 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     }
   }
 
-  // ---- per-level flags, links, ghost ops, open blocks, drag items
+  // ---- per-level flags, links, neighbour bases, halo pages, boundary fills,
+  //      drag items
   std::vector<int> face_nbr(static_cast<size_t>(nb) * 6, -1);
   for (int k = 0; k < t->n_same_level; ++k) {
     const int* r = t->same_level + 3 * k;
     face_nbr[static_cast<size_t>(r[0]) * 6 + r[1]] = r[2];
   }
+  if (ctx->periodic)
+    for (int d = 0; d < 6; ++d) face_nbr[d] = 0;  // fill_periodic_halo: the block is its own neighbour
+  // Diagonal (edge) neighbour: two face steps in either order, the
+  // composition GhostSchedule uses for its same-level edge exchange.
+  auto edge_nbr = [&](int a, int d1, int d2) {
+    int b = face_nbr[static_cast<size_t>(a) * 6 + d1];
+    if (b >= 0 && face_nbr[static_cast<size_t>(b) * 6 + d2] >= 0) return face_nbr[static_cast<size_t>(b) * 6 + d2];
+    b = face_nbr[static_cast<size_t>(a) * 6 + d2];
+    if (b >= 0 && face_nbr[static_cast<size_t>(b) * 6 + d1] >= 0) return face_nbr[static_cast<size_t>(b) * 6 + d1];
+    return -1;
+  };
+  const int np = n + 2, np3 = np * np * np;
+  std::vector<int> hmap(static_cast<size_t>(np3), -1), hpos;
+  for (int X = 0; X < np; ++X)
+    for (int Y = 0; Y < np; ++Y)
+      for (int Z = 0; Z < np; ++Z) {
+        const bool core = X >= 1 && Y >= 1 && Z >= 1 && X <= n && Y <= n && Z <= n;
+        if (!core) {
+          hmap[(X * np + Y) * np + Z] = static_cast<int>(hpos.size());
+          hpos.push_back((X * np + Y) * np + Z);
+        }
+      }
+  const int H = static_cast<int>(hpos.size());
+  auto dir27 = [&](int X, int Y, int Z) {
+    const int ox = X == 0 ? -1 : (X == n + 1 ? 1 : 0), oy = Y == 0 ? -1 : (Y == n + 1 ? 1 : 0),
+              oz = Z == 0 ? -1 : (Z == n + 1 ? 1 : 0);
+    return (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1);
+  };
   for (int l = 0; l < nlev; ++l) {
     Level& L = ctx->levels[l];
     if (L.nblk == 0) continue;
-    const int np = L.np;
     L.has_flags = !ctx->periodic || !save_rows[l].empty();
     if (ctx->periodic) {
       for (long long k = 0; k < n3; ++k) if (t->kinds[k] != kBulk) L.has_flags = true;
     }
-    std::vector<uint8_t> flags(static_cast<size_t>(L.nslots), 0);
-    std::vector<int> lidx;
+    const long long ncore = L.ncore;
+    std::vector<uint8_t> flags(static_cast<size_t>(ncore), 0);
+    std::vector<int> lidx, sidx;
     std::vector<float> lrec;
-    std::vector<int> sidx;
-    if (!ctx->periodic)
-      for (int lb = 0; lb < L.nblk; ++lb)
-        for (int hx = 0; hx < np; ++hx)
-          for (int hy = 0; hy < np; ++hy)
-            for (int hz = 0; hz < np; ++hz) {
-              const bool core = hx >= 1 && hy >= 1 && hz >= 1 && hx <= n && hy <= n && hz <= n;
-              if (!core) flags[slot_of(L, lb, hx, hy, hz)] = kFlagHalo;
-            }
-    for (int lb = 0; lb < L.nblk; ++lb) {
-      const int gb = L.blocks[lb];
-      for (int x = 0; x < n; ++x)
-        for (int y = 0; y < n; ++y)
-          for (int z = 0; z < n; ++z) {
-            const long long s = ctx->periodic ? (static_cast<long long>(x) * n + y) * n + z
-                                              : slot_of(L, lb, x + 1, y + 1, z + 1);
-            flags[s] = t->kinds[gcell(gb, x, y, z)];
-          }
-    }
-    // link records of this level
+    for (int lb = 0; lb < L.nblk; ++lb)
+      std::memcpy(&flags[static_cast<size_t>(lb * n3)], t->kinds + static_cast<size_t>(L.blocks[lb]) * n3,
+                  static_cast<size_t>(n3));
     for (const auto& kv : recs) {
       const int gb = static_cast<int>(kv.first / n3);
       if (ctx->blk_level[gb] != l) continue;
-      const long long c = kv.first % n3;
-      const int x = static_cast<int>(c / (n * n)), y = static_cast<int>((c / n) % n), z = static_cast<int>(c % n);
-      const long long s = slot_of(L, ctx->blk_local[gb], x + 1, y + 1, z + 1);
-      if (lidx.empty()) lidx.assign(static_cast<size_t>(L.nslots), -1);
+      const long long s = static_cast<long long>(ctx->blk_local[gb]) * n3 + kv.first % n3;
+      if (lidx.empty()) lidx.assign(static_cast<size_t>(ncore), -1);
       lidx[s] = static_cast<int>(lrec.size() / 38);
       lrec.insert(lrec.end(), kv.second.begin(), kv.second.end());
       flags[s] |= kFlagLink;
     }
     L.n_links = static_cast<int>(lrec.size() / 38);
     if (!save_rows[l].empty()) {
-      sidx.assign(static_cast<size_t>(L.nslots), -1);
+      sidx.assign(static_cast<size_t>(ncore), -1);
       for (const auto& kv : save_rows[l]) {
         sidx[kv.first] = kv.second;
         flags[kv.first] |= kFlagSave;
@@ -559,19 +565,38 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       L.n_save = static_cast<int>(save_rows[l].size());
     }
 
-    // Ghost ops.  Tree-boundary fills first (apply(), in list order, later
-    // writes of the same halo population win), then same-level faces and
-    // edges (GhostSchedule::exchange, ghost_schedule.h:148-254).
-    std::map<std::pair<long long, int>, BBOp> bbmap;
-    std::vector<std::pair<long long, int>> bborder;
-    auto put_bb = [&](long long dst, int pop, long long src, int src_pop, float add) {
-      const auto key = std::make_pair(dst, pop);
-      if (!bbmap.count(key)) bborder.push_back(key);
-      bbmap[key] = BBOp{dst, src, pop, src_pop, add, 0};
+    // Same-level neighbour of each of the 27 halo directions (faces and edges
+    // only: the exchange fills no corner ghosts), global ids, -1 for none.
+    std::vector<int> nbr27(static_cast<size_t>(L.nblk) * 27, -1);
+    for (int lb = 0; lb < L.nblk; ++lb) {
+      const int gb = L.blocks[lb];
+      for (int ox = -1; ox <= 1; ++ox)
+        for (int oy = -1; oy <= 1; ++oy)
+          for (int oz = -1; oz <= 1; ++oz) {
+            const int o[3] = {ox, oy, oz};
+            int dirs[3], nd = 0;
+            for (int a = 0; a < 3; ++a)
+              if (o[a]) dirs[nd++] = 2 * a + (o[a] > 0 ? 1 : 0);
+            int v = -1;
+            if (nd == 0) v = gb;
+            else if (nd == 1) v = face_nbr[static_cast<size_t>(gb) * 6 + dirs[0]];
+            else if (nd == 2) v = edge_nbr(gb, dirs[0], dirs[1]);
+            nbr27[static_cast<size_t>(lb) * 27 + (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1)] = v;
+          }
+    }
+
+    // Tree-boundary fills (DomainBoundaryHandler::apply(), before the
+    // exchange), in list order; a later write of the same halo population
+    // wins.  Keyed by (block, padded position, population).
+    struct BB { int lb, hlin, pop; long long src; int src_pop; float add; };
+    std::map<std::tuple<int, int, int>, size_t> bbidx;
+    std::vector<BB> bbl;
+    auto put_bb = [&](int lb, int hlin, int pop, long long src, int src_pop, float add) {
+      const auto key = std::make_tuple(lb, hlin, pop);
+      auto it = bbidx.find(key);
+      if (it == bbidx.end()) { bbidx.emplace(key, bbl.size()); bbl.push_back({lb, hlin, pop, src, src_pop, add}); }
+      else bbl[it->second] = {lb, hlin, pop, src, src_pop, add};
     };
-    std::vector<CopyDesc> copies;
-    const long long sx_ = static_cast<long long>(np) * np, sy_ = np, sz_ = 1;
-    const long long astride[3] = {sx_, sy_, sz_};
     for (int k = 0; k < t->n_tree_boundary; ++k) {
       const int gb = t->tree_boundary[2 * k], dir = t->tree_boundary[2 * k + 1];
       if (ctx->blk_level[gb] != l || !t->tree_boundary_spec) continue;
@@ -588,7 +613,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
         for (int b2 = 0; b2 < n + 2; ++b2) {
           int h[3];
           h[ax] = hl; h[t0] = a; h[t1] = b2;
-          const long long hs = slot_of(L, lb, h[0], h[1], h[2]);
+          const int hlin = (h[0] * np + h[1]) * np + h[2];
           if (type == OCTLB_TB_WALL) {
             double shape = 1.0;
             const int pax = static_cast<int>(sp[4]);
@@ -603,115 +628,127 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
               const int xx = h[0] + ci[0], yy = h[1] + ci[1], zz = h[2] + ci[2];
               if (xx < 1 || yy < 1 || zz < 1 || xx > n || yy > n || zz > n) continue;
               const double cu = (ci[0] * sp[1] + ci[1] * sp[2] + ci[2] * sp[3]) * shape;
-              put_bb(hs, i, slot_of(L, lb, xx, yy, zz), opp(i), static_cast<float>(6.0 * wd(i) * cu));
+              put_bb(lb, hlin, i, core_slot_of(n, lb, xx - 1, yy - 1, zz - 1), opp(i),
+                     static_cast<float>(6.0 * wd(i) * cu));
             }
           } else {  // outflow: copy the adjacent interior cell, tangentially clamped
             int src[3];
             src[ax] = hl + nin;
             src[t0] = std::min(std::max(a, 1), n);
             src[t1] = std::min(std::max(b2, 1), n);
-            const long long ss = slot_of(L, lb, src[0], src[1], src[2]);
-            for (int i = 0; i < kQ; ++i) put_bb(hs, i, ss, i, 0.f);
+            const long long ss = core_slot_of(n, lb, src[0] - 1, src[1] - 1, src[2] - 1);
+            for (int i = 0; i < kQ; ++i) put_bb(lb, hlin, i, ss, i, 0.f);
           }
         }
     }
-    // Same-level faces.
-    std::set<std::pair<long long, long long>> seen_copy;
-    for (int k = 0; k < t->n_same_level; ++k) {
-      const int* r = t->same_level + 3 * k;
-      if (ctx->blk_level[r[0]] != l) continue;
-      const int dir = r[1], ax = dir / 2, t0 = std::min((ax + 1) % 3, (ax + 2) % 3),
-                t1 = std::max((ax + 1) % 3, (ax + 2) % 3);
-      const bool is_max = (dir & 1) != 0;
-      int hs[3] = {1, 1, 1}, hd[3] = {1, 1, 1};
-      hs[ax] = is_max ? n : 1;
-      hd[ax] = is_max ? 0 : n + 1;
-      CopyDesc d{};
-      d.src = slot_of(L, ctx->blk_local[r[0]], hs[0], hs[1], hs[2]);
-      d.dst = slot_of(L, ctx->blk_local[r[2]], hd[0], hd[1], hd[2]);
-      d.n0 = n; d.n1 = n;
-      d.s0 = d.d0 = static_cast<int>(astride[t0]);
-      d.s1 = d.d1 = static_cast<int>(astride[t1]);
-      copies.push_back(d);
-    }
-    // Same-level edges by composing face neighbours (ghost_schedule.h:56-95).
-    for (int a = 0; a < nb; ++a) {
-      if (ctx->blk_level[a] != l) continue;
-      for (int d1 = 0; d1 < 6; ++d1)
-        for (int d2 = 0; d2 < 6; ++d2) {
-          if (d1 / 2 == d2 / 2) continue;
-          const int bb = face_nbr[static_cast<size_t>(a) * 6 + d1];
-          if (bb < 0) continue;
-          const int dd = face_nbr[static_cast<size_t>(bb) * 6 + d2];
-          if (dd < 0) continue;
-          const int a1 = d1 / 2, a2 = d2 / 2, a3 = 3 - a1 - a2;
-          int hs[3], hd[3];
-          hs[a1] = (d1 & 1) ? n : 1; hs[a2] = (d2 & 1) ? n : 1; hs[a3] = 1;
-          hd[a1] = (d1 & 1) ? 0 : n + 1; hd[a2] = (d2 & 1) ? 0 : n + 1; hd[a3] = 1;
-          CopyDesc d{};
-          d.src = slot_of(L, ctx->blk_local[a], hs[0], hs[1], hs[2]);
-          d.dst = slot_of(L, ctx->blk_local[dd], hd[0], hd[1], hd[2]);
-          if (!seen_copy.insert({d.dst, d.src}).second) continue;
-          d.n0 = 1; d.n1 = n;
-          d.s0 = d.d0 = 0;
-          d.s1 = d.d1 = static_cast<int>(astride[a3]);
-          copies.push_back(d);
-        }
-    }
-    std::vector<uint32_t> cstart;
-    uint32_t ncells = 0;
-    for (const CopyDesc& d : copies) { cstart.push_back(ncells); ncells += static_cast<uint32_t>(d.n0 * d.n1); }
-    std::vector<BBOp> bbv;
-    for (const auto& key : bborder) bbv.push_back(bbmap[key]);
-    L.n_copy_desc = static_cast<int>(copies.size());
-    L.n_copy_cells = ncells;
-    L.n_bb = static_cast<uint32_t>(bbv.size());
 
-    // Open blocks: some halo population a core read depends on is not
-    // rewritten by the ghost fill, so the halo carries the reference's torus
-    // stream from step to step.
-    std::vector<int> open;
-    std::vector<int> halo_map;
+    // Open blocks: a halo population some core read depends on is neither a
+    // same-level neighbour cell nor rewritten by a boundary fill, so it carries
+    // the reference's torus stream from step to step.
+    std::vector<char> is_open(static_cast<size_t>(L.nblk), 0), needs_page(static_cast<size_t>(L.nblk), 0);
+    for (const BB& op : bbl) needs_page[op.lb] = 1;
     if (!ctx->periodic) {
-      std::set<std::pair<long long, int>> covered;
-      for (const CopyDesc& d : copies)
-        for (int a0 = 0; a0 < d.n0; ++a0)
-          for (int a1 = 0; a1 < d.n1; ++a1)
-            for (int i = 0; i < kQ; ++i) covered.insert({d.dst + static_cast<long long>(a0) * d.d0 + static_cast<long long>(a1) * d.d1, i});
-      for (const BBOp& op : bbv) covered.insert({op.dst, op.pop});
+      auto covered = [&](int lb, int X, int Y, int Z, int pop) {
+        const int d = dir27(X, Y, Z);
+        if (nbr27[static_cast<size_t>(lb) * 27 + d] >= 0) return true;
+        return bbidx.count(std::make_tuple(lb, (X * np + Y) * np + Z, pop)) > 0;
+      };
       for (int lb = 0; lb < L.nblk; ++lb) {
-        bool is_open = false;
-        for (int x = 1; x <= n && !is_open; ++x)
-          for (int y = 1; y <= n && !is_open; ++y)
-            for (int z = 1; z <= n && !is_open; ++z) {
+        bool open = false;
+        for (int x = 1; x <= n && !open; ++x)
+          for (int y = 1; y <= n && !open; ++y)
+            for (int z = 1; z <= n && !open; ++z) {
               if (x > 1 && y > 1 && z > 1 && x < n && y < n && z < n) continue;
-              const long long s = slot_of(L, lb, x, y, z);
+              const long long s = core_slot_of(n, lb, x - 1, y - 1, z - 1);
               const int kind = flags[s] & kKindMask;
-              for (int i = 1; i < kQ && !is_open; ++i) {
+              for (int i = 1; i < kQ && !open; ++i) {
                 const int hx = x - cx(i), hy = y - cy(i), hz = z - cz(i);
                 const bool halo = hx < 1 || hy < 1 || hz < 1 || hx > n || hy > n || hz > n;
                 if (halo) {
                   const bool reads = !links || !(kind == kSolid || reflects_on_pull(kind));
-                  if (reads && !covered.count({slot_of(L, lb, hx, hy, hz), i})) is_open = true;
+                  if (reads && !covered(lb, hx, hy, hz, i)) open = true;
                 }
                 if (links && (flags[s] & kFlagLink)) {
                   const int nx_ = x + cx(i), ny_ = y + cy(i), nz_ = z + cz(i);
                   const bool nhalo = nx_ < 1 || ny_ < 1 || nz_ < 1 || nx_ > n || ny_ > n || nz_ > n;
-                  if (nhalo && !covered.count({slot_of(L, lb, nx_, ny_, nz_), i})) is_open = true;
+                  if (nhalo && !covered(lb, nx_, ny_, nz_, i)) open = true;
                 }
               }
             }
-        if (is_open) open.push_back(lb);
+        is_open[lb] = open;
+        if (open) needs_page[lb] = 1;
       }
-      for (int hx = 0; hx < np; ++hx)
-        for (int hy = 0; hy < np; ++hy)
-          for (int hz = 0; hz < np; ++hz) {
-            const bool core = hx >= 1 && hy >= 1 && hz >= 1 && hx <= n && hy <= n && hz <= n;
-            if (!core) halo_map.push_back((hx * np + hy) * np + hz);
-          }
     }
-    L.n_open = static_cast<int>(open.size());
-    L.n_halo = static_cast<int>(halo_map.size());
+    std::vector<int> page_of(static_cast<size_t>(L.nblk), -1), open_pages;
+    for (int lb = 0; lb < L.nblk; ++lb)
+      if (needs_page[lb]) page_of[lb] = L.n_pages++;
+    // Torus-streamed halo populations of open blocks: the (slot, population)
+    // pairs a core read needs, closed under "slot h's population i is pulled
+    // from slot rot_i(h)" while the source is an uncovered own-halo slot
+    // (block_lattice.cpp:565-577).  Items: page, block, halo index, population.
+    std::vector<int> halo_items;
+    if (!ctx->periodic) {
+      auto covered = [&](int lb, int hlin, int pop) {
+        const int X = hlin / (np * np), Y = (hlin / np) % np, Z = hlin % np;
+        if (nbr27[static_cast<size_t>(lb) * 27 + dir27(X, Y, Z)] >= 0) return true;
+        return bbidx.count(std::make_tuple(lb, hlin, pop)) > 0;
+      };
+      for (int lb = 0; lb < L.nblk; ++lb) {
+        if (!is_open[lb]) continue;
+        std::set<std::pair<int, int>> need;
+        std::vector<std::pair<int, int>> work;
+        auto add = [&](int hlin, int pop) {
+          if (hmap[hlin] < 0 || covered(lb, hlin, pop)) return;
+          if (need.insert({hlin, pop}).second) work.push_back({hlin, pop});
+        };
+        for (int x = 1; x <= n; ++x)
+          for (int y = 1; y <= n; ++y)
+            for (int z = 1; z <= n; ++z) {
+              if (x > 1 && y > 1 && z > 1 && x < n && y < n && z < n) continue;
+              const long long sc = core_slot_of(n, lb, x - 1, y - 1, z - 1);
+              const int kind = flags[sc] & kKindMask;
+              for (int i = 1; i < kQ; ++i) {
+                const bool reads = !links || !(kind == kSolid || reflects_on_pull(kind));
+                if (reads) add(((x - cx(i)) * np + (y - cy(i))) * np + (z - cz(i)), i);
+                if (links && (flags[sc] & kFlagLink)) add(((x + cx(i)) * np + (y + cy(i))) * np + (z + cz(i)), i);
+              }
+            }
+        while (!work.empty()) {
+          const auto [hlin, pop] = work.back();
+          work.pop_back();
+          int src = hlin - (cx(pop) * np * np + cy(pop) * np + cz(pop));
+          src = ((src % np3) + np3) % np3;
+          add(src, pop);
+        }
+        for (const auto& hp : need) {
+          halo_items.push_back(page_of[lb]);
+          halo_items.push_back(lb);
+          halo_items.push_back(hmap[hp.first]);
+          halo_items.push_back(hp.second);
+        }
+      }
+    }
+    open_pages = halo_items;
+    L.n_open = static_cast<int>(halo_items.size() / 4);
+    L.n_halo = L.n_pages > 0 ? H : 0;
+    L.nslots = ncore + static_cast<long long>(L.n_pages) * H;
+    std::vector<BBOp> bbv;
+    for (const BB& op : bbl)
+      bbv.push_back(BBOp{ncore + static_cast<long long>(page_of[op.lb]) * H + hmap[op.hlin], op.src, op.pop,
+                         op.src_pop, op.add, 0});
+    L.n_bb = static_cast<uint32_t>(bbv.size());
+
+    // Slot bases of the 27 directions: own core (centre), the neighbour's core
+    // shifted by one block edge, or the own halo page.
+    std::vector<long long> nbase(static_cast<size_t>(L.nblk) * 27, kOwnPage);
+    for (int lb = 0; lb < L.nblk; ++lb)
+      for (int d = 0; d < 27; ++d) {
+        const int v = nbr27[static_cast<size_t>(lb) * 27 + d];
+        if (v < 0) continue;
+        const int ox = d / 9 - 1, oy = (d / 3) % 3 - 1, oz = d % 3 - 1;
+        const long long vl = ctx->blk_local[v];
+        nbase[static_cast<size_t>(lb) * 27 + d] = (vl - ox) * n3 - static_cast<long long>(oy) * n * n - oz * n;
+      }
 
     // Drag cells (drag_postprocessor.h:73-110).
     std::vector<DragItem> drag;
@@ -733,8 +770,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
               }
               if (!mask) continue;
               DragItem it{};
-              it.slot = ctx->periodic ? (static_cast<long long>(x) * n + y) * n + z
-                                      : slot_of(L, lb, x + 1, y + 1, z + 1);
+              it.slot = core_slot_of(n, lb, x, y, z);
               it.mask = mask;
               drag.push_back(it);
             }
@@ -747,43 +783,58 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     {
       const long long ns = L.nslots;
       auto in = [&](long long v, long long hi) { return v >= 0 && v < hi; };
-      for (const CopyDesc& d : copies) {
-        const long long ls = d.src + static_cast<long long>(d.n0 - 1) * d.s0 + static_cast<long long>(d.n1 - 1) * d.s1;
-        const long long ld = d.dst + static_cast<long long>(d.n0 - 1) * d.d0 + static_cast<long long>(d.n1 - 1) * d.d1;
-        if (!in(d.src, ns) || !in(d.dst, ns) || !in(ls, ns) || !in(ld, ns) || d.s0 < 0 || d.s1 < 0 ||
-            d.d0 < 0 || d.d1 < 0 || d.n0 < 1 || d.n1 < 1)
-          return fail(ctx, OCTLB_EINVAL, "internal: ghost copy out of range");
-      }
       for (const BBOp& op : bbv)
-        if (!in(op.dst, ns) || !in(op.src, ns) || !in(op.pop, kQ) || !in(op.src_pop, kQ))
-          return fail(ctx, OCTLB_EINVAL, "internal: ghost write out of range");
+        if (!in(op.dst, ns) || op.dst < ncore || !in(op.src, ncore) || !in(op.pop, kQ) || !in(op.src_pop, kQ))
+          return fail(ctx, OCTLB_EINVAL, "internal: boundary fill out of range");
       for (int v : lidx) if (v < -1 || v >= L.n_links) return fail(ctx, OCTLB_EINVAL, "internal: link index");
       for (int v : sidx) if (v < -1 || v >= L.n_save) return fail(ctx, OCTLB_EINVAL, "internal: save index");
-      for (int v : open) if (!in(v, L.nblk)) return fail(ctx, OCTLB_EINVAL, "internal: open block");
-      for (int v : halo_map) if (!in(v, L.bstride)) return fail(ctx, OCTLB_EINVAL, "internal: halo map");
-      for (const DragItem& it : drag) if (!in(it.slot, ns)) return fail(ctx, OCTLB_EINVAL, "internal: drag slot");
+      for (size_t k = 0; k < open_pages.size(); k += 4)
+        if (!in(open_pages[k], L.n_pages) || !in(open_pages[k + 1], L.nblk) || !in(open_pages[k + 2], H) ||
+            !in(open_pages[k + 3], kQ))
+          return fail(ctx, OCTLB_EINVAL, "internal: halo item");
+      for (int lb = 0; lb < L.nblk; ++lb)
+        for (int d = 0; d < 27; ++d) {
+          const long long b0 = nbase[static_cast<size_t>(lb) * 27 + d];
+          if (b0 == kOwnPage) continue;
+          // extreme core-linear offsets of the halo region of direction d
+          const int o[3] = {d / 9 - 1, (d / 3) % 3 - 1, d % 3 - 1};
+          long long lo = 0, hi = 0;
+          const long long w[3] = {static_cast<long long>(n) * n, n, 1};
+          for (int a = 0; a < 3; ++a) {
+            const long long cmin = o[a] < 0 ? -1 : (o[a] > 0 ? n : 0);
+            const long long cmax = o[a] < 0 ? -1 : (o[a] > 0 ? n : n - 1);
+            lo += cmin * w[a];
+            hi += cmax * w[a];
+          }
+          if (!in(b0 + lo, ncore) || !in(b0 + hi, ncore))
+            return fail(ctx, OCTLB_EINVAL, "internal: neighbour base out of range");
+        }
+      for (const DragItem& it : drag) if (!in(it.slot, ncore)) return fail(ctx, OCTLB_EINVAL, "internal: drag slot");
       for (const RestrictItem& it : restrict_items[l]) {
         if (!in(it.fine_save, L.n_save) || it.nnb < 0 || it.nnb > 18)
           return fail(ctx, OCTLB_EINVAL, "internal: restriction source");
         for (int k = 0; k < it.nnb; ++k)
           if (!in(it.nb_save[k], L.n_save)) return fail(ctx, OCTLB_EINVAL, "internal: restriction source");
       }
-      if (static_cast<long long>(L.n_open) * L.n_halo + static_cast<long long>(L.nblk) * n3 >= (1LL << 32))
+      if (static_cast<long long>(L.n_open) + ncore >= (1LL << 32))
         return fail(ctx, OCTLB_EINVAL, "level work exceeds 2^32 items");
+      if (L.nslots * static_cast<long long>(kQ) >= (1LL << 40)) return fail(ctx, OCTLB_EINVAL, "level too large");
       if (!L.has_flags && (L.n_save > 0 || !ctx->periodic))
         return fail(ctx, OCTLB_EINVAL, "internal: flags required");
     }
 
-    // uploads
+    // allocations and uploads
+    for (int k = 0; k < 2; ++k) CK(L.buf[k].alloc(static_cast<size_t>(L.nslots) * kQ * sizeof(T)));
     if (L.has_flags) CK(upload(L.flags, flags));
     CK(upload(L.link_idx, lidx));
     CK(upload(L.link_rec, lrec));
     CK(upload(L.save_idx, sidx));
     CK(L.save_buf.alloc(static_cast<size_t>(L.n_save) * kQ * sizeof(float)));
-    CK(upload(L.open_blocks, open));
-    CK(upload(L.halo_map, halo_map));
-    CK(upload(L.copy_desc, copies));
-    CK(upload(L.copy_start, cstart));
+    CK(upload(L.nbase, nbase));
+    CK(upload(L.page_of, page_of));
+    CK(upload(L.hmap, hmap));
+    CK(upload(L.hpos, hpos));
+    CK(upload(L.open_pages, open_pages));
     CK(upload(L.bb_ops, bbv));
     CK(upload(L.prolong_items, prolong[l]));
     CK(upload(L.restrict_items, restrict_items[l]));
@@ -800,30 +851,37 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     A.link_rec = L.link_rec.as<float>();
     A.save_idx = L.save_idx.as<int>();
     A.save_buf = L.save_buf.as<float>();
-    A.open_blocks = L.open_blocks.as<int>();
-    A.halo_map = L.halo_map.as<int>();
+    A.nbase = L.nbase.as<long long>();
+    A.page_of = L.page_of.as<int>();
+    A.hmap = L.hmap.as<int>();
+    A.hpos = L.hpos.as<int>();
+    A.open_pages = L.open_pages.as<int>();
     A.n_open = L.n_open;
     A.n_halo = L.n_halo;
     A.nblk = L.nblk; A.n = n; A.np = np;
-    A.bstride = L.bstride;
-    A.plane = static_cast<long long>(np) * np;
-    A.ncore = static_cast<uint32_t>(L.nblk * n3);
-    A.nitems = A.ncore + static_cast<uint32_t>(L.n_open) * static_cast<uint32_t>(L.n_halo);
+    A.halo_base = ncore;
+    A.ncore = static_cast<uint32_t>(ncore);
+    A.nitems = A.ncore + static_cast<uint32_t>(L.n_open);
     A.div_n = FastDiv(n);
     A.div_n2 = FastDiv(n * n);
     A.div_n3 = FastDiv(static_cast<uint32_t>(n3));
     A.div_halo = FastDiv(L.n_halo > 0 ? L.n_halo : 1);
+    A.div_np = FastDiv(np);
+    A.div_np2 = FastDiv(np * np);
     A.omega = static_cast<float>(p->omega);
     A.scale = L.scale;
     A.inv_scale = L.inv_scale;
-    for (int i = 0; i < kQ; ++i) A.off[i] = static_cast<int>(cx(i) * A.plane + cy(i) * np + cz(i));
+    for (int i = 0; i < kQ; ++i) {
+      A.off[i] = cx(i) * n * n + cy(i) * n + cz(i);
+      A.off_pad[i] = cx(i) * np * np + cy(i) * np + cz(i);
+    }
     A.err = ctx->dev_err.as<int>();
     // One all-kBulk periodic block: paired vector step by default, the
     // pipelined bulk-copy step on request (OCTLB_STEP_KERNEL=bulk), the plain
     // one-cell-per-thread step with OCTLB_STEP_KERNEL=plain.
     const bool uniform = ctx->periodic && !L.has_flags;
     if (uniform && ctx->step_kernel == 0 && pair_step_eligible(n)) L.use_pair = true;
-    if (uniform && ctx->step_kernel == 1 && bulk_step_eligible(n, sizeof(T))) {
+    if (uniform && ctx->step_kernel == 1 && bulk_step_eligible(n, sizeof(T)) && !g_dry_run) {
       const int per_sm = bulk_prepare<T>(n);
       int dev = 0, sms = 0;
       CK(cudaGetDevice(&dev));
@@ -859,7 +917,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
   CK(ctx->audit_out.alloc(5 * sizeof(double)));
 
   // ---- initial state: g = C(f0) on kBulk cells
-  for (int l = 0; l < nlev; ++l) {
+  for (int l = 0; l < nlev && !g_dry_run; ++l) {
     Level& L = ctx->levels[l];
     if (L.nblk == 0) continue;
     std::vector<double> dense(static_cast<size_t>(L.nblk * n3 * kQ));
@@ -1179,6 +1237,34 @@ int octlb_gpu_counters(const octlb_ctx* ctx, int* collide, int* stream, int max_
 
 int octlb_gpu_max_level(const octlb_ctx* ctx) { return ctx ? ctx->max_level : OCTLB_EINVAL; }
 
+int octlb_gpu_plan(const octlb_tables* t, const octlb_params* p, long long* stats, int max_stats) {
+  octlb_ctx ctx;
+  int rc = validate(&ctx, t, p);
+  if (rc) return rc;
+  ctx.n = t->n;
+  ctx.n_blocks = t->n_blocks;
+  ctx.precision = p->precision;
+  ctx.stream_mode = p->stream_mode;
+  ctx.periodic = t->periodic;
+  ctx.drag = p->drag;
+  ctx.omega = p->omega;
+  g_dry_run = true;
+  rc = p->precision == OCTLB_FP32 ? create_impl<float>(&ctx, t, p, nullptr)
+                                  : create_impl<__half>(&ctx, t, p, nullptr);
+  g_dry_run = false;
+  if (rc) return rc;
+  const int nl = static_cast<int>(ctx.levels.size());
+  std::vector<long long> v;
+  v.push_back(nl);
+  for (const Level& L : ctx.levels) {
+    const long long row[10] = {L.nblk, L.n_pages, L.n_open, L.n_bb, L.n_prolong, L.n_restrict,
+                               L.n_save, L.n_links, L.n_drag, L.nslots};
+    v.insert(v.end(), row, row + 10);
+  }
+  for (int k = 0; k < max_stats && k < static_cast<int>(v.size()); ++k) stats[k] = v[k];
+  return static_cast<int>(v.size());
+}
+
 // Host-only check of the multiply-high divider the kernels use for index
 // decomposition (no device work).
 unsigned octlb_gpu_debug_fastdiv(unsigned d, unsigned n) { return FastDiv(d).div(n); }
@@ -1192,7 +1278,7 @@ int octlb_gpu_step_stats(const octlb_ctx* ctx, long long* launches, long long* l
   for (size_t l = 0; l < ctx->levels.size(); ++l) {
     const Level& L = ctx->levels[l];
     if (L.nblk == 0) continue;
-    per[l] = (L.n_copy_cells + L.n_bb > 0 ? 1 : 0) + (L.args.nitems > 0 ? 1 : 0) +
+    per[l] = (L.n_bb > 0 ? 1 : 0) + (L.args.nitems > 0 ? 1 : 0) +
              (ctx->drag && L.n_drag > 0 ? 2 : 0);
   }
   for (size_t l = 0; l < ctx->levels.size(); ++l) {
@@ -1234,19 +1320,10 @@ static double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 template <typename T>
 __global__ void __launch_bounds__(256) k_audit_noalloc(const StepArgs a, double* rows) {
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  const uint32_t n = a.n;
   for (int k = 0; k < 8; ++k) {
     const uint32_t t = blockIdx.x * kNoAllocCellsPerCta + k * 256 + threadIdx.x;
     if (t >= a.ncore) break;
-    const uint32_t b = a.div_n3.div(t);
-    uint32_t r = t - b * n * n * n;
-    const uint32_t x = a.div_n2.div(r);
-    r -= x * n * n;
-    const uint32_t y = a.div_n.div(r);
-    const uint32_t z = r - y * n;
-    const long long slot = a.np == static_cast<int>(n)
-                               ? (static_cast<long long>(x) * n + y) * n + z
-                               : b * a.bstride + ((x + 1) * a.np + (y + 1)) * a.np + (z + 1);
+    const long long slot = t;  // compact core slot
     const T* src = static_cast<const T*>(a.src);
     double drho = 0, jx = 0, jy = 0, jz = 0;
     bool finite = true;

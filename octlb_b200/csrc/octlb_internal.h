@@ -9,35 +9,47 @@
 
 namespace octlb_gpu {
 
-// One octree level on the device.  Every block is a padded (n+2)^3 box with a
-// one-cell halo (the reference's BlockLattice layout, block_lattice.h:294-304),
-// stored structure-of-arrays: population i of slot s lives at
-// pops[i * qs + s], slot s = b * bstride + (hx * np + hy) * np + hz.  A single
-// periodic block drops the halo (np = n) and wraps its pull indices instead.
+// One octree level on the device.  Every block's n^3 core cells are stored
+// compactly, structure of arrays: population i of slot s at pops[i * qs + s],
+// core slot s = block * n^3 + (x * n + y) * n + z.  The reference's one-cell
+// halo (block_lattice.h:294-304) is not stored per block: a pull whose source
+// lies in the halo is resolved through the block's 27-entry base table to the
+// same-level neighbour's core cell that GhostSchedule would have copied there
+// (faces, and edges composed from two faces, ghost_schedule.h:56-95).  Blocks
+// whose halo is written by a tree-boundary fill, or whose halo carries the
+// reference's torus stream because no exchange fills it, own a halo page of
+// (n+2)^3 - n^3 slots after all cores (slot halo_base + page * n_halo + hmap).
+// A single periodic block resolves every halo direction to itself.
 struct StepArgs {
   const void* src;
   void* dst;
-  long long qs;             // elements between population planes
-  const uint8_t* flags;     // [slots] kind + role bits
-  const int* link_idx;      // [slots] link record index (read if kFlagLink)
+  long long qs;             // slots per population plane (cores + halo pages)
+  const uint8_t* flags;     // [ncore] kind + role bits
+  const int* link_idx;      // [ncore] link record index (read if kFlagLink)
   const float* link_rec;    // [n_links][38]: q[19], dw[19]
-  const int* save_idx;      // [slots] save slot (read if kFlagSave)
+  const int* save_idx;      // [ncore] save row (read if kFlagSave)
   float* save_buf;          // [n_save][19] pre-collision populations
-  const int* open_blocks;   // blocks whose halo is torus-streamed
-  const int* halo_map;      // [n_halo] halo slot offsets inside one block
-  int n_open, n_halo;
-  int nblk, n, np;
-  long long bstride, plane; // slots per block, per x-slice
+  const long long* nbase;   // [nblk][27] slot base of the halo direction (or kOwnPage)
+  const int* page_of;       // [nblk] halo page or -1
+  const int* hmap;          // [(n+2)^3] padded position -> halo index (-1 in the core)
+  const int* hpos;          // [n_halo] halo index -> padded linear position
+  const int* open_pages;    // [n_open][4] torus-streamed halo items: page, block, halo index, population
+  int n_open, n_halo;       // items, halo slots per page
+  int nblk, n, np;          // np = n + 2
+  long long halo_base;      // first halo-page slot (= nblk * n^3)
   uint32_t ncore;           // nblk * n^3 core work items
-  uint32_t nitems;          // ncore + n_open * n_halo
-  FastDiv div_n, div_n2, div_n3, div_halo;
+  uint32_t nitems;          // ncore + n_open
+  FastDiv div_n, div_n2, div_n3, div_halo, div_np, div_np2;
   float omega, scale, inv_scale;
-  int off[kQ];              // slot offset of c_i: cx*plane + cy*np + cz
+  int off[kQ];              // core slot offset of c_i: cx*n*n + cy*n + cz
+  int off_pad[kQ];          // padded linear offset of c_i: cx*np*np + cy*np + cz
   int* err;                 // device error word (bounded waits that gave up)
 };
 
+constexpr long long kOwnPage = -(1LL << 62);
+
 // Device error codes written to StepArgs::err.
-enum : int { kErrNone = 0, kErrBulkTimeout = 1 };
+enum : int { kErrNone = 0, kErrBulkTimeout = 1, kErrHalo = 2 };
 
 // Rectangular halo copy (same-level face / edge exchange, outflow ghost copy):
 // dst(a,b) <- src(a,b) for all 19 populations.

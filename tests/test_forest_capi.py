@@ -189,3 +189,29 @@ int main() {
                     "-L", lib_dir, "-loctlb_b200", f"-Wl,-rpath,{lib_dir}"], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0 and "even" in r.stdout
+
+
+@pytest.mark.parametrize("name", ["tgv", "shell", "c1", "c2", "cyl", "c3"])
+def test_plan_dry_run_all_configurations(ob, name):
+    """octlb_gpu_plan flattens every benchmark configuration on the host with
+    all kernel-derived indices bounds-checked, no device needed."""
+    from octlb_b200 import cases
+    cfg = {
+        "tgv": (lambda: cases.tgv_periodic(32), ob.STREAM_ROTATE, False),
+        "shell": (lambda: cases.cavity_shell(16), ob.STREAM_LINKS, False),
+        "c1": (lambda: cases.cavity_forest(cells=32, n=8), ob.STREAM_ROTATE, False),
+        "c2": (lambda: cases.cavity_forest(cells=64, n=8, lid=0.05, tau=0.56, band_cells=8), ob.STREAM_ROTATE, False),
+        "cyl": (lambda: cases.cylinder_forest(length=128, height=32, n=8, diameter=8.0, center=(32.0, 16.0),
+                                              levels=2, u_max=0.05, re=40.0), ob.STREAM_LINKS, True),
+        "c3": (lambda: cases.cylinder_forest(), ob.STREAM_LINKS, True),
+    }[name]
+    mesh, init, info = cfg[0]()
+    pl = ob.plan(mesh, info["omega"], stream_mode=cfg[1], drag=cfg[2])
+    assert sum(d["blocks"] for d in pl) == mesh.n_blocks
+    for l, d in enumerate(pl):
+        if d["blocks"]:
+            assert d["slots"] >= d["blocks"] * mesh.n ** 3
+    if name in ("c2", "c3", "cyl"):
+        assert sum(d["prolong"] for d in pl) > 0 and sum(d["restrict"] for d in pl) > 0
+    if name in ("c3", "cyl"):
+        assert sum(d["drag"] for d in pl) > 0 and sum(d["links"] for d in pl) > 0
