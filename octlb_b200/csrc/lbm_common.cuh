@@ -41,7 +41,9 @@ enum : uint8_t {
 // Per-slot flag byte on the device: bits 0-2 kind, then role bits.
 enum : uint8_t {
   kKindMask = 0x07,
-  kFlagHalo = 0x08,     // padded halo slot (kind reads as kBulk)
+  kFlagNear = 0x08,     // core cell whose pull needs the link rule (a solid /
+                        // Bouzidi source in the own core, a reflecting kind
+                        // with a halo source, or a link record)
   kFlagLink = 0x10,     // core cell with a link record (q / moving-wall term)
   kFlagSave = 0x20,     // save pre-collision populations (coupler source)
 };

@@ -46,6 +46,19 @@ __device__ __forceinline__ Cell cell_of(const StepArgs& a, uint32_t t) {
   return c;
 }
 
+// Own halo-page slot of padded position (X, Y, Z) of block b; positions that
+// no table covers are excluded by construction, the check keeps the access in
+// bounds and records an error if that ever fails.
+__device__ __noinline__ long long page_slot(const StepArgs& a, uint32_t b, int X, int Y, int Z) {
+  const int pg = a.page_of[b];
+  const int h = a.hmap[(X * a.np + Y) * a.np + Z];
+  if (pg < 0 || h < 0) {
+    atomicExch(a.err, kErrHalo);
+    return static_cast<long long>(b) * a.n * a.n * a.n;
+  }
+  return a.halo_base + static_cast<long long>(pg) * a.n_halo + h;
+}
+
 // Slot holding padded position (X, Y, Z) in [0, n+1]^3 of block b: the own
 // core, the same-level neighbour's core cell the reference's exchange copies
 // into that halo position, or the block's own halo page.  in_halo reports a
@@ -62,99 +75,124 @@ __device__ __forceinline__ long long resolve(const StepArgs& a, uint32_t b, int 
   if (!in_halo) return static_cast<long long>(b) * n * n * n + lin;
   const long long base = a.nbase[b * 27 + (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1)];
   if (base != kOwnPage) return base + lin;
-  const int pg = a.page_of[b];
-  const int h = a.hmap[(X * a.np + Y) * a.np + Z];
-  if (pg < 0 || h < 0) {  // excluded by construction; keep the access in bounds
-    atomicExch(a.err, kErrHalo);
-    return static_cast<long long>(b) * n * n * n;
-  }
-  return a.halo_base + static_cast<long long>(pg) * a.n_halo + h;
+  return page_slot(a, b, X, Y, Z);
 }
 
-// Source slot of direction i for core cell c at slot `slot`; `interior` means
-// every D3Q19 source stays in the own core.
-__device__ __forceinline__ long long src_slot(const StepArgs& a, const Cell& c, long long slot, bool interior,
-                                              int i, bool& in_halo) {
-  if (interior) {
-    in_halo = false;
-    return slot - a.off[i];
+// Source slots of the 19 pulls of core cell c (local index tl inside its
+// block, global slot t): direction i reads padded position x + 1 - c_i.  The
+// halo direction of each source follows from which block faces the cell
+// touches, so a boundary cell costs one table read per direction (from the
+// CTA's shared copy of the block's 27 bases when `sb` is given).
+__device__ __forceinline__ void source_slots(const StepArgs& a, const Cell& c, long long t, long long tl,
+                                             const long long* sb, long long (&s)[kQ], uint32_t& halo_mask) {
+  const uint32_t n1 = a.n - 1;
+  const bool xl = c.x == 0, xh = c.x == n1, yl = c.y == 0, yh = c.y == n1, zl = c.z == 0, zh = c.z == n1;
+  halo_mask = 0;
+  if (!(xl | xh | yl | yh | zl | zh)) {
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) s[i] = t - a.off[i];
+    return;
   }
-  return resolve(a, c.b, static_cast<int>(c.x) + 1 - cx(i), static_cast<int>(c.y) + 1 - cy(i),
-                 static_cast<int>(c.z) + 1 - cz(i), in_halo);
-}
-
-// Pull of direction i into core cell c under the per-cell link rule
-// (block_lattice.cpp:613-672).  `fl` is the cell's flag byte, `li` its link
-// record or -1.  Called inside unrolled loops, so i folds to a constant.
-template <typename T>
-__device__ __forceinline__ float pull_link(const StepArgs& a, const T* src, const Cell& c, long long slot,
-                                           bool interior, uint8_t fl, int li, int i) {
-  const int kind = fl & kKindMask;
-  bool halo;
-  const long long s = src_slot(a, c, slot, interior, i, halo);
-  if (reflects_on_pull(kind) && halo) return LD(src, a.qs, opp(i), slot, a.inv_scale);
-  const int sk = halo ? kBulk : (a.flags[s] & kKindMask);
-  if (sk == kSolid || sk == kBouzidi) {
-    float v;
-    const float q = li >= 0 ? a.link_rec[li * 38 + i] : 1.0f;
-    const float f_bb = LD(src, a.qs, opp(i), slot, a.inv_scale);
-    if (q < 1.0f) {
-      const float f_same = LD(src, a.qs, i, slot, a.inv_scale);
-      bool nhalo;
-      const long long nb = interior ? slot + a.off[i]
-                                    : resolve(a, c.b, static_cast<int>(c.x) + 1 + cx(i),
-                                              static_cast<int>(c.y) + 1 + cy(i),
-                                              static_cast<int>(c.z) + 1 + cz(i), nhalo);
-      if (interior) nhalo = false;
-      const int nk = nhalo ? kBulk : (a.flags[nb] & kKindMask);
-      const float f_q = nk == kBulk ? LD(src, a.qs, i, nb, a.inv_scale) : f_same;
-      v = bouzidi(f_bb, f_q, f_same, q);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const int ox = (cx(i) == 1 && xl) ? -1 : ((cx(i) == -1 && xh) ? 1 : 0);
+    const int oy = (cy(i) == 1 && yl) ? -1 : ((cy(i) == -1 && yh) ? 1 : 0);
+    const int oz = (cz(i) == 1 && zl) ? -1 : ((cz(i) == -1 && zh) ? 1 : 0);
+    if ((ox | oy | oz) == 0) {
+      s[i] = t - a.off[i];
     } else {
-      v = f_bb;
+      halo_mask |= 1u << i;
+      const int d = (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1);
+      const long long base = sb ? sb[d] : a.nbase[c.b * 27 + d];
+      s[i] = base != kOwnPage
+                 ? base + tl - a.off[i]
+                 : page_slot(a, c.b, static_cast<int>(c.x) + 1 - cx(i), static_cast<int>(c.y) + 1 - cy(i),
+                             static_cast<int>(c.z) + 1 - cz(i));
     }
-    if (li >= 0) v += a.link_rec[li * 38 + kQ + i];
-    return v;
   }
-  return LD(src, a.qs, i, s, a.inv_scale);
 }
 
-__device__ __forceinline__ bool is_interior(const StepArgs& a, const Cell& c) {
-  const uint32_t m = a.n - 2;  // 1 <= x <= n-2  <=>  x - 1 < n - 2 (unsigned)
-  return (c.x - 1 < m) && (c.y - 1 < m) && (c.z - 1 < m);
+// Per-cell link rule (block_lattice.cpp:613-672) for a cell flagged kFlagNear:
+// pulled[i] holds g_i at the source slot s[i] (already loaded).
+template <typename T>
+__device__ __forceinline__ void apply_links(const StepArgs& a, const T* src, const Cell& c, long long t,
+                                            const long long (&s)[kQ], uint32_t halo_mask, uint8_t fl,
+                                            float (&f)[kQ]) {
+  const int kind = fl & kKindMask;
+  const int li = (fl & kFlagLink) ? a.link_idx[t] : -1;
+  float own[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) own[i] = LD(src, a.qs, i, t, a.inv_scale);
+  uint8_t sk[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) sk[i] = (halo_mask >> i) & 1u ? kBulk : (a.flags[s[i]] & kKindMask);
+#pragma unroll
+  for (int i = 1; i < kQ; ++i) {
+    const bool halo = (halo_mask >> i) & 1u;
+    if (reflects_on_pull(kind) && halo) {
+      f[i] = own[opp(i)];
+      continue;
+    }
+    if (sk[i] == kSolid || sk[i] == kBouzidi) {
+      float v = own[opp(i)];
+      if (li >= 0) {
+        const float q = a.link_rec[li * 38 + i];
+        if (q < 1.0f) {
+          // neighbour x + c_i: in-core cell or a halo position (kind kBulk)
+          bool nhalo;
+          const long long nb = resolve(a, c.b, static_cast<int>(c.x) + 1 + cx(i), static_cast<int>(c.y) + 1 + cy(i),
+                                       static_cast<int>(c.z) + 1 + cz(i), nhalo);
+          const int nk = nhalo ? kBulk : (a.flags[nb] & kKindMask);
+          const float f_q = nk == kBulk ? LD(src, a.qs, i, nb, a.inv_scale) : own[i];
+          v = bouzidi(own[opp(i)], f_q, own[i], q);
+        }
+        v += a.link_rec[li * 38 + kQ + i];
+      }
+      f[i] = v;
+    }
+  }
 }
 
-template <typename T, bool LINKS, bool FLAGS>
+template <typename T, bool LINKS, bool FLAGS, bool BLOCKED>
 __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
-  if (t >= a.nitems) return;
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
-  if (t < a.ncore) {
+  const uint32_t cta0 = blockIdx.x * kThreads;
+  if (cta0 < a.ncore) {
+    // CTAs of core cells (ncore is a multiple of the CTA size when BLOCKED,
+    // and then a CTA never straddles two blocks).
+    __shared__ long long sb[27];
+    const uint32_t n3 = a.n * a.n * a.n;
+    if constexpr (BLOCKED) {
+      const uint32_t b0 = a.div_n3.div(cta0);
+      if (threadIdx.x < 27) sb[threadIdx.x] = a.nbase[b0 * 27 + threadIdx.x];
+      __syncthreads();
+    }
+    if (t >= a.ncore) return;
     const Cell c = cell_of(a, t);
-    const long long slot = t;
-    const bool interior = is_interior(a, c);
-    const uint8_t fl = FLAGS ? a.flags[slot] : 0;
+    const long long tl = t - c.b * n3;
+    const uint8_t fl = FLAGS ? a.flags[t] : 0;
     float f[kQ];
     if constexpr (LINKS) {
       if ((fl & kKindMask) == kSolid) {
         // Solid cells are neither streamed nor collided (block_lattice.cpp:581-583).
 #pragma unroll
-        for (int i = 0; i < kQ; ++i) dst[i * a.qs + slot] = src[i * a.qs + slot];
+        for (int i = 0; i < kQ; ++i) dst[i * a.qs + t] = src[i * a.qs + t];
         return;
       }
-      const int li = (fl & kFlagLink) ? a.link_idx[slot] : -1;
+    }
+    long long s[kQ];
+    uint32_t halo_mask;
+    source_slots(a, c, t, tl, BLOCKED ? sb : nullptr, s, halo_mask);
 #pragma unroll
-      for (int i = 0; i < kQ; ++i) f[i] = pull_link<T>(a, src, c, slot, interior, fl, li, i);
-    } else {
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) {
-        bool halo;
-        f[i] = LD(src, a.qs, i, src_slot(a, c, slot, interior, i, halo), a.inv_scale);
-      }
+    for (int i = 0; i < kQ; ++i) f[i] = LD(src, a.qs, i, s[i], a.inv_scale);
+    if constexpr (LINKS) {
+      if (fl & kFlagNear) apply_links<T>(a, src, c, t, s, halo_mask, fl, f);
     }
     if constexpr (FLAGS) {
       if (fl & kFlagSave) {
-        float* sv = a.save_buf + static_cast<long long>(a.save_idx[slot]) * kQ;
+        float* sv = a.save_buf + static_cast<long long>(a.save_idx[t]) * kQ;
 #pragma unroll
         for (int i = 0; i < kQ; ++i) sv[i] = f[i];
       }
@@ -163,26 +201,29 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
       bgk(f, a.omega);
     }
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + slot, f[i], a.scale);
-  } else {
-    // Torus-streamed halo population of an open block (block_lattice.h:70-89):
-    // item (page, block, halo index, population); no collision; the source
-    // resolves like a core pull (own core, the neighbour core the exchange
-    // copies, or the own halo page).
-    const uint32_t k = t - a.ncore;
-    const int4 it = reinterpret_cast<const int4*>(a.open_pages)[k];
-    const int i = it.w;
-    const int cells = a.np * a.np * a.np;
-    int s = a.hpos[it.z] - a.off_pad[i];
-    s = s < 0 ? s + cells : (s >= cells ? s - cells : s);
-    const int X = static_cast<int>(a.div_np2.div(static_cast<uint32_t>(s)));
-    const int rem = s - X * a.np * a.np;
-    const int Y = static_cast<int>(a.div_np.div(static_cast<uint32_t>(rem)));
-    const int Z = rem - Y * a.np;
-    bool halo;
-    const long long sslot = resolve(a, static_cast<uint32_t>(it.y), X, Y, Z, halo);
-    dst[i * a.qs + a.halo_base + static_cast<long long>(it.x) * a.n_halo + it.z] = src[i * a.qs + sslot];
+    for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + t, f[i], a.scale);
+    return;
   }
+  // Torus-streamed halo population of an open block (block_lattice.h:70-89):
+  // item (page, block, halo index, population); no collision; the source
+  // resolves like a core pull (own core, the neighbour core the exchange
+  // copies, or the own halo page).  Halo items start at the first CTA after
+  // the core CTAs.
+  const uint32_t core_end = ((a.ncore + kThreads - 1) / kThreads) * kThreads;
+  const uint32_t k = t - core_end;
+  if (k >= static_cast<uint32_t>(a.n_open)) return;
+  const int4 it = reinterpret_cast<const int4*>(a.open_pages)[k];
+  const int i = it.w;
+  const int cells = a.np * a.np * a.np;
+  int sp = a.hpos[it.z] - a.off_pad[i];
+  sp = sp < 0 ? sp + cells : (sp >= cells ? sp - cells : sp);
+  const int X = static_cast<int>(a.div_np2.div(static_cast<uint32_t>(sp)));
+  const int rem = sp - X * a.np * a.np;
+  const int Y = static_cast<int>(a.div_np.div(static_cast<uint32_t>(rem)));
+  const int Z = rem - Y * a.np;
+  bool halo;
+  const long long sslot = resolve(a, static_cast<uint32_t>(it.y), X, Y, Z, halo);
+  dst[i * a.qs + a.halo_base + static_cast<long long>(it.x) * a.n_halo + it.z] = src[i * a.qs + sslot];
 }
 
 // Two-element vector access for the paired periodic kernel.
@@ -346,29 +387,38 @@ k_prolong(const ProlongItem* items, int nitems, const float* coarse_save, float*
   for (int i = 0; i < kQ; ++i) Store<T>::st(fine + i * fine_qs + it.fine_slot, f[i], fscale);
 }
 
+// One warp per restriction point: lane k < 1 + nnb reads one source cell's
+// saved populations (the fine cell, then its in-block neighbours) and computes
+// its macro state; the f_neq average is a warp sum.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_restrict(const RestrictItem* items, int nitems, const float* fine_save, T* coarse,
            long long coarse_qs, float scale, float omega, float cscale) {
-  const int t = blockIdx.x * kThreads + threadIdx.x;
-  if (t >= nitems) return;
-  const RestrictItem& it = items[t];
+  const int w = (blockIdx.x * kThreads + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= nitems) return;
+  const RestrictItem& it = items[w];
+  const int row = lane == 0 ? it.fine_save : (lane <= it.nnb ? it.nb_save[lane - 1] : -1);
   Macro m;
-  read_macro(fine_save + static_cast<long long>(it.fine_save) * kQ, m);
+  if (row >= 0) read_macro(fine_save + static_cast<long long>(row) * kQ, m);
   float sum[kQ];
 #pragma unroll
-  for (int i = 0; i < kQ; ++i) sum[i] = 0.f;
-  for (int k = 0; k < it.nnb; ++k) {
-    Macro nm;
-    read_macro(fine_save + static_cast<long long>(it.nb_save[k]) * kQ, nm);
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) sum[i] += nm.fneq[i];
+  for (int i = 0; i < kQ; ++i) {
+    float v = row >= 0 ? m.fneq[i] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    sum[i] = v;
   }
+  const float drho = __shfl_sync(0xffffffffu, m.drho, 0);
+  const float ux = __shfl_sync(0xffffffffu, m.ux, 0), uy = __shfl_sync(0xffffffffu, m.uy, 0),
+              uz = __shfl_sync(0xffffffffu, m.uz, 0);
+  if (lane != 0) return;
+  Macro r;
+  r.drho = drho; r.ux = ux; r.uy = uy; r.uz = uz;
   const float inv = 1.0f / static_cast<float>(it.nnb + 1);
 #pragma unroll
-  for (int i = 0; i < kQ; ++i) m.fneq[i] = (m.fneq[i] + sum[i]) * inv;
+  for (int i = 0; i < kQ; ++i) r.fneq[i] = sum[i] * inv;
   float f[kQ];
-  write_macro_cell(m, scale, it.coarse_kind, omega, f);
+  write_macro_cell(r, scale, it.coarse_kind, omega, f);
 #pragma unroll
   for (int i = 0; i < kQ; ++i) Store<T>::st(coarse + i * coarse_qs + it.coarse_slot, f[i], cscale);
 }
@@ -398,6 +448,11 @@ __device__ inline void block_reduce(double (&v)[N]) {
 // Momentum-exchange force (drag_postprocessor.h:67-115) from the buffer the
 // last step read: f_out = g_i(x) is the post-collide snapshot, and the bounced
 // f_opp(x) is re-pulled from the same buffer with the step's own rule.
+// Momentum-exchange force (drag_postprocessor.h:67-115) from the buffer the
+// last step read.  For a link from kBulk cell x to an in-block obstacle cell
+// x + c_i: f_out = g_i(x) (the post-collide snapshot) and f_bar is the
+// population opp(i) the step pulled from the obstacle: half-way bounce-back
+// g_i(x), or the Bouzidi value with the link's q, plus the moving-wall term.
 template <typename T, bool LINKS>
 __global__ void __launch_bounds__(kThreads)
 k_drag(const StepArgs a, const DragItem* items, int nitems, double* partial) {
@@ -406,21 +461,35 @@ k_drag(const StepArgs a, const DragItem* items, int nitems, double* partial) {
   if (t < nitems) {
     const DragItem it = items[t];
     const T* src = static_cast<const T*>(a.src);
-    const Cell c = cell_of(a, static_cast<uint32_t>(it.slot));
-    const bool interior = is_interior(a, c);
+    float own[kQ];
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) own[i] = LD(src, a.qs, i, it.slot, a.inv_scale);
     const uint8_t fl = a.flags[it.slot];
     const int li = (LINKS && (fl & kFlagLink)) ? a.link_idx[it.slot] : -1;
+    const Cell c = cell_of(a, static_cast<uint32_t>(it.slot));
 #pragma unroll
     for (int i = 1; i < kQ; ++i) {
       if (!(it.mask & (1u << i))) continue;
-      const float f_out = LD(src, a.qs, i, it.slot, a.inv_scale);
+      const int j = opp(i);
       float f_bar;
       if constexpr (LINKS) {
-        f_bar = pull_link<T>(a, src, c, it.slot, interior, fl, li, opp(i));
+        f_bar = own[i];
+        if (li >= 0) {
+          const float q = a.link_rec[li * 38 + j];
+          if (q < 1.0f) {
+            bool nhalo;
+            const long long nb = resolve(a, c.b, static_cast<int>(c.x) + 1 + cx(j),
+                                         static_cast<int>(c.y) + 1 + cy(j), static_cast<int>(c.z) + 1 + cz(j), nhalo);
+            const int nk = nhalo ? kBulk : (a.flags[nb] & kKindMask);
+            const float f_q = nk == kBulk ? LD(src, a.qs, j, nb, a.inv_scale) : own[j];
+            f_bar = bouzidi(own[i], f_q, own[j], q);
+          }
+          f_bar += a.link_rec[li * 38 + kQ + j];
+        }
       } else {
-        f_bar = LD(src, a.qs, opp(i), it.slot + a.off[i], a.inv_scale);  // x + c_i is in-block core
+        f_bar = LD(src, a.qs, j, it.slot + a.off[i], a.inv_scale);  // plain pull from x + c_i
       }
-      const double s = static_cast<double>(f_out) + static_cast<double>(f_bar);
+      const double s = static_cast<double>(own[i]) + static_cast<double>(f_bar);
       acc[0] += s * cx(i); acc[1] += s * cy(i); acc[2] += s * cz(i);
     }
   }
@@ -534,13 +603,21 @@ template <typename T>
 cudaError_t launch_step(const StepArgs& a, bool periodic, bool links, bool flags, cudaStream_t s) {
   (void)periodic;
   if (a.nitems == 0) return cudaSuccess;
-  const dim3 g(grid_for(a.nitems));
-  if (links) {
-    k_step<T, true, true><<<g, kThreads, 0, s>>>(a);
-  } else if (flags) {
-    k_step<T, false, true><<<g, kThreads, 0, s>>>(a);
+  // CTAs aligned to blocks: core cells first (a multiple of the CTA size),
+  // then the halo items in CTAs of their own.
+  const uint32_t n3 = static_cast<uint32_t>(a.n) * a.n * a.n;
+  const bool blocked = n3 % kThreads == 0;
+  const uint32_t core_ctas = grid_for(a.ncore);
+  const dim3 g(core_ctas + grid_for(a.nitems - a.ncore));
+  StepArgs b = a;
+  if (blocked) {
+    if (links) k_step<T, true, true, true><<<g, kThreads, 0, s>>>(b);
+    else if (flags) k_step<T, false, true, true><<<g, kThreads, 0, s>>>(b);
+    else k_step<T, false, false, true><<<g, kThreads, 0, s>>>(b);
   } else {
-    k_step<T, false, false><<<g, kThreads, 0, s>>>(a);
+    if (links) k_step<T, true, true, false><<<g, kThreads, 0, s>>>(b);
+    else if (flags) k_step<T, false, true, false><<<g, kThreads, 0, s>>>(b);
+    else k_step<T, false, false, false><<<g, kThreads, 0, s>>>(b);
   }
   return cudaGetLastError();
 }
@@ -579,18 +656,22 @@ cudaError_t launch_restrict(const RestrictItem* items, int n, const float* fine_
                             long long coarse_qs, float scale, float omega, float cscale,
                             cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_restrict<T><<<grid_for(n), kThreads, 0, s>>>(items, n, fine_save, coarse, coarse_qs, scale,
-                                                 omega, cscale);
+  k_restrict<T><<<grid_for(static_cast<uint32_t>(n) * 32), kThreads, 0, s>>>(items, n, fine_save, coarse,
+                                                                             coarse_qs, scale, omega, cscale);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_drag(const StepArgs& a, bool links, const DragItem* items, int n, double* partial,
-                        double* out, double* accum, cudaStream_t s) {
+                        cudaStream_t s) {
   const uint32_t g = grid_for(static_cast<uint32_t>(n > 0 ? n : 1));
   if (links) k_drag<T, true><<<g, kThreads, 0, s>>>(a, items, n, partial);
   else k_drag<T, false><<<g, kThreads, 0, s>>>(a, items, n, partial);
-  k_sum_partials<<<1, kThreads, 0, s>>>(partial, static_cast<int>(g), 3, out, accum);
+  return cudaGetLastError();
+}
+// Force = fixed-order sum of every level's drag partials; accum += force.
+cudaError_t launch_drag_total(const double* partial, int nparts, double* out, double* accum, cudaStream_t s) {
+  k_sum_partials<<<1, kThreads, 0, s>>>(partial, nparts, 3, out, accum);
   return cudaGetLastError();
 }
 uint32_t drag_partials(int n) { return grid_for(static_cast<uint32_t>(n > 0 ? n : 1)); }
@@ -625,7 +706,7 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
   template cudaError_t launch_restrict<T>(const RestrictItem*, int, const float*, T*, long long,   \
                                           float, float, float, cudaStream_t);                      \
   template cudaError_t launch_drag<T>(const StepArgs&, bool, const DragItem*, int, double*,        \
-                                      double*, double*, cudaStream_t);                             \
+                                      cudaStream_t);                                               \
   template cudaError_t launch_audit<T>(const StepArgs&, double*, double*, cudaStream_t);           \
   template cudaError_t launch_gather<T>(const StepArgs&, double*, double*, int, cudaStream_t);              \
   template cudaError_t launch_scatter<T>(const StepArgs&, const double*, cudaStream_t);

@@ -29,8 +29,8 @@ template <typename T>
 cudaError_t launch_restrict(const RestrictItem*, int, const float*, T*, long long, float, float,
                             float, cudaStream_t);
 template <typename T>
-cudaError_t launch_drag(const StepArgs&, bool, const DragItem*, int, double*, double*, double*,
-                        cudaStream_t);
+cudaError_t launch_drag(const StepArgs&, bool, const DragItem*, int, double*, cudaStream_t);
+cudaError_t launch_drag_total(const double*, int, double*, double*, cudaStream_t);
 template <typename T> cudaError_t launch_audit(const StepArgs&, double*, double*, cudaStream_t);
 template <typename T> cudaError_t launch_gather(const StepArgs&, double*, double*, int, cudaStream_t);
 template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*, cudaStream_t);
@@ -97,8 +97,10 @@ struct Level {
   DevBuf prolong_items, prev, restrict_items;
   int n_prolong = 0, n_restrict = 0;
   // drag
-  DevBuf drag_items, drag_partial;
+  DevBuf drag_items;
   int n_drag = 0;
+  long long drag_off = 0;           // this level's rows in the context's drag partials
+  int substep = 0;                  // steps of this level within the current advance_one
   float scale = 1.f, inv_scale = 1.f;
   bool use_bulk = false;            // pipelined bulk-copy step (periodic block)
   bool use_pair = false;            // two-cells-per-thread step (periodic block)
@@ -121,7 +123,8 @@ struct octlb_ctx {
   std::vector<uint8_t> kinds;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  DevBuf force_lvl, force, force_sum, audit_out, audit_partial, host_tmp, dev_err;
+  DevBuf drag_partial, force, force_sum, audit_out, audit_partial, host_tmp, dev_err;
+  int drag_parts = 0;
   long long force_steps = 0;
   std::vector<int> counters_collide, counters_stream;
   long long launches_per_step = 0, lups_per_step = 0;
@@ -228,10 +231,12 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     CK(launch_step<T>(a, ctx->periodic != 0, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags,
                       ctx->stream));
   }
-  if (ctx->drag && L.n_drag > 0) {
+  // The force after advance_one reads each level's last step (the reference
+  // computes MomentumExchangeDrag once, after advance_one): skip the others.
+  ++L.substep;
+  if (ctx->drag && L.n_drag > 0 && L.substep == (1 << L.lvl)) {
     CK(launch_drag<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.drag_items.as<DragItem>(), L.n_drag,
-                      L.drag_partial.as<double>(), ctx->force_lvl.as<double>() + 3 * L.lvl, nullptr,
-                      ctx->stream));
+                      ctx->drag_partial.as<double>() + 3 * L.drag_off, ctx->stream));
   }
   L.cur = 1 - L.cur;
   return OCTLB_OK;
@@ -263,16 +268,6 @@ int do_advance_level(octlb_ctx* ctx, int l) {
                           static_cast<float>(ctx->omega), L.scale, ctx->stream));
   }
   return OCTLB_OK;
-}
-
-// Sum of the per-level MEM forces into the step force and its running sum.
-__global__ void k_force_total(const double* lvl, int nlvl, double* out, double* sum) {
-  if (threadIdx.x < 3) {
-    double s = 0.0;
-    for (int l = 0; l < nlvl; ++l) s += lvl[3 * l + threadIdx.x];
-    out[threadIdx.x] = s;
-    sum[threadIdx.x] += s;
-  }
 }
 
 int validate(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p) {
@@ -556,6 +551,30 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       flags[s] |= kFlagLink;
     }
     L.n_links = static_cast<int>(lrec.size() / 38);
+    if (links) {
+      // kFlagNear: the cell's pull needs the link rule -- a link record, a
+      // solid / Bouzidi source in the own core, or a reflecting kind with a
+      // source in the halo (block_lattice.cpp:624-670).
+      for (int lb = 0; lb < L.nblk; ++lb)
+        for (int x = 0; x < n; ++x)
+          for (int y = 0; y < n; ++y)
+            for (int z = 0; z < n; ++z) {
+              const long long sc = core_slot_of(n, lb, x, y, z);
+              const int kind = flags[sc] & kKindMask;
+              bool near = (flags[sc] & kFlagLink) != 0;
+              for (int i = 1; i < kQ && !near; ++i) {
+                const int sx = x - cx(i), sy = y - cy(i), sz = z - cz(i);
+                const bool halo = sx < 0 || sy < 0 || sz < 0 || sx >= n || sy >= n || sz >= n;
+                if (halo) {
+                  near = reflects_on_pull(kind);
+                } else {
+                  const int sk = flags[core_slot_of(n, lb, sx, sy, sz)] & kKindMask;
+                  near = sk == kSolid || sk == kBouzidi;
+                }
+              }
+              if (near) flags[sc] |= kFlagNear;
+            }
+    }
     if (!save_rows[l].empty()) {
       sidx.assign(static_cast<size_t>(ncore), -1);
       for (const auto& kv : save_rows[l]) {
@@ -841,7 +860,10 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     L.n_prolong = static_cast<int>(prolong[l].size());
     L.n_restrict = static_cast<int>(restrict_items[l].size());
     CK(upload(L.drag_items, drag));
-    CK(L.drag_partial.alloc(drag_partials(L.n_drag) * 3 * sizeof(double)));
+    if (L.n_drag > 0) {
+      L.drag_off = ctx->drag_parts;
+      ctx->drag_parts += static_cast<int>(drag_partials(L.n_drag));
+    }
 
     StepArgs& A = L.args;
     A = StepArgs{};
@@ -911,7 +933,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     if (ctx->levels[l].n_prolong == 0) continue;
     CK(upload(ctx->levels[l].prev, prev));
   }
-  CK(ctx->force_lvl.alloc(static_cast<size_t>(nlev) * 3 * sizeof(double)));
+  CK(ctx->drag_partial.alloc(static_cast<size_t>(std::max(ctx->drag_parts, 1)) * 3 * sizeof(double)));
   CK(ctx->force.alloc(3 * sizeof(double)));
   CK(ctx->force_sum.alloc(3 * sizeof(double)));
   CK(ctx->audit_out.alloc(5 * sizeof(double)));
@@ -950,12 +972,12 @@ int check_device_error(octlb_ctx* ctx) {
 // One advance_one: the TimeLoop recursion from level 0, then the force total.
 template <typename T>
 int advance_one_launches(octlb_ctx* ctx) {
+  for (auto& L : ctx->levels) L.substep = 0;
   int rc = do_advance_level<T>(ctx, 0);
   if (rc) return rc;
-  if (ctx->drag) {
-    k_force_total<<<1, 32, 0, ctx->stream>>>(ctx->force_lvl.as<double>(), ctx->max_level + 1,
-                                             ctx->force.as<double>(), ctx->force_sum.as<double>());
-    CK(cudaGetLastError());
+  if (ctx->drag && ctx->drag_parts > 0) {
+    CK(launch_drag_total(ctx->drag_partial.as<double>(), ctx->drag_parts, ctx->force.as<double>(),
+                         ctx->force_sum.as<double>(), ctx->stream));
   }
   return OCTLB_OK;
 }
@@ -1278,8 +1300,8 @@ int octlb_gpu_step_stats(const octlb_ctx* ctx, long long* launches, long long* l
   for (size_t l = 0; l < ctx->levels.size(); ++l) {
     const Level& L = ctx->levels[l];
     if (L.nblk == 0) continue;
-    per[l] = (L.n_bb > 0 ? 1 : 0) + (L.args.nitems > 0 ? 1 : 0) +
-             (ctx->drag && L.n_drag > 0 ? 2 : 0);
+    per[l] = (L.n_bb > 0 ? 1 : 0) + (L.args.nitems > 0 ? 1 : 0);
+    if (ctx->drag && L.n_drag > 0) total += 1;  // once per advance_one, last step of the level
   }
   for (size_t l = 0; l < ctx->levels.size(); ++l) {
     const Level& L = ctx->levels[l];
@@ -1290,7 +1312,7 @@ int octlb_gpu_step_stats(const octlb_ctx* ctx, long long* launches, long long* l
       total += (ctx->levels[l + 1].n_restrict > 0 ? 1 : 0) * mult;
     }
   }
-  if (ctx->drag) total += 1;
+  if (ctx->drag && ctx->drag_parts > 0) total += 1;
   if (launches) *launches = total;
   if (lups) *lups = ctx->lups_per_step;
   return OCTLB_OK;
