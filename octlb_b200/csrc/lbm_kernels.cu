@@ -49,7 +49,7 @@ __device__ __forceinline__ Cell cell_of(const StepArgs& a, uint32_t t) {
 // Own halo-page slot of padded position (X, Y, Z) of block b; positions that
 // no table covers are excluded by construction, the check keeps the access in
 // bounds and records an error if that ever fails.
-__device__ __noinline__ long long page_slot(const StepArgs& a, uint32_t b, int X, int Y, int Z) {
+__device__ __forceinline__ long long page_slot(const StepArgs& a, uint32_t b, int X, int Y, int Z) {
   const int pg = a.page_of[b];
   const int h = a.hmap[(X * a.np + Y) * a.np + Z];
   if (pg < 0 || h < 0) {
@@ -182,14 +182,15 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
         return;
       }
     }
+    // Cells next to walls take the link rule in k_step_near.
+    if constexpr (LINKS) {
+      if (fl & kFlagNear) return;
+    }
     long long s[kQ];
     uint32_t halo_mask;
     source_slots(a, c, t, tl, BLOCKED ? sb : nullptr, s, halo_mask);
 #pragma unroll
     for (int i = 0; i < kQ; ++i) f[i] = LD(src, a.qs, i, s[i], a.inv_scale);
-    if constexpr (LINKS) {
-      if (fl & kFlagNear) apply_links<T>(a, src, c, t, s, halo_mask, fl, f);
-    }
     if constexpr (FLAGS) {
       if (fl & kFlagSave) {
         float* sv = a.save_buf + static_cast<long long>(a.save_idx[t]) * kQ;
@@ -224,6 +225,36 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
   bool halo;
   const long long sslot = resolve(a, static_cast<uint32_t>(it.y), X, Y, Z, halo);
   dst[i * a.qs + a.halo_base + static_cast<long long>(it.x) * a.n_halo + it.z] = src[i * a.qs + sslot];
+}
+
+// Cells flagged kFlagNear (links stream rule): the per-cell link rule, then
+// the same save / collide / store as k_step.  A separate launch keeps the
+// register-heavy rule out of the bulk kernel.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_step_near(const StepArgs a, const int* cells, int ncells) {
+  const int k = blockIdx.x * kThreads + threadIdx.x;
+  if (k >= ncells) return;
+  const T* src = static_cast<const T*>(a.src);
+  T* dst = static_cast<T*>(a.dst);
+  const long long t = cells[k];
+  const Cell c = cell_of(a, static_cast<uint32_t>(t));
+  const long long tl = t - static_cast<long long>(c.b) * a.n * a.n * a.n;
+  const uint8_t fl = a.flags[t];
+  long long s[kQ];
+  uint32_t halo_mask;
+  source_slots(a, c, t, tl, nullptr, s, halo_mask);
+  float f[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) f[i] = LD(src, a.qs, i, s[i], a.inv_scale);
+  apply_links<T>(a, src, c, t, s, halo_mask, fl, f);
+  if (fl & kFlagSave) {
+    float* sv = a.save_buf + static_cast<long long>(a.save_idx[t]) * kQ;
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) sv[i] = f[i];
+  }
+  if ((fl & kKindMask) == kBulk) bgk(f, a.omega);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + t, f[i], a.scale);
 }
 
 // Two-element vector access for the paired periodic kernel.
@@ -623,6 +654,13 @@ cudaError_t launch_step(const StepArgs& a, bool periodic, bool links, bool flags
 }
 
 template <typename T>
+cudaError_t launch_step_near(const StepArgs& a, const int* cells, int ncells, cudaStream_t s) {
+  if (ncells == 0) return cudaSuccess;
+  k_step_near<T><<<grid_for(static_cast<uint32_t>(ncells)), kThreads, 0, s>>>(a, cells, ncells);
+  return cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t launch_step_pair(const StepArgs& a, cudaStream_t s) {
   k_step_pair<T><<<grid_for(a.ncore / 2), kThreads, 0, s>>>(a);
   return cudaGetLastError();
@@ -699,6 +737,7 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
 #define OCTLB_INST(T)                                                                              \
   template cudaError_t launch_step<T>(const StepArgs&, bool, bool, bool, cudaStream_t);            \
   template cudaError_t launch_step_pair<T>(const StepArgs&, cudaStream_t);                         \
+  template cudaError_t launch_step_near<T>(const StepArgs&, const int*, int, cudaStream_t);         \
   template cudaError_t launch_ghost<T>(T*, long long, const CopyDesc*, const uint32_t*, int,       \
                                        uint32_t, const BBOp*, uint32_t, float, float, cudaStream_t); \
   template cudaError_t launch_prolong<T>(const ProlongItem*, int, const float*, float*, int, T*,   \

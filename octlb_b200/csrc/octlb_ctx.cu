@@ -37,6 +37,7 @@ template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*,
 template <typename T> cudaError_t launch_step_bulk(const StepArgs&, int, cudaStream_t);
 template <typename T> int bulk_prepare(int n);
 template <typename T> cudaError_t launch_step_pair(const StepArgs&, cudaStream_t);
+template <typename T> cudaError_t launch_step_near(const StepArgs&, const int*, int, cudaStream_t);
 bool pair_step_eligible(int n);
 bool bulk_step_eligible(int n, int elem_bytes);
 uint32_t drag_partials(int n);
@@ -87,7 +88,8 @@ struct Level {
   DevBuf buf[2];
   int cur = 0;
   DevBuf flags, link_idx, link_rec, save_idx, save_buf;
-  DevBuf nbase, page_of, hmap, hpos, open_pages;
+  DevBuf nbase, page_of, hmap, hpos, open_pages, near_cells;
+  int n_near = 0;
   int n_open = 0, n_halo = 0, n_pages = 0, n_save = 0, n_links = 0;
   bool has_flags = false;
   // tree-boundary halo fills
@@ -230,6 +232,7 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
   } else {
     CK(launch_step<T>(a, ctx->periodic != 0, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags,
                       ctx->stream));
+    CK(launch_step_near<T>(a, L.near_cells.as<int>(), L.n_near, ctx->stream));
   }
   // The force after advance_one reads each level's last step (the reference
   // computes MomentumExchangeDrag once, after advance_one): skip the others.
@@ -572,9 +575,13 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
                   near = sk == kSolid || sk == kBouzidi;
                 }
               }
-              if (near) flags[sc] |= kFlagNear;
+              if (near && kind != kSolid) flags[sc] |= kFlagNear;
             }
     }
+    std::vector<int> near_cells;
+    for (long long k = 0; k < ncore; ++k)
+      if (flags[k] & kFlagNear) near_cells.push_back(static_cast<int>(k));
+    L.n_near = static_cast<int>(near_cells.size());
     if (!save_rows[l].empty()) {
       sidx.assign(static_cast<size_t>(ncore), -1);
       for (const auto& kv : save_rows[l]) {
@@ -854,6 +861,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     CK(upload(L.hmap, hmap));
     CK(upload(L.hpos, hpos));
     CK(upload(L.open_pages, open_pages));
+    CK(upload(L.near_cells, near_cells));
     CK(upload(L.bb_ops, bbv));
     CK(upload(L.prolong_items, prolong[l]));
     CK(upload(L.restrict_items, restrict_items[l]));
@@ -1300,7 +1308,7 @@ int octlb_gpu_step_stats(const octlb_ctx* ctx, long long* launches, long long* l
   for (size_t l = 0; l < ctx->levels.size(); ++l) {
     const Level& L = ctx->levels[l];
     if (L.nblk == 0) continue;
-    per[l] = (L.n_bb > 0 ? 1 : 0) + (L.args.nitems > 0 ? 1 : 0);
+    per[l] = (L.n_bb > 0 ? 1 : 0) + (L.args.nitems > 0 ? 1 : 0) + (L.n_near > 0 && !L.use_pair && !L.use_bulk ? 1 : 0);
     if (ctx->drag && L.n_drag > 0) total += 1;  // once per advance_one, last step of the level
   }
   for (size_t l = 0; l < ctx->levels.size(); ++l) {
