@@ -153,6 +153,29 @@ __device__ __forceinline__ void apply_links(const StepArgs& a, const T* src, con
   }
 }
 
+// Torus-streamed halo population of an open block (block_lattice.h:70-89):
+// item k = (page, block, halo index, population); no collision; the source
+// resolves like a core pull (own core, the neighbour core the exchange
+// copies, or the own halo page).
+template <typename T>
+__device__ __forceinline__ void rotate_item(const StepArgs& a, uint32_t k) {
+  if (k >= static_cast<uint32_t>(a.n_open)) return;
+  const T* src = static_cast<const T*>(a.src);
+  T* dst = static_cast<T*>(a.dst);
+  const int4 it = reinterpret_cast<const int4*>(a.open_pages)[k];
+  const int i = it.w;
+  const int cells = a.np * a.np * a.np;
+  int sp = a.hpos[it.z] - a.off_pad[i];
+  sp = sp < 0 ? sp + cells : (sp >= cells ? sp - cells : sp);
+  const int X = static_cast<int>(a.div_np2.div(static_cast<uint32_t>(sp)));
+  const int rem = sp - X * a.np * a.np;
+  const int Y = static_cast<int>(a.div_np.div(static_cast<uint32_t>(rem)));
+  const int Z = rem - Y * a.np;
+  bool halo;
+  const long long sslot = resolve(a, static_cast<uint32_t>(it.y), X, Y, Z, halo);
+  dst[i * a.qs + a.halo_base + static_cast<long long>(it.x) * a.n_halo + it.z] = src[i * a.qs + sslot];
+}
+
 template <typename T, bool LINKS, bool FLAGS, bool BLOCKED>
 __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
@@ -205,26 +228,9 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
     for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + t, f[i], a.scale);
     return;
   }
-  // Torus-streamed halo population of an open block (block_lattice.h:70-89):
-  // item (page, block, halo index, population); no collision; the source
-  // resolves like a core pull (own core, the neighbour core the exchange
-  // copies, or the own halo page).  Halo items start at the first CTA after
-  // the core CTAs.
+  // Halo items start at the first CTA after the core CTAs.
   const uint32_t core_end = ((a.ncore + kThreads - 1) / kThreads) * kThreads;
-  const uint32_t k = t - core_end;
-  if (k >= static_cast<uint32_t>(a.n_open)) return;
-  const int4 it = reinterpret_cast<const int4*>(a.open_pages)[k];
-  const int i = it.w;
-  const int cells = a.np * a.np * a.np;
-  int sp = a.hpos[it.z] - a.off_pad[i];
-  sp = sp < 0 ? sp + cells : (sp >= cells ? sp - cells : sp);
-  const int X = static_cast<int>(a.div_np2.div(static_cast<uint32_t>(sp)));
-  const int rem = sp - X * a.np * a.np;
-  const int Y = static_cast<int>(a.div_np.div(static_cast<uint32_t>(rem)));
-  const int Z = rem - Y * a.np;
-  bool halo;
-  const long long sslot = resolve(a, static_cast<uint32_t>(it.y), X, Y, Z, halo);
-  dst[i * a.qs + a.halo_base + static_cast<long long>(it.x) * a.n_halo + it.z] = src[i * a.qs + sslot];
+  rotate_item<T>(a, t - core_end);
 }
 
 // Cells flagged kFlagNear (links stream rule): the per-cell link rule, then
@@ -278,6 +284,89 @@ template <> struct Pair<__half> {
     *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a, b);
   }
 };
+
+// Forest-level step with a per-block slot map: one CTA per block stages the
+// block's (n+2)^3 map (padded position -> slot: own core, the neighbour core
+// the same-level exchange copies, or the own halo page) in shared memory, so
+// every pull is one shared-memory read and one 32-bit offset, with no
+// per-direction branching at block faces.  Each thread takes cells tl and
+// tl + 256 together (n^3 a multiple of 512), all 38 pulls issued before the
+// two collisions.  Same arithmetic as k_step; kFlagNear cells are left to
+// k_step_near, solid cells of the links rule are copied.  CTAs after the
+// nblk block CTAs stream the open blocks' halo items.
+template <typename T, bool LINKS, bool FLAGS>
+__device__ __forceinline__ bool map_cell_prologue(const StepArgs& a, uint32_t t, const T* src, T* dst, uint8_t& fl) {
+  fl = FLAGS ? a.flags[t] : 0;
+  if constexpr (LINKS) {
+    if ((fl & kKindMask) == kSolid) {
+      // Solid cells are neither streamed nor collided (block_lattice.cpp:581-583).
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) dst[i * a.qs + t] = src[i * a.qs + t];
+      return false;
+    }
+    if (fl & kFlagNear) return false;
+  }
+  return true;
+}
+
+template <typename T, bool FLAGS>
+__device__ __forceinline__ void map_cell_finish(const StepArgs& a, uint32_t t, uint8_t fl, float (&f)[kQ], T* dst) {
+  if constexpr (FLAGS) {
+    if (fl & kFlagSave) {
+      float* sv = a.save_buf + static_cast<long long>(a.save_idx[t]) * kQ;
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) sv[i] = f[i];
+    }
+    if ((fl & kKindMask) == kBulk) bgk(f, a.omega);
+  } else {
+    bgk(f, a.omega);
+  }
+  const uint32_t qs = static_cast<uint32_t>(a.qs);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) Store<T>::st(dst + (static_cast<uint32_t>(i) * qs + t), f[i], a.scale);
+}
+
+template <typename T, bool LINKS, bool FLAGS, int CPT>
+__global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const StepArgs a) {
+  extern __shared__ int smap[];  // (n+2)^3 slots of this block
+  const uint32_t b = blockIdx.x;
+  if (b >= static_cast<uint32_t>(a.nblk)) {
+    rotate_item<T>(a, (b - a.nblk) * kThreads + threadIdx.x);
+    return;
+  }
+  const int np = a.np, np3 = np * np * np;
+  const int* gm = a.slot_map + static_cast<long long>(b) * np3;
+  for (int k = threadIdx.x; k < np3; k += kThreads) smap[k] = gm[k];
+  __syncthreads();
+  const T* src = static_cast<const T*>(a.src);
+  T* dst = static_cast<T*>(a.dst);
+  const uint32_t n = a.n, n3 = n * n * n, qs = static_cast<uint32_t>(a.qs);
+  for (uint32_t tl0 = threadIdx.x; tl0 < n3; tl0 += CPT * kThreads) {
+    uint32_t t[CPT];
+    int P[CPT];
+    uint8_t fl[CPT];
+    bool go[CPT];
+    float f[CPT][kQ];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const uint32_t tl = tl0 + c * kThreads;
+      t[c] = b * n3 + tl;
+      const uint32_t x = a.div_n2.div(tl), r = tl - x * n * n, y = a.div_n.div(r);
+      P[c] = (static_cast<int>(x + 1) * np + static_cast<int>(y + 1)) * np + static_cast<int>(r - y * n + 1);
+      go[c] = map_cell_prologue<T, LINKS, FLAGS>(a, t[c], src, dst, fl[c]);
+    }
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      const uint32_t row = static_cast<uint32_t>(i) * qs;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c)
+        f[c][i] = Store<T>::ld(src + (row + static_cast<uint32_t>(smap[P[c] - a.off_pad[i]])), a.inv_scale);
+    }
+#pragma unroll
+    for (int c = 0; c < CPT; ++c)
+      if (go[c]) map_cell_finish<T, FLAGS>(a, t[c], fl[c], f[c], dst);
+  }
+}
 
 // One periodic all-kBulk block, two consecutive z cells per thread: every
 // population row is read and written with 2-element vector accesses; a z-shift
@@ -653,6 +742,29 @@ cudaError_t launch_step(const StepArgs& a, bool periodic, bool links, bool flags
   return cudaGetLastError();
 }
 
+// Slot-map step: a CTA of 256 threads per block (n^3 a multiple of 512, the
+// (n+2)^3 map within 48 KB of shared memory, 32-bit population offsets).
+bool map_step_eligible(int n, long long nslots) {
+  const long long np = n + 2;
+  return n % 8 == 0 && np * np * np * 4 <= 48 * 1024 && nslots * kQ < (1LL << 32);
+}
+template <typename T>
+cudaError_t launch_step_map(const StepArgs& a, bool links, bool flags, int cpt, cudaStream_t s) {
+  if (a.nitems == 0) return cudaSuccess;
+  const dim3 g(static_cast<uint32_t>(a.nblk) + grid_for(static_cast<uint32_t>(a.n_open)));
+  const size_t smem = static_cast<size_t>(a.np) * a.np * a.np * sizeof(int);
+  if (cpt == 2) {
+    if (links) k_step_map<T, true, true, 2><<<g, kThreads, smem, s>>>(a);
+    else if (flags) k_step_map<T, false, true, 2><<<g, kThreads, smem, s>>>(a);
+    else k_step_map<T, false, false, 2><<<g, kThreads, smem, s>>>(a);
+  } else {
+    if (links) k_step_map<T, true, true, 1><<<g, kThreads, smem, s>>>(a);
+    else if (flags) k_step_map<T, false, true, 1><<<g, kThreads, smem, s>>>(a);
+    else k_step_map<T, false, false, 1><<<g, kThreads, smem, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_step_near(const StepArgs& a, const int* cells, int ncells, cudaStream_t s) {
   if (ncells == 0) return cudaSuccess;
@@ -738,6 +850,7 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
   template cudaError_t launch_step<T>(const StepArgs&, bool, bool, bool, cudaStream_t);            \
   template cudaError_t launch_step_pair<T>(const StepArgs&, cudaStream_t);                         \
   template cudaError_t launch_step_near<T>(const StepArgs&, const int*, int, cudaStream_t);         \
+  template cudaError_t launch_step_map<T>(const StepArgs&, bool, bool, int, cudaStream_t);         \
   template cudaError_t launch_ghost<T>(T*, long long, const CopyDesc*, const uint32_t*, int,       \
                                        uint32_t, const BBOp*, uint32_t, float, float, cudaStream_t); \
   template cudaError_t launch_prolong<T>(const ProlongItem*, int, const float*, float*, int, T*,   \

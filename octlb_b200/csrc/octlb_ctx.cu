@@ -38,7 +38,9 @@ template <typename T> cudaError_t launch_step_bulk(const StepArgs&, int, cudaStr
 template <typename T> int bulk_prepare(int n);
 template <typename T> cudaError_t launch_step_pair(const StepArgs&, cudaStream_t);
 template <typename T> cudaError_t launch_step_near(const StepArgs&, const int*, int, cudaStream_t);
+template <typename T> cudaError_t launch_step_map(const StepArgs&, bool, bool, int, cudaStream_t);
 bool pair_step_eligible(int n);
+bool map_step_eligible(int n, long long nslots);
 bool bulk_step_eligible(int n, int elem_bytes);
 uint32_t drag_partials(int n);
 uint32_t audit_partials(const StepArgs& a);
@@ -88,7 +90,7 @@ struct Level {
   DevBuf buf[2];
   int cur = 0;
   DevBuf flags, link_idx, link_rec, save_idx, save_buf;
-  DevBuf nbase, page_of, hmap, hpos, open_pages, near_cells;
+  DevBuf nbase, page_of, hmap, hpos, open_pages, near_cells, slot_map;
   int n_near = 0;
   int n_open = 0, n_halo = 0, n_pages = 0, n_save = 0, n_links = 0;
   bool has_flags = false;
@@ -106,6 +108,7 @@ struct Level {
   float scale = 1.f, inv_scale = 1.f;
   bool use_bulk = false;            // pipelined bulk-copy step (periodic block)
   bool use_pair = false;            // two-cells-per-thread step (periodic block)
+  bool use_map = false;             // slot-map step (forest level)
   int bulk_grid = 0;
   StepArgs args{};
 };
@@ -131,6 +134,8 @@ struct octlb_ctx {
   std::vector<int> counters_collide, counters_stream;
   long long launches_per_step = 0, lups_per_step = 0;
   int step_kernel = 0;              // OCTLB_STEP_KERNEL: 0 pair (default), 1 bulk, 2 plain
+  int map_cells = 0;                // cells per thread of the slot-map step (OCTLB_MAP_CELLS 1 or 2;
+                                    // default 2, 1 under the links rule whose variant spills at 2)
   // advance_one captured as CUDA graphs, keyed by the A/B parity of every
   // level's buffers (the launch arguments depend on it)
   struct GraphEntry {
@@ -229,6 +234,9 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
   } else if (L.use_pair) {
     CK(launch_step_pair<T>(a, ctx->stream));
+  } else if (L.use_map) {
+    CK(launch_step_map<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags, ctx->map_cells, ctx->stream));
+    CK(launch_step_near<T>(a, L.near_cells.as<int>(), L.n_near, ctx->stream));
   } else {
     CK(launch_step<T>(a, ctx->periodic != 0, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags,
                       ctx->stream));
@@ -757,7 +765,9 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     open_pages = halo_items;
     L.n_open = static_cast<int>(halo_items.size() / 4);
     L.n_halo = L.n_pages > 0 ? H : 0;
+    // even slot count: population rows start on 2-element boundaries
     L.nslots = ncore + static_cast<long long>(L.n_pages) * H;
+    L.nslots += L.nslots & 1;
     std::vector<BBOp> bbv;
     for (const BB& op : bbl)
       bbv.push_back(BBOp{ncore + static_cast<long long>(page_of[op.lb]) * H + hmap[op.hlin], op.src, op.pop,
@@ -775,6 +785,44 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
         const long long vl = ctx->blk_local[v];
         nbase[static_cast<size_t>(lb) * 27 + d] = (vl - ox) * n3 - static_cast<long long>(oy) * n * n - oz * n;
       }
+
+    // Slot of every padded position of every block (the slot-map step's
+    // table): own core, the neighbour core the same-level exchange copies,
+    // or the own halo page.  Positions nothing resolves (the padded box's
+    // corners, and halo positions of closed blocks no table covers) point at
+    // the block's first core slot and must never be pulled: checked below
+    // for every cell the step kernel streams.
+    std::vector<int> slot_map;
+    if (map_step_eligible(n, L.nslots) && !(ctx->periodic && !L.has_flags)) {
+      slot_map.assign(static_cast<size_t>(L.nblk) * np3, 0);
+      std::vector<uint8_t> unresolved(static_cast<size_t>(np3));
+      for (int lb = 0; lb < L.nblk; ++lb) {
+        int* m = slot_map.data() + static_cast<size_t>(lb) * np3;
+        for (int X = 0; X < np; ++X)
+          for (int Y = 0; Y < np; ++Y)
+            for (int Z = 0; Z < np; ++Z) {
+              const int P = (X * np + Y) * np + Z;
+              const long long lin = (static_cast<long long>(X - 1) * n + (Y - 1)) * n + (Z - 1);
+              const int d = dir27(X, Y, Z);
+              long long sl = -1;
+              if (d == 13) sl = static_cast<long long>(lb) * n3 + lin;
+              else if (nbase[static_cast<size_t>(lb) * 27 + d] != kOwnPage) sl = nbase[static_cast<size_t>(lb) * 27 + d] + lin;
+              else if (page_of[lb] >= 0) sl = ncore + static_cast<long long>(page_of[lb]) * H + hmap[P];
+              unresolved[P] = sl < 0;
+              if (sl >= L.nslots) return fail(ctx, OCTLB_EINVAL, "internal: slot map out of range");
+              m[P] = sl < 0 ? static_cast<int>(static_cast<long long>(lb) * n3) : static_cast<int>(sl);
+            }
+        for (int x = 0; x < n; ++x)
+          for (int y = 0; y < n; ++y)
+            for (int z = 0; z < n; ++z) {
+              const uint8_t f = flags[static_cast<size_t>(core_slot_of(n, lb, x, y, z))];
+              if (ctx->stream_mode == OCTLB_STREAM_LINKS && ((f & kKindMask) == kSolid || (f & kFlagNear))) continue;
+              for (int i = 1; i < kQ; ++i)
+                if (unresolved[((x + 1 - cx(i)) * np + (y + 1 - cy(i))) * np + (z + 1 - cz(i))])
+                  return fail(ctx, OCTLB_EINVAL, "internal: pulled halo position without a source");
+            }
+      }
+    }
 
     // Drag cells (drag_postprocessor.h:73-110).
     std::vector<DragItem> drag;
@@ -911,6 +959,14 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     // one-cell-per-thread step with OCTLB_STEP_KERNEL=plain.
     const bool uniform = ctx->periodic && !L.has_flags;
     if (uniform && ctx->step_kernel == 0 && pair_step_eligible(n)) L.use_pair = true;
+    // Any other level: the slot-map step by default, the one-cell-per-thread
+    // k_step with OCTLB_STEP_KERNEL=plain (or bulk, which only periodic
+    // blocks take) or where the map does not fit.
+    if (!uniform && ctx->step_kernel == 0 && map_step_eligible(n, L.nslots)) {
+      L.use_map = true;
+      CK(upload(L.slot_map, slot_map));
+      A.slot_map = L.slot_map.as<int>();
+    }
     if (uniform && ctx->step_kernel == 1 && bulk_step_eligible(n, sizeof(T)) && !g_dry_run) {
       const int per_sm = bulk_prepare<T>(n);
       int dev = 0, sms = 0;
@@ -1157,6 +1213,8 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
     const std::string v(sk);
     ctx->step_kernel = v == "bulk" ? 1 : (v == "plain" ? 2 : 0);
   }
+  ctx->map_cells = p->stream_mode == OCTLB_STREAM_LINKS ? 1 : 2;
+  if (const char* mc = std::getenv("OCTLB_MAP_CELLS")) ctx->map_cells = mc[0] == '1' ? 1 : 2;
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "cudaStreamCreate"); *out = ctx.release(); return rc; }
   ctx->own_stream = true;

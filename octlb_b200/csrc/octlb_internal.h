@@ -34,6 +34,7 @@ struct StepArgs {
   const int* hmap;          // [(n+2)^3] padded position -> halo index (-1 in the core)
   const int* hpos;          // [n_halo] halo index -> padded linear position
   const int* open_pages;    // [n_open][4] torus-streamed halo items: page, block, halo index, population
+  const int* slot_map;      // [nblk][(n+2)^3] slot of every padded position (k_step_map levels)
   int n_open, n_halo;       // items, halo slots per page
   int nblk, n, np;          // np = n + 2
   long long halo_base;      // first halo-page slot (= nblk * n^3)

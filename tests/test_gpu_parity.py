@@ -221,6 +221,34 @@ def test_amr_cavity_fp16_fields(ob, ref):
     assert rel(rho_g, rho_r) <= 5e-3
 
 
+@pytest.mark.parametrize("case", ["cylinder_fp32", "cylinder_fp16", "cavity_band_fp16"])
+def test_forest_map_step_bitwise_equals_plain(ob, case, monkeypatch):
+    """On forest levels the slot-map step (one CTA per block, the block's
+    padded-position -> slot map in shared memory, one or two cells per
+    thread) and the one-cell-per-thread k_step give identical populations
+    and forces: same pulls, same arithmetic."""
+    from octlb_b200 import cases
+    p = ob.FP16_SHIFTED if case.endswith("fp16") else ob.FP32
+    if case.startswith("cylinder"):
+        mesh, init, info = small_cylinder(ob)
+        kw = dict(stream_mode=ob.STREAM_LINKS, drag=True)
+    else:
+        mesh, init, info = cases.cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=8)
+        kw = {}
+    res = []
+    for variant, cells in (("map", "2"), ("map", "1"), ("plain", "2")):
+        monkeypatch.setenv("OCTLB_STEP_KERNEL", variant)
+        monkeypatch.setenv("OCTLB_MAP_CELLS", cells)
+        lat = ob.GpuLattice(mesh, info["omega"], precision=p, init_pops=init, **kw)
+        lat.advance(6)
+        res.append((lat.get_populations(), lat.force() if kw else None))
+        lat.close()
+    for r in res[1:]:
+        assert np.array_equal(res[0][0], r[0])
+        if kw:
+            assert np.array_equal(res[0][1], r[1])
+
+
 def test_graph_replay_bitwise_equals_direct_launches(ob, monkeypatch):
     """advance_one captured as CUDA graphs (one per buffer parity) gives the
     same populations, forces and counters as launching kernel by kernel."""
