@@ -112,47 +112,6 @@ __device__ __forceinline__ void source_slots(const StepArgs& a, const Cell& c, l
   }
 }
 
-// Per-cell link rule (block_lattice.cpp:613-672) for a cell flagged kFlagNear:
-// pulled[i] holds g_i at the source slot s[i] (already loaded).
-template <typename T>
-__device__ __forceinline__ void apply_links(const StepArgs& a, const T* src, const Cell& c, long long t,
-                                            const long long (&s)[kQ], uint32_t halo_mask, uint8_t fl,
-                                            float (&f)[kQ]) {
-  const int kind = fl & kKindMask;
-  const int li = (fl & kFlagLink) ? a.link_idx[t] : -1;
-  float own[kQ];
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) own[i] = LD(src, a.qs, i, t, a.inv_scale);
-  uint8_t sk[kQ];
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) sk[i] = (halo_mask >> i) & 1u ? kBulk : (a.flags[s[i]] & kKindMask);
-#pragma unroll
-  for (int i = 1; i < kQ; ++i) {
-    const bool halo = (halo_mask >> i) & 1u;
-    if (reflects_on_pull(kind) && halo) {
-      f[i] = own[opp(i)];
-      continue;
-    }
-    if (sk[i] == kSolid || sk[i] == kBouzidi) {
-      float v = own[opp(i)];
-      if (li >= 0) {
-        const float q = a.link_rec[li * 38 + i];
-        if (q < 1.0f) {
-          // neighbour x + c_i: in-core cell or a halo position (kind kBulk)
-          bool nhalo;
-          const long long nb = resolve(a, c.b, static_cast<int>(c.x) + 1 + cx(i), static_cast<int>(c.y) + 1 + cy(i),
-                                       static_cast<int>(c.z) + 1 + cz(i), nhalo);
-          const int nk = nhalo ? kBulk : (a.flags[nb] & kKindMask);
-          const float f_q = nk == kBulk ? LD(src, a.qs, i, nb, a.inv_scale) : own[i];
-          v = bouzidi(own[opp(i)], f_q, own[i], q);
-        }
-        v += a.link_rec[li * 38 + kQ + i];
-      }
-      f[i] = v;
-    }
-  }
-}
-
 // Torus-streamed halo population of an open block (block_lattice.h:70-89):
 // item k = (page, block, halo index, population); no collision; the source
 // resolves like a core pull (own core, the neighbour core the exchange
@@ -233,26 +192,36 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
   rotate_item<T>(a, t - core_end);
 }
 
-// Cells flagged kFlagNear (links stream rule): the per-cell link rule, then
-// the same save / collide / store as k_step.  A separate launch keeps the
-// register-heavy rule out of the bulk kernel.
+// Cells flagged kFlagNear (links stream rule): the per-cell link rule of
+// block_lattice.cpp:613-672 with every table lookup done on the host --
+// direction i reads population i at nt.slot[i] and, where the rule applies,
+// reflects own[opp(i)] (half-way bounce-back, reflect-on-pull at the block
+// edge) or interpolates with Bouzidi (bouzidi_pull.h:8-26), then adds the
+// moving-wall term.  Then the same save / collide / store as k_step.
+constexpr int kNearThreads = 64;
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_step_near(const StepArgs a, const int* cells, int ncells) {
-  const int k = blockIdx.x * kThreads + threadIdx.x;
-  if (k >= ncells) return;
+__global__ void __launch_bounds__(kNearThreads) k_step_near(const StepArgs a, const NearTables nt) {
+  const int k = blockIdx.x * kNearThreads + threadIdx.x;
+  if (k >= nt.n) return;
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
-  const long long t = cells[k];
-  const Cell c = cell_of(a, static_cast<uint32_t>(t));
-  const long long tl = t - static_cast<long long>(c.b) * a.n * a.n * a.n;
+  const uint32_t t = static_cast<uint32_t>(nt.cells[k]);
+  const uint32_t mask = nt.mask[k];
   const uint8_t fl = a.flags[t];
-  long long s[kQ];
-  uint32_t halo_mask;
-  source_slots(a, c, t, tl, nullptr, s, halo_mask);
-  float f[kQ];
+  float f[kQ], own[kQ];
 #pragma unroll
-  for (int i = 0; i < kQ; ++i) f[i] = LD(src, a.qs, i, s[i], a.inv_scale);
-  apply_links<T>(a, src, c, t, s, halo_mask, fl, f);
+  for (int i = 0; i < kQ; ++i) {
+    f[i] = LD(src, a.qs, i, nt.slot[i * nt.n + k], a.inv_scale);
+    own[i] = LD(src, a.qs, i, t, a.inv_scale);
+  }
+#pragma unroll
+  for (int i = 1; i < kQ; ++i) {
+    if ((mask >> i) & 1u) {
+      const float q = nt.q[i * nt.n + k];
+      const float v = q < 1.0f ? bouzidi(own[opp(i)], f[i], own[i], q) : own[opp(i)];
+      f[i] = v + nt.add[i * nt.n + k];
+    }
+  }
   if (fl & kFlagSave) {
     float* sv = a.save_buf + static_cast<long long>(a.save_idx[t]) * kQ;
 #pragma unroll
@@ -766,9 +735,9 @@ cudaError_t launch_step_map(const StepArgs& a, bool links, bool flags, int cpt, 
 }
 
 template <typename T>
-cudaError_t launch_step_near(const StepArgs& a, const int* cells, int ncells, cudaStream_t s) {
-  if (ncells == 0) return cudaSuccess;
-  k_step_near<T><<<grid_for(static_cast<uint32_t>(ncells)), kThreads, 0, s>>>(a, cells, ncells);
+cudaError_t launch_step_near(const StepArgs& a, const NearTables& nt, cudaStream_t s) {
+  if (nt.n == 0) return cudaSuccess;
+  k_step_near<T><<<(nt.n + kNearThreads - 1) / kNearThreads, kNearThreads, 0, s>>>(a, nt);
   return cudaGetLastError();
 }
 
@@ -849,7 +818,7 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
 #define OCTLB_INST(T)                                                                              \
   template cudaError_t launch_step<T>(const StepArgs&, bool, bool, bool, cudaStream_t);            \
   template cudaError_t launch_step_pair<T>(const StepArgs&, cudaStream_t);                         \
-  template cudaError_t launch_step_near<T>(const StepArgs&, const int*, int, cudaStream_t);         \
+  template cudaError_t launch_step_near<T>(const StepArgs&, const NearTables&, cudaStream_t);       \
   template cudaError_t launch_step_map<T>(const StepArgs&, bool, bool, int, cudaStream_t);         \
   template cudaError_t launch_ghost<T>(T*, long long, const CopyDesc*, const uint32_t*, int,       \
                                        uint32_t, const BBOp*, uint32_t, float, float, cudaStream_t); \

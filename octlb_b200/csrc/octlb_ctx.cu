@@ -37,7 +37,7 @@ template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*,
 template <typename T> cudaError_t launch_step_bulk(const StepArgs&, int, cudaStream_t);
 template <typename T> int bulk_prepare(int n);
 template <typename T> cudaError_t launch_step_pair(const StepArgs&, cudaStream_t);
-template <typename T> cudaError_t launch_step_near(const StepArgs&, const int*, int, cudaStream_t);
+template <typename T> cudaError_t launch_step_near(const StepArgs&, const NearTables&, cudaStream_t);
 template <typename T> cudaError_t launch_step_map(const StepArgs&, bool, bool, int, cudaStream_t);
 bool pair_step_eligible(int n);
 bool map_step_eligible(int n, long long nslots);
@@ -91,6 +91,8 @@ struct Level {
   int cur = 0;
   DevBuf flags, link_idx, link_rec, save_idx, save_buf;
   DevBuf nbase, page_of, hmap, hpos, open_pages, near_cells, slot_map;
+  DevBuf near_mask, near_slot, near_q, near_add;
+  NearTables near{};
   int n_near = 0;
   int n_open = 0, n_halo = 0, n_pages = 0, n_save = 0, n_links = 0;
   bool has_flags = false;
@@ -236,11 +238,11 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     CK(launch_step_pair<T>(a, ctx->stream));
   } else if (L.use_map) {
     CK(launch_step_map<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags, ctx->map_cells, ctx->stream));
-    CK(launch_step_near<T>(a, L.near_cells.as<int>(), L.n_near, ctx->stream));
+    CK(launch_step_near<T>(a, L.near, ctx->stream));
   } else {
     CK(launch_step<T>(a, ctx->periodic != 0, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags,
                       ctx->stream));
-    CK(launch_step_near<T>(a, L.near_cells.as<int>(), L.n_near, ctx->stream));
+    CK(launch_step_near<T>(a, L.near, ctx->stream));
   }
   // The force after advance_one reads each level's last step (the reference
   // computes MomentumExchangeDrag once, after advance_one): skip the others.
@@ -792,6 +794,16 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     // corners, and halo positions of closed blocks no table covers) point at
     // the block's first core slot and must never be pulled: checked below
     // for every cell the step kernel streams.
+    auto resolve_slot = [&](int lb, int X, int Y, int Z) -> long long {
+      const int P = (X * np + Y) * np + Z;
+      const long long lin = (static_cast<long long>(X - 1) * n + (Y - 1)) * n + (Z - 1);
+      const int d = dir27(X, Y, Z);
+      if (d == 13) return static_cast<long long>(lb) * n3 + lin;
+      const long long b0 = nbase[static_cast<size_t>(lb) * 27 + d];
+      if (b0 != kOwnPage) return b0 + lin;
+      if (page_of[lb] >= 0) return ncore + static_cast<long long>(page_of[lb]) * H + hmap[P];
+      return -1;
+    };
     std::vector<int> slot_map;
     if (map_step_eligible(n, L.nslots) && !(ctx->periodic && !L.has_flags)) {
       slot_map.assign(static_cast<size_t>(L.nblk) * np3, 0);
@@ -802,12 +814,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
           for (int Y = 0; Y < np; ++Y)
             for (int Z = 0; Z < np; ++Z) {
               const int P = (X * np + Y) * np + Z;
-              const long long lin = (static_cast<long long>(X - 1) * n + (Y - 1)) * n + (Z - 1);
-              const int d = dir27(X, Y, Z);
-              long long sl = -1;
-              if (d == 13) sl = static_cast<long long>(lb) * n3 + lin;
-              else if (nbase[static_cast<size_t>(lb) * 27 + d] != kOwnPage) sl = nbase[static_cast<size_t>(lb) * 27 + d] + lin;
-              else if (page_of[lb] >= 0) sl = ncore + static_cast<long long>(page_of[lb]) * H + hmap[P];
+              const long long sl = resolve_slot(lb, X, Y, Z);
               unresolved[P] = sl < 0;
               if (sl >= L.nslots) return fail(ctx, OCTLB_EINVAL, "internal: slot map out of range");
               m[P] = sl < 0 ? static_cast<int>(static_cast<long long>(lb) * n3) : static_cast<int>(sl);
@@ -821,6 +828,52 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
                 if (unresolved[((x + 1 - cx(i)) * np + (y + 1 - cy(i))) * np + (z + 1 - cz(i))])
                   return fail(ctx, OCTLB_EINVAL, "internal: pulled halo position without a source");
             }
+      }
+    }
+
+    // Link rule of the near cells (block_lattice.cpp:613-672), resolved per
+    // direction: pull source, reflect-on-pull at a reflecting kind's block
+    // edge, half-way bounce-back or Bouzidi on a solid / Bouzidi source.
+    std::vector<uint32_t> nmask(near_cells.size(), 0);
+    std::vector<int> nslot(near_cells.size() * kQ);
+    std::vector<float> nq(near_cells.size() * kQ, 1.f), nadd(near_cells.size() * kQ, -0.f);
+    {
+      const size_t nn = near_cells.size();
+      for (size_t k = 0; k < nn; ++k) {
+        const long long tc = near_cells[k];
+        const int lb = static_cast<int>(tc / n3);
+        const int r = static_cast<int>(tc % n3), x = r / (n * n), y = (r / n) % n, z = r % n;
+        const int kind = flags[tc] & kKindMask;
+        const int li = (flags[tc] & kFlagLink) ? lidx[tc] : -1;
+        for (int i = 0; i < kQ; ++i) {
+          const int X = x + 1 - cx(i), Y = y + 1 - cy(i), Z = z + 1 - cz(i);
+          const bool halo = X < 1 || Y < 1 || Z < 1 || X > n || Y > n || Z > n;
+          long long sl = resolve_slot(lb, X, Y, Z);
+          if (sl < 0) return fail(ctx, OCTLB_EINVAL, "internal: pulled halo position without a source");
+          const int sk = halo ? kBulk : (flags[sl] & kKindMask);
+          if (i > 0 && reflects_on_pull(kind) && halo) {
+            nmask[k] |= 1u << i;  // own[opp(i)], nothing added
+          } else if (i > 0 && (sk == kSolid || sk == kBouzidi)) {
+            nmask[k] |= 1u << i;
+            if (li >= 0) {
+              const float q = lrec[static_cast<size_t>(li) * 38 + i];
+              nq[i * nn + k] = q;
+              nadd[i * nn + k] = lrec[static_cast<size_t>(li) * 38 + kQ + i];
+              if (q < 1.0f) {
+                // f_q: population i of x + c_i when that cell is kBulk (a halo
+                // position counts as kBulk), else the cell's own
+                const int Xn = x + 1 + cx(i), Yn = y + 1 + cy(i), Zn = z + 1 + cz(i);
+                const bool nh = Xn < 1 || Yn < 1 || Zn < 1 || Xn > n || Yn > n || Zn > n;
+                const long long nbs = resolve_slot(lb, Xn, Yn, Zn);
+                if (nbs < 0) return fail(ctx, OCTLB_EINVAL, "internal: Bouzidi neighbour without a source");
+                const int nk = nh ? kBulk : (flags[nbs] & kKindMask);
+                sl = nk == kBulk ? nbs : tc;
+              }
+            }
+          }
+          if (sl >= (1LL << 31)) return fail(ctx, OCTLB_EINVAL, "level has more than 2^31 slots");
+          nslot[i * nn + k] = static_cast<int>(sl);
+        }
       }
     }
 
@@ -910,6 +963,12 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     CK(upload(L.hpos, hpos));
     CK(upload(L.open_pages, open_pages));
     CK(upload(L.near_cells, near_cells));
+    CK(upload(L.near_mask, nmask));
+    CK(upload(L.near_slot, nslot));
+    CK(upload(L.near_q, nq));
+    CK(upload(L.near_add, nadd));
+    L.near = NearTables{L.near_cells.as<int>(), L.near_mask.as<uint32_t>(), L.near_slot.as<int>(),
+                        L.near_q.as<float>(), L.near_add.as<float>(), L.n_near};
     CK(upload(L.bb_ops, bbv));
     CK(upload(L.prolong_items, prolong[l]));
     CK(upload(L.restrict_items, restrict_items[l]));

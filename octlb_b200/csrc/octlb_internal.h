@@ -47,6 +47,21 @@ struct StepArgs {
   int* err;                 // device error word (bounded waits that gave up)
 };
 
+// Cells flagged kFlagNear with the link rule resolved on the host: for near
+// cell k and direction i (arrays [kQ][n]), the slot whose population i the
+// rule reads (the pull source, the Bouzidi neighbour x + c_i, or the cell
+// itself), and for directions set in mask[k] the link coefficients q (1 =
+// half-way bounce-back) and the added moving-wall term (-0 when the cell has
+// no link record: an exact no-op).
+struct NearTables {
+  const int* cells;         // [n] core slot
+  const uint32_t* mask;     // [n] bit i: direction i takes the link rule
+  const int* slot;          // [kQ][n]
+  const float* q;           // [kQ][n]
+  const float* add;         // [kQ][n]
+  int n;
+};
+
 constexpr long long kOwnPage = -(1LL << 62);
 
 // Device error codes written to StepArgs::err.
