@@ -74,6 +74,13 @@ struct FastDiv {
 };
 
 // Population element access for the two storage types.
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// stream-serialisation attribute may begin while its predecessor in the
+// stream is still finishing: it runs what reads only constant tables, then
+// waits for the predecessor's completion and memory before touching anything
+// a predecessor writes.  A no-op for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <typename T> struct Store;
 template <> struct Store<float> {
   __device__ static inline float ld(const float* p, float) { return *p; }

@@ -137,6 +137,7 @@ __device__ __forceinline__ void rotate_item(const StepArgs& a, uint32_t k) {
 
 template <typename T, bool LINKS, bool FLAGS, bool BLOCKED>
 __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
+  pdl_wait();
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
@@ -208,10 +209,14 @@ __global__ void __launch_bounds__(kNearThreads) k_step_near(const StepArgs a, co
   const uint32_t t = static_cast<uint32_t>(nt.cells[k]);
   const uint32_t mask = nt.mask[k];
   const uint8_t fl = a.flags[t];
+  int sl[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) sl[i] = nt.slot[i * nt.n + k];
+  pdl_wait();
   float f[kQ], own[kQ];
 #pragma unroll
   for (int i = 0; i < kQ; ++i) {
-    f[i] = LD(src, a.qs, i, nt.slot[i * nt.n + k], a.inv_scale);
+    f[i] = LD(src, a.qs, i, sl[i], a.inv_scale);
     own[i] = LD(src, a.qs, i, t, a.inv_scale);
   }
 #pragma unroll
@@ -300,6 +305,7 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
   extern __shared__ int smap[];  // (n+2)^3 slots of this block
   const uint32_t b = blockIdx.x;
   if (b >= static_cast<uint32_t>(a.nblk)) {
+    pdl_wait();
     rotate_item<T>(a, (b - a.nblk) * kThreads + threadIdx.x);
     return;
   }
@@ -307,6 +313,7 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
   const int* gm = a.slot_map + static_cast<long long>(b) * np3;
   for (int k = threadIdx.x; k < np3; k += kThreads) smap[k] = gm[k];
   __syncthreads();
+  pdl_wait();
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
   const uint32_t n = a.n, n3 = n * n * n, qs = static_cast<uint32_t>(a.qs);
@@ -342,6 +349,7 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
 // of +-1 takes the two aligned pairs around it.  Same arithmetic as k_step.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_step_pair(const StepArgs a) {
+  pdl_wait();
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   const uint32_t n = a.n, half = n >> 1;
   if (t >= a.ncore / 2) return;
@@ -390,6 +398,7 @@ k_ghost(T* pops, long long qs, const CopyDesc* cd, const uint32_t* cd_start, int
         uint32_t ncopy, const BBOp* bb, uint32_t nbb, float scale, float inv_scale) {
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   if (t < ncopy) {
+    pdl_wait();
     int lo = 0, hi = ncd - 1;
     while (lo < hi) {  // last descriptor whose start <= t
       const int mid = (lo + hi + 1) >> 1;
@@ -407,6 +416,7 @@ k_ghost(T* pops, long long qs, const CopyDesc* cd, const uint32_t* cd_start, int
   const uint32_t u = t - ncopy;
   if (u >= nbb) return;
   const BBOp op = bb[u];
+  pdl_wait();
   const float v = Store<T>::ld(pops + op.src_pop * qs + op.src, inv_scale) + op.add;
   Store<T>::st(pops + op.pop * qs + op.dst, v, scale);
 }
@@ -446,13 +456,15 @@ __device__ inline void write_macro_cell(const Macro& m, float s, int kind, float
   if (kind == kBulk) bgk(f, omega);
 }
 
+constexpr int kProlongThreads = 64;  // few items: spread them over more SMs
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kProlongThreads)
 k_prolong(const ProlongItem* items, int nitems, const float* coarse_save, float* prev, int half,
           T* fine, long long fine_qs, float scale, float omega, float fscale) {
-  const int t = blockIdx.x * kThreads + threadIdx.x;
+  const int t = blockIdx.x * kProlongThreads + threadIdx.x;
   if (t >= nitems) return;
   const ProlongItem it = items[t];
+  pdl_wait();
   Macro m;
   read_macro(coarse_save + static_cast<long long>(it.coarse_save) * kQ, m);
   float* pv = prev + static_cast<long long>(it.prev) * 23;
@@ -488,6 +500,7 @@ k_restrict(const RestrictItem* items, int nitems, const float* fine_save, T* coa
   if (w >= nitems) return;
   const RestrictItem& it = items[w];
   const int row = lane == 0 ? it.fine_save : (lane <= it.nnb ? it.nb_save[lane - 1] : -1);
+  pdl_wait();
   Macro m;
   if (row >= 0) read_macro(fine_save + static_cast<long long>(row) * kQ, m);
   float sum[kQ];
@@ -545,6 +558,7 @@ __device__ inline void block_reduce(double (&v)[N]) {
 template <typename T, bool LINKS>
 __global__ void __launch_bounds__(kThreads)
 k_drag(const StepArgs a, const DragItem* items, int nitems, double* partial) {
+  pdl_wait();
   const int t = blockIdx.x * kThreads + threadIdx.x;
   double acc[3] = {0.0, 0.0, 0.0};
   if (t < nitems) {
@@ -594,6 +608,7 @@ k_drag(const StepArgs a, const DragItem* items, int nitems, double* partial) {
 // per-thread sums then a fixed shuffle tree (deterministic).
 __global__ void __launch_bounds__(kThreads)
 k_sum_partials(const double* partial, int nparts, int width, double* out, double* accum) {
+  pdl_wait();
   for (int k = 0; k < width; ++k) {
     double v[1] = {0.0};
     for (int p = threadIdx.x; p < nparts; p += kThreads) v[0] += partial[p * width + k];
@@ -685,11 +700,37 @@ k_scatter(const StepArgs a, const double* in) {
 
 inline uint32_t grid_for(uint32_t items) { return (items + kThreads - 1) / kThreads; }
 
+// Launches of the time-step chain: with the programmatic stream-serialisation
+// attribute when enabled, so each kernel is launched as its predecessor's
+// CTAs exit and runs its constant-table prologue before pdl_wait (every such
+// kernel calls pdl_wait before its first dependent access).  No kernel
+// triggers its dependents early: measured on the forest cases, an early
+// trigger gained nothing over the implicit trigger at CTA exit.
+thread_local bool g_programmatic = false;
+template <typename... P, typename... A>
+cudaError_t launch_chain(void (*k)(P...), dim3 g, dim3 b, size_t smem, cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = g;
+  cfg.blockDim = b;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = g_programmatic ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
+// Programmatic launches for the time-step chain on this host thread.
+void set_programmatic_launch(bool on) { g_programmatic = on; }
+
 template <typename T>
 cudaError_t launch_step(const StepArgs& a, bool periodic, bool links, bool flags, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
   (void)periodic;
   if (a.nitems == 0) return cudaSuccess;
   // CTAs aligned to blocks: core cells first (a multiple of the CTA size),
@@ -700,15 +741,15 @@ cudaError_t launch_step(const StepArgs& a, bool periodic, bool links, bool flags
   const dim3 g(core_ctas + grid_for(a.nitems - a.ncore));
   StepArgs b = a;
   if (blocked) {
-    if (links) k_step<T, true, true, true><<<g, kThreads, 0, s>>>(b);
-    else if (flags) k_step<T, false, true, true><<<g, kThreads, 0, s>>>(b);
-    else k_step<T, false, false, true><<<g, kThreads, 0, s>>>(b);
+    if (links) e = launch_chain(k_step<T, true, true, true>, dim3(g), dim3(kThreads), 0, s, b);
+    else if (flags) e = launch_chain(k_step<T, false, true, true>, dim3(g), dim3(kThreads), 0, s, b);
+    else e = launch_chain(k_step<T, false, false, true>, dim3(g), dim3(kThreads), 0, s, b);
   } else {
-    if (links) k_step<T, true, true, false><<<g, kThreads, 0, s>>>(b);
-    else if (flags) k_step<T, false, true, false><<<g, kThreads, 0, s>>>(b);
-    else k_step<T, false, false, false><<<g, kThreads, 0, s>>>(b);
+    if (links) e = launch_chain(k_step<T, true, true, false>, dim3(g), dim3(kThreads), 0, s, b);
+    else if (flags) e = launch_chain(k_step<T, false, true, false>, dim3(g), dim3(kThreads), 0, s, b);
+    else e = launch_chain(k_step<T, false, false, false>, dim3(g), dim3(kThreads), 0, s, b);
   }
-  return cudaGetLastError();
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 // Slot-map step: a CTA of 256 threads per block (n^3 a multiple of 512, the
@@ -719,32 +760,33 @@ bool map_step_eligible(int n, long long nslots) {
 }
 template <typename T>
 cudaError_t launch_step_map(const StepArgs& a, bool links, bool flags, int cpt, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
   if (a.nitems == 0) return cudaSuccess;
   const dim3 g(static_cast<uint32_t>(a.nblk) + grid_for(static_cast<uint32_t>(a.n_open)));
   const size_t smem = static_cast<size_t>(a.np) * a.np * a.np * sizeof(int);
   if (cpt == 2) {
-    if (links) k_step_map<T, true, true, 2><<<g, kThreads, smem, s>>>(a);
-    else if (flags) k_step_map<T, false, true, 2><<<g, kThreads, smem, s>>>(a);
-    else k_step_map<T, false, false, 2><<<g, kThreads, smem, s>>>(a);
+    if (links) e = launch_chain(k_step_map<T, true, true, 2>, dim3(g), dim3(kThreads), smem, s, a);
+    else if (flags) e = launch_chain(k_step_map<T, false, true, 2>, dim3(g), dim3(kThreads), smem, s, a);
+    else e = launch_chain(k_step_map<T, false, false, 2>, dim3(g), dim3(kThreads), smem, s, a);
   } else {
-    if (links) k_step_map<T, true, true, 1><<<g, kThreads, smem, s>>>(a);
-    else if (flags) k_step_map<T, false, true, 1><<<g, kThreads, smem, s>>>(a);
-    else k_step_map<T, false, false, 1><<<g, kThreads, smem, s>>>(a);
+    if (links) e = launch_chain(k_step_map<T, true, true, 1>, dim3(g), dim3(kThreads), smem, s, a);
+    else if (flags) e = launch_chain(k_step_map<T, false, true, 1>, dim3(g), dim3(kThreads), smem, s, a);
+    else e = launch_chain(k_step_map<T, false, false, 1>, dim3(g), dim3(kThreads), smem, s, a);
   }
-  return cudaGetLastError();
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_step_near(const StepArgs& a, const NearTables& nt, cudaStream_t s) {
   if (nt.n == 0) return cudaSuccess;
-  k_step_near<T><<<(nt.n + kNearThreads - 1) / kNearThreads, kNearThreads, 0, s>>>(a, nt);
-  return cudaGetLastError();
+  const cudaError_t e = launch_chain(k_step_near<T>, dim3((nt.n + kNearThreads - 1) / kNearThreads), dim3(kNearThreads), 0, s, a, nt);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_step_pair(const StepArgs& a, cudaStream_t s) {
-  k_step_pair<T><<<grid_for(a.ncore / 2), kThreads, 0, s>>>(a);
-  return cudaGetLastError();
+  const cudaError_t e = launch_chain(k_step_pair<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 // Paired kernel: even n (aligned pairs), n^3 < 2^31.
 bool pair_step_eligible(int n) { return n >= 4 && (n % 2) == 0 && n <= 1024; }
@@ -755,9 +797,9 @@ cudaError_t launch_ghost(T* pops, long long qs, const CopyDesc* cd, const uint32
                          cudaStream_t s) {
   const uint32_t total = ncopy + nbb;
   if (total == 0) return cudaSuccess;
-  k_ghost<T><<<grid_for(total), kThreads, 0, s>>>(pops, qs, cd, cd_start, ncd, ncopy, bb, nbb, scale,
+  const cudaError_t e = launch_chain(k_ghost<T>, dim3(grid_for(total)), dim3(kThreads), 0, s, pops, qs, cd, cd_start, ncd, ncopy, bb, nbb, scale,
                                                   inv_scale);
-  return cudaGetLastError();
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <typename T>
@@ -765,9 +807,9 @@ cudaError_t launch_prolong(const ProlongItem* items, int n, const float* coarse_
                            int half, T* fine, long long fine_qs, float scale, float omega,
                            float fscale, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_prolong<T><<<grid_for(n), kThreads, 0, s>>>(items, n, coarse_save, prev, half, fine, fine_qs,
+  const cudaError_t e = launch_chain(k_prolong<T>, dim3((n + kProlongThreads - 1) / kProlongThreads), dim3(kProlongThreads), 0, s, items, n, coarse_save, prev, half, fine, fine_qs,
                                                 scale, omega, fscale);
-  return cudaGetLastError();
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <typename T>
@@ -775,23 +817,24 @@ cudaError_t launch_restrict(const RestrictItem* items, int n, const float* fine_
                             long long coarse_qs, float scale, float omega, float cscale,
                             cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_restrict<T><<<grid_for(static_cast<uint32_t>(n) * 32), kThreads, 0, s>>>(items, n, fine_save, coarse,
+  const cudaError_t e = launch_chain(k_restrict<T>, dim3(grid_for(static_cast<uint32_t>(n) * 32)), dim3(kThreads), 0, s, items, n, fine_save, coarse,
                                                                              coarse_qs, scale, omega, cscale);
-  return cudaGetLastError();
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_drag(const StepArgs& a, bool links, const DragItem* items, int n, double* partial,
                         cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
   const uint32_t g = grid_for(static_cast<uint32_t>(n > 0 ? n : 1));
-  if (links) k_drag<T, true><<<g, kThreads, 0, s>>>(a, items, n, partial);
-  else k_drag<T, false><<<g, kThreads, 0, s>>>(a, items, n, partial);
-  return cudaGetLastError();
+  if (links) e = launch_chain(k_drag<T, true>, dim3(g), dim3(kThreads), 0, s, a, items, n, partial);
+  else e = launch_chain(k_drag<T, false>, dim3(g), dim3(kThreads), 0, s, a, items, n, partial);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 // Force = fixed-order sum of every level's drag partials; accum += force.
 cudaError_t launch_drag_total(const double* partial, int nparts, double* out, double* accum, cudaStream_t s) {
-  k_sum_partials<<<1, kThreads, 0, s>>>(partial, nparts, 3, out, accum);
-  return cudaGetLastError();
+  const cudaError_t e = launch_chain(k_sum_partials, dim3(1), dim3(kThreads), 0, s, partial, nparts, 3, out, accum);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 uint32_t drag_partials(int n) { return grid_for(static_cast<uint32_t>(n > 0 ? n : 1)); }
 

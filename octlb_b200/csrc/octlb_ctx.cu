@@ -41,6 +41,7 @@ template <typename T> cudaError_t launch_step_near(const StepArgs&, const NearTa
 template <typename T> cudaError_t launch_step_map(const StepArgs&, bool, bool, int, cudaStream_t);
 bool pair_step_eligible(int n);
 bool map_step_eligible(int n, long long nslots);
+void set_programmatic_launch(bool on);
 bool bulk_step_eligible(int n, int elem_bytes);
 uint32_t drag_partials(int n);
 uint32_t audit_partials(const StepArgs& a);
@@ -147,6 +148,7 @@ struct octlb_ctx {
   };
   std::map<uint64_t, GraphEntry> graphs;
   bool use_graphs = true;           // OCTLB_NO_GRAPH=1 launches kernel by kernel
+  bool use_pdl = true;              // OCTLB_NO_PDL=1: plain stream order between the step's kernels
   float prolong_scale = 0.f, restrict_scale = 0.f;
 };
 
@@ -1112,8 +1114,15 @@ uint64_t parity_mask(const octlb_ctx* ctx) {
   return m;
 }
 
+// Programmatic launches for the duration of one advance call on this thread.
+struct ProgrammaticScope {
+  explicit ProgrammaticScope(bool on) { set_programmatic_launch(on); }
+  ~ProgrammaticScope() { set_programmatic_launch(false); }
+};
+
 template <typename T>
 int advance_impl(octlb_ctx* ctx, int steps) {
+  const ProgrammaticScope pdl(ctx->use_pdl);
   for (int s = 0; s < steps; ++s) {
     if (!ctx->use_graphs) {
       int rc = advance_one_launches<T>(ctx);
@@ -1268,6 +1277,7 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
   ctx->drag = p->drag;
   ctx->omega = p->omega;
   if (const char* ng = std::getenv("OCTLB_NO_GRAPH")) ctx->use_graphs = ng[0] != '1';
+  if (const char* np = std::getenv("OCTLB_NO_PDL")) ctx->use_pdl = np[0] != '1';
   if (const char* sk = std::getenv("OCTLB_STEP_KERNEL")) {
     const std::string v(sk);
     ctx->step_kernel = v == "bulk" ? 1 : (v == "plain" ? 2 : 0);

@@ -249,21 +249,32 @@ def test_forest_map_step_bitwise_equals_plain(ob, case, monkeypatch):
             assert np.array_equal(res[0][1], r[1])
 
 
-def test_graph_replay_bitwise_equals_direct_launches(ob, monkeypatch):
-    """advance_one captured as CUDA graphs (one per buffer parity) gives the
-    same populations, forces and counters as launching kernel by kernel."""
-    mesh, init, info = small_cylinder(ob)
+@pytest.mark.parametrize("case", ["cylinder", "cavity_band"])
+def test_graph_and_programmatic_launch_bitwise_equal(ob, case, monkeypatch):
+    """advance_one captured as CUDA graphs (one per buffer parity), launched
+    kernel by kernel, and either way with or without programmatic dependent
+    launches gives the same populations, forces and counters."""
+    from octlb_b200 import cases
+    if case == "cylinder":
+        mesh, init, info = small_cylinder(ob)
+        kw = dict(stream_mode=ob.STREAM_LINKS, drag=True)
+    else:
+        mesh, init, info = cases.cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=8)
+        kw = {}
     res = []
-    for ng in ("0", "1"):
+    for ng, npdl in (("0", "0"), ("1", "0"), ("0", "1"), ("1", "1")):
         monkeypatch.setenv("OCTLB_NO_GRAPH", ng)
-        lat = ob.GpuLattice(mesh, info["omega"], stream_mode=ob.STREAM_LINKS, drag=True, init_pops=init)
+        monkeypatch.setenv("OCTLB_NO_PDL", npdl)
+        lat = ob.GpuLattice(mesh, info["omega"], init_pops=init, **kw)
         forces = []
         for _ in range(5):
             lat.advance(1)
-            forces.append(lat.force())
+            forces.append(lat.force() if kw else np.zeros(3))
         lat.advance(4)
-        res.append((lat.get_populations(), np.array(forces), lat.counters(), lat.force_sum()))
+        res.append((lat.get_populations(), np.array(forces), lat.counters(),
+                    lat.force_sum() if kw else (np.zeros(3), 9)))
         lat.close()
-    (p0, f0, c0, s0), (p1, f1, c1, s1) = res
-    assert np.array_equal(p0, p1) and np.array_equal(f0, f1) and c0 == c1
-    assert np.array_equal(s0[0], s1[0]) and s0[1] == s1[1] == 9
+    p0, f0, c0, s0 = res[0]
+    for p1, f1, c1, s1 in res[1:]:
+        assert np.array_equal(p0, p1) and np.array_equal(f0, f1) and c0 == c1
+        assert np.array_equal(s0[0], s1[0]) and s0[1] == s1[1] == 9
