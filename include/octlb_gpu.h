@@ -112,6 +112,35 @@ int octlb_gpu_set_stream(octlb_ctx* ctx, void* cuda_stream);
 int octlb_gpu_advance(octlb_ctx* ctx, int n_coarse_steps);
 int octlb_gpu_synchronize(octlb_ctx* ctx);
 
+/* Body force F per core cell, [n_blocks][n^3][3] doubles (stored as FP32),
+ * or NULL to remove it: the forcing term 3 w_i (c_i . F) is added to the
+ * post-collision populations of every kBulk cell once per step of its level
+ * (no reference counterpart: the reference has no body force; this is the
+ * adjoint's per-cell control). */
+int octlb_gpu_set_body_force(octlb_ctx* ctx, const double* force);
+
+/* Discrete adjoint (reverse mode) of n coarse steps.  Objective J = the
+ * `component` of octlb_gpu_force averaged over the last `window` coarse
+ * steps.  Runs the forward from the context's current state with a
+ * checkpoint every `checkpoint_interval` coarse steps (0: ceil(sqrt(n))),
+ * then recomputes each segment from its checkpoint and runs the hand-written
+ * adjoint kernels through it in reverse.  Outputs J, grad[0] = dJ/du_max
+ * (u_max = the largest moving tree-boundary wall speed; all wall velocities
+ * scale with it), grad[1] = dJ/dtau (tau = 1/omega, including the coupler
+ * scales), and, when grad_force is not NULL, dJ/dF for the body force of
+ * every core cell ([n_blocks][n^3][3]; at the current force, zero if none).
+ * FP32 storage, drag enabled, slot-map levels (n a multiple of 8, <= 16).
+ * The context ends in the forward's final state (as after advance(n)).
+ * No reference counterpart: the reference has no adjoint. */
+typedef struct octlb_adj_params {
+  int coarse_steps;
+  int window;
+  int checkpoint_interval;
+  int component;
+} octlb_adj_params;
+int octlb_gpu_adjoint(octlb_ctx* ctx, const octlb_adj_params* params, double* objective, double grad[2],
+                      double* grad_force);
+
 /* Reference state f (post-stream, pre-collision) -> context; the next step
  * starts by colliding it. */
 int octlb_gpu_set_populations(octlb_ctx* ctx, const double* pops);

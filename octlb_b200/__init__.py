@@ -296,6 +296,26 @@ class GpuLattice:
         self._check(self._L.octlb_gpu_step_stats(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    def set_body_force(self, force=None):
+        """Body force [n_blocks][n^3][3] (or None to remove it)."""
+        f = None if force is None else np.ascontiguousarray(force, np.float64)
+        if f is not None and f.size != self._cells() * 3:
+            raise ValueError("body force must hold n_blocks * n^3 * 3 values")
+        self._check(self._L.octlb_gpu_set_body_force(self._h, capi.ptr(f, ctypes.c_double)))
+
+    def adjoint(self, coarse_steps, window, checkpoint_interval=0, component=0, force_grad=True):
+        """Run coarse_steps forward and the adjoint sweep back (octlb_gpu_adjoint).
+        Returns (J, dJ/du_max, dJ/dtau, dJ/dF or None) with J = mean force
+        component over the last `window` coarse steps."""
+        p = capi.AdjParams(int(coarse_steps), int(window), int(checkpoint_interval), int(component))
+        J = np.zeros(1)
+        g = np.zeros(2)
+        gF = np.zeros(self._cells() * 3) if force_grad else None
+        self._check(self._L.octlb_gpu_adjoint(self._h, ctypes.byref(p), capi.ptr(J, ctypes.c_double),
+                                              capi.ptr(g, ctypes.c_double), capi.ptr(gF, ctypes.c_double)))
+        n = self.mesh.n
+        return float(J[0]), float(g[0]), float(g[1]), (None if gF is None else gF.reshape(self.mesh.n_blocks, n ** 3, 3))
+
 
 class GpuTimeLoop:
     """Reference TimeLoop interface (time_loop.h:47-121) over a GpuLattice."""

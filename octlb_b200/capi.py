@@ -51,6 +51,12 @@ class Tables(ctypes.Structure):
     ]
 
 
+class AdjParams(ctypes.Structure):
+    """octlb_adj_params."""
+    _fields_ = [("coarse_steps", ctypes.c_int), ("window", ctypes.c_int),
+                ("checkpoint_interval", ctypes.c_int), ("component", ctypes.c_int)]
+
+
 class Params(ctypes.Structure):
     _fields_ = [
         ("omega", ctypes.c_double), ("precision", ctypes.c_int), ("stream_mode", ctypes.c_int),
@@ -77,6 +83,8 @@ def lib():
         "octlb_gpu_advance": (ctypes.c_int, [P, ctypes.c_int]),
         "octlb_gpu_synchronize": (ctypes.c_int, [P]),
         "octlb_gpu_set_populations": (ctypes.c_int, [P, F64P]),
+        "octlb_gpu_set_body_force": (ctypes.c_int, [P, F64P]),
+        "octlb_gpu_adjoint": (ctypes.c_int, [P, ctypes.POINTER(AdjParams), F64P, F64P, F64P]),
         "octlb_gpu_get_populations": (ctypes.c_int, [P, F64P]),
         "octlb_gpu_get_fields": (ctypes.c_int, [P, F64P, F64P]),
         "octlb_gpu_force": (ctypes.c_int, [P, F64P]),

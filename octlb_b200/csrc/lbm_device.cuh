@@ -1,0 +1,146 @@
+// Device helpers shared by the forward kernels (lbm_kernels.cu) and the
+// adjoint kernels (lbm_adjoint.cu): slot resolution of padded positions, the
+// Lagrava macro state, and a fixed-order FP64 block reduction.
+#ifndef OCTLB_LBM_DEVICE_CUH_
+#define OCTLB_LBM_DEVICE_CUH_
+
+#include "octlb_internal.h"
+
+namespace octlb_gpu {
+namespace {
+
+constexpr int kThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ float LD(const T* base, long long qs, int i, long long slot, float inv) {
+  return Store<T>::ld(base + i * qs + slot, inv);
+}
+
+// Core coordinates of core work item t (slot t).
+struct Cell {
+  uint32_t b, x, y, z;
+};
+__device__ __forceinline__ Cell cell_of(const StepArgs& a, uint32_t t) {
+  const uint32_t n = a.n;
+  Cell c;
+  c.b = a.div_n3.div(t);
+  uint32_t r = t - c.b * n * n * n;
+  c.x = a.div_n2.div(r);
+  r -= c.x * n * n;
+  c.y = a.div_n.div(r);
+  c.z = r - c.y * n;
+  return c;
+}
+
+// Own halo-page slot of padded position (X, Y, Z) of block b; positions that
+// no table covers are excluded by construction, the check keeps the access in
+// bounds and records an error if that ever fails.
+__device__ __forceinline__ long long page_slot(const StepArgs& a, uint32_t b, int X, int Y, int Z) {
+  const int pg = a.page_of[b];
+  const int h = a.hmap[(X * a.np + Y) * a.np + Z];
+  if (pg < 0 || h < 0) {
+    atomicExch(a.err, kErrHalo);
+    return static_cast<long long>(b) * a.n * a.n * a.n;
+  }
+  return a.halo_base + static_cast<long long>(pg) * a.n_halo + h;
+}
+
+// Slot holding padded position (X, Y, Z) in [0, n+1]^3 of block b: the own
+// core, the same-level neighbour's core cell the reference's exchange copies
+// into that halo position, or the block's own halo page.  in_halo reports a
+// position outside the core (the reference sees such sources as kBulk halo
+// cells, block_lattice.cpp:510-518).
+__device__ __forceinline__ long long resolve(const StepArgs& a, uint32_t b, int X, int Y, int Z,
+                                             bool& in_halo) {
+  const int n = a.n;
+  const int ox = X == 0 ? -1 : (X == n + 1 ? 1 : 0);
+  const int oy = Y == 0 ? -1 : (Y == n + 1 ? 1 : 0);
+  const int oz = Z == 0 ? -1 : (Z == n + 1 ? 1 : 0);
+  const long long lin = (static_cast<long long>(X - 1) * n + (Y - 1)) * n + (Z - 1);
+  in_halo = (ox | oy | oz) != 0;
+  if (!in_halo) return static_cast<long long>(b) * n * n * n + lin;
+  const long long base = a.nbase[b * 27 + (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1)];
+  if (base != kOwnPage) return base + lin;
+  return page_slot(a, b, X, Y, Z);
+}
+
+// Halo item k of an open block (block_lattice.h:70-89): item (page, block,
+// halo index, population i); the page slot it writes, and the slot its torus
+// pull reads (own core, the neighbour core the exchange copies, or the own
+// halo page).
+__device__ __forceinline__ void rotate_slots(const StepArgs& a, uint32_t k, long long& dst, long long& src, int& i) {
+  const int4 it = reinterpret_cast<const int4*>(a.open_pages)[k];
+  i = it.w;
+  const int cells = a.np * a.np * a.np;
+  int sp = a.hpos[it.z] - a.off_pad[i];
+  sp = sp < 0 ? sp + cells : (sp >= cells ? sp - cells : sp);
+  const int X = static_cast<int>(a.div_np2.div(static_cast<uint32_t>(sp)));
+  const int rem = sp - X * a.np * a.np;
+  const int Y = static_cast<int>(a.div_np.div(static_cast<uint32_t>(rem)));
+  const int Z = rem - Y * a.np;
+  bool halo;
+  src = resolve(a, static_cast<uint32_t>(it.y), X, Y, Z, halo);
+  dst = a.halo_base + static_cast<long long>(it.x) * a.n_halo + it.z;
+}
+
+// Macro state (rho - 1, u, f_neq) of saved pre-collision populations
+// (LevelCoupler::ReadMacro, level_coupler.cpp:183-189).
+struct Macro {
+  float drho, ux, uy, uz;
+  float fneq[kQ];
+};
+__device__ inline void read_macro(const float* f, Macro& m) {
+  float fr[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) fr[i] = f[i];
+  float drho, jx, jy, jz;
+  moments(fr, drho, jx, jy, jz);
+  const float rho = 1.0f + drho, inv = 1.0f / rho;
+  m.drho = drho; m.ux = jx * inv; m.uy = jy * inv; m.uz = jz * inv;
+  const float usq15 = 1.5f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const float cu = cx(i) * m.ux + cy(i) * m.uy + cz(i) * m.uz;
+    m.fneq[i] = fr[i] - wf(i) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - usq15));
+  }
+}
+// feq(rho,u) + scale * f_neq (WriteProlongation, level_coupler.cpp:191-201),
+// then BGK if the target cell is kBulk: the written state is collided by the
+// next step of its level before it is streamed.
+__device__ inline void write_macro_cell(const Macro& m, float s, int kind, float omega, float (&f)[kQ]) {
+  const float rho = 1.0f + m.drho;
+  const float usq15 = 1.5f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const float cu = cx(i) * m.ux + cy(i) * m.uy + cz(i) * m.uz;
+    f[i] = wf(i) * (m.drho + rho * (3.0f * cu + 4.5f * cu * cu - usq15)) + s * m.fneq[i];
+  }
+  if (kind == kBulk) bgk(f, omega);
+}
+
+// FP64 block reduction of N doubles: warp shuffles, then one warp over the
+// per-warp partials; thread 0 returns the totals.
+template <int N>
+__device__ inline void block_reduce(double (&v)[N]) {
+  __shared__ double sm[kThreads / 32][N];
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < N; ++k) sm[wid][k] = v[k];
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      v[k] = lane < kThreads / 32 ? sm[lane][k] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    }
+  }
+}
+
+}  // namespace
+}  // namespace octlb_gpu
+
+#endif  // OCTLB_LBM_DEVICE_CUH_

@@ -17,66 +17,11 @@
 // stream (time_loop.h:201-217) is therefore a ghost fill followed by k_step.
 #include <cstdio>
 
-#include "octlb_internal.h"
+#include "lbm_device.cuh"
 
 namespace octlb_gpu {
 
 namespace {
-
-constexpr int kThreads = 256;
-
-template <typename T>
-__device__ __forceinline__ float LD(const T* base, long long qs, int i, long long slot, float inv) {
-  return Store<T>::ld(base + i * qs + slot, inv);
-}
-
-// Core coordinates of core work item t (slot t).
-struct Cell {
-  uint32_t b, x, y, z;
-};
-__device__ __forceinline__ Cell cell_of(const StepArgs& a, uint32_t t) {
-  const uint32_t n = a.n;
-  Cell c;
-  c.b = a.div_n3.div(t);
-  uint32_t r = t - c.b * n * n * n;
-  c.x = a.div_n2.div(r);
-  r -= c.x * n * n;
-  c.y = a.div_n.div(r);
-  c.z = r - c.y * n;
-  return c;
-}
-
-// Own halo-page slot of padded position (X, Y, Z) of block b; positions that
-// no table covers are excluded by construction, the check keeps the access in
-// bounds and records an error if that ever fails.
-__device__ __forceinline__ long long page_slot(const StepArgs& a, uint32_t b, int X, int Y, int Z) {
-  const int pg = a.page_of[b];
-  const int h = a.hmap[(X * a.np + Y) * a.np + Z];
-  if (pg < 0 || h < 0) {
-    atomicExch(a.err, kErrHalo);
-    return static_cast<long long>(b) * a.n * a.n * a.n;
-  }
-  return a.halo_base + static_cast<long long>(pg) * a.n_halo + h;
-}
-
-// Slot holding padded position (X, Y, Z) in [0, n+1]^3 of block b: the own
-// core, the same-level neighbour's core cell the reference's exchange copies
-// into that halo position, or the block's own halo page.  in_halo reports a
-// position outside the core (the reference sees such sources as kBulk halo
-// cells, block_lattice.cpp:510-518).
-__device__ __forceinline__ long long resolve(const StepArgs& a, uint32_t b, int X, int Y, int Z,
-                                             bool& in_halo) {
-  const int n = a.n;
-  const int ox = X == 0 ? -1 : (X == n + 1 ? 1 : 0);
-  const int oy = Y == 0 ? -1 : (Y == n + 1 ? 1 : 0);
-  const int oz = Z == 0 ? -1 : (Z == n + 1 ? 1 : 0);
-  const long long lin = (static_cast<long long>(X - 1) * n + (Y - 1)) * n + (Z - 1);
-  in_halo = (ox | oy | oz) != 0;
-  if (!in_halo) return static_cast<long long>(b) * n * n * n + lin;
-  const long long base = a.nbase[b * 27 + (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1)];
-  if (base != kOwnPage) return base + lin;
-  return page_slot(a, b, X, Y, Z);
-}
 
 // Source slots of the 19 pulls of core cell c (local index tl inside its
 // block, global slot t): direction i reads padded position x + 1 - c_i.  The
@@ -112,27 +57,15 @@ __device__ __forceinline__ void source_slots(const StepArgs& a, const Cell& c, l
   }
 }
 
-// Torus-streamed halo population of an open block (block_lattice.h:70-89):
-// item k = (page, block, halo index, population); no collision; the source
-// resolves like a core pull (own core, the neighbour core the exchange
-// copies, or the own halo page).
+// Torus-streamed halo population of an open block (block_lattice.h:70-89),
+// item k: copied without collision.
 template <typename T>
 __device__ __forceinline__ void rotate_item(const StepArgs& a, uint32_t k) {
   if (k >= static_cast<uint32_t>(a.n_open)) return;
-  const T* src = static_cast<const T*>(a.src);
-  T* dst = static_cast<T*>(a.dst);
-  const int4 it = reinterpret_cast<const int4*>(a.open_pages)[k];
-  const int i = it.w;
-  const int cells = a.np * a.np * a.np;
-  int sp = a.hpos[it.z] - a.off_pad[i];
-  sp = sp < 0 ? sp + cells : (sp >= cells ? sp - cells : sp);
-  const int X = static_cast<int>(a.div_np2.div(static_cast<uint32_t>(sp)));
-  const int rem = sp - X * a.np * a.np;
-  const int Y = static_cast<int>(a.div_np.div(static_cast<uint32_t>(rem)));
-  const int Z = rem - Y * a.np;
-  bool halo;
-  const long long sslot = resolve(a, static_cast<uint32_t>(it.y), X, Y, Z, halo);
-  dst[i * a.qs + a.halo_base + static_cast<long long>(it.x) * a.n_halo + it.z] = src[i * a.qs + sslot];
+  long long d, sl;
+  int i;
+  rotate_slots(a, k, d, sl, i);
+  static_cast<T*>(a.dst)[i * a.qs + d] = static_cast<const T*>(a.src)[i * a.qs + sl];
 }
 
 template <typename T, bool LINKS, bool FLAGS, bool BLOCKED>
@@ -390,6 +323,24 @@ __global__ void __launch_bounds__(kThreads) k_step_pair(const StepArgs a) {
   for (int i = 0; i < kQ; ++i) Pair<T>::st(o + i * a.qs, f0[i], f1[i], a.scale);
 }
 
+// Body force: the forcing term 3 w_i (c_i . F) added to the stored
+// (post-collision) populations of kBulk core cells at the start of each level
+// step, before the boundary fills read them.  F is SoA [3][ncore].
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_add_force(const StepArgs a, T* pops, const float* force) {
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= a.ncore) return;
+  const int kind = a.flags ? (a.flags[t] & kKindMask) : kBulk;
+  const float fx = force[t], fy = force[a.ncore + t], fz = force[2ull * a.ncore + t];
+  pdl_wait();
+  if (kind != kBulk) return;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const float v = LD(pops, a.qs, i, t, a.inv_scale) + 3.0f * wf(i) * (cx(i) * fx + cy(i) * fy + cz(i) * fz);
+    Store<T>::st(pops + i * a.qs + t, v, a.scale);
+  }
+}
+
 // Ghost fill: copy descriptors first (one thread per cell of a region, all 19
 // populations), then single-population bounce-back writes.
 template <typename T>
@@ -419,41 +370,6 @@ k_ghost(T* pops, long long qs, const CopyDesc* cd, const uint32_t* cd_start, int
   pdl_wait();
   const float v = Store<T>::ld(pops + op.src_pop * qs + op.src, inv_scale) + op.add;
   Store<T>::st(pops + op.pop * qs + op.dst, v, scale);
-}
-
-// Macro state (rho - 1, u, f_neq) of saved pre-collision populations
-// (LevelCoupler::ReadMacro, level_coupler.cpp:183-189).
-struct Macro {
-  float drho, ux, uy, uz;
-  float fneq[kQ];
-};
-__device__ inline void read_macro(const float* f, Macro& m) {
-  float fr[kQ];
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) fr[i] = f[i];
-  float drho, jx, jy, jz;
-  moments(fr, drho, jx, jy, jz);
-  const float rho = 1.0f + drho, inv = 1.0f / rho;
-  m.drho = drho; m.ux = jx * inv; m.uy = jy * inv; m.uz = jz * inv;
-  const float usq15 = 1.5f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    const float cu = cx(i) * m.ux + cy(i) * m.uy + cz(i) * m.uz;
-    m.fneq[i] = fr[i] - wf(i) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - usq15));
-  }
-}
-// feq(rho,u) + scale * f_neq (WriteProlongation, level_coupler.cpp:191-201),
-// then BGK if the target cell is kBulk: the written state is collided by the
-// next step of its level before it is streamed.
-__device__ inline void write_macro_cell(const Macro& m, float s, int kind, float omega, float (&f)[kQ]) {
-  const float rho = 1.0f + m.drho;
-  const float usq15 = 1.5f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    const float cu = cx(i) * m.ux + cy(i) * m.uy + cz(i) * m.uz;
-    f[i] = wf(i) * (m.drho + rho * (3.0f * cu + 4.5f * cu * cu - usq15)) + s * m.fneq[i];
-  }
-  if (kind == kBulk) bgk(f, omega);
 }
 
 constexpr int kProlongThreads = 64;  // few items: spread them over more SMs
@@ -525,31 +441,6 @@ k_restrict(const RestrictItem* items, int nitems, const float* fine_save, T* coa
   for (int i = 0; i < kQ; ++i) Store<T>::st(coarse + i * coarse_qs + it.coarse_slot, f[i], cscale);
 }
 
-// FP64 block reduction of N doubles: warp shuffles, then one warp over the
-// per-warp partials; thread 0 returns the totals.
-template <int N>
-__device__ inline void block_reduce(double (&v)[N]) {
-  __shared__ double sm[kThreads / 32][N];
-#pragma unroll
-  for (int k = 0; k < N; ++k)
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < N; ++k) sm[wid][k] = v[k];
-  __syncthreads();
-  if (wid == 0) {
-#pragma unroll
-    for (int k = 0; k < N; ++k) {
-      v[k] = lane < kThreads / 32 ? sm[lane][k] : 0.0;
-      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-    }
-  }
-}
-
-// Momentum-exchange force (drag_postprocessor.h:67-115) from the buffer the
-// last step read: f_out = g_i(x) is the post-collide snapshot, and the bounced
-// f_opp(x) is re-pulled from the same buffer with the step's own rule.
 // Momentum-exchange force (drag_postprocessor.h:67-115) from the buffer the
 // last step read.  For a link from kBulk cell x to an in-block obstacle cell
 // x + c_i: f_out = g_i(x) (the post-collide snapshot) and f_bar is the
@@ -792,6 +683,13 @@ cudaError_t launch_step_pair(const StepArgs& a, cudaStream_t s) {
 bool pair_step_eligible(int n) { return n >= 4 && (n % 2) == 0 && n <= 1024; }
 
 template <typename T>
+cudaError_t launch_add_force(const StepArgs& a, T* pops, const float* force, cudaStream_t s) {
+  if (a.ncore == 0) return cudaSuccess;
+  const cudaError_t e = launch_chain(k_add_force<T>, dim3(grid_for(a.ncore)), dim3(kThreads), 0, s, a, pops, force);
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t launch_ghost(T* pops, long long qs, const CopyDesc* cd, const uint32_t* cd_start, int ncd,
                          uint32_t ncopy, const BBOp* bb, uint32_t nbb, float scale, float inv_scale,
                          cudaStream_t s) {
@@ -862,6 +760,7 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
   template cudaError_t launch_step<T>(const StepArgs&, bool, bool, bool, cudaStream_t);            \
   template cudaError_t launch_step_pair<T>(const StepArgs&, cudaStream_t);                         \
   template cudaError_t launch_step_near<T>(const StepArgs&, const NearTables&, cudaStream_t);       \
+  template cudaError_t launch_add_force<T>(const StepArgs&, T*, const float*, cudaStream_t);         \
   template cudaError_t launch_step_map<T>(const StepArgs&, bool, bool, int, cudaStream_t);         \
   template cudaError_t launch_ghost<T>(T*, long long, const CopyDesc*, const uint32_t*, int,       \
                                        uint32_t, const BBOp*, uint32_t, float, float, cudaStream_t); \

@@ -38,10 +38,22 @@ template <typename T> cudaError_t launch_step_bulk(const StepArgs&, int, cudaStr
 template <typename T> int bulk_prepare(int n);
 template <typename T> cudaError_t launch_step_pair(const StepArgs&, cudaStream_t);
 template <typename T> cudaError_t launch_step_near(const StepArgs&, const NearTables&, cudaStream_t);
+template <typename T> cudaError_t launch_add_force(const StepArgs&, T*, const float*, cudaStream_t);
 template <typename T> cudaError_t launch_step_map(const StepArgs&, bool, bool, int, cudaStream_t);
 bool pair_step_eligible(int n);
 bool map_step_eligible(int n, long long nslots);
 void set_programmatic_launch(bool on);
+cudaError_t launch_adj_step(const StepArgs&, bool, bool, const float*, float*, const float*, double*, cudaStream_t);
+cudaError_t launch_adj_near(const StepArgs&, const NearTables&, const float*, float*, const float*, double*,
+                            cudaStream_t);
+cudaError_t launch_adj_ghost(float*, long long, const BBOp*, uint32_t, double*, cudaStream_t);
+cudaError_t launch_adj_force(const StepArgs&, const float*, double*, cudaStream_t);
+cudaError_t launch_adj_drag(const StepArgs&, bool, const DragItem*, int, float*, float, int, cudaStream_t);
+cudaError_t launch_adj_prolong(const ProlongItem*, int, const float*, const float*, int, float*, long long, float,
+                               float, float*, float*, double*, cudaStream_t);
+cudaError_t launch_adj_read_macro(const ProlongItem*, int, const float*, float*, float*, cudaStream_t);
+cudaError_t launch_adj_restrict(const RestrictItem*, int, const float*, float*, long long, float, float, float*,
+                                double*, cudaStream_t);
 bool bulk_step_eligible(int n, int elem_bytes);
 uint32_t drag_partials(int n);
 uint32_t audit_partials(const StepArgs& a);
@@ -113,7 +125,42 @@ struct Level {
   bool use_pair = false;            // two-cells-per-thread step (periodic block)
   bool use_map = false;             // slot-map step (forest level)
   int bulk_grid = 0;
+  DevBuf body_force;                // [3][ncore] float, or empty
+  bool has_force = false;
   StepArgs args{};
+};
+
+// Forward state of one level step kept for the reverse sweep: the step's
+// input after the body force and the boundary fills, the save rows it wrote,
+// and (coarse levels) the prev-macro store before its half-time prolongation.
+constexpr int kGradSlots = 4;       // d/d omega, d/d prolong scale, d/d restrict scale, d/d wall velocity
+
+struct StepRecord {
+  int level = -1;
+  DevBuf snap, save, prev;
+  bool drag = false;                // the objective's force is taken from this input
+};
+
+// Adjoint sweep state (octlb_gpu_adjoint): cotangents per level, the
+// checkpoints of one run and the step records of one recomputed segment.
+struct AdjointState {
+  struct Lv {
+    DevBuf lam[2];                  // cotangent of the level's populations ([19][slots] FP32)
+    int cur = 0;
+    DevBuf lam_save, lam_m, lam_prev, gF;
+  };
+  std::vector<Lv> lv;
+  std::vector<StepRecord> recs;
+  size_t nrec = 0;
+  bool recording = false;
+  int last_rec[32] = {};
+  DevBuf g;                         // parameter-gradient accumulators (FP64)
+  struct Checkpoint {
+    std::vector<DevBuf> buf, prev;
+    std::vector<int> cur;
+  };
+  std::vector<Checkpoint> ck;
+  int comp = 0;
 };
 
 }  // namespace
@@ -150,6 +197,8 @@ struct octlb_ctx {
   bool use_graphs = true;           // OCTLB_NO_GRAPH=1 launches kernel by kernel
   bool use_pdl = true;              // OCTLB_NO_PDL=1: plain stream order between the step's kernels
   float prolong_scale = 0.f, restrict_scale = 0.f;
+  double wall_vscale = 0.0;         // largest moving-wall speed (adjoint velocity parameter)
+  std::unique_ptr<AdjointState> adj;
 };
 
 namespace octlb_host {
@@ -227,13 +276,30 @@ int do_advance_level(octlb_ctx* ctx, int l);
 template <typename T>
 int launch_level_step(octlb_ctx* ctx, Level& L) {
   if (L.nblk == 0) return OCTLB_OK;
-  // Ghost fill into the buffer the step reads (reference: apply() then
-  // exchange() after collide, time_loop.h:207-211).
+  // Body force on the stored post-collision state, then the ghost fill into
+  // the buffer the step reads (reference: apply() then exchange() after
+  // collide, time_loop.h:207-211).
+  if (L.has_force) CK(launch_add_force<T>(L.args, L.buf[L.cur].as<T>(), L.body_force.as<float>(), ctx->stream));
   CK(launch_ghost<T>(L.buf[L.cur].as<T>(), L.nslots, nullptr, nullptr, 0, 0, L.bb_ops.as<BBOp>(), L.n_bb,
                      L.scale, L.inv_scale, ctx->stream));
   StepArgs a = L.args;
   a.src = L.buf[L.cur].p;
   a.dst = L.buf[1 - L.cur].p;
+  StepRecord* rec = nullptr;
+  if (ctx->adj && ctx->adj->recording) {
+    AdjointState& A = *ctx->adj;
+    if (A.nrec == A.recs.size()) A.recs.emplace_back();
+    rec = &A.recs[A.nrec];
+    if (rec->level != L.lvl) {
+      CK(rec->snap.alloc(static_cast<size_t>(L.nslots) * kQ * sizeof(T)));
+      CK(rec->save.alloc(static_cast<size_t>(L.n_save) * kQ * sizeof(float)));
+      CK(rec->prev.alloc(L.n_prolong > 0 ? L.prev.bytes : 0));  // rows indexed by coupling point
+      rec->level = L.lvl;
+    }
+    CK(cudaMemcpyAsync(rec->snap.p, a.src, rec->snap.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    rec->drag = ctx->drag && L.n_drag > 0 && L.substep + 1 == (1 << L.lvl);
+    A.last_rec[L.lvl] = static_cast<int>(A.nrec++);
+  }
   if (L.use_bulk) {
     CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
   } else if (L.use_pair) {
@@ -246,6 +312,8 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
                       ctx->stream));
     CK(launch_step_near<T>(a, L.near, ctx->stream));
   }
+  if (rec && L.n_save > 0)
+    CK(cudaMemcpyAsync(rec->save.p, L.save_buf.p, rec->save.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
   // The force after advance_one reads each level's last step (the reference
   // computes MomentumExchangeDrag once, after advance_one): skip the others.
   ++L.substep;
@@ -266,6 +334,10 @@ int do_advance_level(octlb_ctx* ctx, int l) {
   ++ctx->counters_stream[l];
   if (l >= ctx->max_level) return OCTLB_OK;
   Level& F = ctx->levels[l + 1];
+  if (ctx->adj && ctx->adj->recording && L.n_prolong > 0) {
+    StepRecord& R = ctx->adj->recs[ctx->adj->last_rec[l]];
+    CK(cudaMemcpyAsync(R.prev.p, L.prev.p, R.prev.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
   // apply_half_time(l) -> advance(l+1) -> apply_full_time(l) -> advance(l+1)
   // -> restrict(l+1)  (time_loop.h:228-239)
   for (int phase = 0; phase < 2; ++phase) {
@@ -526,6 +598,16 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     return -1;
   };
   const int np = n + 2, np3 = np * np * np;
+  // Velocity scale of the moving tree-boundary walls (the largest wall speed,
+  // e.g. the inlet u_max): every wall velocity is taken proportional to it
+  // for the adjoint's d/du_max.
+  double wall_vscale = 0.0;
+  for (int k = 0; k < t->n_tree_boundary && t->tree_boundary_spec; ++k) {
+    const double* sp = t->tree_boundary_spec + 8 * k;
+    if (static_cast<int>(sp[0]) == OCTLB_TB_WALL)
+      wall_vscale = std::max(wall_vscale, std::sqrt(sp[1] * sp[1] + sp[2] * sp[2] + sp[3] * sp[3]));
+  }
+  ctx->wall_vscale = wall_vscale;
   std::vector<int> hmap(static_cast<size_t>(np3), -1), hpos;
   for (int X = 0; X < np; ++X)
     for (int Y = 0; Y < np; ++Y)
@@ -626,14 +708,14 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     // Tree-boundary fills (DomainBoundaryHandler::apply(), before the
     // exchange), in list order; a later write of the same halo population
     // wins.  Keyed by (block, padded position, population).
-    struct BB { int lb, hlin, pop; long long src; int src_pop; float add; };
+    struct BB { int lb, hlin, pop; long long src; int src_pop; float add, dadd; };
     std::map<std::tuple<int, int, int>, size_t> bbidx;
     std::vector<BB> bbl;
-    auto put_bb = [&](int lb, int hlin, int pop, long long src, int src_pop, float add) {
+    auto put_bb = [&](int lb, int hlin, int pop, long long src, int src_pop, float add, float dadd) {
       const auto key = std::make_tuple(lb, hlin, pop);
       auto it = bbidx.find(key);
-      if (it == bbidx.end()) { bbidx.emplace(key, bbl.size()); bbl.push_back({lb, hlin, pop, src, src_pop, add}); }
-      else bbl[it->second] = {lb, hlin, pop, src, src_pop, add};
+      if (it == bbidx.end()) { bbidx.emplace(key, bbl.size()); bbl.push_back({lb, hlin, pop, src, src_pop, add, dadd}); }
+      else bbl[it->second] = {lb, hlin, pop, src, src_pop, add, dadd};
     };
     for (int k = 0; k < t->n_tree_boundary; ++k) {
       const int gb = t->tree_boundary[2 * k], dir = t->tree_boundary[2 * k + 1];
@@ -667,7 +749,8 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
               if (xx < 1 || yy < 1 || zz < 1 || xx > n || yy > n || zz > n) continue;
               const double cu = (ci[0] * sp[1] + ci[1] * sp[2] + ci[2] * sp[3]) * shape;
               put_bb(lb, hlin, i, core_slot_of(n, lb, xx - 1, yy - 1, zz - 1), opp(i),
-                     static_cast<float>(6.0 * wd(i) * cu));
+                     static_cast<float>(6.0 * wd(i) * cu),
+                     wall_vscale > 0.0 ? static_cast<float>(6.0 * wd(i) * cu / wall_vscale) : 0.f);
             }
           } else {  // outflow: copy the adjacent interior cell, tangentially clamped
             int src[3];
@@ -675,7 +758,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
             src[t0] = std::min(std::max(a, 1), n);
             src[t1] = std::min(std::max(b2, 1), n);
             const long long ss = core_slot_of(n, lb, src[0] - 1, src[1] - 1, src[2] - 1);
-            for (int i = 0; i < kQ; ++i) put_bb(lb, hlin, i, ss, i, 0.f);
+            for (int i = 0; i < kQ; ++i) put_bb(lb, hlin, i, ss, i, 0.f, 0.f);
           }
         }
     }
@@ -775,7 +858,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     std::vector<BBOp> bbv;
     for (const BB& op : bbl)
       bbv.push_back(BBOp{ncore + static_cast<long long>(page_of[op.lb]) * H + hmap[op.hlin], op.src, op.pop,
-                         op.src_pop, op.add, 0});
+                         op.src_pop, op.add, op.dadd});
     L.n_bb = static_cast<uint32_t>(bbv.size());
 
     // Slot bases of the 27 directions: own core (centre), the neighbour's core
@@ -1163,6 +1246,262 @@ int advance_impl(octlb_ctx* ctx, int steps) {
   return OCTLB_OK;
 }
 
+// ------------------------------------------------------------------ adjoint
+// Discrete adjoint of n coarse steps (advance_one) by a reverse sweep with
+// checkpoints every K coarse steps and recomputation in between: the forward
+// pass stores the state at every checkpoint and evaluates the objective; then,
+// segment by segment from the last, the forward is recomputed from the
+// segment's checkpoint with every level step's input recorded, and the
+// adjoint kernels run through those steps in reverse (TimeLoop::advance's
+// recursion mirrored: restriction, second child, full-time prolongation,
+// first child, half-time prolongation, then the level's own step).
+
+int count_records(const octlb_ctx* ctx, int l) {
+  int c = ctx->levels[l].nblk > 0 ? 1 : 0;
+  if (l < ctx->max_level) c += 2 * count_records(ctx, l + 1);
+  return c;
+}
+
+int adj_step(octlb_ctx* ctx, int l, const StepRecord& R, float coef) {
+  Level& L = ctx->levels[l];
+  AdjointState& A = *ctx->adj;
+  AdjointState::Lv& V = A.lv[l];
+  const bool links = ctx->stream_mode == OCTLB_STREAM_LINKS;
+  StepArgs a = L.args;
+  a.src = R.snap.p;
+  a.dst = nullptr;
+  a.slot_map = L.slot_map.as<int>();
+  float* lamY = V.lam[V.cur].as<float>();
+  float* lamX = V.lam[1 - V.cur].as<float>();
+  double* g = A.g.as<double>();
+  CK(cudaMemsetAsync(lamX, 0, V.lam[1 - V.cur].bytes, ctx->stream));
+  CK(launch_adj_step(a, links, L.has_flags, lamY, lamX, V.lam_save.as<float>(), g, ctx->stream));
+  CK(launch_adj_near(a, L.near, lamY, lamX, V.lam_save.as<float>(), g, ctx->stream));
+  if (R.drag && coef != 0.f)
+    CK(launch_adj_drag(a, links, L.drag_items.as<DragItem>(), L.n_drag, lamX, coef, A.comp, ctx->stream));
+  if (L.n_save > 0) CK(cudaMemsetAsync(V.lam_save.p, 0, V.lam_save.bytes, ctx->stream));
+  CK(launch_adj_ghost(lamX, L.nslots, L.bb_ops.as<BBOp>(), L.n_bb, g, ctx->stream));
+  CK(launch_adj_force(a, lamX, V.gF.as<double>(), ctx->stream));
+  V.cur = 1 - V.cur;
+  return OCTLB_OK;
+}
+
+int adj_level(octlb_ctx* ctx, int l, size_t start, float coef) {
+  Level& L = ctx->levels[l];
+  AdjointState& A = *ctx->adj;
+  const bool own = L.nblk > 0;
+  const size_t c0 = start + (own ? 1 : 0);
+  const float omega = static_cast<float>(ctx->omega);
+  if (own && (start >= A.nrec || A.recs[start].level != l))
+    return fail(ctx, OCTLB_ESTATE, "adjoint: step record out of order");
+  if (l < ctx->max_level) {
+    Level& F = ctx->levels[l + 1];
+    const size_t cc = static_cast<size_t>(count_records(ctx, l + 1));
+    const size_t s1 = c0, s2 = c0 + cc;
+    AdjointState::Lv& V = A.lv[l];
+    AdjointState::Lv& VF = A.lv[l + 1];
+    double* g = A.g.as<double>();
+    if (F.n_restrict > 0)
+      CK(launch_adj_restrict(F.restrict_items.as<RestrictItem>(), F.n_restrict, A.recs[s2].save.as<float>(),
+                             V.lam[V.cur].as<float>(), L.nslots, ctx->restrict_scale, omega,
+                             VF.lam_save.as<float>(), g, ctx->stream));
+    int rc = adj_level(ctx, l + 1, s2, coef);
+    if (rc) return rc;
+    if (L.n_prolong > 0)
+      CK(launch_adj_prolong(L.prolong_items.as<ProlongItem>(), L.n_prolong, A.recs[start].save.as<float>(),
+                            A.recs[start].prev.as<float>(), 0, VF.lam[VF.cur].as<float>(), F.nslots,
+                            ctx->prolong_scale, omega, V.lam_m.as<float>(), V.lam_prev.as<float>(), g,
+                            ctx->stream));
+    rc = adj_level(ctx, l + 1, s1, coef);
+    if (rc) return rc;
+    if (L.n_prolong > 0) {
+      CK(launch_adj_prolong(L.prolong_items.as<ProlongItem>(), L.n_prolong, A.recs[start].save.as<float>(),
+                            A.recs[start].prev.as<float>(), 1, VF.lam[VF.cur].as<float>(), F.nslots,
+                            ctx->prolong_scale, omega, V.lam_m.as<float>(), V.lam_prev.as<float>(), g,
+                            ctx->stream));
+      CK(launch_adj_read_macro(L.prolong_items.as<ProlongItem>(), L.n_prolong, A.recs[start].save.as<float>(),
+                               V.lam_m.as<float>(), V.lam_save.as<float>(), ctx->stream));
+    }
+  }
+  if (own) return adj_step(ctx, l, A.recs[start], coef);
+  return OCTLB_OK;
+}
+
+template <typename T>
+int checkpoint_copy(octlb_ctx* ctx, AdjointState::Checkpoint& c, bool save) {
+  const size_t nl = ctx->levels.size();
+  if (save && c.buf.size() != nl) {
+    c.buf.resize(nl);
+    c.prev.resize(nl);
+    c.cur.assign(nl, 0);
+    for (size_t l = 0; l < nl; ++l) {
+      Level& L = ctx->levels[l];
+      CK(c.buf[l].alloc(static_cast<size_t>(L.nslots) * kQ * sizeof(T)));
+      CK(c.prev[l].alloc(L.n_prolong > 0 ? L.prev.bytes : 0));
+    }
+  }
+  for (size_t l = 0; l < nl; ++l) {
+    Level& L = ctx->levels[l];
+    if (L.nblk == 0) continue;
+    if (save) {
+      c.cur[l] = L.cur;
+      CK(cudaMemcpyAsync(c.buf[l].p, L.buf[L.cur].p, c.buf[l].bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+      if (L.n_prolong > 0)
+        CK(cudaMemcpyAsync(c.prev[l].p, L.prev.p, c.prev[l].bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+      L.cur = c.cur[l];
+      CK(cudaMemcpyAsync(L.buf[L.cur].p, c.buf[l].p, c.buf[l].bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+      if (L.n_prolong > 0)
+        CK(cudaMemcpyAsync(L.prev.p, c.prev[l].p, c.prev[l].bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+  }
+  return OCTLB_OK;
+}
+
+template <typename T>
+int adjoint_impl(octlb_ctx* ctx, const octlb_adj_params* p, double* objective, double* grad,
+                 double* grad_force) {
+  if (ctx->precision != OCTLB_FP32) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates FP32 storage only");
+  if (!ctx->drag) return fail(ctx, OCTLB_ESTATE, "the adjoint's objective needs a context created with drag");
+  const int NT = p->coarse_steps, W = p->window;
+  if (NT < 1 || W < 1 || W > NT || p->component < 0 || p->component > 2 || p->checkpoint_interval < 0)
+    return fail(ctx, OCTLB_EINVAL, "adjoint: need coarse_steps >= 1, 1 <= window <= coarse_steps, component 0..2");
+  for (auto& L : ctx->levels)
+    if (L.nblk > 0 && !L.slot_map.p)
+      return fail(ctx, OCTLB_EINVAL, "adjoint: every level needs the slot-map layout (n a multiple of 8, <= 16)");
+  const int K = p->checkpoint_interval > 0 ? p->checkpoint_interval
+                                           : std::max(1, static_cast<int>(std::ceil(std::sqrt(static_cast<double>(NT)))));
+  const int nck = (NT + K - 1) / K;
+  if (!ctx->adj) ctx->adj = std::make_unique<AdjointState>();
+  AdjointState& A = *ctx->adj;
+  A.comp = p->component;
+  const size_t nl = ctx->levels.size();
+  if (A.lv.size() != nl) {
+    A.lv.clear();
+    A.lv.resize(nl);
+    for (size_t l = 0; l < nl; ++l) {
+      Level& L = ctx->levels[l];
+      AdjointState::Lv& V = A.lv[l];
+      for (int k = 0; k < 2; ++k) CK(V.lam[k].alloc(static_cast<size_t>(L.nslots) * kQ * sizeof(float)));
+      CK(V.lam_save.alloc(static_cast<size_t>(L.n_save) * kQ * sizeof(float)));
+      CK(V.lam_m.alloc(static_cast<size_t>(L.n_prolong) * 23 * sizeof(float)));
+      CK(V.lam_prev.alloc(L.n_prolong > 0 ? L.prev.bytes : 0));
+      CK(V.gF.alloc(static_cast<size_t>(3 * L.ncore) * sizeof(double)));
+    }
+    CK(A.g.alloc(kGradSlots * sizeof(double)));
+  }
+  if (A.ck.size() < static_cast<size_t>(nck + 1)) A.ck.resize(nck + 1);
+  const std::vector<int> c0 = ctx->counters_collide, s0 = ctx->counters_stream;
+
+  // Forward: checkpoints, objective over the window.
+  for (int k = 0; k < NT; ++k) {
+    if (k % K == 0) { int rc = checkpoint_copy<T>(ctx, A.ck[k / K], true); if (rc) return rc; }
+    if (k == NT - W) {
+      CK(cudaMemsetAsync(ctx->force_sum.p, 0, 3 * sizeof(double), ctx->stream));
+      ctx->force_steps = 0;
+    }
+    int rc = advance_impl<T>(ctx, 1);
+    if (rc) return rc;
+  }
+  double fs[3];
+  CK(cudaMemcpyAsync(fs, ctx->force_sum.p, sizeof(fs), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (int rc = check_device_error(ctx)) return rc;
+  const double J = fs[p->component] / W;
+  const long long fsteps = ctx->force_steps;
+  { int rc = checkpoint_copy<T>(ctx, A.ck[nck], true); if (rc) return rc; }
+  DevBuf keep_force, keep_sum;
+  CK(keep_force.alloc(3 * sizeof(double)));
+  CK(keep_sum.alloc(3 * sizeof(double)));
+  CK(cudaMemcpyAsync(keep_force.p, ctx->force.p, 3 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(keep_sum.p, ctx->force_sum.p, 3 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+
+  // Reverse sweep.
+  for (auto& V : A.lv) {
+    for (int k = 0; k < 2; ++k) if (V.lam[k].p) CK(cudaMemsetAsync(V.lam[k].p, 0, V.lam[k].bytes, ctx->stream));
+    if (V.lam_save.p) CK(cudaMemsetAsync(V.lam_save.p, 0, V.lam_save.bytes, ctx->stream));
+    if (V.lam_m.p) CK(cudaMemsetAsync(V.lam_m.p, 0, V.lam_m.bytes, ctx->stream));
+    if (V.lam_prev.p) CK(cudaMemsetAsync(V.lam_prev.p, 0, V.lam_prev.bytes, ctx->stream));
+    if (V.gF.p) CK(cudaMemsetAsync(V.gF.p, 0, V.gF.bytes, ctx->stream));
+    V.cur = 0;
+  }
+  CK(cudaMemsetAsync(A.g.p, 0, A.g.bytes, ctx->stream));
+  const size_t per = static_cast<size_t>(count_records(ctx, 0));
+  const float coef = static_cast<float>(1.0 / W);
+  for (int c = nck - 1; c >= 0; --c) {
+    const int k0 = c * K, k1 = std::min(NT, k0 + K);
+    int rc = checkpoint_copy<T>(ctx, A.ck[c], false);
+    if (rc) return rc;
+    A.recording = true;
+    A.nrec = 0;
+    for (int k = k0; k < k1; ++k) {
+      rc = advance_one_launches<T>(ctx);
+      if (rc) { A.recording = false; return rc; }
+    }
+    A.recording = false;
+    if (A.nrec != per * static_cast<size_t>(k1 - k0)) return fail(ctx, OCTLB_ESTATE, "adjoint: record count mismatch");
+    for (int k = k1 - 1; k >= k0; --k) {
+      rc = adj_level(ctx, 0, per * static_cast<size_t>(k - k0), k >= NT - W ? coef : 0.f);
+      if (rc) return rc;
+    }
+  }
+
+  // Leave the context as the forward left it.
+  { int rc = checkpoint_copy<T>(ctx, A.ck[nck], false); if (rc) return rc; }
+  CK(cudaMemcpyAsync(ctx->force.p, keep_force.p, 3 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->force_sum.p, keep_sum.p, 3 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  ctx->force_steps = fsteps;
+  ctx->counters_collide = c0;
+  ctx->counters_stream = s0;
+  for (size_t l = 0; l < nl; ++l) {
+    ctx->counters_collide[l] += NT << l;
+    ctx->counters_stream[l] += NT << l;
+  }
+
+  double gv[kGradSlots];
+  CK(cudaMemcpyAsync(gv, A.g.p, sizeof(gv), cudaMemcpyDeviceToHost, ctx->stream));
+  const long long n3 = static_cast<long long>(ctx->n) * ctx->n * ctx->n;
+  std::vector<std::vector<double>> gF(nl);
+  if (grad_force) {
+    for (size_t l = 0; l < nl; ++l) {
+      Level& L = ctx->levels[l];
+      if (L.nblk == 0) continue;
+      gF[l].resize(static_cast<size_t>(3 * L.ncore));
+      CK(cudaMemcpyAsync(gF[l].data(), A.lv[l].gF.p, gF[l].size() * sizeof(double), cudaMemcpyDeviceToHost,
+                         ctx->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (int rc = check_device_error(ctx)) return rc;
+  const double tau = 1.0 / ctx->omega;
+  // omega = 1/tau; prolongation scale (tau - 1/4)/tau; restriction scale
+  // tau/(tau - 1/4) (level_coupler.cpp:226-228)
+  const double dtau = gv[0] * (-1.0 / (tau * tau)) + gv[1] * (0.25 / (tau * tau)) +
+                      gv[2] * (-0.25 / ((tau - 0.25) * (tau - 0.25)));
+  if (objective) *objective = J;
+  if (grad) {
+    grad[0] = gv[3];
+    grad[1] = dtau;
+  }
+  if (grad_force) {
+    for (size_t l = 0; l < nl; ++l) {
+      Level& L = ctx->levels[l];
+      for (int lb = 0; lb < L.nblk; ++lb)
+        for (long long c = 0; c < n3; ++c)
+          for (int a = 0; a < 3; ++a)
+            grad_force[(static_cast<size_t>(L.blocks[lb]) * n3 + c) * 3 + a] =
+                gF[l][static_cast<size_t>(a * L.ncore + lb * n3 + c)];
+    }
+  }
+  return OCTLB_OK;
+}
+
+void clear_graphs(octlb_ctx* ctx) {
+  for (auto& kv : ctx->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  ctx->graphs.clear();
+}
+
 // Level-local block order equals a contiguous run of global ids: host
 // arrays can be copied without reordering.
 bool contiguous(const Level& L) {
@@ -1296,9 +1635,7 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
 void octlb_gpu_destroy(octlb_ctx* ctx) {
   if (!ctx) return;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  for (auto& kv : ctx->graphs)
-    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-  ctx->graphs.clear();
+  clear_graphs(ctx);
   cudaStream_t s = ctx->own_stream ? ctx->stream : nullptr;
   ctx->levels.clear();
   if (s) cudaStreamDestroy(s);
@@ -1327,10 +1664,46 @@ int octlb_gpu_advance(octlb_ctx* ctx, int steps) {
   return ctx->precision == OCTLB_FP32 ? advance_impl<float>(ctx, steps) : advance_impl<__half>(ctx, steps);
 }
 
+int octlb_gpu_adjoint(octlb_ctx* ctx, const octlb_adj_params* p, double* objective, double* grad,
+                      double* grad_force) {
+  if (!ctx || !p) return OCTLB_EINVAL;
+  if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
+  if (ctx->precision != OCTLB_FP32) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates FP32 storage only");
+  return adjoint_impl<float>(ctx, p, objective, grad, grad_force);
+}
+
 int octlb_gpu_synchronize(octlb_ctx* ctx) {
   if (!ctx) return OCTLB_EINVAL;
   CK(cudaStreamSynchronize(ctx->stream));
   return check_device_error(ctx);
+}
+
+int octlb_gpu_set_body_force(octlb_ctx* ctx, const double* force) {
+  if (!ctx) return OCTLB_EINVAL;
+  CK(cudaStreamSynchronize(ctx->stream));
+  clear_graphs(ctx);  // the captured launch sequence changes
+  const long long n3 = static_cast<long long>(ctx->n) * ctx->n * ctx->n;
+  for (auto& L : ctx->levels) {
+    L.has_force = false;
+    CK(L.body_force.alloc(0));
+    if (!force || L.nblk == 0) continue;
+    std::vector<float> f(static_cast<size_t>(3 * L.ncore));
+    bool any = false;
+    for (int lb = 0; lb < L.nblk; ++lb)
+      for (long long c = 0; c < n3; ++c) {
+        const double* g = force + (static_cast<size_t>(L.blocks[lb]) * n3 + c) * 3;
+        if (!std::isfinite(g[0]) || !std::isfinite(g[1]) || !std::isfinite(g[2]))
+          return fail(ctx, OCTLB_EINVAL, "non-finite body force");
+        for (int a = 0; a < 3; ++a) {
+          f[static_cast<size_t>(a * L.ncore + lb * n3 + c)] = static_cast<float>(g[a]);
+          any = any || g[a] != 0.0;
+        }
+      }
+    if (!any) continue;
+    CK(upload(L.body_force, f));
+    L.has_force = true;
+  }
+  return OCTLB_OK;
 }
 
 int octlb_gpu_set_populations(octlb_ctx* ctx, const double* pops) {

@@ -80,7 +80,7 @@ struct BBOp {
   long long dst, src;
   int pop, src_pop;
   float add;
-  int pad;
+  float dadd;               // d add / d (velocity scale of the moving walls)
 };
 
 // Lagrava prolongation item (level_coupler.cpp:438-478): a fine core cell

@@ -168,6 +168,14 @@ class Sim:
     def advance(self, steps=1):
         self.L.ref_sim_advance(self.h, ctypes.c_int(steps))
 
+    def set_body_force(self, force):
+        """Body force [n_blocks][n^3][3] (or None): 3 w_i (c_i . F) added to the
+        post-collision populations of kBulk cells of each level step, at the
+        DomainBoundaryHandler::apply() hook (restated; not reference code)."""
+        f = None if force is None else np.ascontiguousarray(force, np.float64)
+        self._keep.append(f)
+        self.L.ref_sim_set_body_force(self.h, _p(f))
+
     def core(self):
         n = self.mesh.n
         out = np.zeros((self.mesh.n_blocks, n, n, n, Q))

@@ -13,7 +13,11 @@
 //   * tree-boundary ghost fills (RestatedBoundary below): half-way bounce-back
 //     walls (optionally moving) and the zero-gradient outflow ghost copy of
 //     outflow_bc.h, written into the halo before the same-level exchange, at the
-//     DomainBoundaryHandler::apply() hook (time_loop.h:207-211).
+//     DomainBoundaryHandler::apply() hook (time_loop.h:207-211);
+//   * an optional body force, the forcing term 3 w_i (c_i . F) added to the
+//     post-collision populations of kBulk cells of the level just collided, at
+//     the same hook before the fills (the reference has no body force; the
+//     adjoint's finite-difference checks need one).
 #include <array>
 #include <cmath>
 #include <cstdint>
@@ -105,10 +109,43 @@ class RestatedBoundary : public DomainBoundaryHandler {
         specs_(std::move(specs)), n_(n) {}
 
   void apply(CollideRhoStats*, double, bool) override {
+    if (!force_.empty() && loop_) AddForce();
     for (std::size_t k = 0; k < faces_.size(); ++k) Fill(faces_[k], specs_[k]);
   }
 
+  // Body force [oct][n^3][3]; the level collided just before apply() is the
+  // one whose collide counter moved since the previous call.
+  void set_force(const TimeLoop* loop, const double* f) {
+    loop_ = loop;
+    const std::size_t n3 = static_cast<std::size_t>(n_) * n_ * n_;
+    if (f) force_.assign(f, f + static_cast<std::size_t>(blocks_.size()) * n3 * 3); else force_.clear();
+    seen_.assign(loop->counters().collide.begin(), loop->counters().collide.end());
+  }
+
  private:
+  void AddForce() {
+    const auto& c = loop_->counters().collide;
+    int level = -1;
+    if (seen_.size() < c.size()) seen_.resize(c.size(), 0);
+    for (std::size_t l = 0; l < c.size(); ++l)
+      if (c[l] != seen_[l]) { level = static_cast<int>(l); seen_[l] = c[l]; }
+    if (level < 0) return;
+    const std::size_t n3 = static_cast<std::size_t>(n_) * n_ * n_;
+    for (label id = 0; id < blocks_.size(); ++id) {
+      if (forest_.quadrant_level(id) != level) continue;
+      Lat& lat = blocks_[id];
+      for (int x = 0; x < n_; ++x)
+        for (int y = 0; y < n_; ++y)
+          for (int z = 0; z < n_; ++z) {
+            if (lat.bc_kind(x, y, z) != BcKind::kBulk) continue;
+            const double* F = force_.data() + ((std::size_t)id * n3 + (x * n_ + y) * n_ + z) * 3;
+            double* f = lat.populations_at_halo(x + 1, y + 1, z + 1);
+            for (int i = 0; i < Q; ++i)
+              f[i] += 3.0 * wt(i) * (cc(i, 0) * F[0] + cc(i, 1) * F[1] + cc(i, 2) * F[2]);
+          }
+    }
+  }
+
   void Fill(const TreeBoundaryFace& f, const FaceSpec& s) {
     if (s.type == 0) return;
     Lat& lat = blocks_[f.octant_id];
@@ -154,6 +191,9 @@ class RestatedBoundary : public DomainBoundaryHandler {
   std::vector<TreeBoundaryFace> faces_;
   std::vector<FaceSpec> specs_;
   int n_;
+  const TimeLoop* loop_ = nullptr;
+  std::vector<double> force_;
+  std::vector<int> seen_;
 };
 
 struct Sim {
@@ -354,6 +394,10 @@ void ref_sim_free(void* h) {
 void ref_sim_advance(void* h, int steps) {
   auto* s = static_cast<Sim*>(h);
   for (int t = 0; t < steps; ++t) s->loop->advance_one();
+}
+void ref_sim_set_body_force(void* h, const double* force) {
+  auto* s = static_cast<Sim*>(h);
+  static_cast<RestatedBoundary*>(s->bc.get())->set_force(s->loop.get(), force);
 }
 int ref_sim_max_level(void* h) { return static_cast<Sim*>(h)->loop->max_level(); }
 // Collide / stream counters per level and the coupler call sequence.
