@@ -11,7 +11,7 @@
 //                  (bouzidi_pull.h:8-26), reflect-on-pull, moving-wall term
 //   k_adj_ghost    boundary fills (bounce-back / moving wall / outflow copy)
 //   k_adj_drag     momentum-exchange force (the objective)
-//   k_adj_prolong, k_adj_read_macro, k_adj_restrict   Lagrava coupling
+//   k_adj_prolong, k_adj_restrict   Lagrava coupling (one warp per item)
 //   k_adj_force    gradient of the per-cell body force
 //
 // Adjoint populations use the forward slot layout [19][slots] in FP32; the
@@ -25,6 +25,94 @@ namespace {
 
 // Gradient accumulator slots.
 enum : int { kGOmega = 0, kGProlongScale = 1, kGRestrictScale = 2, kGWallVelocity = 3, kGSlots = 4 };
+
+// Lane-parallel feq_vjp: mu_i in lane i; every lane gets P and V.
+__device__ __forceinline__ void feq_vjp_lanes(const LaneDir& d, float mu, float rho, float ux, float uy, float uz,
+                                              float& P, float& Vx, float& Vy, float& Vz) {
+  const float usq = ux * ux + uy * uy + uz * uz;
+  const float cu = d.cx * ux + d.cy * uy + d.cz * uz;
+  const float mw = d.act ? mu * d.w : 0.f;
+  P = warp_sum(mw * (1.0f + 3.0f * cu + 4.5f * cu * cu - 1.5f * usq));
+  const float g = mw * (3.0f + 9.0f * cu);
+  const float sx = warp_sum(g * d.cx), sy = warp_sum(g * d.cy), sz = warp_sum(g * d.cz), sw = warp_sum(mw);
+  Vx = rho * (sx - 3.0f * ux * sw);
+  Vy = rho * (sy - 3.0f * uy * sw);
+  Vz = rho * (sz - 3.0f * uz * sw);
+}
+
+// Lane-parallel read_macro: f_i in lane i -> (drho, u) in every lane, f_neq_i
+// in lane i.
+__device__ __forceinline__ void read_macro_lanes(const LaneDir& d, float f, float& drho, float& ux, float& uy,
+                                                 float& uz, float& fneq) {
+  const float fa = d.act ? f : 0.f;
+  drho = warp_sum(fa);
+  const float jx = warp_sum(fa * d.cx), jy = warp_sum(fa * d.cy), jz = warp_sum(fa * d.cz);
+  const float rho = 1.0f + drho, inv = 1.0f / rho;
+  ux = jx * inv; uy = jy * inv; uz = jz * inv;
+  const float usq = ux * ux + uy * uy + uz * uz;
+  const float cu = d.cx * ux + d.cy * uy + d.cz * uz;
+  fneq = fa - d.w * (drho + rho * (3.0f * cu + 4.5f * cu * cu - 1.5f * usq));
+}
+
+// Lane-parallel write_vjp (see write_vjp): macro (drho, u) in every lane,
+// f_neq_i and the cotangent mu_i in lane i -> cotangent of the macro state
+// (ldrho, lu in every lane, lfneq_i in lane i), d/d s and d/d omega (every
+// lane).
+__device__ __forceinline__ void write_vjp_lanes(const LaneDir& d, float drho, float ux, float uy, float uz,
+                                                float fneq, float s, int kind, float omega, float mu, float& lfneq,
+                                                float& ldrho, float& lux, float& luy, float& luz, float& ds,
+                                                float& dom) {
+  const float rho = 1.0f + drho;
+  const float usq = ux * ux + uy * uy + uz * uz;
+  const float cu = d.cx * ux + d.cy * uy + d.cz * uz;
+  const float fp = d.act ? d.w * (drho + rho * (3.0f * cu + 4.5f * cu * cu - 1.5f * usq)) + s * fneq : 0.f;
+  float lf = mu;
+  dom = 0.f;
+  if (kind == kBulk) {
+    const float dh = warp_sum(fp);
+    const float jx = warp_sum(fp * d.cx), jy = warp_sum(fp * d.cy), jz = warp_sum(fp * d.cz);
+    const float r2 = 1.0f + dh, k2 = 1.0f / r2;
+    const float vx = jx * k2, vy = jy * k2, vz = jz * k2;
+    const float vsq = vx * vx + vy * vy + vz * vz;
+    const float cv = d.cx * vx + d.cy * vy + d.cz * vz;
+    const float feq = d.w * (dh + r2 * (3.0f * cv + 4.5f * cv * cv - 1.5f * vsq));
+    dom = warp_sum(d.act ? mu * (feq - fp) : 0.f);
+    float P, Vx, Vy, Vz;
+    feq_vjp_lanes(d, mu, r2, vx, vy, vz, P, Vx, Vy, Vz);
+    lf = (1.0f - omega) * mu + omega * (P + (Vx * (d.cx - vx) + Vy * (d.cy - vy) + Vz * (d.cz - vz)) * k2);
+  }
+  lf = d.act ? lf : 0.f;
+  feq_vjp_lanes(d, lf, rho, ux, uy, uz, ldrho, lux, luy, luz);
+  lfneq = s * lf;
+  ds = warp_sum(lf * (d.act ? fneq : 0.f));
+}
+
+// Lane-parallel body-force gradient of a kBulk coupler target whose stored
+// cotangent mu_i (lane i) is about to be cleared.
+__device__ __forceinline__ void force_grad_lanes(const LaneDir& d, float mu, double* gF, long long ncore, long long t,
+                                                 int lane) {
+  const float v = d.act ? 3.0f * d.w * mu : 0.f;
+  const float sx = warp_sum(v * d.cx), sy = warp_sum(v * d.cy), sz = warp_sum(v * d.cz);
+  if (lane == 0) {
+    gF[t] += sx;
+    gF[ncore + t] += sy;
+    gF[2 * ncore + t] += sz;
+  }
+}
+
+// Lane-parallel read_vjp: f_i and the cotangent lfneq_i in lane i, ldrho and
+// lu in every lane -> cotangent of f_i in lane i.
+__device__ __forceinline__ float read_vjp_lanes(const LaneDir& d, float f, float ldrho, float lux, float luy, float luz,
+                                                float lfneq) {
+  const float fa = d.act ? f : 0.f;
+  const float dh = warp_sum(fa);
+  const float jx = warp_sum(fa * d.cx), jy = warp_sum(fa * d.cy), jz = warp_sum(fa * d.cz);
+  const float rho = 1.0f + dh, inv = 1.0f / rho;
+  const float ux = jx * inv, uy = jy * inv, uz = jz * inv;
+  float P, Vx, Vy, Vz;
+  feq_vjp_lanes(d, lfneq, rho, ux, uy, uz, P, Vx, Vy, Vz);
+  return lfneq + (ldrho - P) + ((lux - Vx) * (d.cx - ux) + (luy - Vy) * (d.cy - uy) + (luz - Vz) * (d.cz - uz)) * inv;
+}
 
 // d feq_i / d (drho, u) contracted with a cotangent mu at the moments
 // (drho, u) (rho = 1 + drho), feq_i = w_i (drho + rho (3 cu + 4.5 cu^2 - 1.5 u^2)):
@@ -77,46 +165,7 @@ __device__ __forceinline__ float bgk_vjp(const float (&f)[kQ], float omega, cons
   return dom;
 }
 
-// Macro state -> pre-BGK populations feq(m) + s f_neq (write_macro_cell
-// without its collision).
-__device__ __forceinline__ void macro_to_f(const Macro& m, float s, float (&f)[kQ]) {
-  const float rho = 1.0f + m.drho;
-  const float usq15 = 1.5f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    const float cu = cx(i) * m.ux + cy(i) * m.uy + cz(i) * m.uz;
-    f[i] = wf(i) * (m.drho + rho * (3.0f * cu + 4.5f * cu * cu - usq15)) + s * m.fneq[i];
-  }
-}
 
-// VJP of write_macro_cell (level_coupler.cpp:191-201 + the collision of a
-// kBulk target): cotangent mu of the written populations -> cotangent of the
-// macro state (lm) and d/d s, d/d omega.
-__device__ __forceinline__ void write_vjp(const Macro& m, float s, int kind, float omega, const float (&mu)[kQ],
-                                          Macro& lm, float& ds, float& dom) {
-  float lf[kQ];
-  dom = 0.f;
-  if (kind == kBulk) {
-    float f[kQ];
-    macro_to_f(m, s, f);
-    dom = bgk_vjp(f, omega, mu, lf);
-  } else {
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) lf[i] = mu[i];
-  }
-  float P, Vx, Vy, Vz;
-  feq_vjp(lf, 1.0f + m.drho, m.ux, m.uy, m.uz, P, Vx, Vy, Vz);
-  lm.drho = P;
-  lm.ux = Vx;
-  lm.uy = Vy;
-  lm.uz = Vz;
-  ds = 0.f;
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    lm.fneq[i] = s * lf[i];
-    ds += lf[i] * m.fneq[i];
-  }
-}
 
 // VJP of read_macro (level_coupler.cpp:183-189) at the saved populations f:
 // cotangent lm of (drho, u, f_neq) -> cotangent lf of f.
@@ -134,18 +183,7 @@ __device__ __forceinline__ void read_vjp(const float (&f)[kQ], const Macro& lm, 
     lf[j] = lm.fneq[j] + a0 + ax * (cx(j) - ux) + ay * (cy(j) - uy) + az * (cz(j) - uz);
 }
 
-__device__ __forceinline__ void load_macro_row(const float* row, Macro& m) {
-  float f[kQ];
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) f[i] = row[i];
-  read_macro(f, m);
-}
 
-__device__ __forceinline__ void macro_from23(const float* p, Macro& m) {
-  m.drho = p[0]; m.ux = p[1]; m.uy = p[2]; m.uz = p[3];
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) m.fneq[i] = p[4 + i];
-}
 
 __device__ __forceinline__ void add_grad(double* g, int slot, double v) {
   double a[1] = {v};
@@ -153,23 +191,42 @@ __device__ __forceinline__ void add_grad(double* g, int slot, double v) {
   if (threadIdx.x == 0 && a[0] != 0.0) atomicAdd(g + slot, a[0]);
 }
 
+// Body-force gradient of one kBulk cell from the cotangent mu of the stored
+// state the forcing term 3 w_i (c_i . F) was added to.  gF is [3][ncore].
+__device__ __forceinline__ void force_grad(const float (&mu)[kQ], double* gF, uint32_t ncore, uint32_t t) {
+  float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const float v = 3.0f * wf(i) * mu[i];
+    sx += cx(i) * v;
+    sy += cy(i) * v;
+    sz += cz(i) * v;
+  }
+  gF[t] += sx;
+  gF[ncore + t] += sy;
+  gF[2ull * ncore + t] += sz;
+}
+
 // Step VJP over the cells the slot-map step streams (one CTA per block, the
 // block's slot map in shared memory); CTAs after the nblk block CTAs take the
 // halo rotation items.  a.src = the step's input (after force and fills);
 // lamY = cotangent of the step's output, lamX += cotangent of its input.
 template <bool LINKS, bool FLAGS>
-__global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const float* __restrict__ lamY,
-                                                      float* lamX, const float* __restrict__ lamS, double* g) {
+__global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, float* __restrict__ lamY,
+                                                      float* lamX, float* __restrict__ lamS, double* g,
+                                                      double* gF) {
   extern __shared__ int smap[];
-  const uint32_t b = blockIdx.x;
+  constexpr uint32_t kParts = 2;  // two CTAs per block, one cell per thread at a time
+  const uint32_t b = blockIdx.x / kParts, part = blockIdx.x % kParts;
   const long long qs = a.qs;
   if (b >= static_cast<uint32_t>(a.nblk)) {
-    const uint32_t k = (b - a.nblk) * kThreads + threadIdx.x;
+    const uint32_t k = (blockIdx.x - a.nblk * kParts) * kThreads + threadIdx.x;
     if (k < static_cast<uint32_t>(a.n_open)) {
       long long d, sl;
       int i;
       rotate_slots(a, k, d, sl, i);
       atomicAdd(lamX + i * qs + sl, lamY[i * qs + d]);
+      lamY[i * qs + d] = 0.f;
     }
     return;
   }
@@ -178,16 +235,19 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const f
   for (int k = threadIdx.x; k < np3; k += kThreads) smap[k] = gm[k];
   __syncthreads();
   const float* src = static_cast<const float*>(a.src);
-  const uint32_t n = a.n, n3 = n * n * n;
+  const uint32_t n = a.n, n3 = n * n * n, span = n3 / kParts;
   double dom = 0.0;
-  for (uint32_t tl = threadIdx.x; tl < n3; tl += kThreads) {
+  for (uint32_t tl = part * span + threadIdx.x; tl < (part + 1) * span; tl += kThreads) {
     const uint32_t t = b * n3 + tl;
     const uint32_t x = a.div_n2.div(tl), r = tl - x * n * n, y = a.div_n.div(r);
     const int P = (static_cast<int>(x + 1) * np + static_cast<int>(y + 1)) * np + static_cast<int>(r - y * n + 1);
     const uint8_t fl = FLAGS ? a.flags[t] : 0;
     if (LINKS && (fl & kKindMask) == kSolid) {
 #pragma unroll
-      for (int i = 0; i < kQ; ++i) atomicAdd(lamX + i * qs + t, lamY[i * qs + t]);
+      for (int i = 0; i < kQ; ++i) {
+        atomicAdd(lamX + i * qs + t, lamY[i * qs + t]);
+        lamY[i * qs + t] = 0.f;
+      }
       continue;
     }
     if (LINKS && (fl & kFlagNear)) continue;  // k_adj_near
@@ -196,17 +256,23 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const f
     for (int i = 0; i < kQ; ++i) {
       f[i] = src[i * qs + smap[P - a.off_pad[i]]];
       mu[i] = lamY[i * qs + t];
+      lamY[i * qs + t] = 0.f;
     }
-    if (!FLAGS || (fl & kKindMask) == kBulk) {
+    const bool bulk = !FLAGS || (fl & kKindMask) == kBulk;
+    if (bulk) force_grad(mu, gF, a.ncore, t);
+    if (bulk) {
       dom += bgk_vjp(f, a.omega, mu, lam);
     } else {
 #pragma unroll
       for (int i = 0; i < kQ; ++i) lam[i] = mu[i];
     }
     if (FLAGS && (fl & kFlagSave)) {
-      const float* ls = lamS + static_cast<long long>(a.save_idx[t]) * kQ;
+      float* ls = lamS + static_cast<long long>(a.save_idx[t]) * kQ;
 #pragma unroll
-      for (int i = 0; i < kQ; ++i) lam[i] += ls[i];
+      for (int i = 0; i < kQ; ++i) {
+        lam[i] += ls[i];
+        ls[i] = 0.f;
+      }
     }
 #pragma unroll
     for (int i = 0; i < kQ; ++i) atomicAdd(lamX + i * qs + smap[P - a.off_pad[i]], lam[i]);
@@ -214,71 +280,80 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const f
   add_grad(g, kGOmega, dom);
 }
 
-// Near-wall cells (the link rule with host-resolved slots, see k_step_near).
-__global__ void __launch_bounds__(kThreads) k_adj_near(const StepArgs a, const NearTables nt,
-                                                      const float* __restrict__ lamY, float* lamX,
-                                                      const float* __restrict__ lamS, double* g) {
-  const int k = blockIdx.x * kThreads + threadIdx.x;
-  double dom = 0.0;
+// Near-wall cells (the link rule with host-resolved slots, see k_step_near),
+// one warp per cell, lane i on direction i.
+__global__ void __launch_bounds__(kThreads) k_adj_near(const StepArgs a, const NearTables nt, float* __restrict__ lamY,
+                                                      float* lamX, float* __restrict__ lamS, double* g, double* gF) {
+  const int k = (blockIdx.x * kThreads + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  float dom = 0.f;
   if (k < nt.n) {
     const float* src = static_cast<const float*>(a.src);
     const long long qs = a.qs;
+    const LaneDir d = lane_dir(lane);
     const uint32_t t = static_cast<uint32_t>(nt.cells[k]);
     const uint32_t mask = nt.mask[k];
     const uint8_t fl = a.flags[t];
-    float own[kQ], f[kQ], mu[kQ], lam[kQ];
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) {
-      own[i] = src[i * qs + t];
-      f[i] = src[i * qs + nt.slot[i * nt.n + k]];
-      mu[i] = lamY[i * qs + t];
+    const bool link = d.act && ((mask >> lane) & 1u);
+    const int sl = d.act ? nt.slot[lane * nt.n + k] : 0;
+    const float q = d.act ? nt.q[lane * nt.n + k] : 1.f;
+    const float val = d.act ? src[lane * qs + sl] : 0.f;
+    const float own = d.act ? src[lane * qs + t] : 0.f;
+    const float own_opp = __shfl_sync(0xffffffffu, own, d.opp);
+    float f = val;
+    if (link) f = (q < 1.0f ? bouzidi(own_opp, val, own, q) : own_opp) + nt.add[lane * nt.n + k];
+    float mu = 0.f;
+    if (d.act) {
+      mu = lamY[lane * qs + t];
+      lamY[lane * qs + t] = 0.f;
     }
-#pragma unroll
-    for (int i = 1; i < kQ; ++i) {
-      if ((mask >> i) & 1u) {
-        const float q = nt.q[i * nt.n + k];
-        const float v = q < 1.0f ? bouzidi(own[opp(i)], f[i], own[i], q) : own[opp(i)];
-        f[i] = v + nt.add[i * nt.n + k];
-      }
-    }
+    float lam = mu;
     if ((fl & kKindMask) == kBulk) {
-      dom = bgk_vjp(f, a.omega, mu, lam);
-    } else {
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) lam[i] = mu[i];
+      force_grad_lanes(d, mu, gF, a.ncore, t, lane);
+      float fa[kQ];
+      gather_lanes(f, fa);
+      float dh, jx, jy, jz;
+      moments(fa, dh, jx, jy, jz);
+      const float rho = 1.0f + dh, kr = 1.0f / rho;
+      const float ux = jx * kr, uy = jy * kr, uz = jz * kr;
+      const float usq = ux * ux + uy * uy + uz * uz;
+      const float cu = d.cx * ux + d.cy * uy + d.cz * uz;
+      const float feq = d.w * (dh + rho * (3.0f * cu + 4.5f * cu * cu - 1.5f * usq));
+      dom = warp_sum(d.act ? mu * (feq - f) : 0.f);
+      float P, Vx, Vy, Vz;
+      feq_vjp_lanes(d, mu, rho, ux, uy, uz, P, Vx, Vy, Vz);
+      lam = (1.0f - a.omega) * mu + a.omega * (P + (Vx * (d.cx - ux) + Vy * (d.cy - uy) + Vz * (d.cz - uz)) * kr);
     }
-    if (fl & kFlagSave) {
-      const float* ls = lamS + static_cast<long long>(a.save_idx[t]) * kQ;
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) lam[i] += ls[i];
+    if ((fl & kFlagSave) && d.act) {
+      float* ls = lamS + static_cast<long long>(a.save_idx[t]) * kQ + lane;
+      lam += *ls;
+      *ls = 0.f;
     }
-    float down[kQ];
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) down[i] = 0.f;
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) {
-      const long long sl = nt.slot[i * nt.n + k];
-      if (i == 0 || !((mask >> i) & 1u)) {
-        atomicAdd(lamX + i * qs + sl, lam[i]);
-        continue;
-      }
-      const float q = nt.q[i * nt.n + k];
+    // the link rule in reverse: shares to own[opp(i)] (to_opp), own[i]
+    // (to_own) and the value read at the slot (to_val)
+    float to_opp = 0.f, to_own = 0.f, to_val = d.act ? lam : 0.f;
+    if (link) {
+      to_val = 0.f;
       if (q >= 1.0f) {
-        down[opp(i)] += lam[i];
+        to_opp = lam;
       } else if (q >= 0.5f) {
         const float inv2q = 0.5f / q;
-        down[opp(i)] += inv2q * lam[i];
-        atomicAdd(lamX + i * qs + sl, (1.0f - inv2q) * lam[i]);
+        to_opp = inv2q * lam;
+        to_val = (1.0f - inv2q) * lam;
       } else {
-        down[opp(i)] += 2.0f * q * lam[i];
-        down[i] += (1.0f - 2.0f * q) * lam[i];
+        to_opp = 2.0f * q * lam;
+        to_own = (1.0f - 2.0f * q) * lam;
       }
     }
-#pragma unroll
-    for (int j = 0; j < kQ; ++j)
-      if (down[j] != 0.f) atomicAdd(lamX + j * qs + t, down[j]);
+    const float own_total = to_own + __shfl_sync(0xffffffffu, to_opp, d.opp);
+    if (d.act) {
+      if (to_val != 0.f) atomicAdd(lamX + lane * qs + sl, to_val);
+      if (own_total != 0.f) atomicAdd(lamX + lane * qs + t, own_total);
+    }
   }
-  add_grad(g, kGOmega, dom);
+  double v[1] = {lane == 0 ? static_cast<double>(dom) : 0.0};
+  block_reduce<1>(v);
+  if (threadIdx.x == 0 && v[0] != 0.0) atomicAdd(g + kGOmega, v[0]);
 }
 
 // Boundary fills in reverse: the fill target's cotangent moves to its source
@@ -376,91 +451,72 @@ __global__ void __launch_bounds__(kThreads) k_adj_drag(const StepArgs a, const D
     if (down[i] != 0.f) atomicAdd(lamX + i * qs + it.slot, down[i]);
 }
 
-// Prolongation in reverse (half = 1: w = (prev + m) / 2; half = 0: w = m and
-// prev <- m).  The fine target's cotangent (zeroed: it was overwritten)
-// becomes the cotangent of w; lam_m collects d/d m per item, lam_prev is the
-// cotangent of the prev store.
-constexpr int kAdjCouplerThreads = 64;
-__global__ void __launch_bounds__(kAdjCouplerThreads)
+// Prolongation in reverse, one warp per item, lane i on population i
+// (half = 1: w = (prev + m) / 2; half = 0: w = m and prev <- m).  The fine
+// target's cotangent (zeroed: it was overwritten) becomes the cotangent of w;
+// lam_m collects d/d m per item and lam_prev is the cotangent of the prev
+// store (lanes 0..18 own the f_neq components 4 + i, lanes 19..22 the
+// components drho, ux, uy, uz).  The half-time call, the last use of m,
+// also takes m's cotangent through read_macro to the coarse save row.
+__global__ void __launch_bounds__(kThreads)
 k_adj_prolong(const ProlongItem* items, int nitems, const float* coarse_save, const float* prev, int half,
-              float* lam_fine, long long fine_qs, float s, float omega, float* lam_m, float* lam_prev, double* g) {
-  const int t = blockIdx.x * kAdjCouplerThreads + threadIdx.x;
+              float* lam_fine, long long fine_qs, float s, float omega, float* lam_m, float* lam_prev,
+              float* lam_save, double* g, double* gF_fine, long long fine_ncore) {
+  const int w = (blockIdx.x * kThreads + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   float ds = 0.f, dom = 0.f;
-  if (t < nitems) {
-    const ProlongItem it = items[t];
-    Macro m, w;
-    load_macro_row(coarse_save + static_cast<long long>(it.coarse_save) * kQ, m);
-    w = m;
+  if (w < nitems) {
+    const ProlongItem it = items[w];
+    const LaneDir d = lane_dir(lane);
+    const float* row = coarse_save + static_cast<long long>(it.coarse_save) * kQ;
+    const float f = d.act ? row[lane] : 0.f;
+    float drho, ux, uy, uz, fneq;
+    read_macro_lanes(d, f, drho, ux, uy, uz, fneq);
+    float* pv = const_cast<float*>(prev) + static_cast<long long>(it.prev) * 23;
+    float wd = drho, wx = ux, wy = uy, wz = uz, wf_ = fneq;
     if (half) {
-      const float* pv = prev + static_cast<long long>(it.prev) * 23;
-      w.drho = 0.5f * (pv[0] + m.drho);
-      w.ux = 0.5f * (pv[1] + m.ux); w.uy = 0.5f * (pv[2] + m.uy); w.uz = 0.5f * (pv[3] + m.uz);
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) w.fneq[i] = 0.5f * (pv[4 + i] + m.fneq[i]);
+      wd = 0.5f * (pv[0] + drho); wx = 0.5f * (pv[1] + ux); wy = 0.5f * (pv[2] + uy); wz = 0.5f * (pv[3] + uz);
+      wf_ = d.act ? 0.5f * (pv[4 + lane] + fneq) : 0.f;
     }
-    float mu[kQ];
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) {
-      float* p = lam_fine + i * fine_qs + it.fine_slot;
-      mu[i] = *p;
+    float mu = 0.f;
+    if (d.act) {
+      float* p = lam_fine + lane * fine_qs + it.fine_slot;
+      mu = *p;
       *p = 0.f;
     }
-    Macro lw;
-    write_vjp(w, s, it.fine_kind, omega, mu, lw, ds, dom);
-    float* lm = lam_m + static_cast<long long>(t) * 23;
+    if (it.fine_kind == kBulk) force_grad_lanes(d, mu, gF_fine, fine_ncore, it.fine_slot, lane);
+    float lfneq, ldrho, lux, luy, luz;
+    write_vjp_lanes(d, wd, wx, wy, wz, wf_, s, it.fine_kind, omega, mu, lfneq, ldrho, lux, luy, luz, ds, dom);
+    // the component this lane owns
+    const int comp = lane < kQ ? 4 + lane : (lane < kQ + 4 ? lane - kQ : -1);
+    const float lw = lane < kQ ? lfneq : (lane == kQ ? ldrho : (lane == kQ + 1 ? lux : (lane == kQ + 2 ? luy : luz)));
+    float* lm = lam_m + static_cast<long long>(w) * 23;
     float* lp = lam_prev + static_cast<long long>(it.prev) * 23;
-    const float lwv[23] = {lw.drho, lw.ux, lw.uy, lw.uz, lw.fneq[0], lw.fneq[1], lw.fneq[2], lw.fneq[3],
-                           lw.fneq[4], lw.fneq[5], lw.fneq[6], lw.fneq[7], lw.fneq[8], lw.fneq[9], lw.fneq[10],
-                           lw.fneq[11], lw.fneq[12], lw.fneq[13], lw.fneq[14], lw.fneq[15], lw.fneq[16],
-                           lw.fneq[17], lw.fneq[18]};
-    if (half) {
-#pragma unroll
-      for (int k = 0; k < 23; ++k) {
-        lm[k] += 0.5f * lwv[k];
-        lp[k] += 0.5f * lwv[k];
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < 23; ++k) {
-        lm[k] += lwv[k] + lp[k];
-        lp[k] = 0.f;
+    float total = 0.f;
+    if (comp >= 0) {
+      if (half) {
+        total = lm[comp] + 0.5f * lw;
+        lp[comp] += 0.5f * lw;
+        lm[comp] = 0.f;
+      } else {
+        lm[comp] += lw + lp[comp];
+        lp[comp] = 0.f;
       }
     }
+    if (half) {
+      // cotangent of m -> coarse save row
+      const float tdrho = __shfl_sync(0xffffffffu, total, kQ), tux = __shfl_sync(0xffffffffu, total, kQ + 1);
+      const float tuy = __shfl_sync(0xffffffffu, total, kQ + 2), tuz = __shfl_sync(0xffffffffu, total, kQ + 3);
+      const float lf = read_vjp_lanes(d, f, tdrho, tux, tuy, tuz, d.act ? total : 0.f);
+      if (d.act) atomicAdd(lam_save + static_cast<long long>(it.coarse_save) * kQ + lane, lf);
+    }
   }
-  double a2[2] = {static_cast<double>(dom), static_cast<double>(ds)};
-  __shared__ double sm[kAdjCouplerThreads / 32][2];
-  for (int k = 0; k < 2; ++k)
-    for (int o = 16; o > 0; o >>= 1) a2[k] += __shfl_down_sync(0xffffffffu, a2[k], o);
-  if ((threadIdx.x & 31) == 0) { sm[threadIdx.x >> 5][0] = a2[0]; sm[threadIdx.x >> 5][1] = a2[1]; }
-  __syncthreads();
+  double a2[2] = {lane == 0 ? static_cast<double>(dom) : 0.0, lane == 0 ? static_cast<double>(ds) : 0.0};
+  block_reduce<2>(a2);
   if (threadIdx.x == 0) {
-    double d0 = 0.0, d1 = 0.0;
-    for (int w = 0; w < kAdjCouplerThreads / 32; ++w) { d0 += sm[w][0]; d1 += sm[w][1]; }
-    if (d0 != 0.0) atomicAdd(g + kGOmega, d0);
-    if (d1 != 0.0) atomicAdd(g + kGProlongScale, d1);
+    if (a2[0] != 0.0) atomicAdd(g + kGOmega, a2[0]);
+    if (a2[1] != 0.0) atomicAdd(g + kGProlongScale, a2[1]);
   }
-}
-
-// Cotangent of the coarse macro states (lam_m per prolongation item) -> the
-// coarse save rows; lam_m is cleared for the next coarse step.
-__global__ void __launch_bounds__(kAdjCouplerThreads)
-k_adj_read_macro(const ProlongItem* items, int nitems, const float* coarse_save, float* lam_m, float* lam_save) {
-  const int t = blockIdx.x * kAdjCouplerThreads + threadIdx.x;
-  if (t >= nitems) return;
-  const ProlongItem it = items[t];
-  float* lmv = lam_m + static_cast<long long>(t) * 23;
-  Macro lm;
-  macro_from23(lmv, lm);
-#pragma unroll
-  for (int k = 0; k < 23; ++k) lmv[k] = 0.f;
-  const float* row = coarse_save + static_cast<long long>(it.coarse_save) * kQ;
-  float f[kQ], lf[kQ];
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) f[i] = row[i];
-  read_vjp(f, lm, lf);
-  float* ls = lam_save + static_cast<long long>(it.coarse_save) * kQ;
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) atomicAdd(ls + i, lf[i]);
 }
 
 // Restriction in reverse, one warp per item as forward: lane 0 recomputes the
@@ -468,7 +524,7 @@ k_adj_read_macro(const ProlongItem* items, int nitems, const float* coarse_save,
 // macro cotangent to the fine centre row and the f_neq average to every row.
 __global__ void __launch_bounds__(kThreads)
 k_adj_restrict(const RestrictItem* items, int nitems, const float* fine_save, float* lam_coarse, long long coarse_qs,
-               float s, float omega, float* lam_save, double* g) {
+               float s, float omega, float* lam_save, double* g, double* gF_coarse, long long coarse_ncore) {
   const int w = (blockIdx.x * kThreads + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   float ds = 0.f, dom = 0.f;
@@ -490,30 +546,33 @@ k_adj_restrict(const RestrictItem* items, int nitems, const float* fine_save, fl
       sum[i] = v;
     }
     const float inv = 1.0f / static_cast<float>(it.nnb + 1);
-    Macro lr;
-    if (lane == 0) {
-      Macro r;
-      r.drho = m.drho; r.ux = m.ux; r.uy = m.uy; r.uz = m.uz;
+    // r = (centre drho, u; f_neq average) spread over the lanes
+    const LaneDir d = lane_dir(lane);
+    float rf = 0.f;
 #pragma unroll
-      for (int i = 0; i < kQ; ++i) r.fneq[i] = sum[i] * inv;
-      float mu[kQ];
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) {
-        float* p = lam_coarse + i * coarse_qs + it.coarse_slot;
-        mu[i] = *p;
-        *p = 0.f;
-      }
-      write_vjp(r, s, it.coarse_kind, omega, mu, lr, ds, dom);
+    for (int i = 0; i < kQ; ++i) {
+      const float v = __shfl_sync(0xffffffffu, sum[i], 0) * inv;
+      if (lane == i) rf = v;
     }
-    // broadcast the cotangent of r
+    const float rd = __shfl_sync(0xffffffffu, m.drho, 0), rx = __shfl_sync(0xffffffffu, m.ux, 0);
+    const float ry = __shfl_sync(0xffffffffu, m.uy, 0), rz = __shfl_sync(0xffffffffu, m.uz, 0);
+    float mu = 0.f;
+    if (d.act) {
+      float* p = lam_coarse + lane * coarse_qs + it.coarse_slot;
+      mu = *p;
+      *p = 0.f;
+    }
+    if (it.coarse_kind == kBulk) force_grad_lanes(d, mu, gF_coarse, coarse_ncore, it.coarse_slot, lane);
+    float lfneq, ldrho, lux, luy, luz;
+    write_vjp_lanes(d, rd, rx, ry, rz, rf, s, it.coarse_kind, omega, mu, lfneq, ldrho, lux, luy, luz, ds, dom);
+    // row k's cotangent: f_neq part inv * lfneq (all rows), drho / u (centre)
     Macro lm;
-    lm.drho = __shfl_sync(0xffffffffu, lr.drho, 0);
-    lm.ux = __shfl_sync(0xffffffffu, lr.ux, 0);
-    lm.uy = __shfl_sync(0xffffffffu, lr.uy, 0);
-    lm.uz = __shfl_sync(0xffffffffu, lr.uz, 0);
+    lm.drho = lane == 0 ? ldrho : 0.f;
+    lm.ux = lane == 0 ? lux : 0.f;
+    lm.uy = lane == 0 ? luy : 0.f;
+    lm.uz = lane == 0 ? luz : 0.f;
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) lm.fneq[i] = __shfl_sync(0xffffffffu, lr.fneq[i], 0) * inv;
-    if (lane != 0) { lm.drho = 0.f; lm.ux = 0.f; lm.uy = 0.f; lm.uz = 0.f; }
+    for (int i = 0; i < kQ; ++i) lm.fneq[i] = __shfl_sync(0xffffffffu, lfneq, i) * inv;
     if (row >= 0) {
       float lf[kQ];
       read_vjp(f, lm, lf);
@@ -522,7 +581,7 @@ k_adj_restrict(const RestrictItem* items, int nitems, const float* fine_save, fl
       for (int i = 0; i < kQ; ++i) atomicAdd(ls + i, lf[i]);
     }
   }
-  double a2[2] = {static_cast<double>(dom), static_cast<double>(ds)};
+  double a2[2] = {lane == 0 ? static_cast<double>(dom) : 0.0, lane == 0 ? static_cast<double>(ds) : 0.0};
   block_reduce<2>(a2);
   if (threadIdx.x == 0) {
     if (a2[0] != 0.0) atomicAdd(g + kGOmega, a2[0]);
@@ -535,19 +594,19 @@ inline uint32_t grid_of(long long items, int threads) { return static_cast<uint3
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
-cudaError_t launch_adj_step(const StepArgs& a, bool links, bool flags, const float* lamY, float* lamX,
-                            const float* lamS, double* g, cudaStream_t s) {
-  const dim3 grid(static_cast<uint32_t>(a.nblk) + grid_of(a.n_open, kThreads));
+cudaError_t launch_adj_step(const StepArgs& a, bool links, bool flags, float* lamY, float* lamX, float* lamS,
+                            double* g, double* gF, cudaStream_t s) {
+  const dim3 grid(static_cast<uint32_t>(a.nblk) * 2 + grid_of(a.n_open, kThreads));
   const size_t smem = static_cast<size_t>(a.np) * a.np * a.np * sizeof(int);
-  if (links) k_adj_step<true, true><<<grid, kThreads, smem, s>>>(a, lamY, lamX, lamS, g);
-  else if (flags) k_adj_step<false, true><<<grid, kThreads, smem, s>>>(a, lamY, lamX, lamS, g);
-  else k_adj_step<false, false><<<grid, kThreads, smem, s>>>(a, lamY, lamX, lamS, g);
+  if (links) k_adj_step<true, true><<<grid, kThreads, smem, s>>>(a, lamY, lamX, lamS, g, gF);
+  else if (flags) k_adj_step<false, true><<<grid, kThreads, smem, s>>>(a, lamY, lamX, lamS, g, gF);
+  else k_adj_step<false, false><<<grid, kThreads, smem, s>>>(a, lamY, lamX, lamS, g, gF);
   return cudaGetLastError();
 }
-cudaError_t launch_adj_near(const StepArgs& a, const NearTables& nt, const float* lamY, float* lamX, const float* lamS,
-                            double* g, cudaStream_t s) {
+cudaError_t launch_adj_near(const StepArgs& a, const NearTables& nt, float* lamY, float* lamX, float* lamS,
+                            double* g, double* gF, cudaStream_t s) {
   if (nt.n == 0) return cudaSuccess;
-  k_adj_near<<<grid_of(nt.n, kThreads), kThreads, 0, s>>>(a, nt, lamY, lamX, lamS, g);
+  k_adj_near<<<grid_of(static_cast<long long>(nt.n) * 32, kThreads), kThreads, 0, s>>>(a, nt, lamY, lamX, lamS, g, gF);
   return cudaGetLastError();
 }
 cudaError_t launch_adj_ghost(float* lam, long long qs, const BBOp* bb, uint32_t nbb, double* g, cudaStream_t s) {
@@ -569,25 +628,20 @@ cudaError_t launch_adj_drag(const StepArgs& a, bool links, const DragItem* items
 }
 cudaError_t launch_adj_prolong(const ProlongItem* items, int n, const float* coarse_save, const float* prev, int half,
                                float* lam_fine, long long fine_qs, float scale, float omega, float* lam_m,
-                               float* lam_prev, double* g, cudaStream_t s) {
+                               float* lam_prev, float* lam_save, double* g, double* gF_fine, long long fine_ncore,
+                               cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_adj_prolong<<<grid_of(n, kAdjCouplerThreads), kAdjCouplerThreads, 0, s>>>(
-      items, n, coarse_save, prev, half, lam_fine, fine_qs, scale, omega, lam_m, lam_prev, g);
-  return cudaGetLastError();
-}
-cudaError_t launch_adj_read_macro(const ProlongItem* items, int n, const float* coarse_save, float* lam_m,
-                                  float* lam_save, cudaStream_t s) {
-  if (n == 0) return cudaSuccess;
-  k_adj_read_macro<<<grid_of(n, kAdjCouplerThreads), kAdjCouplerThreads, 0, s>>>(items, n, coarse_save, lam_m,
-                                                                                  lam_save);
+  k_adj_prolong<<<grid_of(static_cast<long long>(n) * 32, kThreads), kThreads, 0, s>>>(
+      items, n, coarse_save, prev, half, lam_fine, fine_qs, scale, omega, lam_m, lam_prev, lam_save, g, gF_fine,
+      fine_ncore);
   return cudaGetLastError();
 }
 cudaError_t launch_adj_restrict(const RestrictItem* items, int n, const float* fine_save, float* lam_coarse,
                                 long long coarse_qs, float scale, float omega, float* lam_save, double* g,
-                                cudaStream_t s) {
+                                double* gF_coarse, long long coarse_ncore, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   k_adj_restrict<<<grid_of(static_cast<long long>(n) * 32, kThreads), kThreads, 0, s>>>(
-      items, n, fine_save, lam_coarse, coarse_qs, scale, omega, lam_save, g);
+      items, n, fine_save, lam_coarse, coarse_qs, scale, omega, lam_save, g, gF_coarse, coarse_ncore);
   return cudaGetLastError();
 }
 

@@ -83,6 +83,62 @@ __device__ __forceinline__ void rotate_slots(const StepArgs& a, uint32_t k, long
   dst = a.halo_base + static_cast<long long>(it.x) * a.n_halo + it.z;
 }
 
+// Lane-parallel forms (lane i < 19 holds population i): lattice vectors and
+// weights by runtime index, packed 2 bits per component.
+constexpr uint64_t pack_c(int a) {
+  uint64_t v = 0;
+  for (int i = 0; i < kQ; ++i) v |= static_cast<uint64_t>((a == 0 ? cx(i) : (a == 1 ? cy(i) : cz(i))) + 1) << (2 * i);
+  return v;
+}
+constexpr uint64_t kPackCx = pack_c(0), kPackCy = pack_c(1), kPackCz = pack_c(2);
+struct LaneDir {
+  float cx, cy, cz, w;
+  int opp;
+  bool act;
+};
+__device__ __forceinline__ LaneDir lane_dir(int lane) {
+  LaneDir d;
+  d.act = lane < kQ;
+  const int i = d.act ? lane : 0;
+  const int x = static_cast<int>((kPackCx >> (2 * i)) & 3u) - 1;
+  const int y = static_cast<int>((kPackCy >> (2 * i)) & 3u) - 1;
+  const int z = static_cast<int>((kPackCz >> (2 * i)) & 3u) - 1;
+  d.cx = static_cast<float>(x);
+  d.cy = static_cast<float>(y);
+  d.cz = static_cast<float>(z);
+  const int nn = x * x + y * y + z * z;
+  d.w = d.act ? (nn == 0 ? 1.0f / 3.0f : (nn == 1 ? 1.0f / 18.0f : 1.0f / 36.0f)) : 0.f;
+  d.opp = d.act ? opp(i) : lane;
+  return d;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Every lane gets the 19 values held by lanes 0..18.
+__device__ __forceinline__ void gather_lanes(float v, float (&all)[kQ]) {
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) all[i] = __shfl_sync(0xffffffffu, v, i);
+}
+
+// BGK (unit scale) of population i = lane from the gathered pre-collision
+// populations: the same operations and rounding as bgk() for direction i.
+__device__ __forceinline__ float bgk_lane(const LaneDir& d, int lane, const float (&fa)[kQ], float f, float omega) {
+  float dh, jx, jy, jz;
+  moments(fa, dh, jx, jy, jz);
+  const float rho = 1.0f + dh * 1.0f;
+  const float k = 1.0f / rho;
+  const float ux = jx * k, uy = jy * k, uz = jz * k;
+  const float A = 1.0f * rho;
+  const float a3 = 3.0f * A, b45 = 4.5f * A;
+  const float c0 = dh - 1.5f * A * (ux * ux + uy * uy + uz * uz);
+  const float cu = (d.cx != 0.f ? d.cx * ux : 0.f) + (d.cy != 0.f ? d.cy * uy : 0.f) + (d.cz != 0.f ? d.cz * uz : 0.f);
+  const float t = lane == 0 ? c0 : fmaf(cu, fmaf(b45, cu, a3), c0);
+  return fmaf(omega, fmaf(d.w, t, -f), f);
+}
+
 // Macro state (rho - 1, u, f_neq) of saved pre-collision populations
 // (LevelCoupler::ReadMacro, level_coupler.cpp:183-189).
 struct Macro {

@@ -131,43 +131,35 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
 // direction i reads population i at nt.slot[i] and, where the rule applies,
 // reflects own[opp(i)] (half-way bounce-back, reflect-on-pull at the block
 // edge) or interpolates with Bouzidi (bouzidi_pull.h:8-26), then adds the
-// moving-wall term.  Then the same save / collide / store as k_step.
-constexpr int kNearThreads = 64;
+// moving-wall term.  Then the same save / collide / store as k_step.  One
+// warp per cell, lane i on direction i; the collision gathers the 19 values
+// so every lane computes the moments exactly as bgk() does.
 template <typename T>
-__global__ void __launch_bounds__(kNearThreads) k_step_near(const StepArgs a, const NearTables nt) {
-  const int k = blockIdx.x * kNearThreads + threadIdx.x;
+__global__ void __launch_bounds__(kThreads) k_step_near(const StepArgs a, const NearTables nt) {
+  const int k = (blockIdx.x * kThreads + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (k >= nt.n) return;
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
+  const LaneDir d = lane_dir(lane);
   const uint32_t t = static_cast<uint32_t>(nt.cells[k]);
   const uint32_t mask = nt.mask[k];
   const uint8_t fl = a.flags[t];
-  int sl[kQ];
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) sl[i] = nt.slot[i * nt.n + k];
+  const int sl = d.act ? nt.slot[lane * nt.n + k] : 0;
+  const float q = d.act ? nt.q[lane * nt.n + k] : 1.f, add = d.act ? nt.add[lane * nt.n + k] : 0.f;
   pdl_wait();
-  float f[kQ], own[kQ];
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    f[i] = LD(src, a.qs, i, sl[i], a.inv_scale);
-    own[i] = LD(src, a.qs, i, t, a.inv_scale);
+  const float val = d.act ? LD(src, a.qs, lane, sl, a.inv_scale) : 0.f;
+  const float own = d.act ? LD(src, a.qs, lane, t, a.inv_scale) : 0.f;
+  const float own_opp = __shfl_sync(0xffffffffu, own, d.opp);
+  float f = val;
+  if (d.act && ((mask >> lane) & 1u)) f = (q < 1.0f ? bouzidi(own_opp, val, own, q) : own_opp) + add;
+  if ((fl & kFlagSave) && d.act) a.save_buf[static_cast<long long>(a.save_idx[t]) * kQ + lane] = f;
+  if ((fl & kKindMask) == kBulk) {
+    float fa[kQ];
+    gather_lanes(f, fa);
+    f = bgk_lane(d, lane, fa, f, a.omega);
   }
-#pragma unroll
-  for (int i = 1; i < kQ; ++i) {
-    if ((mask >> i) & 1u) {
-      const float q = nt.q[i * nt.n + k];
-      const float v = q < 1.0f ? bouzidi(own[opp(i)], f[i], own[i], q) : own[opp(i)];
-      f[i] = v + nt.add[i * nt.n + k];
-    }
-  }
-  if (fl & kFlagSave) {
-    float* sv = a.save_buf + static_cast<long long>(a.save_idx[t]) * kQ;
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) sv[i] = f[i];
-  }
-  if ((fl & kKindMask) == kBulk) bgk(f, a.omega);
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + t, f[i], a.scale);
+  if (d.act) Store<T>::st(dst + lane * a.qs + t, f, a.scale);
 }
 
 // Two-element vector access for the paired periodic kernel.
@@ -233,13 +225,16 @@ __device__ __forceinline__ void map_cell_finish(const StepArgs& a, uint32_t t, u
   for (int i = 0; i < kQ; ++i) Store<T>::st(dst + (static_cast<uint32_t>(i) * qs + t), f[i], a.scale);
 }
 
+// With one cell per thread (CPT = 1) two CTAs share a block, each over half
+// its cells, so small levels still give every SM work.
 template <typename T, bool LINKS, bool FLAGS, int CPT>
 __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const StepArgs a) {
   extern __shared__ int smap[];  // (n+2)^3 slots of this block
-  const uint32_t b = blockIdx.x;
+  constexpr uint32_t kParts = CPT == 1 ? 2 : 1;
+  const uint32_t b = blockIdx.x / kParts, part = blockIdx.x % kParts;
   if (b >= static_cast<uint32_t>(a.nblk)) {
     pdl_wait();
-    rotate_item<T>(a, (b - a.nblk) * kThreads + threadIdx.x);
+    rotate_item<T>(a, (blockIdx.x - a.nblk * kParts) * kThreads + threadIdx.x);
     return;
   }
   const int np = a.np, np3 = np * np * np;
@@ -250,7 +245,8 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
   const uint32_t n = a.n, n3 = n * n * n, qs = static_cast<uint32_t>(a.qs);
-  for (uint32_t tl0 = threadIdx.x; tl0 < n3; tl0 += CPT * kThreads) {
+  const uint32_t span = n3 / kParts;
+  for (uint32_t tl0 = part * span + threadIdx.x; tl0 < (part + 1) * span; tl0 += CPT * kThreads) {
     uint32_t t[CPT];
     int P[CPT];
     uint8_t fl[CPT];
@@ -653,7 +649,7 @@ template <typename T>
 cudaError_t launch_step_map(const StepArgs& a, bool links, bool flags, int cpt, cudaStream_t s) {
   cudaError_t e = cudaSuccess;
   if (a.nitems == 0) return cudaSuccess;
-  const dim3 g(static_cast<uint32_t>(a.nblk) + grid_for(static_cast<uint32_t>(a.n_open)));
+  const dim3 g(static_cast<uint32_t>(a.nblk) * (cpt == 2 ? 1 : 2) + grid_for(static_cast<uint32_t>(a.n_open)));
   const size_t smem = static_cast<size_t>(a.np) * a.np * a.np * sizeof(int);
   if (cpt == 2) {
     if (links) e = launch_chain(k_step_map<T, true, true, 2>, dim3(g), dim3(kThreads), smem, s, a);
@@ -670,7 +666,7 @@ cudaError_t launch_step_map(const StepArgs& a, bool links, bool flags, int cpt, 
 template <typename T>
 cudaError_t launch_step_near(const StepArgs& a, const NearTables& nt, cudaStream_t s) {
   if (nt.n == 0) return cudaSuccess;
-  const cudaError_t e = launch_chain(k_step_near<T>, dim3((nt.n + kNearThreads - 1) / kNearThreads), dim3(kNearThreads), 0, s, a, nt);
+  const cudaError_t e = launch_chain(k_step_near<T>, dim3(grid_for(static_cast<uint32_t>(nt.n) * 32)), dim3(kThreads), 0, s, a, nt);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 

@@ -3,6 +3,7 @@
 // reference's recursive subcycling (TimeLoop::advance, time_loop.h:201-240) as
 // a sequence of kernel launches on one stream.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -43,17 +44,16 @@ template <typename T> cudaError_t launch_step_map(const StepArgs&, bool, bool, i
 bool pair_step_eligible(int n);
 bool map_step_eligible(int n, long long nslots);
 void set_programmatic_launch(bool on);
-cudaError_t launch_adj_step(const StepArgs&, bool, bool, const float*, float*, const float*, double*, cudaStream_t);
-cudaError_t launch_adj_near(const StepArgs&, const NearTables&, const float*, float*, const float*, double*,
+cudaError_t launch_adj_step(const StepArgs&, bool, bool, float*, float*, float*, double*, double*, cudaStream_t);
+cudaError_t launch_adj_near(const StepArgs&, const NearTables&, float*, float*, float*, double*, double*,
                             cudaStream_t);
 cudaError_t launch_adj_ghost(float*, long long, const BBOp*, uint32_t, double*, cudaStream_t);
 cudaError_t launch_adj_force(const StepArgs&, const float*, double*, cudaStream_t);
 cudaError_t launch_adj_drag(const StepArgs&, bool, const DragItem*, int, float*, float, int, cudaStream_t);
 cudaError_t launch_adj_prolong(const ProlongItem*, int, const float*, const float*, int, float*, long long, float,
-                               float, float*, float*, double*, cudaStream_t);
-cudaError_t launch_adj_read_macro(const ProlongItem*, int, const float*, float*, float*, cudaStream_t);
+                               float, float*, float*, float*, double*, double*, long long, cudaStream_t);
 cudaError_t launch_adj_restrict(const RestrictItem*, int, const float*, float*, long long, float, float, float*,
-                                double*, cudaStream_t);
+                                double*, double*, long long, cudaStream_t);
 bool bulk_step_eligible(int n, int elem_bytes);
 uint32_t drag_partials(int n);
 uint32_t audit_partials(const StepArgs& a);
@@ -127,8 +127,15 @@ struct Level {
   int bulk_grid = 0;
   DevBuf body_force;                // [3][ncore] float, or empty
   bool has_force = false;
+  // While the adjoint recomputes a segment, the level's state and save rows
+  // live in the step records' buffers (null otherwise).
+  void* rec_cur = nullptr;
+  void* rec_save = nullptr;
   StepArgs args{};
 };
+
+inline void* cur_buf(Level& L) { return L.rec_cur ? L.rec_cur : L.buf[L.cur].p; }
+inline float* save_ptr(Level& L) { return static_cast<float*>(L.rec_save ? L.rec_save : L.save_buf.p); }
 
 // Forward state of one level step kept for the reverse sweep: the step's
 // input after the body force and the boundary fills, the save rows it wrote,
@@ -151,6 +158,8 @@ struct AdjointState {
   };
   std::vector<Lv> lv;
   std::vector<StepRecord> recs;
+  std::vector<int> next_same;       // next record of the same level in the pool, or -1
+  std::vector<int> first_rec;       // first record of each level in the pool, or -1
   size_t nrec = 0;
   bool recording = false;
   int last_rec[32] = {};
@@ -161,6 +170,24 @@ struct AdjointState {
   };
   std::vector<Checkpoint> ck;
   int comp = 0;
+  // Recomputation (kind 0) and reverse (kind 1) of one segment captured as
+  // CUDA graphs, keyed by (kind, buffer or cotangent parity, steps, steps in
+  // the objective's window); valid for one adjoint call.
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t out_mask = 0;
+  };
+  std::map<std::array<long long, 4>, Graph> graphs;
+  std::array<long long, 4> graph_params{};  // (steps, window, interval, component) the graphs were made for
+  void clear_graphs() {
+    for (auto& kv : graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    graphs.clear();
+  }
+  AdjointState() = default;
+  AdjointState(const AdjointState&) = delete;
+  AdjointState& operator=(const AdjointState&) = delete;
+  ~AdjointState() { clear_graphs(); }
 };
 
 }  // namespace
@@ -279,24 +306,31 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
   // Body force on the stored post-collision state, then the ghost fill into
   // the buffer the step reads (reference: apply() then exchange() after
   // collide, time_loop.h:207-211).
-  if (L.has_force) CK(launch_add_force<T>(L.args, L.buf[L.cur].as<T>(), L.body_force.as<float>(), ctx->stream));
-  CK(launch_ghost<T>(L.buf[L.cur].as<T>(), L.nslots, nullptr, nullptr, 0, 0, L.bb_ops.as<BBOp>(), L.n_bb,
-                     L.scale, L.inv_scale, ctx->stream));
+  T* cur = static_cast<T*>(cur_buf(L));
+  if (L.has_force) CK(launch_add_force<T>(L.args, cur, L.body_force.as<float>(), ctx->stream));
+  CK(launch_ghost<T>(cur, L.nslots, nullptr, nullptr, 0, 0, L.bb_ops.as<BBOp>(), L.n_bb, L.scale, L.inv_scale,
+                     ctx->stream));
   StepArgs a = L.args;
-  a.src = L.buf[L.cur].p;
+  a.src = cur;
   a.dst = L.buf[1 - L.cur].p;
   StepRecord* rec = nullptr;
+  void* next_cur = nullptr;
   if (ctx->adj && ctx->adj->recording) {
+    // Record the step: its input buffer is the record's (the previous step
+    // of the level wrote there, or the segment's checkpoint was restored
+    // there), its output goes to the next record of the level, its save rows
+    // to the record's.
     AdjointState& A = *ctx->adj;
-    if (A.nrec == A.recs.size()) A.recs.emplace_back();
+    if (A.nrec >= A.recs.size() || A.recs[A.nrec].level != L.lvl)
+      return fail(ctx, OCTLB_ESTATE, "adjoint: step record pool out of order");
     rec = &A.recs[A.nrec];
-    if (rec->level != L.lvl) {
-      CK(rec->snap.alloc(static_cast<size_t>(L.nslots) * kQ * sizeof(T)));
-      CK(rec->save.alloc(static_cast<size_t>(L.n_save) * kQ * sizeof(float)));
-      CK(rec->prev.alloc(L.n_prolong > 0 ? L.prev.bytes : 0));  // rows indexed by coupling point
-      rec->level = L.lvl;
-    }
-    CK(cudaMemcpyAsync(rec->snap.p, a.src, rec->snap.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (rec->snap.p != a.src)
+      CK(cudaMemcpyAsync(rec->snap.p, a.src, rec->snap.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    a.src = rec->snap.p;
+    const int nx = A.next_same[A.nrec];
+    if (nx >= 0) a.dst = next_cur = A.recs[nx].snap.p;
+    a.save_buf = rec->save.as<float>();
+    L.rec_save = rec->save.p;
     rec->drag = ctx->drag && L.n_drag > 0 && L.substep + 1 == (1 << L.lvl);
     A.last_rec[L.lvl] = static_cast<int>(A.nrec++);
   }
@@ -312,16 +346,16 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
                       ctx->stream));
     CK(launch_step_near<T>(a, L.near, ctx->stream));
   }
-  if (rec && L.n_save > 0)
-    CK(cudaMemcpyAsync(rec->save.p, L.save_buf.p, rec->save.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
   // The force after advance_one reads each level's last step (the reference
   // computes MomentumExchangeDrag once, after advance_one): skip the others.
   ++L.substep;
-  if (ctx->drag && L.n_drag > 0 && L.substep == (1 << L.lvl)) {
+  // (The adjoint's recomputation needs no force: it records the inputs.)
+  if (ctx->drag && L.n_drag > 0 && L.substep == (1 << L.lvl) && !rec) {
     CK(launch_drag<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.drag_items.as<DragItem>(), L.n_drag,
                       ctx->drag_partial.as<double>() + 3 * L.drag_off, ctx->stream));
   }
   L.cur = 1 - L.cur;
+  if (rec) L.rec_cur = next_cur;
   return OCTLB_OK;
 }
 
@@ -342,16 +376,16 @@ int do_advance_level(octlb_ctx* ctx, int l) {
   // -> restrict(l+1)  (time_loop.h:228-239)
   for (int phase = 0; phase < 2; ++phase) {
     if (L.n_prolong > 0) {
-      CK(launch_prolong<T>(L.prolong_items.as<ProlongItem>(), L.n_prolong, L.save_buf.as<float>(),
-                           L.prev.as<float>(), phase == 0 ? 1 : 0, F.buf[F.cur].as<T>(), F.nslots,
+      CK(launch_prolong<T>(L.prolong_items.as<ProlongItem>(), L.n_prolong, save_ptr(L),
+                           L.prev.as<float>(), phase == 0 ? 1 : 0, static_cast<T*>(cur_buf(F)), F.nslots,
                            ctx->prolong_scale, static_cast<float>(ctx->omega), F.scale, ctx->stream));
     }
     rc = do_advance_level<T>(ctx, l + 1);
     if (rc) return rc;
   }
   if (F.n_restrict > 0) {
-    CK(launch_restrict<T>(F.restrict_items.as<RestrictItem>(), F.n_restrict, F.save_buf.as<float>(),
-                          L.buf[L.cur].as<T>(), L.nslots, ctx->restrict_scale,
+    CK(launch_restrict<T>(F.restrict_items.as<RestrictItem>(), F.n_restrict, save_ptr(F),
+                          static_cast<T*>(cur_buf(L)), L.nslots, ctx->restrict_scale,
                           static_cast<float>(ctx->omega), L.scale, ctx->stream));
   }
   return OCTLB_OK;
@@ -1183,7 +1217,7 @@ int advance_one_launches(octlb_ctx* ctx) {
   for (auto& L : ctx->levels) L.substep = 0;
   int rc = do_advance_level<T>(ctx, 0);
   if (rc) return rc;
-  if (ctx->drag && ctx->drag_parts > 0) {
+  if (ctx->drag && ctx->drag_parts > 0 && !(ctx->adj && ctx->adj->recording)) {
     CK(launch_drag_total(ctx->drag_partial.as<double>(), ctx->drag_parts, ctx->force.as<double>(),
                          ctx->force_sum.as<double>(), ctx->stream));
   }
@@ -1274,14 +1308,17 @@ int adj_step(octlb_ctx* ctx, int l, const StepRecord& R, float coef) {
   float* lamY = V.lam[V.cur].as<float>();
   float* lamX = V.lam[1 - V.cur].as<float>();
   double* g = A.g.as<double>();
-  CK(cudaMemsetAsync(lamX, 0, V.lam[1 - V.cur].bytes, ctx->stream));
-  CK(launch_adj_step(a, links, L.has_flags, lamY, lamX, V.lam_save.as<float>(), g, ctx->stream));
-  CK(launch_adj_near(a, L.near, lamY, lamX, V.lam_save.as<float>(), g, ctx->stream));
+  // lamX starts zeroed: the adjoint kernels clear every cotangent entry they
+  // consume (lamY, the save rows, the coupler targets), so each buffer is
+  // back to zero when it becomes the accumulator again.  The body-force
+  // gradient of the state this step read is taken where its cotangent is
+  // consumed (the previous step's k_adj_step / k_adj_near, the coupler
+  // kernels for their targets, and a final pass for the initial state).
+  CK(launch_adj_step(a, links, L.has_flags, lamY, lamX, V.lam_save.as<float>(), g, V.gF.as<double>(), ctx->stream));
+  CK(launch_adj_near(a, L.near, lamY, lamX, V.lam_save.as<float>(), g, V.gF.as<double>(), ctx->stream));
   if (R.drag && coef != 0.f)
     CK(launch_adj_drag(a, links, L.drag_items.as<DragItem>(), L.n_drag, lamX, coef, A.comp, ctx->stream));
-  if (L.n_save > 0) CK(cudaMemsetAsync(V.lam_save.p, 0, V.lam_save.bytes, ctx->stream));
   CK(launch_adj_ghost(lamX, L.nslots, L.bb_ops.as<BBOp>(), L.n_bb, g, ctx->stream));
-  CK(launch_adj_force(a, lamX, V.gF.as<double>(), ctx->stream));
   V.cur = 1 - V.cur;
   return OCTLB_OK;
 }
@@ -1304,26 +1341,102 @@ int adj_level(octlb_ctx* ctx, int l, size_t start, float coef) {
     if (F.n_restrict > 0)
       CK(launch_adj_restrict(F.restrict_items.as<RestrictItem>(), F.n_restrict, A.recs[s2].save.as<float>(),
                              V.lam[V.cur].as<float>(), L.nslots, ctx->restrict_scale, omega,
-                             VF.lam_save.as<float>(), g, ctx->stream));
+                             VF.lam_save.as<float>(), g, V.gF.as<double>(), L.ncore, ctx->stream));
     int rc = adj_level(ctx, l + 1, s2, coef);
     if (rc) return rc;
     if (L.n_prolong > 0)
       CK(launch_adj_prolong(L.prolong_items.as<ProlongItem>(), L.n_prolong, A.recs[start].save.as<float>(),
                             A.recs[start].prev.as<float>(), 0, VF.lam[VF.cur].as<float>(), F.nslots,
-                            ctx->prolong_scale, omega, V.lam_m.as<float>(), V.lam_prev.as<float>(), g,
-                            ctx->stream));
+                            ctx->prolong_scale, omega, V.lam_m.as<float>(), V.lam_prev.as<float>(),
+                            V.lam_save.as<float>(), g, VF.gF.as<double>(), F.ncore, ctx->stream));
     rc = adj_level(ctx, l + 1, s1, coef);
     if (rc) return rc;
     if (L.n_prolong > 0) {
       CK(launch_adj_prolong(L.prolong_items.as<ProlongItem>(), L.n_prolong, A.recs[start].save.as<float>(),
                             A.recs[start].prev.as<float>(), 1, VF.lam[VF.cur].as<float>(), F.nslots,
-                            ctx->prolong_scale, omega, V.lam_m.as<float>(), V.lam_prev.as<float>(), g,
-                            ctx->stream));
-      CK(launch_adj_read_macro(L.prolong_items.as<ProlongItem>(), L.n_prolong, A.recs[start].save.as<float>(),
-                               V.lam_m.as<float>(), V.lam_save.as<float>(), ctx->stream));
+                            ctx->prolong_scale, omega, V.lam_m.as<float>(), V.lam_prev.as<float>(),
+                            V.lam_save.as<float>(), g, VF.gF.as<double>(), F.ncore, ctx->stream));
     }
   }
   if (own) return adj_step(ctx, l, A.recs[start], coef);
+  return OCTLB_OK;
+}
+
+// Levels of the step records of one coarse step, in forward order.
+void record_levels(const octlb_ctx* ctx, int l, std::vector<int>& out) {
+  if (ctx->levels[l].nblk > 0) out.push_back(l);
+  if (l < ctx->max_level) {
+    record_levels(ctx, l + 1, out);
+    record_levels(ctx, l + 1, out);
+  }
+}
+
+// The record pool for `steps` coarse steps, allocated before any capture.
+template <typename T>
+int prealloc_records(octlb_ctx* ctx, int steps) {
+  AdjointState& A = *ctx->adj;
+  std::vector<int> seq;
+  record_levels(ctx, 0, seq);
+  const size_t need = seq.size() * static_cast<size_t>(steps);
+  if (A.recs.size() < need) A.recs.resize(need);
+  A.next_same.assign(A.recs.size(), -1);
+  A.first_rec.assign(ctx->levels.size(), -1);
+  {
+    std::vector<int> last(ctx->levels.size(), -1);
+    for (size_t r = 0; r < need; ++r) {
+      const int l = seq[r % seq.size()];
+      if (last[l] >= 0) A.next_same[last[l]] = static_cast<int>(r);
+      else A.first_rec[l] = static_cast<int>(r);
+      last[l] = static_cast<int>(r);
+    }
+  }
+  for (size_t r = 0; r < need; ++r) {
+    StepRecord& R = A.recs[r];
+    const int l = seq[r % seq.size()];
+    if (R.level == l) continue;
+    Level& L = ctx->levels[l];
+    CK(R.snap.alloc(static_cast<size_t>(L.nslots) * kQ * sizeof(T)));
+    CK(R.save.alloc(static_cast<size_t>(L.n_save) * kQ * sizeof(float)));
+    CK(R.prev.alloc(L.n_prolong > 0 ? L.prev.bytes : 0));
+    R.level = l;
+  }
+  return OCTLB_OK;
+}
+
+uint64_t lam_mask(const AdjointState& A) {
+  uint64_t m = 0;
+  for (size_t l = 0; l < A.lv.size(); ++l)
+    if (A.lv[l].cur) m |= 1ull << l;
+  return m;
+}
+
+// Runs body() on the stream, through a CUDA graph captured on first use for
+// `key` when graphs are enabled; set_out applies the captured run's final
+// host-side parity to the context on replay.
+template <typename Body, typename GetMask, typename SetMask>
+int run_captured(octlb_ctx* ctx, const std::array<long long, 4>& key, Body body, GetMask get_mask,
+                 SetMask set_mask) {
+  AdjointState& A = *ctx->adj;
+  if (!ctx->use_graphs) return body();
+  auto it = A.graphs.find(key);
+  if (it == A.graphs.end()) {
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (ee != cudaSuccess) return cuda_fail(ctx, ee, "cudaStreamEndCapture");
+    AdjointState::Graph e;
+    const cudaError_t ei = cudaGraphInstantiate(&e.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return cuda_fail(ctx, ei, "cudaGraphInstantiate");
+    e.out_mask = get_mask();
+    A.graphs.emplace(key, e);
+    CK(cudaGraphLaunch(e.exec, ctx->stream));
+    return OCTLB_OK;
+  }
+  CK(cudaGraphLaunch(it->second.exec, ctx->stream));
+  set_mask(it->second.out_mask);
   return OCTLB_OK;
 }
 
@@ -1428,22 +1541,71 @@ int adjoint_impl(octlb_ctx* ctx, const octlb_adj_params* p, double* objective, d
   CK(cudaMemsetAsync(A.g.p, 0, A.g.bytes, ctx->stream));
   const size_t per = static_cast<size_t>(count_records(ctx, 0));
   const float coef = static_cast<float>(1.0 / W);
+  const std::array<long long, 4> gp{NT, W, K, p->component};
+  if (gp != A.graph_params) {
+    A.clear_graphs();
+    A.graph_params = gp;
+  }
+  { int rc = prealloc_records<T>(ctx, K); if (rc) return rc; }
+  auto set_parity = [&](uint64_t m) {
+    for (size_t l = 0; l < nl; ++l) ctx->levels[l].cur = (m >> l) & 1;
+  };
+  auto set_lam = [&](uint64_t m) {
+    for (size_t l = 0; l < nl; ++l) A.lv[l].cur = (m >> l) & 1;
+  };
   for (int c = nck - 1; c >= 0; --c) {
     const int k0 = c * K, k1 = std::min(NT, k0 + K);
-    int rc = checkpoint_copy<T>(ctx, A.ck[c], false);
+    const int nwin = std::max(0, k1 - std::max(k0, NT - W));
+    // the segment's checkpoint goes straight into each level's first record
+    for (size_t l = 0; l < nl; ++l) {
+      Level& L = ctx->levels[l];
+      if (L.nblk == 0) continue;
+      AdjointState::Checkpoint& ck = A.ck[c];
+      L.cur = ck.cur[l];
+      L.rec_cur = A.recs[A.first_rec[l]].snap.p;
+      CK(cudaMemcpyAsync(L.rec_cur, ck.buf[l].p, ck.buf[l].bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+      if (L.n_prolong > 0)
+        CK(cudaMemcpyAsync(L.prev.p, ck.prev[l].p, ck.prev[l].bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    int rc = OCTLB_OK;
+    // recompute the segment, recording every level step
+    rc = run_captured(
+        ctx, {0, static_cast<long long>(parity_mask(ctx)), k1 - k0, 0},
+        [&]() {
+          A.recording = true;
+          A.nrec = 0;
+          for (int k = k0; k < k1; ++k) {
+            const int r = advance_one_launches<T>(ctx);
+            if (r) { A.recording = false; return r; }
+          }
+          A.recording = false;
+          if (A.nrec != per * static_cast<size_t>(k1 - k0))
+            return fail(ctx, OCTLB_ESTATE, "adjoint: record count mismatch");
+          return static_cast<int>(OCTLB_OK);
+        },
+        [&]() { return parity_mask(ctx); }, set_parity);
+    for (auto& L : ctx->levels) L.rec_cur = L.rec_save = nullptr;
     if (rc) return rc;
-    A.recording = true;
-    A.nrec = 0;
-    for (int k = k0; k < k1; ++k) {
-      rc = advance_one_launches<T>(ctx);
-      if (rc) { A.recording = false; return rc; }
-    }
-    A.recording = false;
-    if (A.nrec != per * static_cast<size_t>(k1 - k0)) return fail(ctx, OCTLB_ESTATE, "adjoint: record count mismatch");
-    for (int k = k1 - 1; k >= k0; --k) {
-      rc = adj_level(ctx, 0, per * static_cast<size_t>(k - k0), k >= NT - W ? coef : 0.f);
-      if (rc) return rc;
-    }
+    A.nrec = per * static_cast<size_t>(k1 - k0);
+    // reverse through it
+    rc = run_captured(
+        ctx, {1, static_cast<long long>(lam_mask(A)), k1 - k0, nwin},
+        [&]() {
+          for (int k = k1 - 1; k >= k0; --k) {
+            const int r = adj_level(ctx, 0, per * static_cast<size_t>(k - k0), k >= NT - W ? coef : 0.f);
+            if (r) return r;
+          }
+          return static_cast<int>(OCTLB_OK);
+        },
+        [&]() { return lam_mask(A); }, set_lam);
+    if (rc) return rc;
+  }
+
+  // Body-force gradient of the initial state (consumed by no earlier step).
+  for (size_t l = 0; l < nl; ++l) {
+    Level& L = ctx->levels[l];
+    if (L.nblk == 0) continue;
+    CK(launch_adj_force(L.args, A.lv[l].lam[A.lv[l].cur].as<float>(), A.lv[l].gF.as<double>(), ctx->stream));
   }
 
   // Leave the context as the forward left it.

@@ -3,9 +3,11 @@ adjoint configuration, computed with the reference's own TimeLoop
 (oracle/_ref, FP64), and saved as golden values:
 
   adjoint_c5.npz   channel 128x32x32 finest cells, two levels, D = 8, Re = 40,
-                   2,000 coarse steps (4,000 finest steps); objective J = the x
-                   component of MomentumExchangeDrag::force_on_fluid_if over the
-                   cylinder, averaged over the last 500 coarse steps (the last
+                   1,000 TimeLoop::advance_one calls (the forest's levels are 1
+                   and 2 and the recursion starts at level 0, so each call
+                   takes 4 finest steps: 4,000 finest steps); objective J = the
+                   x component of MomentumExchangeDrag::force_on_fluid_if over
+                   the cylinder, averaged over the last 250 calls (the last
                    1,000 finest steps).
                    Central differences, h = 1e-4 relative, for the inlet u_max
                    and tau; for the body force, J(+d) - J(-d) over 2 along each
@@ -16,7 +18,7 @@ The body force enters at the reference's DomainBoundaryHandler::apply() hook
 (restated in oracle/ref_capi.cpp; the reference has none).  Runs the 21
 forward runs in parallel worker processes (spawn).
 
-  python tests/golden/make_adjoint_reference.py [--steps 2000] [--window 500] [--workers 7]
+  python tests/golden/make_adjoint_reference.py [--steps 1000] [--window 250] [--workers 7]
   python tests/golden/make_adjoint_reference.py --steps 24 --window 12 --out adjoint_c5_short.npz
 (the second: a 24-coarse-step horizon for a quick test).
 """
@@ -70,8 +72,8 @@ def objective(job):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--window", type=int, default=500)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--window", type=int, default=250)
     ap.add_argument("--workers", type=int, default=7)
     ap.add_argument("--rel", type=float, default=1e-4)
     ap.add_argument("--out", default="adjoint_c5.npz")
