@@ -201,6 +201,97 @@ def run_reference_arm(args, world, rank, pg):
     print(json.dumps(out), flush=True)
 
 
+def forest_measurements(ob, cases, torch, peak):
+    """The forest configurations beside the headline line: MLUPS of the
+    two-level AMR cavity (64^3 + band under the lid) and of the three-level
+    cylinder (256x64x64, D = 16, Re = 100) in FP32 and FP16-shifted storage
+    (an advance_one = a step; CUDA events on the context's stream), the FP16 /
+    FP32 ratio, the cylinder's time-averaged drag over its last 5,000 finest
+    steps against the FP64 run of the reference TimeLoop
+    (tests/golden/long_c3_cylinder.npz), and the adjoint's cost on its own
+    configuration (forward + reverse sweep vs the forward alone, steady state)
+    with its gradients against FP64 finite differences
+    (tests/golden/adjoint_c5.npz)."""
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "tests", "golden"))
+    out = {}
+    cfgs = {
+        "amr_cavity_64": (lambda: cases.cavity_forest(cells=64, n=8, lid=0.05, tau=0.56, band_cells=8),
+                          ob.STREAM_ROTATE, False),
+        "cylinder_256x64x64": (lambda: cases.cylinder_forest(), ob.STREAM_LINKS, True),
+    }
+    for name, (fn, mode, drag) in cfgs.items():
+        mesh, init, info = fn()
+        r = {}
+        for pn, prec in (("fp32", ob.FP32), ("fp16", ob.FP16_SHIFTED)):
+            lat = ob.GpuLattice(mesh, info["omega"], precision=prec, stream_mode=mode, drag=drag, init_pops=init)
+            st = torch.cuda.Stream()
+            lat.set_stream(st.cuda_stream)
+            lat.advance(5)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            K = 100
+            e0.record(st)
+            lat.advance(K)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / K
+            launches, lups = lat.step_stats()
+            bpl = 152 if pn == "fp32" else 76
+            r[pn] = {"mlups": lups / ms / 1e3, "ms_per_step": ms, "launches_per_step": int(launches),
+                     "hbm_frac": bpl * lups / (ms * 1e-3) / 1e9 / peak}
+            if name.startswith("cylinder"):
+                g = np.load(os.path.join(here, "tests", "golden", "long_c3_cylinder.npz"))["force"]
+                lat.close()
+                lat = ob.GpuLattice(mesh, info["omega"], precision=prec, stream_mode=mode, drag=True, init_pops=init)
+                steps = len(g)
+                last = len(g) // 4
+                lat.advance(steps - last)
+                lat.force_reset()
+                lat.advance(last)
+                fs, nsteps = lat.force_sum()
+                ref = g[steps - last:, 0].mean()
+                r[pn]["drag_rel_err_vs_fp64"] = float(abs(fs[0] / nsteps - ref) / abs(ref))
+            lat.close()
+        r["fp16_speedup"] = r["fp16"]["mlups"] / r["fp32"]["mlups"]
+        out[name] = r
+    # adjoint
+    from make_adjoint_reference import case, directions
+    g = np.load(os.path.join(here, "tests", "golden", "adjoint_c5.npz"))
+    steps, window = int(g["steps"]), int(g["window"])
+    mesh, init, info = case()
+    lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP32, stream_mode=ob.STREAM_LINKS, drag=True,
+                        init_pops=init)
+    lat.advance(3)
+    lat.synchronize()
+    t0 = time.perf_counter()
+    lat.advance(steps)
+    lat.synchronize()
+    t_fwd = time.perf_counter() - t0
+    lat.close()
+    lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP32, stream_mode=ob.STREAM_LINKS, drag=True,
+                        init_pops=init)
+    lat.adjoint(steps, window, 16)  # first call captures the sweep's graphs
+    lat.close()
+    lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP32, stream_mode=ob.STREAM_LINKS, drag=True,
+                        init_pops=init)
+    t0 = time.perf_counter()
+    J, du, dtau, gF = lat.adjoint(steps, window, 16)
+    t_adj = time.perf_counter() - t0
+    lat.close()
+    d = directions(mesh)
+    gdir = np.array([np.sum(gF * d[k]) for k in range(len(d))])
+    out["adjoint_channel_128x32x32"] = {
+        "advance_one_calls": steps, "window": window, "checkpoint_interval": 16,
+        "forward_s": t_fwd, "forward_plus_adjoint_s": t_adj,
+        "adjoint_cost_ratio": (t_adj - t_fwd) / t_fwd,
+        "rel_err_vs_fp64_fd": {"u_max": float(abs(du - g["dJ_du"]) / abs(g["dJ_du"])),
+                               "tau": float(abs(dtau - g["dJ_dtau"]) / abs(g["dJ_dtau"])),
+                               "body_force_dirs_max": float(np.max(np.abs(gdir - g["dJ_dir"]) / np.abs(g["dJ_dir"])))},
+    }
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -211,6 +302,7 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
+    ap.add_argument("--no-forest", action="store_true", help="skip the forest / adjoint measurements")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, pg = dist_setup(args)
@@ -300,6 +392,8 @@ def main():
         "fp16_shifted": {"mlups": results["fp16"]["mlups"], "ms_per_step": results["fp16"]["ms_step"],
                          "bytes_per_lu": 76, "speedup_vs_fp32": results["fp16"]["mlups"] / results["fp32"]["mlups"]},
     }
+    if rank == 0 and world == 1 and not args.no_forest:
+        out["forest"] = forest_measurements(ob, cases, torch, peak)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_reference_mlups(n, steps_budget_s=args.ref_seconds)
     if rank == 0:
