@@ -292,6 +292,43 @@ def forest_measurements(ob, cases, torch, peak):
     return out
 
 
+def run_single_case(args, ob, cases, torch):
+    """One forest case alone (for launch lists and ncu captures): --warmup
+    then --steps advance_one calls, or one adjoint sweep over --steps calls."""
+    prec = ob.FP32 if args.precision == "fp32" else ob.FP16_SHIFTED
+    if args.case == "adjoint":
+        here = os.path.dirname(os.path.abspath(__file__))
+        sys.path.insert(0, os.path.join(here, "tests", "golden"))
+        from make_adjoint_reference import case
+        mesh, init, info = case()
+        lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP32, stream_mode=ob.STREAM_LINKS, drag=True,
+                            init_pops=init)
+        t0 = time.perf_counter()
+        J = lat.adjoint(args.steps, max(1, args.steps // 4), 16, force_grad=False)[0]
+        print(json.dumps({"case": "adjoint", "steps": args.steps, "seconds": time.perf_counter() - t0, "J": J}))
+        return
+    if args.case == "amr_cavity_64":
+        mesh, init, info = cases.cavity_forest(cells=64, n=8, lid=0.05, tau=0.56, band_cells=8)
+        mode, drag = ob.STREAM_ROTATE, False
+    else:
+        mesh, init, info = cases.cylinder_forest()
+        mode, drag = ob.STREAM_LINKS, True
+    lat = ob.GpuLattice(mesh, info["omega"], precision=prec, stream_mode=mode, drag=drag, init_pops=init)
+    st = torch.cuda.Stream()
+    lat.set_stream(st.cuda_stream)
+    lat.advance(args.warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    lat.advance(args.steps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches, lups = lat.step_stats()
+    print(json.dumps({"case": args.case, "storage": args.precision, "steps": args.steps, "ms_per_step": ms,
+                      "mlups": lups / ms / 1e3, "launches_per_step": launches}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -303,6 +340,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-forest", action="store_true", help="skip the forest / adjoint measurements")
+    ap.add_argument("--case", default="tgv", choices=["tgv", "amr_cavity_64", "cylinder", "adjoint"],
+                    help="tgv: the headline line; otherwise run only that case for --steps advance_one "
+                         "calls (or one adjoint sweep of --steps calls) and print its timing (profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, pg = dist_setup(args)
@@ -317,6 +357,11 @@ def main():
     torch.cuda.set_device(local)
     import octlb_b200 as ob
     from octlb_b200 import cases
+    if args.case != "tgv":
+        run_single_case(args, ob, cases, torch)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
 
     n = args.n
     results = {}
