@@ -7,8 +7,9 @@
 //   k_adj_step     BGK collide + pull stream (+ save rows, halo rotation,
 //                  solid copies) -> adjoint of the step's input, scattered to
 //                  the pulled slots with FP32 atomics
-//   k_adj_near     the near-wall link rule: half-way bounce-back, Bouzidi
-//                  (bouzidi_pull.h:8-26), reflect-on-pull, moving-wall term
+//                  and, in the same launch, the near-wall link rule:
+//                  half-way bounce-back, Bouzidi (bouzidi_pull.h:8-26),
+//                  reflect-on-pull, moving-wall term
 //   k_adj_ghost    boundary fills (bounce-back / moving wall / outflow copy)
 //   k_adj_drag     momentum-exchange force (the objective)
 //   k_adj_prolong, k_adj_restrict   Lagrava coupling (one warp per item)
@@ -207,85 +208,11 @@ __device__ __forceinline__ void force_grad(const float (&mu)[kQ], double* gF, ui
   gF[2ull * ncore + t] += sz;
 }
 
-// Step VJP over the cells the slot-map step streams (one CTA per block, the
-// block's slot map in shared memory); CTAs after the nblk block CTAs take the
-// halo rotation items.  a.src = the step's input (after force and fills);
-// lamY = cotangent of the step's output, lamX += cotangent of its input.
-template <bool LINKS, bool FLAGS>
-__global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, float* __restrict__ lamY,
-                                                      float* lamX, float* __restrict__ lamS, double* g,
-                                                      double* gF) {
-  extern __shared__ int smap[];
-  constexpr uint32_t kParts = 2;  // two CTAs per block, one cell per thread at a time
-  const uint32_t b = blockIdx.x / kParts, part = blockIdx.x % kParts;
-  const long long qs = a.qs;
-  if (b >= static_cast<uint32_t>(a.nblk)) {
-    const uint32_t k = (blockIdx.x - a.nblk * kParts) * kThreads + threadIdx.x;
-    if (k < static_cast<uint32_t>(a.n_open)) {
-      long long d, sl;
-      int i;
-      rotate_slots(a, k, d, sl, i);
-      atomicAdd(lamX + i * qs + sl, lamY[i * qs + d]);
-      lamY[i * qs + d] = 0.f;
-    }
-    return;
-  }
-  const int np = a.np, np3 = np * np * np;
-  const int* gm = a.slot_map + static_cast<long long>(b) * np3;
-  for (int k = threadIdx.x; k < np3; k += kThreads) smap[k] = gm[k];
-  __syncthreads();
-  const float* src = static_cast<const float*>(a.src);
-  const uint32_t n = a.n, n3 = n * n * n, span = n3 / kParts;
-  double dom = 0.0;
-  for (uint32_t tl = part * span + threadIdx.x; tl < (part + 1) * span; tl += kThreads) {
-    const uint32_t t = b * n3 + tl;
-    const uint32_t x = a.div_n2.div(tl), r = tl - x * n * n, y = a.div_n.div(r);
-    const int P = (static_cast<int>(x + 1) * np + static_cast<int>(y + 1)) * np + static_cast<int>(r - y * n + 1);
-    const uint8_t fl = FLAGS ? a.flags[t] : 0;
-    if (LINKS && (fl & kKindMask) == kSolid) {
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) {
-        atomicAdd(lamX + i * qs + t, lamY[i * qs + t]);
-        lamY[i * qs + t] = 0.f;
-      }
-      continue;
-    }
-    if (LINKS && (fl & kFlagNear)) continue;  // k_adj_near
-    float f[kQ], mu[kQ], lam[kQ];
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) {
-      f[i] = src[i * qs + smap[P - a.off_pad[i]]];
-      mu[i] = lamY[i * qs + t];
-      lamY[i * qs + t] = 0.f;
-    }
-    const bool bulk = !FLAGS || (fl & kKindMask) == kBulk;
-    if (bulk) force_grad(mu, gF, a.ncore, t);
-    if (bulk) {
-      dom += bgk_vjp(f, a.omega, mu, lam);
-    } else {
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) lam[i] = mu[i];
-    }
-    if (FLAGS && (fl & kFlagSave)) {
-      float* ls = lamS + static_cast<long long>(a.save_idx[t]) * kQ;
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) {
-        lam[i] += ls[i];
-        ls[i] = 0.f;
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) atomicAdd(lamX + i * qs + smap[P - a.off_pad[i]], lam[i]);
-  }
-  add_grad(g, kGOmega, dom);
-}
-
 // Near-wall cells (the link rule with host-resolved slots, see k_step_near),
 // one warp per cell, lane i on direction i.
-__global__ void __launch_bounds__(kThreads) k_adj_near(const StepArgs a, const NearTables nt, float* __restrict__ lamY,
-                                                      float* lamX, float* __restrict__ lamS, double* g, double* gF) {
-  const int k = (blockIdx.x * kThreads + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+__device__ __forceinline__ float adj_near_cell(const StepArgs& a, const NearTables& nt, int k, int lane,
+                                               float* __restrict__ lamY, float* lamX, float* __restrict__ lamS,
+                                               double* gF) {
   float dom = 0.f;
   if (k < nt.n) {
     const float* src = static_cast<const float*>(a.src);
@@ -351,9 +278,90 @@ __global__ void __launch_bounds__(kThreads) k_adj_near(const StepArgs a, const N
       if (own_total != 0.f) atomicAdd(lamX + lane * qs + t, own_total);
     }
   }
-  double v[1] = {lane == 0 ? static_cast<double>(dom) : 0.0};
-  block_reduce<1>(v);
-  if (threadIdx.x == 0 && v[0] != 0.0) atomicAdd(g + kGOmega, v[0]);
+  return dom;
+}
+
+// Step VJP over the cells the slot-map step streams (one CTA per block, the
+// block's slot map in shared memory); CTAs after the nblk block CTAs take the
+// halo rotation items.  a.src = the step's input (after force and fills);
+// lamY = cotangent of the step's output, lamX += cotangent of its input.
+template <bool LINKS, bool FLAGS>
+__global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const NearTables nt, float* __restrict__ lamY,
+                                                      float* lamX, float* __restrict__ lamS, double* g,
+                                                      double* gF) {
+  extern __shared__ int smap[];
+  constexpr uint32_t kParts = 2;  // two CTAs per block, one cell per thread at a time
+  // first CTAs: the near-wall cells, one warp each
+  const uint32_t near_ctas = LINKS ? (static_cast<uint32_t>(nt.n) + kThreads / 32 - 1) / (kThreads / 32) : 0;
+  if (LINKS && blockIdx.x < near_ctas) {
+    const int lane = threadIdx.x & 31;
+    const float dom = adj_near_cell(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)), lane,
+                                    lamY, lamX, lamS, gF);
+    add_grad(g, kGOmega, lane == 0 ? static_cast<double>(dom) : 0.0);
+    return;
+  }
+  const uint32_t bid = blockIdx.x - near_ctas;
+  const uint32_t b = bid / kParts, part = bid % kParts;
+  const long long qs = a.qs;
+  if (b >= static_cast<uint32_t>(a.nblk)) {
+    const uint32_t k = (bid - a.nblk * kParts) * kThreads + threadIdx.x;
+    if (k < static_cast<uint32_t>(a.n_open)) {
+      long long d, sl;
+      int i;
+      rotate_slots(a, k, d, sl, i);
+      atomicAdd(lamX + i * qs + sl, lamY[i * qs + d]);
+      lamY[i * qs + d] = 0.f;
+    }
+    return;
+  }
+  const int np = a.np, np3 = np * np * np;
+  const int* gm = a.slot_map + static_cast<long long>(b) * np3;
+  for (int k = threadIdx.x; k < np3; k += kThreads) smap[k] = gm[k];
+  __syncthreads();
+  const float* src = static_cast<const float*>(a.src);
+  const uint32_t n = a.n, n3 = n * n * n, span = n3 / kParts;
+  double dom = 0.0;
+  for (uint32_t tl = part * span + threadIdx.x; tl < (part + 1) * span; tl += kThreads) {
+    const uint32_t t = b * n3 + tl;
+    const uint32_t x = a.div_n2.div(tl), r = tl - x * n * n, y = a.div_n.div(r);
+    const int P = (static_cast<int>(x + 1) * np + static_cast<int>(y + 1)) * np + static_cast<int>(r - y * n + 1);
+    const uint8_t fl = FLAGS ? a.flags[t] : 0;
+    if (LINKS && (fl & kKindMask) == kSolid) {
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) {
+        atomicAdd(lamX + i * qs + t, lamY[i * qs + t]);
+        lamY[i * qs + t] = 0.f;
+      }
+      continue;
+    }
+    if (LINKS && (fl & kFlagNear)) continue;  // k_adj_near
+    float f[kQ], mu[kQ], lam[kQ];
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      f[i] = src[i * qs + smap[P - a.off_pad[i]]];
+      mu[i] = lamY[i * qs + t];
+      lamY[i * qs + t] = 0.f;
+    }
+    const bool bulk = !FLAGS || (fl & kKindMask) == kBulk;
+    if (bulk) force_grad(mu, gF, a.ncore, t);
+    if (bulk) {
+      dom += bgk_vjp(f, a.omega, mu, lam);
+    } else {
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) lam[i] = mu[i];
+    }
+    if (FLAGS && (fl & kFlagSave)) {
+      float* ls = lamS + static_cast<long long>(a.save_idx[t]) * kQ;
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) {
+        lam[i] += ls[i];
+        ls[i] = 0.f;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) atomicAdd(lamX + i * qs + smap[P - a.off_pad[i]], lam[i]);
+  }
+  add_grad(g, kGOmega, dom);
 }
 
 // Boundary fills in reverse: the fill target's cotangent moves to its source
@@ -594,19 +602,14 @@ inline uint32_t grid_of(long long items, int threads) { return static_cast<uint3
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
-cudaError_t launch_adj_step(const StepArgs& a, bool links, bool flags, float* lamY, float* lamX, float* lamS,
-                            double* g, double* gF, cudaStream_t s) {
-  const dim3 grid(static_cast<uint32_t>(a.nblk) * 2 + grid_of(a.n_open, kThreads));
+cudaError_t launch_adj_step(const StepArgs& a, const NearTables& nt, bool links, bool flags, float* lamY, float* lamX,
+                            float* lamS, double* g, double* gF, cudaStream_t s) {
+  const uint32_t near_ctas = links ? grid_of(static_cast<long long>(nt.n) * 32, kThreads) : 0;
+  const dim3 grid(near_ctas + static_cast<uint32_t>(a.nblk) * 2 + grid_of(a.n_open, kThreads));
   const size_t smem = static_cast<size_t>(a.np) * a.np * a.np * sizeof(int);
-  if (links) k_adj_step<true, true><<<grid, kThreads, smem, s>>>(a, lamY, lamX, lamS, g, gF);
-  else if (flags) k_adj_step<false, true><<<grid, kThreads, smem, s>>>(a, lamY, lamX, lamS, g, gF);
-  else k_adj_step<false, false><<<grid, kThreads, smem, s>>>(a, lamY, lamX, lamS, g, gF);
-  return cudaGetLastError();
-}
-cudaError_t launch_adj_near(const StepArgs& a, const NearTables& nt, float* lamY, float* lamX, float* lamS,
-                            double* g, double* gF, cudaStream_t s) {
-  if (nt.n == 0) return cudaSuccess;
-  k_adj_near<<<grid_of(static_cast<long long>(nt.n) * 32, kThreads), kThreads, 0, s>>>(a, nt, lamY, lamX, lamS, g, gF);
+  if (links) k_adj_step<true, true><<<grid, kThreads, smem, s>>>(a, nt, lamY, lamX, lamS, g, gF);
+  else if (flags) k_adj_step<false, true><<<grid, kThreads, smem, s>>>(a, nt, lamY, lamX, lamS, g, gF);
+  else k_adj_step<false, false><<<grid, kThreads, smem, s>>>(a, nt, lamY, lamX, lamS, g, gF);
   return cudaGetLastError();
 }
 cudaError_t launch_adj_ghost(float* lam, long long qs, const BBOp* bb, uint32_t nbb, double* g, cudaStream_t s) {

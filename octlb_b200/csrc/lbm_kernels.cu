@@ -135,9 +135,7 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
 // warp per cell, lane i on direction i; the collision gathers the 19 values
 // so every lane computes the moments exactly as bgk() does.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_step_near(const StepArgs a, const NearTables nt) {
-  const int k = (blockIdx.x * kThreads + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void near_cell(const StepArgs& a, const NearTables& nt, int k, int lane) {
   if (k >= nt.n) return;
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
@@ -160,6 +158,11 @@ __global__ void __launch_bounds__(kThreads) k_step_near(const StepArgs a, const 
     f = bgk_lane(d, lane, fa, f, a.omega);
   }
   if (d.act) Store<T>::st(dst + lane * a.qs + t, f, a.scale);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_step_near(const StepArgs a, const NearTables nt) {
+  near_cell<T>(a, nt, (blockIdx.x * kThreads + threadIdx.x) >> 5, threadIdx.x & 31);
 }
 
 // Two-element vector access for the paired periodic kernel.
@@ -226,15 +229,23 @@ __device__ __forceinline__ void map_cell_finish(const StepArgs& a, uint32_t t, u
 }
 
 // With one cell per thread (CPT = 1) two CTAs share a block, each over half
-// its cells, so small levels still give every SM work.
+// its cells, so small levels still give every SM work.  Under the links rule
+// the first CTAs of the launch take the near-wall cells (one warp each), so
+// they run beside the bulk instead of in a launch of their own.
 template <typename T, bool LINKS, bool FLAGS, int CPT>
-__global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const StepArgs a) {
+__global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const StepArgs a, const NearTables nt) {
   extern __shared__ int smap[];  // (n+2)^3 slots of this block
   constexpr uint32_t kParts = CPT == 1 ? 2 : 1;
-  const uint32_t b = blockIdx.x / kParts, part = blockIdx.x % kParts;
+  const uint32_t near_ctas = LINKS ? (static_cast<uint32_t>(nt.n) + kThreads / 32 - 1) / (kThreads / 32) : 0;
+  if (LINKS && blockIdx.x < near_ctas) {
+    near_cell<T>(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)), threadIdx.x & 31);
+    return;
+  }
+  const uint32_t bid = blockIdx.x - near_ctas;
+  const uint32_t b = bid / kParts, part = bid % kParts;
   if (b >= static_cast<uint32_t>(a.nblk)) {
     pdl_wait();
-    rotate_item<T>(a, (blockIdx.x - a.nblk * kParts) * kThreads + threadIdx.x);
+    rotate_item<T>(a, (bid - a.nblk * kParts) * kThreads + threadIdx.x);
     return;
   }
   const int np = a.np, np3 = np * np * np;
@@ -646,19 +657,20 @@ bool map_step_eligible(int n, long long nslots) {
   return n % 8 == 0 && np * np * np * 4 <= 48 * 1024 && nslots * kQ < (1LL << 32);
 }
 template <typename T>
-cudaError_t launch_step_map(const StepArgs& a, bool links, bool flags, int cpt, cudaStream_t s) {
+cudaError_t launch_step_map(const StepArgs& a, const NearTables& nt, bool links, bool flags, int cpt, cudaStream_t s) {
   cudaError_t e = cudaSuccess;
   if (a.nitems == 0) return cudaSuccess;
-  const dim3 g(static_cast<uint32_t>(a.nblk) * (cpt == 2 ? 1 : 2) + grid_for(static_cast<uint32_t>(a.n_open)));
+  const uint32_t near_ctas = links ? grid_for(static_cast<uint32_t>(nt.n) * 32) : 0;
+  const dim3 g(near_ctas + static_cast<uint32_t>(a.nblk) * (cpt == 2 ? 1 : 2) + grid_for(static_cast<uint32_t>(a.n_open)));
   const size_t smem = static_cast<size_t>(a.np) * a.np * a.np * sizeof(int);
   if (cpt == 2) {
-    if (links) e = launch_chain(k_step_map<T, true, true, 2>, dim3(g), dim3(kThreads), smem, s, a);
-    else if (flags) e = launch_chain(k_step_map<T, false, true, 2>, dim3(g), dim3(kThreads), smem, s, a);
-    else e = launch_chain(k_step_map<T, false, false, 2>, dim3(g), dim3(kThreads), smem, s, a);
+    if (links) e = launch_chain(k_step_map<T, true, true, 2>, dim3(g), dim3(kThreads), smem, s, a, nt);
+    else if (flags) e = launch_chain(k_step_map<T, false, true, 2>, dim3(g), dim3(kThreads), smem, s, a, nt);
+    else e = launch_chain(k_step_map<T, false, false, 2>, dim3(g), dim3(kThreads), smem, s, a, nt);
   } else {
-    if (links) e = launch_chain(k_step_map<T, true, true, 1>, dim3(g), dim3(kThreads), smem, s, a);
-    else if (flags) e = launch_chain(k_step_map<T, false, true, 1>, dim3(g), dim3(kThreads), smem, s, a);
-    else e = launch_chain(k_step_map<T, false, false, 1>, dim3(g), dim3(kThreads), smem, s, a);
+    if (links) e = launch_chain(k_step_map<T, true, true, 1>, dim3(g), dim3(kThreads), smem, s, a, nt);
+    else if (flags) e = launch_chain(k_step_map<T, false, true, 1>, dim3(g), dim3(kThreads), smem, s, a, nt);
+    else e = launch_chain(k_step_map<T, false, false, 1>, dim3(g), dim3(kThreads), smem, s, a, nt);
   }
   return e != cudaSuccess ? e : cudaGetLastError();
 }
@@ -757,7 +769,7 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
   template cudaError_t launch_step_pair<T>(const StepArgs&, cudaStream_t);                         \
   template cudaError_t launch_step_near<T>(const StepArgs&, const NearTables&, cudaStream_t);       \
   template cudaError_t launch_add_force<T>(const StepArgs&, T*, const float*, cudaStream_t);         \
-  template cudaError_t launch_step_map<T>(const StepArgs&, bool, bool, int, cudaStream_t);         \
+  template cudaError_t launch_step_map<T>(const StepArgs&, const NearTables&, bool, bool, int, cudaStream_t); \
   template cudaError_t launch_ghost<T>(T*, long long, const CopyDesc*, const uint32_t*, int,       \
                                        uint32_t, const BBOp*, uint32_t, float, float, cudaStream_t); \
   template cudaError_t launch_prolong<T>(const ProlongItem*, int, const float*, float*, int, T*,   \

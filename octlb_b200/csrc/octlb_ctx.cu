@@ -40,12 +40,11 @@ template <typename T> int bulk_prepare(int n);
 template <typename T> cudaError_t launch_step_pair(const StepArgs&, cudaStream_t);
 template <typename T> cudaError_t launch_step_near(const StepArgs&, const NearTables&, cudaStream_t);
 template <typename T> cudaError_t launch_add_force(const StepArgs&, T*, const float*, cudaStream_t);
-template <typename T> cudaError_t launch_step_map(const StepArgs&, bool, bool, int, cudaStream_t);
+template <typename T> cudaError_t launch_step_map(const StepArgs&, const NearTables&, bool, bool, int, cudaStream_t);
 bool pair_step_eligible(int n);
 bool map_step_eligible(int n, long long nslots);
 void set_programmatic_launch(bool on);
-cudaError_t launch_adj_step(const StepArgs&, bool, bool, float*, float*, float*, double*, double*, cudaStream_t);
-cudaError_t launch_adj_near(const StepArgs&, const NearTables&, float*, float*, float*, double*, double*,
+cudaError_t launch_adj_step(const StepArgs&, const NearTables&, bool, bool, float*, float*, float*, double*, double*,
                             cudaStream_t);
 cudaError_t launch_adj_ghost(float*, long long, const BBOp*, uint32_t, double*, cudaStream_t);
 cudaError_t launch_adj_force(const StepArgs&, const float*, double*, cudaStream_t);
@@ -339,8 +338,8 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
   } else if (L.use_pair) {
     CK(launch_step_pair<T>(a, ctx->stream));
   } else if (L.use_map) {
-    CK(launch_step_map<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags, ctx->map_cells, ctx->stream));
-    CK(launch_step_near<T>(a, L.near, ctx->stream));
+    CK(launch_step_map<T>(a, L.near, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags, ctx->map_cells,
+                          ctx->stream));
   } else {
     CK(launch_step<T>(a, ctx->periodic != 0, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags,
                       ctx->stream));
@@ -1314,8 +1313,8 @@ int adj_step(octlb_ctx* ctx, int l, const StepRecord& R, float coef) {
   // gradient of the state this step read is taken where its cotangent is
   // consumed (the previous step's k_adj_step / k_adj_near, the coupler
   // kernels for their targets, and a final pass for the initial state).
-  CK(launch_adj_step(a, links, L.has_flags, lamY, lamX, V.lam_save.as<float>(), g, V.gF.as<double>(), ctx->stream));
-  CK(launch_adj_near(a, L.near, lamY, lamX, V.lam_save.as<float>(), g, V.gF.as<double>(), ctx->stream));
+  CK(launch_adj_step(a, L.near, links, L.has_flags, lamY, lamX, V.lam_save.as<float>(), g, V.gF.as<double>(),
+                     ctx->stream));
   if (R.drag && coef != 0.f)
     CK(launch_adj_drag(a, links, L.drag_items.as<DragItem>(), L.n_drag, lamX, coef, A.comp, ctx->stream));
   CK(launch_adj_ghost(lamX, L.nslots, L.bb_ops.as<BBOp>(), L.n_bb, g, ctx->stream));
@@ -1970,7 +1969,7 @@ int octlb_gpu_step_stats(const octlb_ctx* ctx, long long* launches, long long* l
   for (size_t l = 0; l < ctx->levels.size(); ++l) {
     const Level& L = ctx->levels[l];
     if (L.nblk == 0) continue;
-    per[l] = (L.n_bb > 0 ? 1 : 0) + (L.args.nitems > 0 ? 1 : 0) + (L.n_near > 0 && !L.use_pair && !L.use_bulk ? 1 : 0);
+    per[l] = (L.n_bb > 0 ? 1 : 0) + (L.args.nitems > 0 ? 1 : 0) + (L.n_near > 0 && !L.use_pair && !L.use_bulk && !L.use_map ? 1 : 0) + (L.has_force ? 1 : 0);
     if (ctx->drag && L.n_drag > 0) total += 1;  // once per advance_one, last step of the level
   }
   for (size_t l = 0; l < ctx->levels.size(); ++l) {
