@@ -10,7 +10,8 @@
 //                  and, in the same launch, the near-wall link rule:
 //                  half-way bounce-back, Bouzidi (bouzidi_pull.h:8-26),
 //                  reflect-on-pull, moving-wall term
-//   k_adj_ghost    boundary fills (bounce-back / moving wall / outflow copy)
+//   (boundary fills: a cotangent landing on a fill target goes to the fill's
+//                  source, with the moving-wall velocity gradient, scatter)
 //   k_adj_drag     momentum-exchange force (the objective)
 //   k_adj_prolong, k_adj_restrict   Lagrava coupling (one warp per item)
 //   k_adj_force    gradient of the per-cell body force
@@ -192,6 +193,22 @@ __device__ __forceinline__ void add_grad(double* g, int slot, double v) {
   if (threadIdx.x == 0 && a[0] != 0.0) atomicAdd(g + slot, a[0]);
 }
 
+// Cotangent v of population i at slot s of the step's input: a boundary-fill
+// target (never stored, see pull_value) passes it to the fill's source and
+// to the moving-wall velocity gradient (gw).
+__device__ __forceinline__ void scatter(const StepArgs& a, float* lamX, int i, long long s, float v, float& gw) {
+  if (s >= a.halo_base && a.fill_of) {
+    const int fo = a.fill_of[(s - a.halo_base) * kQ + i];
+    if (fo >= 0) {
+      const BBOp& op = a.fills[fo];
+      atomicAdd(lamX + op.src_pop * a.qs + op.src, v);
+      gw += v * op.dadd;
+      return;
+    }
+  }
+  atomicAdd(lamX + i * a.qs + s, v);
+}
+
 // Body-force gradient of one kBulk cell from the cotangent mu of the stored
 // state the forcing term 3 w_i (c_i . F) was added to.  gF is [3][ncore].
 __device__ __forceinline__ void force_grad(const float (&mu)[kQ], double* gF, uint32_t ncore, uint32_t t) {
@@ -212,7 +229,7 @@ __device__ __forceinline__ void force_grad(const float (&mu)[kQ], double* gF, ui
 // one warp per cell, lane i on direction i.
 __device__ __forceinline__ float adj_near_cell(const StepArgs& a, const NearTables& nt, int k, int lane,
                                                float* __restrict__ lamY, float* lamX, float* __restrict__ lamS,
-                                               double* gF) {
+                                               double* gF, float& gw) {
   float dom = 0.f;
   if (k < nt.n) {
     const float* src = static_cast<const float*>(a.src);
@@ -224,7 +241,7 @@ __device__ __forceinline__ float adj_near_cell(const StepArgs& a, const NearTabl
     const bool link = d.act && ((mask >> lane) & 1u);
     const int sl = d.act ? nt.slot[lane * nt.n + k] : 0;
     const float q = d.act ? nt.q[lane * nt.n + k] : 1.f;
-    const float val = d.act ? src[lane * qs + sl] : 0.f;
+    const float val = d.act ? pull_value(a, src, lane, sl) : 0.f;
     const float own = d.act ? src[lane * qs + t] : 0.f;
     const float own_opp = __shfl_sync(0xffffffffu, own, d.opp);
     float f = val;
@@ -274,7 +291,7 @@ __device__ __forceinline__ float adj_near_cell(const StepArgs& a, const NearTabl
     }
     const float own_total = to_own + __shfl_sync(0xffffffffu, to_opp, d.opp);
     if (d.act) {
-      if (to_val != 0.f) atomicAdd(lamX + lane * qs + sl, to_val);
+      if (to_val != 0.f) scatter(a, lamX, lane, sl, to_val, gw);
       if (own_total != 0.f) atomicAdd(lamX + lane * qs + t, own_total);
     }
   }
@@ -295,9 +312,11 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const N
   const uint32_t near_ctas = LINKS ? (static_cast<uint32_t>(nt.n) + kThreads / 32 - 1) / (kThreads / 32) : 0;
   if (LINKS && blockIdx.x < near_ctas) {
     const int lane = threadIdx.x & 31;
+    float gw = 0.f;
     const float dom = adj_near_cell(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)), lane,
-                                    lamY, lamX, lamS, gF);
+                                    lamY, lamX, lamS, gF, gw);
     add_grad(g, kGOmega, lane == 0 ? static_cast<double>(dom) : 0.0);
+    add_grad(g, kGWallVelocity, static_cast<double>(gw));
     return;
   }
   const uint32_t bid = blockIdx.x - near_ctas;
@@ -305,13 +324,15 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const N
   const long long qs = a.qs;
   if (b >= static_cast<uint32_t>(a.nblk)) {
     const uint32_t k = (bid - a.nblk * kParts) * kThreads + threadIdx.x;
+    float gw = 0.f;
     if (k < static_cast<uint32_t>(a.n_open)) {
       long long d, sl;
       int i;
       rotate_slots(a, k, d, sl, i);
-      atomicAdd(lamX + i * qs + sl, lamY[i * qs + d]);
+      scatter(a, lamX, i, sl, lamY[i * qs + d], gw);
       lamY[i * qs + d] = 0.f;
     }
+    add_grad(g, kGWallVelocity, static_cast<double>(gw));
     return;
   }
   const int np = a.np, np3 = np * np * np;
@@ -321,6 +342,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const N
   const float* src = static_cast<const float*>(a.src);
   const uint32_t n = a.n, n3 = n * n * n, span = n3 / kParts;
   double dom = 0.0;
+  float gw = 0.f;
   for (uint32_t tl = part * span + threadIdx.x; tl < (part + 1) * span; tl += kThreads) {
     const uint32_t t = b * n3 + tl;
     const uint32_t x = a.div_n2.div(tl), r = tl - x * n * n, y = a.div_n.div(r);
@@ -338,7 +360,9 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const N
     float f[kQ], mu[kQ], lam[kQ];
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
-      f[i] = src[i * qs + smap[P - a.off_pad[i]]];
+      const int sm = smap[P - a.off_pad[i]];  // < 0: bounce-back wall position (see k_step_map)
+      const float v = src[sm >= 0 ? i * qs + sm : opp(i) * qs + t];
+      f[i] = sm < -1 ? v + a.wall_add[(-sm - 2) * kQ + i] : v;
       mu[i] = lamY[i * qs + t];
       lamY[i * qs + t] = 0.f;
     }
@@ -359,28 +383,16 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const N
       }
     }
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) atomicAdd(lamX + i * qs + smap[P - a.off_pad[i]], lam[i]);
+    for (int i = 0; i < kQ; ++i) {
+      const int sm = smap[P - a.off_pad[i]];
+      atomicAdd(lamX + (sm >= 0 ? i * qs + sm : opp(i) * qs + t), lam[i]);
+      if (sm < -1) gw += lam[i] * a.wall_dadd[(-sm - 2) * kQ + i];
+    }
   }
   add_grad(g, kGOmega, dom);
+  add_grad(g, kGWallVelocity, static_cast<double>(gw));
 }
 
-// Boundary fills in reverse: the fill target's cotangent moves to its source
-// (the target was overwritten), and the moving-wall term's velocity
-// derivative collects the wall-velocity gradient.
-__global__ void __launch_bounds__(kThreads) k_adj_ghost(float* lam, long long qs, const BBOp* bb, uint32_t nbb,
-                                                       double* g) {
-  const uint32_t u = blockIdx.x * kThreads + threadIdx.x;
-  double gv = 0.0;
-  if (u < nbb) {
-    const BBOp op = bb[u];
-    float* d = lam + op.pop * qs + op.dst;
-    const float v = *d;
-    *d = 0.f;
-    if (v != 0.f) atomicAdd(lam + op.src_pop * qs + op.src, v);
-    gv = static_cast<double>(v) * op.dadd;
-  }
-  add_grad(g, kGWallVelocity, gv);
-}
 
 // Body-force gradient: the forcing term 3 w_i c_i . F is added to the stored
 // populations of kBulk cells at the start of the step whose input cotangent
@@ -406,11 +418,8 @@ __global__ void __launch_bounds__(kThreads) k_adj_force(const StepArgs a, const 
 // Momentum-exchange force in reverse (see k_drag): the objective adds
 // coef * F[comp], F = -sum (f_out + f_bar) c_i over the item's links.
 template <bool LINKS>
-__global__ void __launch_bounds__(kThreads) k_adj_drag(const StepArgs a, const DragItem* items, int nitems,
-                                                      float* lamX, float coef, int comp) {
-  const int t = blockIdx.x * kThreads + threadIdx.x;
-  if (t >= nitems) return;
-  const DragItem it = items[t];
+__device__ __forceinline__ void adj_drag_item(const StepArgs& a, const DragItem it, float* lamX, float coef, int comp,
+                                              float& gw) {
   const float* src = static_cast<const float*>(a.src);
   const long long qs = a.qs;
   float own[kQ], down[kQ];
@@ -443,7 +452,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_drag(const StepArgs a, const D
         if (qv >= 0.5f) {
           const float inv2q = 0.5f / qv;
           down[i] += inv2q * gs;
-          if (nk == kBulk) atomicAdd(lamX + j * qs + nb, (1.0f - inv2q) * gs);
+          if (nk == kBulk) scatter(a, lamX, j, nb, (1.0f - inv2q) * gs, gw);
           else down[j] += (1.0f - inv2q) * gs;
         } else {
           down[i] += 2.0f * qv * gs;
@@ -458,6 +467,16 @@ __global__ void __launch_bounds__(kThreads) k_adj_drag(const StepArgs a, const D
   for (int i = 0; i < kQ; ++i)
     if (down[i] != 0.f) atomicAdd(lamX + i * qs + it.slot, down[i]);
 }
+
+template <bool LINKS>
+__global__ void __launch_bounds__(kThreads) k_adj_drag(const StepArgs a, const DragItem* items, int nitems,
+                                                      float* lamX, float coef, int comp, double* g) {
+  const int t = blockIdx.x * kThreads + threadIdx.x;
+  float gw = 0.f;
+  if (t < nitems) adj_drag_item<LINKS>(a, items[t], lamX, coef, comp, gw);
+  add_grad(g, kGWallVelocity, static_cast<double>(gw));
+}
+
 
 // Prolongation in reverse, one warp per item, lane i on population i
 // (half = 1: w = (prev + m) / 2; half = 0: w = m and prev <- m).  The fine
@@ -612,21 +631,16 @@ cudaError_t launch_adj_step(const StepArgs& a, const NearTables& nt, bool links,
   else k_adj_step<false, false><<<grid, kThreads, smem, s>>>(a, nt, lamY, lamX, lamS, g, gF);
   return cudaGetLastError();
 }
-cudaError_t launch_adj_ghost(float* lam, long long qs, const BBOp* bb, uint32_t nbb, double* g, cudaStream_t s) {
-  if (nbb == 0) return cudaSuccess;
-  k_adj_ghost<<<grid_of(nbb, kThreads), kThreads, 0, s>>>(lam, qs, bb, nbb, g);
-  return cudaGetLastError();
-}
 cudaError_t launch_adj_force(const StepArgs& a, const float* lam, double* gF, cudaStream_t s) {
   if (a.ncore == 0) return cudaSuccess;
   k_adj_force<<<grid_of(a.ncore, kThreads), kThreads, 0, s>>>(a, lam, gF);
   return cudaGetLastError();
 }
 cudaError_t launch_adj_drag(const StepArgs& a, bool links, const DragItem* items, int n, float* lamX, float coef,
-                            int comp, cudaStream_t s) {
+                            int comp, double* g, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  if (links) k_adj_drag<true><<<grid_of(n, kThreads), kThreads, 0, s>>>(a, items, n, lamX, coef, comp);
-  else k_adj_drag<false><<<grid_of(n, kThreads), kThreads, 0, s>>>(a, items, n, lamX, coef, comp);
+  if (links) k_adj_drag<true><<<grid_of(n, kThreads), kThreads, 0, s>>>(a, items, n, lamX, coef, comp, g);
+  else k_adj_drag<false><<<grid_of(n, kThreads), kThreads, 0, s>>>(a, items, n, lamX, coef, comp, g);
   return cudaGetLastError();
 }
 cudaError_t launch_adj_prolong(const ProlongItem* items, int n, const float* coarse_save, const float* prev, int half,

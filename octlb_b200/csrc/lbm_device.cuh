@@ -64,6 +64,23 @@ __device__ __forceinline__ long long resolve(const StepArgs& a, uint32_t b, int 
   return page_slot(a, b, X, Y, Z);
 }
 
+// Population i at slot s of the step's input.  A halo-page slot that a
+// tree-boundary fill writes (the DomainBoundaryHandler::apply() position,
+// before the pull) is not stored: its value is the fill's, computed from the
+// fill's source (bounce-back: g_opp(i) of the wall-side cell plus the moving
+// wall term; outflow: the clamped interior cell's g_i).
+template <typename T>
+__device__ __forceinline__ float pull_value(const StepArgs& a, const T* src, int i, long long s) {
+  if (s >= a.halo_base && a.fill_of) {
+    const int fo = a.fill_of[(s - a.halo_base) * kQ + i];
+    if (fo >= 0) {
+      const BBOp& op = a.fills[fo];
+      return Store<T>::ld(src + op.src_pop * a.qs + op.src, a.inv_scale) + op.add;
+    }
+  }
+  return Store<T>::ld(src + i * a.qs + s, a.inv_scale);
+}
+
 // Halo item k of an open block (block_lattice.h:70-89): item (page, block,
 // halo index, population i); the page slot it writes, and the slot its torus
 // pull reads (own core, the neighbour core the exchange copies, or the own
@@ -194,6 +211,7 @@ __device__ inline void block_reduce(double (&v)[N]) {
       for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
     }
   }
+  __syncthreads();  // sm is reused by the next reduction of the same width
 }
 
 }  // namespace

@@ -5,8 +5,9 @@
 //               with half-way bounce-back and Bouzidi, K2), moving-wall term,
 //               halo torus-stream of open blocks, and pre-collision save of
 //               coupler source cells.
-//   k_ghost     device ghost fill (K3): same-level face / edge exchange and
-//               tree-boundary halo fills, from flattened tables.
+//   (no ghost kernel: a same-level halo position is read from the neighbour's
+//               core through the slot map, a tree-boundary fill target from
+//               its fill's source, pull_value)
 //   k_prolong   Lagrava prolongation (K4), k_restrict Lagrava restriction (K5).
 //   k_drag      momentum-exchange force (K6), FP64 with warp shuffles.
 //   k_audit     FP64 mass / momentum audit and non-finite check.
@@ -65,7 +66,12 @@ __device__ __forceinline__ void rotate_item(const StepArgs& a, uint32_t k) {
   long long d, sl;
   int i;
   rotate_slots(a, k, d, sl, i);
-  static_cast<T*>(a.dst)[i * a.qs + d] = static_cast<const T*>(a.src)[i * a.qs + sl];
+  const T* src = static_cast<const T*>(a.src);
+  T* dst = static_cast<T*>(a.dst);
+  if (sl >= a.halo_base && a.fill_of && a.fill_of[(sl - a.halo_base) * kQ + i] >= 0)
+    Store<T>::st(dst + i * a.qs + d, pull_value(a, src, i, sl), a.scale);  // source is a boundary fill
+  else
+    dst[i * a.qs + d] = src[i * a.qs + sl];
 }
 
 template <typename T, bool LINKS, bool FLAGS, bool BLOCKED>
@@ -106,7 +112,7 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
     uint32_t halo_mask;
     source_slots(a, c, t, tl, BLOCKED ? sb : nullptr, s, halo_mask);
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) f[i] = LD(src, a.qs, i, s[i], a.inv_scale);
+    for (int i = 0; i < kQ; ++i) f[i] = pull_value(a, src, i, s[i]);
     if constexpr (FLAGS) {
       if (fl & kFlagSave) {
         float* sv = a.save_buf + static_cast<long long>(a.save_idx[t]) * kQ;
@@ -146,7 +152,7 @@ __device__ __forceinline__ void near_cell(const StepArgs& a, const NearTables& n
   const int sl = d.act ? nt.slot[lane * nt.n + k] : 0;
   const float q = d.act ? nt.q[lane * nt.n + k] : 1.f, add = d.act ? nt.add[lane * nt.n + k] : 0.f;
   pdl_wait();
-  const float val = d.act ? LD(src, a.qs, lane, sl, a.inv_scale) : 0.f;
+  const float val = d.act ? pull_value(a, src, lane, sl) : 0.f;
   const float own = d.act ? LD(src, a.qs, lane, t, a.inv_scale) : 0.f;
   const float own_opp = __shfl_sync(0xffffffffu, own, d.opp);
   float f = val;
@@ -189,7 +195,8 @@ template <> struct Pair<__half> {
 
 // Forest-level step with a per-block slot map: one CTA per block stages the
 // block's (n+2)^3 map (padded position -> slot: own core, the neighbour core
-// the same-level exchange copies, or the own halo page) in shared memory, so
+// the same-level exchange copies, the source cell of an outflow ghost copy,
+// the own halo page, or a bounce-back wall marker) in shared memory, so
 // every pull is one shared-memory read and one 32-bit offset, with no
 // per-direction branching at block faces.  Each thread takes cells tl and
 // tl + 256 together (n^3 a multiple of 512), all 38 pulls issued before the
@@ -276,7 +283,15 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
       const uint32_t row = static_cast<uint32_t>(i) * qs;
 #pragma unroll
       for (int c = 0; c < CPT; ++c)
-        f[c][i] = Store<T>::ld(src + (row + static_cast<uint32_t>(smap[P[c] - a.off_pad[i]])), a.inv_scale);
+      {
+        // bounce-back wall position (marker < 0): the cell's own opposite
+        // population, plus the wall term when it moves; branch-free so the
+        // 19 (or 38) loads stay independent
+        const int sm = smap[P[c] - a.off_pad[i]];
+        const uint32_t off = sm >= 0 ? row + static_cast<uint32_t>(sm) : static_cast<uint32_t>(opp(i)) * qs + t[c];
+        const float v = Store<T>::ld(src + off, a.inv_scale);
+        f[c][i] = sm < -1 ? v + a.wall_add[(-sm - 2) * kQ + i] : v;
+      }
     }
 #pragma unroll
     for (int c = 0; c < CPT; ++c)
@@ -348,36 +363,6 @@ __global__ void __launch_bounds__(kThreads) k_add_force(const StepArgs a, T* pop
   }
 }
 
-// Ghost fill: copy descriptors first (one thread per cell of a region, all 19
-// populations), then single-population bounce-back writes.
-template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_ghost(T* pops, long long qs, const CopyDesc* cd, const uint32_t* cd_start, int ncd,
-        uint32_t ncopy, const BBOp* bb, uint32_t nbb, float scale, float inv_scale) {
-  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
-  if (t < ncopy) {
-    pdl_wait();
-    int lo = 0, hi = ncd - 1;
-    while (lo < hi) {  // last descriptor whose start <= t
-      const int mid = (lo + hi + 1) >> 1;
-      if (cd_start[mid] <= t) lo = mid; else hi = mid - 1;
-    }
-    const CopyDesc d = cd[lo];
-    const uint32_t k = t - cd_start[lo];
-    const int a0 = static_cast<int>(k / d.n1), a1 = static_cast<int>(k % d.n1);
-    const long long s = d.src + static_cast<long long>(a0) * d.s0 + static_cast<long long>(a1) * d.s1;
-    const long long o = d.dst + static_cast<long long>(a0) * d.d0 + static_cast<long long>(a1) * d.d1;
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) pops[i * qs + o] = pops[i * qs + s];
-    return;
-  }
-  const uint32_t u = t - ncopy;
-  if (u >= nbb) return;
-  const BBOp op = bb[u];
-  pdl_wait();
-  const float v = Store<T>::ld(pops + op.src_pop * qs + op.src, inv_scale) + op.add;
-  Store<T>::st(pops + op.pop * qs + op.dst, v, scale);
-}
 
 constexpr int kProlongThreads = 64;  // few items: spread them over more SMs
 template <typename T>
@@ -482,7 +467,7 @@ k_drag(const StepArgs a, const DragItem* items, int nitems, double* partial) {
             const long long nb = resolve(a, c.b, static_cast<int>(c.x) + 1 + cx(j),
                                          static_cast<int>(c.y) + 1 + cy(j), static_cast<int>(c.z) + 1 + cz(j), nhalo);
             const int nk = nhalo ? kBulk : (a.flags[nb] & kKindMask);
-            const float f_q = nk == kBulk ? LD(src, a.qs, j, nb, a.inv_scale) : own[j];
+            const float f_q = nk == kBulk ? pull_value(a, src, j, nb) : own[j];
             f_bar = bouzidi(own[i], f_q, own[j], q);
           }
           f_bar += a.link_rec[li * 38 + kQ + j];
@@ -697,16 +682,6 @@ cudaError_t launch_add_force(const StepArgs& a, T* pops, const float* force, cud
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
-template <typename T>
-cudaError_t launch_ghost(T* pops, long long qs, const CopyDesc* cd, const uint32_t* cd_start, int ncd,
-                         uint32_t ncopy, const BBOp* bb, uint32_t nbb, float scale, float inv_scale,
-                         cudaStream_t s) {
-  const uint32_t total = ncopy + nbb;
-  if (total == 0) return cudaSuccess;
-  const cudaError_t e = launch_chain(k_ghost<T>, dim3(grid_for(total)), dim3(kThreads), 0, s, pops, qs, cd, cd_start, ncd, ncopy, bb, nbb, scale,
-                                                  inv_scale);
-  return e != cudaSuccess ? e : cudaGetLastError();
-}
 
 template <typename T>
 cudaError_t launch_prolong(const ProlongItem* items, int n, const float* coarse_save, float* prev,
@@ -770,8 +745,6 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
   template cudaError_t launch_step_near<T>(const StepArgs&, const NearTables&, cudaStream_t);       \
   template cudaError_t launch_add_force<T>(const StepArgs&, T*, const float*, cudaStream_t);         \
   template cudaError_t launch_step_map<T>(const StepArgs&, const NearTables&, bool, bool, int, cudaStream_t); \
-  template cudaError_t launch_ghost<T>(T*, long long, const CopyDesc*, const uint32_t*, int,       \
-                                       uint32_t, const BBOp*, uint32_t, float, float, cudaStream_t); \
   template cudaError_t launch_prolong<T>(const ProlongItem*, int, const float*, float*, int, T*,   \
                                          long long, float, float, float, cudaStream_t);            \
   template cudaError_t launch_restrict<T>(const RestrictItem*, int, const float*, T*, long long,   \

@@ -21,9 +21,6 @@ namespace octlb_gpu {
 
 template <typename T> cudaError_t launch_step(const StepArgs&, bool, bool, bool, cudaStream_t);
 template <typename T>
-cudaError_t launch_ghost(T*, long long, const CopyDesc*, const uint32_t*, int, uint32_t, const BBOp*,
-                         uint32_t, float, float, cudaStream_t);
-template <typename T>
 cudaError_t launch_prolong(const ProlongItem*, int, const float*, float*, int, T*, long long, float,
                            float, float, cudaStream_t);
 template <typename T>
@@ -46,9 +43,8 @@ bool map_step_eligible(int n, long long nslots);
 void set_programmatic_launch(bool on);
 cudaError_t launch_adj_step(const StepArgs&, const NearTables&, bool, bool, float*, float*, float*, double*, double*,
                             cudaStream_t);
-cudaError_t launch_adj_ghost(float*, long long, const BBOp*, uint32_t, double*, cudaStream_t);
 cudaError_t launch_adj_force(const StepArgs&, const float*, double*, cudaStream_t);
-cudaError_t launch_adj_drag(const StepArgs&, bool, const DragItem*, int, float*, float, int, cudaStream_t);
+cudaError_t launch_adj_drag(const StepArgs&, bool, const DragItem*, int, float*, float, int, double*, cudaStream_t);
 cudaError_t launch_adj_prolong(const ProlongItem*, int, const float*, const float*, int, float*, long long, float,
                                float, float*, float*, float*, double*, double*, long long, cudaStream_t);
 cudaError_t launch_adj_restrict(const RestrictItem*, int, const float*, float*, long long, float, float, float*,
@@ -109,7 +105,8 @@ struct Level {
   int n_open = 0, n_halo = 0, n_pages = 0, n_save = 0, n_links = 0;
   bool has_flags = false;
   // tree-boundary halo fills
-  DevBuf bb_ops;
+  DevBuf bb_ops, fill_of;           // fills, and per (page slot, population) the fill index or -1
+  DevBuf wall_add, wall_dadd;       // slot-map wall markers' terms
   uint32_t n_bb = 0;
   // coupler: this level as coarse (prolong) and as fine (restrict)
   DevBuf prolong_items, prev, restrict_items;
@@ -302,13 +299,14 @@ int do_advance_level(octlb_ctx* ctx, int l);
 template <typename T>
 int launch_level_step(octlb_ctx* ctx, Level& L) {
   if (L.nblk == 0) return OCTLB_OK;
-  // Body force on the stored post-collision state, then the ghost fill into
-  // the buffer the step reads (reference: apply() then exchange() after
-  // collide, time_loop.h:207-211).
+  // Body force on the stored post-collision state (the reference's apply()
+  // hook after collide, time_loop.h:207-211).  The boundary fills and the
+  // same-level exchange that follow there need no launch: the step reads
+  // neighbour cores through the slot map and fill targets from their
+  // sources.
   T* cur = static_cast<T*>(cur_buf(L));
   if (L.has_force) CK(launch_add_force<T>(L.args, cur, L.body_force.as<float>(), ctx->stream));
-  CK(launch_ghost<T>(cur, L.nslots, nullptr, nullptr, 0, 0, L.bb_ops.as<BBOp>(), L.n_bb, L.scale, L.inv_scale,
-                     ctx->stream));
+
   StepArgs a = L.args;
   a.src = cur;
   a.dst = L.buf[1 - L.cur].p;
@@ -893,6 +891,9 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       bbv.push_back(BBOp{ncore + static_cast<long long>(page_of[op.lb]) * H + hmap[op.hlin], op.src, op.pop,
                          op.src_pop, op.add, op.dadd});
     L.n_bb = static_cast<uint32_t>(bbv.size());
+    std::vector<int> fill_of_h(static_cast<size_t>(L.n_pages) * H * kQ, -1);
+    for (size_t k = 0; k < bbv.size(); ++k)
+      fill_of_h[static_cast<size_t>(bbv[k].dst - ncore) * kQ + bbv[k].pop] = static_cast<int>(k);
 
     // Slot bases of the 27 directions: own core (centre), the neighbour's core
     // shifted by one block edge, or the own halo page.
@@ -923,6 +924,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       return -1;
     };
     std::vector<int> slot_map;
+    std::vector<float> wall_add, wall_dadd;  // per moving-wall position: the 19 wall terms, their velocity derivative
     if (map_step_eligible(n, L.nslots) && !(ctx->periodic && !L.has_flags)) {
       slot_map.assign(static_cast<size_t>(L.nblk) * np3, 0);
       std::vector<uint8_t> unresolved(static_cast<size_t>(np3));
@@ -936,6 +938,52 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
               unresolved[P] = sl < 0;
               if (sl >= L.nslots) return fail(ctx, OCTLB_EINVAL, "internal: slot map out of range");
               m[P] = sl < 0 ? static_cast<int>(static_cast<long long>(lb) * n3) : static_cast<int>(sl);
+              if (sl < ncore) continue;
+              // A halo-page position whose pulled populations are boundary
+              // fills: an outflow copy becomes its source cell's slot, a
+              // bounce-back wall the marker -1 (at rest) or -(2 + k) (moving,
+              // row k of the wall-term table); the pull then reads the
+              // cell's own opposite population.
+              int nfill = 0, npull = 0, ncopy = 0, nbb = 0;
+              long long copy_src = -1;
+              bool moving = false;
+              for (int i = 1; i < kQ; ++i) {
+                const int Xs = X + cx(i), Ys = Y + cy(i), Zs = Z + cz(i);
+                if (Xs < 1 || Ys < 1 || Zs < 1 || Xs > n || Ys > n || Zs > n) continue;
+                ++npull;
+                const int fo = fill_of_h[static_cast<size_t>(sl - ncore) * kQ + i];
+                if (fo < 0) continue;
+                ++nfill;
+                const BBOp& op = bbv[fo];
+                if (op.src_pop == i) {
+                  if (copy_src >= 0 && copy_src != op.src) return fail(ctx, OCTLB_EINVAL, "internal: mixed fill position");
+                  copy_src = op.src;
+                  ++ncopy;
+                } else if (op.src_pop == opp(i) && op.src == core_slot_of(n, lb, Xs - 1, Ys - 1, Zs - 1)) {
+                  ++nbb;
+                  moving = moving || op.add != 0.f;
+                } else {
+                  return fail(ctx, OCTLB_EINVAL, "internal: unexpected fill source");
+                }
+              }
+              if (nfill == 0) continue;
+              if (nfill != npull || (ncopy > 0 && nbb > 0)) return fail(ctx, OCTLB_EINVAL, "internal: mixed fill position");
+              if (ncopy > 0) {
+                m[P] = static_cast<int>(copy_src);
+              } else if (!moving) {
+                m[P] = -1;
+              } else {
+                const int k = static_cast<int>(wall_add.size() / kQ);
+                wall_add.resize(wall_add.size() + kQ, 0.f);
+                wall_dadd.resize(wall_dadd.size() + kQ, 0.f);
+                for (int i = 1; i < kQ; ++i) {
+                  const int fo = fill_of_h[static_cast<size_t>(sl - ncore) * kQ + i];
+                  if (fo < 0) continue;
+                  wall_add[static_cast<size_t>(k) * kQ + i] = bbv[fo].add;
+                  wall_dadd[static_cast<size_t>(k) * kQ + i] = bbv[fo].dadd;
+                }
+                m[P] = -(2 + k);
+              }
             }
         for (int x = 0; x < n; ++x)
           for (int y = 0; y < n; ++y)
@@ -1088,6 +1136,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     L.near = NearTables{L.near_cells.as<int>(), L.near_mask.as<uint32_t>(), L.near_slot.as<int>(),
                         L.near_q.as<float>(), L.near_add.as<float>(), L.n_near};
     CK(upload(L.bb_ops, bbv));
+    CK(upload(L.fill_of, fill_of_h));
     CK(upload(L.prolong_items, prolong[l]));
     CK(upload(L.restrict_items, restrict_items[l]));
     L.n_prolong = static_cast<int>(prolong[l].size());
@@ -1131,6 +1180,8 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       A.off_pad[i] = cx(i) * np * np + cy(i) * np + cz(i);
     }
     A.err = ctx->dev_err.as<int>();
+    A.fill_of = L.n_bb > 0 ? L.fill_of.as<int>() : nullptr;
+    A.fills = L.bb_ops.as<BBOp>();
     // One all-kBulk periodic block: paired vector step by default, the
     // pipelined bulk-copy step on request (OCTLB_STEP_KERNEL=bulk), the plain
     // one-cell-per-thread step with OCTLB_STEP_KERNEL=plain.
@@ -1142,7 +1193,11 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     if (!uniform && ctx->step_kernel == 0 && map_step_eligible(n, L.nslots)) {
       L.use_map = true;
       CK(upload(L.slot_map, slot_map));
+      CK(upload(L.wall_add, wall_add));
+      CK(upload(L.wall_dadd, wall_dadd));
       A.slot_map = L.slot_map.as<int>();
+      A.wall_add = L.wall_add.as<float>();
+      A.wall_dadd = L.wall_dadd.as<float>();
     }
     if (uniform && ctx->step_kernel == 1 && bulk_step_eligible(n, sizeof(T)) && !g_dry_run) {
       const int per_sm = bulk_prepare<T>(n);
@@ -1316,8 +1371,7 @@ int adj_step(octlb_ctx* ctx, int l, const StepRecord& R, float coef) {
   CK(launch_adj_step(a, L.near, links, L.has_flags, lamY, lamX, V.lam_save.as<float>(), g, V.gF.as<double>(),
                      ctx->stream));
   if (R.drag && coef != 0.f)
-    CK(launch_adj_drag(a, links, L.drag_items.as<DragItem>(), L.n_drag, lamX, coef, A.comp, ctx->stream));
-  CK(launch_adj_ghost(lamX, L.nslots, L.bb_ops.as<BBOp>(), L.n_bb, g, ctx->stream));
+    CK(launch_adj_drag(a, links, L.drag_items.as<DragItem>(), L.n_drag, lamX, coef, A.comp, g, ctx->stream));
   V.cur = 1 - V.cur;
   return OCTLB_OK;
 }
@@ -1969,7 +2023,7 @@ int octlb_gpu_step_stats(const octlb_ctx* ctx, long long* launches, long long* l
   for (size_t l = 0; l < ctx->levels.size(); ++l) {
     const Level& L = ctx->levels[l];
     if (L.nblk == 0) continue;
-    per[l] = (L.n_bb > 0 ? 1 : 0) + (L.args.nitems > 0 ? 1 : 0) + (L.n_near > 0 && !L.use_pair && !L.use_bulk && !L.use_map ? 1 : 0) + (L.has_force ? 1 : 0);
+    per[l] = (L.args.nitems > 0 ? 1 : 0) + (L.n_near > 0 && !L.use_pair && !L.use_bulk && !L.use_map ? 1 : 0) + (L.has_force ? 1 : 0);
     if (ctx->drag && L.n_drag > 0) total += 1;  // once per advance_one, last step of the level
   }
   for (size_t l = 0; l < ctx->levels.size(); ++l) {

@@ -35,6 +35,10 @@ struct StepArgs {
   const int* hpos;          // [n_halo] halo index -> padded linear position
   const int* open_pages;    // [n_open][4] torus-streamed halo items: page, block, halo index, population
   const int* slot_map;      // [nblk][(n+2)^3] slot of every padded position (k_step_map levels)
+  const int* fill_of;       // [n_pages * n_halo][19] boundary fill writing (page slot, population), or -1
+  const struct BBOp* fills; // the fills (never materialised: readers take the source, pull_value)
+  const float* wall_add;    // [k][19] wall terms of slot-map marker -(2 + k) (moving bounce-back wall)
+  const float* wall_dadd;   // [k][19] their derivative by the wall-velocity scale
   int n_open, n_halo;       // items, halo slots per page
   int nblk, n, np;          // np = n + 2
   long long halo_base;      // first halo-page slot (= nblk * n^3)
@@ -67,15 +71,9 @@ constexpr long long kOwnPage = -(1LL << 62);
 // Device error codes written to StepArgs::err.
 enum : int { kErrNone = 0, kErrBulkTimeout = 1, kErrHalo = 2 };
 
-// Rectangular halo copy (same-level face / edge exchange, outflow ghost copy):
-// dst(a,b) <- src(a,b) for all 19 populations.
-struct CopyDesc {
-  long long src, dst;       // first slot
-  int n0, n1;
-  int s0, s1, d0, d1;       // slot strides along the two region axes
-};
-// Single-population halo write: pops[pop][dst] = pops[src_pop][src] + add
-// (bounce-back wall: src_pop = opp(pop); outflow ghost copy: src_pop = pop).
+// Tree-boundary fill of one halo-page population: value(dst, pop) =
+// g_src_pop(src) + add (bounce-back wall: src_pop = opp(pop); outflow ghost
+// copy: src_pop = pop).  Never stored: readers evaluate it (pull_value).
 struct BBOp {
   long long dst, src;
   int pop, src_pop;
