@@ -167,7 +167,28 @@ __device__ __forceinline__ float bgk_vjp(const float (&f)[kQ], float omega, cons
   return dom;
 }
 
-
+// bgk_vjp with the cotangent replaced in place (mu -> lam), to spare the
+// registers of a third 19-wide array.
+__device__ __forceinline__ float bgk_vjp_inplace(const float (&f)[kQ], float omega, float (&mu)[kQ]) {
+  float dh, jx, jy, jz;
+  moments(f, dh, jx, jy, jz);
+  const float rho = 1.0f + dh, k = 1.0f / rho;
+  const float ux = jx * k, uy = jy * k, uz = jz * k;
+  const float usq = ux * ux + uy * uy + uz * uz;
+  float dom = 0.f;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const float cu = cx(i) * ux + cy(i) * uy + cz(i) * uz;
+    const float feq = wf(i) * (dh + rho * (3.0f * cu + 4.5f * cu * cu - 1.5f * usq));
+    dom += mu[i] * (feq - f[i]);
+  }
+  float P, Vx, Vy, Vz;
+  feq_vjp(mu, rho, ux, uy, uz, P, Vx, Vy, Vz);
+#pragma unroll
+  for (int j = 0; j < kQ; ++j)
+    mu[j] = (1.0f - omega) * mu[j] + omega * (P + (Vx * (cx(j) - ux) + Vy * (cy(j) - uy) + Vz * (cz(j) - uz)) * k);
+  return dom;
+}
 
 // VJP of read_macro (level_coupler.cpp:183-189) at the saved populations f:
 // cotangent lm of (drho, u, f_neq) -> cotangent lf of f.
@@ -254,10 +275,10 @@ __device__ __forceinline__ float adj_near_cell(const StepArgs& a, const NearTabl
     float lam = mu;
     if ((fl & kKindMask) == kBulk) {
       force_grad_lanes(d, mu, gF, a.ncore, t, lane);
-      float fa[kQ];
-      gather_lanes(f, fa);
-      float dh, jx, jy, jz;
-      moments(fa, dh, jx, jy, jz);
+      // moments by warp sums (the linearisation point needs no bitwise match)
+      const float fa = d.act ? f : 0.f;
+      const float dh = warp_sum(fa);
+      const float jx = warp_sum(fa * d.cx), jy = warp_sum(fa * d.cy), jz = warp_sum(fa * d.cz);
       const float rho = 1.0f + dh, kr = 1.0f / rho;
       const float ux = jx * kr, uy = jy * kr, uz = jz * kr;
       const float usq = ux * ux + uy * uy + uz * uz;
@@ -303,7 +324,7 @@ __device__ __forceinline__ float adj_near_cell(const StepArgs& a, const NearTabl
 // halo rotation items.  a.src = the step's input (after force and fills);
 // lamY = cotangent of the step's output, lamX += cotangent of its input.
 template <bool LINKS, bool FLAGS>
-__global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const NearTables nt, float* __restrict__ lamY,
+__global__ void __launch_bounds__(kThreads, 3) k_adj_step(const StepArgs a, const NearTables nt, float* __restrict__ lamY,
                                                       float* lamX, float* __restrict__ lamS, double* g,
                                                       double* gF) {
   extern __shared__ int smap[];
@@ -311,6 +332,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const N
   // first CTAs: the near-wall cells, one warp each
   const uint32_t near_ctas = LINKS ? (static_cast<uint32_t>(nt.n) + kThreads / 32 - 1) / (kThreads / 32) : 0;
   if (LINKS && blockIdx.x < near_ctas) {
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     float gw = 0.f;
     const float dom = adj_near_cell(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)), lane,
@@ -323,6 +345,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const N
   const uint32_t b = bid / kParts, part = bid % kParts;
   const long long qs = a.qs;
   if (b >= static_cast<uint32_t>(a.nblk)) {
+    pdl_wait();
     const uint32_t k = (bid - a.nblk * kParts) * kThreads + threadIdx.x;
     float gw = 0.f;
     if (k < static_cast<uint32_t>(a.n_open)) {
@@ -339,6 +362,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const N
   const int* gm = a.slot_map + static_cast<long long>(b) * np3;
   for (int k = threadIdx.x; k < np3; k += kThreads) smap[k] = gm[k];
   __syncthreads();
+  pdl_wait();
   const float* src = static_cast<const float*>(a.src);
   const uint32_t n = a.n, n3 = n * n * n, span = n3 / kParts;
   double dom = 0.0;
@@ -357,22 +381,19 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const N
       continue;
     }
     if (LINKS && (fl & kFlagNear)) continue;  // k_adj_near
-    float f[kQ], mu[kQ], lam[kQ];
+    float f[kQ], lam[kQ];
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
       const int sm = smap[P - a.off_pad[i]];  // < 0: bounce-back wall position (see k_step_map)
       const float v = src[sm >= 0 ? i * qs + sm : opp(i) * qs + t];
       f[i] = sm < -1 ? v + a.wall_add[(-sm - 2) * kQ + i] : v;
-      mu[i] = lamY[i * qs + t];
+      lam[i] = lamY[i * qs + t];  // the output's cotangent, turned into the input's below
       lamY[i * qs + t] = 0.f;
     }
     const bool bulk = !FLAGS || (fl & kKindMask) == kBulk;
-    if (bulk) force_grad(mu, gF, a.ncore, t);
     if (bulk) {
-      dom += bgk_vjp(f, a.omega, mu, lam);
-    } else {
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) lam[i] = mu[i];
+      force_grad(lam, gF, a.ncore, t);
+      dom += bgk_vjp_inplace(f, a.omega, lam);
     }
     if (FLAGS && (fl & kFlagSave)) {
       float* ls = lamS + static_cast<long long>(a.save_idx[t]) * kQ;
@@ -399,6 +420,8 @@ __global__ void __launch_bounds__(kThreads) k_adj_step(const StepArgs a, const N
 // is lam.  gF is [3][ncore] FP64.
 __global__ void __launch_bounds__(kThreads) k_adj_force(const StepArgs a, const float* __restrict__ lam,
                                                        double* gF) {
+  pdl_wait();
+
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   if (t >= a.ncore) return;
   if (a.flags && (a.flags[t] & kKindMask) != kBulk) return;
@@ -471,6 +494,7 @@ __device__ __forceinline__ void adj_drag_item(const StepArgs& a, const DragItem 
 template <bool LINKS>
 __global__ void __launch_bounds__(kThreads) k_adj_drag(const StepArgs a, const DragItem* items, int nitems,
                                                       float* lamX, float coef, int comp, double* g) {
+  pdl_wait();
   const int t = blockIdx.x * kThreads + threadIdx.x;
   float gw = 0.f;
   if (t < nitems) adj_drag_item<LINKS>(a, items[t], lamX, coef, comp, gw);
@@ -489,6 +513,8 @@ __global__ void __launch_bounds__(kThreads)
 k_adj_prolong(const ProlongItem* items, int nitems, const float* coarse_save, const float* prev, int half,
               float* lam_fine, long long fine_qs, float s, float omega, float* lam_m, float* lam_prev,
               float* lam_save, double* g, double* gF_fine, long long fine_ncore) {
+  pdl_wait();
+
   const int w = (blockIdx.x * kThreads + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   float ds = 0.f, dom = 0.f;
@@ -552,6 +578,8 @@ k_adj_prolong(const ProlongItem* items, int nitems, const float* coarse_save, co
 __global__ void __launch_bounds__(kThreads)
 k_adj_restrict(const RestrictItem* items, int nitems, const float* fine_save, float* lam_coarse, long long coarse_qs,
                float s, float omega, float* lam_save, double* g, double* gF_coarse, long long coarse_ncore) {
+  pdl_wait();
+
   const int w = (blockIdx.x * kThreads + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   float ds = 0.f, dom = 0.f;
@@ -623,43 +651,48 @@ inline uint32_t grid_of(long long items, int threads) { return static_cast<uint3
 // ---------------------------------------------------------------- launchers
 cudaError_t launch_adj_step(const StepArgs& a, const NearTables& nt, bool links, bool flags, float* lamY, float* lamX,
                             float* lamS, double* g, double* gF, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
   const uint32_t near_ctas = links ? grid_of(static_cast<long long>(nt.n) * 32, kThreads) : 0;
   const dim3 grid(near_ctas + static_cast<uint32_t>(a.nblk) * 2 + grid_of(a.n_open, kThreads));
   const size_t smem = static_cast<size_t>(a.np) * a.np * a.np * sizeof(int);
-  if (links) k_adj_step<true, true><<<grid, kThreads, smem, s>>>(a, nt, lamY, lamX, lamS, g, gF);
-  else if (flags) k_adj_step<false, true><<<grid, kThreads, smem, s>>>(a, nt, lamY, lamX, lamS, g, gF);
-  else k_adj_step<false, false><<<grid, kThreads, smem, s>>>(a, nt, lamY, lamX, lamS, g, gF);
-  return cudaGetLastError();
+  if (links) e = launch_chain(k_adj_step<true, true>, dim3(grid), dim3(kThreads), smem, s, a, nt, lamY, lamX, lamS, g, gF);
+  else if (flags) e = launch_chain(k_adj_step<false, true>, dim3(grid), dim3(kThreads), smem, s, a, nt, lamY, lamX, lamS, g, gF);
+  else e = launch_chain(k_adj_step<false, false>, dim3(grid), dim3(kThreads), smem, s, a, nt, lamY, lamX, lamS, g, gF);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 cudaError_t launch_adj_force(const StepArgs& a, const float* lam, double* gF, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
   if (a.ncore == 0) return cudaSuccess;
-  k_adj_force<<<grid_of(a.ncore, kThreads), kThreads, 0, s>>>(a, lam, gF);
-  return cudaGetLastError();
+  e = launch_chain(k_adj_force, dim3(grid_of(a.ncore, kThreads)), dim3(kThreads), 0, s, a, lam, gF);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 cudaError_t launch_adj_drag(const StepArgs& a, bool links, const DragItem* items, int n, float* lamX, float coef,
                             int comp, double* g, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
   if (n == 0) return cudaSuccess;
-  if (links) k_adj_drag<true><<<grid_of(n, kThreads), kThreads, 0, s>>>(a, items, n, lamX, coef, comp, g);
-  else k_adj_drag<false><<<grid_of(n, kThreads), kThreads, 0, s>>>(a, items, n, lamX, coef, comp, g);
-  return cudaGetLastError();
+  if (links) e = launch_chain(k_adj_drag<true>, dim3(grid_of(n, kThreads)), dim3(kThreads), 0, s, a, items, n, lamX, coef, comp, g);
+  else e = launch_chain(k_adj_drag<false>, dim3(grid_of(n, kThreads)), dim3(kThreads), 0, s, a, items, n, lamX, coef, comp, g);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 cudaError_t launch_adj_prolong(const ProlongItem* items, int n, const float* coarse_save, const float* prev, int half,
                                float* lam_fine, long long fine_qs, float scale, float omega, float* lam_m,
                                float* lam_prev, float* lam_save, double* g, double* gF_fine, long long fine_ncore,
                                cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
   if (n == 0) return cudaSuccess;
-  k_adj_prolong<<<grid_of(static_cast<long long>(n) * 32, kThreads), kThreads, 0, s>>>(
+  e = launch_chain(k_adj_prolong, dim3(grid_of(static_cast<long long>(n) * 32, kThreads)), dim3(kThreads), 0, s,
       items, n, coarse_save, prev, half, lam_fine, fine_qs, scale, omega, lam_m, lam_prev, lam_save, g, gF_fine,
       fine_ncore);
-  return cudaGetLastError();
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 cudaError_t launch_adj_restrict(const RestrictItem* items, int n, const float* fine_save, float* lam_coarse,
                                 long long coarse_qs, float scale, float omega, float* lam_save, double* g,
                                 double* gF_coarse, long long coarse_ncore, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
   if (n == 0) return cudaSuccess;
-  k_adj_restrict<<<grid_of(static_cast<long long>(n) * 32, kThreads), kThreads, 0, s>>>(
+  e = launch_chain(k_adj_restrict, dim3(grid_of(static_cast<long long>(n) * 32, kThreads)), dim3(kThreads), 0, s,
       items, n, fine_save, lam_coarse, coarse_qs, scale, omega, lam_save, g, gF_coarse, coarse_ncore);
-  return cudaGetLastError();
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 }  // namespace octlb_gpu

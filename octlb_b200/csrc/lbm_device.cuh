@@ -7,6 +7,8 @@
 #include "octlb_internal.h"
 
 namespace octlb_gpu {
+// Programmatic dependent launches enabled on this host thread (lbm_kernels.cu).
+bool programmatic_launch();
 namespace {
 
 constexpr int kThreads = 256;
@@ -214,6 +216,26 @@ __device__ inline void block_reduce(double (&v)[N]) {
   __syncthreads();  // sm is reused by the next reduction of the same width
 }
 
+// Launches of the time-step chain: with the programmatic stream-serialisation
+// attribute when enabled, so each kernel is launched as its predecessor's
+// CTAs exit and runs its constant-table prologue before pdl_wait (every such
+// kernel calls pdl_wait before its first dependent access).  No kernel
+// triggers its dependents early: measured on the forest cases, an early
+// trigger gained nothing over the implicit trigger at CTA exit.
+template <typename... P, typename... A>
+cudaError_t launch_chain(void (*k)(P...), dim3 g, dim3 b, size_t smem, cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = g;
+  cfg.blockDim = b;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = programmatic_launch() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
 }  // namespace
 }  // namespace octlb_gpu
 

@@ -583,33 +583,16 @@ k_scatter(const StepArgs a, const double* in) {
 
 inline uint32_t grid_for(uint32_t items) { return (items + kThreads - 1) / kThreads; }
 
-// Launches of the time-step chain: with the programmatic stream-serialisation
-// attribute when enabled, so each kernel is launched as its predecessor's
-// CTAs exit and runs its constant-table prologue before pdl_wait (every such
-// kernel calls pdl_wait before its first dependent access).  No kernel
-// triggers its dependents early: measured on the forest cases, an early
-// trigger gained nothing over the implicit trigger at CTA exit.
-thread_local bool g_programmatic = false;
-template <typename... P, typename... A>
-cudaError_t launch_chain(void (*k)(P...), dim3 g, dim3 b, size_t smem, cudaStream_t s, A&&... args) {
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = g;
-  cfg.blockDim = b;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = g_programmatic ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
-}
 
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
 // Programmatic launches for the time-step chain on this host thread.
+namespace {
+thread_local bool g_programmatic = false;
+}
 void set_programmatic_launch(bool on) { g_programmatic = on; }
+bool programmatic_launch() { return g_programmatic; }
 
 template <typename T>
 cudaError_t launch_step(const StepArgs& a, bool periodic, bool links, bool flags, cudaStream_t s) {

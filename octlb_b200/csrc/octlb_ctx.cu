@@ -1600,6 +1600,7 @@ int adjoint_impl(octlb_ctx* ctx, const octlb_adj_params* p, double* objective, d
     A.graph_params = gp;
   }
   { int rc = prealloc_records<T>(ctx, K); if (rc) return rc; }
+  const ProgrammaticScope pdl(ctx->use_pdl);
   auto set_parity = [&](uint64_t m) {
     for (size_t l = 0; l < nl; ++l) ctx->levels[l].cur = (m >> l) & 1;
   };
