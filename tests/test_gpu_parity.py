@@ -278,3 +278,54 @@ def test_graph_and_programmatic_launch_bitwise_equal(ob, case, monkeypatch):
     for p1, f1, c1, s1 in res[1:]:
         assert np.array_equal(p0, p1) and np.array_equal(f0, f1) and c0 == c1
         assert np.array_equal(s0[0], s1[0]) and s0[1] == s1[1] == 9
+
+
+def test_body_force_matches_reference(ob, ref):
+    """A nonzero per-cell body force: GPU fields and MEM force per coarse step
+    against the reference TimeLoop with the same forcing term added at its
+    DomainBoundaryHandler::apply() hook (restated there)."""
+    mesh, init, info = small_cylinder(ob)
+    rng = np.random.default_rng(7)
+    F = rng.normal(0.0, 1e-5, size=(mesh.n_blocks, mesh.n ** 3, 3))
+    F[..., 0] += 2e-5
+    lat = ob.GpuLattice(mesh, info["omega"], stream_mode=ob.STREAM_LINKS, drag=True, init_pops=init)
+    lat.set_body_force(F)
+    sim = oracle.Sim(ref, mesh, info["omega"], init, link_mode=True)
+    sim.set_body_force(F)
+    for step in range(10):
+        lat.advance(1)
+        sim.advance(1)
+        fg, fr = lat.force(), sim.drag(mesh.obstacle)
+        assert np.max(np.abs(fg - fr)) <= 1e-5 * max(np.max(np.abs(fr)), 1e-6), (step, fg, fr)
+    rho_g, u_g = lat.get_fields()
+    rho_r, u_r = fields_of(sim.core())
+    fl = mesh.kinds == ob.BULK
+    assert rel(rho_g[fl], rho_r[fl]) <= TOL32
+    assert rel(u_g[fl], u_r[fl]) <= TOL32
+    # removing the force restores the plain forward
+    lat.set_body_force(None)
+    lat.close()
+
+
+def test_adjoint_and_body_force_argument_checks(ob):
+    mesh, init, info = small_cylinder(ob)
+    lat16 = ob.GpuLattice(mesh, info["omega"], precision=ob.FP16_SHIFTED, stream_mode=ob.STREAM_LINKS, drag=True,
+                          init_pops=init)
+    with pytest.raises(ob.OctlbError):
+        lat16.adjoint(4, 2)                  # FP16 storage is not differentiated
+    lat16.close()
+    nodrag = ob.GpuLattice(mesh, info["omega"], stream_mode=ob.STREAM_LINKS, init_pops=init)
+    with pytest.raises(ob.OctlbError):
+        nodrag.adjoint(4, 2)                 # the objective needs the drag
+    nodrag.close()
+    lat = ob.GpuLattice(mesh, info["omega"], stream_mode=ob.STREAM_LINKS, drag=True, init_pops=init)
+    for steps, window in ((0, 0), (4, 0), (4, 5)):
+        with pytest.raises(ob.OctlbError):
+            lat.adjoint(steps, window)
+    bad = np.zeros((mesh.n_blocks, mesh.n ** 3, 3))
+    bad[0, 0, 0] = np.nan
+    with pytest.raises(ob.OctlbError):
+        lat.set_body_force(bad)
+    with pytest.raises(ValueError):
+        lat.set_body_force(np.zeros(5))
+    lat.close()
