@@ -315,6 +315,9 @@ def run_single_case(args, ob, cases, torch):
     if args.case == "amr_cavity_64":
         mesh, init, info = cases.cavity_forest(cells=64, n=8, lid=0.05, tau=0.56, band_cells=8)
         mode, drag = ob.STREAM_ROTATE, False
+    elif args.case == "cylinder_512":
+        mesh, init, info = cases.cylinder_forest(length=512, height=128, diameter=32.0, center=(128.0, 64.0))
+        mode, drag = ob.STREAM_LINKS, True
     else:
         mesh, init, info = cases.cylinder_forest()
         mode, drag = ob.STREAM_LINKS, True
@@ -345,7 +348,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-forest", action="store_true", help="skip the forest / adjoint measurements")
-    ap.add_argument("--case", default="tgv", choices=["tgv", "amr_cavity_64", "cylinder", "adjoint"],
+    ap.add_argument("--case", default="tgv", choices=["tgv", "amr_cavity_64", "cylinder", "cylinder_512", "adjoint"],
                     help="tgv: the headline line; otherwise run only that case for --steps advance_one "
                          "calls (or one adjoint sweep of --steps calls) and print its timing (profiling)")
     args = ap.parse_args()
