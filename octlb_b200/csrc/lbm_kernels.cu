@@ -239,9 +239,9 @@ __device__ __forceinline__ void map_cell_finish(const StepArgs& a, uint32_t t, u
 // its cells, so small levels still give every SM work.  Under the links rule
 // the first CTAs of the launch take the near-wall cells (one warp each), so
 // they run beside the bulk instead of in a launch of their own.
-template <typename T, bool LINKS, bool FLAGS, int CPT>
+template <typename T, bool LINKS, bool FLAGS, int CPT, bool GMAP>
 __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const StepArgs a, const NearTables nt) {
-  extern __shared__ int smap[];  // (n+2)^3 slots of this block
+  extern __shared__ int smap_s[];  // (n+2)^3 slots of this block
   constexpr uint32_t kParts = CPT == 1 ? 2 : 1;
   const uint32_t near_ctas = LINKS ? (static_cast<uint32_t>(nt.n) + kThreads / 32 - 1) / (kThreads / 32) : 0;
   if (LINKS && blockIdx.x < near_ctas) {
@@ -257,8 +257,13 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
   }
   const int np = a.np, np3 = np * np * np;
   const int* gm = a.slot_map + static_cast<long long>(b) * np3;
-  for (int k = threadIdx.x; k < np3; k += kThreads) smap[k] = gm[k];
-  __syncthreads();
+  if constexpr (!GMAP) {
+    for (int k = threadIdx.x; k < np3; k += kThreads) smap_s[k] = gm[k];
+    __syncthreads();
+  }
+  // GMAP: the map is read through the read-only L1 path instead (no staging
+  // barrier); 4 KB per block stays L1-resident for the CTA
+  const int* smap = GMAP ? gm : smap_s;
   pdl_wait();
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
@@ -287,7 +292,7 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
         // bounce-back wall position (marker < 0): the cell's own opposite
         // population, plus the wall term when it moves; branch-free so the
         // 19 (or 38) loads stay independent
-        const int sm = smap[P[c] - a.off_pad[i]];
+        const int sm = GMAP ? __ldg(smap + P[c] - a.off_pad[i]) : smap[P[c] - a.off_pad[i]];
         const uint32_t off = sm >= 0 ? row + static_cast<uint32_t>(sm) : static_cast<uint32_t>(opp(i)) * qs + t[c];
         const float v = Store<T>::ld(src + off, a.inv_scale);
         f[c][i] = sm < -1 ? v + a.wall_add[(-sm - 2) * kQ + i] : v;
@@ -625,21 +630,23 @@ bool map_step_eligible(int n, long long nslots) {
   return n % 8 == 0 && np * np * np * 4 <= 48 * 1024 && nslots * kQ < (1LL << 32);
 }
 template <typename T>
-cudaError_t launch_step_map(const StepArgs& a, const NearTables& nt, bool links, bool flags, int cpt, cudaStream_t s) {
+cudaError_t launch_step_map(const StepArgs& a, const NearTables& nt, bool links, bool flags, int cpt, bool gmap,
+                            cudaStream_t s) {
   cudaError_t e = cudaSuccess;
   if (a.nitems == 0) return cudaSuccess;
   const uint32_t near_ctas = links ? grid_for(static_cast<uint32_t>(nt.n) * 32) : 0;
   const dim3 g(near_ctas + static_cast<uint32_t>(a.nblk) * (cpt == 2 ? 1 : 2) + grid_for(static_cast<uint32_t>(a.n_open)));
-  const size_t smem = static_cast<size_t>(a.np) * a.np * a.np * sizeof(int);
+  const size_t smem = gmap ? 0 : static_cast<size_t>(a.np) * a.np * a.np * sizeof(int);
+#define OCTLB_MAP_LAUNCH(C, G)                                                                              \
+  if (links) e = launch_chain(k_step_map<T, true, true, C, G>, g, dim3(kThreads), smem, s, a, nt);          \
+  else if (flags) e = launch_chain(k_step_map<T, false, true, C, G>, g, dim3(kThreads), smem, s, a, nt);    \
+  else e = launch_chain(k_step_map<T, false, false, C, G>, g, dim3(kThreads), smem, s, a, nt);
   if (cpt == 2) {
-    if (links) e = launch_chain(k_step_map<T, true, true, 2>, dim3(g), dim3(kThreads), smem, s, a, nt);
-    else if (flags) e = launch_chain(k_step_map<T, false, true, 2>, dim3(g), dim3(kThreads), smem, s, a, nt);
-    else e = launch_chain(k_step_map<T, false, false, 2>, dim3(g), dim3(kThreads), smem, s, a, nt);
+    if (gmap) { OCTLB_MAP_LAUNCH(2, true) } else { OCTLB_MAP_LAUNCH(2, false) }
   } else {
-    if (links) e = launch_chain(k_step_map<T, true, true, 1>, dim3(g), dim3(kThreads), smem, s, a, nt);
-    else if (flags) e = launch_chain(k_step_map<T, false, true, 1>, dim3(g), dim3(kThreads), smem, s, a, nt);
-    else e = launch_chain(k_step_map<T, false, false, 1>, dim3(g), dim3(kThreads), smem, s, a, nt);
+    if (gmap) { OCTLB_MAP_LAUNCH(1, true) } else { OCTLB_MAP_LAUNCH(1, false) }
   }
+#undef OCTLB_MAP_LAUNCH
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -727,7 +734,7 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
   template cudaError_t launch_step_pair<T>(const StepArgs&, cudaStream_t);                         \
   template cudaError_t launch_step_near<T>(const StepArgs&, const NearTables&, cudaStream_t);       \
   template cudaError_t launch_add_force<T>(const StepArgs&, T*, const float*, cudaStream_t);         \
-  template cudaError_t launch_step_map<T>(const StepArgs&, const NearTables&, bool, bool, int, cudaStream_t); \
+  template cudaError_t launch_step_map<T>(const StepArgs&, const NearTables&, bool, bool, int, bool, cudaStream_t); \
   template cudaError_t launch_prolong<T>(const ProlongItem*, int, const float*, float*, int, T*,   \
                                          long long, float, float, float, cudaStream_t);            \
   template cudaError_t launch_restrict<T>(const RestrictItem*, int, const float*, T*, long long,   \

@@ -37,7 +37,7 @@ template <typename T> int bulk_prepare(int n);
 template <typename T> cudaError_t launch_step_pair(const StepArgs&, cudaStream_t);
 template <typename T> cudaError_t launch_step_near(const StepArgs&, const NearTables&, cudaStream_t);
 template <typename T> cudaError_t launch_add_force(const StepArgs&, T*, const float*, cudaStream_t);
-template <typename T> cudaError_t launch_step_map(const StepArgs&, const NearTables&, bool, bool, int, cudaStream_t);
+template <typename T> cudaError_t launch_step_map(const StepArgs&, const NearTables&, bool, bool, int, bool, cudaStream_t);
 bool pair_step_eligible(int n);
 bool map_step_eligible(int n, long long nslots);
 void set_programmatic_launch(bool on);
@@ -207,6 +207,7 @@ struct octlb_ctx {
   std::vector<int> counters_collide, counters_stream;
   long long launches_per_step = 0, lups_per_step = 0;
   int step_kernel = 0;              // OCTLB_STEP_KERNEL: 0 pair (default), 1 bulk, 2 plain
+  bool map_global = true;           // slot map read through L1 (OCTLB_MAP_SMEM=1: staged in shared memory)
   int map_cells = 0;                // cells per thread of the slot-map step (OCTLB_MAP_CELLS 1 or 2;
                                     // default 2, 1 under the links rule whose variant spills at 2)
   // advance_one captured as CUDA graphs, keyed by the A/B parity of every
@@ -337,7 +338,7 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     CK(launch_step_pair<T>(a, ctx->stream));
   } else if (L.use_map) {
     CK(launch_step_map<T>(a, L.near, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags, ctx->map_cells,
-                          ctx->stream));
+                          ctx->map_global, ctx->stream));
   } else {
     CK(launch_step<T>(a, ctx->periodic != 0, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags,
                       ctx->stream));
@@ -1839,6 +1840,7 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
   }
   ctx->map_cells = p->stream_mode == OCTLB_STREAM_LINKS ? 1 : 2;
   if (const char* mc = std::getenv("OCTLB_MAP_CELLS")) ctx->map_cells = mc[0] == '1' ? 1 : 2;
+  if (const char* ms = std::getenv("OCTLB_MAP_SMEM")) ctx->map_global = ms[0] != '1';
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "cudaStreamCreate"); *out = ctx.release(); return rc; }
   ctx->own_stream = true;
