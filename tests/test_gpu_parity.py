@@ -118,10 +118,12 @@ def test_links_bouzidi_random_state_one_step(ob, ref):
     assert rel(g1, core) <= 1e-5
 
 
-@pytest.mark.parametrize("band", [0, 8])
-def test_cavity_forest_matches_reference(ob, ref, band):
+@pytest.mark.parametrize("band,n", [(0, 8), (8, 8), (16, 16)])
+def test_cavity_forest_matches_reference(ob, ref, band, n):
+    """Cavity forests (one level, or a refined band under the moving lid) with
+    8^3 and 16^3 blocks, fields and counters against the reference TimeLoop."""
     from octlb_b200 import cases
-    mesh, init, info = cases.cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=band)
+    mesh, init, info = cases.cavity_forest(cells=32 if n == 8 else 64, n=n, lid=0.1, tau=0.6, band_cells=band)
     steps = 10
     lat = ob.GpuLattice(mesh, info["omega"], init_pops=init)
     lat.advance(steps)
@@ -165,17 +167,25 @@ def test_step_kernel_variants_bitwise_equal(ob, prec, monkeypatch):
     assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
 
 
-def small_cylinder(ob):
+def small_cylinder(ob, n=8):
     from octlb_b200 import cases
+    if n == 16:
+        return cases.cylinder_forest(length=128, height=64, n=16, diameter=8.0, center=(32.0, 32.0),
+                                     levels=2, u_max=0.05, re=40.0)
     return cases.cylinder_forest(length=128, height=32, n=8, diameter=8.0, center=(32.0, 16.0),
                                  levels=2, u_max=0.05, re=40.0)
 
 
-def test_cylinder_two_levels_matches_reference_with_drag(ob, ref):
+@pytest.mark.parametrize("n", [8, 16])
+def test_cylinder_two_levels_matches_reference_with_drag(ob, ref, n):
     """Two-level channel with an exact-circle Bouzidi cylinder, parabolic
     inlet, zero-gradient outlet, periodic z: fields and the momentum-exchange
-    force per coarse step against the reference TimeLoop + MomentumExchangeDrag."""
-    mesh, init, info = small_cylinder(ob)
+    force per coarse step against the reference TimeLoop + MomentumExchangeDrag
+    (8^3 and 16^3 blocks).  The force is a sum of ~10^3 link terms of the
+    shifted populations; while the start-up wave reaches the cylinder it is a
+    small difference of those (1e-4 against terms of ~1e-3), whose FP32
+    rounding is ~1e-8 absolute, so the tolerance is 1e-5 of max(|F|, 1e-2)."""
+    mesh, init, info = small_cylinder(ob, n)
     assert len(mesh.link_q) > 0 and len(mesh.coarse_fine) > 0
     lat = ob.GpuLattice(mesh, info["omega"], stream_mode=ob.STREAM_LINKS, drag=True, init_pops=init)
     sim = oracle.Sim(ref, mesh, info["omega"], init, link_mode=True)
@@ -183,14 +193,14 @@ def test_cylinder_two_levels_matches_reference_with_drag(ob, ref):
         lat.advance(1)
         sim.advance(1)
         fg, fr = lat.force(), sim.drag(mesh.obstacle)
-        assert np.max(np.abs(fg - fr)) <= 1e-5 * max(np.max(np.abs(fr)), 1e-6), (step, fg, fr)
+        assert np.max(np.abs(fg - fr)) <= 1e-5 * max(np.max(np.abs(fr)), 1e-2), (step, fg, fr)
     rho_g, u_g = lat.get_fields()
     rho_r, u_r = fields_of(sim.core())
     fl = mesh.kinds == ob.BULK
     assert rel(rho_g[fl], rho_r[fl]) <= TOL32
     assert rel(u_g[fl], u_r[fl]) <= TOL32
-    fs, n = lat.force_sum()
-    assert n == 12 and np.all(np.isfinite(fs))
+    fs, nsteps = lat.force_sum()
+    assert nsteps == 12 and np.all(np.isfinite(fs))
 
 
 def test_cylinder_fp16_drag_close_to_fp32(ob):
