@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_adj_step(const StepArgs a, cons
       }
       continue;
     }
-    if (LINKS && (fl & kFlagNear)) continue;  // k_adj_near
+    if (LINKS && (fl & kFlagNear)) continue;  // the near-cell CTAs take it
     float f[kQ], lam[kQ];
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {

@@ -1367,7 +1367,7 @@ int adj_step(octlb_ctx* ctx, int l, const StepRecord& R, float coef) {
   // consume (lamY, the save rows, the coupler targets), so each buffer is
   // back to zero when it becomes the accumulator again.  The body-force
   // gradient of the state this step read is taken where its cotangent is
-  // consumed (the previous step's k_adj_step / k_adj_near, the coupler
+  // consumed (the previous step's k_adj_step, the coupler
   // kernels for their targets, and a final pass for the initial state).
   CK(launch_adj_step(a, L.near, links, L.has_flags, lamY, lamX, V.lam_save.as<float>(), g, V.gF.as<double>(),
                      ctx->stream));
