@@ -95,10 +95,10 @@ __device__ __forceinline__ void force_grad_lanes(const LaneDir& d, float mu, dou
                                                  int lane) {
   const float v = d.act ? 3.0f * d.w * mu : 0.f;
   const float sx = warp_sum(v * d.cx), sy = warp_sum(v * d.cy), sz = warp_sum(v * d.cz);
-  if (lane == 0) {
-    gF[t] += sx;
-    gF[ncore + t] += sy;
-    gF[2 * ncore + t] += sz;
+  if (lane == 0) {  // one contributor per cell and launch: the adds need no return trip
+    atomicAdd(gF + t, static_cast<double>(sx));
+    atomicAdd(gF + ncore + t, static_cast<double>(sy));
+    atomicAdd(gF + 2 * ncore + t, static_cast<double>(sz));
   }
 }
 
@@ -219,7 +219,7 @@ __device__ __forceinline__ void add_grad(double* g, int slot, double v) {
 // to the moving-wall velocity gradient (gw).
 __device__ __forceinline__ void scatter(const StepArgs& a, float* lamX, int i, long long s, float v, float& gw) {
   if (s >= a.halo_base && a.fill_of) {
-    const int fo = a.fill_of[(s - a.halo_base) * kQ + i];
+    const int fo = __ldg(a.fill_of + (s - a.halo_base) * kQ + i);
     if (fo >= 0) {
       const BBOp& op = a.fills[fo];
       atomicAdd(lamX + op.src_pop * a.qs + op.src, v);
@@ -230,24 +230,11 @@ __device__ __forceinline__ void scatter(const StepArgs& a, float* lamX, int i, l
   atomicAdd(lamX + i * a.qs + s, v);
 }
 
-// Body-force gradient of one kBulk cell from the cotangent mu of the stored
-// state the forcing term 3 w_i (c_i . F) was added to.  gF is [3][ncore].
-__device__ __forceinline__ void force_grad(const float (&mu)[kQ], double* gF, uint32_t ncore, uint32_t t) {
-  float sx = 0.f, sy = 0.f, sz = 0.f;
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    const float v = 3.0f * wf(i) * mu[i];
-    sx += cx(i) * v;
-    sy += cy(i) * v;
-    sz += cz(i) * v;
-  }
-  gF[t] += sx;
-  gF[ncore + t] += sy;
-  gF[2ull * ncore + t] += sz;
-}
-
 // Near-wall cells (the link rule with host-resolved slots, see k_step_near),
-// one warp per cell, lane i on direction i.
+// one warp per cell, lane i on direction i.  Every load (tables, the fill
+// behind the pulled slot, the input, the cotangents) is issued before the
+// first store, so the warp waits for memory about three times, not once per
+// dependent access.
 __device__ __forceinline__ float adj_near_cell(const StepArgs& a, const NearTables& nt, int k, int lane,
                                                float* __restrict__ lamY, float* lamX, float* __restrict__ lamS,
                                                double* gF, float& gw) {
@@ -256,22 +243,42 @@ __device__ __forceinline__ float adj_near_cell(const StepArgs& a, const NearTabl
     const float* src = static_cast<const float*>(a.src);
     const long long qs = a.qs;
     const LaneDir d = lane_dir(lane);
-    const uint32_t t = static_cast<uint32_t>(nt.cells[k]);
-    const uint32_t mask = nt.mask[k];
-    const uint8_t fl = a.flags[t];
+    const uint32_t t = static_cast<uint32_t>(__ldg(nt.cells + k));
+    const uint32_t mask = __ldg(nt.mask + k);
+    const int sl = d.act ? __ldg(nt.slot + lane * nt.n + k) : 0;
+    const float q = d.act ? __ldg(nt.q + lane * nt.n + k) : 1.f;
+    const float wadd = d.act ? __ldg(nt.add + lane * nt.n + k) : 0.f;
     const bool link = d.act && ((mask >> lane) & 1u);
-    const int sl = d.act ? nt.slot[lane * nt.n + k] : 0;
-    const float q = d.act ? nt.q[lane * nt.n + k] : 1.f;
-    const float val = d.act ? pull_value(a, src, lane, sl) : 0.f;
-    const float own = d.act ? src[lane * qs + t] : 0.f;
+    // the slot's value (a boundary fill is evaluated from its source) and
+    // where its cotangent goes
+    long long tgt = lane * qs + sl;
+    float fadd = 0.f, fdadd = 0.f;
+    bool fill = false;
+    if (d.act && sl >= a.halo_base && a.fill_of) {
+      const int fo = __ldg(a.fill_of + (sl - a.halo_base) * kQ + lane);
+      if (fo >= 0) {
+        const BBOp op = a.fills[fo];
+        tgt = op.src_pop * qs + op.src;
+        fadd = op.add;
+        fdadd = op.dadd;
+        fill = true;
+      }
+    }
+    const uint8_t fl = __ldg(a.flags + t);
+    const float val = d.act ? __ldg(src + tgt) + fadd : 0.f;
+    const float own = d.act ? __ldg(src + lane * qs + t) : 0.f;
+    const float mu = d.act ? lamY[lane * qs + t] : 0.f;
+    float* ls = nullptr;
+    float lsv = 0.f;
+    if ((fl & kFlagSave) && d.act) {
+      ls = lamS + static_cast<long long>(__ldg(a.save_idx + t)) * kQ + lane;
+      lsv = *ls;
+    }
+    if (d.act) lamY[lane * qs + t] = 0.f;
+    if (ls) *ls = 0.f;
     const float own_opp = __shfl_sync(0xffffffffu, own, d.opp);
     float f = val;
-    if (link) f = (q < 1.0f ? bouzidi(own_opp, val, own, q) : own_opp) + nt.add[lane * nt.n + k];
-    float mu = 0.f;
-    if (d.act) {
-      mu = lamY[lane * qs + t];
-      lamY[lane * qs + t] = 0.f;
-    }
+    if (link) f = (q < 1.0f ? bouzidi(own_opp, val, own, q) : own_opp) + wadd;
     float lam = mu;
     if ((fl & kKindMask) == kBulk) {
       force_grad_lanes(d, mu, gF, a.ncore, t, lane);
@@ -289,11 +296,7 @@ __device__ __forceinline__ float adj_near_cell(const StepArgs& a, const NearTabl
       feq_vjp_lanes(d, mu, rho, ux, uy, uz, P, Vx, Vy, Vz);
       lam = (1.0f - a.omega) * mu + a.omega * (P + (Vx * (d.cx - ux) + Vy * (d.cy - uy) + Vz * (d.cz - uz)) * kr);
     }
-    if ((fl & kFlagSave) && d.act) {
-      float* ls = lamS + static_cast<long long>(a.save_idx[t]) * kQ + lane;
-      lam += *ls;
-      *ls = 0.f;
-    }
+    lam += lsv;
     // the link rule in reverse: shares to own[opp(i)] (to_opp), own[i]
     // (to_own) and the value read at the slot (to_val)
     float to_opp = 0.f, to_own = 0.f, to_val = d.act ? lam : 0.f;
@@ -312,7 +315,10 @@ __device__ __forceinline__ float adj_near_cell(const StepArgs& a, const NearTabl
     }
     const float own_total = to_own + __shfl_sync(0xffffffffu, to_opp, d.opp);
     if (d.act) {
-      if (to_val != 0.f) scatter(a, lamX, lane, sl, to_val, gw);
+      if (to_val != 0.f) {
+        atomicAdd(lamX + tgt, to_val);
+        if (fill) gw += to_val * fdadd;
+      }
       if (own_total != 0.f) atomicAdd(lamX + lane * qs + t, own_total);
     }
   }
@@ -324,7 +330,7 @@ __device__ __forceinline__ float adj_near_cell(const StepArgs& a, const NearTabl
 // halo rotation items.  a.src = the step's input (after force and fills);
 // lamY = cotangent of the step's output, lamX += cotangent of its input.
 template <bool LINKS, bool FLAGS>
-__global__ void __launch_bounds__(kThreads, 3) k_adj_step(const StepArgs a, const NearTables nt, float* __restrict__ lamY,
+__global__ void __launch_bounds__(kThreads, LINKS ? 3 : 2) k_adj_step(const StepArgs a, const NearTables nt, float* __restrict__ lamY,
                                                       float* lamX, float* __restrict__ lamS, double* g,
                                                       double* gF) {
   extern __shared__ int smap[];
@@ -371,7 +377,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_adj_step(const StepArgs a, cons
     const uint32_t t = b * n3 + tl;
     const uint32_t x = a.div_n2.div(tl), r = tl - x * n * n, y = a.div_n.div(r);
     const int P = (static_cast<int>(x + 1) * np + static_cast<int>(y + 1)) * np + static_cast<int>(r - y * n + 1);
-    const uint8_t fl = FLAGS ? a.flags[t] : 0;
+    const uint8_t fl = FLAGS ? __ldg(a.flags + t) : 0;
     if (LINKS && (fl & kKindMask) == kSolid) {
 #pragma unroll
       for (int i = 0; i < kQ; ++i) {
@@ -381,33 +387,65 @@ __global__ void __launch_bounds__(kThreads, 3) k_adj_step(const StepArgs a, cons
       continue;
     }
     if (LINKS && (fl & kFlagNear)) continue;  // the near-cell CTAs take it
+    // All loads are issued before the first store: a warp issues in order,
+    // and a load the compiler may not move above a store (lamY[i] and
+    // lamY[i + 1] may alias for all it knows) costs a full memory round trip.
+    // The recorded input is read through the read-only path.
     float f[kQ], lam[kQ];
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
       const int sm = smap[P - a.off_pad[i]];  // < 0: bounce-back wall position (see k_step_map)
-      const float v = src[sm >= 0 ? i * qs + sm : opp(i) * qs + t];
-      f[i] = sm < -1 ? v + a.wall_add[(-sm - 2) * kQ + i] : v;
+      f[i] = __ldg(src + (sm >= 0 ? i * qs + sm : opp(i) * qs + t));
       lam[i] = lamY[i * qs + t];  // the output's cotangent, turned into the input's below
-      lamY[i * qs + t] = 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      const int sm = smap[P - a.off_pad[i]];
+      if (sm < -1) f[i] += __ldg(a.wall_add + (-sm - 2) * kQ + i);
     }
     const bool bulk = !FLAGS || (fl & kKindMask) == kBulk;
+    double gf0 = 0.0, gf1 = 0.0, gf2 = 0.0;  // body-force gradient of this cell (one writer per launch)
     if (bulk) {
-      force_grad(lam, gF, a.ncore, t);
+      gf0 = gF[t];
+      gf1 = gF[a.ncore + t];
+      gf2 = gF[2ull * a.ncore + t];
+    }
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) lamY[i * qs + t] = 0.f;
+    if (bulk) {
+      float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) {
+        const float v = 3.0f * wf(i) * lam[i];
+        sx += cx(i) * v;
+        sy += cy(i) * v;
+        sz += cz(i) * v;
+      }
+      gF[t] = gf0 + sx;
+      gF[a.ncore + t] = gf1 + sy;
+      gF[2ull * a.ncore + t] = gf2 + sz;
       dom += bgk_vjp_inplace(f, a.omega, lam);
     }
     if (FLAGS && (fl & kFlagSave)) {
-      float* ls = lamS + static_cast<long long>(a.save_idx[t]) * kQ;
+      float* ls = lamS + static_cast<long long>(__ldg(a.save_idx + t)) * kQ;
+      float lsv[kQ];
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) lsv[i] = ls[i];
 #pragma unroll
       for (int i = 0; i < kQ; ++i) {
-        lam[i] += ls[i];
+        lam[i] += lsv[i];
         ls[i] = 0.f;
       }
     }
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
       const int sm = smap[P - a.off_pad[i]];
+      if (sm < -1) gw += lam[i] * __ldg(a.wall_dadd + (-sm - 2) * kQ + i);
+    }
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      const int sm = smap[P - a.off_pad[i]];
       atomicAdd(lamX + (sm >= 0 ? i * qs + sm : opp(i) * qs + t), lam[i]);
-      if (sm < -1) gw += lam[i] * a.wall_dadd[(-sm - 2) * kQ + i];
     }
   }
   add_grad(g, kGOmega, dom);
@@ -521,38 +559,42 @@ k_adj_prolong(const ProlongItem* items, int nitems, const float* coarse_save, co
   if (w < nitems) {
     const ProlongItem it = items[w];
     const LaneDir d = lane_dir(lane);
+    // every load first (see adj_near_cell)
     const float* row = coarse_save + static_cast<long long>(it.coarse_save) * kQ;
-    const float f = d.act ? row[lane] : 0.f;
+    const float f = d.act ? __ldg(row + lane) : 0.f;
+    const float* pv = prev + static_cast<long long>(it.prev) * 23;
+    float pv0 = 0.f, pv1 = 0.f, pv2 = 0.f, pv3 = 0.f, pvf = 0.f;
+    if (half) {
+      pv0 = __ldg(pv); pv1 = __ldg(pv + 1); pv2 = __ldg(pv + 2); pv3 = __ldg(pv + 3);
+      pvf = d.act ? __ldg(pv + 4 + lane) : 0.f;
+    }
+    float* p = lam_fine + lane * fine_qs + it.fine_slot;
+    const float mu = d.act ? *p : 0.f;
+    // the component of the prev / m cotangents this lane owns
+    const int comp = lane < kQ ? 4 + lane : (lane < kQ + 4 ? lane - kQ : -1);
+    float* lm = lam_m + static_cast<long long>(w) * 23;
+    float* lp = lam_prev + static_cast<long long>(it.prev) * 23;
+    const float lmv = comp >= 0 ? lm[comp] : 0.f, lpv = comp >= 0 ? lp[comp] : 0.f;
+    if (d.act) *p = 0.f;
     float drho, ux, uy, uz, fneq;
     read_macro_lanes(d, f, drho, ux, uy, uz, fneq);
-    float* pv = const_cast<float*>(prev) + static_cast<long long>(it.prev) * 23;
     float wd = drho, wx = ux, wy = uy, wz = uz, wf_ = fneq;
     if (half) {
-      wd = 0.5f * (pv[0] + drho); wx = 0.5f * (pv[1] + ux); wy = 0.5f * (pv[2] + uy); wz = 0.5f * (pv[3] + uz);
-      wf_ = d.act ? 0.5f * (pv[4 + lane] + fneq) : 0.f;
-    }
-    float mu = 0.f;
-    if (d.act) {
-      float* p = lam_fine + lane * fine_qs + it.fine_slot;
-      mu = *p;
-      *p = 0.f;
+      wd = 0.5f * (pv0 + drho); wx = 0.5f * (pv1 + ux); wy = 0.5f * (pv2 + uy); wz = 0.5f * (pv3 + uz);
+      wf_ = d.act ? 0.5f * (pvf + fneq) : 0.f;
     }
     if (it.fine_kind == kBulk) force_grad_lanes(d, mu, gF_fine, fine_ncore, it.fine_slot, lane);
     float lfneq, ldrho, lux, luy, luz;
     write_vjp_lanes(d, wd, wx, wy, wz, wf_, s, it.fine_kind, omega, mu, lfneq, ldrho, lux, luy, luz, ds, dom);
-    // the component this lane owns
-    const int comp = lane < kQ ? 4 + lane : (lane < kQ + 4 ? lane - kQ : -1);
     const float lw = lane < kQ ? lfneq : (lane == kQ ? ldrho : (lane == kQ + 1 ? lux : (lane == kQ + 2 ? luy : luz)));
-    float* lm = lam_m + static_cast<long long>(w) * 23;
-    float* lp = lam_prev + static_cast<long long>(it.prev) * 23;
     float total = 0.f;
     if (comp >= 0) {
       if (half) {
-        total = lm[comp] + 0.5f * lw;
-        lp[comp] += 0.5f * lw;
+        total = lmv + 0.5f * lw;
+        lp[comp] = lpv + 0.5f * lw;
         lm[comp] = 0.f;
       } else {
-        lm[comp] += lw + lp[comp];
+        lm[comp] = lmv + (lw + lpv);
         lp[comp] = 0.f;
       }
     }
@@ -586,13 +628,17 @@ k_adj_restrict(const RestrictItem* items, int nitems, const float* fine_save, fl
   if (w < nitems) {
     const RestrictItem& it = items[w];
     const int row = lane == 0 ? it.fine_save : (lane <= it.nnb ? it.nb_save[lane - 1] : -1);
+    const LaneDir d = lane_dir(lane);
+    float* p = lam_coarse + lane * coarse_qs + it.coarse_slot;
+    const float mu = d.act ? *p : 0.f;
     Macro m;
     float f[kQ];
     if (row >= 0) {
 #pragma unroll
-      for (int i = 0; i < kQ; ++i) f[i] = fine_save[static_cast<long long>(row) * kQ + i];
+      for (int i = 0; i < kQ; ++i) f[i] = __ldg(fine_save + static_cast<long long>(row) * kQ + i);
       read_macro(f, m);
     }
+    if (d.act) *p = 0.f;
     float sum[kQ];
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
@@ -602,7 +648,6 @@ k_adj_restrict(const RestrictItem* items, int nitems, const float* fine_save, fl
     }
     const float inv = 1.0f / static_cast<float>(it.nnb + 1);
     // r = (centre drho, u; f_neq average) spread over the lanes
-    const LaneDir d = lane_dir(lane);
     float rf = 0.f;
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
@@ -611,12 +656,6 @@ k_adj_restrict(const RestrictItem* items, int nitems, const float* fine_save, fl
     }
     const float rd = __shfl_sync(0xffffffffu, m.drho, 0), rx = __shfl_sync(0xffffffffu, m.ux, 0);
     const float ry = __shfl_sync(0xffffffffu, m.uy, 0), rz = __shfl_sync(0xffffffffu, m.uz, 0);
-    float mu = 0.f;
-    if (d.act) {
-      float* p = lam_coarse + lane * coarse_qs + it.coarse_slot;
-      mu = *p;
-      *p = 0.f;
-    }
     if (it.coarse_kind == kBulk) force_grad_lanes(d, mu, gF_coarse, coarse_ncore, it.coarse_slot, lane);
     float lfneq, ldrho, lux, luy, luz;
     write_vjp_lanes(d, rd, rx, ry, rz, rf, s, it.coarse_kind, omega, mu, lfneq, ldrho, lux, luy, luz, ds, dom);
