@@ -379,9 +379,12 @@ __global__ void __launch_bounds__(kThreads, LINKS ? 3 : 2) k_adj_step(const Step
     const int P = (static_cast<int>(x + 1) * np + static_cast<int>(y + 1)) * np + static_cast<int>(r - y * n + 1);
     const uint8_t fl = FLAGS ? __ldg(a.flags + t) : 0;
     if (LINKS && (fl & kKindMask) == kSolid) {
+      float v[kQ];  // loads before stores (see below)
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) v[i] = lamY[i * qs + t];
 #pragma unroll
       for (int i = 0; i < kQ; ++i) {
-        atomicAdd(lamX + i * qs + t, lamY[i * qs + t]);
+        atomicAdd(lamX + i * qs + t, v[i]);
         lamY[i * qs + t] = 0.f;
       }
       continue;

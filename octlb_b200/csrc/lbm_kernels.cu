@@ -58,6 +58,18 @@ __device__ __forceinline__ void source_slots(const StepArgs& a, const Cell& c, l
   }
 }
 
+// The 19 populations of cell t copied unchanged; all loads are issued
+// before the first store (for all the compiler knows, a store to row i may
+// alias the load from row i + 1, which would cost a round trip each).
+template <typename T>
+__device__ __forceinline__ void copy_cell(const T* src, T* dst, long long qs, uint32_t t) {
+  T v[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) v[i] = src[i * qs + t];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) dst[i * qs + t] = v[i];
+}
+
 // Torus-streamed halo population of an open block (block_lattice.h:70-89),
 // item k: copied without collision.
 template <typename T>
@@ -99,8 +111,7 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
     if constexpr (LINKS) {
       if ((fl & kKindMask) == kSolid) {
         // Solid cells are neither streamed nor collided (block_lattice.cpp:581-583).
-#pragma unroll
-        for (int i = 0; i < kQ; ++i) dst[i * a.qs + t] = src[i * a.qs + t];
+        copy_cell(src, dst, a.qs, t);
         return;
       }
     }
@@ -209,8 +220,7 @@ __device__ __forceinline__ bool map_cell_prologue(const StepArgs& a, uint32_t t,
   if constexpr (LINKS) {
     if ((fl & kKindMask) == kSolid) {
       // Solid cells are neither streamed nor collided (block_lattice.cpp:581-583).
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) dst[i * a.qs + t] = src[i * a.qs + t];
+      copy_cell(src, dst, a.qs, t);
       return false;
     }
     if (fl & kFlagNear) return false;
