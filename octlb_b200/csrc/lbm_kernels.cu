@@ -379,73 +379,109 @@ __global__ void __launch_bounds__(kThreads) k_add_force(const StepArgs a, T* pop
 }
 
 
-constexpr int kProlongThreads = 64;  // few items: spread them over more SMs
+// Lagrava prolongation (level_coupler.cpp:455-476), one warp per item, lane
+// i on population i: every lane gathers the coarse save row and forms the
+// macro state with the same operations as read_macro (so the result does not
+// depend on the lane layout), then writes its own population.  Parallel
+// lanes keep the item's dependent chain short: the launch is latency-bound
+// (a few thousand items).
 template <typename T>
-__global__ void __launch_bounds__(kProlongThreads)
+__global__ void __launch_bounds__(kThreads)
 k_prolong(const ProlongItem* items, int nitems, const float* coarse_save, float* prev, int half,
           T* fine, long long fine_qs, float scale, float omega, float fscale) {
-  const int t = blockIdx.x * kProlongThreads + threadIdx.x;
-  if (t >= nitems) return;
-  const ProlongItem it = items[t];
+  const int w = static_cast<int>((blockIdx.x * kThreads + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= nitems) return;  // whole warps
+  const ProlongItem it = items[w];
+  const LaneDir d = lane_dir(lane);
   pdl_wait();
-  Macro m;
-  read_macro(coarse_save + static_cast<long long>(it.coarse_save) * kQ, m);
+  const float fr = d.act ? coarse_save[static_cast<long long>(it.coarse_save) * kQ + lane] : 0.f;
   float* pv = prev + static_cast<long long>(it.prev) * 23;
-  Macro w = m;
+  float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f, pf = 0.f;
+  if (half) {
+    p0 = pv[0]; p1 = pv[1]; p2 = pv[2]; p3 = pv[3];
+    pf = d.act ? pv[4 + lane] : 0.f;
+  }
+  float fa[kQ];
+  gather_lanes(fr, fa);
+  float drho, jx, jy, jz;
+  moments(fa, drho, jx, jy, jz);
+  const float rho = 1.0f + drho, inv = 1.0f / rho;
+  const float ux = jx * inv, uy = jy * inv, uz = jz * inv;
+  const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
+  const float cu = d.cx * ux + d.cy * uy + d.cz * uz;
+  const float fneq = fr - d.w * (drho + rho * (3.0f * cu + 4.5f * cu * cu - usq15));
+  float wd = drho, wx = ux, wy = uy, wz = uz, wn = fneq;
   if (half) {
     // Half-time: average of previous and current coarse macros
     // (level_coupler.cpp:455-465).
-    w.drho = 0.5f * (pv[0] + m.drho);
-    w.ux = 0.5f * (pv[1] + m.ux); w.uy = 0.5f * (pv[2] + m.uy); w.uz = 0.5f * (pv[3] + m.uz);
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) w.fneq[i] = 0.5f * (pv[4 + i] + m.fneq[i]);
+    wd = 0.5f * (p0 + drho);
+    wx = 0.5f * (p1 + ux); wy = 0.5f * (p2 + uy); wz = 0.5f * (p3 + uz);
+    wn = 0.5f * (pf + fneq);
   } else {
     // Full-time: prev <- current (level_coupler.cpp:470-476).
-    pv[0] = m.drho; pv[1] = m.ux; pv[2] = m.uy; pv[3] = m.uz;
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) pv[4 + i] = m.fneq[i];
+    if (d.act) pv[4 + lane] = fneq;
+    if (lane == kQ) pv[0] = drho;
+    if (lane == kQ + 1) pv[1] = ux;
+    if (lane == kQ + 2) pv[2] = uy;
+    if (lane == kQ + 3) pv[3] = uz;
   }
-  float f[kQ];
-  write_macro_cell(w, scale, it.fine_kind, omega, f);
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) Store<T>::st(fine + i * fine_qs + it.fine_slot, f[i], fscale);
+  // feq(w) + scale * f_neq (WriteProlongation, level_coupler.cpp:191-201),
+  // collided when the target is kBulk (as write_macro_cell)
+  const float wrho = 1.0f + wd;
+  const float wusq15 = 1.5f * (wx * wx + wy * wy + wz * wz);
+  const float wcu = d.cx * wx + d.cy * wy + d.cz * wz;
+  float f = d.w * (wd + wrho * (3.0f * wcu + 4.5f * wcu * wcu - wusq15)) + scale * wn;
+  if (it.fine_kind == kBulk) {
+    gather_lanes(f, fa);
+    f = bgk_lane(d, lane, fa, f, omega);
+  }
+  if (d.act) Store<T>::st(fine + lane * fine_qs + it.fine_slot, f, fscale);
 }
 
-// One warp per restriction point: lane k < 1 + nnb reads one source cell's
-// saved populations (the fine cell, then its in-block neighbours) and computes
-// its macro state; the f_neq average is a warp sum.
+// Lagrava restriction (level_coupler.cpp:613-654), one warp per item: lane
+// k <= nnb reads one source row (the fine cell, then its in-block
+// neighbours) and forms its macro state; the f_neq rows meet in shared
+// memory, where lane i sums population i over the neighbours in the
+// reference's order and averages with the centre; then lane i writes
+// population i of the coarse target.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_restrict(const RestrictItem* items, int nitems, const float* fine_save, T* coarse,
            long long coarse_qs, float scale, float omega, float cscale) {
-  const int w = (blockIdx.x * kThreads + threadIdx.x) >> 5;
+  __shared__ float fneq_s[kThreads / 32][kQ][kQ + 1];  // [warp][row][population]
+  const int w = static_cast<int>((blockIdx.x * kThreads + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
-  if (w >= nitems) return;
+  if (w >= nitems) return;  // whole warps
   const RestrictItem& it = items[w];
-  const int row = lane == 0 ? it.fine_save : (lane <= it.nnb ? it.nb_save[lane - 1] : -1);
+  const int nnb = it.nnb;
+  const int row = lane == 0 ? it.fine_save : (lane <= nnb ? it.nb_save[lane - 1] : -1);
   pdl_wait();
+  float (*fs)[kQ + 1] = fneq_s[threadIdx.x >> 5];
   Macro m;
-  if (row >= 0) read_macro(fine_save + static_cast<long long>(row) * kQ, m);
-  float sum[kQ];
+  if (row >= 0) {
+    read_macro(fine_save + static_cast<long long>(row) * kQ, m);
 #pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    float v = row >= 0 ? m.fneq[i] : 0.f;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    sum[i] = v;
+    for (int i = 0; i < kQ; ++i) fs[lane][i] = m.fneq[i];
   }
-  const float drho = __shfl_sync(0xffffffffu, m.drho, 0);
-  const float ux = __shfl_sync(0xffffffffu, m.ux, 0), uy = __shfl_sync(0xffffffffu, m.uy, 0),
-              uz = __shfl_sync(0xffffffffu, m.uz, 0);
-  if (lane != 0) return;
-  Macro r;
-  r.drho = drho; r.ux = ux; r.uy = uy; r.uz = uz;
-  const float inv = 1.0f / static_cast<float>(it.nnb + 1);
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) r.fneq[i] = sum[i] * inv;
-  float f[kQ];
-  write_macro_cell(r, scale, it.coarse_kind, omega, f);
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) Store<T>::st(coarse + i * coarse_qs + it.coarse_slot, f[i], cscale);
+  __syncwarp();
+  const LaneDir d = lane_dir(lane);
+  float nsum = 0.f;
+  for (int r = 1; r <= nnb; ++r) nsum += d.act ? fs[r][lane] : 0.f;
+  const float inv = 1.0f / static_cast<float>(nnb + 1);
+  const float rn = d.act ? (fs[0][lane] + nsum) * inv : 0.f;
+  const float rd = __shfl_sync(0xffffffffu, m.drho, 0), rx = __shfl_sync(0xffffffffu, m.ux, 0);
+  const float ry = __shfl_sync(0xffffffffu, m.uy, 0), rz = __shfl_sync(0xffffffffu, m.uz, 0);
+  const float rho = 1.0f + rd;
+  const float usq15 = 1.5f * (rx * rx + ry * ry + rz * rz);
+  const float cu = d.cx * rx + d.cy * ry + d.cz * rz;
+  float f = d.w * (rd + rho * (3.0f * cu + 4.5f * cu * cu - usq15)) + scale * rn;
+  if (it.coarse_kind == kBulk) {
+    float fa[kQ];
+    gather_lanes(f, fa);
+    f = bgk_lane(d, lane, fa, f, omega);
+  }
+  if (d.act) Store<T>::st(coarse + lane * coarse_qs + it.coarse_slot, f, cscale);
 }
 
 // Momentum-exchange force (drag_postprocessor.h:67-115) from the buffer the
@@ -456,42 +492,53 @@ k_restrict(const RestrictItem* items, int nitems, const float* fine_save, T* coa
 template <typename T, bool LINKS>
 __global__ void __launch_bounds__(kThreads)
 k_drag(const StepArgs a, const DragItem* items, int nitems, double* partial) {
-  pdl_wait();
-  const int t = blockIdx.x * kThreads + threadIdx.x;
+  // One warp per item, lane i on direction i: the links' dependent lookups
+  // (link record, neighbour, its kind, a boundary fill) run side by side.
+  const int w = static_cast<int>((blockIdx.x * kThreads + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
   double acc[3] = {0.0, 0.0, 0.0};
-  if (t < nitems) {
-    const DragItem it = items[t];
+  pdl_wait();
+  if (w < nitems) {
+    const DragItem it = items[w];
     const T* src = static_cast<const T*>(a.src);
-    float own[kQ];
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) own[i] = LD(src, a.qs, i, it.slot, a.inv_scale);
-    const uint8_t fl = a.flags[it.slot];
-    const int li = (LINKS && (fl & kFlagLink)) ? a.link_idx[it.slot] : -1;
-    const Cell c = cell_of(a, static_cast<uint32_t>(it.slot));
-#pragma unroll
-    for (int i = 1; i < kQ; ++i) {
-      if (!(it.mask & (1u << i))) continue;
-      const int j = opp(i);
-      float f_bar;
+    const LaneDir d = lane_dir(lane);
+    const float own = d.act ? LD(src, a.qs, lane, it.slot, a.inv_scale) : 0.f;  // g_i(x)
+    const float own_j = __shfl_sync(0xffffffffu, own, d.opp);                    // g_opp(i)(x)
+    const bool link = d.act && lane > 0 && ((it.mask >> lane) & 1u);
+    float f_bar = 0.f;
+    if (link) {
+      const int j = d.opp;
       if constexpr (LINKS) {
-        f_bar = own[i];
+        f_bar = own;
+        const uint8_t fl = a.flags[it.slot];
+        const int li = (fl & kFlagLink) ? a.link_idx[it.slot] : -1;
         if (li >= 0) {
           const float q = a.link_rec[li * 38 + j];
           if (q < 1.0f) {
+            const Cell c = cell_of(a, static_cast<uint32_t>(it.slot));
+            const int ax = static_cast<int>(d.cx), ay = static_cast<int>(d.cy), az = static_cast<int>(d.cz);
             bool nhalo;
-            const long long nb = resolve(a, c.b, static_cast<int>(c.x) + 1 + cx(j),
-                                         static_cast<int>(c.y) + 1 + cy(j), static_cast<int>(c.z) + 1 + cz(j), nhalo);
+            const long long nb = resolve(a, c.b, static_cast<int>(c.x) + 1 - ax, static_cast<int>(c.y) + 1 - ay,
+                                         static_cast<int>(c.z) + 1 - az, nhalo);
             const int nk = nhalo ? kBulk : (a.flags[nb] & kKindMask);
-            const float f_q = nk == kBulk ? pull_value(a, src, j, nb) : own[j];
-            f_bar = bouzidi(own[i], f_q, own[j], q);
+            const float f_q = nk == kBulk ? pull_value(a, src, j, nb) : own_j;
+            f_bar = bouzidi(own, f_q, own_j, q);
           }
           f_bar += a.link_rec[li * 38 + kQ + j];
         }
       } else {
-        f_bar = LD(src, a.qs, j, it.slot + a.off[i], a.inv_scale);  // plain pull from x + c_i
+        f_bar = LD(src, a.qs, j, it.slot + a.off[lane], a.inv_scale);  // plain pull from x + c_i
       }
-      const double s = static_cast<double>(own[i]) + static_cast<double>(f_bar);
-      acc[0] += s * cx(i); acc[1] += s * cy(i); acc[2] += s * cz(i);
+    }
+    const double sv = link ? static_cast<double>(own) + static_cast<double>(f_bar) : 0.0;
+    double v[3] = {sv * d.cx, sv * d.cy, sv * d.cz};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    if (lane == 0) {
+      acc[0] = v[0];
+      acc[1] = v[1];
+      acc[2] = v[2];
     }
   }
   block_reduce<3>(acc);
@@ -688,8 +735,8 @@ cudaError_t launch_prolong(const ProlongItem* items, int n, const float* coarse_
                            int half, T* fine, long long fine_qs, float scale, float omega,
                            float fscale, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  const cudaError_t e = launch_chain(k_prolong<T>, dim3((n + kProlongThreads - 1) / kProlongThreads), dim3(kProlongThreads), 0, s, items, n, coarse_save, prev, half, fine, fine_qs,
-                                                scale, omega, fscale);
+  const cudaError_t e = launch_chain(k_prolong<T>, dim3(grid_for(static_cast<uint32_t>(n) * 32)), dim3(kThreads), 0, s,
+                                     items, n, coarse_save, prev, half, fine, fine_qs, scale, omega, fscale);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -703,11 +750,14 @@ cudaError_t launch_restrict(const RestrictItem* items, int n, const float* fine_
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
+// Drag partials of n items: one per CTA of the warp-per-item launch.
+uint32_t drag_partials(int n) { return grid_for(static_cast<uint32_t>(n > 0 ? n : 1) * 32); }
+
 template <typename T>
 cudaError_t launch_drag(const StepArgs& a, bool links, const DragItem* items, int n, double* partial,
                         cudaStream_t s) {
   cudaError_t e = cudaSuccess;
-  const uint32_t g = grid_for(static_cast<uint32_t>(n > 0 ? n : 1));
+  const uint32_t g = drag_partials(n);
   if (links) e = launch_chain(k_drag<T, true>, dim3(g), dim3(kThreads), 0, s, a, items, n, partial);
   else e = launch_chain(k_drag<T, false>, dim3(g), dim3(kThreads), 0, s, a, items, n, partial);
   return e != cudaSuccess ? e : cudaGetLastError();
@@ -717,7 +767,6 @@ cudaError_t launch_drag_total(const double* partial, int nparts, double* out, do
   const cudaError_t e = launch_chain(k_sum_partials, dim3(1), dim3(kThreads), 0, s, partial, nparts, 3, out, accum);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
-uint32_t drag_partials(int n) { return grid_for(static_cast<uint32_t>(n > 0 ? n : 1)); }
 
 template <typename T>
 cudaError_t launch_audit(const StepArgs& a, double* partial, double* out, cudaStream_t s) {

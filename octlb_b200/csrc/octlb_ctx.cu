@@ -201,6 +201,11 @@ struct octlb_ctx {
   std::vector<uint8_t> kinds;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // The momentum-exchange force runs on a forked stream inside advance_one
+  // (it only reads the last finest step's input) and joins at its end.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool side_busy = false;
   DevBuf drag_partial, force, force_sum, audit_out, audit_partial, host_tmp, dev_err;
   int drag_parts = 0;
   long long force_steps = 0;
@@ -332,6 +337,18 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     rec->drag = ctx->drag && L.n_drag > 0 && L.substep + 1 == (1 << L.lvl);
     A.last_rec[L.lvl] = static_cast<int>(A.nrec++);
   }
+  // The force after advance_one reads the input of each level's last step
+  // (the reference computes MomentumExchangeDrag once, after advance_one):
+  // launched on the side stream before that step, so it overlaps the step
+  // and what follows it.  (The adjoint's recomputation needs no force: it
+  // records the inputs.)
+  if (ctx->drag && L.n_drag > 0 && L.substep + 1 == (1 << L.lvl) && !rec) {
+    CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+    CK(launch_drag<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.drag_items.as<DragItem>(), L.n_drag,
+                      ctx->drag_partial.as<double>() + 3 * L.drag_off, ctx->side));
+    ctx->side_busy = true;
+  }
   if (L.use_bulk) {
     CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
   } else if (L.use_pair) {
@@ -344,14 +361,7 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
                       ctx->stream));
     CK(launch_step_near<T>(a, L.near, ctx->stream));
   }
-  // The force after advance_one reads each level's last step (the reference
-  // computes MomentumExchangeDrag once, after advance_one): skip the others.
   ++L.substep;
-  // (The adjoint's recomputation needs no force: it records the inputs.)
-  if (ctx->drag && L.n_drag > 0 && L.substep == (1 << L.lvl) && !rec) {
-    CK(launch_drag<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.drag_items.as<DragItem>(), L.n_drag,
-                      ctx->drag_partial.as<double>() + 3 * L.drag_off, ctx->stream));
-  }
   L.cur = 1 - L.cur;
   if (rec) L.rec_cur = next_cur;
   return OCTLB_OK;
@@ -1272,9 +1282,12 @@ int advance_one_launches(octlb_ctx* ctx) {
   for (auto& L : ctx->levels) L.substep = 0;
   int rc = do_advance_level<T>(ctx, 0);
   if (rc) return rc;
-  if (ctx->drag && ctx->drag_parts > 0 && !(ctx->adj && ctx->adj->recording)) {
+  if (ctx->side_busy) {
     CK(launch_drag_total(ctx->drag_partial.as<double>(), ctx->drag_parts, ctx->force.as<double>(),
-                         ctx->force_sum.as<double>(), ctx->stream));
+                         ctx->force_sum.as<double>(), ctx->side));
+    CK(cudaEventRecord(ctx->ev_join, ctx->side));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
+    ctx->side_busy = false;
   }
   return OCTLB_OK;
 }
@@ -1844,6 +1857,10 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "cudaStreamCreate"); *out = ctx.release(); return rc; }
   ctx->own_stream = true;
+  e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
+  if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "side stream"); *out = ctx.release(); return rc; }
   rc = p->precision == OCTLB_FP32 ? create_impl<float>(ctx.get(), t, p, init)
                                   : create_impl<__half>(ctx.get(), t, p, init);
   *out = ctx.release();
@@ -1857,6 +1874,12 @@ void octlb_gpu_destroy(octlb_ctx* ctx) {
   cudaStream_t s = ctx->own_stream ? ctx->stream : nullptr;
   ctx->levels.clear();
   if (s) cudaStreamDestroy(s);
+  if (ctx->side) {
+    cudaStreamSynchronize(ctx->side);
+    cudaStreamDestroy(ctx->side);
+  }
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   delete ctx;
 }
 
