@@ -141,52 +141,70 @@ __device__ __forceinline__ void feq_vjp(const float (&mu)[kQ], float rho, float 
   Vz = rho * (sz - 3.0f * uz * sw);
 }
 
-// VJP of bgk(f, omega) (unit scale) at the pre-collision f: lam = J^T mu with
-// J = (1 - omega) I + omega d feq / d f; returns sum_i mu_i (feq_i - f_i), the
-// derivative with respect to omega.
-__device__ __forceinline__ float bgk_vjp(const float (&f)[kQ], float omega, const float (&mu)[kQ],
-                                         float (&lam)[kQ]) {
+// VJP of bgk(f, omega) (unit scale) at the pre-collision f, in place
+// (mu -> lam = J^T mu, J = (1 - omega) I + omega d feq / d f), through
+// weighted moments of the cotangent: the equilibrium is quadratic in c_i, so every contraction of mu with
+// d feq / d(rho, u) is a combination of
+//   M0 = sum w_i mu_i,  M1 = sum w_i c_i mu_i,  M2 = sum w_i c_i c_i^T mu_i,
+// formed from the opposite-pair sums and differences of mu (D3Q19 order:
+// directions 10..18 are c_10 = +x, +y, +z, (1,1,0), (1,-1,0), (1,0,1),
+// (1,0,-1), (0,1,1), (0,1,-1), and 1..9 their opposites):
+//   P = M0 (1 - 1.5 u^2) + 3 u.M1 + 4.5 u.M2.u,
+//   V = rho (3 M1 + 9 M2 u - 3 M0 u),
+//   lam_j = (1 - omega) mu_j + omega (P - V.u / rho + V.c_j / rho).
+// Returns sum_i mu_i (feq_i - f_i) (d/d omega); fg = 3 M1, the gradient of
+// the body-force term 3 w_i c_i.F added to the cell whose cotangent is mu.
+__device__ __forceinline__ float bgk_vjp_moments(const float (&f)[kQ], float omega, float (&mu)[kQ], float& fgx,
+                                                 float& fgy, float& fgz) {
   float dh, jx, jy, jz;
   moments(f, dh, jx, jy, jz);
   const float rho = 1.0f + dh, k = 1.0f / rho;
   const float ux = jx * k, uy = jy * k, uz = jz * k;
   const float usq = ux * ux + uy * uy + uz * uz;
-  float dom = 0.f;
+  constexpr float w0 = 1.0f / 3.0f, wa = 1.0f / 18.0f, wg = 1.0f / 36.0f;  // rest, axis, diagonal
+  float sp[10], dp[10];
 #pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    const float cu = cx(i) * ux + cy(i) * uy + cz(i) * uz;
-    const float feq = wf(i) * (dh + rho * (3.0f * cu + 4.5f * cu * cu - 1.5f * usq));
-    dom += mu[i] * (feq - f[i]);
+  for (int q = 1; q <= 9; ++q) {
+    sp[q] = mu[q + 9] + mu[q];
+    dp[q] = mu[q + 9] - mu[q];
   }
-  float P, Vx, Vy, Vz;
-  feq_vjp(mu, rho, ux, uy, uz, P, Vx, Vy, Vz);
+  const float m1x = fmaf(wa, dp[1], wg * ((dp[4] + dp[5]) + (dp[6] + dp[7])));
+  const float m1y = fmaf(wa, dp[2], wg * ((dp[4] - dp[5]) + (dp[8] + dp[9])));
+  const float m1z = fmaf(wa, dp[3], wg * ((dp[6] - dp[7]) + (dp[8] - dp[9])));
+  const float mxx = fmaf(wa, sp[1], wg * ((sp[4] + sp[5]) + (sp[6] + sp[7])));
+  const float myy = fmaf(wa, sp[2], wg * ((sp[4] + sp[5]) + (sp[8] + sp[9])));
+  const float mzz = fmaf(wa, sp[3], wg * ((sp[6] + sp[7]) + (sp[8] + sp[9])));
+  const float mxy = wg * (sp[4] - sp[5]), mxz = wg * (sp[6] - sp[7]), myz = wg * (sp[8] - sp[9]);
+  const float m0 = fmaf(w0, mu[0], fmaf(wa, (sp[1] + sp[2]) + sp[3],
+                                        wg * (((sp[4] + sp[5]) + (sp[6] + sp[7])) + (sp[8] + sp[9]))));
+  float sf = 0.f;
 #pragma unroll
-  for (int j = 0; j < kQ; ++j)
-    lam[j] = (1.0f - omega) * mu[j] +
-             omega * (P + (Vx * (cx(j) - ux) + Vy * (cy(j) - uy) + Vz * (cz(j) - uz)) * k);
-  return dom;
-}
-
-// bgk_vjp with the cotangent replaced in place (mu -> lam), to spare the
-// registers of a third 19-wide array.
-__device__ __forceinline__ float bgk_vjp_inplace(const float (&f)[kQ], float omega, float (&mu)[kQ]) {
-  float dh, jx, jy, jz;
-  moments(f, dh, jx, jy, jz);
-  const float rho = 1.0f + dh, k = 1.0f / rho;
-  const float ux = jx * k, uy = jy * k, uz = jz * k;
-  const float usq = ux * ux + uy * uy + uz * uz;
-  float dom = 0.f;
+  for (int i = 0; i < kQ; ++i) sf = fmaf(mu[i], f[i], sf);
+  const float mux = mxx * ux + mxy * uy + mxz * uz;  // M2 u
+  const float muy = mxy * ux + myy * uy + myz * uz;
+  const float muz = mxz * ux + myz * uy + mzz * uz;
+  const float um1 = ux * m1x + uy * m1y + uz * m1z;
+  const float um2u = ux * mux + uy * muy + uz * muz;
+  const float quad = 3.0f * um1 + 4.5f * um2u - 1.5f * usq * m0;
+  const float P = m0 + quad;
+  const float dom = fmaf(dh, m0, rho * quad) - sf;
+  const float vx = rho * (3.0f * m1x + 9.0f * mux - 3.0f * ux * m0);
+  const float vy = rho * (3.0f * m1y + 9.0f * muy - 3.0f * uy * m0);
+  const float vz = rho * (3.0f * m1z + 9.0f * muz - 3.0f * uz * m0);
+  const float oA = omega * (P - (vx * ux + vy * uy + vz * uz) * k);
+  const float obx = omega * vx * k, oby = omega * vy * k, obz = omega * vz * k;
+  const float om1 = 1.0f - omega;
 #pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    const float cu = cx(i) * ux + cy(i) * uy + cz(i) * uz;
-    const float feq = wf(i) * (dh + rho * (3.0f * cu + 4.5f * cu * cu - 1.5f * usq));
-    dom += mu[i] * (feq - f[i]);
+  for (int j = 0; j < kQ; ++j) {
+    float t = oA;
+    if (cx(j) != 0) t += cx(j) > 0 ? obx : -obx;
+    if (cy(j) != 0) t += cy(j) > 0 ? oby : -oby;
+    if (cz(j) != 0) t += cz(j) > 0 ? obz : -obz;
+    mu[j] = fmaf(om1, mu[j], t);
   }
-  float P, Vx, Vy, Vz;
-  feq_vjp(mu, rho, ux, uy, uz, P, Vx, Vy, Vz);
-#pragma unroll
-  for (int j = 0; j < kQ; ++j)
-    mu[j] = (1.0f - omega) * mu[j] + omega * (P + (Vx * (cx(j) - ux) + Vy * (cy(j) - uy) + Vz * (cz(j) - uz)) * k);
+  fgx = 3.0f * m1x;
+  fgy = 3.0f * m1y;
+  fgz = 3.0f * m1z;
   return dom;
 }
 
@@ -343,8 +361,12 @@ __global__ void __launch_bounds__(kThreads, LINKS ? 3 : 2) k_adj_step(const Step
     float gw = 0.f;
     const float dom = adj_near_cell(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)), lane,
                                     lamY, lamX, lamS, gF, gw);
-    add_grad(g, kGOmega, lane == 0 ? static_cast<double>(dom) : 0.0);
-    add_grad(g, kGWallVelocity, static_cast<double>(gw));
+    double a2[2] = {lane == 0 ? static_cast<double>(dom) : 0.0, static_cast<double>(gw)};
+    block_reduce<2>(a2);
+    if (threadIdx.x == 0) {
+      if (a2[0] != 0.0) atomicAdd(g + kGOmega, a2[0]);
+      if (a2[1] != 0.0) atomicAdd(g + kGWallVelocity, a2[1]);
+    }
     return;
   }
   const uint32_t bid = blockIdx.x - near_ctas;
@@ -408,37 +430,30 @@ __global__ void __launch_bounds__(kThreads, LINKS ? 3 : 2) k_adj_step(const Step
     }
     const bool bulk = !FLAGS || (fl & kKindMask) == kBulk;
     double gf0 = 0.0, gf1 = 0.0, gf2 = 0.0;  // body-force gradient of this cell (one writer per launch)
+    float fgx = 0.f, fgy = 0.f, fgz = 0.f;
     if (bulk) {
       gf0 = gF[t];
       gf1 = gF[a.ncore + t];
       gf2 = gF[2ull * a.ncore + t];
+      dom += bgk_vjp_moments(f, a.omega, lam, fgx, fgy, fgz);
+    }
+    // no store before this point: the save row's loads need not wait
+    const bool save = FLAGS && (fl & kFlagSave);
+    float* ls = save ? lamS + static_cast<long long>(__ldg(a.save_idx + t)) * kQ : nullptr;
+    if (save) {
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) lam[i] += ls[i];
     }
 #pragma unroll
     for (int i = 0; i < kQ; ++i) lamY[i * qs + t] = 0.f;
-    if (bulk) {
-      float sx = 0.f, sy = 0.f, sz = 0.f;
+    if (save) {
 #pragma unroll
-      for (int i = 0; i < kQ; ++i) {
-        const float v = 3.0f * wf(i) * lam[i];
-        sx += cx(i) * v;
-        sy += cy(i) * v;
-        sz += cz(i) * v;
-      }
-      gF[t] = gf0 + sx;
-      gF[a.ncore + t] = gf1 + sy;
-      gF[2ull * a.ncore + t] = gf2 + sz;
-      dom += bgk_vjp_inplace(f, a.omega, lam);
+      for (int i = 0; i < kQ; ++i) ls[i] = 0.f;
     }
-    if (FLAGS && (fl & kFlagSave)) {
-      float* ls = lamS + static_cast<long long>(__ldg(a.save_idx + t)) * kQ;
-      float lsv[kQ];
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) lsv[i] = ls[i];
-#pragma unroll
-      for (int i = 0; i < kQ; ++i) {
-        lam[i] += lsv[i];
-        ls[i] = 0.f;
-      }
+    if (bulk) {
+      gF[t] = gf0 + fgx;
+      gF[a.ncore + t] = gf1 + fgy;
+      gF[2ull * a.ncore + t] = gf2 + fgz;
     }
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
@@ -451,8 +466,12 @@ __global__ void __launch_bounds__(kThreads, LINKS ? 3 : 2) k_adj_step(const Step
       atomicAdd(lamX + (sm >= 0 ? i * qs + sm : opp(i) * qs + t), lam[i]);
     }
   }
-  add_grad(g, kGOmega, dom);
-  add_grad(g, kGWallVelocity, static_cast<double>(gw));
+  double a2[2] = {dom, static_cast<double>(gw)};
+  block_reduce<2>(a2);
+  if (threadIdx.x == 0) {
+    if (a2[0] != 0.0) atomicAdd(g + kGOmega, a2[0]);
+    if (a2[1] != 0.0) atomicAdd(g + kGWallVelocity, a2[1]);
+  }
 }
 
 
@@ -554,13 +573,13 @@ __global__ void __launch_bounds__(kThreads)
 k_adj_prolong(const ProlongItem* items, int nitems, const float* coarse_save, const float* prev, int half,
               float* lam_fine, long long fine_qs, float s, float omega, float* lam_m, float* lam_prev,
               float* lam_save, double* g, double* gF_fine, long long fine_ncore) {
-  pdl_wait();
-
   const int w = (blockIdx.x * kThreads + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
+  ProlongItem it{};
+  if (w < nitems) it = items[w];  // constant table: read before the wait
+  pdl_wait();
   float ds = 0.f, dom = 0.f;
   if (w < nitems) {
-    const ProlongItem it = items[w];
     const LaneDir d = lane_dir(lane);
     // every load first (see adj_near_cell)
     const float* row = coarse_save + static_cast<long long>(it.coarse_save) * kQ;
@@ -623,16 +642,18 @@ k_adj_prolong(const ProlongItem* items, int nitems, const float* coarse_save, co
 __global__ void __launch_bounds__(kThreads)
 k_adj_restrict(const RestrictItem* items, int nitems, const float* fine_save, float* lam_coarse, long long coarse_qs,
                float s, float omega, float* lam_save, double* g, double* gF_coarse, long long coarse_ncore) {
-  pdl_wait();
-
   const int w = (blockIdx.x * kThreads + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
+  const RestrictItem& it = items[w < nitems ? w : 0];
+  // constant table: read before the wait
+  const int row = w >= nitems ? -1 : (lane == 0 ? it.fine_save : (lane <= it.nnb ? it.nb_save[lane - 1] : -1));
+  const long long cslot = w < nitems ? it.coarse_slot : 0;
+  const int ckind = w < nitems ? it.coarse_kind : 0, nnb = w < nitems ? it.nnb : 0;
+  pdl_wait();
   float ds = 0.f, dom = 0.f;
   if (w < nitems) {
-    const RestrictItem& it = items[w];
-    const int row = lane == 0 ? it.fine_save : (lane <= it.nnb ? it.nb_save[lane - 1] : -1);
     const LaneDir d = lane_dir(lane);
-    float* p = lam_coarse + lane * coarse_qs + it.coarse_slot;
+    float* p = lam_coarse + lane * coarse_qs + cslot;
     const float mu = d.act ? *p : 0.f;
     Macro m;
     float f[kQ];
@@ -649,7 +670,7 @@ k_adj_restrict(const RestrictItem* items, int nitems, const float* fine_save, fl
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
       sum[i] = v;
     }
-    const float inv = 1.0f / static_cast<float>(it.nnb + 1);
+    const float inv = 1.0f / static_cast<float>(nnb + 1);
     // r = (centre drho, u; f_neq average) spread over the lanes
     float rf = 0.f;
 #pragma unroll
@@ -659,9 +680,9 @@ k_adj_restrict(const RestrictItem* items, int nitems, const float* fine_save, fl
     }
     const float rd = __shfl_sync(0xffffffffu, m.drho, 0), rx = __shfl_sync(0xffffffffu, m.ux, 0);
     const float ry = __shfl_sync(0xffffffffu, m.uy, 0), rz = __shfl_sync(0xffffffffu, m.uz, 0);
-    if (it.coarse_kind == kBulk) force_grad_lanes(d, mu, gF_coarse, coarse_ncore, it.coarse_slot, lane);
+    if (ckind == kBulk) force_grad_lanes(d, mu, gF_coarse, coarse_ncore, cslot, lane);
     float lfneq, ldrho, lux, luy, luz;
-    write_vjp_lanes(d, rd, rx, ry, rz, rf, s, it.coarse_kind, omega, mu, lfneq, ldrho, lux, luy, luz, ds, dom);
+    write_vjp_lanes(d, rd, rx, ry, rz, rf, s, ckind, omega, mu, lfneq, ldrho, lux, luy, luz, ds, dom);
     // row k's cotangent: f_neq part inv * lfneq (all rows), drho / u (centre)
     Macro lm;
     lm.drho = lane == 0 ? ldrho : 0.f;
