@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(kThreads) k_add_force(const StepArgs a, T* pop
 // (a few thousand items).
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_prolong(const ProlongItem* items, int nitems, const float* coarse_save, float* prev, int half,
+k_prolong(const ProlongItem* items, int nitems, const float* coarse_save, float* prev, int half, float* rec_prev,
           T* fine, long long fine_qs, float scale, float omega, float fscale) {
   const int w = static_cast<int>((blockIdx.x * kThreads + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
@@ -401,6 +401,14 @@ k_prolong(const ProlongItem* items, int nitems, const float* coarse_save, float*
   if (half) {
     p0 = pv[0]; p1 = pv[1]; p2 = pv[2]; p3 = pv[3];
     pf = d.act ? pv[4 + lane] : 0.f;
+    if (rec_prev) {  // the adjoint's record of the rows read here
+      float* rp = rec_prev + static_cast<long long>(it.prev) * 23;
+      if (d.act) rp[4 + lane] = pf;
+      if (lane == kQ) rp[0] = p0;
+      if (lane == kQ + 1) rp[1] = p1;
+      if (lane == kQ + 2) rp[2] = p2;
+      if (lane == kQ + 3) rp[3] = p3;
+    }
   }
   float fa[kQ];
   gather_lanes(fr, fa);
@@ -732,11 +740,11 @@ cudaError_t launch_add_force(const StepArgs& a, T* pops, const float* force, cud
 
 template <typename T>
 cudaError_t launch_prolong(const ProlongItem* items, int n, const float* coarse_save, float* prev,
-                           int half, T* fine, long long fine_qs, float scale, float omega,
+                           int half, float* rec_prev, T* fine, long long fine_qs, float scale, float omega,
                            float fscale, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   const cudaError_t e = launch_chain(k_prolong<T>, dim3(grid_for(static_cast<uint32_t>(n) * 32)), dim3(kThreads), 0, s,
-                                     items, n, coarse_save, prev, half, fine, fine_qs, scale, omega, fscale);
+                                     items, n, coarse_save, prev, half, rec_prev, fine, fine_qs, scale, omega, fscale);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -794,7 +802,7 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
   template cudaError_t launch_step_near<T>(const StepArgs&, const NearTables&, cudaStream_t);       \
   template cudaError_t launch_add_force<T>(const StepArgs&, T*, const float*, cudaStream_t);         \
   template cudaError_t launch_step_map<T>(const StepArgs&, const NearTables&, bool, bool, int, bool, cudaStream_t); \
-  template cudaError_t launch_prolong<T>(const ProlongItem*, int, const float*, float*, int, T*,   \
+  template cudaError_t launch_prolong<T>(const ProlongItem*, int, const float*, float*, int, float*, T*, \
                                          long long, float, float, float, cudaStream_t);            \
   template cudaError_t launch_restrict<T>(const RestrictItem*, int, const float*, T*, long long,   \
                                           float, float, float, cudaStream_t);                      \

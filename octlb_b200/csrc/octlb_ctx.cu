@@ -21,7 +21,7 @@ namespace octlb_gpu {
 
 template <typename T> cudaError_t launch_step(const StepArgs&, bool, bool, bool, cudaStream_t);
 template <typename T>
-cudaError_t launch_prolong(const ProlongItem*, int, const float*, float*, int, T*, long long, float,
+cudaError_t launch_prolong(const ProlongItem*, int, const float*, float*, int, float*, T*, long long, float,
                            float, float, cudaStream_t);
 template <typename T>
 cudaError_t launch_restrict(const RestrictItem*, int, const float*, T*, long long, float, float,
@@ -376,17 +376,19 @@ int do_advance_level(octlb_ctx* ctx, int l) {
   ++ctx->counters_stream[l];
   if (l >= ctx->max_level) return OCTLB_OK;
   Level& F = ctx->levels[l + 1];
-  if (ctx->adj && ctx->adj->recording && L.n_prolong > 0) {
-    StepRecord& R = ctx->adj->recs[ctx->adj->last_rec[l]];
-    CK(cudaMemcpyAsync(R.prev.p, L.prev.p, R.prev.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-  }
+  // Recording: the half-time prolongation copies the prev-macro rows it
+  // reads into the step record (its adjoint needs them).
+  float* rec_prev = nullptr;
+  if (ctx->adj && ctx->adj->recording && L.n_prolong > 0)
+    rec_prev = ctx->adj->recs[ctx->adj->last_rec[l]].prev.as<float>();
   // apply_half_time(l) -> advance(l+1) -> apply_full_time(l) -> advance(l+1)
   // -> restrict(l+1)  (time_loop.h:228-239)
   for (int phase = 0; phase < 2; ++phase) {
     if (L.n_prolong > 0) {
       CK(launch_prolong<T>(L.prolong_items.as<ProlongItem>(), L.n_prolong, save_ptr(L),
-                           L.prev.as<float>(), phase == 0 ? 1 : 0, static_cast<T*>(cur_buf(F)), F.nslots,
-                           ctx->prolong_scale, static_cast<float>(ctx->omega), F.scale, ctx->stream));
+                           L.prev.as<float>(), phase == 0 ? 1 : 0, phase == 0 ? rec_prev : nullptr,
+                           static_cast<T*>(cur_buf(F)), F.nslots, ctx->prolong_scale,
+                           static_cast<float>(ctx->omega), F.scale, ctx->stream));
     }
     rc = do_advance_level<T>(ctx, l + 1);
     if (rc) return rc;
