@@ -389,6 +389,7 @@ __global__ void __launch_bounds__(kThreads, LINKS ? 3 : 2) k_adj_step(const Step
   const int np = a.np, np3 = np * np * np;
   const int* gm = a.slot_map + static_cast<long long>(b) * np3;
   for (int k = threadIdx.x; k < np3; k += kThreads) smap[k] = gm[k];
+  const bool moving = a.blk_moving[b] != 0;  // uniform over the CTA
   __syncthreads();
   pdl_wait();
   const float* src = static_cast<const float*>(a.src);
@@ -423,10 +424,12 @@ __global__ void __launch_bounds__(kThreads, LINKS ? 3 : 2) k_adj_step(const Step
       f[i] = __ldg(src + (sm >= 0 ? i * qs + sm : opp(i) * qs + t));
       lam[i] = lamY[i * qs + t];  // the output's cotangent, turned into the input's below
     }
+    if (moving) {  // moving-wall markers: only blocks flagged in blk_moving
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) {
-      const int sm = smap[P - a.off_pad[i]];
-      if (sm < -1) f[i] += __ldg(a.wall_add + (-sm - 2) * kQ + i);
+      for (int i = 0; i < kQ; ++i) {
+        const int sm = smap[P - a.off_pad[i]];
+        if (sm < -1) f[i] += __ldg(a.wall_add + (-sm - 2) * kQ + i);
+      }
     }
     const bool bulk = !FLAGS || (fl & kKindMask) == kBulk;
     double gf0 = 0.0, gf1 = 0.0, gf2 = 0.0;  // body-force gradient of this cell (one writer per launch)
@@ -455,10 +458,12 @@ __global__ void __launch_bounds__(kThreads, LINKS ? 3 : 2) k_adj_step(const Step
       gF[a.ncore + t] = gf1 + fgy;
       gF[2ull * a.ncore + t] = gf2 + fgz;
     }
+    if (moving) {
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) {
-      const int sm = smap[P - a.off_pad[i]];
-      if (sm < -1) gw += lam[i] * __ldg(a.wall_dadd + (-sm - 2) * kQ + i);
+      for (int i = 0; i < kQ; ++i) {
+        const int sm = smap[P - a.off_pad[i]];
+        if (sm < -1) gw += lam[i] * __ldg(a.wall_dadd + (-sm - 2) * kQ + i);
+      }
     }
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {

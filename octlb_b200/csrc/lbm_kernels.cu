@@ -274,6 +274,7 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
   // GMAP: the map is read through the read-only L1 path instead (no staging
   // barrier); 4 KB per block stays L1-resident for the CTA
   const int* smap = GMAP ? gm : smap_s;
+  const bool moving = a.blk_moving[b] != 0;  // uniform over the CTA
   pdl_wait();
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
@@ -297,16 +298,28 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
     for (int i = 0; i < kQ; ++i) {
       const uint32_t row = static_cast<uint32_t>(i) * qs;
 #pragma unroll
-      for (int c = 0; c < CPT; ++c)
-      {
+      for (int c = 0; c < CPT; ++c) {
         // bounce-back wall position (marker < 0): the cell's own opposite
-        // population, plus the wall term when it moves; branch-free so the
-        // 19 (or 38) loads stay independent
+        // population; branch-free so the 19 (or 38) loads stay independent
         const int sm = GMAP ? __ldg(smap + P[c] - a.off_pad[i]) : smap[P[c] - a.off_pad[i]];
         const uint32_t off = sm >= 0 ? row + static_cast<uint32_t>(sm) : static_cast<uint32_t>(opp(i)) * qs + t[c];
         const float v = Store<T>::ld(src + off, a.inv_scale);
-        f[c][i] = sm < -1 ? v + a.wall_add[(-sm - 2) * kQ + i] : v;
+        // two cells per thread: the moving-wall term inline (a separate pass
+        // costs these variants registers)
+        if constexpr (CPT == 2) f[c][i] = sm < -1 ? v + a.wall_add[(-sm - 2) * kQ + i] : v;
+        else f[c][i] = v;
       }
+    }
+    if (CPT == 1 && moving) {
+      // moving-wall markers (< -1) add the wall term: only blocks flagged in
+      // blk_moving hold one, the others skip this pass
+#pragma unroll
+      for (int i = 0; i < kQ; ++i)
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          const int sm = GMAP ? __ldg(smap + P[c] - a.off_pad[i]) : smap[P[c] - a.off_pad[i]];
+          if (sm < -1) f[c][i] += a.wall_add[(-sm - 2) * kQ + i];
+        }
     }
 #pragma unroll
     for (int c = 0; c < CPT; ++c)

@@ -107,6 +107,7 @@ struct Level {
   // tree-boundary halo fills
   DevBuf bb_ops, fill_of;           // fills, and per (page slot, population) the fill index or -1
   DevBuf wall_add, wall_dadd;       // slot-map wall markers' terms
+  DevBuf blk_moving;                // per block: its map holds a moving-wall marker
   uint32_t n_bb = 0;
   // coupler: this level as coarse (prolong) and as fine (restrict)
   DevBuf prolong_items, prev, restrict_items;
@@ -1208,6 +1209,12 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       CK(upload(L.slot_map, slot_map));
       CK(upload(L.wall_add, wall_add));
       CK(upload(L.wall_dadd, wall_dadd));
+      std::vector<uint8_t> moving(static_cast<size_t>(L.nblk), 0);
+      for (int lb = 0; lb < L.nblk; ++lb)
+        for (int k = 0; k < np3 && !moving[lb]; ++k)
+          if (slot_map[static_cast<size_t>(lb) * np3 + k] < -1) moving[lb] = 1;
+      CK(upload(L.blk_moving, moving));
+      A.blk_moving = L.blk_moving.as<uint8_t>();
       A.slot_map = L.slot_map.as<int>();
       A.wall_add = L.wall_add.as<float>();
       A.wall_dadd = L.wall_dadd.as<float>();

@@ -39,6 +39,7 @@ struct StepArgs {
   const struct BBOp* fills; // the fills (never materialised: readers take the source, pull_value)
   const float* wall_add;    // [k][19] wall terms of slot-map marker -(2 + k) (moving bounce-back wall)
   const float* wall_dadd;   // [k][19] their derivative by the wall-velocity scale
+  const uint8_t* blk_moving; // [nblk] 1 where the block's slot map holds a moving-wall marker
   int n_open, n_halo;       // items, halo slots per page
   int nblk, n, np;          // np = n + 2
   long long halo_base;      // first halo-page slot (= nblk * n^3)
