@@ -432,14 +432,8 @@ __global__ void __launch_bounds__(kThreads, LINKS ? 3 : 2) k_adj_step(const Step
       }
     }
     const bool bulk = !FLAGS || (fl & kKindMask) == kBulk;
-    double gf0 = 0.0, gf1 = 0.0, gf2 = 0.0;  // body-force gradient of this cell (one writer per launch)
-    float fgx = 0.f, fgy = 0.f, fgz = 0.f;
-    if (bulk) {
-      gf0 = gF[t];
-      gf1 = gF[a.ncore + t];
-      gf2 = gF[2ull * a.ncore + t];
-      dom += bgk_vjp_moments(f, a.omega, lam, fgx, fgy, fgz);
-    }
+    float fgx = 0.f, fgy = 0.f, fgz = 0.f;  // body-force gradient of this cell
+    if (bulk) dom += bgk_vjp_moments(f, a.omega, lam, fgx, fgy, fgz);
     // no store before this point: the save row's loads need not wait
     const bool save = FLAGS && (fl & kFlagSave);
     float* ls = save ? lamS + static_cast<long long>(__ldg(a.save_idx + t)) * kQ : nullptr;
@@ -453,10 +447,10 @@ __global__ void __launch_bounds__(kThreads, LINKS ? 3 : 2) k_adj_step(const Step
 #pragma unroll
       for (int i = 0; i < kQ; ++i) ls[i] = 0.f;
     }
-    if (bulk) {
-      gF[t] = gf0 + fgx;
-      gF[a.ncore + t] = gf1 + fgy;
-      gF[2ull * a.ncore + t] = gf2 + fgz;
+    if (bulk) {  // one contributor per cell and launch: no return trip needed
+      atomicAdd(gF + t, static_cast<double>(fgx));
+      atomicAdd(gF + a.ncore + t, static_cast<double>(fgy));
+      atomicAdd(gF + 2ull * a.ncore + t, static_cast<double>(fgz));
     }
     if (moving) {
 #pragma unroll
