@@ -7,6 +7,9 @@ by the product.
   GhostSchedule / TimeLoop / MomentumExchangeDrag, compiled from its sources by
   `make -C oracle ref` where the reference tree is available; prebuilt files
   travel with the repository.
+* ``_ref/liboctlb_ref_tlm.so`` -- the same sources compiled on a forward-mode
+  dual number (`make -C oracle tlm`): the tangent-linear FP64 reference, whose
+  force carries its derivatives along seeded parameter directions.
 """
 import ctypes
 import os
@@ -17,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_PATH = os.path.join(HERE, "liboctlb_oracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "liboctlb_ref.so")
+TLM_PATH = os.path.join(HERE, "_ref", "liboctlb_ref_tlm.so")
 Q = 19
 P = ctypes.c_void_p
 
@@ -30,11 +34,13 @@ def build(ref=True):
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     src = os.environ.get("OCTLB_REFERENCE", "/root/reference")
     if ref and os.path.isdir(os.path.join(src, "src", "solver", "lbm")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={src}"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "tlm", f"REF={src}"], check=True)
 
 
 def load(which):
-    path = ORC_PATH if which == "orc" else REF_PATH
+    """'orc' (C restatement), 'ref' (the reference) or 'tlm' (the reference
+    on dual numbers; same ref_* entry points plus tlm_*)."""
+    path = {"orc": ORC_PATH, "ref": REF_PATH, "tlm": TLM_PATH}[which]
     if not os.path.exists(path):
         return None
     L = ctypes.CDLL(path)
@@ -46,6 +52,8 @@ def load(which):
         getattr(L, pre + fn).restype = ctypes.c_double
         getattr(L, pre + fn).argtypes = ([ctypes.c_int] + [ctypes.c_double] * 4 if fn == "feq"
                                          else [ctypes.c_double] * 4)
+    if which == "tlm":
+        L.tlm_dirs.restype = ctypes.c_int
     if which == "orc":
         L.orc_periodic_slabs_mlups.restype = ctypes.c_double
         L.orc_periodic_slabs_mlups.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double, ctypes.c_int]
@@ -142,10 +150,18 @@ def rho_u(pops):
 
 
 class Sim:
-    """TimeLoop over a forest (reference oracle only: ref_sim_*)."""
+    """TimeLoop over a forest (reference oracle only: ref_sim_*).  On the
+    tangent-linear library, omega_seed[k] / wall_seed[k] seed direction k:
+    d omega, and d u_w / u_w for every tree-boundary wall velocity."""
 
-    def __init__(self, L, mesh, omega, init_pops=None, link_mode=False):
+    def __init__(self, L, mesh, omega, init_pops=None, link_mode=False, omega_seed=None, wall_seed=None):
         self.L, self.mesh = L, mesh
+        if hasattr(L, "tlm_set_seeds"):
+            nd = L.tlm_dirs()
+            om = np.zeros(nd) if omega_seed is None else np.ascontiguousarray(omega_seed, np.float64)
+            ws = np.zeros(nd) if wall_seed is None else np.ascontiguousarray(wall_seed, np.float64)
+            assert om.shape == (nd,) and ws.shape == (nd,)
+            L.tlm_set_seeds(_p(om), _p(ws))
         n = mesh.n
         self._keep = [mesh]
         init = None if init_pops is None else np.ascontiguousarray(init_pops, np.float64)
@@ -175,6 +191,23 @@ class Sim:
         f = None if force is None else np.ascontiguousarray(force, np.float64)
         self._keep.append(f)
         self.L.ref_sim_set_body_force(self.h, _p(f))
+
+    def set_body_force_tlm(self, force, dirs):
+        """Tangent-linear library: body force (or None = 0) with its
+        derivative dirs[k] ([k][n_blocks][n^3][3]) along direction k."""
+        m = self.mesh.n_blocks * self.mesh.n ** 3 * 3
+        f = None if force is None else np.ascontiguousarray(force, np.float64).reshape(m)
+        d = np.ascontiguousarray(dirs, np.float64).reshape(-1, m)
+        self._keep += [f, d]
+        self.L.tlm_sim_set_body_force(self.h, _p(f), _p(d), ctypes.c_int(d.shape[0]))
+
+    def drag_tlm(self, mask=None):
+        """Tangent-linear library: the force (3,) and its derivatives (3, k)."""
+        nd = self.L.tlm_dirs()
+        out, dout = np.zeros(3), np.zeros((3, nd))
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        self.L.tlm_sim_drag(self.h, _p(m, ctypes.c_uint8), _p(out), _p(dout))
+        return out, dout
 
     def core(self):
         n = self.mesh.n

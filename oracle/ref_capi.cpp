@@ -18,6 +18,12 @@
 //     post-collision populations of kBulk cells of the level just collided, at
 //     the same hook before the fills (the reference has no body force; the
 //     adjoint's finite-difference checks need one).
+//
+// The same file also builds the tangent-linear library (ref_tlm.cpp, with the
+// reference's floating type replaced by a forward-mode dual number): the C
+// ABI therefore uses f64 (always a plain double) and copies its buffers
+// element by element, and omega and the wall velocities pass through the
+// seed hooks, identities in this build.
 #include <array>
 #include <cmath>
 #include <cstdint>
@@ -48,6 +54,13 @@ using D = olb::descriptors::D3Q19<>;
 using Lat = BlockLattice<double, D>;
 static constexpr int Q = 19;
 
+#ifndef OCTLB_REF_TLM
+using f64 = double;
+inline f64 to_f64(double x) { return x; }
+inline double seed_omega(double omega) { return omega; }
+inline double seed_wall(double u) { return u; }
+#endif
+
 namespace {
 
 inline int cc(int i, int d) { return olb::descriptors::c<D>(i, d); }
@@ -65,7 +78,7 @@ struct Block {
 // per-cell path (block_lattice.cpp:536-548,639-670): non-solid core cells
 // whose source x-c_i is a solid / Bouzidi core cell.
 void AddMovingWallTerm(Lat& lat, int nx, int ny, int nz, const uint8_t* moving,
-                       const double* uw) {
+                       const f64* uw) {
   auto cidx = [&](int x, int y, int z) { return (x * ny + y) * nz + z; };
   for (int x = 0; x < nx; ++x)
     for (int y = 0; y < ny; ++y)
@@ -208,6 +221,21 @@ struct Sim {
   std::unique_ptr<TimeLoop> loop;
 };
 
+// Sum of MomentumExchangeDrag::force_on_fluid_if over all blocks (see
+// ref_sim_drag).
+std::array<double, 3> SimDrag(Sim* s, const uint8_t* mask) {
+  const int n = s->n, n3 = n * n * n;
+  std::array<double, 3> out{0.0, 0.0, 0.0};
+  for (label id = 0; id < s->blocks->size(); ++id) {
+    MomentumExchangeDrag drag((*s->blocks)[id]);
+    const uint8_t* m = mask ? mask + (std::size_t)id * n3 : nullptr;
+    auto f = drag.force_on_fluid_if([&](int x, int y, int z) {
+      return m == nullptr || m[(x * n + y) * n + z] != 0;
+    });
+    out[0] += f[0]; out[1] += f[1]; out[2] += f[2];
+  }
+  return out;
+}
 }  // namespace
 
 extern "C" {
@@ -221,7 +249,7 @@ void* ref_block_new(int nx, int ny, int nz) {
 }
 void ref_block_free(void* h) { delete static_cast<Block*>(h); }
 
-void ref_block_initialize(void* h, double rho, double ux, double uy, double uz) {
+void ref_block_initialize(void* h, f64 rho, f64 ux, f64 uy, f64 uz) {
   const double u[3] = {ux, uy, uz};
   static_cast<Block*>(h)->lat->initialize(rho, u);
 }
@@ -234,24 +262,26 @@ void ref_block_set_kinds(void* h, const uint8_t* kinds) {
 }
 // Padded storage [(nx+2)][(ny+2)][(nz+2)][19], the reference's own layout
 // (block_lattice.h:294-304).
-void ref_block_get_padded(void* h, double* out) {
+void ref_block_get_padded(void* h, f64* out) {
   auto* b = static_cast<Block*>(h);
   const std::size_t n = (std::size_t)(b->nx + 2) * (b->ny + 2) * (b->nz + 2) * Q;
-  std::memcpy(out, b->lat->populations_at_halo(0, 0, 0), n * sizeof(double));
+  const double* p = b->lat->populations_at_halo(0, 0, 0);
+  for (std::size_t k = 0; k < n; ++k) out[k] = to_f64(p[k]);
 }
-void ref_block_set_padded(void* h, const double* in) {
+void ref_block_set_padded(void* h, const f64* in) {
   auto* b = static_cast<Block*>(h);
   const std::size_t n = (std::size_t)(b->nx + 2) * (b->ny + 2) * (b->nz + 2) * Q;
-  std::memcpy(b->lat->populations_at_halo(0, 0, 0), in, n * sizeof(double));
+  double* p = b->lat->populations_at_halo(0, 0, 0);
+  for (std::size_t k = 0; k < n; ++k) p[k] = in[k];
 }
-void ref_block_collide(void* h, double omega) { static_cast<Block*>(h)->lat->collide(omega); }
+void ref_block_collide(void* h, f64 omega) { static_cast<Block*>(h)->lat->collide(omega); }
 void ref_block_fill_periodic(void* h) { static_cast<Block*>(h)->lat->fill_periodic_halo(); }
 void ref_block_stream(void* h) { static_cast<Block*>(h)->lat->stream(); }
 void ref_block_snapshot(void* h) { static_cast<Block*>(h)->lat->take_post_collide_snapshot(); }
 
 // Attach a BouzidiLinkData table (q defaults to 1.0 = half-way bounce-back,
 // bouzidi_link_data.cpp:107-116) with the given cut links overriding it.
-void ref_block_set_links(void* h, int n_links, const int* cell_pop, const double* q) {
+void ref_block_set_links(void* h, int n_links, const int* cell_pop, const f64* q) {
   auto* b = static_cast<Block*>(h);
   b->links = std::make_unique<BouzidiLinkData>(1, b->nx, b->ny, b->nz, Q);
   for (int k = 0; k < n_links; ++k)
@@ -259,14 +289,14 @@ void ref_block_set_links(void* h, int n_links, const int* cell_pop, const double
                          cell_pop[4 * k + 3], q[k]);
   b->lat->set_bouzidi_links(b->links.get());
 }
-void ref_block_add_moving_wall(void* h, const uint8_t* moving, const double* uw) {
+void ref_block_add_moving_wall(void* h, const uint8_t* moving, const f64* uw) {
   auto* b = static_cast<Block*>(h);
   AddMovingWallTerm(*b->lat, b->nx, b->ny, b->nz, moving, uw);
 }
 
 // Periodic box: collide -> fill_periodic_halo -> stream, the loop of
 // tests/unit/solver/test_collision_bgk.cpp:56-60.
-void ref_block_run_periodic(void* h, double omega, int steps) {
+void ref_block_run_periodic(void* h, f64 omega, int steps) {
   auto* b = static_cast<Block*>(h);
   for (int t = 0; t < steps; ++t) {
     b->lat->collide(omega);
@@ -275,8 +305,8 @@ void ref_block_run_periodic(void* h, double omega, int steps) {
   }
 }
 // Walled box (solid shell + q table): collide -> stream -> moving-wall term.
-void ref_block_run_walls(void* h, double omega, int steps, const uint8_t* moving,
-                         const double* uw) {
+void ref_block_run_walls(void* h, f64 omega, int steps, const uint8_t* moving,
+                         const f64* uw) {
   auto* b = static_cast<Block*>(h);
   for (int t = 0; t < steps; ++t) {
     b->lat->collide(omega);
@@ -286,27 +316,28 @@ void ref_block_run_walls(void* h, double omega, int steps, const uint8_t* moving
 }
 // MomentumExchangeDrag::force_on_fluid_if over this block
 // (drag_postprocessor.h:67-115); obstacle mask over core cells or null.
-void ref_block_drag(void* h, const uint8_t* mask, double* out) {
+void ref_block_drag(void* h, const uint8_t* mask, f64* out) {
   auto* b = static_cast<Block*>(h);
   MomentumExchangeDrag drag(*b->lat);
   const int ny = b->ny, nz = b->nz;
   auto f = drag.force_on_fluid_if([&](int x, int y, int z) {
     return mask == nullptr || mask[(x * ny + y) * nz + z] != 0;
   });
-  out[0] = f[0]; out[1] = f[1]; out[2] = f[2];
+  out[0] = to_f64(f[0]); out[1] = to_f64(f[1]); out[2] = to_f64(f[2]);
 }
 
 // ------------------------------------------------------------- octree + loop
 // Forest description: leaves (level, bounds), and the FacePairList lists.
-void* ref_sim_new(int n_oct, const int* levels, const double* bounds, int n_sl,
+void* ref_sim_new(int n_oct, const int* levels, const f64* bounds, int n_sl,
                   const int* sl /* local, dir, remote */, int n_cf,
                   const int* cf /* coarse, f0..f3, normal, clevel, flevel */,
-                  const double* cf_bounds /* coarse 6 + 4 x fine 6 */, int n_tb,
-                  const int* tb /* oct, dir */, const double* tb_spec /* 7 per face */,
-                  int n, double omega, const uint8_t* kinds /* [oct][n^3] */,
-                  const double* core_pops /* [oct][n^3][19] or null */,
+                  const f64* cf_bounds /* coarse 6 + 4 x fine 6 */, int n_tb,
+                  const int* tb /* oct, dir */, const f64* tb_spec /* 7 per face */,
+                  int n, f64 omega_in, const uint8_t* kinds /* [oct][n^3] */,
+                  const f64* core_pops /* [oct][n^3][19] or null */,
                   int n_links, const int* link_cells /* oct,x,y,z,pop */,
-                  const double* link_q, int link_mode) {
+                  const f64* link_q, int link_mode) {
+  const double omega = seed_omega(omega_in);
   auto* s = new Sim;
   s->n = n;
   s->forest = std::make_unique<OctreeForest>(MPI_COMM_WORLD, BoundingBox{});
@@ -322,7 +353,7 @@ void* ref_sim_new(int n_oct, const int* levels, const double* bounds, int n_sl,
   for (int i = 0; i < n_cf; ++i) {
     CoarseFineFace e{};
     const int* r = cf + 8 * i;
-    const double* bd = cf_bounds + 30 * i;
+    const f64* bd = cf_bounds + 30 * i;
     e.coarse_id = r[0];
     for (int k = 0; k < 4; ++k) { e.fine_ids[k] = r[1 + k]; e.remote_ranks[k] = 0; e.comm_tags[k] = 0; }
     e.normal = static_cast<FaceDir>(r[5]);
@@ -331,7 +362,7 @@ void* ref_sim_new(int n_oct, const int* levels, const double* bounds, int n_sl,
     e.coarse_remote_rank = 0;
     e.coarse_bounds = {bd[0], bd[1], bd[2], bd[3], bd[4], bd[5]};
     for (int k = 0; k < 4; ++k) {
-      const double* fb = bd + 6 + 6 * k;
+      const f64* fb = bd + 6 + 6 * k;
       e.fine_bounds[k] = {fb[0], fb[1], fb[2], fb[3], fb[4], fb[5]};
     }
     cfv[i] = e;
@@ -340,8 +371,9 @@ void* ref_sim_new(int n_oct, const int* levels, const double* bounds, int n_sl,
   std::vector<FaceSpec> specs(n_tb);
   for (int i = 0; i < n_tb; ++i) {
     tbv[i] = {tb[2 * i], static_cast<FaceDir>(tb[2 * i + 1])};
-    const double* p = tb_spec + 8 * i;
-    specs[i] = {static_cast<int>(p[0]), {p[1], p[2], p[3]}, static_cast<int>(p[4]), p[5], p[6]};
+    const f64* p = tb_spec + 8 * i;
+    specs[i] = {static_cast<int>(p[0]), {seed_wall(p[1]), seed_wall(p[2]), seed_wall(p[3])},
+                static_cast<int>(p[4]), p[5], p[6]};
   }
   OracleForestInject(*s->forest, lv, bx, slv, cfv, tbv);
   s->faces = std::make_unique<FacePairList>(*s->forest);
@@ -364,7 +396,8 @@ void* ref_sim_new(int n_oct, const int* levels, const double* bounds, int n_sl,
           lat.set_bc_kind(x, y, z, static_cast<BcKind>(kinds[(std::size_t)id * n3 + c]));
           if (core_pops) {
             double* f = lat.populations_at_halo(x + 1, y + 1, z + 1);
-            std::memcpy(f, core_pops + ((std::size_t)id * n3 + c) * Q, sizeof(double) * Q);
+            const f64* src = core_pops + ((std::size_t)id * n3 + c) * Q;
+            for (int i = 0; i < Q; ++i) f[i] = src[i];
           }
         }
     if (!core_pops) {
@@ -395,9 +428,14 @@ void ref_sim_advance(void* h, int steps) {
   auto* s = static_cast<Sim*>(h);
   for (int t = 0; t < steps; ++t) s->loop->advance_one();
 }
-void ref_sim_set_body_force(void* h, const double* force) {
+void ref_sim_set_body_force(void* h, const f64* force) {
   auto* s = static_cast<Sim*>(h);
-  static_cast<RestatedBoundary*>(s->bc.get())->set_force(s->loop.get(), force);
+  std::vector<double> f;
+  if (force) {
+    const std::size_t m = static_cast<std::size_t>(s->blocks->size()) * s->n * s->n * s->n * 3;
+    f.assign(force, force + m);
+  }
+  static_cast<RestatedBoundary*>(s->bc.get())->set_force(s->loop.get(), force ? f.data() : nullptr);
 }
 int ref_sim_max_level(void* h) { return static_cast<Sim*>(h)->loop->max_level(); }
 // Collide / stream counters per level and the coupler call sequence.
@@ -414,38 +452,32 @@ int ref_sim_counters(void* h, int* collide, int* stream, int* calls, int max_cal
   }
   return static_cast<int>(c.coupler_calls.size());
 }
-void ref_sim_get_core(void* h, double* out) {
+void ref_sim_get_core(void* h, f64* out) {
   auto* s = static_cast<Sim*>(h);
   const int n = s->n, n3 = n * n * n;
   for (label id = 0; id < s->blocks->size(); ++id)
     for (int x = 0; x < n; ++x)
       for (int y = 0; y < n; ++y)
-        for (int z = 0; z < n; ++z)
-          std::memcpy(out + ((std::size_t)id * n3 + (x * n + y) * n + z) * Q,
-                      (*s->blocks)[id].populations_at_halo(x + 1, y + 1, z + 1),
-                      sizeof(double) * Q);
+        for (int z = 0; z < n; ++z) {
+          f64* o = out + ((std::size_t)id * n3 + (x * n + y) * n + z) * Q;
+          const double* f = (*s->blocks)[id].populations_at_halo(x + 1, y + 1, z + 1);
+          for (int i = 0; i < Q; ++i) o[i] = to_f64(f[i]);
+        }
 }
-void ref_sim_get_padded(void* h, double* out) {
+void ref_sim_get_padded(void* h, f64* out) {
   auto* s = static_cast<Sim*>(h);
   const std::size_t m = (std::size_t)(s->n + 2) * (s->n + 2) * (s->n + 2) * Q;
-  for (label id = 0; id < s->blocks->size(); ++id)
-    std::memcpy(out + id * m, (*s->blocks)[id].populations_at_halo(0, 0, 0), m * sizeof(double));
+  for (label id = 0; id < s->blocks->size(); ++id) {
+    const double* f = (*s->blocks)[id].populations_at_halo(0, 0, 0);
+    for (std::size_t k = 0; k < m; ++k) out[id * m + k] = to_f64(f[k]);
+  }
 }
 // Sum of MomentumExchangeDrag::force_on_fluid_if over all blocks with an
 // obstacle mask [oct][n^3] (or null = every solid / Bouzidi neighbour), the
 // aggregation of examples/cylinder3d/cylinder3d_case.h:473-517 on one rank.
-void ref_sim_drag(void* h, const uint8_t* mask, double* out) {
-  auto* s = static_cast<Sim*>(h);
-  const int n = s->n, n3 = n * n * n;
-  out[0] = out[1] = out[2] = 0.0;
-  for (label id = 0; id < s->blocks->size(); ++id) {
-    MomentumExchangeDrag drag((*s->blocks)[id]);
-    const uint8_t* m = mask ? mask + (std::size_t)id * n3 : nullptr;
-    auto f = drag.force_on_fluid_if([&](int x, int y, int z) {
-      return m == nullptr || m[(x * n + y) * n + z] != 0;
-    });
-    out[0] += f[0]; out[1] += f[1]; out[2] += f[2];
-  }
+void ref_sim_drag(void* h, const uint8_t* mask, f64* out) {
+  const std::array<double, 3> f = SimDrag(static_cast<Sim*>(h), mask);
+  out[0] = to_f64(f[0]); out[1] = to_f64(f[1]); out[2] = to_f64(f[2]);
 }
 // Number of coupling points and the plan itself (coarse id,ci,cj,ck, fine
 // id,fi,fj,fk, coarse level, fine level) for topology checks.
@@ -471,12 +503,12 @@ void ref_sim_coupler_half(void* h, int coarse_level) { static_cast<Sim*>(h)->cou
 void ref_sim_coupler_restrict(void* h, int fine_level) { static_cast<Sim*>(h)->coupler->restrict(fine_level); }
 
 // Reference arithmetic atoms for known-answer checks.
-double ref_bouzidi_pull(double f_bb, double f_q, double f_same, double q) {
-  return boundary::BouzidiPostCollisionPull(f_bb, f_q, f_same, q);
+f64 ref_bouzidi_pull(f64 f_bb, f64 f_q, f64 f_same, f64 q) {
+  return to_f64(boundary::BouzidiPostCollisionPull(double(f_bb), double(f_q), double(f_same), double(q)));
 }
-double ref_feq(int i, double rho, double ux, double uy, double uz) {
+f64 ref_feq(int i, f64 rho, f64 ux, f64 uy, f64 uz) {
   const double u[3] = {ux, uy, uz};
-  return olb::equilibrium<D>::secondOrder(i, rho, u, ux * ux + uy * uy + uz * uz);
+  return to_f64(olb::equilibrium<D>::secondOrder(i, double(rho), u, double(ux * ux + uy * uy + uz * uz)));
 }
 
 }  // extern "C"

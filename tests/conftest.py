@@ -36,3 +36,12 @@ def ref():
     if L is None:
         pytest.skip("reference oracle (oracle/_ref) not built")
     return L
+
+
+@pytest.fixture(scope="session")
+def tlm():
+    from oracle import oracle
+    L = oracle.load("tlm")
+    if L is None:
+        pytest.skip("tangent-linear reference (oracle/_ref/liboctlb_ref_tlm.so) not built")
+    return L

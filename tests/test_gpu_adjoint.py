@@ -9,6 +9,11 @@ tests/golden/make_adjoint_reference.py:
                         over the last 250 calls (1,000 finest steps),
                         checkpoints every 16 calls (64 finest steps).
 
+and against the exact derivatives of the same discrete FP64 map from the
+tangent-linear reference (the reference's TimeLoop on forward-mode dual
+numbers, tests/golden/make_tlm_reference.py): adjoint_c5_short_tlm.npz,
+adjoint_c5_tlm.npz.
+
 Gradients: inlet u_max, tau, and the per-cell body force along 8 seeded
 N(0, 1e-6) directions.  Tolerance: 1e-4 relative.  The adjoint is wrapped in
 a torch.autograd.Function here, in the test harness only.
@@ -50,6 +55,14 @@ def check(ob, name, checkpoint):
     assert abs(dtau - g["dJ_dtau"]) <= TOL * abs(g["dJ_dtau"]), (dtau, float(g["dJ_dtau"]))
     err = np.abs(gdir - g["dJ_dir"]) / np.abs(g["dJ_dir"])
     assert np.all(err <= TOL), err
+    tname = os.path.join(HERE, "golden", name.replace(".npz", "_tlm.npz"))
+    if os.path.exists(tname):  # the tangent-linear FP64 reference
+        t = np.load(tname)
+        assert int(t["steps"]) == steps and int(t["window"]) == window
+        assert abs(du - t["dJ_du"]) <= TOL * abs(t["dJ_du"]), (du, float(t["dJ_du"]))
+        assert abs(dtau - t["dJ_dtau"]) <= TOL * abs(t["dJ_dtau"]), (dtau, float(t["dJ_dtau"]))
+        terr = np.abs(gdir - t["dJ_dir"]) / np.abs(t["dJ_dir"])
+        assert np.all(terr <= TOL), terr
     return steps, window
 
 
