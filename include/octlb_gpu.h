@@ -184,7 +184,9 @@ int octlb_gpu_plan(const octlb_tables* tables, const octlb_params* params, long 
 /* Per-level collide / stream counts and max level (TimeLoop::counters). */
 int octlb_gpu_counters(const octlb_ctx* ctx, int* collide, int* stream, int max_levels);
 int octlb_gpu_max_level(const octlb_ctx* ctx);
-/* Kernel launches one coarse step issues, and lattice updates it performs. */
+/* Kernel launches one coarse step issues (as counted when the last
+ * advance_one was issued; before the first, without shared coupler launches),
+ * and lattice updates it performs. */
 int octlb_gpu_step_stats(const octlb_ctx* ctx, long long* launches, long long* lattice_updates);
 
 #ifdef __cplusplus

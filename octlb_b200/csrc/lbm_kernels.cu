@@ -399,17 +399,16 @@ __global__ void __launch_bounds__(kThreads) k_add_force(const StepArgs a, T* pop
 // lanes keep the item's dependent chain short: the launch is latency-bound
 // (a few thousand items).
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_prolong(const ProlongItem* items, int nitems, const float* coarse_save, float* prev, int half, float* rec_prev,
-          T* fine, long long fine_qs, float scale, float omega, float fscale) {
-  const int w = static_cast<int>((blockIdx.x * kThreads + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (w >= nitems) return;  // whole warps
-  const ProlongItem it = items[w];
+__device__ __forceinline__ void prolong_warp(const ProlongOp& op, int w, int lane) {
+  if (w >= op.n) return;  // whole warps
+  const ProlongItem it = op.items[w];
+  const int half = op.half;
+  float* rec_prev = op.rec_prev;
+  const float scale = op.scale, omega = op.omega;
   const LaneDir d = lane_dir(lane);
   pdl_wait();
-  const float fr = d.act ? coarse_save[static_cast<long long>(it.coarse_save) * kQ + lane] : 0.f;
-  float* pv = prev + static_cast<long long>(it.prev) * 23;
+  const float fr = d.act ? op.coarse_save[static_cast<long long>(it.coarse_save) * kQ + lane] : 0.f;
+  float* pv = op.prev + static_cast<long long>(it.prev) * 23;
   float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f, pf = 0.f;
   if (half) {
     p0 = pv[0]; p1 = pv[1]; p2 = pv[2]; p3 = pv[3];
@@ -457,7 +456,7 @@ k_prolong(const ProlongItem* items, int nitems, const float* coarse_save, float*
     gather_lanes(f, fa);
     f = bgk_lane(d, lane, fa, f, omega);
   }
-  if (d.act) Store<T>::st(fine + lane * fine_qs + it.fine_slot, f, fscale);
+  if (d.act) Store<T>::st(static_cast<T*>(op.fine) + lane * op.fine_qs + it.fine_slot, f, op.fscale);
 }
 
 // Lagrava restriction (level_coupler.cpp:613-654), one warp per item: lane
@@ -467,21 +466,16 @@ k_prolong(const ProlongItem* items, int nitems, const float* coarse_save, float*
 // reference's order and averages with the centre; then lane i writes
 // population i of the coarse target.
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_restrict(const RestrictItem* items, int nitems, const float* fine_save, T* coarse,
-           long long coarse_qs, float scale, float omega, float cscale) {
-  __shared__ float fneq_s[kThreads / 32][kQ][kQ + 1];  // [warp][row][population]
-  const int w = static_cast<int>((blockIdx.x * kThreads + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (w >= nitems) return;  // whole warps
-  const RestrictItem& it = items[w];
+__device__ __forceinline__ void restrict_warp(const RestrictOp& op, int w, int lane, float (*fs)[kQ + 1]) {
+  if (w >= op.n) return;  // whole warps
+  const RestrictItem& it = op.items[w];
+  const float scale = op.scale, omega = op.omega;
   const int nnb = it.nnb;
   const int row = lane == 0 ? it.fine_save : (lane <= nnb ? it.nb_save[lane - 1] : -1);
   pdl_wait();
-  float (*fs)[kQ + 1] = fneq_s[threadIdx.x >> 5];
   Macro m;
   if (row >= 0) {
-    read_macro(fine_save + static_cast<long long>(row) * kQ, m);
+    read_macro(op.fine_save + static_cast<long long>(row) * kQ, m);
 #pragma unroll
     for (int i = 0; i < kQ; ++i) fs[lane][i] = m.fneq[i];
   }
@@ -502,7 +496,33 @@ k_restrict(const RestrictItem* items, int nitems, const float* fine_save, T* coa
     gather_lanes(f, fa);
     f = bgk_lane(d, lane, fa, f, omega);
   }
-  if (d.act) Store<T>::st(coarse + lane * coarse_qs + it.coarse_slot, f, cscale);
+  if (d.act) Store<T>::st(static_cast<T*>(op.coarse) + lane * op.coarse_qs + it.coarse_slot, f, op.cscale);
+}
+
+// One coupler launch: the prolongation's items, then each restriction's, one
+// warp per item, each on its own range of CTAs.  Operations that nothing
+// between them orders (a restriction into level l and the full-time
+// prolongation into level l with disjoint targets; two restrictions) share a
+// launch this way.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_couple(const ProlongOp p, const RestrictOp r0, const RestrictOp r1) {
+  __shared__ float fneq_s[kThreads / 32][kQ][kQ + 1];  // restriction: [warp][row][population]
+  const uint32_t gp = (static_cast<uint32_t>(p.n) * 32 + kThreads - 1) / kThreads;
+  const uint32_t g0 = (static_cast<uint32_t>(r0.n) * 32 + kThreads - 1) / kThreads;
+  const int lane = threadIdx.x & 31;
+  uint32_t b = blockIdx.x;
+  if (b < gp) {
+    prolong_warp<T>(p, static_cast<int>((b * kThreads + threadIdx.x) >> 5), lane);
+    return;
+  }
+  b -= gp;
+  float (*fs)[kQ + 1] = fneq_s[threadIdx.x >> 5];
+  if (b < g0) {
+    restrict_warp<T>(r0, static_cast<int>((b * kThreads + threadIdx.x) >> 5), lane, fs);
+    return;
+  }
+  b -= g0;
+  restrict_warp<T>(r1, static_cast<int>((b * kThreads + threadIdx.x) >> 5), lane, fs);
 }
 
 // Momentum-exchange force (drag_postprocessor.h:67-115) from the buffer the
@@ -752,22 +772,11 @@ cudaError_t launch_add_force(const StepArgs& a, T* pops, const float* force, cud
 
 
 template <typename T>
-cudaError_t launch_prolong(const ProlongItem* items, int n, const float* coarse_save, float* prev,
-                           int half, float* rec_prev, T* fine, long long fine_qs, float scale, float omega,
-                           float fscale, cudaStream_t s) {
-  if (n == 0) return cudaSuccess;
-  const cudaError_t e = launch_chain(k_prolong<T>, dim3(grid_for(static_cast<uint32_t>(n) * 32)), dim3(kThreads), 0, s,
-                                     items, n, coarse_save, prev, half, rec_prev, fine, fine_qs, scale, omega, fscale);
-  return e != cudaSuccess ? e : cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t launch_restrict(const RestrictItem* items, int n, const float* fine_save, T* coarse,
-                            long long coarse_qs, float scale, float omega, float cscale,
-                            cudaStream_t s) {
-  if (n == 0) return cudaSuccess;
-  const cudaError_t e = launch_chain(k_restrict<T>, dim3(grid_for(static_cast<uint32_t>(n) * 32)), dim3(kThreads), 0, s, items, n, fine_save, coarse,
-                                                                             coarse_qs, scale, omega, cscale);
+cudaError_t launch_couple(const ProlongOp& p, const RestrictOp& r0, const RestrictOp& r1, cudaStream_t s) {
+  const uint32_t g = grid_for(static_cast<uint32_t>(p.n) * 32) + grid_for(static_cast<uint32_t>(r0.n) * 32) +
+                     grid_for(static_cast<uint32_t>(r1.n) * 32);
+  if (g == 0) return cudaSuccess;
+  const cudaError_t e = launch_chain(k_couple<T>, dim3(g), dim3(kThreads), 0, s, p, r0, r1);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -815,10 +824,8 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
   template cudaError_t launch_step_near<T>(const StepArgs&, const NearTables&, cudaStream_t);       \
   template cudaError_t launch_add_force<T>(const StepArgs&, T*, const float*, cudaStream_t);         \
   template cudaError_t launch_step_map<T>(const StepArgs&, const NearTables&, bool, bool, int, bool, cudaStream_t); \
-  template cudaError_t launch_prolong<T>(const ProlongItem*, int, const float*, float*, int, float*, T*, \
-                                         long long, float, float, float, cudaStream_t);            \
-  template cudaError_t launch_restrict<T>(const RestrictItem*, int, const float*, T*, long long,   \
-                                          float, float, float, cudaStream_t);                      \
+  template cudaError_t launch_couple<T>(const ProlongOp&, const RestrictOp&, const RestrictOp&,    \
+                                        cudaStream_t);                                             \
   template cudaError_t launch_drag<T>(const StepArgs&, bool, const DragItem*, int, double*,        \
                                       cudaStream_t);                                               \
   template cudaError_t launch_audit<T>(const StepArgs&, double*, double*, cudaStream_t);           \

@@ -12,6 +12,7 @@
 #include <memory>
 #include <set>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 #include "octlb_internal.h"
@@ -21,11 +22,7 @@ namespace octlb_gpu {
 
 template <typename T> cudaError_t launch_step(const StepArgs&, bool, bool, bool, cudaStream_t);
 template <typename T>
-cudaError_t launch_prolong(const ProlongItem*, int, const float*, float*, int, float*, T*, long long, float,
-                           float, float, cudaStream_t);
-template <typename T>
-cudaError_t launch_restrict(const RestrictItem*, int, const float*, T*, long long, float, float,
-                            float, cudaStream_t);
+cudaError_t launch_couple(const ProlongOp&, const RestrictOp&, const RestrictOp&, cudaStream_t);
 template <typename T>
 cudaError_t launch_drag(const StepArgs&, bool, const DragItem*, int, double*, cudaStream_t);
 cudaError_t launch_drag_total(const double*, int, double*, double*, cudaStream_t);
@@ -111,6 +108,10 @@ struct Level {
   uint32_t n_bb = 0;
   // coupler: this level as coarse (prolong) and as fine (restrict)
   DevBuf prolong_items, prev, restrict_items;
+  // The restriction into this level (from level + 1) may share a launch with
+  // the full-time prolongation into it (from level - 1): their target cells
+  // are disjoint.
+  bool fuse_restrict = false;
   int n_prolong = 0, n_restrict = 0;
   // drag
   DevBuf drag_items;
@@ -202,6 +203,13 @@ struct octlb_ctx {
   std::vector<uint8_t> kinds;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // Restrictions not launched yet: each shares the next coupler launch unless
+  // a step comes first (then they are launched alone, two per launch).
+  struct PendingRestrict {
+    RestrictOp op;
+    int level;  // the coarse level written
+  };
+  std::vector<PendingRestrict> pending_restrict;
   // The momentum-exchange force runs on a forked stream inside advance_one
   // (it only reads the last finest step's input) and joins at its end.
   cudaStream_t side = nullptr;
@@ -212,6 +220,7 @@ struct octlb_ctx {
   long long force_steps = 0;
   std::vector<int> counters_collide, counters_stream;
   long long launches_per_step = 0, lups_per_step = 0;
+  long long launch_count = 0;       // kernels issued by the advance_one being built
   int step_kernel = 0;              // OCTLB_STEP_KERNEL: 0 pair (default), 1 bulk, 2 plain
   bool map_global = true;           // slot map read through L1 (OCTLB_MAP_SMEM=1: staged in shared memory)
   int map_cells = 0;                // cells per thread of the slot-map step (OCTLB_MAP_CELLS 1 or 2;
@@ -303,16 +312,34 @@ void host_macro(const double* f, float out[23]) {
 template <typename T>
 int do_advance_level(octlb_ctx* ctx, int l);
 
+// Launches the pending restrictions (two per launch).
+template <typename T>
+int flush_restricts(octlb_ctx* ctx) {
+  auto& P = ctx->pending_restrict;
+  const ProlongOp none_p{};
+  const RestrictOp none_r{};
+  for (size_t k = 0; k < P.size(); k += 2) {
+    CK(launch_couple<T>(none_p, P[k].op, k + 1 < P.size() ? P[k + 1].op : none_r, ctx->stream));
+    ++ctx->launch_count;
+  }
+  P.clear();
+  return OCTLB_OK;
+}
+
 template <typename T>
 int launch_level_step(octlb_ctx* ctx, Level& L) {
   if (L.nblk == 0) return OCTLB_OK;
+  { const int rc = flush_restricts<T>(ctx); if (rc) return rc; }  // the step reads what they write
   // Body force on the stored post-collision state (the reference's apply()
   // hook after collide, time_loop.h:207-211).  The boundary fills and the
   // same-level exchange that follow there need no launch: the step reads
   // neighbour cores through the slot map and fill targets from their
   // sources.
   T* cur = static_cast<T*>(cur_buf(L));
-  if (L.has_force) CK(launch_add_force<T>(L.args, cur, L.body_force.as<float>(), ctx->stream));
+  if (L.has_force) {
+    CK(launch_add_force<T>(L.args, cur, L.body_force.as<float>(), ctx->stream));
+    ++ctx->launch_count;
+  }
 
   StepArgs a = L.args;
   a.src = cur;
@@ -349,6 +376,7 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     CK(launch_drag<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.drag_items.as<DragItem>(), L.n_drag,
                       ctx->drag_partial.as<double>() + 3 * L.drag_off, ctx->side));
     ctx->side_busy = true;
+    ++ctx->launch_count;
   }
   if (L.use_bulk) {
     CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
@@ -361,7 +389,9 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     CK(launch_step<T>(a, ctx->periodic != 0, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags,
                       ctx->stream));
     CK(launch_step_near<T>(a, L.near, ctx->stream));
+    if (L.near.n > 0) ++ctx->launch_count;
   }
+  if (L.args.nitems > 0) ++ctx->launch_count;  // the step
   ++L.substep;
   L.cur = 1 - L.cur;
   if (rec) L.rec_cur = next_cur;
@@ -384,20 +414,51 @@ int do_advance_level(octlb_ctx* ctx, int l) {
     rec_prev = ctx->adj->recs[ctx->adj->last_rec[l]].prev.as<float>();
   // apply_half_time(l) -> advance(l+1) -> apply_full_time(l) -> advance(l+1)
   // -> restrict(l+1)  (time_loop.h:228-239)
+  // A restriction is not launched where the recursion reaches it: it shares
+  // the next coupler launch (the parent's full-time prolongation, or another
+  // restriction), and is launched before the next step otherwise -- nothing
+  // in between reads what it writes.
+  auto& pend = ctx->pending_restrict;
   for (int phase = 0; phase < 2; ++phase) {
     if (L.n_prolong > 0) {
-      CK(launch_prolong<T>(L.prolong_items.as<ProlongItem>(), L.n_prolong, save_ptr(L),
-                           L.prev.as<float>(), phase == 0 ? 1 : 0, phase == 0 ? rec_prev : nullptr,
-                           static_cast<T*>(cur_buf(F)), F.nslots, ctx->prolong_scale,
-                           static_cast<float>(ctx->omega), F.scale, ctx->stream));
+      ProlongOp p{};
+      p.items = L.prolong_items.as<ProlongItem>();
+      p.n = L.n_prolong;
+      p.half = phase == 0 ? 1 : 0;
+      p.coarse_save = save_ptr(L);
+      p.prev = L.prev.as<float>();
+      p.rec_prev = phase == 0 ? rec_prev : nullptr;
+      p.fine = cur_buf(F);
+      p.fine_qs = F.nslots;
+      p.scale = ctx->prolong_scale;
+      p.omega = static_cast<float>(ctx->omega);
+      p.fscale = F.scale;
+      bool share = pend.size() <= 2;
+      for (const auto& q : pend)
+        if (q.level == l + 1 && !F.fuse_restrict) share = false;
+      if (!share) { rc = flush_restricts<T>(ctx); if (rc) return rc; }
+      RestrictOp r0{}, r1{};
+      if (!pend.empty()) r0 = pend[0].op;
+      if (pend.size() > 1) r1 = pend[1].op;
+      pend.clear();
+      CK(launch_couple<T>(p, r0, r1, ctx->stream));
+      ++ctx->launch_count;
     }
     rc = do_advance_level<T>(ctx, l + 1);
     if (rc) return rc;
   }
   if (F.n_restrict > 0) {
-    CK(launch_restrict<T>(F.restrict_items.as<RestrictItem>(), F.n_restrict, save_ptr(F),
-                          static_cast<T*>(cur_buf(L)), L.nslots, ctx->restrict_scale,
-                          static_cast<float>(ctx->omega), L.scale, ctx->stream));
+    if (pend.size() >= 2) { rc = flush_restricts<T>(ctx); if (rc) return rc; }
+    RestrictOp r{};
+    r.items = F.restrict_items.as<RestrictItem>();
+    r.n = F.n_restrict;
+    r.fine_save = save_ptr(F);
+    r.coarse = cur_buf(L);
+    r.coarse_qs = L.nslots;
+    r.scale = ctx->restrict_scale;
+    r.omega = static_cast<float>(ctx->omega);
+    r.cscale = L.scale;
+    pend.push_back({r, l});
   }
   return OCTLB_OK;
 }
@@ -1153,6 +1214,13 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     CK(upload(L.fill_of, fill_of_h));
     CK(upload(L.prolong_items, prolong[l]));
     CK(upload(L.restrict_items, restrict_items[l]));
+    if (l >= 1 && l + 1 < nlev) {
+      std::unordered_set<long long> ptarget;
+      for (const ProlongItem& it : prolong[l - 1]) ptarget.insert(it.fine_slot);
+      L.fuse_restrict = true;
+      for (const RestrictItem& it : restrict_items[l + 1])
+        if (ptarget.count(it.coarse_slot)) L.fuse_restrict = false;
+    }
     L.n_prolong = static_cast<int>(prolong[l].size());
     L.n_restrict = static_cast<int>(restrict_items[l].size());
     CK(upload(L.drag_items, drag));
@@ -1289,7 +1357,10 @@ int check_device_error(octlb_ctx* ctx) {
 template <typename T>
 int advance_one_launches(octlb_ctx* ctx) {
   for (auto& L : ctx->levels) L.substep = 0;
+  ctx->launch_count = 0;
   int rc = do_advance_level<T>(ctx, 0);
+  if (rc) return rc;
+  rc = flush_restricts<T>(ctx);
   if (rc) return rc;
   if (ctx->side_busy) {
     CK(launch_drag_total(ctx->drag_partial.as<double>(), ctx->drag_parts, ctx->force.as<double>(),
@@ -1297,7 +1368,9 @@ int advance_one_launches(octlb_ctx* ctx) {
     CK(cudaEventRecord(ctx->ev_join, ctx->side));
     CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
     ctx->side_busy = false;
+    ++ctx->launch_count;
   }
+  if (!(ctx->adj && ctx->adj->recording)) ctx->launches_per_step = ctx->launch_count;
   return OCTLB_OK;
 }
 
@@ -2051,7 +2124,12 @@ unsigned octlb_gpu_debug_fastdiv(unsigned d, unsigned n) { return FastDiv(d).div
 
 int octlb_gpu_step_stats(const octlb_ctx* ctx, long long* launches, long long* lups) {
   if (!ctx) return OCTLB_EINVAL;
-  long long total = 0;
+  if (ctx->launches_per_step > 0) {  // counted while the last advance_one was issued
+    if (launches) *launches = ctx->launches_per_step;
+    if (lups) *lups = ctx->lups_per_step;
+    return OCTLB_OK;
+  }
+  long long total = 0;  // before any advance: the unfused count
   // Per level advance: ghost fill (if any ops) + step (+ drag + partial sum);
   // per coarse level: two prolongations, per fine level: one restriction.
   std::vector<long long> per(ctx->levels.size(), 0);

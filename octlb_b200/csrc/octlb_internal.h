@@ -100,6 +100,26 @@ struct RestrictItem {
   int coarse_kind;
   int pad;
 };
+// Operands of one coupler launch (k_couple): a prolongation and up to two
+// restrictions, each on its own range of CTAs (n = 0: absent).
+struct ProlongOp {
+  const ProlongItem* items;
+  int n, half;
+  const float* coarse_save;
+  float* prev;
+  float* rec_prev;          // the adjoint's record of the prev rows read (half time), or null
+  void* fine;
+  long long fine_qs;
+  float scale, omega, fscale;
+};
+struct RestrictOp {
+  const RestrictItem* items;
+  int n;
+  const float* fine_save;
+  void* coarse;
+  long long coarse_qs;
+  float scale, omega, cscale;
+};
 // MEM drag cell: kBulk core cell with at least one obstacle link; bit i of
 // mask set when x + c_i is an in-block solid / Bouzidi obstacle cell
 // (drag_postprocessor.h:86-110).
