@@ -276,12 +276,13 @@ def forest_measurements(ob, cases, torch, peak):
     lat.close()
     lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP32, stream_mode=ob.STREAM_LINKS, drag=True,
                         init_pops=init)
-    lat.adjoint(steps, window, 16)  # first call captures the sweep's graphs
-    lat.close()
-    lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP32, stream_mode=ob.STREAM_LINKS, drag=True,
-                        init_pops=init)
-    t0 = time.perf_counter()
+    # the first call (from the initial state) gives the checked gradients and
+    # captures the sweep's graphs; the second, from the forward's final
+    # state, reuses them and is timed (the same work)
     J, du, dtau, gF = lat.adjoint(steps, window, 16)
+    lat.synchronize()
+    t0 = time.perf_counter()
+    lat.adjoint(steps, window, 16)
     t_adj = time.perf_counter() - t0
     lat.close()
     d = directions(mesh)
@@ -294,6 +295,13 @@ def forest_measurements(ob, cases, torch, peak):
                                "tau": float(abs(dtau - g["dJ_dtau"]) / abs(g["dJ_dtau"])),
                                "body_force_dirs_max": float(np.max(np.abs(gdir - g["dJ_dir"]) / np.abs(g["dJ_dir"])))},
     }
+    tpath = os.path.join(here, "tests", "golden", "adjoint_c5_tlm.npz")
+    if os.path.exists(tpath):  # exact FP64 derivatives of the reference (tangent-linear)
+        t = np.load(tpath)
+        out["adjoint_channel_128x32x32"]["rel_err_vs_fp64_tangent_linear"] = {
+            "u_max": float(abs(du - t["dJ_du"]) / abs(t["dJ_du"])),
+            "tau": float(abs(dtau - t["dJ_dtau"]) / abs(t["dJ_dtau"])),
+            "body_force_dirs_max": float(np.max(np.abs(gdir - t["dJ_dir"]) / np.abs(t["dJ_dir"])))}
     return out
 
 

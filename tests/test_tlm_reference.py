@@ -24,14 +24,17 @@ def golden(name):
 @pytest.mark.parametrize("tlm_name,fd_name", [("adjoint_c5_short_tlm.npz", "adjoint_c5_short.npz"),
                                               ("adjoint_c5_tlm.npz", "adjoint_c5.npz")])
 def test_tlm_goldens_agree_with_finite_differences(tlm_name, fd_name):
-    """Same objective value; derivatives within the central differences'
-    O(h^2) truncation (h = 1e-4 relative)."""
+    """Same objective value; u_max and tau derivatives within the central
+    differences' O(h^2) truncation (h = 1e-4 relative).  The body-force
+    differences are taken over a 1e-6 perturbation, so their rounding floor is
+    absolute (~1e-10 on the 1,000-call horizon, 4e-5 relative for its smallest
+    component): the bound is relative to the largest component."""
     t, f = golden(tlm_name), golden(fd_name)
     assert int(t["steps"]) == int(f["steps"]) and int(t["window"]) == int(f["window"])
     assert abs(t["J"] - f["J"]) <= 1e-12 * abs(f["J"])
     assert abs(t["dJ_du"] - f["dJ_du"]) <= 1e-6 * abs(f["dJ_du"])
     assert abs(t["dJ_dtau"] - f["dJ_dtau"]) <= 1e-5 * abs(f["dJ_dtau"])
-    assert np.all(np.abs(t["dJ_dir"] - f["dJ_dir"]) <= 1e-5 * np.abs(f["dJ_dir"]))
+    assert np.all(np.abs(t["dJ_dir"] - f["dJ_dir"]) <= 1e-5 * np.max(np.abs(f["dJ_dir"])))
 
 
 def test_tlm_library_matches_central_differences(ref, tlm):
