@@ -155,10 +155,16 @@ struct AdjointState {
     DevBuf lam_save, lam_m, lam_prev, gF;
   };
   std::vector<Lv> lv;
-  std::vector<StepRecord> recs;
-  std::vector<int> next_same;       // next record of the same level in the pool, or -1
-  std::vector<int> first_rec;       // first record of each level in the pool, or -1
+  // Two record sets, one per segment parity: the recomputation of the next
+  // segment (set (c - 1) % 2) runs on rstream beside the reverse of the
+  // current one (set c % 2) on the context's stream.
+  std::vector<StepRecord> recs;     // [2][set_size]
+  size_t set_size = 0;
+  std::vector<int> next_same;       // next record of the same level in the same set, or -1
+  std::vector<int> first_rec;       // first record of each level in set 0, or -1 (set 1: + set_size)
   size_t nrec = 0;
+  cudaStream_t rstream = nullptr;
+  cudaEvent_t ev_fwd = nullptr, ev_rec[2] = {nullptr, nullptr}, ev_rev[2] = {nullptr, nullptr};
   bool recording = false;
   int last_rec[32] = {};
   DevBuf g;                         // parameter-gradient accumulators (FP64)
@@ -185,7 +191,13 @@ struct AdjointState {
   AdjointState() = default;
   AdjointState(const AdjointState&) = delete;
   AdjointState& operator=(const AdjointState&) = delete;
-  ~AdjointState() { clear_graphs(); }
+  ~AdjointState() {
+    if (rstream) cudaStreamSynchronize(rstream);
+    clear_graphs();
+    for (cudaEvent_t e : {ev_fwd, ev_rec[0], ev_rec[1], ev_rev[0], ev_rev[1]})
+      if (e) cudaEventDestroy(e);
+    if (rstream) cudaStreamDestroy(rstream);
+  }
 };
 
 }  // namespace
@@ -1527,19 +1539,24 @@ int prealloc_records(octlb_ctx* ctx, int steps) {
   std::vector<int> seq;
   record_levels(ctx, 0, seq);
   const size_t need = seq.size() * static_cast<size_t>(steps);
-  if (A.recs.size() < need) A.recs.resize(need);
+  if (A.set_size != need) {  // the two sets' layout: set 1 = set 0 shifted by need
+    A.recs.clear();
+    A.recs.resize(2 * need);
+    A.set_size = need;
+  }
   A.next_same.assign(A.recs.size(), -1);
   A.first_rec.assign(ctx->levels.size(), -1);
-  {
+  for (int set = 0; set < 2; ++set) {
     std::vector<int> last(ctx->levels.size(), -1);
     for (size_t r = 0; r < need; ++r) {
       const int l = seq[r % seq.size()];
-      if (last[l] >= 0) A.next_same[last[l]] = static_cast<int>(r);
-      else A.first_rec[l] = static_cast<int>(r);
-      last[l] = static_cast<int>(r);
+      const int abs_r = static_cast<int>(set * need + r);
+      if (last[l] >= 0) A.next_same[last[l]] = abs_r;
+      else if (set == 0) A.first_rec[l] = abs_r;
+      last[l] = abs_r;
     }
   }
-  for (size_t r = 0; r < need; ++r) {
+  for (size_t r = 0; r < 2 * need; ++r) {
     StepRecord& R = A.recs[r];
     const int l = seq[r % seq.size()];
     if (R.level == l) continue;
@@ -1559,12 +1576,19 @@ uint64_t lam_mask(const AdjointState& A) {
   return m;
 }
 
-// Runs body() on the stream, through a CUDA graph captured on first use for
-// `key` when graphs are enabled; set_out applies the captured run's final
-// host-side parity to the context on replay.
+// Runs body() on stream s (the context's stream is pointed at s meanwhile),
+// through a CUDA graph captured on first use for `key` when graphs are
+// enabled; set_out applies the captured run's final host-side parity to the
+// context on replay.
 template <typename Body, typename GetMask, typename SetMask>
 int run_captured(octlb_ctx* ctx, const std::array<long long, 4>& key, Body body, GetMask get_mask,
-                 SetMask set_mask) {
+                 SetMask set_mask, cudaStream_t s) {
+  struct StreamSwap {
+    octlb_ctx* c;
+    cudaStream_t keep;
+    ~StreamSwap() { c->stream = keep; }
+  } swap_back{ctx, ctx->stream};
+  ctx->stream = s;
   AdjointState& A = *ctx->adj;
   if (!ctx->use_graphs) return body();
   auto it = A.graphs.find(key);
@@ -1703,51 +1727,82 @@ int adjoint_impl(octlb_ctx* ctx, const octlb_adj_params* p, double* objective, d
   auto set_lam = [&](uint64_t m) {
     for (size_t l = 0; l < nl; ++l) A.lv[l].cur = (m >> l) & 1;
   };
-  for (int c = nck - 1; c >= 0; --c) {
+  // Segments from the last: segment c's recomputation fills record set c % 2
+  // on rstream; its reverse reads that set on the context's stream while
+  // segment c - 1 is recomputed into the other set.  Events order each
+  // reverse after its recomputation and each recomputation after the reverse
+  // that last read its set.
+  if (!A.rstream) {
+    CK(cudaStreamCreateWithFlags(&A.rstream, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&A.ev_fwd, &A.ev_rec[0], &A.ev_rec[1], &A.ev_rev[0], &A.ev_rev[1]})
+      CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  }
+  CK(cudaEventRecord(A.ev_fwd, ctx->stream));
+  CK(cudaStreamWaitEvent(A.rstream, A.ev_fwd, 0));
+  bool rev_used[2] = {false, false};
+  auto recompute = [&](int c) -> int {
+    const int set = c & 1;
+    const size_t base = static_cast<size_t>(set) * A.set_size;
     const int k0 = c * K, k1 = std::min(NT, k0 + K);
-    const int nwin = std::max(0, k1 - std::max(k0, NT - W));
+    if (rev_used[set]) CK(cudaStreamWaitEvent(A.rstream, A.ev_rev[set], 0));
     // the segment's checkpoint goes straight into each level's first record
     for (size_t l = 0; l < nl; ++l) {
       Level& L = ctx->levels[l];
       if (L.nblk == 0) continue;
       AdjointState::Checkpoint& ck = A.ck[c];
       L.cur = ck.cur[l];
-      L.rec_cur = A.recs[A.first_rec[l]].snap.p;
-      CK(cudaMemcpyAsync(L.rec_cur, ck.buf[l].p, ck.buf[l].bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+      L.rec_cur = A.recs[base + A.first_rec[l]].snap.p;
+      CK(cudaMemcpyAsync(L.rec_cur, ck.buf[l].p, ck.buf[l].bytes, cudaMemcpyDeviceToDevice, A.rstream));
       if (L.n_prolong > 0)
-        CK(cudaMemcpyAsync(L.prev.p, ck.prev[l].p, ck.prev[l].bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(L.prev.p, ck.prev[l].p, ck.prev[l].bytes, cudaMemcpyDeviceToDevice, A.rstream));
     }
-    int rc = OCTLB_OK;
     // recompute the segment, recording every level step
-    rc = run_captured(
-        ctx, {0, static_cast<long long>(parity_mask(ctx)), k1 - k0, 0},
+    const int rc = run_captured(
+        ctx, {2 * set, static_cast<long long>(parity_mask(ctx)), k1 - k0, 0},
         [&]() {
           A.recording = true;
-          A.nrec = 0;
+          A.nrec = base;
           for (int k = k0; k < k1; ++k) {
             const int r = advance_one_launches<T>(ctx);
             if (r) { A.recording = false; return r; }
           }
           A.recording = false;
-          if (A.nrec != per * static_cast<size_t>(k1 - k0))
+          if (A.nrec != base + per * static_cast<size_t>(k1 - k0))
             return fail(ctx, OCTLB_ESTATE, "adjoint: record count mismatch");
           return static_cast<int>(OCTLB_OK);
         },
-        [&]() { return parity_mask(ctx); }, set_parity);
+        [&]() { return parity_mask(ctx); }, set_parity, A.rstream);
     for (auto& L : ctx->levels) L.rec_cur = L.rec_save = nullptr;
     if (rc) return rc;
-    A.nrec = per * static_cast<size_t>(k1 - k0);
-    // reverse through it
-    rc = run_captured(
-        ctx, {1, static_cast<long long>(lam_mask(A)), k1 - k0, nwin},
+    CK(cudaEventRecord(A.ev_rec[set], A.rstream));
+    return OCTLB_OK;
+  };
+  auto reverse = [&](int c) -> int {
+    const int set = c & 1;
+    const size_t base = static_cast<size_t>(set) * A.set_size;
+    const int k0 = c * K, k1 = std::min(NT, k0 + K);
+    const int nwin = std::max(0, k1 - std::max(k0, NT - W));
+    CK(cudaStreamWaitEvent(ctx->stream, A.ev_rec[set], 0));
+    A.nrec = base + per * static_cast<size_t>(k1 - k0);
+    const int rc = run_captured(
+        ctx, {2 * set + 1, static_cast<long long>(lam_mask(A)), k1 - k0, nwin},
         [&]() {
           for (int k = k1 - 1; k >= k0; --k) {
-            const int r = adj_level(ctx, 0, per * static_cast<size_t>(k - k0), k >= NT - W ? coef : 0.f);
+            const int r = adj_level(ctx, 0, base + per * static_cast<size_t>(k - k0), k >= NT - W ? coef : 0.f);
             if (r) return r;
           }
           return static_cast<int>(OCTLB_OK);
         },
-        [&]() { return lam_mask(A); }, set_lam);
+        [&]() { return lam_mask(A); }, set_lam, ctx->stream);
+    if (rc) return rc;
+    CK(cudaEventRecord(A.ev_rev[set], ctx->stream));
+    rev_used[set] = true;
+    return OCTLB_OK;
+  };
+  { const int rc = recompute(nck - 1); if (rc) return rc; }
+  for (int c = nck - 1; c >= 0; --c) {
+    if (c >= 1) { const int rc = recompute(c - 1); if (rc) return rc; }
+    const int rc = reverse(c);
     if (rc) return rc;
   }
 
