@@ -124,7 +124,10 @@ int octlb_gpu_set_body_force(octlb_ctx* ctx, const double* force);
  * steps.  Runs the forward from the context's current state with a
  * checkpoint every `checkpoint_interval` coarse steps (0: ceil(sqrt(n))),
  * then recomputes each segment from its checkpoint and runs the hand-written
- * adjoint kernels through it in reverse.  Outputs J, grad[0] = dJ/du_max
+ * adjoint kernels through it in reverse (a segment's recomputation on a
+ * stream of its own beside the next-later segment's reverse).  Device memory
+ * it allocates and keeps with the context: ceil(n / interval) + 1 states and
+ * 2 x interval coarse steps of step inputs.  Outputs J, grad[0] = dJ/du_max
  * (u_max = the largest moving tree-boundary wall speed; all wall velocities
  * scale with it), grad[1] = dJ/dtau (tau = 1/omega, including the coupler
  * scales), and, when grad_force is not NULL, dJ/dF for the body force of
