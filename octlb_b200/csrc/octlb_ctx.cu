@@ -71,6 +71,10 @@ struct DevBuf {
     if (b == 0) return cudaSuccess;
     cudaError_t e = cudaMalloc(&p, b);
     if (e == cudaSuccess) e = cudaMemset(p, 0, b);
+    // The zero fill runs on the legacy default stream, which the context's
+    // non-blocking streams do not wait for: it must land before any of them
+    // touches the buffer.
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
     return e;
   }
   template <typename U> U* as() const { return static_cast<U*>(p); }
@@ -80,7 +84,13 @@ template <typename U>
 cudaError_t upload(DevBuf& d, const std::vector<U>& h) {
   cudaError_t e = d.alloc(h.size() * sizeof(U));
   if (e != cudaSuccess || h.empty() || g_dry_run) return e;
-  return cudaMemcpy(d.p, h.data(), h.size() * sizeof(U), cudaMemcpyHostToDevice);
+  e = cudaMemcpy(d.p, h.data(), h.size() * sizeof(U), cudaMemcpyHostToDevice);
+  // From pageable memory cudaMemcpy may return before its last DMA chunk has
+  // landed (on the legacy stream, which the context's non-blocking streams do
+  // not wait for); a kernel on those streams would read the buffer's tail
+  // early.
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+  return e;
 }
 
 struct PlanPoint {  // CouplingPoint (level_coupler.h:18-30)

@@ -215,3 +215,35 @@ def test_plan_dry_run_all_configurations(ob, name):
         assert sum(d["prolong"] for d in pl) > 0 and sum(d["restrict"] for d in pl) > 0
     if name in ("c3", "cyl"):
         assert sum(d["drag"] for d in pl) > 0 and sum(d["links"] for d in pl) > 0
+
+
+@pytest.mark.parametrize("name", ["amr_cavity", "cylinder"])
+def test_coupler_items_are_the_reference_plan(ob, ref, name):
+    """The Lagrava plan (level_coupler.cpp:70-118, tested by the reference in
+    test_lagrava_coupler.cpp:126-192): every coupling point's indices lie
+    inside its blocks, the pairs are unique, and the GPU's prolongation /
+    restriction items are exactly the plan's distinct fine / coarse targets
+    per level (a later point writing the same cell wins)."""
+    from octlb_b200 import cases
+    from oracle import oracle
+    if name == "amr_cavity":
+        mesh, init, info = cases.cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=8)
+        mode = ob.STREAM_ROTATE
+    else:
+        mesh, init, info = cases.cylinder_forest(length=128, height=32, n=8, diameter=8.0, center=(32.0, 16.0),
+                                                 levels=2)
+        mode = ob.STREAM_LINKS
+    sim = oracle.Sim(ref, mesh, info["omega"], init, link_mode=mode == ob.STREAM_LINKS)
+    plan = sim.plan()
+    n = mesh.n
+    assert len(plan) > 0
+    assert np.all((plan[:, [1, 2, 3, 5, 6, 7]] >= 0) & (plan[:, [1, 2, 3, 5, 6, 7]] < n))
+    assert np.all(mesh.levels[plan[:, 0]] == plan[:, 8]) and np.all(mesh.levels[plan[:, 4]] == plan[:, 9])
+    assert np.all(plan[:, 9] == plan[:, 8] + 1)
+    assert len({tuple(r) for r in plan[:, :8]}) == len(plan)
+    stats = ob.plan(mesh, info["omega"], stream_mode=mode)
+    for l, st in enumerate(stats):
+        fine_targets = {tuple(r) for r in plan[plan[:, 8] == l][:, 4:8]}
+        coarse_targets = {tuple(r) for r in plan[plan[:, 9] == l][:, 0:4]}
+        assert st["prolong"] == len(fine_targets), (l, st, len(fine_targets))
+        assert st["restrict"] == len(coarse_targets), (l, st, len(coarse_targets))

@@ -339,3 +339,42 @@ def test_adjoint_and_body_force_argument_checks(ob):
     with pytest.raises(ValueError):
         lat.set_body_force(np.zeros(5))
     lat.close()
+
+
+@pytest.mark.parametrize("prec,tol", [("fp32", TOL32), ("fp16", TOL16)])
+def test_periodic_three_level_forest_matches_reference(ob, ref, prec, tol):
+    """A fully periodic forest with interior hanging faces on two nested
+    levels (32^3 base cells at level 2, the central half refined to level 3
+    and its central quarter to level 4), started from a uniform moving state:
+    fields against the reference TimeLoop, and the collide counters in its
+    1:2:4 ratio (test_time_loop_levels.cpp:66-149).  (The reference does not
+    keep this state uniform: the coarse blocks' ghost cells toward a finer
+    neighbour are never filled and keep their initial rest values.)"""
+    from octlb_b200 import C, Forest, Mesh
+    f = Forest((1, 1, 1), (1, 1, 1), (0, 0, 0, 1, 1, 1)).refine_uniform(2)
+    f.refine_box((0.25, 0.25, 0.25, 0.75, 0.75, 0.75), 3)
+    f.refine_box((0.375, 0.375, 0.375, 0.625, 0.625, 0.625), 4)
+    f.balance().build()
+    n = 8
+    mesh = Mesh.from_forest(f, n)
+    assert sorted(set(mesh.levels.tolist())) == [2, 3, 4]
+    rho0, u0 = 1.02, np.array([0.03, -0.02, 0.01])
+    Cf = C.astype(np.float64)
+    w = np.where(np.abs(Cf).sum(1) == 0, 1 / 3, np.where(np.abs(Cf).sum(1) == 1, 1 / 18, 1 / 36))
+    cu = Cf @ u0
+    feq = w * (rho0 * (1 + 3 * cu + 4.5 * cu * cu - 1.5 * u0 @ u0) - 1)
+    init = np.broadcast_to(feq, (mesh.n_blocks, n, n, n, 19)).copy()
+    omega, steps = 1.0 / 0.6, 3
+    lat = ob.GpuLattice(mesh, omega, precision=ob.FP32 if prec == "fp32" else ob.FP16_SHIFTED, init_pops=init)
+    sim = oracle.Sim(ref, mesh, omega, init)
+    lat.advance(steps)
+    sim.advance(steps)
+    rho_g, u_g = lat.get_fields()
+    c, s = lat.counters()
+    lat.close()
+    rho_r, u_r = fields_of(sim.core())
+    cr, sr, _ = sim.counters()
+    assert rel(rho_g, rho_r) <= tol
+    assert rel(u_g, u_r) <= tol
+    assert c == cr and s == sr
+    assert c[2] == steps * 4 and c[3] == 2 * c[2] and c[4] == 4 * c[2]
