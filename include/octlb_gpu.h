@@ -119,6 +119,25 @@ int octlb_gpu_synchronize(octlb_ctx* ctx);
  * adjoint's per-cell control). */
 int octlb_gpu_set_body_force(octlb_ctx* ctx, const double* force);
 
+/* ConstRhoBGK on (1) or off (0): the TimeLoop constructor argument
+ * use_const_rho_bgk with ConstRhoStatsScope::kFluidAndBoundary
+ * (time_loop.h:47-54; collide block_lattice.cpp:441-455 and
+ * block_lattice.h:134-151; statistics time_loop.h:201-222).  Every kBulk
+ * cell collides with ratio_rho = 1 + (1 - average_rho) / rho, and after each
+ * step average_rho becomes the mean of rho + (1 - average_rho) over the kBulk
+ * cells of that collide (the reference starts at 1).  Before the first
+ * advance only (OCTLB_ESTATE after it), on single-level meshes (OCTLB_EINVAL
+ * otherwise: the stored state is one collide ahead of the reference's, so a
+ * coarse level would need the average of finest steps that have not run).
+ * The adjoint refuses a ConstRhoBGK context.  get_fields returns the
+ * reference's post-stream rho (the stored post-collision state minus the
+ * 1 - average_rho the collide added to each kBulk cell; u is unchanged). */
+int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on);
+
+/* TimeLoop::average_rho() (time_loop.h:87-88): the average density the next
+ * ConstRhoBGK collide uses; 1 without ConstRhoBGK.  Synchronises the stream. */
+int octlb_gpu_average_rho(octlb_ctx* ctx, double* out);
+
 /* Discrete adjoint (reverse mode) of n coarse steps.  Objective J = the
  * `component` of octlb_gpu_force averaged over the last `window` coarse
  * steps.  Runs the forward from the context's current state with a

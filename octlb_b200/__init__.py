@@ -303,6 +303,17 @@ class GpuLattice:
             raise ValueError("body force must hold n_blocks * n^3 * 3 values")
         self._check(self._L.octlb_gpu_set_body_force(self._h, capi.ptr(f, ctypes.c_double)))
 
+    def set_const_rho(self, on=True):
+        """ConstRhoBGK (TimeLoop's use_const_rho_bgk): before the first
+        advance, on a single-level mesh."""
+        self._check(self._L.octlb_gpu_set_const_rho(self._h, 1 if on else 0))
+
+    def average_rho(self):
+        """TimeLoop::average_rho(): the density the next ConstRhoBGK collide uses."""
+        out = np.zeros(1)
+        self._check(self._L.octlb_gpu_average_rho(self._h, capi.ptr(out, ctypes.c_double)))
+        return float(out[0])
+
     def adjoint(self, coarse_steps, window, checkpoint_interval=0, component=0, force_grad=True):
         """Run coarse_steps forward and the adjoint sweep back (octlb_gpu_adjoint).
         Returns (J, dJ/du_max, dJ/dtau, dJ/dF or None) with J = mean force

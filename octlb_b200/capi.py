@@ -84,6 +84,8 @@ def lib():
         "octlb_gpu_synchronize": (ctypes.c_int, [P]),
         "octlb_gpu_set_populations": (ctypes.c_int, [P, F64P]),
         "octlb_gpu_set_body_force": (ctypes.c_int, [P, F64P]),
+        "octlb_gpu_set_const_rho": (ctypes.c_int, [P, ctypes.c_int]),
+        "octlb_gpu_average_rho": (ctypes.c_int, [P, F64P]),
         "octlb_gpu_adjoint": (ctypes.c_int, [P, ctypes.POINTER(AdjParams), F64P, F64P, F64P]),
         "octlb_gpu_get_populations": (ctypes.c_int, [P, F64P]),
         "octlb_gpu_get_fields": (ctypes.c_int, [P, F64P, F64P]),

@@ -143,6 +143,34 @@ __device__ __forceinline__ void bgk(float (&f)[kQ], float omega, float s = 1.0f,
   }
 }
 
+// ConstRhoBGK (OpenLB collision::ConstRhoBGK as block_lattice.h:134-151
+// restates it, unit scale):
+//   f_i <- ratio (feq_i + w_i) - w_i + (1 - omega)(f_i - feq_i),
+//   ratio = 1 + dr / rho,  dr = 1 - average_rho (ratio = 1 for rho <= 1e-12).
+// With feq_i + w_i = w_i rho P_i, P_i = 1 + 3 c.u + 4.5 (c.u)^2 - 1.5 |u|^2,
+// that is the BGK update plus dr w_i P_i: the same relaxation arithmetic as
+// bgk() (s = 1) and one extra term.  The term adds dr to the density and
+// dr u to the momentum, so u is unchanged.  Returns rho - 1 before the
+// collision (the density the reference's statistics sum,
+// block_lattice.cpp:441-455).
+__device__ __forceinline__ float bgk_const_rho(float (&f)[kQ], float omega, float dr) {
+  float dh, jx, jy, jz;
+  moments(f, dh, jx, jy, jz);
+  const float rho = 1.0f + dh;
+  const float k = 1.0f / rho;
+  const float ux = jx * k, uy = jy * k, uz = jz * k;
+  const float u15 = 1.5f * (ux * ux + uy * uy + uz * uz);
+  const float d = rho > 1e-12f ? dr : 0.0f;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const float cu = (cx(i) ? cx(i) * ux : 0.f) + (cy(i) ? cy(i) * uy : 0.f) + (cz(i) ? cz(i) * uz : 0.f);
+    const float q = i == 0 ? -u15 : fmaf(cu, fmaf(4.5f, cu, 3.0f), -u15);  // P_i - 1
+    const float t = fmaf(rho, q, dh);                                       // (feq_i - w_i) / w_i
+    f[i] = fmaf(wf(i) * d, 1.0f + q, fmaf(omega, fmaf(wf(i), t, -f[i]), f[i]));
+  }
+  return dh;
+}
+
 // Bouzidi interpolated bounce-back with the reference's argument roles
 // (src/solver/lbm/boundary/bouzidi_pull.h:8-26); q in (0,1) guaranteed by the
 // caller (q = 1 means plain half-way bounce-back).

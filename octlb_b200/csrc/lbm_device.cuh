@@ -158,6 +158,24 @@ __device__ __forceinline__ float bgk_lane(const LaneDir& d, int lane, const floa
   return fmaf(omega, fmaf(d.w, t, -f), f);
 }
 
+// ConstRhoBGK of population i = lane (the arithmetic of bgk_const_rho for
+// direction i); dh_out = rho - 1 before the collision, on every lane.
+__device__ __forceinline__ float bgk_lane_const_rho(const LaneDir& d, int lane, const float (&fa)[kQ], float f,
+                                                    float omega, float dr, float& dh_out) {
+  float dh, jx, jy, jz;
+  moments(fa, dh, jx, jy, jz);
+  const float rho = 1.0f + dh;
+  const float k = 1.0f / rho;
+  const float ux = jx * k, uy = jy * k, uz = jz * k;
+  const float u15 = 1.5f * (ux * ux + uy * uy + uz * uz);
+  const float dd = rho > 1e-12f ? dr : 0.0f;
+  const float cu = (d.cx != 0.f ? d.cx * ux : 0.f) + (d.cy != 0.f ? d.cy * uy : 0.f) + (d.cz != 0.f ? d.cz * uz : 0.f);
+  const float q = lane == 0 ? -u15 : fmaf(cu, fmaf(4.5f, cu, 3.0f), -u15);
+  const float t = fmaf(rho, q, dh);
+  dh_out = dh;
+  return fmaf(d.w * dd, 1.0f + q, fmaf(omega, fmaf(d.w, t, -f), f));
+}
+
 // Macro state (rho - 1, u, f_neq) of saved pre-collision populations
 // (LevelCoupler::ReadMacro, level_coupler.cpp:183-189).
 struct Macro {

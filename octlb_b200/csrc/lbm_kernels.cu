@@ -86,59 +86,99 @@ __device__ __forceinline__ void rotate_item(const StepArgs& a, uint32_t k) {
     dst[i * a.qs + d] = src[i * a.qs + sl];
 }
 
+// One core cell of k_step / k_step_cr: pull, save, collide (kBulk cells:
+// BGK, or ConstRhoBGK with dr = 1 - average_rho when CR), store.  Returns
+// rho - 1 before the collision for a cell the ConstRhoBGK collided, else 0.
+template <typename T, bool LINKS, bool FLAGS, bool CR>
+__device__ __forceinline__ float core_cell(const StepArgs& a, uint32_t t, const long long* sb, float dr) {
+  const T* src = static_cast<const T*>(a.src);
+  T* dst = static_cast<T*>(a.dst);
+  const uint32_t n3 = a.n * a.n * a.n;
+  const Cell c = cell_of(a, t);
+  const long long tl = t - c.b * n3;
+  const uint8_t fl = FLAGS ? a.flags[t] : 0;
+  float f[kQ];
+  if constexpr (LINKS) {
+    if ((fl & kKindMask) == kSolid) {
+      // Solid cells are neither streamed nor collided (block_lattice.cpp:581-583).
+      copy_cell(src, dst, a.qs, t);
+      return 0.f;
+    }
+  }
+  // Cells next to walls take the link rule in k_step_near.
+  if constexpr (LINKS) {
+    if (fl & kFlagNear) return 0.f;
+  }
+  long long s[kQ];
+  uint32_t halo_mask;
+  source_slots(a, c, t, tl, sb, s, halo_mask);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) f[i] = pull_value(a, src, i, s[i]);
+  float dh = 0.f;
+  bool bulk = true;
+  if constexpr (FLAGS) {
+    if (fl & kFlagSave) {
+      float* sv = a.save_buf + static_cast<long long>(a.save_idx[t]) * kQ;
+#pragma unroll
+      for (int i = 0; i < kQ; ++i) sv[i] = f[i];
+    }
+    bulk = (fl & kKindMask) == kBulk;
+  }
+  if (bulk) {
+    if constexpr (CR) dh = bgk_const_rho(f, a.omega, dr);
+    else bgk(f, a.omega);
+  }
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + t, f[i], a.scale);
+  return dh;
+}
+
 template <typename T, bool LINKS, bool FLAGS, bool BLOCKED>
 __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
   pdl_wait();
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
-  const T* src = static_cast<const T*>(a.src);
-  T* dst = static_cast<T*>(a.dst);
   const uint32_t cta0 = blockIdx.x * kThreads;
   if (cta0 < a.ncore) {
     // CTAs of core cells (ncore is a multiple of the CTA size when BLOCKED,
     // and then a CTA never straddles two blocks).
     __shared__ long long sb[27];
-    const uint32_t n3 = a.n * a.n * a.n;
     if constexpr (BLOCKED) {
       const uint32_t b0 = a.div_n3.div(cta0);
       if (threadIdx.x < 27) sb[threadIdx.x] = a.nbase[b0 * 27 + threadIdx.x];
       __syncthreads();
     }
     if (t >= a.ncore) return;
-    const Cell c = cell_of(a, t);
-    const long long tl = t - c.b * n3;
-    const uint8_t fl = FLAGS ? a.flags[t] : 0;
-    float f[kQ];
-    if constexpr (LINKS) {
-      if ((fl & kKindMask) == kSolid) {
-        // Solid cells are neither streamed nor collided (block_lattice.cpp:581-583).
-        copy_cell(src, dst, a.qs, t);
-        return;
-      }
-    }
-    // Cells next to walls take the link rule in k_step_near.
-    if constexpr (LINKS) {
-      if (fl & kFlagNear) return;
-    }
-    long long s[kQ];
-    uint32_t halo_mask;
-    source_slots(a, c, t, tl, BLOCKED ? sb : nullptr, s, halo_mask);
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) f[i] = pull_value(a, src, i, s[i]);
-    if constexpr (FLAGS) {
-      if (fl & kFlagSave) {
-        float* sv = a.save_buf + static_cast<long long>(a.save_idx[t]) * kQ;
-#pragma unroll
-        for (int i = 0; i < kQ; ++i) sv[i] = f[i];
-      }
-      if ((fl & kKindMask) == kBulk) bgk(f, a.omega);
-    } else {
-      bgk(f, a.omega);
-    }
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + t, f[i], a.scale);
+    core_cell<T, LINKS, FLAGS, false>(a, t, BLOCKED ? sb : nullptr, 0.f);
     return;
   }
   // Halo items start at the first CTA after the core CTAs.
+  const uint32_t core_end = ((a.ncore + kThreads - 1) / kThreads) * kThreads;
+  rotate_item<T>(a, t - core_end);
+}
+
+// ConstRhoBGK step (TimeLoop with use_const_rho_bgk, time_loop.h:173-187 and
+// 201-222): k_step's cells with the ConstRhoBGK collide at the average density
+// *cr_avg, and each core CTA's sum of rho - 1 over the kBulk cells it
+// collided in cr_part[blockIdx.x] (a fixed shuffle tree).
+template <typename T, bool LINKS, bool FLAGS, bool BLOCKED>
+__global__ void __launch_bounds__(kThreads) k_step_cr(const StepArgs a) {
+  pdl_wait();
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  const uint32_t cta0 = blockIdx.x * kThreads;
+  if (cta0 < a.ncore) {
+    __shared__ long long sb[27];
+    if constexpr (BLOCKED) {
+      const uint32_t b0 = a.div_n3.div(cta0);
+      if (threadIdx.x < 27) sb[threadIdx.x] = a.nbase[b0 * 27 + threadIdx.x];
+      __syncthreads();
+    }
+    const float dr = static_cast<float>(1.0 - *a.cr_avg);
+    double v[1] = {0.0};
+    if (t < a.ncore) v[0] = core_cell<T, LINKS, FLAGS, true>(a, t, BLOCKED ? sb : nullptr, dr);
+    block_reduce<1>(v);
+    if (threadIdx.x == 0) a.cr_part[blockIdx.x] = v[0];
+    return;
+  }
   const uint32_t core_end = ((a.ncore + kThreads - 1) / kThreads) * kThreads;
   rotate_item<T>(a, t - core_end);
 }
@@ -151,9 +191,9 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
 // moving-wall term.  Then the same save / collide / store as k_step.  One
 // warp per cell, lane i on direction i; the collision gathers the 19 values
 // so every lane computes the moments exactly as bgk() does.
-template <typename T>
-__device__ __forceinline__ void near_cell(const StepArgs& a, const NearTables& nt, int k, int lane) {
-  if (k >= nt.n) return;
+template <typename T, bool CR = false>
+__device__ __forceinline__ float near_cell(const StepArgs& a, const NearTables& nt, int k, int lane, float dr = 0.f) {
+  if (k >= nt.n) return 0.f;
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
   const LaneDir d = lane_dir(lane);
@@ -169,17 +209,34 @@ __device__ __forceinline__ void near_cell(const StepArgs& a, const NearTables& n
   float f = val;
   if (d.act && ((mask >> lane) & 1u)) f = (q < 1.0f ? bouzidi(own_opp, val, own, q) : own_opp) + add;
   if ((fl & kFlagSave) && d.act) a.save_buf[static_cast<long long>(a.save_idx[t]) * kQ + lane] = f;
+  float dh = 0.f;
   if ((fl & kKindMask) == kBulk) {
     float fa[kQ];
     gather_lanes(f, fa);
-    f = bgk_lane(d, lane, fa, f, a.omega);
+    if constexpr (CR) f = bgk_lane_const_rho(d, lane, fa, f, a.omega, dr, dh);
+    else f = bgk_lane(d, lane, fa, f, a.omega);
   }
   if (d.act) Store<T>::st(dst + lane * a.qs + t, f, a.scale);
+  return dh;
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_step_near(const StepArgs a, const NearTables nt) {
   near_cell<T>(a, nt, (blockIdx.x * kThreads + threadIdx.x) >> 5, threadIdx.x & 31);
+}
+
+// Near-wall cells under ConstRhoBGK: one warp per cell as k_step_near; each
+// CTA's sum of rho - 1 over its collided kBulk cells in
+// cr_part[part_off + blockIdx.x].
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_step_near_cr(const StepArgs a, const NearTables nt, int part_off) {
+  pdl_wait();
+  const float dr = static_cast<float>(1.0 - *a.cr_avg);
+  const int lane = threadIdx.x & 31;
+  const float dh = near_cell<T, true>(a, nt, (blockIdx.x * kThreads + threadIdx.x) >> 5, lane, dr);
+  double v[1] = {lane == 0 ? static_cast<double>(dh) : 0.0};
+  block_reduce<1>(v);
+  if (threadIdx.x == 0) a.cr_part[part_off + blockIdx.x] = v[0];
 }
 
 // Two-element vector access for the paired periodic kernel.
@@ -660,7 +717,10 @@ k_gather(const StepArgs a, double* out, double* out_u, int mode /*0 pops, 1 fiel
       drho += v; jx += cx(i) * v; jy += cy(i) * v; jz += cz(i) * v;
     }
     const double rho = 1.0 + drho;
-    out[t] = rho;
+    // ConstRhoBGK: the stored state is one collide ahead, which added
+    // 1 - average_rho to the density of a kBulk cell and left u unchanged
+    const bool cr = a.cr_avg && (a.flags ? (a.flags[slot] & kKindMask) : kBulk) == kBulk;
+    out[t] = cr ? rho - (1.0 - *a.cr_avg) : rho;
     out_u[static_cast<long long>(t) * 3 + 0] = jx / rho;
     out_u[static_cast<long long>(t) * 3 + 1] = jy / rho;
     out_u[static_cast<long long>(t) * 3 + 2] = jz / rho;
@@ -668,20 +728,70 @@ k_gather(const StepArgs a, double* out, double* out_u, int mode /*0 pops, 1 fiel
 }
 
 // Reference state f (pre-collision, FP64) -> stored g = C(f) for kBulk cells.
+// Under ConstRhoBGK the collide is taken at *cr_avg, and each CTA's sum of
+// rho - 1 over its kBulk cells goes to cr_part[blockIdx.x] (the statistics of
+// that collide; the near-wall partials after them, near_parts, are zeroed).
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_scatter(const StepArgs a, const double* in) {
+k_scatter(const StepArgs a, const double* in, int near_parts) {
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
-  if (t >= a.ncore) return;
-  const long long slot = t;  // compact core slot
-  float f[kQ];
+  double v[1] = {0.0};
+  if (t < a.ncore) {
+    const long long slot = t;  // compact core slot
+    float f[kQ];
 #pragma unroll
-  for (int i = 0; i < kQ; ++i) f[i] = static_cast<float>(in[static_cast<long long>(t) * kQ + i]);
-  const int kind = a.flags ? (a.flags[slot] & kKindMask) : kBulk;
-  if (kind == kBulk) bgk(f, a.omega);
-  T* dst = static_cast<T*>(a.dst);
+    for (int i = 0; i < kQ; ++i) f[i] = static_cast<float>(in[static_cast<long long>(t) * kQ + i]);
+    const int kind = a.flags ? (a.flags[slot] & kKindMask) : kBulk;
+    if (kind == kBulk) {
+      if (a.cr_avg) v[0] = bgk_const_rho(f, a.omega, static_cast<float>(1.0 - *a.cr_avg));
+      else bgk(f, a.omega);
+    }
+    T* dst = static_cast<T*>(a.dst);
 #pragma unroll
-  for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + slot, f[i], a.scale);
+    for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + slot, f[i], a.scale);
+  }
+  if (a.cr_part) {
+    block_reduce<1>(v);
+    if (threadIdx.x == 0) a.cr_part[blockIdx.x] = v[0];
+    if (blockIdx.x == 0)
+      for (int p = threadIdx.x; p < near_parts; p += kThreads) a.cr_part[gridDim.x + p] = 0.0;
+  }
+}
+
+// ConstRhoBGK statistics of a stored state that BGK collided (which keeps
+// each cell's density): per CTA the sum of rho - 1 over kBulk core cells, as
+// k_scatter lays them out.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_cr_seed(const StepArgs a, int near_parts) {
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  double v[1] = {0.0};
+  if (t < a.ncore && (a.flags ? (a.flags[t] & kKindMask) : kBulk) == kBulk) {
+    const T* src = static_cast<const T*>(a.src);
+    float f[kQ];
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) f[i] = LD(src, a.qs, i, t, a.inv_scale);
+    float dh, jx, jy, jz;
+    moments(f, dh, jx, jy, jz);
+    v[0] = dh;
+  }
+  block_reduce<1>(v);
+  if (threadIdx.x == 0) a.cr_part[blockIdx.x] = v[0];
+  if (blockIdx.x == 0)
+    for (int p = threadIdx.x; p < near_parts; p += kThreads) a.cr_part[gridDim.x + p] = 0.0;
+}
+
+// average_rho <- CollideRhoStats::average() of the last collide
+// (block_lattice.h:22-32, time_loop.h:220-222): the statistic of a cell is
+// rho + (1 - average_rho) with the average that collide used, so the mean
+// over `count` kBulk cells is 2 - average_rho + sum(rho - 1) / count (1 when
+// there are none).  The partials are summed in a fixed order.
+__global__ void __launch_bounds__(kThreads)
+k_cr_update(double* avg, const double* part, int nparts, long long count) {
+  pdl_wait();
+  double v[1] = {0.0};
+  for (int p = threadIdx.x; p < nparts; p += kThreads) v[0] += part[p];
+  block_reduce<1>(v);
+  if (threadIdx.x == 0) *avg = count > 0 ? (2.0 - *avg) + v[0] / static_cast<double>(count) : 1.0;
 }
 
 inline uint32_t grid_for(uint32_t items) { return (items + kThreads - 1) / kThreads; }
@@ -813,9 +923,48 @@ cudaError_t launch_gather(const StepArgs& a, double* out, double* out_u, int mod
   return cudaGetLastError();
 }
 template <typename T>
-cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) {
-  k_scatter<T><<<grid_for(a.ncore), kThreads, 0, s>>>(a, in);
+cudaError_t launch_scatter(const StepArgs& a, const double* in, int near_parts, cudaStream_t s) {
+  k_scatter<T><<<grid_for(a.ncore), kThreads, 0, s>>>(a, in, near_parts);
   return cudaGetLastError();
+}
+
+// ConstRhoBGK partials of a level: one per core CTA of k_step_cr (the CTAs of
+// k_scatter / k_cr_seed), then one per CTA of k_step_near_cr.
+uint32_t cr_core_parts(const StepArgs& a) { return grid_for(a.ncore); }
+uint32_t cr_near_parts(const NearTables& nt) { return nt.n > 0 ? grid_for(static_cast<uint32_t>(nt.n) * 32) : 0; }
+
+template <typename T>
+cudaError_t launch_step_cr(const StepArgs& a, const NearTables& nt, bool links, bool flags, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
+  if (a.nitems == 0) return cudaSuccess;
+  const uint32_t n3 = static_cast<uint32_t>(a.n) * a.n * a.n;
+  const bool blocked = n3 % kThreads == 0;
+  const uint32_t core_ctas = grid_for(a.ncore);
+  const dim3 g(core_ctas + grid_for(a.nitems - a.ncore));
+  if (blocked) {
+    if (links) e = launch_chain(k_step_cr<T, true, true, true>, g, dim3(kThreads), 0, s, a);
+    else if (flags) e = launch_chain(k_step_cr<T, false, true, true>, g, dim3(kThreads), 0, s, a);
+    else e = launch_chain(k_step_cr<T, false, false, true>, g, dim3(kThreads), 0, s, a);
+  } else {
+    if (links) e = launch_chain(k_step_cr<T, true, true, false>, g, dim3(kThreads), 0, s, a);
+    else if (flags) e = launch_chain(k_step_cr<T, false, true, false>, g, dim3(kThreads), 0, s, a);
+    else e = launch_chain(k_step_cr<T, false, false, false>, g, dim3(kThreads), 0, s, a);
+  }
+  if (e == cudaSuccess && nt.n > 0)
+    e = launch_chain(k_step_near_cr<T>, dim3(cr_near_parts(nt)), dim3(kThreads), 0, s, a, nt,
+                     static_cast<int>(core_ctas));
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_cr_seed(const StepArgs& a, int near_parts, cudaStream_t s) {
+  k_cr_seed<T><<<grid_for(a.ncore), kThreads, 0, s>>>(a, near_parts);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cr_update(double* avg, const double* part, int nparts, long long count, cudaStream_t s) {
+  const cudaError_t e = launch_chain(k_cr_update, dim3(1), dim3(kThreads), 0, s, avg, part, nparts, count);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 #define OCTLB_INST(T)                                                                              \
@@ -830,7 +979,9 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, cudaStream_t s) 
                                       cudaStream_t);                                               \
   template cudaError_t launch_audit<T>(const StepArgs&, double*, double*, cudaStream_t);           \
   template cudaError_t launch_gather<T>(const StepArgs&, double*, double*, int, cudaStream_t);              \
-  template cudaError_t launch_scatter<T>(const StepArgs&, const double*, cudaStream_t);
+  template cudaError_t launch_scatter<T>(const StepArgs&, const double*, int, cudaStream_t);     \
+  template cudaError_t launch_step_cr<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
+  template cudaError_t launch_cr_seed<T>(const StepArgs&, int, cudaStream_t);
 
 OCTLB_INST(float)
 OCTLB_INST(__half)

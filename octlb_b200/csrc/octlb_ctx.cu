@@ -28,7 +28,13 @@ cudaError_t launch_drag(const StepArgs&, bool, const DragItem*, int, double*, cu
 cudaError_t launch_drag_total(const double*, int, double*, double*, cudaStream_t);
 template <typename T> cudaError_t launch_audit(const StepArgs&, double*, double*, cudaStream_t);
 template <typename T> cudaError_t launch_gather(const StepArgs&, double*, double*, int, cudaStream_t);
-template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*, cudaStream_t);
+template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*, int, cudaStream_t);
+template <typename T>
+cudaError_t launch_step_cr(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
+template <typename T> cudaError_t launch_cr_seed(const StepArgs&, int, cudaStream_t);
+cudaError_t launch_cr_update(double*, const double*, int, long long, cudaStream_t);
+uint32_t cr_core_parts(const StepArgs& a);
+uint32_t cr_near_parts(const NearTables& nt);
 template <typename T> cudaError_t launch_step_bulk(const StepArgs&, int, cudaStream_t);
 template <typename T> int bulk_prepare(int n);
 template <typename T> cudaError_t launch_step_pair(const StepArgs&, cudaStream_t);
@@ -110,6 +116,7 @@ struct Level {
   NearTables near{};
   int n_near = 0;
   int n_open = 0, n_halo = 0, n_pages = 0, n_save = 0, n_links = 0;
+  long long n_bulk = 0;             // kBulk core cells
   bool has_flags = false;
   // tree-boundary halo fills
   DevBuf bb_ops, fill_of;           // fills, and per (page slot, population) the fill index or -1
@@ -260,6 +267,13 @@ struct octlb_ctx {
   float prolong_scale = 0.f, restrict_scale = 0.f;
   double wall_vscale = 0.0;         // largest moving-wall speed (adjoint velocity parameter)
   std::unique_ptr<AdjointState> adj;
+  // ConstRhoBGK (TimeLoop's use_const_rho_bgk, single-level meshes): the
+  // average density on the device (TimeLoop::average_rho_) and the partial
+  // sums of the last collide's statistics, over cr_count kBulk cells
+  bool const_rho = false;
+  DevBuf cr_avg, cr_part;
+  int cr_level = -1, cr_nparts = 0, cr_near = 0;
+  long long cr_count = 0;
 };
 
 namespace octlb_host {
@@ -400,7 +414,14 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     ctx->side_busy = true;
     ++ctx->launch_count;
   }
-  if (L.use_bulk) {
+  if (ctx->const_rho) {
+    // ConstRhoBGK: average_rho from the last collide's statistics
+    // (time_loop.h:220-222), then the step whose collide uses it
+    CK(launch_cr_update(ctx->cr_avg.as<double>(), ctx->cr_part.as<double>(), ctx->cr_nparts, ctx->cr_count,
+                        ctx->stream));
+    CK(launch_step_cr<T>(a, L.near, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags, ctx->stream));
+    ctx->launch_count += 1 + (L.near.n > 0 ? 1 : 0);
+  } else if (L.use_bulk) {
     CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
   } else if (L.use_pair) {
     CK(launch_step_pair<T>(a, ctx->stream));
@@ -766,6 +787,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     for (int lb = 0; lb < L.nblk; ++lb)
       std::memcpy(&flags[static_cast<size_t>(lb * n3)], t->kinds + static_cast<size_t>(L.blocks[lb]) * n3,
                   static_cast<size_t>(n3));
+    L.n_bulk = std::count(flags.begin(), flags.end(), static_cast<uint8_t>(kBulk));
     for (const auto& kv : recs) {
       const int gb = static_cast<int>(kv.first / n3);
       if (ctx->blk_level[gb] != l) continue;
@@ -1356,7 +1378,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     CK(upload(d, dense));
     StepArgs a = L.args;
     a.dst = L.buf[L.cur].p;
-    CK(launch_scatter<T>(a, d.as<double>(), ctx->stream));
+    CK(launch_scatter<T>(a, d.as<double>(), 0, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
   }
   long long lups = 0;
@@ -1946,7 +1968,7 @@ int scatter_impl(octlb_ctx* ctx, const double* in) {
     }
     StepArgs a = L.args;
     a.dst = L.buf[L.cur].p;
-    CK(launch_scatter<T>(a, d.as<double>(), ctx->stream));
+    CK(launch_scatter<T>(a, d.as<double>(), a.cr_part ? ctx->cr_near : 0, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
   }
   return OCTLB_OK;
@@ -2057,7 +2079,65 @@ int octlb_gpu_adjoint(octlb_ctx* ctx, const octlb_adj_params* p, double* objecti
   if (!ctx || !p) return OCTLB_EINVAL;
   if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
   if (ctx->precision != OCTLB_FP32) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates FP32 storage only");
+  if (ctx->const_rho) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates the BGK collide, not ConstRhoBGK");
   return adjoint_impl<float>(ctx, p, objective, grad, grad_force);
+}
+
+int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on) {
+  if (!ctx) return OCTLB_EINVAL;
+  if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
+  for (int c : ctx->counters_collide)
+    if (c != 0) return fail(ctx, OCTLB_ESTATE, "ConstRhoBGK is chosen before the first advance");
+  if ((on != 0) == ctx->const_rho) return OCTLB_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  clear_graphs(ctx);  // the captured launch sequence changes
+  int lev = -1, used = 0;
+  for (size_t l = 0; l < ctx->levels.size(); ++l)
+    if (ctx->levels[l].nblk > 0) { lev = static_cast<int>(l); ++used; }
+  if (!on) {
+    if (ctx->cr_level >= 0) {
+      ctx->levels[ctx->cr_level].args.cr_avg = nullptr;
+      ctx->levels[ctx->cr_level].args.cr_part = nullptr;
+    }
+    ctx->const_rho = false;
+    ctx->cr_level = -1;
+    return OCTLB_OK;
+  }
+  // The stored state is one collide ahead of the reference's, so a coarse
+  // level would collide before the finest steps that set its average density
+  // have run: ConstRhoBGK is built for one level, as the reference uses it.
+  if (used != 1) return fail(ctx, OCTLB_EINVAL, "ConstRhoBGK needs a single-level mesh");
+  Level& L = ctx->levels[lev];
+  CK(upload(ctx->cr_avg, std::vector<double>{1.0}));  // TimeLoop starts at average_rho_ = 1
+  const uint32_t core = cr_core_parts(L.args), near = cr_near_parts(L.near);
+  ctx->cr_nparts = static_cast<int>(core + near);
+  ctx->cr_near = static_cast<int>(near);
+  ctx->cr_count = L.n_bulk;
+  CK(ctx->cr_part.alloc(static_cast<size_t>(std::max(ctx->cr_nparts, 1)) * sizeof(double)));
+  L.args.cr_avg = ctx->cr_avg.as<double>();
+  L.args.cr_part = ctx->cr_part.as<double>();
+  // The stored state was collided by BGK, which is ConstRhoBGK at
+  // average_rho = 1 and keeps each cell's density: its statistics are the
+  // stored densities.
+  StepArgs a = L.args;
+  a.src = cur_buf(L);
+  CK(ctx->precision == OCTLB_FP32 ? launch_cr_seed<float>(a, ctx->cr_near, ctx->stream)
+                                  : launch_cr_seed<__half>(a, ctx->cr_near, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->const_rho = true;
+  ctx->cr_level = lev;
+  return OCTLB_OK;
+}
+
+int octlb_gpu_average_rho(octlb_ctx* ctx, double* out) {
+  if (!ctx || !out) return OCTLB_EINVAL;
+  if (!ctx->const_rho) {
+    *out = 1.0;
+    return OCTLB_OK;
+  }
+  CK(cudaMemcpyAsync(out, ctx->cr_avg.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return OCTLB_OK;
 }
 
 int octlb_gpu_synchronize(octlb_ctx* ctx) {

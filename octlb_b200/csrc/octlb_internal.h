@@ -49,6 +49,10 @@ struct StepArgs {
   float omega, scale, inv_scale;
   int off[kQ];              // core slot offset of c_i: cx*n*n + cy*n + cz
   int off_pad[kQ];          // padded linear offset of c_i: cx*np*np + cy*np + cz
+  // ConstRhoBGK (null for BGK): the average density the collide uses, and
+  // per-CTA partial sums of rho - 1 over the kBulk cells it collided
+  const double* cr_avg;
+  double* cr_part;
   int* err;                 // device error word (bounded waits that gave up)
 };
 

@@ -52,6 +52,9 @@ def load(which):
         getattr(L, pre + fn).restype = ctypes.c_double
         getattr(L, pre + fn).argtypes = ([ctypes.c_int] + [ctypes.c_double] * 4 if fn == "feq"
                                          else [ctypes.c_double] * 4)
+    if hasattr(L, "ref_sim_average_rho"):
+        L.ref_sim_average_rho.restype = ctypes.c_double
+        L.ref_sim_average_rho.argtypes = [P]
     if which == "tlm":
         L.tlm_dirs.restype = ctypes.c_int
     if which == "orc":
@@ -183,6 +186,15 @@ class Sim:
 
     def advance(self, steps=1):
         self.L.ref_sim_advance(self.h, ctypes.c_int(steps))
+
+    def set_const_rho(self, on=True):
+        """The reference TimeLoop rebuilt with use_const_rho_bgk (before the
+        first advance)."""
+        self.L.ref_sim_set_const_rho(self.h, ctypes.c_int(1 if on else 0))
+
+    def average_rho(self):
+        """TimeLoop::average_rho()."""
+        return float(self.L.ref_sim_average_rho(self.h))
 
     def set_body_force(self, force):
         """Body force [n_blocks][n^3][3] (or None): 3 w_i (c_i . F) added to the

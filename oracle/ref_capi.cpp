@@ -219,6 +219,7 @@ struct Sim {
   std::unique_ptr<LevelCoupler> coupler;
   std::unique_ptr<DomainBoundaryHandler> bc;
   std::unique_ptr<TimeLoop> loop;
+  double omega = 0.0;
 };
 
 // Sum of MomentumExchangeDrag::force_on_fluid_if over all blocks (see
@@ -415,8 +416,19 @@ void* ref_sim_new(int n_oct, const int* levels, const f64* bounds, int n_sl,
   s->loop = std::make_unique<TimeLoop>(*s->forest, *s->blocks, *s->ghosts, *s->coupler,
                                        *s->bc, omega);
   s->loop->set_snapshot_post_collide(true);
+  s->omega = omega;
   return s;
 }
+// The TimeLoop rebuilt with use_const_rho_bgk (ConstRhoStatsScope::
+// kFluidAndBoundary, the constructor's default); before the first advance
+// and before ref_sim_set_body_force.
+void ref_sim_set_const_rho(void* h, int on) {
+  auto* s = static_cast<Sim*>(h);
+  s->loop = std::make_unique<TimeLoop>(*s->forest, *s->blocks, *s->ghosts, *s->coupler,
+                                       *s->bc, s->omega, on != 0);
+  s->loop->set_snapshot_post_collide(true);
+}
+f64 ref_sim_average_rho(void* h) { return to_f64(static_cast<Sim*>(h)->loop->average_rho()); }
 void ref_sim_free(void* h) {
   auto* s = static_cast<Sim*>(h);
   // TimeLoop / coupler / ghosts hold references: tear down in reverse order.
