@@ -224,12 +224,19 @@ def forest_measurements(ob, cases, torch, peak):
         # per-launch latency
         "cylinder_512x128x128": (lambda: cases.cylinder_forest(length=512, height=128, diameter=32.0,
                                                                center=(128.0, 64.0)), ob.STREAM_LINKS, True),
+        # single-level 128^3 cavity (the reference's cavity3d collision),
+        # ConstRhoBGK; BGK on the same mesh beside it
+        "const_rho_cavity_128": (lambda: cases.cavity_forest(cells=128, n=8, lid=0.05, tau=0.56),
+                                 ob.STREAM_ROTATE, False),
     }
     for name, (fn, mode, drag) in cfgs.items():
         mesh, init, info = fn()
         r = {}
-        for pn, prec in (("fp32", ob.FP32), ("fp16", ob.FP16_SHIFTED)):
+        const_rho = name.startswith("const_rho")
+        for pn, prec in (("fp32", ob.FP32), ("fp16", ob.FP16_SHIFTED)) + ((("bgk_fp32", ob.FP32),) if const_rho else ()):
             lat = ob.GpuLattice(mesh, info["omega"], precision=prec, stream_mode=mode, drag=drag, init_pops=init)
+            if const_rho and pn != "bgk_fp32":
+                lat.set_const_rho(True)
             st = torch.cuda.Stream()
             lat.set_stream(st.cuda_stream)
             lat.advance(5)
@@ -242,7 +249,7 @@ def forest_measurements(ob, cases, torch, peak):
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / K
             launches, lups = lat.step_stats()
-            bpl = 152 if pn == "fp32" else 76
+            bpl = 76 if pn == "fp16" else 152
             r[pn] = {"mlups": lups / ms / 1e3, "ms_per_step": ms, "launches_per_step": int(launches),
                      "hbm_frac": bpl * lups / (ms * 1e-3) / 1e9 / peak}
             if name == "cylinder_256x64x64":
@@ -259,6 +266,8 @@ def forest_measurements(ob, cases, torch, peak):
                 r[pn]["drag_rel_err_vs_fp64"] = float(abs(fs[0] / nsteps - ref) / abs(ref))
             lat.close()
         r["fp16_speedup"] = r["fp16"]["mlups"] / r["fp32"]["mlups"]
+        if const_rho:
+            r["const_rho_over_bgk_fp32"] = r["fp32"]["mlups"] / r["bgk_fp32"]["mlups"]
         out[name] = r
     # adjoint
     from make_adjoint_reference import case, directions
@@ -320,9 +329,13 @@ def run_single_case(args, ob, cases, torch):
         J = lat.adjoint(args.steps, max(1, args.steps // 4), 16, force_grad=False)[0]
         print(json.dumps({"case": "adjoint", "steps": args.steps, "seconds": time.perf_counter() - t0, "J": J}))
         return
+    const_rho = False
     if args.case == "amr_cavity_64":
         mesh, init, info = cases.cavity_forest(cells=64, n=8, lid=0.05, tau=0.56, band_cells=8)
         mode, drag = ob.STREAM_ROTATE, False
+    elif args.case == "const_rho_cavity_128":
+        mesh, init, info = cases.cavity_forest(cells=128, n=8, lid=0.05, tau=0.56)
+        mode, drag, const_rho = ob.STREAM_ROTATE, False, True
     elif args.case == "cylinder_512":
         mesh, init, info = cases.cylinder_forest(length=512, height=128, diameter=32.0, center=(128.0, 64.0))
         mode, drag = ob.STREAM_LINKS, True
@@ -330,6 +343,8 @@ def run_single_case(args, ob, cases, torch):
         mesh, init, info = cases.cylinder_forest()
         mode, drag = ob.STREAM_LINKS, True
     lat = ob.GpuLattice(mesh, info["omega"], precision=prec, stream_mode=mode, drag=drag, init_pops=init)
+    if const_rho:
+        lat.set_const_rho(True)
     st = torch.cuda.Stream()
     lat.set_stream(st.cuda_stream)
     lat.advance(args.warmup)
@@ -356,7 +371,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-forest", action="store_true", help="skip the forest / adjoint measurements")
-    ap.add_argument("--case", default="tgv", choices=["tgv", "amr_cavity_64", "cylinder", "cylinder_512", "adjoint"],
+    ap.add_argument("--case", default="tgv", choices=["tgv", "amr_cavity_64", "cylinder", "cylinder_512", "adjoint",
+                                                      "const_rho_cavity_128"],
                     help="tgv: the headline line; otherwise run only that case for --steps advance_one "
                          "calls (or one adjoint sweep of --steps calls) and print its timing (profiling)")
     args = ap.parse_args()

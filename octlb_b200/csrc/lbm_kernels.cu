@@ -86,6 +86,17 @@ __device__ __forceinline__ void rotate_item(const StepArgs& a, uint32_t k) {
     dst[i * a.qs + d] = src[i * a.qs + sl];
 }
 
+// ConstRhoBGK statistics of a step launch: this CTA's sum into
+// cr_part[blockIdx.x]; CTA 0 also zeroes the partials from `written` (the
+// CTAs that write one) up to cr_total, which the average update sums.
+__device__ __forceinline__ void cr_store_partial(const StepArgs& a, double v0, uint32_t written) {
+  double v[1] = {v0};
+  block_reduce<1>(v);
+  if (threadIdx.x == 0) a.cr_part[blockIdx.x] = v[0];
+  if (blockIdx.x == 0)
+    for (int p = static_cast<int>(written) + threadIdx.x; p < a.cr_total; p += kThreads) a.cr_part[p] = 0.0;
+}
+
 // One core cell of k_step / k_step_cr: pull, save, collide (kBulk cells:
 // BGK, or ConstRhoBGK with dr = 1 - average_rho when CR), store.  Returns
 // rho - 1 before the collision for a cell the ConstRhoBGK collided, else 0.
@@ -173,10 +184,10 @@ __global__ void __launch_bounds__(kThreads) k_step_cr(const StepArgs a) {
       __syncthreads();
     }
     const float dr = static_cast<float>(1.0 - *a.cr_avg);
-    double v[1] = {0.0};
-    if (t < a.ncore) v[0] = core_cell<T, LINKS, FLAGS, true>(a, t, BLOCKED ? sb : nullptr, dr);
-    block_reduce<1>(v);
-    if (threadIdx.x == 0) a.cr_part[blockIdx.x] = v[0];
+    float dh = 0.f;
+    if (t < a.ncore) dh = core_cell<T, LINKS, FLAGS, true>(a, t, BLOCKED ? sb : nullptr, dr);
+    // the near-cell CTAs of k_step_near_cr write the partials after these
+    cr_store_partial(a, static_cast<double>(dh), static_cast<uint32_t>(a.cr_total));
     return;
   }
   const uint32_t core_end = ((a.ncore + kThreads - 1) / kThreads) * kThreads;
@@ -285,34 +296,53 @@ __device__ __forceinline__ bool map_cell_prologue(const StepArgs& a, uint32_t t,
   return true;
 }
 
-template <typename T, bool FLAGS>
-__device__ __forceinline__ void map_cell_finish(const StepArgs& a, uint32_t t, uint8_t fl, float (&f)[kQ], T* dst) {
+template <typename T, bool FLAGS, bool CR = false>
+__device__ __forceinline__ float map_cell_finish(const StepArgs& a, uint32_t t, uint8_t fl, float (&f)[kQ], T* dst,
+                                                 float dr = 0.f) {
+  float dh = 0.f;
+  bool bulk = true;
   if constexpr (FLAGS) {
     if (fl & kFlagSave) {
       float* sv = a.save_buf + static_cast<long long>(a.save_idx[t]) * kQ;
 #pragma unroll
       for (int i = 0; i < kQ; ++i) sv[i] = f[i];
     }
-    if ((fl & kKindMask) == kBulk) bgk(f, a.omega);
-  } else {
-    bgk(f, a.omega);
+    bulk = (fl & kKindMask) == kBulk;
+  }
+  if (bulk) {
+    if constexpr (CR) dh = bgk_const_rho(f, a.omega, dr);
+    else bgk(f, a.omega);
   }
   const uint32_t qs = static_cast<uint32_t>(a.qs);
 #pragma unroll
   for (int i = 0; i < kQ; ++i) Store<T>::st(dst + (static_cast<uint32_t>(i) * qs + t), f[i], a.scale);
+  return dh;
 }
 
 // With one cell per thread (CPT = 1) two CTAs share a block, each over half
 // its cells, so small levels still give every SM work.  Under the links rule
 // the first CTAs of the launch take the near-wall cells (one warp each), so
 // they run beside the bulk instead of in a launch of their own.
-template <typename T, bool LINKS, bool FLAGS, int CPT, bool GMAP>
+//
+// CR: the ConstRhoBGK collide at average density *cr_avg, and per near-cell
+// and block CTA the sum of rho - 1 over its collided kBulk cells in
+// cr_part[blockIdx.x] (the halo-item CTAs after them write none).
+template <typename T, bool LINKS, bool FLAGS, int CPT, bool GMAP, bool CR = false>
 __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const StepArgs a, const NearTables nt) {
   extern __shared__ int smap_s[];  // (n+2)^3 slots of this block
   constexpr uint32_t kParts = CPT == 1 ? 2 : 1;
   const uint32_t near_ctas = LINKS ? (static_cast<uint32_t>(nt.n) + kThreads / 32 - 1) / (kThreads / 32) : 0;
   if (LINKS && blockIdx.x < near_ctas) {
-    near_cell<T>(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)), threadIdx.x & 31);
+    if constexpr (CR) {
+      pdl_wait();
+      const float dr = static_cast<float>(1.0 - *a.cr_avg);
+      const float dh = near_cell<T, true>(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)),
+                                          threadIdx.x & 31, dr);
+      cr_store_partial(a, (threadIdx.x & 31) == 0 ? static_cast<double>(dh) : 0.0,
+                       near_ctas + static_cast<uint32_t>(a.nblk) * kParts);
+    } else {
+      near_cell<T>(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)), threadIdx.x & 31);
+    }
     return;
   }
   const uint32_t bid = blockIdx.x - near_ctas;
@@ -337,6 +367,8 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
   T* dst = static_cast<T*>(a.dst);
   const uint32_t n = a.n, n3 = n * n * n, qs = static_cast<uint32_t>(a.qs);
   const uint32_t span = n3 / kParts;
+  const float dr = CR ? static_cast<float>(1.0 - *a.cr_avg) : 0.f;
+  float acc = 0.f;
   for (uint32_t tl0 = part * span + threadIdx.x; tl0 < (part + 1) * span; tl0 += CPT * kThreads) {
     uint32_t t[CPT];
     int P[CPT];
@@ -380,8 +412,12 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
     }
 #pragma unroll
     for (int c = 0; c < CPT; ++c)
-      if (go[c]) map_cell_finish<T, FLAGS>(a, t[c], fl[c], f[c], dst);
+      if (go[c]) {
+        if constexpr (CR) acc += map_cell_finish<T, FLAGS, true>(a, t[c], fl[c], f[c], dst, dr);
+        else map_cell_finish<T, FLAGS>(a, t[c], fl[c], f[c], dst);
+      }
   }
+  if constexpr (CR) cr_store_partial(a, static_cast<double>(acc), near_ctas + static_cast<uint32_t>(a.nblk) * kParts);
 }
 
 // One periodic all-kBulk block, two consecutive z cells per thread: every
@@ -858,6 +894,20 @@ cudaError_t launch_step_map(const StepArgs& a, const NearTables& nt, bool links,
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
+// ConstRhoBGK slot-map step: the default variants only (one cell per thread
+// under the links rule, two otherwise; slot map read through L1).
+template <typename T>
+cudaError_t launch_step_map_cr(const StepArgs& a, const NearTables& nt, bool links, bool flags, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
+  if (a.nitems == 0) return cudaSuccess;
+  const uint32_t near_ctas = links ? grid_for(static_cast<uint32_t>(nt.n) * 32) : 0;
+  const dim3 g(near_ctas + static_cast<uint32_t>(a.nblk) * (links ? 2 : 1) + grid_for(static_cast<uint32_t>(a.n_open)));
+  if (links) e = launch_chain(k_step_map<T, true, true, 1, true, true>, g, dim3(kThreads), 0, s, a, nt);
+  else if (flags) e = launch_chain(k_step_map<T, false, true, 2, true, true>, g, dim3(kThreads), 0, s, a, nt);
+  else e = launch_chain(k_step_map<T, false, false, 2, true, true>, g, dim3(kThreads), 0, s, a, nt);
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_step_near(const StepArgs& a, const NearTables& nt, cudaStream_t s) {
   if (nt.n == 0) return cudaSuccess;
@@ -981,6 +1031,7 @@ cudaError_t launch_cr_update(double* avg, const double* part, int nparts, long l
   template cudaError_t launch_gather<T>(const StepArgs&, double*, double*, int, cudaStream_t);              \
   template cudaError_t launch_scatter<T>(const StepArgs&, const double*, int, cudaStream_t);     \
   template cudaError_t launch_step_cr<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
+  template cudaError_t launch_step_map_cr<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
   template cudaError_t launch_cr_seed<T>(const StepArgs&, int, cudaStream_t);
 
 OCTLB_INST(float)

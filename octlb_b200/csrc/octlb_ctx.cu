@@ -32,6 +32,8 @@ template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*,
 template <typename T>
 cudaError_t launch_step_cr(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
 template <typename T> cudaError_t launch_cr_seed(const StepArgs&, int, cudaStream_t);
+template <typename T>
+cudaError_t launch_step_map_cr(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
 cudaError_t launch_cr_update(double*, const double*, int, long long, cudaStream_t);
 uint32_t cr_core_parts(const StepArgs& a);
 uint32_t cr_near_parts(const NearTables& nt);
@@ -419,8 +421,14 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     // (time_loop.h:220-222), then the step whose collide uses it
     CK(launch_cr_update(ctx->cr_avg.as<double>(), ctx->cr_part.as<double>(), ctx->cr_nparts, ctx->cr_count,
                         ctx->stream));
-    CK(launch_step_cr<T>(a, L.near, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags, ctx->stream));
-    ctx->launch_count += 1 + (L.near.n > 0 ? 1 : 0);
+    const bool links = ctx->stream_mode == OCTLB_STREAM_LINKS;
+    if (L.use_map && ctx->map_global && ctx->map_cells == (links ? 1 : 2)) {
+      CK(launch_step_map_cr<T>(a, L.near, links, L.has_flags, ctx->stream));
+      ++ctx->launch_count;
+    } else {
+      CK(launch_step_cr<T>(a, L.near, links, L.has_flags, ctx->stream));
+      ctx->launch_count += 1 + (L.near.n > 0 ? 1 : 0);
+    }
   } else if (L.use_bulk) {
     CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
   } else if (L.use_pair) {
@@ -2116,6 +2124,7 @@ int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on) {
   CK(ctx->cr_part.alloc(static_cast<size_t>(std::max(ctx->cr_nparts, 1)) * sizeof(double)));
   L.args.cr_avg = ctx->cr_avg.as<double>();
   L.args.cr_part = ctx->cr_part.as<double>();
+  L.args.cr_total = ctx->cr_nparts;
   // The stored state was collided by BGK, which is ConstRhoBGK at
   // average_rho = 1 and keeps each cell's density: its statistics are the
   // stored densities.

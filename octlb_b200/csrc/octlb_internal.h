@@ -53,6 +53,7 @@ struct StepArgs {
   // per-CTA partial sums of rho - 1 over the kBulk cells it collided
   const double* cr_avg;
   double* cr_part;
+  int cr_total;             // partials the average update sums
   int* err;                 // device error word (bounded waits that gave up)
 };
 

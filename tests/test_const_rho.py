@@ -76,11 +76,14 @@ def test_reference_const_rho_statistics(ref):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec,tol", [("fp32", TOL32), ("fp16", TOL16)])
-def test_const_rho_cavity_matches_reference(ob, ref, prec, tol):
+@pytest.mark.parametrize("prec,tol,kernel", [("fp32", TOL32, "map"), ("fp16", TOL16, "map"), ("fp32", TOL32, "plain")])
+def test_const_rho_cavity_matches_reference(ob, ref, prec, tol, kernel, monkeypatch):
     """Moving-lid cavity, torus-rotate stream rule with wall fills, from a
     perturbed rest state at mean density 1.02: average_rho after every call
-    and the fields after 1 and 12 calls against the reference TimeLoop."""
+    and the fields after 1 and 12 calls against the reference TimeLoop (the
+    slot-map step and the plain step)."""
+    if kernel == "plain":
+        monkeypatch.setenv("OCTLB_STEP_KERNEL", "plain")
     mesh, info = brick_cavity()
     init = rest_state(mesh, perturbed_density(mesh, 1.02, 5))
     lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP32 if prec == "fp32" else ob.FP16_SHIFTED,
@@ -110,10 +113,13 @@ def test_const_rho_cavity_matches_reference(ob, ref, prec, tol):
 
 
 @pytest.mark.gpu
-def test_const_rho_cylinder_links_matches_reference(ob, ref):
+@pytest.mark.parametrize("kernel", ["map", "plain"])
+def test_const_rho_cylinder_links_matches_reference(ob, ref, kernel, monkeypatch):
     """Single-level channel with a Bouzidi cylinder (links stream rule, near-wall
     cells on their own warps, parabolic moving-wall inlet, outflow copy),
     from a perturbed rest state at mean density 1.01."""
+    if kernel == "plain":
+        monkeypatch.setenv("OCTLB_STEP_KERNEL", "plain")
     from octlb_b200 import cases
     mesh, init0, info = cases.cylinder_forest(length=64, height=32, n=8, diameter=8.0, center=(16.0, 16.0),
                                               levels=1)
