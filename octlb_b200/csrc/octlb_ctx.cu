@@ -85,6 +85,15 @@ struct DevBuf {
     if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
     return e;
   }
+  // Capacity of at least b bytes, kept across calls and not zero-filled:
+  // staging that every use overwrites before it is read.
+  cudaError_t reserve(size_t b) {
+    if (p && bytes >= b) return cudaSuccess;
+    if (p) { cudaFree(p); p = nullptr; }
+    bytes = b;
+    if (g_dry_run || b == 0) return cudaSuccess;
+    return cudaMalloc(&p, b);
+  }
   template <typename U> U* as() const { return static_cast<U*>(p); }
 };
 
@@ -247,6 +256,9 @@ struct octlb_ctx {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool side_busy = false;
   DevBuf drag_partial, force, force_sum, audit_out, audit_partial, host_tmp, dev_err;
+  // FP64 host-layout staging of set/get_populations and get_fields (grown on
+  // demand, kept until destroy: no allocation per call)
+  DevBuf stage_a, stage_b;
   int drag_parts = 0;
   long long force_steps = 0;
   std::vector<int> counters_collide, counters_stream;
@@ -1924,9 +1936,12 @@ int gather_impl(octlb_ctx* ctx, double* pops, double* rho, double* u) {
     if (L.nblk == 0) continue;
     const long long cells = L.nblk * n3;
     const int mode = pops ? 0 : 1;
-    DevBuf d, du;
-    CK(d.alloc(static_cast<size_t>(cells * (mode == 0 ? kQ : 1)) * sizeof(double)));
-    if (mode == 1) CK(du.alloc(static_cast<size_t>(cells * 3) * sizeof(double)));
+    DevBuf& d = ctx->stage_a;
+    DevBuf& du = ctx->stage_b;
+    const size_t bytes0 = static_cast<size_t>(cells * (mode == 0 ? kQ : 1)) * sizeof(double);
+    const size_t bytes1 = static_cast<size_t>(cells * 3) * sizeof(double);
+    CK(d.reserve(bytes0));
+    if (mode == 1) CK(du.reserve(bytes1));
     StepArgs a = L.args;
     a.src = L.buf[L.cur].p;
     CK(launch_gather<T>(a, d.as<double>(), du.as<double>(), mode, ctx->stream));
@@ -1940,8 +1955,8 @@ int gather_impl(octlb_ctx* ctx, double* pops, double* rho, double* u) {
       o0 = h0.data();
       if (mode == 1) { h1.resize(static_cast<size_t>(cells * 3)); o1 = h1.data(); }
     }
-    CK(cudaMemcpyAsync(o0, d.p, d.bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    if (mode == 1) CK(cudaMemcpyAsync(o1, du.p, du.bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(o0, d.p, bytes0, cudaMemcpyDeviceToHost, ctx->stream));
+    if (mode == 1) CK(cudaMemcpyAsync(o1, du.p, bytes1, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (!direct) {
       for (int lb = 0; lb < L.nblk; ++lb) {
@@ -1964,10 +1979,11 @@ int scatter_impl(octlb_ctx* ctx, const double* in) {
   for (auto& L : ctx->levels) {
     if (L.nblk == 0) continue;
     const long long cells = L.nblk * n3;
-    DevBuf d;
-    CK(d.alloc(static_cast<size_t>(cells * kQ) * sizeof(double)));
+    DevBuf& d = ctx->stage_a;
+    const size_t bytes = static_cast<size_t>(cells * kQ) * sizeof(double);
+    CK(d.reserve(bytes));
     if (contiguous(L)) {
-      CK(cudaMemcpyAsync(d.p, in + static_cast<long long>(L.blocks[0]) * n3 * kQ, d.bytes,
+      CK(cudaMemcpyAsync(d.p, in + static_cast<long long>(L.blocks[0]) * n3 * kQ, bytes,
                          cudaMemcpyHostToDevice, ctx->stream));
     } else {
       for (int lb = 0; lb < L.nblk; ++lb)
