@@ -138,6 +138,41 @@ int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on);
  * ConstRhoBGK collide uses; 1 without ConstRhoBGK.  Synchronises the stream. */
 int octlb_gpu_average_rho(octlb_ctx* ctx, double* out);
 
+/* ---- VTK output (src/solver/io/vtk_writer/) ------------------------------
+ * The files of the reference's writer, byte for byte for the same values: an
+ * XML StructuredGrid .vts per block with binary (base64, UInt32 header)
+ * Float64 cell data and vertex coordinates (WriteStructuredGridVts,
+ * structured_grid_writer.cpp:49-100), a vtkMultiBlockDataSet .vtm per
+ * timestep and a Collection .pvd series (WriteVtmIndex / AppendPvdTimestep,
+ * parallel_vtk_index.cpp:117-172). */
+#define OCTLB_VTK_VELOCITY 1 /* "velocity", 3 components (VtkVelocityField) */
+#define OCTLB_VTK_DENSITY 2  /* "density" (VtkDensityField) */
+#define OCTLB_VTK_PRESSURE 4 /* "pressure" = rho c_s^2 (VtkPressureField) */
+
+/* AmrVtkWriter::WriteTimestep + WriteVtmAndPvd (amr_vtk_writer.h:25-33), each
+ * block with its own fields: one file output_dir/base_r<rank>_oct<block>_T<step,
+ * 5 digits>.vts per block, with the chosen fields (a mask of OCTLB_VTK_*, in
+ * the order velocity, density, pressure) from the reference's post-stream
+ * rho and u (as octlb_gpu_get_fields); with write_index, also
+ * base_T<step>.vtm listing them and the step appended to base.pvd (a run of
+ * several ranks writes the index once, with octlb_vtk_write_index).
+ * Creates output_dir.  Synchronises the stream. */
+int octlb_gpu_write_vtk(octlb_ctx* ctx, const char* output_dir, const char* base_name, int step, int rank,
+                        int fields, int write_index);
+
+/* WriteStructuredGridVts for one block of nx x ny x nz cells on
+ * bounds = {x_min, y_min, z_min, x_max, y_max, z_max}: nfields cell fields,
+ * field f named names[f] with comps[f] (1..3) components, values data[f] in
+ * the file's cell order (i fastest, then j, then k).  Host only. */
+int octlb_vtk_write_block(const char* path, int nx, int ny, int nz, const double bounds[6], int nfields,
+                          const char* const* names, const int* comps, const double* const* data);
+
+/* WriteVtmIndex + AppendPvdTimestep for one timestep: output_dir/base_T<step>.vtm
+ * listing the .vts paths (relative to output_dir), and its entry appended to
+ * output_dir/base.pvd (created on first use).  Host only. */
+int octlb_vtk_write_index(const char* output_dir, const char* base_name, int step, int n_files,
+                          const char* const* vts_relative_paths);
+
 /* Discrete adjoint (reverse mode) of n coarse steps.  Objective J = the
  * `component` of octlb_gpu_force averaged over the last `window` coarse
  * steps.  Runs the forward from the context's current state with a

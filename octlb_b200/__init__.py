@@ -187,6 +187,45 @@ def plan(mesh, omega, precision=FP32, stream_mode=STREAM_ROTATE, drag=False):
     return [dict(zip(keys, [buf[1 + 10 * l + k] for k in range(10)])) for l in range(nl)]
 
 
+_VTK_FIELDS = {"velocity": capi.VTK_VELOCITY, "density": capi.VTK_DENSITY, "pressure": capi.VTK_PRESSURE}
+
+
+def vtk_write_block(path, bounds, fields):
+    """One StructuredGrid .vts (octlb_vtk_write_block): fields is a list of
+    (name, values [nx][ny][nz] or [nx][ny][nz][c]) on the cells of a block
+    with the given bounds (x_min, y_min, z_min, x_max, y_max, z_max)."""
+    L = capi.lib()
+    arrs, names, comps = [], [], []
+    shape = None
+    for name, v in fields:
+        v = np.asarray(v, np.float64)
+        c = 1 if v.ndim == 3 else v.shape[3]
+        shape = v.shape[:3] if shape is None else shape
+        if v.shape[:3] != shape:
+            raise ValueError("all fields take the block's cell shape")
+        # file order: i (x) fastest, then j, then k
+        arrs.append(np.ascontiguousarray(np.transpose(v.reshape(shape + (c,)), (2, 1, 0, 3))).reshape(-1))
+        names.append(name.encode())
+        comps.append(c)
+    nx, ny, nz = shape
+    b = np.ascontiguousarray(bounds, np.float64)
+    data = (capi.F64P * len(arrs))(*[capi.ptr(a, ctypes.c_double) for a in arrs])
+    rc = L.octlb_vtk_write_block(str(path).encode(), nx, ny, nz, capi.ptr(b, ctypes.c_double), len(arrs),
+                                 (ctypes.c_char_p * len(names))(*names), (ctypes.c_int * len(comps))(*comps), data)
+    if rc:
+        raise OctlbError(rc, "vtk_write_block failed")
+
+
+def vtk_write_index(output_dir, base_name, step, vts_relative_paths):
+    """The .vtm of one timestep and its .pvd entry (octlb_vtk_write_index)."""
+    L = capi.lib()
+    p = [str(x).encode() for x in vts_relative_paths]
+    rc = L.octlb_vtk_write_index(str(output_dir).encode(), str(base_name).encode(), int(step), len(p),
+                                 (ctypes.c_char_p * max(len(p), 1))(*p))
+    if rc:
+        raise OctlbError(rc, "vtk_write_index failed")
+
+
 class GpuLattice:
     """One octlb_gpu context (include/octlb_gpu.h)."""
 
@@ -302,6 +341,15 @@ class GpuLattice:
         if f is not None and f.size != self._cells() * 3:
             raise ValueError("body force must hold n_blocks * n^3 * 3 values")
         self._check(self._L.octlb_gpu_set_body_force(self._h, capi.ptr(f, ctypes.c_double)))
+
+    def write_vtk(self, output_dir, base_name, step, fields=("velocity", "pressure"), rank=0, write_index=True):
+        """One .vts per block of the current rho / u (octlb_gpu_write_vtk),
+        plus the .vtm index and the .pvd entry of the step."""
+        mask = 0
+        for f in fields:
+            mask |= _VTK_FIELDS[f]
+        self._check(self._L.octlb_gpu_write_vtk(self._h, str(output_dir).encode(), str(base_name).encode(),
+                                                int(step), int(rank), mask, 1 if write_index else 0))
 
     def set_const_rho(self, on=True):
         """ConstRhoBGK (TimeLoop's use_const_rho_bgk): before the first

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liboctlb_b200.so")
-SOURCES = ["lbm_kernels.cu", "lbm_bulk.cu", "lbm_adjoint.cu", "octlb_ctx.cu", "forest.cpp"]
+SOURCES = ["lbm_kernels.cu", "lbm_bulk.cu", "lbm_adjoint.cu", "octlb_ctx.cu", "forest.cpp", "vtk_writer.cpp"]
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -57,6 +57,9 @@ class AdjParams(ctypes.Structure):
                 ("checkpoint_interval", ctypes.c_int), ("component", ctypes.c_int)]
 
 
+VTK_VELOCITY, VTK_DENSITY, VTK_PRESSURE = 1, 2, 4
+
+
 class Params(ctypes.Structure):
     _fields_ = [
         ("omega", ctypes.c_double), ("precision", ctypes.c_int), ("stream_mode", ctypes.c_int),
@@ -85,6 +88,13 @@ def lib():
         "octlb_gpu_set_populations": (ctypes.c_int, [P, F64P]),
         "octlb_gpu_set_body_force": (ctypes.c_int, [P, F64P]),
         "octlb_gpu_set_const_rho": (ctypes.c_int, [P, ctypes.c_int]),
+        "octlb_gpu_write_vtk": (ctypes.c_int, [P, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int]),
+        "octlb_vtk_write_block": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, F64P,
+                                                 ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), I32P,
+                                                 ctypes.POINTER(F64P)]),
+        "octlb_vtk_write_index": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.POINTER(ctypes.c_char_p)]),
         "octlb_gpu_average_rho": (ctypes.c_int, [P, F64P]),
         "octlb_gpu_adjoint": (ctypes.c_int, [P, ctypes.POINTER(AdjParams), F64P, F64P, F64P]),
         "octlb_gpu_get_populations": (ctypes.c_int, [P, F64P]),

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <filesystem>
 #include <map>
 #include <memory>
 #include <set>
@@ -241,6 +242,7 @@ struct octlb_ctx {
   std::vector<Level> levels;
   std::vector<int> blk_level, blk_local;
   std::vector<uint8_t> kinds;
+  std::vector<double> bounds;       // [n_blocks][6] leaf bounds (VTK output)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   // Restrictions not launched yet: each shares the next coupler launch unless
@@ -2033,6 +2035,7 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
   if (rc) { *out = ctx.release(); return rc; }
   ctx->n = t->n;
   ctx->n_blocks = t->n_blocks;
+  if (t->bounds) ctx->bounds.assign(t->bounds, t->bounds + 6 * static_cast<size_t>(t->n_blocks));
   ctx->precision = p->precision;
   ctx->stream_mode = p->stream_mode;
   ctx->periodic = t->periodic;
@@ -2216,6 +2219,58 @@ int octlb_gpu_get_fields(octlb_ctx* ctx, double* rho, double* u) {
   if (int rc = check_device_error(ctx)) return rc;
   return ctx->precision == OCTLB_FP32 ? gather_impl<float>(ctx, nullptr, rho, u)
                                       : gather_impl<__half>(ctx, nullptr, rho, u);
+}
+
+int octlb_gpu_write_vtk(octlb_ctx* ctx, const char* output_dir, const char* base_name, int step, int rank,
+                        int fields, int write_index) {
+  if (!ctx || !output_dir || !base_name || rank < 0) return OCTLB_EINVAL;
+  if (fields <= 0 || (fields & ~(OCTLB_VTK_VELOCITY | OCTLB_VTK_DENSITY | OCTLB_VTK_PRESSURE)))
+    return fail(ctx, OCTLB_EINVAL, "write_vtk: fields is a nonzero mask of OCTLB_VTK_*");
+  if (ctx->bounds.size() != 6 * static_cast<size_t>(ctx->n_blocks))
+    return fail(ctx, OCTLB_EINVAL, "write_vtk: the tables gave no block bounds");
+  const int n = ctx->n;
+  const long long n3 = static_cast<long long>(n) * n * n;
+  std::vector<double> rho(static_cast<size_t>(ctx->n_blocks * n3)), u(rho.size() * 3);
+  if (int rc = octlb_gpu_get_fields(ctx, rho.data(), u.data())) return rc;
+  std::error_code ec;
+  std::filesystem::create_directories(output_dir, ec);
+  // AmrVtkWriter's names (amr_vtk_writer.cpp): base_r<rank>_oct<id>_T<step, 5 digits>.vts
+  char tag[16];
+  std::snprintf(tag, sizeof(tag), "%05d", step);
+  std::vector<std::string> rel;
+  std::vector<double> vel(static_cast<size_t>(n3) * 3), den(static_cast<size_t>(n3)), pre(static_cast<size_t>(n3));
+  for (int b = 0; b < ctx->n_blocks; ++b) {
+    // cell (i, j, k) of the file (i fastest) is core cell (x, y, z) = (i, j, k)
+    size_t c = 0;
+    for (int k = 0; k < n; ++k)
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i, ++c) {
+          const size_t s = static_cast<size_t>(b * n3 + (static_cast<long long>(i) * n + j) * n + k);
+          for (int d = 0; d < 3; ++d) vel[3 * c + d] = u[3 * s + d];
+          den[c] = rho[s];
+          pre[c] = rho[s] * (1.0 / 3.0);  // p = rho c_s^2 (VtkPressureField)
+        }
+    const char* names[3];
+    int comps[3];
+    const double* data[3];
+    int nf = 0;
+    if (fields & OCTLB_VTK_VELOCITY) { names[nf] = "velocity"; comps[nf] = 3; data[nf++] = vel.data(); }
+    if (fields & OCTLB_VTK_DENSITY) { names[nf] = "density"; comps[nf] = 1; data[nf++] = den.data(); }
+    if (fields & OCTLB_VTK_PRESSURE) { names[nf] = "pressure"; comps[nf] = 1; data[nf++] = pre.data(); }
+    const std::string name = std::string(base_name) + "_r" + std::to_string(rank) + "_oct" + std::to_string(b) +
+                             "_T" + tag + ".vts";
+    const int rc = octlb_vtk_write_block((std::string(output_dir) + "/" + name).c_str(), n, n, n,
+                                         &ctx->bounds[6 * static_cast<size_t>(b)], nf, names, comps, data);
+    if (rc) return fail(ctx, rc, "write_vtk: cannot write " + name);
+    rel.push_back(name);
+  }
+  if (write_index) {
+    std::vector<const char*> p;
+    for (const std::string& r : rel) p.push_back(r.c_str());
+    const int rc = octlb_vtk_write_index(output_dir, base_name, step, static_cast<int>(p.size()), p.data());
+    if (rc) return fail(ctx, rc, "write_vtk: cannot write the .vtm / .pvd index");
+  }
+  return OCTLB_OK;
 }
 
 int octlb_gpu_force(octlb_ctx* ctx, double out[3]) {

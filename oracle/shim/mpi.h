@@ -24,6 +24,7 @@ typedef struct { int source, tag, error; } MPI_Status;
 #define MPI_BYTE 1
 #define MPI_INT 2
 #define MPI_DOUBLE 3
+#define MPI_CHAR 4
 #define MPI_MAX 10
 #define MPI_SUM 11
 #define MPI_TAG_UB 100
@@ -31,13 +32,24 @@ typedef struct { int source, tag, error; } MPI_Status;
 #define MPI_STATUSES_IGNORE ((MPI_Status*)0)
 
 inline int octlb_shim_mpi_sizeof(MPI_Datatype t) {
-  return t == MPI_BYTE ? 1 : t == MPI_INT ? 4 : 8;
+  return (t == MPI_BYTE || t == MPI_CHAR) ? 1 : t == MPI_INT ? 4 : 8;
 }
 inline int MPI_Comm_rank(MPI_Comm, int* r) { *r = 0; return 0; }
 inline int MPI_Comm_size(MPI_Comm, int* s) { *s = 1; return 0; }
 inline int MPI_Allreduce(const void* in, void* out, int n, MPI_Datatype t,
                          MPI_Op, MPI_Comm) {
   if (in != MPI_IN_PLACE) std::memcpy(out, in, (size_t)n * octlb_shim_mpi_sizeof(t));
+  return 0;
+}
+// Gathers over one rank: the local contribution is the whole result.
+inline int MPI_Allgather(const void* in, int n, MPI_Datatype t, void* out, int, MPI_Datatype, MPI_Comm) {
+  std::memcpy(out, in, (size_t)n * octlb_shim_mpi_sizeof(t));
+  return 0;
+}
+inline int MPI_Allgatherv(const void* in, int n, MPI_Datatype t, void* out, const int*, const int* displs,
+                          MPI_Datatype, MPI_Comm) {
+  std::memcpy(static_cast<char*>(out) + (size_t)displs[0] * octlb_shim_mpi_sizeof(t), in,
+              (size_t)n * octlb_shim_mpi_sizeof(t));
   return 0;
 }
 [[noreturn]] inline void octlb_shim_mpi_p2p() {
