@@ -378,3 +378,27 @@ def test_periodic_three_level_forest_matches_reference(ob, ref, prec, tol):
     assert rel(u_g, u_r) <= tol
     assert c == cr and s == sr
     assert c[2] == steps * 4 and c[3] == 2 * c[2] and c[4] == 4 * c[2]
+
+
+def test_host_staging_reuse_across_calls(ob):
+    """set/get_populations and get_fields stage through FP64 buffers the
+    context keeps: calls of different sizes in any order give the values a
+    fresh context gives."""
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=8)
+    rng = np.random.default_rng(11)
+    state = init + 1e-3 * rng.standard_normal(init.shape)
+    lat = ob.GpuLattice(mesh, info["omega"], init_pops=init)
+    lat.advance(2)
+    rho1, u1 = (a.copy() for a in lat.get_fields())      # fields staging first
+    pops = lat.get_populations().copy()                    # then the larger populations staging
+    rho2, u2 = lat.get_fields()
+    assert np.array_equal(rho1, rho2) and np.array_equal(u1, u2)
+    rho_p, u_p = oracle.rho_u(pops)
+    assert rel(rho_p, rho1) <= 1e-12 and rel(u_p, u1) <= 1e-10
+    lat.set_populations(state)
+    fresh = ob.GpuLattice(mesh, info["omega"], init_pops=state)
+    assert np.array_equal(lat.get_populations(), fresh.get_populations())
+    assert np.array_equal(lat.get_fields()[0], fresh.get_fields()[0])
+    lat.close()
+    fresh.close()
