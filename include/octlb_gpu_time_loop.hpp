@@ -9,6 +9,9 @@
 //   loop.advance_one();
 //   loop.counters();  loop.max_level();
 //   auto f = loop.force_on_fluid();     // MomentumExchangeDrag::force_on_fluid_if
+//   octlb::GpuTimeLoop cav(tables, params, init_pops, true);   // use_const_rho_bgk
+//   cav.average_rho();                  // TimeLoop::average_rho
+//   loop.write_vtk("out", "cylinder3d", it);   // AmrVtkWriter::WriteTimestep + WriteVtmAndPvd
 //
 // Errors surface as std::runtime_error, the reference's convention
 // (block_lattice.cpp:35-36, level_coupler.cpp:72-74).
@@ -31,9 +34,12 @@ struct GpuTimeLoopCounters {
 
 class GpuTimeLoop {
  public:
+  // use_const_rho_bgk: the TimeLoop constructor argument (time_loop.h:47-54),
+  // single-level meshes
   GpuTimeLoop(const octlb_tables& tables, const octlb_params& params,
-              const double* init_pops = nullptr) {
-    const int rc = octlb_gpu_create(&tables, &params, init_pops, &ctx_);
+              const double* init_pops = nullptr, bool use_const_rho_bgk = false) {
+    int rc = octlb_gpu_create(&tables, &params, init_pops, &ctx_);
+    if (rc == OCTLB_OK && use_const_rho_bgk) rc = octlb_gpu_set_const_rho(ctx_, 1);
     if (rc != OCTLB_OK) {
       const std::string msg = ctx_ ? octlb_gpu_last_error(ctx_) : "octlb_gpu_create failed";
       octlb_gpu_destroy(ctx_);
@@ -79,6 +85,18 @@ class GpuTimeLoop {
     double a[4];
     check(octlb_gpu_audit(ctx_, a));
     return a[0];
+  }
+  // TimeLoop::average_rho() (time_loop.h:87-88): 1 without ConstRhoBGK
+  double average_rho() {
+    double a = 1.0;
+    check(octlb_gpu_average_rho(ctx_, &a));
+    return a;
+  }
+  // One .vts per block (base_r<rank>_oct<id>_T<step>.vts), the step's .vtm and
+  // its .pvd entry, as AmrVtkWriter::WriteTimestep + WriteVtmAndPvd
+  void write_vtk(const std::string& output_dir, const std::string& base_name, int step,
+                 int fields = OCTLB_VTK_VELOCITY | OCTLB_VTK_PRESSURE, int rank = 0, bool write_index = true) {
+    check(octlb_gpu_write_vtk(ctx_, output_dir.c_str(), base_name.c_str(), step, rank, fields, write_index ? 1 : 0));
   }
   octlb_ctx* handle() { return ctx_; }
 

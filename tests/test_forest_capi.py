@@ -166,6 +166,12 @@ def test_cpp_adapter_compiles_links_and_reports_errors(ob, tmp_path):
     src.write_text(r'''
 #include "octlb_gpu_time_loop.hpp"
 #include <cstdio>
+// the whole adapter surface compiles and links
+double use(octlb::GpuTimeLoop& loop) {
+  loop.advance_one();
+  loop.write_vtk("out", "case", 1);
+  return loop.average_rho() + loop.total_mass() + loop.force_on_fluid()[0] + loop.counters().collide.size();
+}
 int main() {
   octlb_tables t{};
   octlb_params p{};
