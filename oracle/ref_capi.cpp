@@ -40,6 +40,9 @@
 #include "src/solver/lbm/time_loop/time_loop.h"
 #include "src/solver/field/ghost_schedule.h"
 #include "src/mesh/topology/face_pair_list.h"
+#ifndef OCTLB_REF_TLM
+#include "src/solver/lbm/bc_installer.h"
+#endif
 
 namespace octlb {
 void OracleForestInject(OctreeForest& forest, const std::vector<int>& levels,
@@ -220,6 +223,7 @@ struct Sim {
   std::unique_ptr<DomainBoundaryHandler> bc;
   std::unique_ptr<TimeLoop> loop;
   double omega = 0.0;
+  std::vector<TreeBoundaryFace> tree_faces;
 };
 
 // Sum of MomentumExchangeDrag::force_on_fluid_if over all blocks (see
@@ -417,6 +421,7 @@ void* ref_sim_new(int n_oct, const int* levels, const f64* bounds, int n_sl,
                                        *s->bc, omega);
   s->loop->set_snapshot_post_collide(true);
   s->omega = omega;
+  s->tree_faces = tbv;
   return s;
 }
 // The TimeLoop rebuilt with use_const_rho_bgk (ConstRhoStatsScope::
@@ -429,6 +434,36 @@ void ref_sim_set_const_rho(void* h, int on) {
   s->loop->set_snapshot_post_collide(true);
 }
 f64 ref_sim_average_rho(void* h) { return to_f64(static_cast<Sim*>(h)->loop->average_rho()); }
+
+#ifndef OCTLB_REF_TLM
+// The reference's own domain boundary conditions in place of the restated
+// fills: a ConcreteDomainBoundaryHandler (domain_boundary_handler.cpp) over
+// every tree-boundary face, face f in FaceDir order (x-, x+, y-, y+, z-, z+)
+// with spec type types[f] (DomainBcType), wall velocity u_wall[3f .. 3f + 2]
+// and target density rho_target[f]; the face cells stamped with the spec's
+// BcKind (bc::StampTreeBoundaryCells, bc_installer.h:96-140) and the TimeLoop
+// rebuilt around the handler, optionally with ConstRhoBGK -- the cavity3d
+// construction (cavity3d_case.h:152-197).  padding_mode: OverlapPaddingMode.
+// Before the first advance.
+void ref_sim_set_fd_boundary(void* h, const int* types, const f64* u_wall, const f64* rho_target,
+                             int padding_mode, int const_rho) {
+  auto* s = static_cast<Sim*>(h);
+  std::vector<DomainBcSpec> specs(6);
+  for (int f = 0; f < 6; ++f) {
+    specs[f].face = static_cast<FaceDir>(f);
+    specs[f].type = static_cast<DomainBcType>(types[f]);
+    specs[f].u_wall = {u_wall[3 * f], u_wall[3 * f + 1], u_wall[3 * f + 2]};
+    specs[f].rho_target = rho_target[f];
+  }
+  bc::StampTreeBoundaryCells(*s->blocks, s->tree_faces, specs, s->n, s->n, s->n);
+  s->loop.reset();
+  s->bc = std::make_unique<ConcreteDomainBoundaryHandler>(*s->blocks, s->tree_faces, specs, s->n, s->n, s->n,
+                                                          s->omega, static_cast<OverlapPaddingMode>(padding_mode));
+  s->loop = std::make_unique<TimeLoop>(*s->forest, *s->blocks, *s->ghosts, *s->coupler, *s->bc, s->omega,
+                                       const_rho != 0);
+  s->loop->set_snapshot_post_collide(true);
+}
+#endif
 void ref_sim_free(void* h) {
   auto* s = static_cast<Sim*>(h);
   // TimeLoop / coupler / ghosts hold references: tear down in reverse order.

@@ -1,0 +1,106 @@
+"""The reference's own domain boundary conditions in the oracle: a
+ConcreteDomainBoundaryHandler (Skordos InterpolatedVelocity and pressure
+Dirichlet, interpolated_velocity.h:571-1037, domain_boundary_handler.cpp:
+60-89) installed in the reference TimeLoop by oracle.Sim.set_fd_boundary.
+The GPU path does not have these conditions yet. These CPU tests pin the
+oracle it will be checked against, on properties of the reconstruction:
+* a rest state is a fixed point, as in the reference's
+  test_interpolated_velocity_compute_rho.cpp equilibrium cases;
+* after the post-stream reconstruction every boundary cell carries its
+  prescribed velocity, and every plane pressure cell its target density;
+* ConstRhoBGK's statistics include the boundary cells."""
+import numpy as np
+
+from oracle import oracle
+
+S = oracle.Sim
+
+
+def faces_mask(n):
+    m = np.zeros((n, n, n), bool)
+    m[0] = m[-1] = True
+    m[:, 0] = m[:, -1] = True
+    m[:, :, 0] = m[:, :, -1] = True
+    return m
+
+
+def plane_x_max(n):
+    m = np.zeros((n, n, n), bool)
+    m[-1, 1:-1, 1:-1] = True
+    return m
+
+
+def test_rest_state_is_a_fixed_point(ref):
+    """Every face an InterpolatedVelocity wall at rest: the equilibrium at
+    rho = 1 stays exactly (the reference's CornerEdge_Equilibrium tests)."""
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=16, n=16, lid=0.0, tau=0.6)
+    sim = S(ref, mesh, info["omega"], init)
+    sim.set_fd_boundary([S.INTERPOLATED_VELOCITY] * 6)
+    sim.advance(10)
+    assert np.abs(sim.core()).max() == 0.0
+
+
+def test_moving_lid_boundary_cells_carry_the_prescribed_velocity(ref):
+    """cavity3d's boundary: InterpolatedVelocity on all faces, the lid's
+    velocity on the interior top-face cells only (edges and corners of the
+    top face stay at rest, interpolated_velocity.h:64-118)."""
+    from octlb_b200 import cases
+    n = 16
+    mesh, init, info = cases.cavity_forest(cells=n, n=n, lid=0.05, tau=0.6)
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    sim = S(ref, mesh, info["omega"], init)
+    sim.set_fd_boundary([S.INTERPOLATED_VELOCITY] * 6, u)
+    sim.advance(50)
+    rho, vel = oracle.rho_u(sim.core())
+    face = faces_mask(n)
+    expect = np.zeros((n, n, n, 3))
+    expect[1:-1, -1, 1:-1, 0] = 0.05
+    assert np.abs(vel[0][face] - expect[face]).max() <= 1e-14
+    assert np.abs(vel[0][~face]).max() > 0.01              # the lid drives the cavity
+    assert abs(rho[0].mean() - 1.0) < 1e-3                 # the FD walls hold the mass close
+
+
+def test_pressure_outlet_cells_carry_the_target_density(ref):
+    """Lid-driven cavity with a pressure Dirichlet outlet on x+ (rho_target
+    1): the outlet's plane cells hold the target density.  Without an inlet
+    field the FD path prescribes only the lid's velocity, on the interior
+    top-face cells (PrescribedBoundaryU, interpolated_velocity.h:69-117): the
+    x- wall's u_wall is not used, so its cells stay at rest."""
+    from octlb_b200 import cases
+    n = 16
+    mesh, init, info = cases.cavity_forest(cells=n, n=n, lid=0.0, tau=0.6)
+    types = [S.INTERPOLATED_VELOCITY, S.INTERPOLATED_PRESSURE] + [S.INTERPOLATED_VELOCITY] * 4
+    u = np.zeros((6, 3))
+    u[0, 0] = 0.02                                          # ignored without an inlet field
+    u[3, 0] = 0.05                                          # the lid
+    sim = S(ref, mesh, info["omega"], init)
+    sim.set_fd_boundary(types, u, rho_target=np.ones(6))
+    sim.advance(40)
+    rho, vel = oracle.rho_u(sim.core())
+    assert np.abs(rho[0][plane_x_max(n)] - 1.0).max() <= 1e-14
+    assert np.abs(vel[0][0, 1:-1, 1:-1]).max() <= 1e-14
+    assert np.abs(vel[0][1:-1, -1, 1:-1, 0] - 0.05).max() <= 1e-14
+    assert np.abs(vel[0][~faces_mask(n)]).max() > 1e-3     # the lid drives the flow
+
+
+def test_const_rho_statistics_include_the_boundary_cells(ref):
+    """With ConstRhoBGK and the FD handler (kFluidAndBoundary statistics,
+    time_loop.h:109-115) the average density moves off 1 after a step from a
+    compressed state, and the collide holds the mean density near 1."""
+    from octlb_b200 import cases, C
+    n = 16
+    mesh, init, info = cases.cavity_forest(cells=n, n=n, lid=0.05, tau=0.6)
+    Cf = C.astype(np.float64)
+    w = np.where(np.abs(Cf).sum(1) == 0, 1 / 3, np.where(np.abs(Cf).sum(1) == 1, 1 / 18, 1 / 36))
+    init = np.broadcast_to(w * 1.02 - w, init.shape).copy()
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    sim = S(ref, mesh, info["omega"], init)
+    sim.set_fd_boundary([S.INTERPOLATED_VELOCITY] * 6, u, const_rho=True)
+    sim.advance(1)
+    assert abs(sim.average_rho() - 1.02) < 5e-3
+    sim.advance(30)
+    rho, _ = oracle.rho_u(sim.core())
+    assert abs(rho[0].mean() - 1.0) < 2e-3
