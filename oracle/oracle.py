@@ -196,6 +196,23 @@ class Sim:
         """TimeLoop::average_rho()."""
         return float(self.L.ref_sim_average_rho(self.h))
 
+    def advance_phases(self):
+        """One advance_one of a single-level mesh; the core populations after
+        the stream and after the post-stream boundary pass (the two sides of
+        the FD reconstruction), [n_blocks][n][n][n][19] each."""
+        n = self.mesh.n
+        a = np.zeros((self.mesh.n_blocks, n, n, n, Q))
+        b = np.zeros_like(a)
+        self.L.ref_sim_advance_phases(self.h, _p(a), _p(b))
+        return a, b
+
+    def kinds(self):
+        """BcKind of every core cell, [n_blocks][n][n][n]."""
+        n = self.mesh.n
+        out = np.zeros((self.mesh.n_blocks, n, n, n), np.uint8)
+        self.L.ref_sim_get_kinds(self.h, _p(out, ctypes.c_uint8))
+        return out
+
     # DomainBcType and OverlapPaddingMode (domain_boundary_handler.h:14-36)
     NO_SLIP, MOVING_LID, INTERPOLATED_VELOCITY, OUTFLOW, INTERPOLATED_PRESSURE = range(5)
     PADDING_POST_STREAM, PADDING_MIRROR, PADDING_HYBRID = range(3)

@@ -463,6 +463,31 @@ void ref_sim_set_fd_boundary(void* h, const int* types, const f64* u_wall, const
                                        const_rho != 0);
   s->loop->set_snapshot_post_collide(true);
 }
+
+void ref_sim_get_core(void* h, f64* out);
+
+// BcKind of every core cell, [oct][n^3] (after set_fd_boundary's stamping).
+void ref_sim_get_kinds(void* h, uint8_t* out) {
+  auto* s = static_cast<Sim*>(h);
+  const int n = s->n, n3 = n * n * n;
+  for (label id = 0; id < s->blocks->size(); ++id)
+    for (int x = 0; x < n; ++x)
+      for (int y = 0; y < n; ++y)
+        for (int z = 0; z < n; ++z)
+          out[(std::size_t)id * n3 + (x * n + y) * n + z] = static_cast<uint8_t>((*s->blocks)[id].bc_kind(x, y, z));
+}
+
+// One advance_one of a single-level mesh through TimeLoop::advance_one_with_hooks
+// (time_loop.h:278-310), with the core populations after the stream
+// (after_stream) and after the post-stream boundary pass (after_post_stream),
+// [oct][n^3][19] each: the two sides of the FD reconstruction.
+void ref_sim_advance_phases(void* h, f64* after_stream, f64* after_post_stream) {
+  auto* s = static_cast<Sim*>(h);
+  s->loop->advance_one_with_hooks([&](TimeLoop::FlatPhase ph) {
+    if (ph == TimeLoop::FlatPhase::kAfterStream) ref_sim_get_core(h, after_stream);
+    if (ph == TimeLoop::FlatPhase::kAfterPostStream) ref_sim_get_core(h, after_post_stream);
+  });
+}
 #endif
 void ref_sim_free(void* h) {
   auto* s = static_cast<Sim*>(h);

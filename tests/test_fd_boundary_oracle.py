@@ -104,3 +104,57 @@ def test_const_rho_statistics_include_the_boundary_cells(ref):
     sim.advance(30)
     rho, _ = oracle.rho_u(sim.core())
     assert abs(rho[0].mean() - 1.0) < 2e-3
+
+
+def _pass_states(ref, types, u, steps=20):
+    from octlb_b200 import cases
+    n = 16
+    mesh, init, info = cases.cavity_forest(cells=n, n=n, lid=0.0, tau=0.6)
+    sim = S(ref, mesh, info["omega"], init)
+    sim.set_fd_boundary(types, u, rho_target=np.ones(6))
+    sim.advance(steps)
+    before, after = sim.advance_phases()
+    return before[0], after[0], sim.kinds()[0], info["omega"]
+
+
+def test_restated_pass_matches_the_reference(ref):
+    """oracle/fd_boundary.py (the post-stream reconstruction as plane, edge
+    and corner phases, each reading a neighbour's rewritten populations
+    exactly when the reference's in-place walk has already rewritten it)
+    takes the reference's state after the stream to its state after the
+    pass: the moving-lid cavity, and the same with a pressure outlet."""
+    from oracle import fd_boundary
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    for types in ([S.INTERPOLATED_VELOCITY] * 6,
+                  [S.INTERPOLATED_VELOCITY, S.INTERPOLATED_PRESSURE] + [S.INTERPOLATED_VELOCITY] * 4):
+        before, after, kinds, omega = _pass_states(ref, types, u)
+        assert np.abs(after - before).max() > 1e-3            # the pass rewrites the boundary
+        got = fd_boundary.reconstruct(before, kinds, omega, u_lid=u[3])
+        assert np.abs(got - after).max() <= 1e-14
+
+
+def test_the_walk_order_matters(ref):
+    """Reading every neighbour's original populations instead (no order)
+    misses the reference by far more than rounding: edges and corners read
+    densities of boundary cells the walk has already rewritten."""
+    from oracle import fd_boundary
+
+    class NoOrder(fd_boundary.Block):
+        def pops(self, cell, reader):
+            return self.f_pre[cell]
+
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    before, after, kinds, omega = _pass_states(ref, [S.INTERPOLATED_VELOCITY] * 6, u)
+    b = NoOrder(before, kinds, omega, u_lid=u[3])
+    cells = [tuple(c) for c in np.argwhere(np.isin(kinds, (fd_boundary.VELOCITY, fd_boundary.PRESSURE)))]
+    count = {c: sum(1 for f in b.faces(*c) if f) for c in cells}
+    for want, fn in ((1, b.plane), (2, b.edge), (3, b.corner)):
+        for c in cells:
+            if count[c] == want:
+                fn(c)
+    got = before.copy()
+    for c, f in b.new.items():
+        got[c] = f
+    assert np.abs(got - after).max() > 1e-4
