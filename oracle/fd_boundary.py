@@ -236,3 +236,46 @@ def reconstruct(f_pre, kinds, omega, u_lid=(0.0, 0.0, 0.0), rho_target=None, hal
     for c, f in b.new.items():
         out[c] = f
     return out
+
+
+def collide(f, kinds, omega, u_lid=(0.0, 0.0, 0.0)):
+    """The collide of a block with the FD domain conditions, OpenLB order
+    (BcDispatcher::collide, bc_dispatcher.h:33-79): kBulk cells f <- (1 - omega)
+    f + omega f_eq(rho, u) (lbm.h:395-403) at their own moments; velocity-
+    Dirichlet cells the same at the prescribed velocity and the density of
+    BoundaryCellStatisticRho (interpolated_velocity.h:815-884: velocityBMRho
+    on plane cells, 1 + sum f on edges and corners); other kinds unchanged.
+    Every cell reads only itself, so the order does not matter."""
+    b = Block(f, kinds, omega, u_lid)
+    out = b.f_pre.copy()
+    n = b.n
+    for x in range(n):
+        for y in range(n):
+            for z in range(n):
+                c = (x, y, z)
+                k = b.kinds[c]
+                g = b.f_pre[c]
+                if k == 0:
+                    rho = 1.0 + g.sum()
+                    u = (C.T @ g) / rho
+                elif k == VELOCITY:
+                    u = b.prescribed_u(*c)
+                    fl = b.flat(*c)
+                    rho = _velocity_bm_rho(g, fl[0], fl[1], u) if fl else 1.0 + g.sum()
+                else:
+                    continue
+                out[c] = g * (1.0 - omega) + omega * _eq(rho, u)
+    return out
+
+
+def stream_padded(p):
+    """The torus-rotate stream of a padded block ([n+2][n+2][n+2][19], halo 1):
+    population i of padded cell s comes from cell s - (c_x (n+2)^2 + c_y (n+2)
+    + c_z), wrapped over the block's linear index
+    (OpenLbPaddedBlockStreamSourceLinear; block_lattice.cpp:554-575)."""
+    m = p.shape[0]
+    flat = p.reshape(-1, 19)
+    out = np.empty_like(flat)
+    for i in range(19):
+        out[:, i] = np.roll(flat[:, i], int(C[i][0] * m * m + C[i][1] * m + C[i][2]))
+    return out.reshape(p.shape)

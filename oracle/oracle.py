@@ -206,6 +206,15 @@ class Sim:
         self.L.ref_sim_advance_phases(self.h, _p(a), _p(b))
         return a, b
 
+    def advance_phases_padded(self):
+        """One advance_one of a single-level mesh; the padded populations
+        (halo 1) at the start and after collide, ghost exchange, stream and
+        the post-stream pass: [5][n_blocks][n+2][n+2][n+2][19]."""
+        m = self.mesh.n + 2
+        out = np.zeros((5, self.mesh.n_blocks, m, m, m, Q))
+        self.L.ref_sim_advance_phases_padded(self.h, _p(out))
+        return out
+
     def kinds(self):
         """BcKind of every core cell, [n_blocks][n][n][n]."""
         n = self.mesh.n

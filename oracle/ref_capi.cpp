@@ -465,6 +465,24 @@ void ref_sim_set_fd_boundary(void* h, const int* types, const f64* u_wall, const
 }
 
 void ref_sim_get_core(void* h, f64* out);
+void ref_sim_get_padded(void* h, f64* out);
+
+// One advance_one of a single-level mesh with the padded block populations
+// (halo 1, [oct][(n+2)^3][19]) at the start and after each phase of
+// TimeLoop::advance_one_with_hooks: out[0] start, [1] collide (boundary cells
+// first, the OpenLB order), [2] ghost exchange, [3] stream, [4] post-stream
+// boundary pass.
+void ref_sim_advance_phases_padded(void* h, f64* out) {
+  auto* s = static_cast<Sim*>(h);
+  const std::size_t m = (std::size_t)s->blocks->size() * (s->n + 2) * (s->n + 2) * (s->n + 2) * Q;
+  ref_sim_get_padded(h, out);
+  s->loop->advance_one_with_hooks([&](TimeLoop::FlatPhase ph) {
+    if (ph == TimeLoop::FlatPhase::kAfterCollide) ref_sim_get_padded(h, out + m);
+    if (ph == TimeLoop::FlatPhase::kAfterGhostExchange) ref_sim_get_padded(h, out + 2 * m);
+    if (ph == TimeLoop::FlatPhase::kAfterStream) ref_sim_get_padded(h, out + 3 * m);
+    if (ph == TimeLoop::FlatPhase::kAfterPostStream) ref_sim_get_padded(h, out + 4 * m);
+  });
+}
 
 // BcKind of every core cell, [oct][n^3] (after set_fd_boundary's stamping).
 void ref_sim_get_kinds(void* h, uint8_t* out) {

@@ -158,3 +158,41 @@ def test_the_walk_order_matters(ref):
     for c, f in b.new.items():
         got[c] = f
     assert np.abs(got - after).max() > 1e-4
+
+
+def test_fd_step_restated_phase_by_phase(ref):
+    """A whole step of the reference with the FD conditions, single block
+    (halo 1, torus-rotate stream), from its own padded state after each phase
+    of TimeLoop::advance_one_with_hooks: the collide (Dirichlet cells at the
+    prescribed velocity), no ghost exchange on one block, the linear-rotate
+    stream over the padded block (exact, halo included), the post-stream
+    padding fill (no change at halo 1) and the reconstruction; composed, the
+    restated step gives the reference's state after the step."""
+    from octlb_b200 import cases
+    from oracle import fd_boundary as fb
+    n = 16
+    mesh, init, info = cases.cavity_forest(cells=n, n=n, lid=0.0, tau=0.6)
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    sim = S(ref, mesh, info["omega"], init)
+    sim.set_fd_boundary([S.INTERPOLATED_VELOCITY] * 6, u)
+    sim.advance(20)
+    P = sim.advance_phases_padded()[:, 0]
+    kinds = sim.kinds()[0]
+    om = info["omega"]
+    core = (slice(1, -1),) * 3
+    collided = fb.collide(P[0][core], kinds, om, u[3])
+    assert np.abs(collided - P[1][core]).max() <= 1e-15
+    halo = np.ones((n + 2,) * 3, bool)
+    halo[core] = False
+    assert np.array_equal(P[1][halo], P[0][halo])          # the halo is not collided
+    assert np.array_equal(P[2], P[1])                      # nothing to exchange on one block
+    assert np.array_equal(fb.stream_padded(P[2]), P[3])    # exact, halo included
+    assert np.array_equal(P[4][halo], P[3][halo])          # the padding fill leaves halo 1 as it is
+    assert np.abs(fb.reconstruct(P[3][core], kinds, om, u_lid=u[3]) - P[4][core]).max() <= 1e-14
+    # the whole step restated
+    p = P[0].copy()
+    p[core] = fb.collide(p[core], kinds, om, u[3])
+    p = fb.stream_padded(p)
+    p[core] = fb.reconstruct(p[core], kinds, om, u_lid=u[3])
+    assert np.abs(p - P[4]).max() <= 1e-14
