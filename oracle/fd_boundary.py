@@ -70,7 +70,7 @@ def _velocity_bm_rho(f, direction, orientation, u):
 class Block:
     """One block's kinds, prescribed boundary data and state for the pass."""
 
-    def __init__(self, f_pre, kinds, omega, u_lid=(0.0, 0.0, 0.0), rho_target=None, halo=1):
+    def __init__(self, f_pre, kinds, omega, u_lid=(0.0, 0.0, 0.0), rho_target=None, halo=1, inlets=None, t=0.0):
         self.f_pre = np.asarray(f_pre, np.float64)
         self.kinds = np.asarray(kinds)
         self.n = self.kinds.shape[0]
@@ -79,6 +79,9 @@ class Block:
         self.u_lid = np.asarray(u_lid, np.float64)
         self.rho_target = np.ones(6) if rho_target is None else np.asarray(rho_target, np.float64)
         self.stencil = min(int(halo), 2)  # kInterpolatedVelocityOverlap = 2
+        # face index (x-, x+, y-, y+, z-, z+) -> (u_const, ramp_end_t) of a uniform inlet
+        self.inlets = dict(inlets or {})
+        self.t = float(t)
         self.new = {}
 
     def inside(self, cell):
@@ -102,9 +105,26 @@ class Block:
         fs = [f for f in self.faces(x, y, z) if f]
         return fs[0] if len(fs) == 1 else None
 
+    @staticmethod
+    def ramp(t, t_end):
+        """PolynomialStartScale: 10 x^3 - 15 x^4 + 6 x^5, x = t / t_end in [0, 1]."""
+        if t_end <= 0.0:
+            return 1.0
+        x = min(max(t / t_end, 0.0), 1.0)
+        x2 = x * x
+        x3 = x2 * x
+        return x3 * (10.0 + x * (-15.0 + 6.0 * x))
+
     def prescribed_u(self, x, y, z):
-        # no inlet field: the lid's velocity on the interior top-face cells
+        # PrescribedBoundaryU (interpolated_velocity.h:69-117): the inlet field
+        # of the first face the cell touches that has one; else the lid's
+        # velocity on the interior top-face cells
         n1 = self.n - 1
+        for face, on in enumerate((x == 0, x == n1, y == 0, y == n1, z == 0, z == n1)):
+            if on and face in self.inlets:
+                u_const, t_end = self.inlets[face]
+                r = self.ramp(self.t, t_end)
+                return np.array([r * u_const[d] for d in range(3)])
         if y == n1 and 0 < x < n1 and 0 < z < n1:
             return self.u_lid.copy()
         return np.zeros(3)
@@ -221,11 +241,11 @@ class Block:
         self.write(cell, rho, self.compute_u(cell), du)
 
 
-def reconstruct(f_pre, kinds, omega, u_lid=(0.0, 0.0, 0.0), rho_target=None, halo=1):
+def reconstruct(f_pre, kinds, omega, u_lid=(0.0, 0.0, 0.0), rho_target=None, halo=1, inlets=None, t=0.0):
     """The block's populations after the pass: boundary cells (velocity or
     pressure Dirichlet on the block's faces) rewritten in three phases, the
     others unchanged."""
-    b = Block(f_pre, kinds, omega, u_lid, rho_target, halo)
+    b = Block(f_pre, kinds, omega, u_lid, rho_target, halo, inlets, t)
     cells = [tuple(c) for c in np.argwhere(np.isin(b.kinds, (VELOCITY, PRESSURE)))]
     count = {c: sum(1 for f in b.faces(*c) if f) for c in cells}
     for want, fn in ((1, b.plane), (2, b.edge), (3, b.corner)):

@@ -226,18 +226,22 @@ class Sim:
     NO_SLIP, MOVING_LID, INTERPOLATED_VELOCITY, OUTFLOW, INTERPOLATED_PRESSURE = range(5)
     PADDING_POST_STREAM, PADDING_MIRROR, PADDING_HYBRID = range(3)
 
-    def set_fd_boundary(self, types, u_wall=None, rho_target=None, padding_mode=2, const_rho=False):
+    def set_fd_boundary(self, types, u_wall=None, rho_target=None, padding_mode=2, const_rho=False, inlet_u=None,
+                        ramp_end_t=0.0):
         """The reference's ConcreteDomainBoundaryHandler on every tree-boundary
         face (faces in FaceDir order x-, x+, y-, y+, z-, z+): spec types,
         wall velocities [6][3], target densities [6]; the face cells stamped
         with the spec's BcKind and the TimeLoop rebuilt around the handler
-        (optionally with ConstRhoBGK).  Before the first advance."""
+        (optionally with ConstRhoBGK); faces with a nonzero inlet_u row [6][3]
+        take a uniform inlet of that velocity ramped over ramp_end_t steps.
+        Before the first advance."""
         t = np.ascontiguousarray(types, np.int32).reshape(6)
         u = np.zeros((6, 3)) if u_wall is None else np.ascontiguousarray(u_wall, np.float64).reshape(6, 3)
         r = np.ones(6) if rho_target is None else np.ascontiguousarray(rho_target, np.float64).reshape(6)
-        self._keep += [t, u, r]
+        iu = None if inlet_u is None else np.ascontiguousarray(inlet_u, np.float64).reshape(6, 3)
+        self._keep += [t, u, r, iu]
         self.L.ref_sim_set_fd_boundary(self.h, _p(t, ctypes.c_int), _p(u), _p(r), ctypes.c_int(padding_mode),
-                                       ctypes.c_int(1 if const_rho else 0))
+                                       ctypes.c_int(1 if const_rho else 0), _p(iu), ctypes.c_double(ramp_end_t))
 
     def set_body_force(self, force):
         """Body force [n_blocks][n^3][3] (or None): 3 w_i (c_i . F) added to the

@@ -444,9 +444,11 @@ f64 ref_sim_average_rho(void* h) { return to_f64(static_cast<Sim*>(h)->loop->ave
 // BcKind (bc::StampTreeBoundaryCells, bc_installer.h:96-140) and the TimeLoop
 // rebuilt around the handler, optionally with ConstRhoBGK -- the cavity3d
 // construction (cavity3d_case.h:152-197).  padding_mode: OverlapPaddingMode.
-// Before the first advance.
+// inlet_u (null: none): faces with a nonzero row take a UniformInletProfile
+// of that velocity ramped over ramp_end_t steps (inlet_velocity_field.h:
+// 128-162).  Before the first advance.
 void ref_sim_set_fd_boundary(void* h, const int* types, const f64* u_wall, const f64* rho_target,
-                             int padding_mode, int const_rho) {
+                             int padding_mode, int const_rho, const f64* inlet_u, f64 ramp_end_t) {
   auto* s = static_cast<Sim*>(h);
   std::vector<DomainBcSpec> specs(6);
   for (int f = 0; f < 6; ++f) {
@@ -454,6 +456,9 @@ void ref_sim_set_fd_boundary(void* h, const int* types, const f64* u_wall, const
     specs[f].type = static_cast<DomainBcType>(types[f]);
     specs[f].u_wall = {u_wall[3 * f], u_wall[3 * f + 1], u_wall[3 * f + 2]};
     specs[f].rho_target = rho_target[f];
+    if (inlet_u && (inlet_u[3 * f] != 0.0 || inlet_u[3 * f + 1] != 0.0 || inlet_u[3 * f + 2] != 0.0))
+      specs[f].inlet_field = std::make_shared<boundary::UniformInletProfile>(
+          std::array<double, 3>{inlet_u[3 * f], inlet_u[3 * f + 1], inlet_u[3 * f + 2]}, ramp_end_t);
   }
   bc::StampTreeBoundaryCells(*s->blocks, s->tree_faces, specs, s->n, s->n, s->n);
   s->loop.reset();

@@ -222,3 +222,31 @@ def test_restated_pass_matches_the_reference_per_block(ref):
     for b in range(mesh.n_blocks):
         got = fb.reconstruct(before[b], kinds[b], info["omega"], u_lid=u[3])
         assert np.abs(got - after[b]).max() <= 1e-14, b
+
+
+def test_uniform_inlet_with_ramp(ref):
+    """A uniform inlet field on x- (UniformInletProfile, inlet_velocity_field.h:
+    128-162) and a pressure outlet on x+: every x- cell, edges and corners
+    included, carries the ramped inlet velocity (the first face a cell touches
+    with an inlet field wins, interpolated_velocity.h:69-102), and the
+    restated pass matches the reference.  Steps taken through the hooks keep
+    the handler's time at the last advance_one's (19 after 20 steps)."""
+    from octlb_b200 import cases
+    from oracle import fd_boundary as fb
+    n = 16
+    mesh, init, info = cases.cavity_forest(cells=n, n=n, lid=0.0, tau=0.6)
+    types = [S.INTERPOLATED_VELOCITY, S.INTERPOLATED_PRESSURE] + [S.INTERPOLATED_VELOCITY] * 4
+    inlet = np.zeros((6, 3))
+    inlet[0, 0] = 0.02
+    for ramp_end, t in ((0.0, 0.0), (50.0, 19.0)):
+        sim = S(ref, mesh, info["omega"], init)
+        sim.set_fd_boundary(types, rho_target=np.ones(6), inlet_u=inlet, ramp_end_t=ramp_end)
+        sim.advance(20)
+        before, after = sim.advance_phases()
+        kinds = sim.kinds()[0]
+        got = fb.reconstruct(before[0], kinds, info["omega"], inlets={0: (inlet[0], ramp_end)}, t=t)
+        assert np.abs(got - after[0]).max() <= 1e-14
+        _, vel = oracle.rho_u(after)
+        r = fb.Block.ramp(t, ramp_end)
+        assert np.abs(vel[0][0, :, :, 0] - r * 0.02).max() <= 1e-14
+        assert (r == 1.0) == (ramp_end == 0.0)
