@@ -258,14 +258,20 @@ def reconstruct(f_pre, kinds, omega, u_lid=(0.0, 0.0, 0.0), rho_target=None, hal
     return out
 
 
-def collide(f, kinds, omega, u_lid=(0.0, 0.0, 0.0)):
+def collide(f, kinds, omega, u_lid=(0.0, 0.0, 0.0), average_rho=None, stats=None):
     """The collide of a block with the FD domain conditions, OpenLB order
     (BcDispatcher::collide, bc_dispatcher.h:33-79): kBulk cells f <- (1 - omega)
     f + omega f_eq(rho, u) (lbm.h:395-403) at their own moments; velocity-
     Dirichlet cells the same at the prescribed velocity and the density of
     BoundaryCellStatisticRho (interpolated_velocity.h:815-884: velocityBMRho
     on plane cells, 1 + sum f on edges and corners); other kinds unchanged.
-    Every cell reads only itself, so the order does not matter."""
+    Every cell reads only itself, so the order does not matter.
+
+    average_rho (ConstRhoBGK): kBulk cells take ratio (f_eq + t) - t +
+    (1 - omega)(f - f_eq), ratio = 1 + (1 - average_rho) / rho
+    (block_lattice.h:134-151); stats (a list) gets rho + 1 - average_rho per
+    kBulk cell and the raw boundary density per velocity-Dirichlet cell (the
+    kFluidAndBoundary scope)."""
     b = Block(f, kinds, omega, u_lid)
     out = b.f_pre.copy()
     n = b.n
@@ -284,7 +290,16 @@ def collide(f, kinds, omega, u_lid=(0.0, 0.0, 0.0)):
                     rho = _velocity_bm_rho(g, fl[0], fl[1], u) if fl else 1.0 + g.sum()
                 else:
                     continue
-                out[c] = g * (1.0 - omega) + omega * _eq(rho, u)
+                feq = _eq(rho, u)
+                if k == 0 and average_rho is not None:
+                    ratio = 1.0 + (1.0 - average_rho) / rho if rho > 1e-12 else 1.0
+                    out[c] = ratio * (feq + W) - W + (1.0 - omega) * (g - feq)
+                    if stats is not None:
+                        stats.append(rho + (1.0 - average_rho))
+                    continue
+                if k == VELOCITY and average_rho is not None and stats is not None:
+                    stats.append(rho)
+                out[c] = g * (1.0 - omega) + omega * feq
     return out
 
 

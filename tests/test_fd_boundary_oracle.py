@@ -250,3 +250,32 @@ def test_uniform_inlet_with_ramp(ref):
         r = fb.Block.ramp(t, ramp_end)
         assert np.abs(vel[0][0, :, :, 0] - r * 0.02).max() <= 1e-14
         assert (r == 1.0) == (ramp_end == 0.0)
+
+
+def test_const_rho_collide_with_fd_conditions_restated(ref):
+    """cavity3d's collision: ConstRhoBGK on kBulk cells and the Dirichlet BGK
+    on the boundary cells, with the average density from both
+    (kFluidAndBoundary): the restated collide gives the reference's state
+    after the collide, and the mean of its statistics the reference's next
+    average_rho."""
+    from octlb_b200 import cases, C
+    from oracle import fd_boundary as fb
+    n = 16
+    mesh, init, info = cases.cavity_forest(cells=n, n=n, lid=0.0, tau=0.6)
+    Cf = C.astype(np.float64)
+    w = np.where(np.abs(Cf).sum(1) == 0, 1 / 3, np.where(np.abs(Cf).sum(1) == 1, 1 / 18, 1 / 36))
+    init = np.broadcast_to(w * 1.01 - w, init.shape).copy()
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    sim = S(ref, mesh, info["omega"], init)
+    sim.set_fd_boundary([S.INTERPOLATED_VELOCITY] * 6, u, const_rho=True)
+    sim.advance(7)
+    avg = sim.average_rho()
+    P = sim.advance_phases_padded()[:, 0]
+    kinds = sim.kinds()[0]
+    core = (slice(1, -1),) * 3
+    stats = []
+    got = fb.collide(P[0][core], kinds, info["omega"], u[3], average_rho=avg, stats=stats)
+    assert np.abs(got - P[1][core]).max() <= 1e-15
+    assert abs(np.mean(stats) - sim.average_rho()) <= 1e-14
+    assert abs(avg - 1.0) > 1e-6                             # the correction is active
