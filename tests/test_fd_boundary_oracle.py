@@ -279,3 +279,31 @@ def test_const_rho_collide_with_fd_conditions_restated(ref):
     assert np.abs(got - P[1][core]).max() <= 1e-15
     assert abs(np.mean(stats) - sim.average_rho()) <= 1e-14
     assert abs(avg - 1.0) > 1e-6                             # the correction is active
+
+
+def test_restated_steps_follow_the_reference_over_time(ref):
+    """30 steps of the restated step (collide, linear-rotate stream over the
+    padded block, reconstruction) from the reference's padded state stay
+    with the reference's own 30 steps: the halo evolves as the reference's,
+    so the specification holds over time, not only step by step."""
+    from octlb_b200 import cases
+    from oracle import fd_boundary as fb
+    n = 12
+    mesh, init, info = cases.cavity_forest(cells=n, n=n, lid=0.0, tau=0.6)
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    sim = S(ref, mesh, info["omega"], init)
+    sim.set_fd_boundary([S.INTERPOLATED_VELOCITY] * 6, u)
+    sim.advance(5)
+    P = sim.advance_phases_padded()[:, 0]
+    kinds = sim.kinds()[0]
+    core = (slice(1, -1),) * 3
+    p = P[4].copy()
+    for _ in range(30):
+        p[core] = fb.collide(p[core], kinds, info["omega"], u[3])
+        p = fb.stream_padded(p)
+        p[core] = fb.reconstruct(p[core], kinds, info["omega"], u_lid=u[3])
+    for _ in range(30):
+        q = sim.advance_phases_padded()[4, 0]
+    assert np.abs(p - q).max() <= 1e-13
+    assert np.abs(q - P[4]).max() > 1e-3                     # the flow moved on
