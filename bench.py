@@ -58,59 +58,99 @@ def committed_traffic(kernel_key):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled around the timed region.
+
+    Sampling starts before the region (the first sample is awaited, up to 5 s)
+    and continues until one sample after it has arrived, so a region shorter
+    than the sampling interval is still bracketed by the samples on either
+    side.  summary() reports the samples that arrived during the region, or
+    else the last one before and the first one after it (`bracketing`), or an
+    `error` string when nvidia-smi gave none."""
 
     Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, index):
+    def __init__(self, index, interval_ms=50):
         self.index = index
+        self.interval_ms = interval_ms
         self.proc = None
-        self.lines = []
+        self.samples = []          # (arrival time, line)
+        self.error = None
+        self.t0 = self.t1 = None
+        self._cv = threading.Condition()
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except Exception:
-            self.proc = None
+                 "-lms", str(self.interval_ms)], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+        except Exception as e:  # no nvidia-smi
+            self.error = f"nvidia-smi could not start: {e}"
+            return self
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+        with self._cv:
+            self._cv.wait_for(lambda: self.samples or self.proc.poll() is not None, timeout=5.0)
+        if not self.samples:
+            self.error = "nvidia-smi gave no sample within 5 s"
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            with self._cv:
+                self.samples.append((time.perf_counter(), line.strip()))
+                self._cv.notify_all()
+
+    def start(self):
+        self.t0 = time.perf_counter()
+
+    def stop(self):
+        self.t1 = time.perf_counter()
 
     def __exit__(self, *a):
+        if self.t1 is None:
+            self.stop()
         if self.proc:
+            with self._cv:
+                self._cv.wait_for(lambda: any(t > self.t1 for t, _ in self.samples) or self.proc.poll() is not None,
+                                  timeout=2.0)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            p = [x.strip() for x in ln.split(",")]
-            if len(p) < 7:
-                continue
-            try:
-                sm.append(float(p[0]))
-                mx = float(p[1])
-            except ValueError:
-                continue
-            for k, nm in enumerate(names):
-                if p[3 + k].lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
+    def _parse(self, line):
+        p = [x.strip() for x in line.split(",")]
+        if len(p) < 7:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        try:
+            sm, mx = float(p[0]), float(p[1])
+        except ValueError:
+            return None
+        reasons = {nm for k, nm in enumerate(self.NAMES) if p[3 + k].lower().startswith("active")}
+        return sm, mx, reasons
+
+    def summary(self):
+        parsed = [(t, self._parse(ln)) for t, ln in self.samples]
+        parsed = [(t, v) for t, v in parsed if v is not None]
+        if not parsed:
+            return {"error": self.error or f"no parsable nvidia-smi sample ({len(self.samples)} lines)"}
+        t0 = self.t0 if self.t0 is not None else parsed[0][0]
+        t1 = self.t1 if self.t1 is not None else parsed[-1][0]
+        inside = [v for t, v in parsed if t0 <= t <= t1]
+        how = "during"
+        if not inside:
+            before = [v for t, v in parsed if t < t0][-1:]
+            after = [v for t, v in parsed if t > t1][:1]
+            inside = before + after
+            how = "bracketing"
+        sm = [v[0] for v in inside]
+        reasons = sorted(set().union(*[v[2] for v in inside]))
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": inside[-1][1], "reasons": reasons,
+                "samples": len(inside), "sampling": how, "region_ms": (t1 - t0) * 1e3}
 
 
 def dist_setup(args):
@@ -201,6 +241,73 @@ def run_reference_arm(args, world, rank, pg):
     print(json.dumps(out), flush=True)
 
 
+def accuracy_vs_fp64(ob, cases, n, steps, fields_fp32, threads=None):
+    """Errors of the headline workload against FP64 runs of the reference's
+    algorithm (north star: each result states its error against FP64):
+
+    * the 256^3 box after `steps` steps (the e2e run's fields for FP32, a
+      separate run for FP16) against the oracle's C restatement of the
+      reference BlockLattice<double> collide / fill_periodic_halo / stream
+      (pinned to the reference build at 1e-13), run on the host threads;
+    * the same physics at 64^3 over 1,000 steps: the kinetic-energy history
+      (every 10 steps) and the final fields on a 16^3 lattice of cells against
+      the reference's own BlockLattice<double> run
+      (tests/golden/tgv64_reference.npz)."""
+    from oracle import oracle
+    orc = oracle.load("orc")
+    rho0, u0 = cases.tgv_fields(n, n, n, 0.05)
+    init = ob.feq(rho0, u0)
+    blk = oracle.Block(orc, n)
+    blk.set_core(init)
+    del init
+    t0 = time.perf_counter()
+    blk.run_periodic_mt(1.0 / 0.55, steps, threads)
+    cpu_s = time.perf_counter() - t0
+    rho_r, u_r = blk.fields()
+    del blk
+    out = {"tgv256": {"steps": steps, "reference": "C restatement of BlockLattice<double>, FP64",
+                      "host_seconds": cpu_s}}
+
+    def rel(a, b):
+        return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+    mesh = ob.Mesh(n, [0], [0, 0, 0, 1, 1, 1], periodic=1)
+    for name, prec in (("fp32", ob.FP32), ("fp16", ob.FP16_SHIFTED)):
+        if name == "fp32" and fields_fp32 is not None:
+            rho_g, u_g = fields_fp32
+        else:
+            lat = ob.GpuLattice(mesh, 1.0 / 0.55, precision=prec)
+            lat.set_equilibrium(rho0.reshape(-1), u0.reshape(-1, 3))
+            lat.advance(steps)
+            rho_g, u_g = lat.get_fields()
+            lat.close()
+        out["tgv256"][name] = {"rel_err_rho_max": rel(np.asarray(rho_g).reshape(rho_r.shape), rho_r),
+                               "rel_err_u_max": rel(np.asarray(u_g).reshape(u_r.shape), u_r)}
+    del rho_r, u_r
+    g = np.load(os.path.join(ROOT, "tests", "golden", "tgv64_reference.npz"))
+    m, every, total = int(g["n"]), int(g["every"]), int(g["steps"])
+    mesh64, init64, info64 = cases.tgv_periodic(m, u0=float(g["u0"]), tau=float(g["tau"]))
+    out["tgv64_1000"] = {"reference": "BlockLattice<double> (oracle/_ref), FP64"}
+    lat_ke = {}
+    for name, prec in (("fp32", ob.FP32), ("fp16", ob.FP16_SHIFTED)):
+        lat = ob.GpuLattice(mesh64, info64["omega"], precision=prec, init_pops=init64)
+        ke = []
+        for k in range(total // every + 1):
+            if k:
+                lat.advance(every)
+            rho, u = lat.get_fields()
+            ke.append(0.5 * float(np.sum(rho * np.sum(u * u, axis=-1))))
+        lat.close()
+        sl = (0, slice(2, None, 4), slice(2, None, 4), slice(2, None, 4))
+        ke = np.array(ke)
+        lat_ke[name] = ke
+        out["tgv64_1000"][name] = {
+            "ke_rel_err_max": float(np.max(np.abs(ke - g["ke"]) / g["ke"])),
+            "ke_decay": float(ke[-1] / ke[0]), "ke_decay_reference": float(g["ke"][-1] / g["ke"][0]),
+            "rel_err_u_sampled": rel(u[sl], g["sample_u"]), "rel_err_rho_sampled": rel(rho[sl], g["sample_rho"])}
+    return out
+
+
 def forest_measurements(ob, cases, torch, peak):
     """The forest configurations beside the headline line: MLUPS of the
     two-level AMR cavity (64^3 + band under the lid) and of the three-level
@@ -213,7 +320,6 @@ def forest_measurements(ob, cases, torch, peak):
     with its gradients against FP64 finite differences
     (tests/golden/adjoint_c5.npz)."""
     here = os.path.dirname(os.path.abspath(__file__))
-    sys.path.insert(0, os.path.join(here, "tests", "golden"))
     out = {}
     cfgs = {
         "amr_cavity_64": (lambda: cases.cavity_forest(cells=64, n=8, lid=0.05, tau=0.56, band_cells=8),
@@ -270,7 +376,7 @@ def forest_measurements(ob, cases, torch, peak):
             r["const_rho_over_bgk_fp32"] = r["fp32"]["mlups"] / r["bgk_fp32"]["mlups"]
         out[name] = r
     # adjoint
-    from make_adjoint_reference import case, directions
+    case, directions = cases.adjoint_channel, cases.adjoint_directions
     g = np.load(os.path.join(here, "tests", "golden", "adjoint_c5.npz"))
     steps, window = int(g["steps"]), int(g["window"])
     mesh, init, info = case()
@@ -319,10 +425,7 @@ def run_single_case(args, ob, cases, torch):
     then --steps advance_one calls, or one adjoint sweep over --steps calls."""
     prec = ob.FP32 if args.precision == "fp32" else ob.FP16_SHIFTED
     if args.case == "adjoint":
-        here = os.path.dirname(os.path.abspath(__file__))
-        sys.path.insert(0, os.path.join(here, "tests", "golden"))
-        from make_adjoint_reference import case
-        mesh, init, info = case()
+        mesh, init, info = cases.adjoint_channel()
         lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP32, stream_mode=ob.STREAM_LINKS, drag=True,
                             init_pops=init)
         t0 = time.perf_counter()
@@ -371,6 +474,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-forest", action="store_true", help="skip the forest / adjoint measurements")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the errors against the FP64 runs")
     ap.add_argument("--case", default="tgv", choices=["tgv", "amr_cavity_64", "cylinder", "cylinder_512", "adjoint",
                                                       "const_rho_cavity_128"],
                     help="tgv: the headline line; otherwise run only that case for --steps advance_one "
@@ -412,10 +516,12 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         with ClockSampler(local) as cs:
+            cs.start()
             e0.record(stream)
             lat.advance(args.steps)
             e1.record(stream)
             torch.cuda.synchronize()
+            cs.stop()
         barrier(pg)
         ms = e0.elapsed_time(e1)
         ms_max = max_over_ranks(pg, ms)
@@ -424,30 +530,36 @@ def main():
         bytes_per_lu = 152 if prec == ob.FP32 else 76
         results[prec_name] = {"mlups": mlups, "ms_step": ms_step, "launches": launches,
                               "bytes_per_lu": bytes_per_lu, "clocks": cs.summary(), "lups": lups}
-        # e2e: the same job through the C ABI from host memory
+        # e2e: the same job through the C ABI from host memory: the
+        # Taylor-Green fields (rho, u per cell, FP64, pinned) uploaded and
+        # turned into the equilibrium state, K steps, rho / u read back
         if prec_name == args.precision:
-            pinned = torch.from_numpy(np.ascontiguousarray(init.reshape(-1))).pin_memory()
-            init_host = pinned.numpy()
+            rho0, u0 = cases.tgv_fields(n, n, n, 0.05)
+            rho_in = torch.from_numpy(np.ascontiguousarray(rho0.reshape(-1))).pin_memory().numpy()
+            u_in = torch.from_numpy(np.ascontiguousarray(u0.reshape(-1))).pin_memory().numpy()
+            del rho0, u0
             rho_host = torch.empty(n ** 3, dtype=torch.float64).pin_memory().numpy()
             u_host = torch.empty(3 * n ** 3, dtype=torch.float64).pin_memory().numpy()
             e2e_steps = args.steps
             # untimed warm-up of the same calls (first-use costs of the
             # staging buffers and pinned pages)
-            lat.set_populations(init_host)
+            lat.set_equilibrium(rho_in, u_in)
             lat.advance(args.warmup)
             lat.get_fields(rho_host, u_host)
             torch.cuda.synchronize()
             barrier(pg)
             t0 = time.perf_counter()
-            lat.set_populations(init_host)
+            lat.set_equilibrium(rho_in, u_in)
             lat.advance(e2e_steps)
             rho, u = lat.get_fields(rho_host, u_host)
             t1 = time.perf_counter()
             e2e_s = max_over_ranks(pg, t1 - t0)
             results["e2e"] = {"value": world * lups * e2e_steps / e2e_s / 1e6, "unit": "MLUPS",
-                              "h2d_bytes_per_step": int(init_host.nbytes / e2e_steps),
+                              "h2d_bytes_per_step": int((rho_in.nbytes + u_in.nbytes) / e2e_steps),
                               "d2h_bytes_per_step": int((rho.nbytes + u.nbytes) / e2e_steps),
                               "steps": e2e_steps, "seconds": e2e_s}
+            if e2e_steps <= 20 and prec_name == "fp32":
+                results["e2e_fields"] = (rho.copy(), u.copy())
         lat.close()
         del lat
         torch.cuda.empty_cache()
@@ -474,6 +586,10 @@ def main():
         "fp16_shifted": {"mlups": results["fp16"]["mlups"], "ms_per_step": results["fp16"]["ms_step"],
                          "bytes_per_lu": 76, "speedup_vs_fp32": results["fp16"]["mlups"] / results["fp32"]["mlups"]},
     }
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        m = min(args.steps, 20)
+        out["accuracy_vs_fp64"] = accuracy_vs_fp64(ob, cases, n, m,
+                                                   results.get("e2e_fields") if m == args.steps else None)
     if rank == 0 and world == 1 and not args.no_forest:
         out["forest"] = forest_measurements(ob, cases, torch, peak)
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -201,6 +201,14 @@ int octlb_gpu_adjoint(octlb_ctx* ctx, const octlb_adj_params* params, double* ob
 /* Reference state f (post-stream, pre-collision) -> context; the next step
  * starts by colliding it. */
 int octlb_gpu_set_populations(octlb_ctx* ctx, const double* pops);
+/* Equilibrium initialisation from per-cell fields: every core cell takes
+ * f_i = feq_i(rho, u) (the shifted second-order equilibrium) and the next
+ * step starts by colliding it -- BlockLattice::initialize(rho0, u0)
+ * (block_lattice.cpp:273-285) and initialize_from_material
+ * (lattice_material_init.cpp:11-33) with a rho and u per cell instead of one
+ * pair.  rho [n_blocks][n^3], u [n_blocks][n^3][3]; equal to
+ * octlb_gpu_set_populations of that equilibrium, at a fifth of its upload. */
+int octlb_gpu_set_equilibrium(octlb_ctx* ctx, const double* rho, const double* u);
 /* Post-collision populations the next stream reads (what the reference's
  * take_post_collide_snapshot holds after the next collide), core cells. */
 int octlb_gpu_get_populations(octlb_ctx* ctx, double* pops);
@@ -226,7 +234,10 @@ int octlb_gpu_audit(octlb_ctx* ctx, double out[4]);
  * the process exits; levels of more than 33,554,432 cells are rejected with
  * OCTLB_EINVAL.  The first call made on a device looks up that array's device
  * address (cudaGetSymbolAddress), so make that first call before any stream
- * capture; call with the context's device current.  All calls share the
+ * capture; call with the context's device current.  The address is kept for
+ * the life of the process: after a cudaDeviceReset of that device the entry
+ * point must not be used again.  Like octlb_gpu_audit it first reports a
+ * bounded device wait that gave up (OCTLB_ETIMEOUT).  All calls share the
  * array: calls that overlap on the GPU race. */
 int octlb_gpu_audit_noalloc(octlb_ctx* ctx, double out[4]);
 

@@ -291,6 +291,15 @@ class GpuLattice:
         assert a.size == self._cells() * Q
         self._check(self._L.octlb_gpu_set_populations(self._h, capi.ptr(a, ctypes.c_double)))
 
+    def set_equilibrium(self, rho, u):
+        """Equilibrium of per-cell fields (octlb_gpu_set_equilibrium): rho
+        [n_blocks*n^3], u [n_blocks*n^3][3], float64 (ideally pinned)."""
+        r = np.ascontiguousarray(rho, np.float64)
+        v = np.ascontiguousarray(u, np.float64)
+        assert r.size == self._cells() and v.size == 3 * self._cells()
+        self._check(self._L.octlb_gpu_set_equilibrium(self._h, capi.ptr(r, ctypes.c_double),
+                                                      capi.ptr(v, ctypes.c_double)))
+
     def get_fields(self, rho=None, u=None):
         """rho, u of every core cell; pass preallocated (ideally pinned)
         float64 arrays of n_blocks*n^3 and n_blocks*n^3*3 to fill in place."""

@@ -86,6 +86,7 @@ def lib():
         "octlb_gpu_advance": (ctypes.c_int, [P, ctypes.c_int]),
         "octlb_gpu_synchronize": (ctypes.c_int, [P]),
         "octlb_gpu_set_populations": (ctypes.c_int, [P, F64P]),
+        "octlb_gpu_set_equilibrium": (ctypes.c_int, [P, F64P, F64P]),
         "octlb_gpu_set_body_force": (ctypes.c_int, [P, F64P]),
         "octlb_gpu_set_const_rho": (ctypes.c_int, [P, ctypes.c_int]),
         "octlb_gpu_write_vtk": (ctypes.c_int, [P, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,

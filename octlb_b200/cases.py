@@ -180,3 +180,24 @@ def cylinder_forest(length=256, height=64, n=8, diameter=16.0, center=(64.0, 32.
     tau = 3.0 * nu + 0.5
     init = np.zeros((mesh.n_blocks, n, n, n, Q))
     return mesh, init, {"omega": 1.0 / tau, "tau": tau, "forest": f, "tree_cells": tree_cells}
+
+
+# The adjoint configuration: channel 128x32x32 finest cells, two levels, D = 8,
+# Re = 40; body-force perturbation directions drawn from a recorded seed.
+ADJOINT_SEED = 20261203
+ADJOINT_DIRS = 8
+
+
+def adjoint_channel(u_max=0.05, tau=None):
+    """The adjoint channel; tau defaults to the Re = 40 value."""
+    mesh, init, info = cylinder_forest(length=128, height=32, n=8, diameter=8.0, center=(32.0, 16.0),
+                                       levels=2, u_max=u_max, re=40.0)
+    if tau is not None:
+        info["tau"], info["omega"] = tau, 1.0 / tau
+    return mesh, init, info
+
+
+def adjoint_directions(mesh, seed=ADJOINT_SEED, count=ADJOINT_DIRS):
+    """Per-cell body-force directions d ~ N(0, 1e-6), [count][blocks][n^3][3]."""
+    rng = np.random.default_rng(seed)
+    return rng.normal(0.0, 1e-6, size=(count, mesh.n_blocks, mesh.n ** 3, 3))

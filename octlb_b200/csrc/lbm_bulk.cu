@@ -10,17 +10,19 @@
 // element is read exactly once per step, so the shared-memory staging buys
 // latency hiding (many KB in flight per SM with few threads), not reuse.
 //
-// Every mbarrier wait is bounded (~1 s of %globaltimer): on expiry the CTA
-// agrees via __syncthreads_and, records kErrBulkTimeout in *err, drains its own
-// copies in flight (again bounded) and returns; the host reports
-// OCTLB_ETIMEOUT.
+// Every mbarrier wait is bounded (StepArgs::wait_ns of %globaltimer, 1 s by
+// default): on expiry the CTA agrees via __syncthreads_and, records
+// kErrBulkTimeout in *err, drains the copies it has issued and not yet seen
+// land (again bounded; kErrBulkDrainTimeout if that expires too) and returns;
+// the host reports OCTLB_ETIMEOUT (OCTLB_ECUDA after a failed drain).
+// StepArgs::stall_first_row makes CTA 0 skip issuing its first row, so its
+// first wait runs out: the test of this path (no fault, no hang).
 #include "octlb_internal.h"
 
 namespace octlb_gpu {
 namespace {
 
 constexpr int kStages = 4;
-constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -49,11 +51,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait for the phase with the given parity.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, unsigned long long limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (global_ns() - t0 > kWaitNs) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   }
   return true;
 }
@@ -104,28 +106,38 @@ __global__ void __launch_bounds__(1024) k_step_bulk(const StepArgs a) {
 
   // rows of this CTA: blockIdx.x + k * gridDim.x, k = 0..my_rows-1
   const uint32_t my_rows = blockIdx.x < rows ? (rows - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  // Thread 0's record of which rows it issued (rows k .. k + kStages - 2 are
+  // in flight while row k is consumed): bit j % kStages.
+  uint32_t issued = 0;
   if (threadIdx.x == 0) {
-    for (uint32_t k = 0; k < my_rows && k < kStages - 1; ++k)
+    for (uint32_t k = 0; k < my_rows && k < kStages - 1; ++k) {
+      if (k == 0 && a.stall_first_row && blockIdx.x == 0) continue;
       issue_row<T>(a, src, stages + k * stage_elems, &bars[k], blockIdx.x + k * gridDim.x);
+      issued |= 1u << k;
+    }
   }
   for (uint32_t k = 0; k < my_rows; ++k) {
     const uint32_t s = k % kStages;
-    bool ok = mbar_wait_bounded(&bars[s], (k / kStages) & 1);
+    bool ok = mbar_wait_bounded(&bars[s], (k / kStages) & 1, a.wait_ns);
     ok = __syncthreads_and(ok) != 0;
     if (!ok) {
       if (threadIdx.x == 0) {
-        atomicExch(a.err, kErrBulkTimeout);
-        // drain the copies this CTA still has in flight (bounded)
+        int code = kErrBulkTimeout;
+        // drain the copies this CTA issued and has not seen land (bounded)
         for (uint32_t j = k; j < my_rows && j < k + kStages - 1; ++j)
-          mbar_wait_bounded(&bars[j % kStages], (j / kStages) & 1);
+          if ((issued >> (j % kStages)) & 1u)
+            if (!mbar_wait_bounded(&bars[j % kStages], (j / kStages) & 1, a.wait_ns)) code = kErrBulkDrainTimeout;
+        atomicMax(a.err, code);
       }
       return;
     }
+    if (threadIdx.x == 0) issued &= ~(1u << s);
     // every thread has finished reading stage (k-1) % kStages: refill it
     if (threadIdx.x == 0 && k + kStages - 1 < my_rows) {
       const uint32_t kk = k + kStages - 1;
       issue_row<T>(a, src, stages + (kk % kStages) * stage_elems, &bars[kk % kStages],
                    blockIdx.x + kk * gridDim.x);
+      issued |= 1u << (kk % kStages);
     }
     const T* S = stages + s * stage_elems;
     float f[kQ];

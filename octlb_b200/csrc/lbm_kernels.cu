@@ -794,6 +794,54 @@ k_scatter(const StepArgs a, const double* in, int near_parts) {
   }
 }
 
+// Equilibrium state from macroscopic fields (BlockLattice::initialize and
+// initialize_from_material with a per-cell rho, u: block_lattice.cpp:273-285,
+// lattice_material_init.cpp:11-33): f_i = feq_i(rho, u) - w_i in FP64, then
+// the same conversion and collide as k_scatter.  in = [rho | u] (ncore, then
+// ncore x 3).  The FP64 operations are rounded one by one in the order
+// rho w_i (1 + 3 cu + 4.5 cu cu - 1.5 u.u) - w_i is written (no contraction
+// into fused multiply-adds), so the state equals k_scatter's of the same
+// equilibrium formed on the host in that order.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_scatter_eq(const StepArgs a, const double* in, int near_parts) {
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  double v[1] = {0.0};
+  if (t < a.ncore) {
+    const long long slot = t;
+    const double rho = in[t];
+    const double* up = in + a.ncore + 3ll * t;
+    const double ux = up[0], uy = up[1], uz = up[2];
+    const double usq = __dadd_rn(__dadd_rn(__dmul_rn(ux, ux), __dmul_rn(uy, uy)), __dmul_rn(uz, uz));
+    const double t6 = __dmul_rn(1.5, usq);
+    float f[kQ];
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      // c_i has at most two nonzero components: cu is exact or one rounding
+      double cu = 0.0;
+      if (cx(i)) cu = cx(i) > 0 ? ux : -ux;
+      if (cy(i)) cu = __dadd_rn(cu, cy(i) > 0 ? uy : -uy);
+      if (cz(i)) cu = __dadd_rn(cu, cz(i) > 0 ? uz : -uz);
+      const double p = __dsub_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(3.0, cu)), __dmul_rn(__dmul_rn(4.5, cu), cu)), t6);
+      f[i] = static_cast<float>(__dsub_rn(__dmul_rn(__dmul_rn(rho, wd(i)), p), wd(i)));
+    }
+    const int kind = a.flags ? (a.flags[slot] & kKindMask) : kBulk;
+    if (kind == kBulk) {
+      if (a.cr_avg) v[0] = bgk_const_rho(f, a.omega, static_cast<float>(1.0 - *a.cr_avg));
+      else bgk(f, a.omega);
+    }
+    T* dst = static_cast<T*>(a.dst);
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + slot, f[i], a.scale);
+  }
+  if (a.cr_part) {
+    block_reduce<1>(v);
+    if (threadIdx.x == 0) a.cr_part[blockIdx.x] = v[0];
+    if (blockIdx.x == 0)
+      for (int p = threadIdx.x; p < near_parts; p += kThreads) a.cr_part[gridDim.x + p] = 0.0;
+  }
+}
+
 // ConstRhoBGK statistics of a stored state that BGK collided (which keeps
 // each cell's density): per CTA the sum of rho - 1 over kBulk core cells, as
 // k_scatter lays them out.
@@ -977,6 +1025,11 @@ cudaError_t launch_scatter(const StepArgs& a, const double* in, int near_parts, 
   k_scatter<T><<<grid_for(a.ncore), kThreads, 0, s>>>(a, in, near_parts);
   return cudaGetLastError();
 }
+template <typename T>
+cudaError_t launch_scatter_eq(const StepArgs& a, const double* in, int near_parts, cudaStream_t s) {
+  k_scatter_eq<T><<<grid_for(a.ncore), kThreads, 0, s>>>(a, in, near_parts);
+  return cudaGetLastError();
+}
 
 // ConstRhoBGK partials of a level: one per core CTA of k_step_cr (the CTAs of
 // k_scatter / k_cr_seed), then one per CTA of k_step_near_cr.
@@ -1030,6 +1083,7 @@ cudaError_t launch_cr_update(double* avg, const double* part, int nparts, long l
   template cudaError_t launch_audit<T>(const StepArgs&, double*, double*, cudaStream_t);           \
   template cudaError_t launch_gather<T>(const StepArgs&, double*, double*, int, cudaStream_t);              \
   template cudaError_t launch_scatter<T>(const StepArgs&, const double*, int, cudaStream_t);     \
+  template cudaError_t launch_scatter_eq<T>(const StepArgs&, const double*, int, cudaStream_t);  \
   template cudaError_t launch_step_cr<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
   template cudaError_t launch_step_map_cr<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
   template cudaError_t launch_cr_seed<T>(const StepArgs&, int, cudaStream_t);

@@ -11,6 +11,7 @@
 #include <filesystem>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <set>
 #include <string>
 #include <unordered_set>
@@ -30,6 +31,7 @@ cudaError_t launch_drag_total(const double*, int, double*, double*, cudaStream_t
 template <typename T> cudaError_t launch_audit(const StepArgs&, double*, double*, cudaStream_t);
 template <typename T> cudaError_t launch_gather(const StepArgs&, double*, double*, int, cudaStream_t);
 template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*, int, cudaStream_t);
+template <typename T> cudaError_t launch_scatter_eq(const StepArgs&, const double*, int, cudaStream_t);
 template <typename T>
 cudaError_t launch_step_cr(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
 template <typename T> cudaError_t launch_cr_seed(const StepArgs&, int, cudaStream_t);
@@ -268,6 +270,13 @@ struct octlb_ctx {
   long long launch_count = 0;       // kernels issued by the advance_one being built
   int step_kernel = 0;              // OCTLB_STEP_KERNEL: 0 pair (default), 1 bulk, 2 plain
   bool map_global = true;           // slot map read through L1 (OCTLB_MAP_SMEM=1: staged in shared memory)
+  // Bounded device waits: their limit (OCTLB_WAIT_MS, default 1 s) and the
+  // test of the give-up path (OCTLB_TEST_BULK_STALL=1: one CTA of the bulk
+  // step waits for a row it never requested).  After a give-up whose own
+  // copies did not drain either, the context refuses further work.
+  unsigned long long wait_ns = 1000000000ull;
+  int stall_first_row = 0;
+  bool unusable = false;
   int map_cells = 0;                // cells per thread of the slot-map step (OCTLB_MAP_CELLS 1 or 2;
                                     // default 2, 1 under the links rule whose variant spills at 2)
   // advance_one captured as CUDA graphs, keyed by the A/B parity of every
@@ -610,12 +619,9 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     ctx->blk_local[b] = static_cast<int>(L.blocks.size());
     L.blocks.push_back(b);
   }
-  // Equilibrium at rest when no initial state is given (block_lattice.cpp:272-285).
-  std::vector<double> init_pops;
-  if (!init) {
-    init_pops.assign(static_cast<size_t>(n3 * nb * kQ), 0.0);
-    init = init_pops.data();
-  }
+  // Equilibrium at rest when no initial state is given (block_lattice.cpp:272-285):
+  // shifted populations f - w = 0, whose collision is 0 too, so the
+  // zero-filled buffers already hold it and nothing is uploaded.
 
   // ---- per-level storage and flags
   for (int l = 0; l < nlev; ++l) {
@@ -710,8 +716,9 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
   std::vector<std::vector<ProlongItem>> prolong(nlev);
   std::vector<std::vector<RestrictItem>> restrict_items(nlev);
   std::vector<float> prev(plan.size() * 23, 0.f);
-  for (size_t k = 0; k < plan.size(); ++k)
-    host_macro(init + gcell(plan[k].coarse_id, plan[k].ci, plan[k].cj, plan[k].ck) * kQ, &prev[k * 23]);
+  if (init)
+    for (size_t k = 0; k < plan.size(); ++k)
+      host_macro(init + gcell(plan[k].coarse_id, plan[k].ci, plan[k].cj, plan[k].ck) * kQ, &prev[k * 23]);
   {
     // Prolongation writes a fine cell per point; a later point writing the
     // same cell wins (plan order, level_coupler.cpp:440-477).
@@ -1328,6 +1335,8 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       A.off_pad[i] = cx(i) * np * np + cy(i) * np + cz(i);
     }
     A.err = ctx->dev_err.as<int>();
+    A.wait_ns = ctx->wait_ns;
+    A.stall_first_row = ctx->stall_first_row;
     A.fill_of = L.n_bb > 0 ? L.fill_of.as<int>() : nullptr;
     A.fills = L.bb_ops.as<BBOp>();
     // One all-kBulk periodic block: paired vector step by default, the
@@ -1389,7 +1398,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
   CK(ctx->audit_out.alloc(5 * sizeof(double)));
 
   // ---- initial state: g = C(f0) on kBulk cells
-  for (int l = 0; l < nlev && !g_dry_run; ++l) {
+  for (int l = 0; l < nlev && !g_dry_run && init; ++l) {
     Level& L = ctx->levels[l];
     if (L.nblk == 0) continue;
     std::vector<double> dense(static_cast<size_t>(L.nblk * n3 * kQ));
@@ -1414,7 +1423,14 @@ int check_device_error(octlb_ctx* ctx) {
   int h = 0;
   CK(cudaMemcpyAsync(&h, ctx->dev_err.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  if (h == kErrBulkTimeout) return fail(ctx, OCTLB_ETIMEOUT, "bulk-copy wait gave up after 1 s");
+  if (h == kErrBulkTimeout)
+    return fail(ctx, OCTLB_ETIMEOUT,
+                "bulk-copy wait gave up after " + std::to_string(ctx->wait_ns / 1000000ull) + " ms");
+  if (h == kErrBulkDrainTimeout) {
+    ctx->unusable = true;
+    return fail(ctx, OCTLB_ECUDA,
+                "bulk-copy wait gave up and its copies in flight did not drain either: context unusable");
+  }
   if (h != 0) return fail(ctx, OCTLB_ECUDA, "device error word set");
   return OCTLB_OK;
 }
@@ -2000,6 +2016,41 @@ int scatter_impl(octlb_ctx* ctx, const double* in) {
   return OCTLB_OK;
 }
 
+// Equilibrium from per-cell rho [n_blocks][n^3] and u [n_blocks][n^3][3]:
+// per level, the level's rows of both are staged as [rho | u] and
+// k_scatter_eq forms, collides and stores the state.  One stream sync at
+// the end (the staging buffer is reused per level, each level's copies are
+// ordered after the previous level's kernel on the same stream).
+template <typename T>
+int scatter_eq_impl(octlb_ctx* ctx, const double* rho, const double* u) {
+  const long long n3 = static_cast<long long>(ctx->n) * ctx->n * ctx->n;
+  for (auto& L : ctx->levels) {
+    if (L.nblk == 0) continue;
+    const long long cells = L.nblk * n3;
+    DevBuf& d = ctx->stage_a;
+    CK(d.reserve(static_cast<size_t>(cells * 4) * sizeof(double)));
+    double* dr = d.as<double>();
+    double* du = dr + cells;
+    if (contiguous(L)) {
+      const long long b0 = static_cast<long long>(L.blocks[0]) * n3;
+      CK(cudaMemcpyAsync(dr, rho + b0, sizeof(double) * cells, cudaMemcpyHostToDevice, ctx->stream));
+      CK(cudaMemcpyAsync(du, u + 3 * b0, sizeof(double) * 3 * cells, cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+      for (int lb = 0; lb < L.nblk; ++lb) {
+        const long long b0 = static_cast<long long>(L.blocks[lb]) * n3;
+        CK(cudaMemcpyAsync(dr + lb * n3, rho + b0, sizeof(double) * n3, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(du + 3 * lb * n3, u + 3 * b0, sizeof(double) * 3 * n3, cudaMemcpyHostToDevice,
+                           ctx->stream));
+      }
+    }
+    StepArgs a = L.args;
+    a.dst = L.buf[L.cur].p;
+    CK(launch_scatter_eq<T>(a, dr, a.cr_part ? ctx->cr_near : 0, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  return OCTLB_OK;
+}
+
 template <typename T>
 int audit_impl(octlb_ctx* ctx, double out[4]) {
   double tot[5] = {0, 0, 0, 0, 0};
@@ -2050,6 +2101,11 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
   ctx->map_cells = p->stream_mode == OCTLB_STREAM_LINKS ? 1 : 2;
   if (const char* mc = std::getenv("OCTLB_MAP_CELLS")) ctx->map_cells = mc[0] == '1' ? 1 : 2;
   if (const char* ms = std::getenv("OCTLB_MAP_SMEM")) ctx->map_global = ms[0] != '1';
+  if (const char* wm = std::getenv("OCTLB_WAIT_MS")) {
+    const long long ms = std::atoll(wm);
+    if (ms >= 1 && ms <= 60000) ctx->wait_ns = static_cast<unsigned long long>(ms) * 1000000ull;
+  }
+  if (const char* st = std::getenv("OCTLB_TEST_BULK_STALL")) ctx->stall_first_row = st[0] == '1' ? 1 : 0;
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "cudaStreamCreate"); *out = ctx.release(); return rc; }
   ctx->own_stream = true;
@@ -2098,6 +2154,7 @@ int octlb_gpu_set_stream(octlb_ctx* ctx, void* s) {
 int octlb_gpu_advance(octlb_ctx* ctx, int steps) {
   if (!ctx || steps < 0) return OCTLB_EINVAL;
   if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
+  if (ctx->unusable) return fail(ctx, OCTLB_ESTATE, "context unusable after a failed drain of a bounded wait");
   return ctx->precision == OCTLB_FP32 ? advance_impl<float>(ctx, steps) : advance_impl<__half>(ctx, steps);
 }
 
@@ -2105,6 +2162,7 @@ int octlb_gpu_adjoint(octlb_ctx* ctx, const octlb_adj_params* p, double* objecti
                       double* grad_force) {
   if (!ctx || !p) return OCTLB_EINVAL;
   if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
+  if (ctx->unusable) return fail(ctx, OCTLB_ESTATE, "context unusable after a failed drain of a bounded wait");
   if (ctx->precision != OCTLB_FP32) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates FP32 storage only");
   if (ctx->const_rho) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates the BGK collide, not ConstRhoBGK");
   return adjoint_impl<float>(ctx, p, objective, grad, grad_force);
@@ -2205,6 +2263,12 @@ int octlb_gpu_set_body_force(octlb_ctx* ctx, const double* force) {
 int octlb_gpu_set_populations(octlb_ctx* ctx, const double* pops) {
   if (!ctx || !pops) return OCTLB_EINVAL;
   return ctx->precision == OCTLB_FP32 ? scatter_impl<float>(ctx, pops) : scatter_impl<__half>(ctx, pops);
+}
+
+int octlb_gpu_set_equilibrium(octlb_ctx* ctx, const double* rho, const double* u) {
+  if (!ctx || !rho || !u) return OCTLB_EINVAL;
+  if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
+  return ctx->precision == OCTLB_FP32 ? scatter_eq_impl<float>(ctx, rho, u) : scatter_eq_impl<__half>(ctx, rho, u);
 }
 
 int octlb_gpu_get_populations(octlb_ctx* ctx, double* pops) {
@@ -2398,7 +2462,10 @@ constexpr long long kNoAllocMaxCells = static_cast<long long>(kNoAllocRows) * kN
 constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_scratch[(kNoAllocRows + 1) * 5];
+// Device address of the array per device, looked up once under the mutex (two
+// host threads making their first call at once look it up once).
 static double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+static std::mutex g_noalloc_mutex;
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_audit_noalloc(const StepArgs a, double* rows) {
@@ -2501,14 +2568,22 @@ extern "C" int octlb_gpu_audit_noalloc(octlb_ctx* ctx, double out[4]) {
     break;
   }
   if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(ctx, OCTLB_EINVAL, "device ordinal out of range");
+  // A bounded device wait that gave up left a partly written state: report
+  // it as octlb_gpu_audit does instead of summing that state.
+  if (int rc = check_device_error(ctx)) return rc;
   // One-time set-up on this device: the scratch array's device address.  In
   // host code the array's name is only a host-side stand-in, never a device
   // address, so the kernels receive this pointer.
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+      g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    scratch = g_noalloc_ptr[dev];
   }
-  return ctx->precision == OCTLB_FP32 ? audit_noalloc_impl<float>(ctx, g_noalloc_ptr[dev], out)
-                                      : audit_noalloc_impl<__half>(ctx, g_noalloc_ptr[dev], out);
+  return ctx->precision == OCTLB_FP32 ? audit_noalloc_impl<float>(ctx, scratch, out)
+                                      : audit_noalloc_impl<__half>(ctx, scratch, out);
 }

@@ -55,6 +55,8 @@ struct StepArgs {
   double* cr_part;
   int cr_total;             // partials the average update sums
   int* err;                 // device error word (bounded waits that gave up)
+  unsigned long long wait_ns; // limit of every bounded device wait
+  int stall_first_row;      // test of the bounded wait: CTA 0 never issues its first row
 };
 
 // Cells flagged kFlagNear with the link rule resolved on the host: for near
@@ -75,7 +77,9 @@ struct NearTables {
 constexpr long long kOwnPage = -(1LL << 62);
 
 // Device error codes written to StepArgs::err.
-enum : int { kErrNone = 0, kErrBulkTimeout = 1, kErrHalo = 2 };
+// kErrBulkDrainTimeout: a CTA that gave up could not see its own copies in
+// flight land either, so shared memory may still be written after it exited.
+enum : int { kErrNone = 0, kErrBulkTimeout = 1, kErrHalo = 2, kErrBulkDrainTimeout = 3 };
 
 // Tree-boundary fill of one halo-page population: value(dst, pop) =
 // g_src_pop(src) + add (bounce-back wall: src_pop = opp(pop); outflow ghost

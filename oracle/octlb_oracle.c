@@ -343,3 +343,66 @@ double orc_periodic_slabs_mlups(int nx, int ny, int nz, int slabs, int threads, 
   free(bl); free(th); free(jobs);
   return (double)nx * ny * (double)(nzs * slabs) * steps / sec / 1e6;
 }
+
+/* The periodic loop above (collide -> fill_periodic_halo -> stream) with the
+ * collide and the torus stream split over `threads` POSIX threads by x
+ * planes: every cell gets the same arithmetic as in the serial loop, so the
+ * result is bitwise the serial one (only the work is shared).  For boxes the
+ * serial loop takes minutes on (the 256^3 throughput box). */
+typedef struct { orc_block* b; double omega; int phase, x0, x1; } mt_job;
+static void* mt_worker(void* arg) {
+  mt_job* j = (mt_job*)arg;
+  orc_block* b = j->b;
+  const int NY = b->NY, NZ = b->NZ;
+  if (j->phase == 0) {
+    for (int x = j->x0; x < j->x1; ++x)
+      for (int y = 0; y < b->ny; ++y)
+        for (int z = 0; z < b->nz; ++z)
+          if (b->kind[kidx(b, x, y, z)] == K_BULK) bgk(b->f + hidx(b, x + 1, y + 1, z + 1), j->omega);
+  } else if (j->phase == 1) {
+    for (int hx = j->x0; hx < j->x1; ++hx)
+      for (int hy = 0; hy < NY; ++hy)
+        for (int hz = 0; hz < NZ; ++hz) {
+          const long lin = ((long)hx * NY + hy) * NZ + hz;
+          for (int i = 0; i < Q; ++i) b->tmp[lin * Q + i] = b->f[rotate_src(b, lin, i)];
+        }
+  } else {
+    const size_t plane = (size_t)NY * NZ * Q;
+    memcpy(b->f + (size_t)j->x0 * plane, b->tmp + (size_t)j->x0 * plane,
+           (size_t)(j->x1 - j->x0) * plane * sizeof(double));
+  }
+  return NULL;
+}
+static void mt_phase(orc_block* b, double omega, int phase, int planes, int threads) {
+  pthread_t th[256];
+  mt_job jobs[256];
+  if (threads > 256) threads = 256;
+  if (threads > planes) threads = planes;
+  for (int k = 0; k < threads; ++k) {
+    jobs[k] = (mt_job){b, omega, phase, planes * k / threads, planes * (k + 1) / threads};
+    pthread_create(&th[k], NULL, mt_worker, &jobs[k]);
+  }
+  for (int k = 0; k < threads; ++k) pthread_join(th[k], NULL);
+}
+int orc_block_run_periodic_mt(orc_block* b, double omega, int steps, int threads) {
+  if (b->q) return -1; /* the torus stream only (no link table) */
+  if (threads < 1) threads = 1;
+  for (int t = 0; t < steps; ++t) {
+    mt_phase(b, omega, 0, b->nx, threads);
+    orc_block_fill_periodic(b);
+    mt_phase(b, omega, 1, b->NX, threads);
+    mt_phase(b, omega, 2, b->NX, threads);
+  }
+  return 0;
+}
+
+/* rho and u of every core cell, [nx][ny][nz] and [nx][ny][nz][3]
+ * (block_lattice.h:113-125), without a padded copy. */
+void orc_block_fields(const orc_block* b, double* rho, double* u) {
+  for (int x = 0; x < b->nx; ++x)
+    for (int y = 0; y < b->ny; ++y)
+      for (int z = 0; z < b->nz; ++z) {
+        const size_t k = (size_t)kidx(b, x, y, z);
+        rho_u(b->f + hidx(b, x + 1, y + 1, z + 1), &rho[k], &u[3 * k]);
+      }
+}

@@ -36,9 +36,14 @@ void orc_block_run_periodic(orc_block* b, double omega, int steps);
 void orc_block_run_walls(orc_block* b, double omega, int steps, const uint8_t* moving,
                          const double* uw);
 void orc_block_drag(const orc_block* b, const uint8_t* mask, double out[3]);
+/* orc_block_run_periodic on `threads` POSIX threads, bitwise equal to it
+ * (blocks without a link table; -1 otherwise). */
+int orc_block_run_periodic_mt(orc_block* b, double omega, int steps, int threads);
+/* rho [nx][ny][nz] and u [nx][ny][nz][3] of the core cells. */
+void orc_block_fields(const orc_block* b, double* rho, double* u);
 
 /* Periodic box as independent slabs (z-slices of the full box each own a
- * periodic halo), run on `threads` OpenMP threads: the multi-core CPU
+ * periodic halo), run on `threads` POSIX threads: the multi-core CPU
  * baseline (one slab per core, no halo exchange between slabs). */
 double orc_periodic_slabs_mlups(int nx, int ny, int nz, int slabs, int threads,
                                 double omega, int steps);

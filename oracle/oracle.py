@@ -5,10 +5,10 @@ by the product.
 * ``liboctlb_oracle.so``  -- plain-C restatement (octlb_oracle.c), always built.
 * ``_ref/liboctlb_ref.so`` -- the reference's own BlockLattice / LevelCoupler /
   GhostSchedule / TimeLoop / MomentumExchangeDrag, compiled from its sources by
-  `make -C oracle ref` where the reference tree is available; prebuilt files
+  `make -C oracle ref REF=<reference tree>` where the reference tree is available; prebuilt files
   travel with the repository.
 * ``_ref/liboctlb_ref_tlm.so`` -- the same sources compiled on a forward-mode
-  dual number (`make -C oracle tlm`): the tangent-linear FP64 reference, whose
+  dual number (`make -C oracle tlm REF=<reference tree>`): the tangent-linear FP64 reference, whose
   force carries its derivatives along seeded parameter directions.
 """
 import ctypes
@@ -29,12 +29,18 @@ def _p(a, t=ctypes.c_double):
     return None if a is None else a.ctypes.data_as(ctypes.POINTER(t))
 
 
-def build(ref=True):
-    """make -C oracle (and the reference build when its sources exist)."""
+def build(ref=True, reference_tree=None):
+    """make -C oracle, and with ref the reference build from its source tree
+    (`reference_tree`, else the OCTLB_REFERENCE environment variable).  A tree
+    that is named but holds no reference sources is an error; with none named
+    the reference build is skipped (its prebuilt files, if any, stay)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    src = os.environ.get("OCTLB_REFERENCE", "/root/reference")
-    if ref and os.path.isdir(os.path.join(src, "src", "solver", "lbm")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", "tlm", f"REF={src}"], check=True)
+    src = reference_tree or os.environ.get("OCTLB_REFERENCE")
+    if not ref or not src:
+        return
+    if not os.path.isdir(os.path.join(src, "src", "solver", "lbm")):
+        raise FileNotFoundError(f"{src} holds no reference sources (src/solver/lbm)")
+    subprocess.run(["make", "-s", "-C", HERE, "ref", "tlm", f"REF={src}"], check=True)
 
 
 def load(which):
@@ -130,6 +136,21 @@ class Block:
 
     def run_periodic(self, omega, steps):
         self._f("block_run_periodic")(self.h, ctypes.c_double(omega), ctypes.c_int(steps))
+
+    def run_periodic_mt(self, omega, steps, threads=None):
+        """run_periodic on several host threads (C restatement only), bitwise
+        equal to it."""
+        threads = threads or os.cpu_count() or 1
+        rc = self._f("block_run_periodic_mt")(self.h, ctypes.c_double(omega), ctypes.c_int(steps),
+                                              ctypes.c_int(threads))
+        assert rc == 0, "run_periodic_mt needs a block without a link table"
+
+    def fields(self):
+        """rho [nx][ny][nz] and u [nx][ny][nz][3] of the core (C restatement)."""
+        rho = np.zeros(self.shape)
+        u = np.zeros(self.shape + (3,))
+        self._f("block_fields")(self.h, _p(rho), _p(u))
+        return rho, u
 
     def run_walls(self, omega, steps, moving=None, wall_u=None):
         m = None if moving is None else np.ascontiguousarray(moving, np.uint8)

@@ -32,24 +32,19 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 HERE = os.path.dirname(os.path.abspath(__file__))
-SEED = 20261203
-N_DIRS = 8
+sys.path.insert(0, ROOT)
+from octlb_b200.cases import ADJOINT_SEED as SEED, ADJOINT_DIRS as N_DIRS  # noqa: E402
 
 
 def case(u_max=0.05, tau=None):
-    """The adjoint channel; tau defaults to the Re = 40 value."""
-    sys.path.insert(0, ROOT)
+    """The adjoint channel (octlb_b200.cases.adjoint_channel)."""
     from octlb_b200 import cases
-    mesh, init, info = cases.cylinder_forest(length=128, height=32, n=8, diameter=8.0, center=(32.0, 16.0),
-                                             levels=2, u_max=u_max, re=40.0)
-    if tau is not None:
-        info["tau"], info["omega"] = tau, 1.0 / tau
-    return mesh, init, info
+    return cases.adjoint_channel(u_max, tau)
 
 
 def directions(mesh):
-    rng = np.random.default_rng(SEED)
-    return rng.normal(0.0, 1e-6, size=(N_DIRS, mesh.n_blocks, mesh.n ** 3, 3))
+    from octlb_b200 import cases
+    return cases.adjoint_directions(mesh)
 
 
 def objective(job):

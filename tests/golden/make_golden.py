@@ -1,5 +1,5 @@
 """Generates the golden vectors in this folder from the reference's own code
-(oracle/_ref/liboctlb_ref.so, built by `make -C oracle ref` from the reference
+(oracle/_ref/liboctlb_ref.so, built by `make -C oracle ref REF=<reference tree>` from the reference
 sources).  Run from the repository root:  python tests/golden/make_golden.py
 """
 import os
@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 def main():
     ref = oracle.load("ref")
-    assert ref is not None, "build oracle/_ref first (make -C oracle ref)"
+    assert ref is not None, "build oracle/_ref first (make -C oracle ref REF=<reference tree>)"
     n, steps, omega = 6, 7, 1.7
     rng = np.random.default_rng(11)
     pin = rng.standard_normal((n + 2, n + 2, n + 2, 19)) * 1e-3

@@ -7,7 +7,10 @@ benchmark configurations, saved as small golden vectors:
   long_c2_amr.npz       two-level cavity, 64^3 base + refined band under the
                         lid, tau 0.56 (one global omega), lid 0.05, 625 coarse
                         steps (5,000 base-level steps): total mass per coarse
-                        step, centreline velocity profiles at the end
+                        step, centreline velocity profiles at the end, the
+                        final rho and u (float32) on every cell of even local
+                        indices (1 in 8, all blocks), and sum |u|^2, sum rho
+                        over all cells
   long_c3_cylinder.npz  three-level channel 256x64x64 finest cells, D = 16
                         exact-circle Bouzidi cylinder, u_max 0.05, Re 100,
                         2,500 coarse steps (20,000 finest steps): the
@@ -84,7 +87,7 @@ def main():
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
     ref = oracle.load("ref")
-    assert ref is not None, "build oracle/_ref first (make -C oracle ref)"
+    assert ref is not None, "build oracle/_ref first (make -C oracle ref REF=<reference tree>)"
     mesh, init, info, steps, links = config(args.name)
     sim = oracle.Sim(ref, mesh, info["omega"], init, link_mode=links)
     forces, masses = [], []
@@ -107,7 +110,13 @@ def main():
         np.savez_compressed(os.path.join(HERE, "long_c1_cavity.npz"), steps=steps,
                             rho=rho.astype(np.float32), u=u.astype(np.float32))
     elif args.name == "c2":
+        # the final fields on the cells of even local indices (1 cell in 8,
+        # every block of both levels) for the field-wide L2 of u, and the sums
+        # of |u|^2 and rho over every cell
+        lat = (slice(None), slice(0, None, 2), slice(0, None, 2), slice(0, None, 2))
         np.savez_compressed(os.path.join(HERE, "long_c2_amr.npz"), steps=steps, mass=np.asarray(masses),
+                            lattice_rho=rho[lat].astype(np.float32), lattice_u=u[lat].astype(np.float32),
+                            sum_u2=float(np.sum(u * u)), sum_rho=float(np.sum(rho)),
                             **centerlines(mesh, rho, u))
     else:
         np.savez_compressed(os.path.join(HERE, "long_c3_cylinder.npz"), steps=steps, force=np.asarray(forces))

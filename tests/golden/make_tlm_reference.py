@@ -1,6 +1,6 @@
 """Tangent-linear FP64 derivatives of the time-averaged drag for the adjoint
 configuration, computed by the reference's own TimeLoop on forward-mode dual
-numbers (oracle/_ref/liboctlb_ref_tlm.so, `make -C oracle tlm`), and saved as
+numbers (oracle/_ref/liboctlb_ref_tlm.so, `make -C oracle tlm REF=<reference tree>`), and saved as
 golden values beside the finite-difference ones of make_adjoint_reference.py:
 
   adjoint_c5_tlm.npz        1,000 advance_one calls, objective over the last 250
@@ -35,7 +35,7 @@ def tlm_objective(steps, window, u_max=0.05, progress=False):
     from oracle import oracle
     L = oracle.load("tlm")
     if L is None:
-        raise RuntimeError("oracle/_ref/liboctlb_ref_tlm.so is missing: make -C oracle tlm")
+        raise RuntimeError("oracle/_ref/liboctlb_ref_tlm.so is missing: make -C oracle tlm REF=<reference tree>")
     mesh, init, info = case(u_max)
     nd = L.tlm_dirs()
     omega = info["omega"]

@@ -74,12 +74,23 @@ def test_c2_amr_mass_drift_and_centrelines(ob, prec, tol_mass, tol_line):
         assert l2 <= tol_line, (k, l2)
 
 
-@pytest.mark.parametrize("prec,tol", [("fp32", 2e-4), ("fp16", 1e-3)])
-def test_c3_cylinder_time_averaged_drag(ob, prec, tol):
-    """Drag averaged over the last 5,000 finest steps (the last quarter)."""
+@pytest.mark.parametrize("prec,tol,tol_hist", [("fp32", 2e-4, 1e-4), ("fp16", 1e-3, 5e-3)])
+def test_c3_cylinder_time_averaged_drag_and_lift(ob, prec, tol, tol_hist):
+    """Drag and lift averaged over the last 5,000 finest steps (the last
+    quarter): drag within `tol` of the FP64 run relative to the drag, lift
+    within `tol` of it relative to the drag too (the time-averaged lift of
+    the symmetric channel is a small difference of large terms, so the drag
+    is its scale); the whole force history (all three components, every
+    coarse step) within `tol_hist` of max |F|."""
     fr = golden("long_c3_cylinder.npz")["force"]
     _, _, _, f = run(ob, "c3", ob.FP32 if prec == "fp32" else ob.FP16_SHIFTED)
-    last = slice(len(fr) - len(fr) // 4, None)
-    err = abs(f[last, 0].mean() - fr[last, 0].mean()) / abs(fr[last, 0].mean())
-    assert err <= tol, err
     assert np.all(np.isfinite(f))
+    last = slice(len(fr) - len(fr) // 4, None)
+    drag_ref = fr[last, 0].mean()
+    err_drag = abs(f[last, 0].mean() - drag_ref) / abs(drag_ref)
+    err_lift = abs(f[last, 1].mean() - fr[last, 1].mean()) / abs(drag_ref)
+    err_hist = float(np.max(np.abs(f - fr)) / np.max(np.abs(fr)))
+    print(f"c3 {prec}: drag {err_drag:.2e} lift {err_lift:.2e} history {err_hist:.2e}")
+    assert err_drag <= tol, err_drag
+    assert err_lift <= tol, err_lift
+    assert err_hist <= tol_hist, err_hist

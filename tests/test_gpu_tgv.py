@@ -1,0 +1,119 @@
+"""The throughput configuration's workload against FP64 runs of the
+reference's algorithm, on the GPU through the C ABI:
+
+* 64^3 Taylor-Green vortex (u0 = 0.05, tau = 0.55) for 1,000 steps against
+  the reference's own BlockLattice<double> run
+  (tests/golden/tgv64_reference.npz, tests/golden/make_tgv_reference.py):
+  the kinetic-energy history every 10 steps and the final rho, u on a 16^3
+  lattice of cells;
+* the headline size itself, 256^3, for 10 steps against the oracle's C
+  restatement of BlockLattice<double> (collide / fill_periodic_halo / stream,
+  pinned to the reference build at 1e-13) run on the host threads: every
+  cell's rho and u;
+* octlb_gpu_set_equilibrium (the fields-to-state entry the end-to-end bench
+  uses) equals octlb_gpu_set_populations of the same equilibrium.
+
+Tolerances (max |gpu - ref| / max |ref| over the cells): FP32 rho, u 1e-5;
+FP16-shifted 2e-3.  Kinetic energy (max over the history of |E_gpu - E_ref| /
+E_ref): FP32 1e-5; FP16-shifted 2e-3.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+TOL = {"fp32": 1e-5, "fp16": 2e-3}
+KE_TOL = {"fp32": 1e-5, "fp16": 2e-3}
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def prec_of(ob, name):
+    return ob.FP32 if name == "fp32" else ob.FP16_SHIFTED
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_tgv64_1000_steps_against_reference(ob, prec):
+    from octlb_b200 import cases
+    g = np.load(os.path.join(HERE, "golden", "tgv64_reference.npz"))
+    n, every, steps = int(g["n"]), int(g["every"]), int(g["steps"])
+    mesh, init, info = cases.tgv_periodic(n, u0=float(g["u0"]), tau=float(g["tau"]))
+    lat = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec), init_pops=init)
+    ke, mass = [], []
+    for k in range(steps // every + 1):
+        if k:
+            lat.advance(every)
+        rho, u = lat.get_fields()
+        ke.append(0.5 * float(np.sum(rho * np.sum(u * u, axis=-1))))
+        mass.append(float(np.sum(rho)))
+    lat.close()
+    ke = np.array(ke)
+    ke_err = float(np.max(np.abs(ke - g["ke"]) / g["ke"]))
+    sl = (0, slice(2, None, 4), slice(2, None, 4), slice(2, None, 4))
+    eu, er = rel(u[sl], g["sample_u"]), rel(rho[sl], g["sample_rho"])
+    print(f"tgv64 {prec}: ke {ke_err:.2e} u {eu:.2e} rho {er:.2e} decay {ke[-1] / ke[0]:.6f} "
+          f"(reference {g['ke'][-1] / g['ke'][0]:.6f})")
+    assert ke_err <= KE_TOL[prec]
+    assert eu <= TOL[prec] and er <= TOL[prec]
+    # the periodic BGK conserves mass to rounding
+    assert np.max(np.abs(np.array(mass) - g["mass"]) / g["mass"]) <= TOL[prec]
+    # the field-wide sums of the reference run
+    assert abs(float(np.sum(u * u)) - float(g["sum_u2"])) <= 2 * TOL[prec] * float(g["sum_u2"])
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_tgv256_headline_size_against_restatement(ob, orc, prec):
+    from octlb_b200 import cases
+    n, steps, tau = 256, 10, 0.55
+    rho0, u0 = cases.tgv_fields(n, n, n, 0.05)
+    mesh = ob.Mesh(n, [0], [0, 0, 0, 1, 1, 1], periodic=1)
+    lat = ob.GpuLattice(mesh, 1.0 / tau, precision=prec_of(ob, prec))
+    lat.set_equilibrium(rho0.reshape(-1), u0.reshape(-1, 3))
+    lat.advance(steps)
+    rho_g, u_g = lat.get_fields()
+    lat.close()
+    blk = oracle.Block(orc, n)
+    blk.set_core(ob.feq(rho0, u0))
+    blk.run_periodic_mt(1.0 / tau, steps)
+    rho_r, u_r = blk.fields()
+    del blk
+    eu, er = rel(u_g[0], u_r), rel(rho_g[0], rho_r)
+    print(f"tgv256 {prec}: u {eu:.2e} rho {er:.2e}")
+    assert eu <= TOL[prec] and er <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_set_equilibrium_equals_set_populations(ob, prec):
+    from octlb_b200 import cases
+    n = 32
+    rho0, u0 = cases.tgv_fields(n, n, n, 0.05)
+    mesh = ob.Mesh(n, [0], [0, 0, 0, 1, 1, 1], periodic=1)
+    a = ob.GpuLattice(mesh, 1.0 / 0.55, precision=prec_of(ob, prec))
+    b = ob.GpuLattice(mesh, 1.0 / 0.55, precision=prec_of(ob, prec))
+    a.set_equilibrium(rho0.reshape(-1), u0.reshape(-1, 3))
+    b.set_populations(ob.feq(rho0, u0))
+    assert np.array_equal(a.get_populations(), b.get_populations())
+    a.advance(3)
+    b.advance(3)
+    assert np.array_equal(a.get_populations(), b.get_populations())
+    a.close()
+    b.close()
+    # a forest mesh (kinds, several blocks, two levels)
+    mesh, init, info = cases.cavity_forest(cells=16, n=8, lid=0.1, tau=0.6, band_cells=8)
+    rng = np.random.default_rng(7)
+    cells = mesh.n_blocks * mesh.n ** 3
+    rho = 1.0 + 0.01 * rng.standard_normal(cells)
+    u = 0.03 * rng.standard_normal((cells, 3))
+    a = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec))
+    b = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec))
+    a.set_equilibrium(rho, u)
+    b.set_populations(ob.feq(rho, u))
+    assert np.array_equal(a.get_populations(), b.get_populations())
+    a.close()
+    b.close()

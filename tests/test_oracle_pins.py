@@ -18,6 +18,8 @@ import pytest
 
 from oracle import oracle
 
+HERE = os.path.dirname(os.path.abspath(__file__))
+
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 Q = 19
 C = np.array([[0, 0, 0], [-1, 0, 0], [0, -1, 0], [0, 0, -1], [-1, -1, 0], [-1, 1, 0], [-1, 0, -1],
@@ -210,3 +212,40 @@ def test_golden_amr_cavity_reference_state(ref):
     sim.advance(int(g["steps"]))
     rho, u = oracle.rho_u(sim.core())
     assert np.max(np.abs(rho - g["rho"])) < 1e-12 and np.max(np.abs(u - g["u"])) < 1e-12
+
+
+def test_threaded_restatement_reproduces_reference_tgv64_history(orc):
+    """The C restatement's threaded periodic loop (the checker of the 256^3
+    GPU test and of the bench's accuracy leg) reproduces the reference's own
+    BlockLattice<double> run of the 64^3 Taylor-Green vortex over 1,000 steps
+    (tests/golden/tgv64_reference.npz): kinetic energy and mass every 10
+    steps, final fields on the sampled lattice, all to 1e-12."""
+    from octlb_b200 import cases
+    g = np.load(os.path.join(HERE, "golden", "tgv64_reference.npz"))
+    n, every, steps = int(g["n"]), int(g["every"]), int(g["steps"])
+    mesh, init, info = cases.tgv_periodic(n, u0=float(g["u0"]), tau=float(g["tau"]))
+    b = oracle.Block(orc, n)
+    b.set_core(init[0])
+    ke = []
+    for k in range(steps // every + 1):
+        if k:
+            b.run_periodic_mt(info["omega"], every)
+        rho, u = b.fields()
+        ke.append(0.5 * float(np.sum(rho * np.sum(u * u, axis=-1))))
+    assert np.max(np.abs(np.array(ke) - g["ke"]) / g["ke"]) <= 1e-12
+    sl = (slice(2, None, 4),) * 3
+    assert np.max(np.abs(u[sl] - g["sample_u"])) <= 1e-12 * np.max(np.abs(g["sample_u"]))
+    assert np.max(np.abs(rho[sl] - g["sample_rho"])) <= 1e-12
+
+
+def test_threaded_restatement_is_the_serial_loop(orc):
+    """run_periodic_mt only shares the serial loop's work: bitwise equal."""
+    from octlb_b200 import cases
+    mesh, init, info = cases.tgv_periodic(20, u0=0.05, tau=0.55)
+    a = oracle.Block(orc, 20)
+    a.set_core(init[0])
+    a.run_periodic(info["omega"], 6)
+    b = oracle.Block(orc, 20)
+    b.set_core(init[0])
+    b.run_periodic_mt(info["omega"], 6, 3)
+    assert np.array_equal(a.padded(), b.padded())

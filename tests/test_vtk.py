@@ -18,7 +18,7 @@ REF_VTK = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 @pytest.fixture(scope="module")
 def ref_vtk():
     """The reference's writer as a program (oracle/_ref/ref_vtk, built with
-    `make -C oracle ref`)."""
+    `make -C oracle ref REF=<reference tree>`)."""
     if not os.path.exists(REF_VTK):
         pytest.skip("oracle/_ref/ref_vtk not built")
     return REF_VTK

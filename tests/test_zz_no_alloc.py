@@ -48,3 +48,41 @@ def test_audit_noalloc_matches_audit_twice(ob, case):
     lat.advance(3)
     assert close(audit_noalloc(ob, lat), lat.audit())
     lat.close()
+
+
+def test_audit_noalloc_rejects_levels_beyond_its_scratch(ob):
+    """A level of more cells than the fixed array covers (33,554,432) is
+    refused with OCTLB_EINVAL and a message that names the limit; nothing is
+    launched.  A periodic 324^3 box (34,012,224 cells) in FP16 storage, at
+    rest (no initial populations are uploaded)."""
+    n = 324
+    mesh = ob.Mesh(n, [0], [0, 0, 0, 1, 1, 1], periodic=1)
+    lat = ob.GpuLattice(mesh, 1.0 / 0.55, precision=ob.FP16_SHIFTED)
+    L = ob.capi.lib()
+    out = np.zeros(4)
+    rc = L.octlb_gpu_audit_noalloc(lat._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    msg = L.octlb_gpu_last_error(lat._h).decode()
+    assert rc == ob.capi.OCTLB_EINVAL, (rc, msg)
+    assert "33554432" in msg and str(n ** 3) in msg, msg
+    # the allocating audit still covers it: the state at rest, mass = cells
+    assert abs(lat.audit()[0] - n ** 3) <= 1e-9 * n ** 3
+    lat.close()
+
+
+def test_audit_noalloc_reports_a_bounded_wait_that_gave_up(ob, monkeypatch):
+    """After a bounded device wait gave up (the test stall of the bulk-copy
+    step: one CTA waits for a row it never requested, 50 ms limit), the
+    allocation-free audit reports OCTLB_ETIMEOUT as octlb_gpu_audit does,
+    instead of summing the partly written state."""
+    from octlb_b200 import cases
+    monkeypatch.setenv("OCTLB_STEP_KERNEL", "bulk")
+    monkeypatch.setenv("OCTLB_TEST_BULK_STALL", "1")
+    monkeypatch.setenv("OCTLB_WAIT_MS", "50")
+    mesh, init, info = cases.tgv_periodic(64, u0=0.05, tau=0.55)
+    lat = ob.GpuLattice(mesh, info["omega"], init_pops=init)
+    lat.advance(1)
+    L = ob.capi.lib()
+    out = np.zeros(4)
+    rc = L.octlb_gpu_audit_noalloc(lat._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    assert rc == ob.capi.OCTLB_ETIMEOUT, (rc, L.octlb_gpu_last_error(lat._h).decode())
+    lat.close()
