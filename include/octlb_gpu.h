@@ -241,6 +241,58 @@ int octlb_gpu_audit(octlb_ctx* ctx, double out[4]);
  * array: calls that overlap on the GPU race. */
 int octlb_gpu_audit_noalloc(octlb_ctx* ctx, double out[4]);
 
+/* ---- Ranks: the leaves shared over several contexts -----------------------
+ * The reference runs one MPI rank per core: p4est partitions the leaves by
+ * weight (OctreeForest::partition with make_level_weight_fn, weight 2^level,
+ * octree_forest.cpp:273-280, weighted_load_balancer.cpp:7-12), GhostSchedule
+ * exchanges face and edge layers between ranks before every level step
+ * (ghost_schedule.h:121-255), LevelCoupler sends its interface payloads
+ * across ranks (level_coupler.cpp:325-436, 492-585) and the cases sum the
+ * force and mass with MPI_Allreduce (cylinder3d_case.h:502, 620).  Here one
+ * context per GPU (a "rank context") steps the leaves its rank owns; it keeps
+ * the same-level neighbours of its leaves that other ranks own as mirror
+ * blocks, refreshed before every step of their level, and receives the save
+ * rows (pre-collision populations of coupler source cells) its coupler items
+ * read after every step of their level.  Forces and audits come back summed
+ * over the ranks.  Every rank passes the same global tables and initial
+ * state; get_fields / get_populations / set_* / write_vtk touch the rank's
+ * own blocks only.  ConstRhoBGK and the adjoint are single-context only. */
+
+/* The reference's partition: leaves in the forest's order, weight 2^level;
+ * rank k owns the leaves whose weight prefix lies in [k W / P, (k+1) W / P). */
+int octlb_gpu_partition(const octlb_tables* tables, int nranks, int* owner);
+
+/* Transport between the rank contexts.  Every rank context makes the same
+ * exchanges in the same order (its octlb_gpu_advance calls), so every rank
+ * must advance by the same number of steps. */
+typedef struct octlb_comm octlb_comm;
+/* The rank contexts of one process, each driven by its own host thread (on
+ * one device or several): device copies ordered by events, two host barriers
+ * per exchange; a rank that does not arrive within OCTLB_COMM_TIMEOUT_S
+ * seconds (default 60) ends the others' calls with OCTLB_ETIMEOUT. */
+int octlb_comm_create_local(int nranks, octlb_comm** out);
+/* One process per GPU over NCCL (opened at run time): rank 0 makes the id,
+ * every rank passes it (through the caller's launcher) to create_nccl with
+ * its device current.  Synchronising calls give up after
+ * OCTLB_COMM_TIMEOUT_S seconds (default 300) and abort the communicator. */
+int octlb_comm_nccl_unique_id(unsigned char id[128]);
+int octlb_comm_create_nccl(const unsigned char id[128], int nranks, int rank, octlb_comm** out);
+/* After every context using it is destroyed. */
+void octlb_comm_destroy(octlb_comm* comm);
+/* Why the NCCL transport could not be opened (empty if it could). */
+const char* octlb_comm_last_error(void);
+
+typedef struct octlb_partition {
+  int rank;                       /* this context's rank */
+  int nranks;
+  const int* owner;               /* [n_blocks] owning rank of every leaf */
+  octlb_comm* comm;
+} octlb_partition;
+
+/* octlb_gpu_create for one rank of a partition. */
+int octlb_gpu_create_part(const octlb_tables* tables, const octlb_params* params, const double* init_pops,
+                          const octlb_partition* part, octlb_ctx** out);
+
 /* Host-only dry run of octlb_gpu_create: validates and flattens the tables
  * (every index the kernels derive is bounds-checked) without touching a
  * device, and reports the plan: stats[0] = levels, then per level 10 values
@@ -248,6 +300,16 @@ int octlb_gpu_audit_noalloc(octlb_ctx* ctx, double out[4]);
  * restriction items, saved cells, link records, drag cells, slots).  Returns
  * the number of values, or a negative error code. */
 int octlb_gpu_plan(const octlb_tables* tables, const octlb_params* params, long long* stats, int max_stats);
+
+/* Host-only dry run of octlb_gpu_create_part for `rank` (no comm, no
+ * device): validates and flattens the tables as that rank would and writes
+ * its exchange lists as records of 4 values -- level, kind (0 cells sent, 1
+ * cells received before each step of the level; 2 save rows sent, 3 save
+ * rows received after it), peer rank, global cell (block * n^3 + cell) -- in
+ * the order they travel.  Returns the number of records (at most
+ * max_records are written), or a negative error code. */
+int octlb_gpu_plan_part(const octlb_tables* tables, const octlb_params* params, int rank, int nranks,
+                        const int* owner, long long* records, long long max_records);
 
 /* Per-level collide / stream counts and max level (TimeLoop::counters). */
 int octlb_gpu_counters(const octlb_ctx* ctx, int* collide, int* stream, int max_levels);

@@ -226,11 +226,85 @@ def vtk_write_index(output_dir, base_name, step, vts_relative_paths):
         raise OctlbError(rc, "vtk_write_index failed")
 
 
+def partition(mesh, nranks):
+    """The reference's weighted partition (octlb_gpu_partition): owning rank
+    of every leaf, contiguous runs of the forest order of equal 2^level
+    weight."""
+    owner = np.zeros(mesh.n_blocks, np.int32)
+    rc = capi.lib().octlb_gpu_partition(ctypes.byref(mesh.c_tables()), int(nranks), capi.ptr(owner, ctypes.c_int))
+    if rc:
+        raise OctlbError(rc, "partition failed")
+    return owner
+
+
+def plan_part(mesh, omega, rank, owner, precision=FP32, stream_mode=STREAM_ROTATE, drag=False):
+    """Host-only dry run of a rank context (octlb_gpu_plan_part): its
+    exchange lists as an int64 array of (level, kind, peer, global cell)
+    rows, kind 0 / 1 cells sent / received before a level step, 2 / 3 save
+    rows sent / received after it."""
+    L = capi.lib()
+    p = capi.Params()
+    p.omega, p.precision, p.stream_mode, p.drag = float(omega), int(precision), int(stream_mode), int(bool(drag))
+    own = np.ascontiguousarray(owner, np.int32)
+    nranks = int(own.max()) + 1
+    n = L.octlb_gpu_plan_part(ctypes.byref(mesh.c_tables()), ctypes.byref(p), int(rank), nranks,
+                              capi.ptr(own, ctypes.c_int), None, 0)
+    if n < 0:
+        raise OctlbError(n, "plan_part failed")
+    out = np.zeros((max(n, 1), 4), np.int64)
+    n = L.octlb_gpu_plan_part(ctypes.byref(mesh.c_tables()), ctypes.byref(p), int(rank), nranks,
+                              capi.ptr(own, ctypes.c_int), out.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                              len(out))
+    return out[:n]
+
+
+class Comm:
+    """Transport between rank contexts (octlb_comm): ``Comm.local(n)`` for n
+    rank contexts of this process (one host thread each), ``Comm.nccl(id, n,
+    rank)`` for one process per GPU (``Comm.nccl_unique_id()`` on rank 0,
+    shared by the caller's launcher)."""
+
+    def __init__(self, handle, nranks):
+        self._h, self.nranks = handle, nranks
+
+    @classmethod
+    def local(cls, nranks):
+        h = capi.P()
+        rc = capi.lib().octlb_comm_create_local(int(nranks), ctypes.byref(h))
+        if rc:
+            raise OctlbError(rc, "local comm")
+        return cls(h, nranks)
+
+    @staticmethod
+    def nccl_unique_id():
+        buf = (ctypes.c_ubyte * 128)()
+        rc = capi.lib().octlb_comm_nccl_unique_id(buf)
+        if rc:
+            raise OctlbError(rc, "nccl unique id: " + capi.lib().octlb_comm_last_error().decode())
+        return bytes(buf)
+
+    @classmethod
+    def nccl(cls, uid, nranks, rank):
+        buf = (ctypes.c_ubyte * 128).from_buffer_copy(uid)
+        h = capi.P()
+        rc = capi.lib().octlb_comm_create_nccl(buf, int(nranks), int(rank), ctypes.byref(h))
+        if rc:
+            raise OctlbError(rc, "nccl comm: " + capi.lib().octlb_comm_last_error().decode())
+        return cls(h, nranks)
+
+    def close(self):
+        if self._h:
+            capi.lib().octlb_comm_destroy(self._h)
+            self._h = None
+
+
 class GpuLattice:
-    """One octlb_gpu context (include/octlb_gpu.h)."""
+    """One octlb_gpu context (include/octlb_gpu.h).  With ``part=(rank,
+    owner, comm)`` a rank context (octlb_gpu_create_part) stepping the leaves
+    with owner == rank."""
 
     def __init__(self, mesh, omega, precision=FP32, stream_mode=STREAM_ROTATE, drag=False,
-                 init_pops=None, fp16_scale=None):
+                 init_pops=None, fp16_scale=None, part=None):
         self._L = capi.lib()
         self.mesh = mesh
         self.omega = float(omega)
@@ -245,8 +319,17 @@ class GpuLattice:
         if self._init is not None:
             assert self._init.size == mesh.n_blocks * mesh.n ** 3 * Q
         h = capi.P()
-        rc = self._L.octlb_gpu_create(ctypes.byref(mesh.c_tables()), ctypes.byref(p),
-                                      capi.ptr(self._init, ctypes.c_double), ctypes.byref(h))
+        self.rank, self.owner = 0, None
+        if part is None:
+            rc = self._L.octlb_gpu_create(ctypes.byref(mesh.c_tables()), ctypes.byref(p),
+                                          capi.ptr(self._init, ctypes.c_double), ctypes.byref(h))
+        else:
+            rank, owner, comm = part
+            self.rank, self.owner = int(rank), np.ascontiguousarray(owner, np.int32)
+            pt = capi.Partition(self.rank, comm.nranks, capi.ptr(self.owner, ctypes.c_int), comm._h)
+            rc = self._L.octlb_gpu_create_part(ctypes.byref(mesh.c_tables()), ctypes.byref(p),
+                                               capi.ptr(self._init, ctypes.c_double), ctypes.byref(pt),
+                                               ctypes.byref(h))
         self._h = h
         if rc != 0:
             msg = self._L.octlb_gpu_last_error(h).decode() if h else "create failed"

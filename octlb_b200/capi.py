@@ -60,6 +60,12 @@ class AdjParams(ctypes.Structure):
 VTK_VELOCITY, VTK_DENSITY, VTK_PRESSURE = 1, 2, 4
 
 
+class Partition(ctypes.Structure):
+    """octlb_partition."""
+    _fields_ = [("rank", ctypes.c_int), ("nranks", ctypes.c_int), ("owner", ctypes.POINTER(ctypes.c_int)),
+                ("comm", ctypes.c_void_p)]
+
+
 class Params(ctypes.Structure):
     _fields_ = [
         ("omega", ctypes.c_double), ("precision", ctypes.c_int), ("stream_mode", ctypes.c_int),
@@ -80,6 +86,18 @@ def lib():
     L = ctypes.CDLL(LIB_PATH)
     sig = {
         "octlb_gpu_create": (ctypes.c_int, [ctypes.POINTER(Tables), ctypes.POINTER(Params), F64P, ctypes.POINTER(P)]),
+        "octlb_gpu_create_part": (ctypes.c_int, [ctypes.POINTER(Tables), ctypes.POINTER(Params), F64P,
+                                                 ctypes.POINTER(Partition), ctypes.POINTER(P)]),
+        "octlb_gpu_partition": (ctypes.c_int, [ctypes.POINTER(Tables), ctypes.c_int, I32P]),
+        "octlb_gpu_plan_part": (ctypes.c_int, [ctypes.POINTER(Tables), ctypes.POINTER(Params), ctypes.c_int,
+                                               ctypes.c_int, I32P, ctypes.POINTER(ctypes.c_longlong),
+                                               ctypes.c_longlong]),
+        "octlb_comm_create_local": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(P)]),
+        "octlb_comm_nccl_unique_id": (ctypes.c_int, [ctypes.POINTER(ctypes.c_ubyte)]),
+        "octlb_comm_create_nccl": (ctypes.c_int, [ctypes.POINTER(ctypes.c_ubyte), ctypes.c_int, ctypes.c_int,
+                                                  ctypes.POINTER(P)]),
+        "octlb_comm_destroy": (None, [P]),
+        "octlb_comm_last_error": (ctypes.c_char_p, []),
         "octlb_gpu_destroy": (None, [P]),
         "octlb_gpu_last_error": (ctypes.c_char_p, [P]),
         "octlb_gpu_set_stream": (ctypes.c_int, [P, P]),

@@ -432,7 +432,8 @@ __global__ void __launch_bounds__(kThreads) k_step_pair(const StepArgs a) {
   const uint32_t row = a.div_n.div(2 * t);  // = t / (n / 2)
   const uint32_t z = (t - row * half) * 2;
   const uint32_t x = a.div_n.div(row), y = row - x * n;
-  const uint32_t xm = x == 0 ? n - 1 : x - 1, xp = x == n - 1 ? 0 : x + 1;
+  const uint32_t xm = x == 0 ? static_cast<uint32_t>(a.wrap_lo) : x - 1;
+  const uint32_t xp = x == n - 1 ? static_cast<uint32_t>(a.wrap_hi) : x + 1;
   const uint32_t ym = y == 0 ? n - 1 : y - 1, yp = y == n - 1 ? 0 : y + 1;
   const uint32_t zm2 = z == 0 ? n - 2 : z - 2, zp2 = z + 2 == n ? 0 : z + 2;
   const T* src = static_cast<const T*>(a.src);

@@ -2,304 +2,7 @@
 // into per-level device tables, owns every device allocation, and drives the
 // reference's recursive subcycling (TimeLoop::advance, time_loop.h:201-240) as
 // a sequence of kernel launches on one stream.
-#include <algorithm>
-#include <array>
-#include <cmath>
-#include <cstdio>
-#include <cstdlib>
-#include <cstring>
-#include <filesystem>
-#include <map>
-#include <memory>
-#include <mutex>
-#include <set>
-#include <string>
-#include <unordered_set>
-#include <vector>
-
-#include "octlb_internal.h"
-#include "../../include/octlb_gpu.h"
-
-namespace octlb_gpu {
-
-template <typename T> cudaError_t launch_step(const StepArgs&, bool, bool, bool, cudaStream_t);
-template <typename T>
-cudaError_t launch_couple(const ProlongOp&, const RestrictOp&, const RestrictOp&, cudaStream_t);
-template <typename T>
-cudaError_t launch_drag(const StepArgs&, bool, const DragItem*, int, double*, cudaStream_t);
-cudaError_t launch_drag_total(const double*, int, double*, double*, cudaStream_t);
-template <typename T> cudaError_t launch_audit(const StepArgs&, double*, double*, cudaStream_t);
-template <typename T> cudaError_t launch_gather(const StepArgs&, double*, double*, int, cudaStream_t);
-template <typename T> cudaError_t launch_scatter(const StepArgs&, const double*, int, cudaStream_t);
-template <typename T> cudaError_t launch_scatter_eq(const StepArgs&, const double*, int, cudaStream_t);
-template <typename T>
-cudaError_t launch_step_cr(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
-template <typename T> cudaError_t launch_cr_seed(const StepArgs&, int, cudaStream_t);
-template <typename T>
-cudaError_t launch_step_map_cr(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
-cudaError_t launch_cr_update(double*, const double*, int, long long, cudaStream_t);
-uint32_t cr_core_parts(const StepArgs& a);
-uint32_t cr_near_parts(const NearTables& nt);
-template <typename T> cudaError_t launch_step_bulk(const StepArgs&, int, cudaStream_t);
-template <typename T> int bulk_prepare(int n);
-template <typename T> cudaError_t launch_step_pair(const StepArgs&, cudaStream_t);
-template <typename T> cudaError_t launch_step_near(const StepArgs&, const NearTables&, cudaStream_t);
-template <typename T> cudaError_t launch_add_force(const StepArgs&, T*, const float*, cudaStream_t);
-template <typename T> cudaError_t launch_step_map(const StepArgs&, const NearTables&, bool, bool, int, bool, cudaStream_t);
-bool pair_step_eligible(int n);
-bool map_step_eligible(int n, long long nslots);
-void set_programmatic_launch(bool on);
-cudaError_t launch_adj_step(const StepArgs&, const NearTables&, bool, bool, float*, float*, float*, double*, double*,
-                            cudaStream_t);
-cudaError_t launch_adj_force(const StepArgs&, const float*, double*, cudaStream_t);
-cudaError_t launch_adj_drag(const StepArgs&, bool, const DragItem*, int, float*, float, int, double*, cudaStream_t);
-cudaError_t launch_adj_prolong(const ProlongItem*, int, const float*, const float*, int, float*, long long, float,
-                               float, float*, float*, float*, double*, double*, long long, cudaStream_t);
-cudaError_t launch_adj_restrict(const RestrictItem*, int, const float*, float*, long long, float, float, float*,
-                                double*, double*, long long, cudaStream_t);
-bool bulk_step_eligible(int n, int elem_bytes);
-uint32_t drag_partials(int n);
-uint32_t audit_partials(const StepArgs& a);
-
-namespace {
-
-// Host-only planning (octlb_gpu_plan): every allocation, upload and launch is
-// skipped while the tables are flattened and checked.
-thread_local bool g_dry_run = false;
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  DevBuf() = default;
-  DevBuf(const DevBuf&) = delete;
-  DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
-  ~DevBuf() { if (p) cudaFree(p); }
-  cudaError_t alloc(size_t b) {
-    if (p) { cudaFree(p); p = nullptr; }
-    bytes = b;
-    if (g_dry_run) return cudaSuccess;
-    if (b == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(&p, b);
-    if (e == cudaSuccess) e = cudaMemset(p, 0, b);
-    // The zero fill runs on the legacy default stream, which the context's
-    // non-blocking streams do not wait for: it must land before any of them
-    // touches the buffer.
-    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
-    return e;
-  }
-  // Capacity of at least b bytes, kept across calls and not zero-filled:
-  // staging that every use overwrites before it is read.
-  cudaError_t reserve(size_t b) {
-    if (p && bytes >= b) return cudaSuccess;
-    if (p) { cudaFree(p); p = nullptr; }
-    bytes = b;
-    if (g_dry_run || b == 0) return cudaSuccess;
-    return cudaMalloc(&p, b);
-  }
-  template <typename U> U* as() const { return static_cast<U*>(p); }
-};
-
-template <typename U>
-cudaError_t upload(DevBuf& d, const std::vector<U>& h) {
-  cudaError_t e = d.alloc(h.size() * sizeof(U));
-  if (e != cudaSuccess || h.empty() || g_dry_run) return e;
-  e = cudaMemcpy(d.p, h.data(), h.size() * sizeof(U), cudaMemcpyHostToDevice);
-  // From pageable memory cudaMemcpy may return before its last DMA chunk has
-  // landed (on the legacy stream, which the context's non-blocking streams do
-  // not wait for); a kernel on those streams would read the buffer's tail
-  // early.
-  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
-  return e;
-}
-
-struct PlanPoint {  // CouplingPoint (level_coupler.h:18-30)
-  int coarse_id, ci, cj, ck, fine_id, fi, fj, fk, normal, coarse_level, fine_level, slot;
-};
-
-struct Level {
-  int lvl = 0;
-  std::vector<int> blocks;          // global block ids, level-local order
-  int nblk = 0, n = 0;
-  long long ncore = 0, nslots = 0;  // core slots, core + halo-page slots
-  DevBuf buf[2];
-  int cur = 0;
-  DevBuf flags, link_idx, link_rec, save_idx, save_buf;
-  DevBuf nbase, page_of, hmap, hpos, open_pages, near_cells, slot_map;
-  DevBuf near_mask, near_slot, near_q, near_add;
-  NearTables near{};
-  int n_near = 0;
-  int n_open = 0, n_halo = 0, n_pages = 0, n_save = 0, n_links = 0;
-  long long n_bulk = 0;             // kBulk core cells
-  bool has_flags = false;
-  // tree-boundary halo fills
-  DevBuf bb_ops, fill_of;           // fills, and per (page slot, population) the fill index or -1
-  DevBuf wall_add, wall_dadd;       // slot-map wall markers' terms
-  DevBuf blk_moving;                // per block: its map holds a moving-wall marker
-  uint32_t n_bb = 0;
-  // coupler: this level as coarse (prolong) and as fine (restrict)
-  DevBuf prolong_items, prev, restrict_items;
-  // The restriction into this level (from level + 1) may share a launch with
-  // the full-time prolongation into it (from level - 1): their target cells
-  // are disjoint.
-  bool fuse_restrict = false;
-  int n_prolong = 0, n_restrict = 0;
-  // drag
-  DevBuf drag_items;
-  int n_drag = 0;
-  long long drag_off = 0;           // this level's rows in the context's drag partials
-  int substep = 0;                  // steps of this level within the current advance_one
-  float scale = 1.f, inv_scale = 1.f;
-  bool use_bulk = false;            // pipelined bulk-copy step (periodic block)
-  bool use_pair = false;            // two-cells-per-thread step (periodic block)
-  bool use_map = false;             // slot-map step (forest level)
-  int bulk_grid = 0;
-  DevBuf body_force;                // [3][ncore] float, or empty
-  bool has_force = false;
-  // While the adjoint recomputes a segment, the level's state and save rows
-  // live in the step records' buffers (null otherwise).
-  void* rec_cur = nullptr;
-  void* rec_save = nullptr;
-  StepArgs args{};
-};
-
-inline void* cur_buf(Level& L) { return L.rec_cur ? L.rec_cur : L.buf[L.cur].p; }
-inline float* save_ptr(Level& L) { return static_cast<float*>(L.rec_save ? L.rec_save : L.save_buf.p); }
-
-// Forward state of one level step kept for the reverse sweep: the step's
-// input after the body force and the boundary fills, the save rows it wrote,
-// and (coarse levels) the prev-macro store before its half-time prolongation.
-constexpr int kGradSlots = 4;       // d/d omega, d/d prolong scale, d/d restrict scale, d/d wall velocity
-
-struct StepRecord {
-  int level = -1;
-  DevBuf snap, save, prev;
-  bool drag = false;                // the objective's force is taken from this input
-};
-
-// Adjoint sweep state (octlb_gpu_adjoint): cotangents per level, the
-// checkpoints of one run and the step records of one recomputed segment.
-struct AdjointState {
-  struct Lv {
-    DevBuf lam[2];                  // cotangent of the level's populations ([19][slots] FP32)
-    int cur = 0;
-    DevBuf lam_save, lam_m, lam_prev, gF;
-  };
-  std::vector<Lv> lv;
-  // Two record sets, one per segment parity: the recomputation of the next
-  // segment (set (c - 1) % 2) runs on rstream beside the reverse of the
-  // current one (set c % 2) on the context's stream.
-  std::vector<StepRecord> recs;     // [2][set_size]
-  size_t set_size = 0;
-  std::vector<int> next_same;       // next record of the same level in the same set, or -1
-  std::vector<int> first_rec;       // first record of each level in set 0, or -1 (set 1: + set_size)
-  size_t nrec = 0;
-  cudaStream_t rstream = nullptr;
-  cudaEvent_t ev_fwd = nullptr, ev_rec[2] = {nullptr, nullptr}, ev_rev[2] = {nullptr, nullptr};
-  bool recording = false;
-  int last_rec[32] = {};
-  DevBuf g;                         // parameter-gradient accumulators (FP64)
-  struct Checkpoint {
-    std::vector<DevBuf> buf, prev;
-    std::vector<int> cur;
-  };
-  std::vector<Checkpoint> ck;
-  int comp = 0;
-  // Recomputation (kind 0) and reverse (kind 1) of one segment captured as
-  // CUDA graphs, keyed by (kind, buffer or cotangent parity, steps, steps in
-  // the objective's window); valid for one adjoint call.
-  struct Graph {
-    cudaGraphExec_t exec = nullptr;
-    uint64_t out_mask = 0;
-  };
-  std::map<std::array<long long, 4>, Graph> graphs;
-  std::array<long long, 4> graph_params{};  // (steps, window, interval, component) the graphs were made for
-  void clear_graphs() {
-    for (auto& kv : graphs)
-      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    graphs.clear();
-  }
-  AdjointState() = default;
-  AdjointState(const AdjointState&) = delete;
-  AdjointState& operator=(const AdjointState&) = delete;
-  ~AdjointState() {
-    if (rstream) cudaStreamSynchronize(rstream);
-    clear_graphs();
-    for (cudaEvent_t e : {ev_fwd, ev_rec[0], ev_rec[1], ev_rev[0], ev_rev[1]})
-      if (e) cudaEventDestroy(e);
-    if (rstream) cudaStreamDestroy(rstream);
-  }
-};
-
-}  // namespace
-}  // namespace octlb_gpu
-
-using namespace octlb_gpu;
-
-struct octlb_ctx {
-  std::string err;
-  int n = 0, n_blocks = 0, precision = 0, stream_mode = 0, periodic = 0, drag = 0;
-  double omega = 1.0;
-  int max_level = 0;
-  std::vector<Level> levels;
-  std::vector<int> blk_level, blk_local;
-  std::vector<uint8_t> kinds;
-  std::vector<double> bounds;       // [n_blocks][6] leaf bounds (VTK output)
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  // Restrictions not launched yet: each shares the next coupler launch unless
-  // a step comes first (then they are launched alone, two per launch).
-  struct PendingRestrict {
-    RestrictOp op;
-    int level;  // the coarse level written
-  };
-  std::vector<PendingRestrict> pending_restrict;
-  // The momentum-exchange force runs on a forked stream inside advance_one
-  // (it only reads the last finest step's input) and joins at its end.
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  bool side_busy = false;
-  DevBuf drag_partial, force, force_sum, audit_out, audit_partial, host_tmp, dev_err;
-  // FP64 host-layout staging of set/get_populations and get_fields (grown on
-  // demand, kept until destroy: no allocation per call)
-  DevBuf stage_a, stage_b;
-  int drag_parts = 0;
-  long long force_steps = 0;
-  std::vector<int> counters_collide, counters_stream;
-  long long launches_per_step = 0, lups_per_step = 0;
-  long long launch_count = 0;       // kernels issued by the advance_one being built
-  int step_kernel = 0;              // OCTLB_STEP_KERNEL: 0 pair (default), 1 bulk, 2 plain
-  bool map_global = true;           // slot map read through L1 (OCTLB_MAP_SMEM=1: staged in shared memory)
-  // Bounded device waits: their limit (OCTLB_WAIT_MS, default 1 s) and the
-  // test of the give-up path (OCTLB_TEST_BULK_STALL=1: one CTA of the bulk
-  // step waits for a row it never requested).  After a give-up whose own
-  // copies did not drain either, the context refuses further work.
-  unsigned long long wait_ns = 1000000000ull;
-  int stall_first_row = 0;
-  bool unusable = false;
-  int map_cells = 0;                // cells per thread of the slot-map step (OCTLB_MAP_CELLS 1 or 2;
-                                    // default 2, 1 under the links rule whose variant spills at 2)
-  // advance_one captured as CUDA graphs, keyed by the A/B parity of every
-  // level's buffers (the launch arguments depend on it)
-  struct GraphEntry {
-    cudaGraphExec_t exec = nullptr;
-    uint64_t out_mask = 0;
-    std::vector<int> dcollide;
-  };
-  std::map<uint64_t, GraphEntry> graphs;
-  bool use_graphs = true;           // OCTLB_NO_GRAPH=1 launches kernel by kernel
-  bool use_pdl = true;              // OCTLB_NO_PDL=1: plain stream order between the step's kernels
-  float prolong_scale = 0.f, restrict_scale = 0.f;
-  double wall_vscale = 0.0;         // largest moving-wall speed (adjoint velocity parameter)
-  std::unique_ptr<AdjointState> adj;
-  // ConstRhoBGK (TimeLoop's use_const_rho_bgk, single-level meshes): the
-  // average density on the device (TimeLoop::average_rho_) and the partial
-  // sums of the last collide's statistics, over cr_count kBulk cells
-  bool const_rho = false;
-  DevBuf cr_avg, cr_part;
-  int cr_level = -1, cr_nparts = 0, cr_near = 0;
-  long long cr_count = 0;
-};
+#include "octlb_ctx.h"
 
 namespace octlb_host {
 
@@ -309,16 +12,6 @@ int fail(octlb_ctx* c, int code, const std::string& msg) {
 }
 int cuda_fail(octlb_ctx* c, cudaError_t e, const char* where) {
   return fail(c, OCTLB_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
-}
-#define CK(call)                                                   \
-  do {                                                             \
-    cudaError_t e_ = (call);                                       \
-    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);       \
-  } while (0)
-
-inline long long core_slot_of(int n, int local_blk, int x, int y, int z) {
-  const long long n3 = static_cast<long long>(n) * n * n;
-  return local_blk * n3 + (static_cast<long long>(x) * n + y) * n + z;
 }
 
 // Coupling plan of the reference (AppendFaceCouplingPoints,
@@ -389,18 +82,25 @@ int flush_restricts(octlb_ctx* ctx) {
 
 template <typename T>
 int launch_level_step(octlb_ctx* ctx, Level& L) {
-  if (L.nblk == 0) return OCTLB_OK;
+  if (L.nblk == 0) {
+    // A rank context with no block on this level still takes part in the
+    // level's two exchanges (it may receive save rows for its coupler items).
+    if (int rc = exchange_cells<T>(ctx, L)) return rc;
+    return exchange_rows(ctx, L);  // (slab contexts own every level's block)
+  }
   { const int rc = flush_restricts<T>(ctx); if (rc) return rc; }  // the step reads what they write
   // Body force on the stored post-collision state (the reference's apply()
   // hook after collide, time_loop.h:207-211).  The boundary fills and the
   // same-level exchange that follow there need no launch: the step reads
   // neighbour cores through the slot map and fill targets from their
-  // sources.
+  // sources.  Rank contexts then refresh their mirror blocks: the cells of
+  // other ranks' blocks this level's pulls read.
   T* cur = static_cast<T*>(cur_buf(L));
   if (L.has_force) {
     CK(launch_add_force<T>(L.args, cur, L.body_force.as<float>(), ctx->stream));
     ++ctx->launch_count;
   }
+  if (int rc = ctx->slab ? exchange_slab<T>(ctx, L) : exchange_cells<T>(ctx, L)) return rc;
 
   StepArgs a = L.args;
   a.src = cur;
@@ -469,7 +169,8 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
   ++L.substep;
   L.cur = 1 - L.cur;
   if (rec) L.rec_cur = next_cur;
-  return OCTLB_OK;
+  // the save rows other ranks' coupler items read, and those this rank's read
+  return exchange_rows(ctx, L);
 }
 
 template <typename T>
@@ -613,9 +314,58 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
   ctx->prolong_scale = static_cast<float>((tau - 0.25) / tau);   // level_coupler.cpp:226-228
   ctx->restrict_scale = static_cast<float>(tau / (tau - 0.25));
   for (int l = 0; l < nlev; ++l) ctx->levels[l].lvl = l;
+  std::vector<int> face_nbr(static_cast<size_t>(nb) * 6, -1);
+  for (int k = 0; k < t->n_same_level; ++k) {
+    const int* r = t->same_level + 3 * k;
+    face_nbr[static_cast<size_t>(r[0]) * 6 + r[1]] = r[2];
+  }
+  if (ctx->periodic)
+    for (int d = 0; d < 6; ++d) face_nbr[d] = 0;  // fill_periodic_halo: the block is its own neighbour
+  // Diagonal (edge) neighbour: two face steps in either order, the
+  // composition GhostSchedule uses for its same-level edge exchange.
+  auto edge_nbr = [&](int a, int d1, int d2) {
+    int b = face_nbr[static_cast<size_t>(a) * 6 + d1];
+    if (b >= 0 && face_nbr[static_cast<size_t>(b) * 6 + d2] >= 0) return face_nbr[static_cast<size_t>(b) * 6 + d2];
+    b = face_nbr[static_cast<size_t>(a) * 6 + d2];
+    if (b >= 0 && face_nbr[static_cast<size_t>(b) * 6 + d1] >= 0) return face_nbr[static_cast<size_t>(b) * 6 + d1];
+    return -1;
+  };
+  // Same-level neighbour of global block gb in halo direction (ox, oy, oz):
+  // itself (centre), the face neighbour, the composed edge neighbour, or -1
+  // (corners: the exchange fills no corner ghosts, D3Q19 has no corner links).
+  auto nbr_dir = [&](int gb, int ox, int oy, int oz) {
+    const int o[3] = {ox, oy, oz};
+    int dirs[3], nd = 0;
+    for (int a = 0; a < 3; ++a)
+      if (o[a]) dirs[nd++] = 2 * a + (o[a] > 0 ? 1 : 0);
+    if (nd == 0) return gb;
+    if (nd == 1) return face_nbr[static_cast<size_t>(gb) * 6 + dirs[0]];
+    if (nd == 2) return edge_nbr(gb, dirs[0], dirs[1]);
+    return -1;
+  };
+  // Owned blocks first (global order), then the mirror blocks: neighbours
+  // (face or edge) of owned blocks that another rank owns.
+  std::vector<char> mirror(static_cast<size_t>(nb), 0);
   for (int b = 0; b < nb; ++b) {
-    Level& L = ctx->levels[t->levels[b]];
     ctx->blk_level[b] = t->levels[b];
+    if (!ctx->owns(b)) continue;
+    for (int d = 0; d < 27; ++d) {
+      if (d == 13) continue;
+      const int v = nbr_dir(b, d / 9 - 1, (d / 3) % 3 - 1, d % 3 - 1);
+      if (v >= 0 && !ctx->owns(v)) mirror[v] = 1;
+    }
+  }
+  std::fill(ctx->blk_local.begin(), ctx->blk_local.end(), -1);
+  for (int b = 0; b < nb; ++b) {
+    if (!ctx->owns(b)) continue;
+    Level& L = ctx->levels[t->levels[b]];
+    ctx->blk_local[b] = static_cast<int>(L.blocks.size());
+    L.blocks.push_back(b);
+  }
+  for (auto& L : ctx->levels) L.nblk = static_cast<int>(L.blocks.size());
+  for (int b = 0; b < nb; ++b) {
+    if (!mirror[b]) continue;
+    Level& L = ctx->levels[t->levels[b]];
     ctx->blk_local[b] = static_cast<int>(L.blocks.size());
     L.blocks.push_back(b);
   }
@@ -626,15 +376,16 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
   // ---- per-level storage and flags
   for (int l = 0; l < nlev; ++l) {
     Level& L = ctx->levels[l];
-    L.nblk = static_cast<int>(L.blocks.size());
+    L.nmir = static_cast<int>(L.blocks.size()) - L.nblk;
     L.n = n;
     L.ncore = L.nblk * n3;
+    L.core_end = static_cast<long long>(L.nblk + L.nmir) * n3;
     double sc = p->fp16_scale[l < 32 ? l : 31];
     if (!(sc > 0)) sc = 65536.0;
     L.scale = p->precision == OCTLB_FP16_SHIFTED ? static_cast<float>(sc) : 1.f;
     L.inv_scale = 1.f / L.scale;
     if (L.nblk == 0) continue;
-    if (L.ncore >= (1LL << 31)) return fail(ctx, OCTLB_EINVAL, "level has more than 2^31 cells");
+    if (L.core_end >= (1LL << 31)) return fail(ctx, OCTLB_EINVAL, "level has more than 2^31 cells");
   }
 
   // Link records: q per direction (1 = half-way bounce-back) and the moving-wall
@@ -699,82 +450,114 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
         if (l != plan[k].coarse_level && static_cast<int>(k) >= lo[l] && static_cast<int>(k) <= hi[l])
           return fail(ctx, OCTLB_EINVAL, "coarse-fine faces must be grouped by coarse level");
   }
-  // save rows: level -> (local slot -> row)
-  std::vector<std::map<long long, int>> save_rows(nlev);
-  auto save_row = [&](int l, long long slot) {
-    auto& m = save_rows[l];
-    auto it = m.find(slot);
-    if (it != m.end()) return it->second;
-    const int r = static_cast<int>(m.size());
-    m.emplace(slot, r);
-    return r;
-  };
   auto core_slot = [&](int gblk, int x, int y, int z) { return core_slot_of(n, ctx->blk_local[gblk], x, y, z); };
   auto gcell = [&](int gblk, int x, int y, int z) {
     return gblk * n3 + (static_cast<long long>(x) * n + y) * n + z;
   };
-  std::vector<std::vector<ProlongItem>> prolong(nlev);
-  std::vector<std::vector<RestrictItem>> restrict_items(nlev);
+  auto owner_of = [&](long long g) { return ctx->owner.empty() ? ctx->rank : ctx->owner[g / n3]; };
   std::vector<float> prev(plan.size() * 23, 0.f);
   if (init)
     for (size_t k = 0; k < plan.size(); ++k)
       host_macro(init + gcell(plan[k].coarse_id, plan[k].ci, plan[k].cj, plan[k].ck) * kQ, &prev[k * 23]);
+  // Coupler items of the whole forest, by global cell.  Prolongation writes a
+  // fine cell per point and restriction a coarse cell per point from the fine
+  // cell and its in-block D3Q19 neighbours; a later point writing the same
+  // cell wins (plan order, level_coupler.cpp:440-477, 613-654).  An item runs
+  // on the rank owning the cell it writes.
+  struct PSrc { long long fine_g, coarse_g; int k; };
+  struct RSrc { long long coarse_g, fine_g; int nnb; long long nb_g[18]; };
+  std::vector<std::vector<PSrc>> pall(nlev);   // by coarse level
+  std::vector<std::vector<RSrc>> rall(nlev);   // by fine level
   {
-    // Prolongation writes a fine cell per point; a later point writing the
-    // same cell wins (plan order, level_coupler.cpp:440-477).
-    std::vector<std::map<long long, size_t>> last(nlev);
-    for (size_t k = 0; k < plan.size(); ++k)
+    std::vector<std::map<long long, size_t>> last(nlev), lastc(nlev);
+    for (size_t k = 0; k < plan.size(); ++k) {
       last[plan[k].coarse_level][gcell(plan[k].fine_id, plan[k].fi, plan[k].fj, plan[k].fk)] = k;
-    for (size_t k = 0; k < plan.size(); ++k) {
-      const PlanPoint& pt = plan[k];
-      if (last[pt.coarse_level][gcell(pt.fine_id, pt.fi, pt.fj, pt.fk)] != k) continue;
-      ProlongItem it{};
-      it.fine_slot = core_slot(pt.fine_id, pt.fi, pt.fj, pt.fk);
-      it.coarse_save = save_row(pt.coarse_level, core_slot(pt.coarse_id, pt.ci, pt.cj, pt.ck));
-      it.prev = static_cast<int>(k);
-      it.fine_kind = t->kinds[gcell(pt.fine_id, pt.fi, pt.fj, pt.fk)];
-      prolong[pt.coarse_level].push_back(it);
-    }
-    // Restriction writes a coarse cell per point from the fine cell and its
-    // in-block D3Q19 neighbours (level_coupler.cpp:613-654).
-    std::vector<std::map<long long, size_t>> lastc(nlev);
-    for (size_t k = 0; k < plan.size(); ++k)
       lastc[plan[k].fine_level][gcell(plan[k].coarse_id, plan[k].ci, plan[k].cj, plan[k].ck)] = k;
+    }
     for (size_t k = 0; k < plan.size(); ++k) {
       const PlanPoint& pt = plan[k];
-      if (lastc[pt.fine_level][gcell(pt.coarse_id, pt.ci, pt.cj, pt.ck)] != k) continue;
-      RestrictItem it{};
-      it.coarse_slot = core_slot(pt.coarse_id, pt.ci, pt.cj, pt.ck);
-      it.coarse_kind = t->kinds[gcell(pt.coarse_id, pt.ci, pt.cj, pt.ck)];
-      it.fine_save = save_row(pt.fine_level, core_slot(pt.fine_id, pt.fi, pt.fj, pt.fk));
-      it.nnb = 0;
-      for (int j = 1; j < kQ; ++j) {
-        const int x = pt.fi + cx(j), y = pt.fj + cy(j), z = pt.fk + cz(j);
-        if (x < 0 || y < 0 || z < 0 || x >= n || y >= n || z >= n) continue;
-        it.nb_save[it.nnb++] = save_row(pt.fine_level, core_slot(pt.fine_id, x, y, z));
+      const long long fg = gcell(pt.fine_id, pt.fi, pt.fj, pt.fk), cg = gcell(pt.coarse_id, pt.ci, pt.cj, pt.ck);
+      if (last[pt.coarse_level][fg] == k) pall[pt.coarse_level].push_back({fg, cg, static_cast<int>(k)});
+      if (lastc[pt.fine_level][cg] == k) {
+        RSrc r{cg, fg, 0, {}};
+        for (int j = 1; j < kQ; ++j) {
+          const int x = pt.fi + cx(j), y = pt.fj + cy(j), z = pt.fk + cz(j);
+          if (x < 0 || y < 0 || z < 0 || x >= n || y >= n || z >= n) continue;
+          r.nb_g[r.nnb++] = gcell(pt.fine_id, x, y, z);
+        }
+        rall[pt.fine_level].push_back(r);
       }
-      restrict_items[pt.fine_level].push_back(it);
+    }
+  }
+  // Save rows per source level, keyed by global cell: first every owned cell
+  // some item (on any rank) reads, sorted; then the cells of other ranks that
+  // this rank's items read, grouped by owner rank and sorted -- each peer's
+  // rows arrive as one contiguous run.  Rows of owned cells that a peer's
+  // items read are sent to it after every step of the level.
+  std::vector<std::map<long long, int>> save_rows(nlev);   // owned: local slot -> row
+  std::vector<std::map<long long, int>> row_of(nlev);      // global cell -> row
+  std::vector<int> n_save_all(nlev, 0);
+  std::vector<std::map<int, std::vector<long long>>> row_send_g(nlev), row_recv_g(nlev);  // peer -> cells
+  for (int l = 0; l < nlev; ++l) {
+    std::set<long long> own;
+    std::map<int, std::set<long long>> remote, send;
+    auto use = [&](long long g, int exec) {
+      const int o = owner_of(g);
+      if (o == ctx->rank) {
+        own.insert(g);
+        if (exec != ctx->rank) send[exec].insert(g);
+      } else if (exec == ctx->rank) {
+        remote[o].insert(g);
+      }
+    };
+    for (const PSrc& it : pall[l]) use(it.coarse_g, owner_of(it.fine_g));
+    for (const RSrc& it : rall[l]) {
+      const int exec = owner_of(it.coarse_g);
+      use(it.fine_g, exec);
+      for (int j = 0; j < it.nnb; ++j) use(it.nb_g[j], exec);
+    }
+    int r = 0;
+    for (long long g : own) {
+      row_of[l][g] = r;
+      save_rows[l][core_slot(static_cast<int>(g / n3), 0, 0, 0) + g % n3] = r;
+      ++r;
+    }
+    for (auto& [peer, cells] : remote) {
+      for (long long g : cells) row_of[l][g] = r++;
+      row_recv_g[l][peer].assign(cells.begin(), cells.end());
+    }
+    for (auto& [peer, cells] : send) row_send_g[l][peer].assign(cells.begin(), cells.end());
+    n_save_all[l] = r;
+    ctx->levels[l].n_save_own = static_cast<int>(own.size());
+  }
+  std::vector<std::vector<ProlongItem>> prolong(nlev);
+  std::vector<std::vector<RestrictItem>> restrict_items(nlev);
+  for (int l = 0; l < nlev; ++l) {
+    for (const PSrc& ps : pall[l]) {
+      if (owner_of(ps.fine_g) != ctx->rank) continue;
+      const int fb = static_cast<int>(ps.fine_g / n3);
+      ProlongItem it{};
+      it.fine_slot = core_slot(fb, 0, 0, 0) + ps.fine_g % n3;
+      it.coarse_save = row_of[l].at(ps.coarse_g);
+      it.prev = ps.k;
+      it.fine_kind = t->kinds[ps.fine_g];
+      prolong[l].push_back(it);
+    }
+    for (const RSrc& rs : rall[l]) {
+      if (owner_of(rs.coarse_g) != ctx->rank) continue;
+      const int cb = static_cast<int>(rs.coarse_g / n3);
+      RestrictItem it{};
+      it.coarse_slot = core_slot(cb, 0, 0, 0) + rs.coarse_g % n3;
+      it.coarse_kind = t->kinds[rs.coarse_g];
+      it.fine_save = row_of[l].at(rs.fine_g);
+      it.nnb = rs.nnb;
+      for (int j = 0; j < rs.nnb; ++j) it.nb_save[j] = row_of[l].at(rs.nb_g[j]);
+      restrict_items[l].push_back(it);
     }
   }
 
   // ---- per-level flags, links, neighbour bases, halo pages, boundary fills,
   //      drag items
-  std::vector<int> face_nbr(static_cast<size_t>(nb) * 6, -1);
-  for (int k = 0; k < t->n_same_level; ++k) {
-    const int* r = t->same_level + 3 * k;
-    face_nbr[static_cast<size_t>(r[0]) * 6 + r[1]] = r[2];
-  }
-  if (ctx->periodic)
-    for (int d = 0; d < 6; ++d) face_nbr[d] = 0;  // fill_periodic_halo: the block is its own neighbour
-  // Diagonal (edge) neighbour: two face steps in either order, the
-  // composition GhostSchedule uses for its same-level edge exchange.
-  auto edge_nbr = [&](int a, int d1, int d2) {
-    int b = face_nbr[static_cast<size_t>(a) * 6 + d1];
-    if (b >= 0 && face_nbr[static_cast<size_t>(b) * 6 + d2] >= 0) return face_nbr[static_cast<size_t>(b) * 6 + d2];
-    b = face_nbr[static_cast<size_t>(a) * 6 + d2];
-    if (b >= 0 && face_nbr[static_cast<size_t>(b) * 6 + d1] >= 0) return face_nbr[static_cast<size_t>(b) * 6 + d1];
-    return -1;
-  };
   const int np = n + 2, np3 = np * np * np;
   // Velocity scale of the moving tree-boundary walls (the largest wall speed,
   // e.g. the inlet u_max): every wall velocity is taken proportional to it
@@ -804,12 +587,25 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
   };
   for (int l = 0; l < nlev; ++l) {
     Level& L = ctx->levels[l];
-    if (L.nblk == 0) continue;
+    if (L.nblk == 0) {
+      // No owned block on this level (rank contexts): only the save rows
+      // received for this rank's coupler items and those items.
+      L.n_save = n_save_all[l];
+      CK(L.save_buf.alloc(static_cast<size_t>(L.n_save) * kQ * sizeof(float)));
+      CK(upload(L.prolong_items, prolong[l]));
+      CK(upload(L.restrict_items, restrict_items[l]));
+      L.n_prolong = static_cast<int>(prolong[l].size());
+      L.n_restrict = static_cast<int>(restrict_items[l].size());
+      L.args = StepArgs{};
+      L.args.save_buf = L.save_buf.as<float>();
+      L.args.err = ctx->dev_err.as<int>();
+      continue;
+    }
     L.has_flags = !ctx->periodic || !save_rows[l].empty();
     if (ctx->periodic) {
       for (long long k = 0; k < n3; ++k) if (t->kinds[k] != kBulk) L.has_flags = true;
     }
-    const long long ncore = L.ncore;
+    const long long ncore = L.ncore, core_end = L.core_end;
     std::vector<uint8_t> flags(static_cast<size_t>(ncore), 0);
     std::vector<int> lidx, sidx;
     std::vector<float> lrec;
@@ -819,7 +615,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     L.n_bulk = std::count(flags.begin(), flags.end(), static_cast<uint8_t>(kBulk));
     for (const auto& kv : recs) {
       const int gb = static_cast<int>(kv.first / n3);
-      if (ctx->blk_level[gb] != l) continue;
+      if (ctx->blk_level[gb] != l || !ctx->owns(gb)) continue;
       const long long s = static_cast<long long>(ctx->blk_local[gb]) * n3 + kv.first % n3;
       if (lidx.empty()) lidx.assign(static_cast<size_t>(ncore), -1);
       lidx[s] = static_cast<int>(lrec.size() / 38);
@@ -861,28 +657,15 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
         sidx[kv.first] = kv.second;
         flags[kv.first] |= kFlagSave;
       }
-      L.n_save = static_cast<int>(save_rows[l].size());
     }
+    L.n_save = n_save_all[l];
 
     // Same-level neighbour of each of the 27 halo directions (faces and edges
     // only: the exchange fills no corner ghosts), global ids, -1 for none.
     std::vector<int> nbr27(static_cast<size_t>(L.nblk) * 27, -1);
-    for (int lb = 0; lb < L.nblk; ++lb) {
-      const int gb = L.blocks[lb];
-      for (int ox = -1; ox <= 1; ++ox)
-        for (int oy = -1; oy <= 1; ++oy)
-          for (int oz = -1; oz <= 1; ++oz) {
-            const int o[3] = {ox, oy, oz};
-            int dirs[3], nd = 0;
-            for (int a = 0; a < 3; ++a)
-              if (o[a]) dirs[nd++] = 2 * a + (o[a] > 0 ? 1 : 0);
-            int v = -1;
-            if (nd == 0) v = gb;
-            else if (nd == 1) v = face_nbr[static_cast<size_t>(gb) * 6 + dirs[0]];
-            else if (nd == 2) v = edge_nbr(gb, dirs[0], dirs[1]);
-            nbr27[static_cast<size_t>(lb) * 27 + (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1)] = v;
-          }
-    }
+    for (int lb = 0; lb < L.nblk; ++lb)
+      for (int d = 0; d < 27; ++d)
+        nbr27[static_cast<size_t>(lb) * 27 + d] = nbr_dir(L.blocks[lb], d / 9 - 1, (d / 3) % 3 - 1, d % 3 - 1);
 
     // Tree-boundary fills (DomainBoundaryHandler::apply(), before the
     // exchange), in list order; a later write of the same halo population
@@ -898,7 +681,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     };
     for (int k = 0; k < t->n_tree_boundary; ++k) {
       const int gb = t->tree_boundary[2 * k], dir = t->tree_boundary[2 * k + 1];
-      if (ctx->blk_level[gb] != l || !t->tree_boundary_spec) continue;
+      if (ctx->blk_level[gb] != l || !t->tree_boundary_spec || !ctx->owns(gb)) continue;
       const double* sp = t->tree_boundary_spec + 8 * k;
       const int type = static_cast<int>(sp[0]);
       if (type == OCTLB_TB_NONE) continue;
@@ -1032,16 +815,17 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     L.n_open = static_cast<int>(halo_items.size() / 4);
     L.n_halo = L.n_pages > 0 ? H : 0;
     // even slot count: population rows start on 2-element boundaries
-    L.nslots = ncore + static_cast<long long>(L.n_pages) * H;
+    L.nslots = core_end + static_cast<long long>(L.n_pages) * H;
+    if (ctx->slab) L.nslots = core_end + 2LL * n * n;  // the two ghost x planes
     L.nslots += L.nslots & 1;
     std::vector<BBOp> bbv;
     for (const BB& op : bbl)
-      bbv.push_back(BBOp{ncore + static_cast<long long>(page_of[op.lb]) * H + hmap[op.hlin], op.src, op.pop,
+      bbv.push_back(BBOp{core_end + static_cast<long long>(page_of[op.lb]) * H + hmap[op.hlin], op.src, op.pop,
                          op.src_pop, op.add, op.dadd});
     L.n_bb = static_cast<uint32_t>(bbv.size());
     std::vector<int> fill_of_h(static_cast<size_t>(L.n_pages) * H * kQ, -1);
     for (size_t k = 0; k < bbv.size(); ++k)
-      fill_of_h[static_cast<size_t>(bbv[k].dst - ncore) * kQ + bbv[k].pop] = static_cast<int>(k);
+      fill_of_h[static_cast<size_t>(bbv[k].dst - core_end) * kQ + bbv[k].pop] = static_cast<int>(k);
 
     // Slot bases of the 27 directions: own core (centre), the neighbour's core
     // shifted by one block edge, or the own halo page.
@@ -1068,7 +852,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       if (d == 13) return static_cast<long long>(lb) * n3 + lin;
       const long long b0 = nbase[static_cast<size_t>(lb) * 27 + d];
       if (b0 != kOwnPage) return b0 + lin;
-      if (page_of[lb] >= 0) return ncore + static_cast<long long>(page_of[lb]) * H + hmap[P];
+      if (page_of[lb] >= 0) return core_end + static_cast<long long>(page_of[lb]) * H + hmap[P];
       return -1;
     };
     std::vector<int> slot_map;
@@ -1086,7 +870,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
               unresolved[P] = sl < 0;
               if (sl >= L.nslots) return fail(ctx, OCTLB_EINVAL, "internal: slot map out of range");
               m[P] = sl < 0 ? static_cast<int>(static_cast<long long>(lb) * n3) : static_cast<int>(sl);
-              if (sl < ncore) continue;
+              if (sl < core_end) continue;
               // A halo-page position whose pulled populations are boundary
               // fills: an outflow copy becomes its source cell's slot, a
               // bounce-back wall the marker -1 (at rest) or -(2 + k) (moving,
@@ -1099,7 +883,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
                 const int Xs = X + cx(i), Ys = Y + cy(i), Zs = Z + cz(i);
                 if (Xs < 1 || Ys < 1 || Zs < 1 || Xs > n || Ys > n || Zs > n) continue;
                 ++npull;
-                const int fo = fill_of_h[static_cast<size_t>(sl - ncore) * kQ + i];
+                const int fo = fill_of_h[static_cast<size_t>(sl - core_end) * kQ + i];
                 if (fo < 0) continue;
                 ++nfill;
                 const BBOp& op = bbv[fo];
@@ -1125,7 +909,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
                 wall_add.resize(wall_add.size() + kQ, 0.f);
                 wall_dadd.resize(wall_dadd.size() + kQ, 0.f);
                 for (int i = 1; i < kQ; ++i) {
-                  const int fo = fill_of_h[static_cast<size_t>(sl - ncore) * kQ + i];
+                  const int fo = fill_of_h[static_cast<size_t>(sl - core_end) * kQ + i];
                   if (fo < 0) continue;
                   wall_add[static_cast<size_t>(k) * kQ + i] = bbv[fo].add;
                   wall_dadd[static_cast<size_t>(k) * kQ + i] = bbv[fo].dadd;
@@ -1225,7 +1009,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       const long long ns = L.nslots;
       auto in = [&](long long v, long long hi) { return v >= 0 && v < hi; };
       for (const BBOp& op : bbv)
-        if (!in(op.dst, ns) || op.dst < ncore || !in(op.src, ncore) || !in(op.pop, kQ) || !in(op.src_pop, kQ))
+        if (!in(op.dst, ns) || op.dst < core_end || !in(op.src, ncore) || !in(op.pop, kQ) || !in(op.src_pop, kQ))
           return fail(ctx, OCTLB_EINVAL, "internal: boundary fill out of range");
       for (int v : lidx) if (v < -1 || v >= L.n_links) return fail(ctx, OCTLB_EINVAL, "internal: link index");
       for (int v : sidx) if (v < -1 || v >= L.n_save) return fail(ctx, OCTLB_EINVAL, "internal: save index");
@@ -1247,7 +1031,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
             lo += cmin * w[a];
             hi += cmax * w[a];
           }
-          if (!in(b0 + lo, ncore) || !in(b0 + hi, ncore))
+          if (!in(b0 + lo, core_end) || !in(b0 + hi, core_end))
             return fail(ctx, OCTLB_EINVAL, "internal: neighbour base out of range");
         }
       for (const DragItem& it : drag) if (!in(it.slot, ncore)) return fail(ctx, OCTLB_EINVAL, "internal: drag slot");
@@ -1318,7 +1102,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     A.n_open = L.n_open;
     A.n_halo = L.n_halo;
     A.nblk = L.nblk; A.n = n; A.np = np;
-    A.halo_base = ncore;
+    A.halo_base = core_end;
     A.ncore = static_cast<uint32_t>(ncore);
     A.nitems = A.ncore + static_cast<uint32_t>(L.n_open);
     A.div_n = FastDiv(n);
@@ -1344,6 +1128,10 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     // one-cell-per-thread step with OCTLB_STEP_KERNEL=plain.
     const bool uniform = ctx->periodic && !L.has_flags;
     if (uniform && ctx->step_kernel == 0 && pair_step_eligible(n)) L.use_pair = true;
+    A.wrap_lo = ctx->slab ? n : n - 1;
+    A.wrap_hi = ctx->slab ? n + 1 : 0;
+    if (ctx->slab && !L.use_pair)
+      return fail(ctx, OCTLB_EINVAL, "a periodic block shared over ranks needs the paired step (all kBulk, even n)");
     // Any other level: the slot-map step by default, the one-cell-per-thread
     // k_step with OCTLB_STEP_KERNEL=plain (or bulk, which only periodic
     // blocks take) or where the map does not fit.
@@ -1373,6 +1161,95 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       }
     }
   }
+  // ---- cross-rank exchange tables (rank contexts).  For every pair of
+  // same-level blocks b, m = neighbour of b in a face or edge direction with
+  // different owners: the cells of m in b's halo region of that direction
+  // travel from m's owner to b's owner before every step of the level (the
+  // face layer of n^2 or the edge row of n cells, all 19 populations, as
+  // GhostSchedule sends them).  Both ends list them in global cell order.
+  if (!ctx->owner.empty()) {
+    for (int l = 0; l < nlev; ++l) {
+      Level& L = ctx->levels[l];
+      std::map<int, std::vector<long long>> send_c, recv_c;
+      for (int b = 0; b < nb; ++b) {
+        if (t->levels[b] != l) continue;
+        const int ob = ctx->owner[b];
+        for (int d = 0; d < 27; ++d) {
+          if (d == 13) continue;
+          const int o[3] = {d / 9 - 1, (d / 3) % 3 - 1, d % 3 - 1};
+          const int m = nbr_dir(b, o[0], o[1], o[2]);
+          if (m < 0) continue;
+          const int om = ctx->owner[m];
+          const bool recv = ob == ctx->rank && om != ctx->rank, send = om == ctx->rank && ob != ctx->rank;
+          if (!recv && !send) continue;
+          std::vector<long long>& dst = recv ? recv_c[om] : send_c[ob];
+          int lo[3], hi[3];
+          for (int a = 0; a < 3; ++a) {
+            lo[a] = o[a] < 0 ? n - 1 : 0;
+            hi[a] = o[a] > 0 ? 0 : n - 1;
+          }
+          for (int x = lo[0]; x <= hi[0]; ++x)
+            for (int y = lo[1]; y <= hi[1]; ++y)
+              for (int z = lo[2]; z <= hi[2]; ++z) dst.push_back(gcell(m, x, y, z));
+        }
+      }
+      auto record = [&](int kind, const std::map<int, std::vector<long long>>& by_peer) {
+        if (!ctx->plan_lists) return;
+        for (const auto& [peer, v] : by_peer)
+          for (long long g : v) ctx->plan_lists->insert(ctx->plan_lists->end(), {l, kind, peer, g});
+      };
+      auto to_slots = [&](std::map<int, std::vector<long long>>& by_peer) {
+        for (auto& [peer, v] : by_peer) {
+          std::sort(v.begin(), v.end());
+          v.erase(std::unique(v.begin(), v.end()), v.end());
+          for (long long& g : v) g = core_slot(static_cast<int>(g / n3), 0, 0, 0) + g % n3;
+        }
+      };
+      for (auto* m : {&send_c, &recv_c})
+        for (auto& [peer, v] : *m) {
+          std::sort(v.begin(), v.end());
+          v.erase(std::unique(v.begin(), v.end()), v.end());
+        }
+      record(0, send_c);
+      record(1, recv_c);
+      record(2, row_send_g[l]);
+      record(3, row_recv_g[l]);
+      to_slots(send_c);
+      to_slots(recv_c);
+      const size_t cell_bytes = kQ * sizeof(T);
+      if (int rc = setup_xfer(ctx, L.cell_send, send_c, cell_bytes, true)) return rc;
+      if (int rc = setup_xfer(ctx, L.cell_recv, recv_c, cell_bytes, true)) return rc;
+      // save rows: rows of owned cells out, runs of received rows in
+      std::map<int, std::vector<long long>> rsend, rrecv;
+      for (const auto& [peer, cells] : row_send_g[l])
+        for (long long g : cells) rsend[peer].push_back(row_of[l].at(g));
+      L.row_recv_first.clear();
+      for (const auto& [peer, cells] : row_recv_g[l]) {
+        for (long long g : cells) rrecv[peer].push_back(row_of[l].at(g));
+        const std::vector<long long>& rows = rrecv[peer];
+        for (size_t k = 1; k < rows.size(); ++k)
+          if (rows[k] != rows[0] + static_cast<long long>(k))
+            return fail(ctx, OCTLB_EINVAL, "internal: received save rows not contiguous");
+        if (!rows.empty()) L.row_recv_first.push_back(rows[0]);
+      }
+      if (int rc = setup_xfer(ctx, L.row_send, rsend, kQ * sizeof(float), true)) return rc;
+      if (int rc = setup_xfer(ctx, L.row_recv, rrecv, kQ * sizeof(float), false)) return rc;
+      // every index the pack / unpack kernels derive
+      for (const auto& [peer, v] : send_c)
+        for (long long sl : v)
+          if (sl < 0 || sl >= L.ncore) return fail(ctx, OCTLB_EINVAL, "internal: sent cell not owned");
+      for (const auto& [peer, v] : recv_c)
+        for (long long sl : v)
+          if (sl < L.ncore || sl >= L.core_end) return fail(ctx, OCTLB_EINVAL, "internal: received cell not a mirror");
+      for (const auto& [peer, v] : rsend)
+        for (long long r : v)
+          if (r < 0 || r >= L.n_save_own) return fail(ctx, OCTLB_EINVAL, "internal: sent save row");
+      for (const auto& [peer, v] : rrecv)
+        for (long long r : v)
+          if (r < L.n_save_own || r >= L.n_save) return fail(ctx, OCTLB_EINVAL, "internal: received save row");
+    }
+  }
+
   // Cross-level coupler indices: prolongation targets live on level l+1,
   // restriction targets on level l-1.
   for (int l = 0; l < nlev; ++l) {
@@ -2066,6 +1943,7 @@ int audit_impl(octlb_ctx* ctx, double out[4]) {
     CK(cudaStreamSynchronize(ctx->stream));
     for (int k = 0; k < 5; ++k) tot[k] += h[k];
   }
+  if (int rc = comm_allreduce(ctx, tot, 5)) return rc;  // rank contexts: the sum over ranks
   for (int k = 0; k < 4; ++k) out[k] = tot[k];
   if (tot[4] != 0.0) return fail(ctx, OCTLB_ENAN, "non-finite populations");
   return OCTLB_OK;
@@ -2078,12 +1956,36 @@ using namespace octlb_host;
 // ====================================================================== C ABI
 extern "C" {
 
-int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double* init, octlb_ctx** out) {
+static int create_common(const octlb_tables* t, const octlb_params* p, const double* init,
+                         const octlb_partition* part, octlb_ctx** out) {
   if (!out) return OCTLB_EINVAL;
   *out = nullptr;
   auto ctx = std::make_unique<octlb_ctx>();
   int rc = validate(ctx.get(), t, p);
   if (rc) { *out = ctx.release(); return rc; }
+  if (part) {
+    if (part->nranks < 1 || part->rank < 0 || part->rank >= part->nranks || (!part->owner && !t->periodic) ||
+        !part->comm) {
+      *out = ctx.release();
+      return fail(*out, OCTLB_EINVAL, "partition: rank, nranks, owner and comm are required");
+    }
+    if (comm_nranks(part->comm) != part->nranks) {
+      *out = ctx.release();
+      return fail(*out, OCTLB_EINVAL, "partition: the comm has another number of ranks");
+    }
+    for (int b = 0; b < t->n_blocks && !t->periodic; ++b)
+      if (part->owner[b] < 0 || part->owner[b] >= part->nranks) {
+        *out = ctx.release();
+        return fail(*out, OCTLB_EINVAL, "partition: owner out of range");
+      }
+    // A periodic block: rank r owns x slab r (owner is not read); one rank
+    // exchanges its ghost planes with itself.
+    if (t->periodic) ctx->slab = true;
+    ctx->rank = part->rank;
+    ctx->nranks = part->nranks;
+    if (!t->periodic) ctx->owner.assign(part->owner, part->owner + t->n_blocks);
+    ctx->comm = part->comm;
+  }
   ctx->n = t->n;
   ctx->n_blocks = t->n_blocks;
   if (t->bounds) ctx->bounds.assign(t->bounds, t->bounds + 6 * static_cast<size_t>(t->n_blocks));
@@ -2113,15 +2015,35 @@ int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double*
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
   if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "side stream"); *out = ctx.release(); return rc; }
+  if (ctx->comm) {
+    // The exchanges sit between the launches of a level step and the local
+    // transport meets the other ranks on the host: launched one by one, in
+    // plain stream order.
+    ctx->use_graphs = false;
+    ctx->use_pdl = false;
+    rc = comm_attach(ctx.get());
+    if (rc) { *out = ctx.release(); return rc; }
+  }
   rc = p->precision == OCTLB_FP32 ? create_impl<float>(ctx.get(), t, p, init)
                                   : create_impl<__half>(ctx.get(), t, p, init);
   *out = ctx.release();
   return rc;
 }
 
+int octlb_gpu_create(const octlb_tables* t, const octlb_params* p, const double* init, octlb_ctx** out) {
+  return create_common(t, p, init, nullptr, out);
+}
+
+int octlb_gpu_create_part(const octlb_tables* t, const octlb_params* p, const double* init,
+                          const octlb_partition* part, octlb_ctx** out) {
+  if (!part) return OCTLB_EINVAL;
+  return create_common(t, p, init, part, out);
+}
+
 void octlb_gpu_destroy(octlb_ctx* ctx) {
   if (!ctx) return;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  comm_detach(ctx);
   clear_graphs(ctx);
   cudaStream_t s = ctx->own_stream ? ctx->stream : nullptr;
   ctx->levels.clear();
@@ -2164,6 +2086,7 @@ int octlb_gpu_adjoint(octlb_ctx* ctx, const octlb_adj_params* p, double* objecti
   if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
   if (ctx->unusable) return fail(ctx, OCTLB_ESTATE, "context unusable after a failed drain of a bounded wait");
   if (ctx->precision != OCTLB_FP32) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates FP32 storage only");
+  if (ctx->comm) return fail(ctx, OCTLB_EINVAL, "the adjoint runs on one context, not rank contexts");
   if (ctx->const_rho) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates the BGK collide, not ConstRhoBGK");
   return adjoint_impl<float>(ctx, p, objective, grad, grad_force);
 }
@@ -2171,6 +2094,7 @@ int octlb_gpu_adjoint(octlb_ctx* ctx, const octlb_adj_params* p, double* objecti
 int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on) {
   if (!ctx) return OCTLB_EINVAL;
   if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
+  if (ctx->comm && on) return fail(ctx, OCTLB_EINVAL, "ConstRhoBGK is built for one context, not rank contexts");
   for (int c : ctx->counters_collide)
     if (c != 0) return fail(ctx, OCTLB_ESTATE, "ConstRhoBGK is chosen before the first advance");
   if ((on != 0) == ctx->const_rho) return OCTLB_OK;
@@ -2228,7 +2152,7 @@ int octlb_gpu_average_rho(octlb_ctx* ctx, double* out) {
 
 int octlb_gpu_synchronize(octlb_ctx* ctx) {
   if (!ctx) return OCTLB_EINVAL;
-  CK(cudaStreamSynchronize(ctx->stream));
+  if (int rc = comm_synchronize(ctx)) return rc;  // bounded for the NCCL transport
   return check_device_error(ctx);
 }
 
@@ -2304,6 +2228,7 @@ int octlb_gpu_write_vtk(octlb_ctx* ctx, const char* output_dir, const char* base
   std::vector<std::string> rel;
   std::vector<double> vel(static_cast<size_t>(n3) * 3), den(static_cast<size_t>(n3)), pre(static_cast<size_t>(n3));
   for (int b = 0; b < ctx->n_blocks; ++b) {
+    if (!ctx->owns(b)) continue;  // rank contexts write their own blocks
     // cell (i, j, k) of the file (i fastest) is core cell (x, y, z) = (i, j, k)
     size_t c = 0;
     for (int k = 0; k < n; ++k)
@@ -2342,7 +2267,7 @@ int octlb_gpu_force(octlb_ctx* ctx, double out[3]) {
   if (!ctx->drag) return fail(ctx, OCTLB_ESTATE, "context created without drag");
   CK(cudaMemcpyAsync(out, ctx->force.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  return OCTLB_OK;
+  return comm_allreduce(ctx, out, 3);  // rank contexts: the sum over ranks
 }
 
 int octlb_gpu_force_sum(octlb_ctx* ctx, double out[3], long long* steps) {
@@ -2351,7 +2276,7 @@ int octlb_gpu_force_sum(octlb_ctx* ctx, double out[3], long long* steps) {
   CK(cudaMemcpyAsync(out, ctx->force_sum.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   if (steps) *steps = ctx->force_steps;
-  return OCTLB_OK;
+  return comm_allreduce(ctx, out, 3);
 }
 
 int octlb_gpu_force_reset(octlb_ctx* ctx) {
@@ -2405,6 +2330,38 @@ int octlb_gpu_plan(const octlb_tables* t, const octlb_params* p, long long* stat
   }
   for (int k = 0; k < max_stats && k < static_cast<int>(v.size()); ++k) stats[k] = v[k];
   return static_cast<int>(v.size());
+}
+
+int octlb_gpu_plan_part(const octlb_tables* t, const octlb_params* p, int rank, int nranks, const int* owner,
+                        long long* records, long long max_records) {
+  if (!owner || nranks < 1 || rank < 0 || rank >= nranks) return OCTLB_EINVAL;
+  octlb_ctx ctx;
+  int rc = validate(&ctx, t, p);
+  if (rc) return rc;
+  for (int b = 0; b < t->n_blocks; ++b)
+    if (owner[b] < 0 || owner[b] >= nranks) return OCTLB_EINVAL;
+  if (t->periodic) return OCTLB_EINVAL;
+  ctx.n = t->n;
+  ctx.n_blocks = t->n_blocks;
+  ctx.precision = p->precision;
+  ctx.stream_mode = p->stream_mode;
+  ctx.periodic = t->periodic;
+  ctx.drag = p->drag;
+  ctx.omega = p->omega;
+  ctx.rank = rank;
+  ctx.nranks = nranks;
+  ctx.owner.assign(owner, owner + t->n_blocks);
+  std::vector<long long> lists;
+  ctx.plan_lists = &lists;
+  g_dry_run = true;
+  rc = p->precision == OCTLB_FP32 ? create_impl<float>(&ctx, t, p, nullptr)
+                                  : create_impl<__half>(&ctx, t, p, nullptr);
+  g_dry_run = false;
+  if (rc) return rc;
+  const long long nrec = static_cast<long long>(lists.size() / 4);
+  if (records)
+    for (long long k = 0; k < 4 * std::min(nrec, max_records); ++k) records[k] = lists[k];
+  return static_cast<int>(std::min<long long>(nrec, 2147483647LL));
 }
 
 // Host-only check of the multiply-high divider the kernels use for index

@@ -55,6 +55,11 @@ struct StepArgs {
   double* cr_part;
   int cr_total;             // partials the average update sums
   int* err;                 // device error word (bounded waits that gave up)
+  // Periodic block (paired step): the x plane a cell at x = 0 pulls from for
+  // c_x = +1 and the one a cell at x = n - 1 pulls from for c_x = -1 -- n - 1
+  // and 0 for a block periodic in itself, the two ghost planes after the core
+  // (n and n + 1) for an x slab of a periodic box shared over ranks.
+  int wrap_lo, wrap_hi;
   unsigned long long wait_ns; // limit of every bounded device wait
   int stall_first_row;      // test of the bounded wait: CTA 0 never issues its first row
 };

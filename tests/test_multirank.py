@@ -1,5 +1,9 @@
-"""N > 1 host logic on CPU ranks (gloo, world size 2): the replica bench's
-max-over-ranks timing and the reference arm's rank-0-only rule."""
+"""N > 1 host logic on CPU ranks (gloo, world size 2 and 3): the bench's
+max-over-ranks timing, the reference arm's rank-0-only rule, and the rank
+contexts' exchange protocol -- each rank plans its own context (the
+library's host-only dry run of octlb_gpu_create_part) and the lists it would
+send travel over gloo to the peers, which check them against the lists they
+expect to receive, in order."""
 import json
 import os
 import socket
@@ -73,3 +77,54 @@ def test_reference_arm_rank0_only():
     line = json.loads(outs[0].splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["e2e"]["h2d_bytes_per_step"] == 0
     assert outs[1] == ""
+
+
+EXCH = r"""
+import os, sys, json
+sys.path.insert(0, os.environ["ROOT"])
+import numpy as np
+import torch
+import torch.distributed as dist
+from datetime import timedelta
+dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+rank, world = dist.get_rank(), dist.get_world_size()
+import octlb_b200 as ob
+from octlb_b200 import cases
+mesh, init, info = (cases.cylinder_forest() if os.environ["CASE"] == "cylinder"
+                    else cases.cavity_forest(cells=64, n=8, lid=0.05, tau=0.56, band_cells=8))
+owner = ob.partition(mesh, world)
+links = os.environ["CASE"] == "cylinder"
+recs = ob.plan_part(mesh, info["omega"], rank, owner, stream_mode=ob.STREAM_LINKS if links else ob.STREAM_ROTATE,
+                    drag=links)
+checked = 0
+for kind_send, kind_recv in ((0, 1), (2, 3)):
+    for src in range(world):
+        for dst in range(world):
+            if src == dst:
+                continue
+            if rank == src:
+                mine = recs[(recs[:, 1] == kind_send) & (recs[:, 2] == dst)][:, [0, 3]]
+                n = torch.tensor([len(mine)], dtype=torch.int64)
+                dist.send(n, dst)
+                if len(mine):
+                    dist.send(torch.from_numpy(np.ascontiguousarray(mine)), dst)
+            elif rank == dst:
+                n = torch.zeros(1, dtype=torch.int64)
+                dist.recv(n, src)
+                got = torch.zeros((int(n), 2), dtype=torch.int64)
+                if int(n):
+                    dist.recv(got, src)
+                want = recs[(recs[:, 1] == kind_recv) & (recs[:, 2] == src)][:, [0, 3]]
+                assert np.array_equal(got.numpy(), want), (src, dst, kind_send, len(got), len(want))
+                checked += len(want)
+            dist.barrier()
+print(json.dumps({"rank": rank, "checked": checked, "records": int(len(recs))}), flush=True)
+dist.destroy_process_group()
+"""
+
+
+@pytest.mark.parametrize("case,world", [("cylinder", 2), ("amr", 3)])
+def test_rank_exchange_lists_agree_over_gloo(case, world):
+    outs = run_ranks(EXCH, world=world, extra_env={"CASE": case})
+    res = [json.loads(o.strip().splitlines()[-1]) for o in outs]
+    assert all(r["checked"] > 0 for r in res)
