@@ -6,13 +6,17 @@ A step is one TimeLoop::advance_one (one fused pull-stream + collide launch).
 `value` is whole-job MLUPS (all ranks) with the state resident in HBM; the
 lattice (2 x 1.27 GB FP32) is larger than L2 (126 MB), so no L2 flush is
 needed between steps.  `e2e` runs the same job through the C ABI from host
-memory: FP64 initial populations uploaded, K steps, fields read back.
+memory: the Taylor-Green fields (rho, u per cell) uploaded and turned into
+the equilibrium state, K steps, the fields read back.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--precision fp32|fp16] [--n 256]
 
-N > 1 (torchrun) runs N independent replicas (weak scaling, no collective in
-the data path), timed as the max over ranks.
+N > 1 (torchrun, one process per GPU): weak scaling over x slabs -- rank r
+holds slab r (256^3) of the periodic (N 256) x 256 x 256 box and exchanges
+its two ghost x planes with the neighbouring slabs before every step
+(rank contexts over NCCL, octlb_gpu_create_part); timed as the max over
+ranks of the device time.
 """
 import argparse
 import json
@@ -154,6 +158,8 @@ class ClockSampler:
 
 
 def dist_setup(args):
+    """Host plumbing of N > 1 (barriers, the max over ranks, the NCCL id):
+    a gloo process group with a short timeout."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -164,6 +170,18 @@ def dist_setup(args):
         dist.init_process_group("gloo", timeout=timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
+
+
+def slab_comm(ob, pg, world, rank):
+    """The NCCL transport of the rank contexts (None on one GPU): rank 0 makes
+    the id, the gloo group carries it to the others."""
+    if pg is None:
+        return None
+    os.environ.setdefault("NCCL_SOCKET_IFNAME", "lo")  # one node: the ranks meet on the loopback
+    os.environ.setdefault("OCTLB_COMM_TIMEOUT_S", "120")
+    obj = [ob.Comm.nccl_unique_id() if rank == 0 else None]
+    pg.broadcast_object_list(obj, src=0)
+    return ob.Comm.nccl(obj[0], world, rank)
 
 
 def max_over_ranks(pg, v):
@@ -501,10 +519,12 @@ def main():
 
     n = args.n
     results = {}
+    comm = slab_comm(ob, pg, world, rank)
+    part = None if comm is None else (rank, np.zeros(1, np.int32), comm)
     for prec_name in (["fp32", "fp16"] if args.precision == "fp32" else ["fp16", "fp32"]):
         prec = ob.FP32 if prec_name == "fp32" else ob.FP16_SHIFTED
         mesh, init, info = cases.tgv_periodic(n, u0=0.05, tau=0.55)
-        lat = ob.GpuLattice(mesh, info["omega"], precision=prec, init_pops=init)
+        lat = ob.GpuLattice(mesh, info["omega"], precision=prec, init_pops=init, part=part)
         # A dedicated (non-default) stream shared by the context and the events.
         stream = torch.cuda.Stream()
         lat.set_stream(stream.cuda_stream)
@@ -520,6 +540,7 @@ def main():
             e0.record(stream)
             lat.advance(args.steps)
             e1.record(stream)
+            lat.synchronize()  # bounded under NCCL
             torch.cuda.synchronize()
             cs.stop()
         barrier(pg)
@@ -574,8 +595,9 @@ def main():
         "metric": "MLUPS", "value": main_r["mlups"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": main_r["ms_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"tgv_periodic_{n}^3", "cells": n ** 3, "tau": 0.55, "u0": 0.05,
-                   "storage": args.precision, "parallelism": f"replicas{world}",
+        "config": {"workload": f"tgv_periodic_{n}^3" + (f" per rank, x slabs of ({world}x{n})x{n}x{n}" if world > 1 else ""),
+                   "cells": n ** 3 * world, "tau": 0.55, "u0": 0.05,
+                   "storage": args.precision, "parallelism": f"xslab{world}" if world > 1 else "single",
                    "l2": "lattice 2x{:.2f} GB > L2, no flush".format(n ** 3 * 19 * (4 if args.precision == 'fp32' else 2) / 1e9)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
@@ -596,6 +618,9 @@ def main():
         out["cpu_baseline"] = cpu_reference_mlups(n, steps_budget_s=args.ref_seconds)
     if rank == 0:
         print(json.dumps(out), flush=True)
+    if comm is not None:
+        barrier(pg)
+        comm.close()
     if pg is not None:
         pg.destroy_process_group()
 

@@ -88,12 +88,28 @@ typedef struct octlb_tables {
   int periodic;                   /* 1: single block, periodic in x, y, z */
 } octlb_tables;
 
+/* Coupler / relaxation mode.  REFERENCE (parity with the reference): one
+ * global omega collides every level (time_loop.h:183-187) and the Lagrava
+ * scales are (tau - 1/4) / tau and tau / (tau - 1/4) of that tau
+ * (level_coupler.cpp:226-228).  PHYSICAL: every level relaxes with its own
+ * tau_l, tau_{l+1} - 1/2 = 2 (tau_l - 1/2) (the viscosity is the same on every
+ * level under the 2:1 time step), and the coupler rescales the
+ * non-equilibrium part by tau_f / (2 tau_c) coarse -> fine and 2 tau_c / tau_f
+ * fine -> coarse (Dupuis and Chopard), which is the reference's pair of
+ * scales with tau = tau_c. */
+#define OCTLB_COUPLER_REFERENCE 0
+#define OCTLB_COUPLER_PHYSICAL 1
+
 typedef struct octlb_params {
-  double omega;                   /* one global BGK rate (time_loop.h:183-187) */
+  double omega;                   /* REFERENCE: the global BGK rate; PHYSICAL: the
+                                     rate of the coarsest level with blocks */
   int precision;                  /* OCTLB_FP32 or OCTLB_FP16_SHIFTED */
   int stream_mode;                /* OCTLB_STREAM_ROTATE or OCTLB_STREAM_LINKS */
   int drag;                       /* 1: MEM force every coarse step */
   double fp16_scale[32];          /* per-level scale; 0 = default 2^16 */
+  int coupler_mode;               /* OCTLB_COUPLER_REFERENCE (0) or _PHYSICAL */
+  double omega_level[32];         /* PHYSICAL: explicit rate of level l, or 0 for
+                                     the rescaled one */
 } octlb_params;
 
 typedef struct octlb_ctx octlb_ctx;

@@ -22,7 +22,7 @@ import numpy as np
 from . import capi
 from .capi import (BULK, SOLID, BOUNCE_BACK, MOVING_BOUNCE_BACK, BOUZIDI, VELOCITY_DIRICHLET,
                    PRESSURE_DIRICHLET, OUTFLOW, FP32, FP16_SHIFTED, STREAM_ROTATE, STREAM_LINKS,
-                   TB_NONE, TB_WALL, TB_OUTFLOW, OctlbError)
+                   TB_NONE, TB_WALL, TB_OUTFLOW, COUPLER_REFERENCE, COUPLER_PHYSICAL, OctlbError)
 
 capi.lib()  # fail loudly at import when the library is missing
 
@@ -304,7 +304,8 @@ class GpuLattice:
     with owner == rank."""
 
     def __init__(self, mesh, omega, precision=FP32, stream_mode=STREAM_ROTATE, drag=False,
-                 init_pops=None, fp16_scale=None, part=None):
+                 init_pops=None, fp16_scale=None, part=None, coupler_mode=capi.COUPLER_REFERENCE,
+                 omega_level=None):
         self._L = capi.lib()
         self.mesh = mesh
         self.omega = float(omega)
@@ -315,6 +316,10 @@ class GpuLattice:
             sc = np.broadcast_to(np.asarray(fp16_scale, dtype=np.float64), (32,))
             for i in range(32):
                 p.fp16_scale[i] = float(sc[i])
+        p.coupler_mode = int(coupler_mode)
+        if omega_level is not None:
+            for i, w in enumerate(omega_level):
+                p.omega_level[i] = float(w)
         self._init = None if init_pops is None else np.ascontiguousarray(init_pops, np.float64)
         if self._init is not None:
             assert self._init.size == mesh.n_blocks * mesh.n ** 3 * Q

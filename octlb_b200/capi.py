@@ -25,6 +25,8 @@ FP32 = 0
 FP16_SHIFTED = 1
 STREAM_ROTATE = 0
 STREAM_LINKS = 1
+COUPLER_REFERENCE = 0
+COUPLER_PHYSICAL = 1
 TB_NONE = 0
 TB_WALL = 1
 TB_OUTFLOW = 2
@@ -70,6 +72,7 @@ class Params(ctypes.Structure):
     _fields_ = [
         ("omega", ctypes.c_double), ("precision", ctypes.c_int), ("stream_mode", ctypes.c_int),
         ("drag", ctypes.c_int), ("fp16_scale", ctypes.c_double * 32),
+        ("coupler_mode", ctypes.c_int), ("omega_level", ctypes.c_double * 32),
     ]
 
 

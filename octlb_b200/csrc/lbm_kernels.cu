@@ -17,6 +17,8 @@
 // g_{n+1} = C(f_{n+1}).  The reference's per-step order collide -> exchange ->
 // stream (time_loop.h:201-217) is therefore a ghost fill followed by k_step.
 #include <cstdio>
+#include <cstdlib>
+#include <type_traits>
 
 #include "lbm_device.cuh"
 
@@ -465,6 +467,68 @@ __global__ void __launch_bounds__(kThreads) k_step_pair(const StepArgs a) {
   T* o = dst + static_cast<long long>(row) * n + z;
 #pragma unroll
   for (int i = 0; i < kQ; ++i) Pair<T>::st(o + i * a.qs, f0[i], f1[i], a.scale);
+}
+
+// The same step for FP16-shifted storage with four consecutive z cells per
+// thread: every population row is read and written with 8-byte (four-half)
+// accesses, half the memory instructions per cell of the paired kernel; a
+// z-shift of +-1 takes the aligned four around the cells and one half beyond
+// them.  Per cell the arithmetic is the paired kernel's (conversions to and
+// from half are exact / round-to-nearest alike), so the results are bitwise
+// equal.  n % 4 == 0 (rows and population planes on 8-byte boundaries).
+__device__ __forceinline__ void ld4h(const __half* p, float& a, float& b, float& c, float& d) {
+  const uint2 u = *reinterpret_cast<const uint2*>(p);
+  const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+  const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+  a = lo.x; b = lo.y; c = hi.x; d = hi.y;
+}
+__device__ __forceinline__ void st4h(__half* p, float a, float b, float c, float d) {
+  const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
+  uint2 u;
+  u.x = *reinterpret_cast<const uint32_t*>(&lo);
+  u.y = *reinterpret_cast<const uint32_t*>(&hi);
+  *reinterpret_cast<uint2*>(p) = u;
+}
+
+__global__ void __launch_bounds__(kThreads) k_step_quad_h(const StepArgs a) {
+  pdl_wait();
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  const uint32_t n = a.n, q4 = n >> 2;
+  if (t >= a.ncore / 4) return;
+  const uint32_t row = a.div_n.div(4 * t);  // = t / (n / 4)
+  const uint32_t z = (t - row * q4) * 4;
+  const uint32_t x = a.div_n.div(row), y = row - x * n;
+  const uint32_t xm = x == 0 ? static_cast<uint32_t>(a.wrap_lo) : x - 1;
+  const uint32_t xp = x == n - 1 ? static_cast<uint32_t>(a.wrap_hi) : x + 1;
+  const uint32_t ym = y == 0 ? n - 1 : y - 1, yp = y == n - 1 ? 0 : y + 1;
+  const uint32_t zm1 = z == 0 ? n - 1 : z - 1, zp4 = z + 4 == n ? 0 : z + 4;
+  const __half* src = static_cast<const __half*>(a.src);
+  __half* dst = static_cast<__half*>(a.dst);
+  float f0[kQ], f1[kQ], f2[kQ], f3[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const uint32_t sx = cx(i) == 1 ? xm : (cx(i) == -1 ? xp : x);
+    const uint32_t sy = cy(i) == 1 ? ym : (cy(i) == -1 ? yp : y);
+    const __half* r = src + i * a.qs + (static_cast<long long>(sx) * n + sy) * n;
+    if (cz(i) == 0) {
+      ld4h(r + z, f0[i], f1[i], f2[i], f3[i]);
+    } else if (cz(i) == 1) {  // cells z..z+3 pull z-1..z+2
+      float w;
+      ld4h(r + z, f1[i], f2[i], f3[i], w);
+      f0[i] = __half2float(r[zm1]);
+    } else {                  // cells z..z+3 pull z+1..z+4
+      float w;
+      ld4h(r + z, w, f0[i], f1[i], f2[i]);
+      f3[i] = __half2float(r[zp4]);
+    }
+  }
+  bgk(f0, a.omega, a.scale, a.inv_scale);
+  bgk(f1, a.omega, a.scale, a.inv_scale);
+  bgk(f2, a.omega, a.scale, a.inv_scale);
+  bgk(f3, a.omega, a.scale, a.inv_scale);
+  __half* o = dst + static_cast<long long>(row) * n + z;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) st4h(o + i * a.qs, f0[i], f1[i], f2[i], f3[i]);
 }
 
 // Body force: the forcing term 3 w_i (c_i . F) added to the stored
@@ -966,7 +1030,15 @@ cudaError_t launch_step_near(const StepArgs& a, const NearTables& nt, cudaStream
 
 template <typename T>
 cudaError_t launch_step_pair(const StepArgs& a, cudaStream_t s) {
-  const cudaError_t e = launch_chain(k_step_pair<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a);
+  // FP16 storage: four cells per thread when n % 4 == 0 (OCTLB_FP16_PAIR=1
+  // keeps two, for comparison)
+  const char* env = std::getenv("OCTLB_FP16_PAIR");
+  const bool pair16 = env && env[0] == '1';
+  cudaError_t e;
+  if (std::is_same<T, __half>::value && a.n % 4 == 0 && !pair16)
+    e = launch_chain(k_step_quad_h, dim3(grid_for(a.ncore / 4)), dim3(kThreads), 0, s, a);
+  else
+    e = launch_chain(k_step_pair<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 // Paired kernel: even n (aligned pairs), n^3 < 2^31.

@@ -205,8 +205,8 @@ int do_advance_level(octlb_ctx* ctx, int l) {
       p.rec_prev = phase == 0 ? rec_prev : nullptr;
       p.fine = cur_buf(F);
       p.fine_qs = F.nslots;
-      p.scale = ctx->prolong_scale;
-      p.omega = static_cast<float>(ctx->omega);
+      p.scale = ctx->pscale_l[l];
+      p.omega = static_cast<float>(ctx->omega_l[l + 1]);  // the written fine cell collides with its level's rate
       p.fscale = F.scale;
       bool share = pend.size() <= 2;
       for (const auto& q : pend)
@@ -230,8 +230,8 @@ int do_advance_level(octlb_ctx* ctx, int l) {
     r.fine_save = save_ptr(F);
     r.coarse = cur_buf(L);
     r.coarse_qs = L.nslots;
-    r.scale = ctx->restrict_scale;
-    r.omega = static_cast<float>(ctx->omega);
+    r.scale = ctx->rscale_l[l];
+    r.omega = static_cast<float>(ctx->omega_l[l]);
     r.cscale = L.scale;
     pend.push_back({r, l});
   }
@@ -247,6 +247,11 @@ int validate(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p) {
   if (p->stream_mode != OCTLB_STREAM_ROTATE && p->stream_mode != OCTLB_STREAM_LINKS)
     return fail(ctx, OCTLB_EINVAL, "unknown stream mode");
   if (!(p->omega > 0.0 && p->omega < 2.0)) return fail(ctx, OCTLB_EINVAL, "omega must lie in (0, 2)");
+  if (p->coupler_mode != OCTLB_COUPLER_REFERENCE && p->coupler_mode != OCTLB_COUPLER_PHYSICAL)
+    return fail(ctx, OCTLB_EINVAL, "unknown coupler mode");
+  for (int l = 0; l < 32 && p->coupler_mode == OCTLB_COUPLER_PHYSICAL; ++l)
+    if (p->omega_level[l] != 0.0 && !(p->omega_level[l] > 0.0 && p->omega_level[l] < 2.0))
+      return fail(ctx, OCTLB_EINVAL, "omega_level must be 0 or lie in (0, 2)");
   for (int b = 0; b < t->n_blocks; ++b)
     if (t->levels[b] < 0 || t->levels[b] > 30) return fail(ctx, OCTLB_EINVAL, "block level out of range");
   const long long n3 = static_cast<long long>(t->n) * t->n * t->n;
@@ -313,6 +318,26 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
   const double tau = 1.0 / p->omega;
   ctx->prolong_scale = static_cast<float>((tau - 0.25) / tau);   // level_coupler.cpp:226-228
   ctx->restrict_scale = static_cast<float>(tau / (tau - 0.25));
+  // Per-level rates and coupler scales: the reference's global ones, or the
+  // physical rescaling from the coarsest level with blocks.
+  ctx->coupler_mode = p->coupler_mode;
+  ctx->omega_l.assign(nlev, p->omega);
+  ctx->pscale_l.assign(nlev, ctx->prolong_scale);
+  ctx->rscale_l.assign(nlev, ctx->restrict_scale);
+  if (p->coupler_mode == OCTLB_COUPLER_PHYSICAL) {
+    int lmin = nlev;
+    for (int b = 0; b < nb; ++b) lmin = std::min(lmin, t->levels[b]);
+    std::vector<double> tl(nlev);
+    for (int l = 0; l < nlev; ++l) {
+      const double given = p->omega_level[l < 32 ? l : 31];
+      tl[l] = given > 0.0 ? 1.0 / given : std::ldexp(tau - 0.5, l - lmin) + 0.5;
+      ctx->omega_l[l] = 1.0 / tl[l];
+    }
+    for (int l = 0; l + 1 < nlev; ++l) {
+      ctx->pscale_l[l] = static_cast<float>(tl[l + 1] / (2.0 * tl[l]));
+      ctx->rscale_l[l] = static_cast<float>(2.0 * tl[l] / tl[l + 1]);
+    }
+  }
   for (int l = 0; l < nlev; ++l) ctx->levels[l].lvl = l;
   std::vector<int> face_nbr(static_cast<size_t>(nb) * 6, -1);
   for (int k = 0; k < t->n_same_level; ++k) {
@@ -1111,7 +1136,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
     A.div_halo = FastDiv(L.n_halo > 0 ? L.n_halo : 1);
     A.div_np = FastDiv(np);
     A.div_np2 = FastDiv(np * np);
-    A.omega = static_cast<float>(p->omega);
+    A.omega = static_cast<float>(ctx->omega_l[l]);
     A.scale = L.scale;
     A.inv_scale = L.inv_scale;
     for (int i = 0; i < kQ; ++i) {
@@ -2087,6 +2112,8 @@ int octlb_gpu_adjoint(octlb_ctx* ctx, const octlb_adj_params* p, double* objecti
   if (ctx->unusable) return fail(ctx, OCTLB_ESTATE, "context unusable after a failed drain of a bounded wait");
   if (ctx->precision != OCTLB_FP32) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates FP32 storage only");
   if (ctx->comm) return fail(ctx, OCTLB_EINVAL, "the adjoint runs on one context, not rank contexts");
+  if (ctx->coupler_mode != OCTLB_COUPLER_REFERENCE)
+    return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates the reference coupler mode (one global tau)");
   if (ctx->const_rho) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates the BGK collide, not ConstRhoBGK");
   return adjoint_impl<float>(ctx, p, objective, grad, grad_force);
 }

@@ -308,6 +308,11 @@ struct octlb_ctx {
   bool use_graphs = true;           // OCTLB_NO_GRAPH=1 launches kernel by kernel
   bool use_pdl = true;              // OCTLB_NO_PDL=1: plain stream order between the step's kernels
   float prolong_scale = 0.f, restrict_scale = 0.f;
+  // Per level: the BGK rate, and the Lagrava scales of the pair (l, l + 1)
+  // (all equal in the reference coupler mode).
+  int coupler_mode = 0;
+  std::vector<double> omega_l;
+  std::vector<float> pscale_l, rscale_l;
   double wall_vscale = 0.0;         // largest moving-wall speed (adjoint velocity parameter)
   std::unique_ptr<AdjointState> adj;
   // ConstRhoBGK (TimeLoop's use_const_rho_bgk, single-level meshes): the

@@ -208,6 +208,16 @@ class Sim:
     def advance(self, steps=1):
         self.L.ref_sim_advance(self.h, ctypes.c_int(steps))
 
+    def set_physical(self, omega_level):
+        """The physical coupler mode (not the reference's loop): level l
+        collides with omega_level[l] and the pair (l, l + 1) is coupled by a
+        LevelCoupler built with omega_level[l]; TimeLoop::advance's phase
+        order restated around the reference's own components.  Before the
+        first advance."""
+        w = np.ascontiguousarray(omega_level, np.float64)
+        self._keep.append(w)
+        self.L.ref_sim_set_physical(self.h, _p(w), ctypes.c_int(len(w)))
+
     def set_const_rho(self, on=True):
         """The reference TimeLoop rebuilt with use_const_rho_bgk (before the
         first advance)."""

@@ -224,7 +224,39 @@ struct Sim {
   std::unique_ptr<TimeLoop> loop;
   double omega = 0.0;
   std::vector<TreeBoundaryFace> tree_faces;
+  // Physical coupler mode (ref_sim_set_physical): per-level rates and one
+  // LevelCoupler per level pair, built with the coarse level's rate.
+  bool physical = false;
+  std::vector<double> omega_level;
+  std::vector<std::unique_ptr<LevelCoupler>> pair_couplers;
+  std::vector<std::vector<label>> by_level;
+  int max_level = 0;
+  long long step = 0;
 };
+
+// TimeLoop::advance (time_loop.h:201-240) restated for the physical mode:
+// the same phase order, each level collided with its own rate omega_level[l],
+// and the pair (l, l + 1) coupled by the LevelCoupler built with omega_level[l]
+// -- whose scales (tau_c - 1/4) / tau_c and tau_c / (tau_c - 1/4)
+// (level_coupler.cpp:226-228) are the Dupuis-Chopard factors tau_f / (2 tau_c)
+// and 2 tau_c / tau_f for tau_f = 2 tau_c - 1/2.  Not the reference's loop: the
+// reference collides every level with one rate.
+void PhysicalAdvance(Sim* s, int level) {
+  const auto& ids = s->by_level[static_cast<std::size_t>(level)];
+  for (label id : ids) (*s->blocks)[id].collide(s->omega_level[static_cast<std::size_t>(level)]);
+  s->bc->apply(nullptr, 1.0, false);
+  s->ghosts->exchange();
+  for (label id : ids) (*s->blocks)[id].take_post_collide_snapshot();
+  for (label id : ids) (*s->blocks)[id].stream();
+  s->bc->apply_post_stream();
+  if (level >= s->max_level) return;
+  LevelCoupler& c = *s->pair_couplers[static_cast<std::size_t>(level)];
+  c.apply_half_time(level);
+  PhysicalAdvance(s, level + 1);
+  c.apply_full_time(level);
+  PhysicalAdvance(s, level + 1);
+  c.restrict(level + 1);
+}
 
 // Sum of MomentumExchangeDrag::force_on_fluid_if over all blocks (see
 // ref_sim_drag).
@@ -515,13 +547,36 @@ void ref_sim_advance_phases(void* h, f64* after_stream, f64* after_post_stream) 
 void ref_sim_free(void* h) {
   auto* s = static_cast<Sim*>(h);
   // TimeLoop / coupler / ghosts hold references: tear down in reverse order.
-  s->loop.reset(); s->bc.reset(); s->coupler.reset(); s->ghosts.reset();
+  s->loop.reset(); s->pair_couplers.clear(); s->bc.reset(); s->coupler.reset(); s->ghosts.reset();
   s->blocks.reset(); s->faces.reset(); s->forest.reset();
   delete s;
 }
 void ref_sim_advance(void* h, int steps) {
   auto* s = static_cast<Sim*>(h);
-  for (int t = 0; t < steps; ++t) s->loop->advance_one();
+  for (int t = 0; t < steps; ++t) {
+    if (!s->physical) {
+      s->loop->advance_one();
+      continue;
+    }
+    s->bc->set_time(static_cast<double>(s->step));  // TimeLoop::advance_one (time_loop.h:242-246)
+    PhysicalAdvance(s, 0);
+    ++s->step;
+  }
+}
+// The physical coupler mode: omega_level[l] the rate of level l (nlev
+// levels); before the first advance.
+void ref_sim_set_physical(void* h, const f64* omega_level, int nlev) {
+  auto* s = static_cast<Sim*>(h);
+  s->physical = true;
+  s->omega_level.assign(omega_level, omega_level + nlev);
+  s->max_level = nlev - 1;
+  s->by_level.assign(static_cast<std::size_t>(nlev), {});
+  for (label id = 0; id < s->blocks->size(); ++id)
+    s->by_level[static_cast<std::size_t>(s->forest->quadrant_level(id))].push_back(id);
+  s->pair_couplers.clear();
+  for (int l = 0; l + 1 < nlev; ++l)
+    s->pair_couplers.push_back(std::make_unique<LevelCoupler>(MPI_COMM_WORLD, *s->faces, *s->forest, *s->blocks,
+                                                              s->n, s->n, s->n, to_f64(omega_level[l])));
 }
 void ref_sim_set_body_force(void* h, const f64* force) {
   auto* s = static_cast<Sim*>(h);

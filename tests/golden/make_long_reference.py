@@ -11,13 +11,17 @@ benchmark configurations, saved as small golden vectors:
                         final rho and u (float32) on every cell of even local
                         indices (1 in 8, all blocks), and sum |u|^2, sum rho
                         over all cells
+  long_c2_amr_physical.npz  the same cavity with tau rescaled per level
+                        (tau_coarse 0.56, tau_fine 0.62: the physical coupler
+                        mode, restated around the reference's components), the
+                        same records
   long_c3_cylinder.npz  three-level channel 256x64x64 finest cells, D = 16
                         exact-circle Bouzidi cylinder, u_max 0.05, Re 100,
                         2,500 coarse steps (20,000 finest steps): the
                         momentum-exchange force after every coarse step
 
 Run from the repository root:
-  python tests/golden/make_long_reference.py c1|c2|c3 [--out DIR]
+  python tests/golden/make_long_reference.py c1|c2|c3|c2p [--out DIR]
 Full final fields are also written (float32) to DIR when given.
 """
 import argparse
@@ -46,7 +50,17 @@ def config(name):
     if name == "c3":
         mesh, init, info = cases.cylinder_forest()
         return mesh, init, info, 2500, True
+    if name == "c2p":  # C2 with tau rescaled per level (physical coupler mode)
+        mesh, init, info = cases.cavity_forest(cells=64, n=8, lid=0.05, tau=0.56, band_cells=8)
+        return mesh, init, info, 625, False
     raise ValueError(name)
+
+
+def physical_omegas(mesh, tau):
+    """Per-level rates of the physical coupler mode: tau_{l+1} - 1/2 =
+    2 (tau_l - 1/2) from the coarsest level with blocks."""
+    lmin, lmax = int(mesh.levels.min()), int(mesh.levels.max())
+    return np.array([1.0 / (2.0 ** (l - lmin) * (tau - 0.5) + 0.5) for l in range(lmax + 1)])
 
 
 def centerlines(mesh, rho, u):
@@ -83,20 +97,22 @@ def centerlines(mesh, rho, u):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("name", choices=["c1", "c2", "c3"])
+    ap.add_argument("name", choices=["c1", "c2", "c3", "c2p"])
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
     ref = oracle.load("ref")
     assert ref is not None, "build oracle/_ref first (make -C oracle ref REF=<reference tree>)"
     mesh, init, info, steps, links = config(args.name)
     sim = oracle.Sim(ref, mesh, info["omega"], init, link_mode=links)
+    if args.name == "c2p":
+        sim.set_physical(physical_omegas(mesh, info["tau"]))
     forces, masses = [], []
     t0 = time.time()
     for s in range(steps):
         sim.advance(1)
         if args.name == "c3":
             forces.append(sim.drag(mesh.obstacle))
-        if args.name == "c2":
+        if args.name in ("c2", "c2p"):
             rho, _ = oracle.rho_u(sim.core())
             masses.append(rho[mesh.kinds == 0].sum())
         if s % 50 == 0:
@@ -109,12 +125,13 @@ def main():
     if args.name == "c1":
         np.savez_compressed(os.path.join(HERE, "long_c1_cavity.npz"), steps=steps,
                             rho=rho.astype(np.float32), u=u.astype(np.float32))
-    elif args.name == "c2":
+    elif args.name in ("c2", "c2p"):
         # the final fields on the cells of even local indices (1 cell in 8,
         # every block of both levels) for the field-wide L2 of u, and the sums
         # of |u|^2 and rho over every cell
         lat = (slice(None), slice(0, None, 2), slice(0, None, 2), slice(0, None, 2))
-        np.savez_compressed(os.path.join(HERE, "long_c2_amr.npz"), steps=steps, mass=np.asarray(masses),
+        np.savez_compressed(os.path.join(HERE, "long_c2_amr.npz" if args.name == "c2" else "long_c2_amr_physical.npz"),
+                            steps=steps, mass=np.asarray(masses),
                             lattice_rho=rho[lat].astype(np.float32), lattice_u=u[lat].astype(np.float32),
                             sum_u2=float(np.sum(u * u)), sum_rho=float(np.sum(rho)),
                             **centerlines(mesh, rho, u))

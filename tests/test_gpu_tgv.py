@@ -117,3 +117,20 @@ def test_set_equilibrium_equals_set_populations(ob, prec):
     assert np.array_equal(a.get_populations(), b.get_populations())
     a.close()
     b.close()
+
+
+def test_fp16_four_cell_step_equals_paired_step(ob, monkeypatch):
+    """The four-cells-per-thread FP16 periodic step (8-byte accesses) and the
+    paired one (OCTLB_FP16_PAIR=1) give bitwise equal states, on a plain
+    periodic box and on x slabs (ghost planes)."""
+    from octlb_b200 import cases
+    n = 64
+    mesh, init, info = cases.tgv_periodic(n, u0=0.05, tau=0.55)
+    out = []
+    for pair in ("0", "1"):
+        monkeypatch.setenv("OCTLB_FP16_PAIR", pair)
+        lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP16_SHIFTED, init_pops=init)
+        lat.advance(7)
+        out.append(lat.get_populations())
+        lat.close()
+    assert np.array_equal(out[0], out[1])

@@ -249,3 +249,18 @@ def test_threaded_restatement_is_the_serial_loop(orc):
     b.set_core(init[0])
     b.run_periodic_mt(info["omega"], 6, 3)
     assert np.array_equal(a.padded(), b.padded())
+
+
+def test_physical_mode_restatement_with_one_rate_is_the_reference_loop(ref):
+    """The physical coupler mode's restated TimeLoop::advance (per-level
+    rates, one LevelCoupler per level pair), given the same rate on every
+    level, is the reference TimeLoop bit for bit: the restatement keeps the
+    reference's phase order."""
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=16, n=8, lid=0.1, tau=0.6, band_cells=8)
+    a = oracle.Sim(ref, mesh, info["omega"], init)
+    a.advance(3)
+    b = oracle.Sim(ref, mesh, info["omega"], init)
+    b.set_physical(np.full(int(mesh.levels.max()) + 1, info["omega"]))
+    b.advance(3)
+    assert np.array_equal(a.core(), b.core())
