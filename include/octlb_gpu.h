@@ -154,6 +154,45 @@ int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on);
  * ConstRhoBGK collide uses; 1 without ConstRhoBGK.  Synchronises the stream. */
 int octlb_gpu_average_rho(octlb_ctx* ctx, double* out);
 
+/* ---- Finite-difference domain boundary conditions -------------------------
+ * The reference's ConcreteDomainBoundaryHandler (domain_boundary_handler.cpp:
+ * 55-89) on the tree-boundary faces, types as DomainBcType
+ * (domain_boundary_handler.h:16-22): 2 InterpolatedVelocity, 4
+ * InterpolatedPressure (the two finite-difference conditions; the other
+ * types are not built on the device).  Every step, after the pull and the
+ * collide of the fluid cells, the velocity- and pressure-Dirichlet cells are
+ * rebuilt from the finite-difference stencil of Skordos' method (plane, edge
+ * and corner cells by their block's extents, in the reference's walk order,
+ * interpolated_velocity.h:571-1037) and the velocity cells then collide at
+ * their prescribed velocity (bc_dispatcher.h:55-72).  Prescribed velocity:
+ * the inlet field of the first face the cell touches that has one (uniform
+ * inlet_u[face] ramped by 10x^3 - 15x^4 + 6x^5, x = t / ramp_end_t), else
+ * u_wall of the y+ face on the interior top-face cells (cavity3d's lid);
+ * pressure cells hold rho_target[face].  The cells must carry their kinds in
+ * the tables (octlb_fd_stamp_kinds), the faces no restated fill
+ * (OCTLB_TB_NONE).  One context, the rotate stream rule, BGK, one level at
+ * forest level 0, blocks of n >= 4; before the first advance. */
+#define OCTLB_FD_VELOCITY 2
+#define OCTLB_FD_PRESSURE 4
+int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double u_wall[18],
+                              const double rho_target[6], const double* inlet_u /* [18] or NULL */,
+                              double ramp_end_t);
+/* bc::StampTreeBoundaryCells (bc_installer.h:95-138): kinds_out = the
+ * tables' kinds with the face slab of every tree-boundary face set to the
+ * kind of that face's type (types as above, plus 0 no-slip, 1 moving lid, 3
+ * outflow), solid cells kept; [n_blocks][n^3].  Host only. */
+int octlb_fd_stamp_kinds(const octlb_tables* tables, const int types[6], uint8_t* kinds_out);
+/* Host-only dry run of octlb_gpu_set_fd_boundary on the tables (every block
+ * at forest level 0, kinds stamped): the per-cell records of the pass (one
+ * per velocity / pressure Dirichlet cell, octlb_fd_record_bytes() bytes
+ * each, the library's internal layout) -- for checking the stencil
+ * resolution on the host.  Returns the number of records, or a negative
+ * error code. */
+int octlb_fd_plan(const octlb_tables* tables, const int types[6], const double u_wall[18],
+                  const double rho_target[6], const double* inlet_u, double ramp_end_t, void* records,
+                  int max_records);
+int octlb_fd_record_bytes(void);
+
 /* ---- VTK output (src/solver/io/vtk_writer/) ------------------------------
  * The files of the reference's writer, byte for byte for the same values: an
  * XML StructuredGrid .vts per block with binary (base64, UInt32 header)

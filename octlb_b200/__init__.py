@@ -226,6 +226,26 @@ def vtk_write_index(output_dir, base_name, step, vts_relative_paths):
         raise OctlbError(rc, "vtk_write_index failed")
 
 
+FD_VELOCITY, FD_PRESSURE = 2, 4
+
+
+def stamp_fd_kinds(mesh, types):
+    """The mesh with its tree-boundary face slabs stamped by face type
+    (octlb_fd_stamp_kinds, the reference's StampTreeBoundaryCells)."""
+    t = np.ascontiguousarray(types, np.int32).reshape(6)
+    kinds = np.zeros_like(mesh.kinds)
+    rc = capi.lib().octlb_fd_stamp_kinds(ctypes.byref(mesh.c_tables()), capi.ptr(t, ctypes.c_int),
+                                         capi.ptr(kinds, ctypes.c_uint8))
+    if rc:
+        raise OctlbError(rc, "stamp_fd_kinds failed")
+    out = Mesh(mesh.n, mesh.levels, mesh.bounds, kinds=kinds, same_level=mesh.same_level,
+               coarse_fine=mesh.coarse_fine, coarse_fine_bounds=mesh.coarse_fine_bounds,
+               tree_boundary=mesh.tree_boundary, tree_boundary_spec=np.zeros_like(mesh.tree_boundary_spec),
+               link_cells=mesh.link_cells, link_q=mesh.link_q, moving=mesh.moving, wall_u=mesh.wall_u,
+               obstacle=mesh.obstacle, periodic=mesh.periodic)
+    return out
+
+
 def partition(mesh, nranks):
     """The reference's weighted partition (octlb_gpu_partition): owning rank
     of every leaf, contiguous runs of the forest order of equal 2^level
@@ -447,6 +467,20 @@ class GpuLattice:
             mask |= _VTK_FIELDS[f]
         self._check(self._L.octlb_gpu_write_vtk(self._h, str(output_dir).encode(), str(base_name).encode(),
                                                 int(step), int(rank), mask, 1 if write_index else 0))
+
+    def set_fd_boundary(self, types, u_wall=None, rho_target=None, inlet_u=None, ramp_end_t=0.0):
+        """The finite-difference domain conditions (octlb_gpu_set_fd_boundary):
+        types per face (x-, x+, y-, y+, z-, z+), FD_VELOCITY or FD_PRESSURE;
+        u_wall [6][3] (the y+ row is the lid), rho_target [6], inlet_u [6][3]
+        (a nonzero row: that face's uniform inlet, ramped over ramp_end_t
+        steps).  The mesh's kinds must be stamped (stamp_fd_kinds)."""
+        t = np.ascontiguousarray(types, np.int32).reshape(6)
+        u = np.zeros((6, 3)) if u_wall is None else np.ascontiguousarray(u_wall, np.float64).reshape(6, 3)
+        r = np.ones(6) if rho_target is None else np.ascontiguousarray(rho_target, np.float64).reshape(6)
+        iu = None if inlet_u is None else np.ascontiguousarray(inlet_u, np.float64).reshape(6, 3)
+        self._check(self._L.octlb_gpu_set_fd_boundary(self._h, capi.ptr(t, ctypes.c_int), capi.ptr(u, ctypes.c_double),
+                                                      capi.ptr(r, ctypes.c_double),
+                                                      capi.ptr(iu, ctypes.c_double), float(ramp_end_t)))
 
     def set_const_rho(self, on=True):
         """ConstRhoBGK (TimeLoop's use_const_rho_bgk): before the first

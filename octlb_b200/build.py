@@ -15,8 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liboctlb_b200.so")
 OBJ = os.path.join(HERE, "..", "_build")
-SOURCES = ["lbm_kernels.cu", "lbm_bulk.cu", "lbm_adjoint.cu", "lbm_exchange.cu", "octlb_ctx.cu", "octlb_part.cu",
-           "forest.cpp", "vtk_writer.cpp"]
+SOURCES = ["lbm_kernels.cu", "lbm_bulk.cu", "lbm_adjoint.cu", "lbm_exchange.cu", "lbm_fd.cu", "octlb_ctx.cu",
+           "octlb_part.cu", "octlb_fd.cu", "forest.cpp", "vtk_writer.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo"] + ARCH + ["-Xcompiler", "-fPIC"]
 

@@ -110,6 +110,11 @@ def lib():
         "octlb_gpu_set_equilibrium": (ctypes.c_int, [P, F64P, F64P]),
         "octlb_gpu_set_body_force": (ctypes.c_int, [P, F64P]),
         "octlb_gpu_set_const_rho": (ctypes.c_int, [P, ctypes.c_int]),
+        "octlb_gpu_set_fd_boundary": (ctypes.c_int, [P, I32P, F64P, F64P, F64P, ctypes.c_double]),
+        "octlb_fd_stamp_kinds": (ctypes.c_int, [ctypes.POINTER(Tables), I32P, U8P]),
+        "octlb_fd_plan": (ctypes.c_int, [ctypes.POINTER(Tables), I32P, F64P, F64P, F64P, ctypes.c_double, P,
+                                         ctypes.c_int]),
+        "octlb_fd_record_bytes": (ctypes.c_int, []),
         "octlb_gpu_write_vtk": (ctypes.c_int, [P, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, ctypes.c_int]),
         "octlb_vtk_write_block": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, F64P,

@@ -1,0 +1,275 @@
+// Finite-difference domain boundary conditions on the device: the post-stream
+// reconstruction of velocity- and pressure-Dirichlet cells (Skordos
+// InterpolatedVelocity, ApplyInterpolatedVelocityBoundaryCells,
+// interpolated_velocity.h:951-1037: plane :571-636, edge :687-752, corner
+// :638-685, the BoundaryLatticeView reads :213-445) and their Dirichlet
+// collide (BcDispatcher::collide's velocity arm, bc_dispatcher.h:55-72 with
+// BoundaryCellStatisticRho, interpolated_velocity.h:815-884).
+//
+// After a level step the state buffer holds, for a boundary cell, its
+// post-stream populations f (the step leaves non-kBulk cells uncollided) and,
+// for a fluid cell, its post-collision populations, whose velocity is the
+// post-stream one (the collide keeps rho u).  The reference rewrites the
+// boundary cells in place in (ix, iy, iz) order; a cell's stencil reads the
+// densities of boundary cells one and two cells inward, rewritten or not by
+// that order.  Edge cells read plane cells and corners read edge cells, so the
+// pass runs as three launches -- planes, edges, corners -- each writing the
+// rewritten populations to its own rows and reading an earlier phase's row
+// where the reference's walk would have rewritten the cell already.  A fourth
+// launch collides the rewritten cells (velocity cells at the prescribed
+// velocity, the next step's time; pressure cells are not collided) into the
+// state buffer.  Every read a cell makes is resolved on the host into a table
+// (FdCell): which slot or row, the velocity source (fluid populations, the
+// prescribed velocity of a boundary cell, the overlap padding at rest, or a
+// mirror image with flipped normal components), the density source.
+// Arithmetic FP32; storage FP32 or FP16-shifted.
+#include "octlb_internal.h"
+
+namespace octlb_gpu {
+
+namespace {
+
+constexpr int kFdThreads = 128;
+
+// PolynomialStartScale: 10 x^3 - 15 x^4 + 6 x^5, x = t / t_end clamped to [0, 1].
+__device__ __forceinline__ float ramp(float t, float t_end) {
+  if (t_end <= 0.f) return 1.f;
+  const float x = fminf(fmaxf(t / t_end, 0.f), 1.f);
+  return x * x * x * (10.f + x * (-15.f + 6.f * x));
+}
+
+__device__ __forceinline__ void prescribed(const FdCell* cells, int row, float t, float u[3]) {
+  const FdCell& b = cells[row];
+  const float r = ramp(t, b.ramp_end);
+  u[0] = r * b.u_base[0];
+  u[1] = r * b.u_base[1];
+  u[2] = r * b.u_base[2];
+}
+
+template <typename T>
+__device__ __forceinline__ void load_pops(const T* state, long long qs, long long slot, float inv_s, float f[kQ]) {
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) f[i] = Store<T>::ld(state + i * qs + slot, inv_s);
+}
+
+__device__ __forceinline__ float sum_pops(const float f[kQ]) {
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) s += f[i];
+  return s;
+}
+
+// velocityBMRho: (2 sum_{c_d = o} f + sum_{c_d = 0} f + 1) / (1 + o u_d).
+__device__ __forceinline__ float bm_rho(const float f[kQ], int d, int o, const float u[3]) {
+  float out = 0.f, wall = 0.f;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const int c = d == 0 ? cx(i) : (d == 1 ? cy(i) : cz(i));
+    if (c == 0) wall += f[i];
+    else if (c == o) out += f[i];
+  }
+  return (2.f * out + wall + 1.f) / (1.f + o * u[d]);
+}
+
+// Shifted second-order equilibrium, rho w (1 + 3 cu + 4.5 cu^2 - 1.5 u^2) - w.
+__device__ __forceinline__ float feq_i(int i, float rho, const float u[3], float usq) {
+  const float cu = cx(i) * u[0] + cy(i) * u[1] + cz(i) * u[2];
+  return rho * wf(i) * (1.f + 3.f * cu + 4.5f * cu * cu - 1.5f * usq) - wf(i);
+}
+
+template <typename T>
+struct FdCtx {
+  const T* state;
+  long long qs;
+  float inv_s;
+  const FdCell* cells;
+  const float* fnew;  // [rows][19]
+  float t;
+};
+
+template <typename T>
+__device__ __forceinline__ void read_u(const FdCtx<T>& c, const FdURead& r, float u[3]) {
+  if (r.code == kFdZero) {
+    u[0] = u[1] = u[2] = 0.f;
+  } else if (r.code == kFdFluid) {
+    float f[kQ];
+    load_pops(c.state, c.qs, r.idx, c.inv_s, f);
+    float dh, jx, jy, jz;
+    moments(f, dh, jx, jy, jz);
+    const float k = 1.f / (1.f + dh);
+    u[0] = jx * k; u[1] = jy * k; u[2] = jz * k;
+  } else {
+    prescribed(c.cells, static_cast<int>(r.idx), c.t, u);
+  }
+  if (r.flip & 1) u[0] = -u[0];
+  if (r.flip & 2) u[1] = -u[1];
+  if (r.flip & 4) u[2] = -u[2];
+}
+
+template <typename T>
+__device__ __forceinline__ float read_rho(const FdCtx<T>& c, const FdRRead& r) {
+  if (r.code == kFdRhoConst) return r.val;
+  float f[kQ];
+  if (r.code == kFdRhoSumPre || r.code == kFdRhoBmPre) {
+    load_pops(c.state, c.qs, r.idx, c.inv_s, f);
+  } else {
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) f[i] = c.fnew[r.idx * kQ + i];
+  }
+  if (r.code == kFdRhoSumPre || r.code == kFdRhoSumNew) return 1.f + sum_pops(f);
+  float u[3];
+  prescribed(c.cells, r.urow, c.t, u);
+  return bm_rho(f, r.d, r.o, u);
+}
+
+// Gradient along `axis` by the one-sided second-order stencil
+// -n (-3 u0 + 4 u1 - u2) / 2 (u1, u2 one and two cells inward).
+__device__ __forceinline__ void normal_grad(const float u0[3], const float u1[3], const float u2[3], int n,
+                                            float g[3]) {
+#pragma unroll
+  for (int b = 0; b < 3; ++b) g[b] = -n * (-3.f * u0[b] + 4.f * u1[b] - u2[b]) * 0.5f;
+}
+
+// One boundary cell of role `role` (1 plane, 2 edge, 3 corner): rewritten
+// populations feq(rho, u) + f_neq(Pi), Pi = -rho / (3 omega) (du + du^T), into
+// its row of fnew.
+template <typename T>
+__global__ void __launch_bounds__(kFdThreads)
+k_fd_reconstruct(const T* state, long long qs, float inv_s, const FdCell* cells, const int* list, int n,
+                 float* fnew, const double* time, float omega) {
+  const int k = blockIdx.x * kFdThreads + threadIdx.x;
+  if (k >= n) return;
+  const int row = list[k];
+  const FdCell& cell = cells[row];
+  FdCtx<T> c{state, qs, inv_s, cells, fnew, static_cast<float>(*time)};
+  float uu[7][3];
+#pragma unroll
+  for (int j = 0; j < 7; ++j) read_u(c, cell.u[j], uu[j]);
+  float du[3][3];
+  float rho;
+  if (cell.role == 1) {
+    const int d = cell.d, o = cell.o;
+    if (cell.kind == kPressureDirichlet) {
+      rho = cell.rho_target;
+    } else {
+      float f[kQ];
+      load_pops(state, qs, cell.slot, inv_s, f);
+      rho = bm_rho(f, d, o, uu[0]);
+    }
+    normal_grad(uu[0], uu[1], uu[2], o, du[d]);
+    const int t0 = (d + 1) % 3 < (d + 2) % 3 ? (d + 1) % 3 : (d + 2) % 3;
+    const int t1 = 3 - d - t0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      du[t0][b] = (uu[3][b] - uu[4][b]) * 0.5f;
+      du[t1][b] = (uu[5][b] - uu[6][b]) * 0.5f;
+    }
+  } else if (cell.role == 2) {
+    const int p = cell.ax[0], d1 = cell.ax[1], d2 = cell.ax[2];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) du[p][b] = (uu[1][b] - uu[2][b]) * 0.5f;
+    normal_grad(uu[0], uu[3], uu[4], cell.nrm[0], du[d1]);
+    normal_grad(uu[0], uu[5], uu[6], cell.nrm[1], du[d2]);
+    rho = 2.f / 3.f * (read_rho(c, cell.r[0]) + read_rho(c, cell.r[1])) -
+          1.f / 6.f * (read_rho(c, cell.r[2]) + read_rho(c, cell.r[3]));
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) normal_grad(uu[0], uu[1 + 2 * a], uu[2 + 2 * a], cell.nrm[a], du[a]);
+    rho = 4.f / 9.f * (read_rho(c, cell.r[0]) + read_rho(c, cell.r[1]) + read_rho(c, cell.r[2])) -
+          1.f / 9.f * (read_rho(c, cell.r[3]) + read_rho(c, cell.r[4]) + read_rho(c, cell.r[5]));
+  }
+  const float s = -rho / 3.f / omega;
+  const float pi[6] = {2.f * du[0][0] * s, (du[0][1] + du[1][0]) * s, (du[0][2] + du[2][0]) * s,
+                       2.f * du[1][1] * s, (du[1][2] + du[2][1]) * s, 2.f * du[2][2] * s};
+  const float* u = uu[0];
+  const float usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  float* out = fnew + static_cast<long long>(row) * kQ;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const float c3[3] = {static_cast<float>(cx(i)), static_cast<float>(cy(i)), static_cast<float>(cz(i))};
+    // f_neq from the symmetric stress (lbm.h:248-270): sum over a <= b of
+    // (c_a c_b - delta_ab / 3) (x2 off the diagonal) Pi_ab, times w 9 / 2
+    float q = 0.f;
+    int m = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = a; b < 3; ++b, ++m) {
+        float qq = c3[a] * c3[b] - (a == b ? 1.f / 3.f : 0.f);
+        if (a != b) qq *= 2.f;
+        q += qq * pi[m];
+      }
+    out[i] = feq_i(i, rho, u, usq) + q * wf(i) * 4.5f;
+  }
+}
+
+// The Dirichlet collide of the boundary cells into the state buffer: velocity
+// cells f (1 - omega) + omega feq(rho, u_presc(t)), rho = velocityBMRho on
+// plane cells and 1 + sum f on edges and corners; pressure cells unchanged.
+// Source: the rewritten rows (after the pass) or the state itself (the
+// initial state, before the first step).
+template <typename T>
+__global__ void __launch_bounds__(kFdThreads)
+k_fd_collide(T* state, long long qs, float scale, float inv_s, const FdCell* cells, int n, const float* fnew,
+             const double* time, double time_shift, float omega) {
+  const int row = blockIdx.x * kFdThreads + threadIdx.x;
+  if (row >= n) return;
+  const FdCell& cell = cells[row];
+  float f[kQ];
+  if (fnew) {
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) f[i] = fnew[static_cast<long long>(row) * kQ + i];
+  } else {
+    load_pops(state, qs, cell.slot, inv_s, f);
+  }
+  if (cell.kind == kVelocityDirichlet) {
+    float u[3];
+    prescribed(cells, row, static_cast<float>(*time + time_shift), u);
+    const float rho = cell.role == 1 ? bm_rho(f, cell.d, cell.o, u) : 1.f + sum_pops(f);
+    const float usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) f[i] = f[i] * (1.f - omega) + omega * feq_i(i, rho, u, usq);
+  }
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) Store<T>::st(state + i * qs + cell.slot, f[i], scale);
+}
+
+__global__ void k_fd_tick(double* time) { *time += 1.0; }
+
+inline unsigned fd_grid(int n) { return static_cast<unsigned>((n + kFdThreads - 1) / kFdThreads); }
+
+}  // namespace
+
+template <typename T>
+cudaError_t launch_fd_reconstruct(const void* state, long long qs, float inv_s, const FdCell* cells, const int* list,
+                                  int n, float* fnew, const double* time, float omega, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_fd_reconstruct<T><<<fd_grid(n), kFdThreads, 0, s>>>(static_cast<const T*>(state), qs, inv_s, cells, list, n,
+                                                         fnew, time, omega);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_fd_collide(void* state, long long qs, float scale, float inv_s, const FdCell* cells, int n,
+                              const float* fnew, const double* time, double time_shift, float omega,
+                              cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_fd_collide<T><<<fd_grid(n), kFdThreads, 0, s>>>(static_cast<T*>(state), qs, scale, inv_s, cells, n, fnew, time,
+                                                     time_shift, omega);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fd_tick(double* time, cudaStream_t s) {
+  k_fd_tick<<<1, 1, 0, s>>>(time);
+  return cudaGetLastError();
+}
+
+#define OCTLB_FD_INST(T)                                                                                      \
+  template cudaError_t launch_fd_reconstruct<T>(const void*, long long, float, const FdCell*, const int*, int, \
+                                                float*, const double*, float, cudaStream_t);                \
+  template cudaError_t launch_fd_collide<T>(void*, long long, float, float, const FdCell*, int, const float*,  \
+                                            const double*, double, float, cudaStream_t);
+OCTLB_FD_INST(float)
+OCTLB_FD_INST(__half)
+
+}  // namespace octlb_gpu

@@ -169,6 +169,8 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
   ++L.substep;
   L.cur = 1 - L.cur;
   if (rec) L.rec_cur = next_cur;
+  // the finite-difference domain boundary pass on the new state
+  if (int rc = fd_after_step<T>(ctx, L)) return rc;
   // the save rows other ranks' coupler items read, and those this rank's read
   return exchange_rows(ctx, L);
 }
@@ -1354,6 +1356,7 @@ int advance_one_launches(octlb_ctx* ctx) {
     ctx->side_busy = false;
     ++ctx->launch_count;
   }
+  if (int rc2 = fd_end_of_step(ctx)) return rc2;
   if (!(ctx->adj && ctx->adj->recording)) ctx->launches_per_step = ctx->launch_count;
   return OCTLB_OK;
 }
@@ -2114,6 +2117,7 @@ int octlb_gpu_adjoint(octlb_ctx* ctx, const octlb_adj_params* p, double* objecti
   if (ctx->comm) return fail(ctx, OCTLB_EINVAL, "the adjoint runs on one context, not rank contexts");
   if (ctx->coupler_mode != OCTLB_COUPLER_REFERENCE)
     return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates the reference coupler mode (one global tau)");
+  if (ctx->fd_on) return fail(ctx, OCTLB_EINVAL, "the adjoint does not differentiate the fd boundary pass");
   if (ctx->const_rho) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates the BGK collide, not ConstRhoBGK");
   return adjoint_impl<float>(ctx, p, objective, grad, grad_force);
 }
@@ -2122,6 +2126,7 @@ int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on) {
   if (!ctx) return OCTLB_EINVAL;
   if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
   if (ctx->comm && on) return fail(ctx, OCTLB_EINVAL, "ConstRhoBGK is built for one context, not rank contexts");
+  if (ctx->fd_on && on) return fail(ctx, OCTLB_EINVAL, "ConstRhoBGK with the fd boundary pass is not built");
   for (int c : ctx->counters_collide)
     if (c != 0) return fail(ctx, OCTLB_ESTATE, "ConstRhoBGK is chosen before the first advance");
   if ((on != 0) == ctx->const_rho) return OCTLB_OK;

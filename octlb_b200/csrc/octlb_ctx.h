@@ -332,6 +332,14 @@ struct octlb_ctx {
   // periodic (nranks n) x n x n box, with two ghost x planes after its core
   // that the neighbouring slabs fill before every step.
   bool slab = false;
+  // Finite-difference domain boundary conditions (octlb_gpu_set_fd_boundary):
+  // one record per Dirichlet cell, the cells of each role (plane, edge,
+  // corner) as runs of fd_lists, the rewritten rows, and the time of the
+  // current advance_one (the inlet ramp's clock).
+  bool fd_on = false;
+  DevBuf fd_cells, fd_lists, fd_new, fd_time;
+  int fd_rows = 0;
+  std::vector<int> fd_first, fd_count;
   bool owns(int b) const { return owner.empty() || owner[b] == rank; }
   // Host-only planning of a rank context (octlb_gpu_plan_part): the exchange
   // lists as (level, kind, peer, global cell) records, kind 0 / 1 cells sent /
@@ -360,6 +368,10 @@ int comm_allreduce(octlb_ctx* ctx, double* v, int n);
 int comm_synchronize(octlb_ctx* ctx);
 int comm_attach(octlb_ctx* ctx);
 int comm_nranks(const octlb_comm* comm);
+// Finite-difference domain boundary pass (octlb_fd.cu).
+template <typename T> int fd_after_step(octlb_ctx* ctx, Level& L);
+int fd_end_of_step(octlb_ctx* ctx);
+void clear_graphs(octlb_ctx* ctx);
 void comm_detach(octlb_ctx* ctx);
 
 inline long long core_slot_of(int n, int local_blk, int x, int y, int z) {

@@ -1,0 +1,412 @@
+// Host side of the finite-difference domain boundary conditions
+// (octlb_gpu_set_fd_boundary): the reference's ConcreteDomainBoundaryHandler
+// (domain_boundary_handler.cpp:55-89) with InterpolatedVelocity and
+// InterpolatedPressure faces.  Every velocity / pressure Dirichlet cell's
+// stencil (ApplyInterpolatedVelocityBoundaryCells,
+// interpolated_velocity.h:951-1037) is resolved here into an FdCell record:
+// the cell's role from its block's extents (plane, edge, corner), its
+// prescribed velocity (PrescribedBoundaryU, :69-117: the first touched face
+// with an inlet field, else the y+ face's wall velocity on interior top-face
+// cells), and each velocity and density read -- inside the block, in the
+// overlap padding (rho = 1, u = 0 within min(halo, 2) = 1 cell of the
+// block), or mirrored back inside with the crossed components negated, as
+// the BoundaryLatticeView reads them (:213-445).  A density read of a
+// boundary cell takes the rewritten populations when the reference's in-place
+// (ix, iy, iz) walk has rewritten that cell before the reader.
+#include "octlb_ctx.h"
+
+namespace octlb_gpu {
+template <typename T>
+cudaError_t launch_fd_reconstruct(const void*, long long, float, const FdCell*, const int*, int, float*,
+                                  const double*, float, cudaStream_t);
+template <typename T>
+cudaError_t launch_fd_collide(void*, long long, float, float, const FdCell*, int, const float*, const double*,
+                              double, float, cudaStream_t);
+cudaError_t launch_fd_tick(double*, cudaStream_t);
+}  // namespace octlb_gpu
+
+using namespace octlb_gpu;
+using namespace octlb_host;
+
+namespace {
+
+struct Pos {
+  int x, y, z;
+  int& operator[](int a) { return a == 0 ? x : (a == 1 ? y : z); }
+  int operator[](int a) const { return a == 0 ? x : (a == 1 ? y : z); }
+  bool operator<(const Pos& o) const { return x != o.x ? x < o.x : (y != o.y ? y < o.y : z < o.z); }
+};
+
+struct Builder {
+  octlb_ctx* ctx;
+  int n, lb;                       // block edge, local block
+  const uint8_t* kinds;            // this block's kinds [n^3]
+  const std::vector<int>* row_of;  // this block's cell -> row (-1: not a boundary cell)
+  const std::vector<FdCell>* cells;
+  std::vector<int>* role_of;       // row -> role
+  const double* rho_target;        // [6]
+
+  bool inside(const Pos& p) const { return p.x >= 0 && p.y >= 0 && p.z >= 0 && p.x < n && p.y < n && p.z < n; }
+  // The overlap padding the view reads as rest (halo 1: one cell outside).
+  bool padding(const Pos& p) const {
+    return !inside(p) && p.x >= -1 && p.y >= -1 && p.z >= -1 && p.x <= n && p.y <= n && p.z <= n;
+  }
+  Pos mirror(const Pos& p) const {
+    Pos m = p;
+    for (int a = 0; a < 3; ++a) {
+      if (m[a] < 0) m[a] = -m[a];
+      else if (m[a] >= n) m[a] = 2 * (n - 1) - m[a];
+    }
+    return m;
+  }
+  int cell(const Pos& p) const { return (p.x * n + p.y) * n + p.z; }
+  long long slot(const Pos& p) const { return core_slot_of(n, lb, p.x, p.y, p.z); }
+  int kind(const Pos& p) const { return kinds[cell(p)]; }
+  // the single face a cell lies on, or none (axis -1)
+  void flat(const Pos& p, int& d, int& o) const {
+    int cnt = 0;
+    d = -1;
+    o = 0;
+    for (int a = 0; a < 3; ++a) {
+      if (p[a] == 0) { d = a; o = -1; ++cnt; }
+      else if (p[a] == n - 1) { d = a; o = 1; ++cnt; }
+    }
+    if (cnt != 1) d = -1;
+  }
+
+  int resolve_u(Pos p, int flips, FdURead& out, int depth = 0) const {
+    if (depth > 8) return fail(ctx, OCTLB_EINVAL, "fd boundary: velocity read does not resolve");
+    if (!inside(p)) {
+      if (padding(p)) {
+        out = {0, kFdZero, flips};
+        return OCTLB_OK;
+      }
+      int f = flips;
+      for (int a = 0; a < 3; ++a)
+        if (p[a] < 0 || p[a] >= n) f ^= 1 << a;
+      return resolve_u(mirror(p), f, out, depth + 1);
+    }
+    const int k = kind(p);
+    if (k == kVelocityDirichlet) {
+      out = {(*row_of)[cell(p)], kFdPrescribed, flips};
+      return OCTLB_OK;
+    }
+    if (k == kPressureDirichlet) {  // ExtrapolatedU: the inward neighbour's velocity
+      int d, o;
+      flat(p, d, o);
+      if (d < 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: a pressure cell off the faces' planes");
+      p[d] -= o;
+      return resolve_u(p, flips, out, depth + 1);
+    }
+    out = {slot(p), kFdFluid, flips};
+    return OCTLB_OK;
+  }
+
+  int resolve_rho(Pos p, const Pos& reader, int reader_role, FdRRead& out, int depth = 0) const {
+    if (depth > 8) return fail(ctx, OCTLB_EINVAL, "fd boundary: density read does not resolve");
+    if (!inside(p)) {
+      if (padding(p)) {
+        out = {0, 1.f, kFdRhoConst, 0, 0, 0};
+        return OCTLB_OK;
+      }
+      return resolve_rho(mirror(p), reader, reader_role, out, depth + 1);
+    }
+    const int k = kind(p);
+    int d, o;
+    flat(p, d, o);
+    if (k == kPressureDirichlet) {
+      if (d < 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: a pressure cell off the faces' planes");
+      out = {0, static_cast<float>(rho_target[2 * d + (o > 0)]), kFdRhoConst, 0, 0, 0};
+      return OCTLB_OK;
+    }
+    const int row = (*row_of)[cell(p)];
+    bool fresh = false;
+    if (row >= 0 && p < reader) {
+      const int pr = (*role_of)[row];
+      if (pr == reader_role) return fail(ctx, OCTLB_EINVAL, "fd boundary: blocks of n >= 4 only");
+      fresh = pr < reader_role;
+    }
+    if (k == kVelocityDirichlet && d >= 0) {
+      out = {fresh ? row : slot(p), 0.f, fresh ? kFdRhoBmNew : kFdRhoBmPre, row, d, o};
+    } else {
+      out = {fresh ? row : slot(p), 0.f, fresh ? kFdRhoSumNew : kFdRhoSumPre, 0, 0, 0};
+    }
+    return OCTLB_OK;
+  }
+};
+
+}  // namespace
+
+namespace octlb_host {
+
+// The pass after a step of level L: planes, edges, corners, then the
+// Dirichlet collide of the rewritten cells at the next step's time.
+template <typename T>
+int fd_after_step(octlb_ctx* ctx, Level& L) {
+  if (!ctx->fd_on || L.nblk == 0) return OCTLB_OK;
+  void* state = cur_buf(L);
+  const FdCell* cells = ctx->fd_cells.as<FdCell>();
+  float* fnew = ctx->fd_new.as<float>();
+  const double* time = ctx->fd_time.as<double>();
+  const float omega = static_cast<float>(ctx->omega_l[L.lvl]);
+  for (int role = 1; role <= 3; ++role) {
+    const int n = ctx->fd_count[role];
+    if (n == 0) continue;
+    CK(launch_fd_reconstruct<T>(state, L.nslots, L.inv_scale, cells, ctx->fd_lists.as<int>() + ctx->fd_first[role],
+                                n, fnew, time, omega, ctx->stream));
+    ++ctx->launch_count;
+  }
+  CK(launch_fd_collide<T>(state, L.nslots, L.scale, L.inv_scale, cells, ctx->fd_rows, fnew, time, 1.0, omega,
+                          ctx->stream));
+  ++ctx->launch_count;
+  return OCTLB_OK;
+}
+template int fd_after_step<float>(octlb_ctx*, Level&);
+template int fd_after_step<__half>(octlb_ctx*, Level&);
+
+int fd_end_of_step(octlb_ctx* ctx) {
+  if (!ctx->fd_on) return OCTLB_OK;
+  CK(launch_fd_tick(ctx->fd_time.as<double>(), ctx->stream));
+  ++ctx->launch_count;
+  return OCTLB_OK;
+}
+
+}  // namespace octlb_host
+
+extern "C" {
+
+int octlb_fd_stamp_kinds(const octlb_tables* t, const int types[6], uint8_t* kinds) {
+  if (!t || !types || !kinds || !t->tree_boundary || t->n < 1) return OCTLB_EINVAL;
+  const int n = t->n;
+  const long long n3 = static_cast<long long>(n) * n * n;
+  std::memcpy(kinds, t->kinds, static_cast<size_t>(n3 * t->n_blocks));
+  // BcKindFromSpecType (bc_installer.h:44-58) and StampTreeBoundaryCells
+  // (:95-138): the face slab of every tree-boundary face, solid cells kept.
+  static const uint8_t kind_of[5] = {kBounceBack, kMovingBounceBack, kVelocityDirichlet, kOutflow,
+                                     kPressureDirichlet};
+  for (int f = 0; f < 6; ++f)
+    if (types[f] < 0 || types[f] > 4) return OCTLB_EINVAL;
+  for (int k = 0; k < t->n_tree_boundary; ++k) {
+    const int b = t->tree_boundary[2 * k], dir = t->tree_boundary[2 * k + 1];
+    if (b < 0 || b >= t->n_blocks || dir < 0 || dir > 5) return OCTLB_EINVAL;
+    const int ax = dir / 2, side = (dir & 1) ? n - 1 : 0;
+    for (int a = 0; a < n; ++a)
+      for (int c = 0; c < n; ++c) {
+        int p[3];
+        p[ax] = side;
+        p[(ax + 1) % 3] = a;
+        p[(ax + 2) % 3] = c;
+        const long long g = b * n3 + (static_cast<long long>(p[0]) * n + p[1]) * n + p[2];
+        if (kinds[g] != kSolid) kinds[g] = kind_of[types[dir]];
+      }
+  }
+  return OCTLB_OK;
+}
+
+}  // extern "C"
+
+namespace octlb_host {
+
+// The records of the pass for the blocks `blocks` (global ids, all of forest
+// level 0, in local order) with the given kinds: cells in (block, x, y, z)
+// order, and per role the rows of that role.  Host only.
+int fd_build(octlb_ctx* ctx, int n, const std::vector<int>& blocks, const uint8_t* kinds, const int types[6],
+             const double* u_wall, const double* rho_target, const double* inlet_u, double ramp_end_t,
+             std::vector<FdCell>& cells, std::vector<int>& lists, std::vector<int>& first, std::vector<int>& count) {
+  for (int f = 0; f < 6; ++f)
+    if (types[f] != 2 && types[f] != 4)
+      return fail(ctx, OCTLB_EINVAL, "fd boundary: faces take InterpolatedVelocity (2) or InterpolatedPressure (4)");
+  if (n < 4) return fail(ctx, OCTLB_EINVAL, "fd boundary: blocks of n >= 4 only");
+  const long long n3 = static_cast<long long>(n) * n * n;
+  const int nblk = static_cast<int>(blocks.size());
+  // rows: boundary cells in (block, x, y, z) order
+  cells.clear();
+  std::vector<std::vector<int>> row_of(static_cast<size_t>(nblk), std::vector<int>(static_cast<size_t>(n3), -1));
+  for (int lb = 0; lb < nblk; ++lb) {
+    const uint8_t* kb = kinds + static_cast<size_t>(blocks[lb]) * n3;
+    for (long long c = 0; c < n3; ++c)
+      if (kb[c] == kVelocityDirichlet || kb[c] == kPressureDirichlet) {
+        row_of[lb][c] = static_cast<int>(cells.size());
+        FdCell fc{};
+        fc.slot = lb * n3 + c;
+        fc.kind = kb[c];
+        cells.push_back(fc);
+      }
+  }
+  if (cells.empty()) return fail(ctx, OCTLB_EINVAL, "fd boundary: no velocity or pressure Dirichlet cells");
+  std::vector<int> role(cells.size());
+  for (int lb = 0; lb < nblk; ++lb)
+    for (long long c = 0; c < n3; ++c) {
+      const int r = row_of[lb][c];
+      if (r < 0) continue;
+      const int x = static_cast<int>(c / (n * n)), y = static_cast<int>((c / n) % n), z = static_cast<int>(c % n);
+      int cnt = 0;
+      for (int v : {x, y, z}) cnt += (v == 0 || v == n - 1) ? 1 : 0;
+      if (cnt == 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: a Dirichlet cell off its block's faces");
+      role[r] = cnt;
+    }
+  for (int lb = 0; lb < nblk; ++lb) {
+    Builder B{ctx, n, lb, kinds + static_cast<size_t>(blocks[lb]) * n3, &row_of[lb], &cells, &role, rho_target};
+    for (long long c = 0; c < n3; ++c) {
+      const int r = row_of[lb][c];
+      if (r < 0) continue;
+      FdCell& fc = cells[r];
+      const Pos p{static_cast<int>(c / (n * n)), static_cast<int>((c / n) % n), static_cast<int>(c % n)};
+      fc.role = role[r];
+      // prescribed velocity
+      const bool on[6] = {p.x == 0, p.x == n - 1, p.y == 0, p.y == n - 1, p.z == 0, p.z == n - 1};
+      bool done = false;
+      for (int f = 0; f < 6 && !done; ++f) {
+        if (!on[f] || !inlet_u) continue;
+        const double* iu = inlet_u + 3 * f;
+        if (iu[0] == 0.0 && iu[1] == 0.0 && iu[2] == 0.0) continue;
+        for (int a = 0; a < 3; ++a) fc.u_base[a] = static_cast<float>(iu[a]);
+        fc.ramp_end = static_cast<float>(ramp_end_t);
+        done = true;
+      }
+      if (!done && p.y == n - 1 && p.x > 0 && p.x < n - 1 && p.z > 0 && p.z < n - 1)
+        for (int a = 0; a < 3; ++a) fc.u_base[a] = static_cast<float>(u_wall[3 * 3 + a]);
+      int side[3];
+      for (int a = 0; a < 3; ++a) side[a] = p[a] == 0 ? -1 : (p[a] == n - 1 ? 1 : 0);
+      auto at = [&](std::initializer_list<std::pair<int, int>> steps) {
+        Pos q = p;
+        for (const auto& s : steps) q[s.first] += s.second;
+        return q;
+      };
+      int rc = OCTLB_OK;
+      if (fc.role == 1) {
+        int d, o;
+        B.flat(p, d, o);
+        fc.d = d;
+        fc.o = o;
+        if (fc.kind == kPressureDirichlet) fc.rho_target = static_cast<float>(rho_target[2 * d + (o > 0)]);
+        const int t0 = std::min((d + 1) % 3, (d + 2) % 3), t1 = 3 - d - t0;
+        const Pos q[7] = {p, at({{d, -o}}), at({{d, -2 * o}}), at({{t0, 1}}), at({{t0, -1}}), at({{t1, 1}}),
+                          at({{t1, -1}})};
+        for (int j = 0; j < 7 && !rc; ++j) rc = B.resolve_u(q[j], 0, fc.u[j]);
+      } else if (fc.role == 2) {
+        // ApplyInterpolatedVelocityBoundaryCells' pairing of the edge's two
+        // normals (interpolated_velocity.h:991-1012): x & y -> axis z,
+        // x & z -> axis y with d1 = z, d2 = x, y & z -> axis x.
+        int plane, n1, n2;
+        if (side[0] && side[1]) { plane = 2; n1 = side[0]; n2 = side[1]; }
+        else if (side[0] && side[2]) { plane = 1; n1 = side[0]; n2 = side[2]; }
+        else { plane = 0; n1 = side[1]; n2 = side[2]; }
+        const int d1 = (plane + 1) % 3, d2 = (plane + 2) % 3;
+        fc.ax[0] = plane; fc.ax[1] = d1; fc.ax[2] = d2;
+        fc.nrm[0] = n1; fc.nrm[1] = n2;
+        const Pos q[7] = {p, at({{plane, 1}}), at({{plane, -1}}), at({{d1, -n1}}), at({{d1, -2 * n1}}),
+                          at({{d2, -n2}}), at({{d2, -2 * n2}})};
+        for (int j = 0; j < 7 && !rc; ++j) rc = B.resolve_u(q[j], 0, fc.u[j]);
+        const Pos rq[4] = {at({{d2, -n2}}), at({{d1, -n1}}), at({{d2, -2 * n2}}), at({{d1, -2 * n1}})};
+        for (int j = 0; j < 4 && !rc; ++j) rc = B.resolve_rho(rq[j], p, 2, fc.r[j]);
+      } else {
+        for (int a = 0; a < 3; ++a) fc.nrm[a] = side[a];
+        const Pos q[7] = {p, at({{0, -side[0]}}), at({{0, -2 * side[0]}}), at({{1, -side[1]}}),
+                          at({{1, -2 * side[1]}}), at({{2, -side[2]}}), at({{2, -2 * side[2]}})};
+        for (int j = 0; j < 7 && !rc; ++j) rc = B.resolve_u(q[j], 0, fc.u[j]);
+        const Pos rq[6] = {at({{2, -side[2]}}), at({{1, -side[1]}}), at({{0, -side[0]}}),
+                           at({{2, -2 * side[2]}}), at({{1, -2 * side[1]}}), at({{0, -2 * side[0]}})};
+        for (int j = 0; j < 6 && !rc; ++j) rc = B.resolve_rho(rq[j], p, 3, fc.r[j]);
+      }
+      if (rc) return rc;
+    }
+  }
+  const long long ncore_owned = nblk * n3;
+  // every index the kernels derive
+  const long long nrows = static_cast<long long>(cells.size());
+  for (const FdCell& fc : cells) {
+    if (fc.slot < 0 || fc.slot >= ncore_owned) return fail(ctx, OCTLB_EINVAL, "internal: fd slot");
+    for (const FdURead& u : fc.u) {
+      if (u.code == kFdFluid && (u.idx < 0 || u.idx >= ncore_owned)) return fail(ctx, OCTLB_EINVAL, "internal: fd u");
+      if (u.code == kFdPrescribed && (u.idx < 0 || u.idx >= nrows)) return fail(ctx, OCTLB_EINVAL, "internal: fd u");
+    }
+    for (int j = 0; j < (fc.role == 2 ? 4 : fc.role == 3 ? 6 : 0); ++j) {
+      const FdRRead& r = fc.r[j];
+      const bool pre = r.code == kFdRhoSumPre || r.code == kFdRhoBmPre;
+      const bool nw = r.code == kFdRhoSumNew || r.code == kFdRhoBmNew;
+      if ((pre && (r.idx < 0 || r.idx >= ncore_owned)) || (nw && (r.idx < 0 || r.idx >= nrows)))
+        return fail(ctx, OCTLB_EINVAL, "internal: fd density read");
+      if ((r.code == kFdRhoBmPre || r.code == kFdRhoBmNew) && (r.urow < 0 || r.urow >= nrows || r.d < 0 || r.d > 2))
+        return fail(ctx, OCTLB_EINVAL, "internal: fd density read");
+    }
+  }
+  lists.clear();
+  first.assign(4, 0);
+  count.assign(4, 0);
+  for (int rl = 1; rl <= 3; ++rl) {
+    first[rl] = static_cast<int>(lists.size());
+    for (size_t r = 0; r < cells.size(); ++r)
+      if (cells[r].role == rl) lists.push_back(static_cast<int>(r));
+    count[rl] = static_cast<int>(lists.size()) - first[rl];
+  }
+  return OCTLB_OK;
+}
+
+}  // namespace octlb_host
+
+extern "C" {
+
+int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* u_wall, const double* rho_target,
+                              const double* inlet_u, double ramp_end_t) {
+  if (!ctx || !types || !u_wall || !rho_target) return OCTLB_EINVAL;
+  if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
+  for (int c : ctx->counters_collide)
+    if (c != 0) return fail(ctx, OCTLB_ESTATE, "set_fd_boundary comes before the first advance");
+  if (ctx->fd_on) return fail(ctx, OCTLB_ESTATE, "fd boundary already set");
+  if (ctx->max_level != 0)
+    return fail(ctx, OCTLB_EINVAL, "fd boundary: single-level meshes at forest level 0 (one step per advance_one)");
+  if (ctx->stream_mode != OCTLB_STREAM_ROTATE || ctx->periodic || ctx->comm || ctx->const_rho)
+    return fail(ctx, OCTLB_EINVAL, "fd boundary: one context, rotate stream rule, BGK, not periodic");
+  Level& L = ctx->levels[0];
+  if (L.n_bb > 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: the tree-boundary faces must carry no restated fill");
+  std::vector<FdCell> cells;
+  std::vector<int> lists;
+  if (int rc = fd_build(ctx, ctx->n, L.blocks, ctx->kinds.data(), types, u_wall, rho_target, inlet_u, ramp_end_t,
+                        cells, lists, ctx->fd_first, ctx->fd_count))
+    return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(upload(ctx->fd_cells, cells));
+  CK(upload(ctx->fd_lists, lists));
+  CK(ctx->fd_new.alloc(cells.size() * kQ * sizeof(float)));
+  CK(upload(ctx->fd_time, std::vector<double>{0.0}));
+  ctx->fd_rows = static_cast<int>(cells.size());
+  // The first step's collide of the Dirichlet cells (at time 0): the stored
+  // initial state holds them uncollided (the initial collide takes kBulk
+  // cells only).
+  const float omega = static_cast<float>(ctx->omega_l[0]);
+  const cudaError_t e =
+      ctx->precision == OCTLB_FP32
+          ? launch_fd_collide<float>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, ctx->fd_cells.as<FdCell>(),
+                                     ctx->fd_rows, nullptr, ctx->fd_time.as<double>(), 0.0, omega, ctx->stream)
+          : launch_fd_collide<__half>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, ctx->fd_cells.as<FdCell>(),
+                                      ctx->fd_rows, nullptr, ctx->fd_time.as<double>(), 0.0, omega, ctx->stream);
+  CK(e);
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->fd_on = true;
+  clear_graphs(ctx);  // the captured launch sequence changes
+  return OCTLB_OK;
+}
+
+int octlb_fd_plan(const octlb_tables* t, const int types[6], const double* u_wall, const double* rho_target,
+                  const double* inlet_u, double ramp_end_t, void* records, int max_records) {
+  if (!t || !types || !u_wall || !rho_target || t->n_blocks < 1) return OCTLB_EINVAL;
+  std::vector<int> blocks(t->n_blocks);
+  for (int b = 0; b < t->n_blocks; ++b) {
+    if (t->levels[b] != 0) return OCTLB_EINVAL;
+    blocks[b] = b;
+  }
+  octlb_ctx ctx;
+  std::vector<FdCell> cells;
+  std::vector<int> lists, first, count;
+  if (int rc = fd_build(&ctx, t->n, blocks, t->kinds, types, u_wall, rho_target, inlet_u, ramp_end_t, cells, lists,
+                        first, count))
+    return rc;
+  if (records)
+    std::memcpy(records, cells.data(), sizeof(FdCell) * std::min<size_t>(cells.size(), max_records));
+  return static_cast<int>(cells.size());
+}
+
+int octlb_fd_record_bytes(void) { return static_cast<int>(sizeof(FdCell)); }
+
+}  // extern "C"

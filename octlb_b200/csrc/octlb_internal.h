@@ -143,4 +143,37 @@ struct DragItem {
   int pad;
 };
 
+// Finite-difference domain boundary pass (lbm_fd.cu): one record per
+// velocity- or pressure-Dirichlet cell (its row), with every read of its
+// stencil resolved on the host.  Velocity reads: kFdZero (the overlap padding
+// at rest), kFdFluid (idx = slot: the velocity of the populations there),
+// kFdPrescribed (idx = row: that boundary cell's prescribed velocity); flip
+// bit a negates component a (a mirror image across face a).  Density reads:
+// kFdRhoConst (val), 1 + sum f of the populations before the pass (idx =
+// slot) or of a rewritten row (idx = row), or velocityBMRho of either with
+// face (d, o) and the prescribed velocity of row urow.
+enum : int { kFdZero = 0, kFdFluid = 1, kFdPrescribed = 2 };
+enum : int { kFdRhoConst = 0, kFdRhoSumPre = 1, kFdRhoSumNew = 2, kFdRhoBmPre = 3, kFdRhoBmNew = 4 };
+struct FdURead {
+  long long idx;
+  int code, flip;
+};
+struct FdRRead {
+  long long idx;
+  float val;
+  int code, urow, d, o;
+};
+struct FdCell {
+  long long slot;
+  int kind, role;             // role 1 plane, 2 edge, 3 corner (faces of its block it lies on)
+  int d, o;                   // plane: the face's axis and side (-1 / +1)
+  int ax[3];                  // edge: the edge's own axis, then the two normal axes d1, d2
+  int nrm[3];                 // edge: sides along d1, d2; corner: sides along x, y, z
+  float u_base[3];            // prescribed velocity before the inlet ramp
+  float ramp_end;             // inlet ramp length in steps (0: no ramp)
+  float rho_target;           // pressure plane cell: the face's target density
+  FdURead u[7];               // velocity reads (order fixed per role, lbm_fd.cu)
+  FdRRead r[6];               // density reads (edges 4, corners 6)
+};
+
 }  // namespace octlb_gpu

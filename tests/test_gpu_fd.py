@@ -1,0 +1,92 @@
+"""Finite-difference domain boundary conditions on the GPU
+(octlb_gpu_set_fd_boundary) against the reference's own
+ConcreteDomainBoundaryHandler in the reference TimeLoop (oracle/_ref,
+oracle.Sim.set_fd_boundary): the fields after N steps, FP32 <= 1e-5 relative
+(max |gpu - ref| / max |ref| over all cells), FP16-shifted <= 2e-3.
+
+* cavity3d's boundary: InterpolatedVelocity on every face, the y+ face's
+  wall velocity on the interior lid cells (one 16^3 block);
+* a channel: a uniform inlet on x- ramped over 20 steps, a pressure outlet
+  on x+ (target density 1), velocity walls elsewhere;
+* eight 8^3 blocks (the roles of a block's rim cells come from its own
+  extents, as in the reference);
+* a rest state stays exactly at rest."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+S = oracle.Sim
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def run_pair(ob, ref, mesh, init, omega, types, u, rho_t, steps, prec, inlet=None, ramp=0.0):
+    stamped = ob.stamp_fd_kinds(mesh, types)
+    lat = ob.GpuLattice(stamped, omega, precision=prec, init_pops=init)
+    lat.set_fd_boundary(types, u, rho_t, inlet, ramp)
+    lat.advance(steps)
+    rho_g, u_g = lat.get_fields()
+    lat.close()
+    sim = S(ref, mesh, omega, init)
+    sim.set_fd_boundary(types, u, rho_target=rho_t, inlet_u=inlet, ramp_end_t=ramp)
+    sim.advance(steps)
+    rho_r, u_r = oracle.rho_u(sim.core())
+    return rho_g, u_g, rho_r, u_r
+
+
+@pytest.mark.parametrize("prec,tol", [("fp32", 1e-5), ("fp16", 2e-3)])
+def test_cavity3d_boundary(ob, ref, prec, tol):
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=16, n=16, lid=0.0, tau=0.6)
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    rho_g, u_g, rho_r, u_r = run_pair(ob, ref, mesh, init, info["omega"], [S.INTERPOLATED_VELOCITY] * 6, u,
+                                      np.ones(6), 60, ob.FP32 if prec == "fp32" else ob.FP16_SHIFTED)
+    print(f"fd cavity {prec}: u {rel(u_g, u_r):.2e} rho {rel(rho_g, rho_r):.2e}")
+    assert np.abs(u_r).max() > 0.01
+    assert rel(u_g, u_r) <= tol and rel(rho_g, rho_r) <= tol
+
+
+def test_inlet_and_pressure_outlet(ob, ref):
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=16, n=16, lid=0.0, tau=0.6)
+    types = [S.INTERPOLATED_VELOCITY, S.INTERPOLATED_PRESSURE] + [S.INTERPOLATED_VELOCITY] * 4
+    inlet = np.zeros((6, 3))
+    inlet[0, 0] = 0.02
+    rho_g, u_g, rho_r, u_r = run_pair(ob, ref, mesh, init, info["omega"], types, np.zeros((6, 3)), np.ones(6), 40,
+                                      ob.FP32, inlet, 20.0)
+    print(f"fd channel: u {rel(u_g, u_r):.2e} rho {rel(rho_g, rho_r):.2e}")
+    assert np.abs(u_r).max() > 0.005
+    assert rel(u_g, u_r) <= 1e-5 and rel(rho_g, rho_r) <= 1e-5
+
+
+def test_eight_blocks(ob, ref):
+    sys.path.insert(0, HERE)
+    from test_const_rho import brick_cavity
+    mesh, info = brick_cavity(lid=0.0, n=8)
+    init = np.zeros((mesh.n_blocks, 8, 8, 8, 19))
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    rho_g, u_g, rho_r, u_r = run_pair(ob, ref, mesh, init, info["omega"], [S.INTERPOLATED_VELOCITY] * 6, u,
+                                      np.ones(6), 30, ob.FP32)
+    print(f"fd 8 blocks: u {rel(u_g, u_r):.2e} rho {rel(rho_g, rho_r):.2e}")
+    assert rel(u_g, u_r) <= 1e-5 and rel(rho_g, rho_r) <= 1e-5
+
+
+def test_rest_state_is_a_fixed_point(ob):
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=16, n=16, lid=0.0, tau=0.6)
+    types = [S.INTERPOLATED_VELOCITY] * 6
+    lat = ob.GpuLattice(ob.stamp_fd_kinds(mesh, types), info["omega"], init_pops=init)
+    lat.set_fd_boundary(types)
+    lat.advance(10)
+    assert np.abs(lat.get_populations()).max() == 0.0
+    lat.close()
