@@ -4,8 +4,9 @@ stored as golden vectors by tests/golden/make_long_reference.py:
 * C1 cavity 32^3, 1,000 cell steps: final rho, u (plain FP32 <= 1e-5
   relative in rho and u);
 * C2 two-level AMR cavity, 625 coarse steps (5,000 base-level steps): the
-  FP64 mass audit per coarse step (the reference's own mass drift) and the
-  centreline velocity profiles;
+  FP64 mass audit per coarse step (the reference's own mass drift), the
+  centreline velocity profiles, and the field-wide L2 of u over a regular
+  lattice of 1 in 8 cells of every block;
 * C3 three-level cylinder, 2,500 coarse steps (20,000 finest steps): the
   momentum-exchange force after every coarse step; FP16-shifted storage keeps
   the time-averaged drag within 1e-3 of the FP64 run.
@@ -72,6 +73,14 @@ def test_c2_amr_mass_drift_and_centrelines(ob, prec, tol_mass, tol_line):
         assert np.array_equal(lines[k + "_pos"], g[k + "_pos"])
         l2 = float(np.sqrt(np.sum((lines[k] - g[k]) ** 2) / np.sum(g[k] ** 2)))
         assert l2 <= tol_line, (k, l2)
+    # the field-wide L2 of u on every cell of even local indices (1 in 8,
+    # every block of both levels), and sum |u|^2 over all cells
+    lat = (slice(None), slice(0, None, 2), slice(0, None, 2), slice(0, None, 2))
+    ur = g["lattice_u"].astype(np.float64)
+    l2 = float(np.sqrt(np.sum((u[lat] - ur) ** 2) / np.sum(ur ** 2)))
+    print(f"c2 {prec}: field L2(u) {l2:.2e}")
+    assert l2 <= tol_line, l2
+    assert abs(float(np.sum(u * u)) - float(g["sum_u2"])) <= 2 * tol_line * float(g["sum_u2"])
 
 
 @pytest.mark.parametrize("prec,tol,tol_hist", [("fp32", 2e-4, 1e-4), ("fp16", 1e-3, 5e-3)])
