@@ -236,6 +236,39 @@ k_fd_collide(T* state, long long qs, float scale, float inv_s, const FdCell* cel
 
 __global__ void k_fd_tick(double* time) { *time += 1.0; }
 
+// The Dirichlet cells' populations before their collide (the initial state)
+// into their rows: what the reference holds for them after a step.
+template <typename T>
+__global__ void __launch_bounds__(kFdThreads)
+k_fd_rows_from_state(const T* state, long long qs, float inv_s, const FdCell* cells, int n, float* fnew) {
+  const int row = blockIdx.x * kFdThreads + threadIdx.x;
+  if (row >= n) return;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i)
+    fnew[static_cast<long long>(row) * kQ + i] = Store<T>::ld(state + i * qs + cells[row].slot, inv_s);
+}
+
+// rho and u of the Dirichlet cells from their rows (the populations after the
+// pass, before the next collide -- the reference's state after the step),
+// over the fields the gather wrote from the stored (collided) state.
+__global__ void __launch_bounds__(kFdThreads)
+k_fd_fields(const FdCell* cells, int n, const float* fnew, double* rho, double* u) {
+  const int row = blockIdx.x * kFdThreads + threadIdx.x;
+  if (row >= n) return;
+  double dr = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const double v = fnew[static_cast<long long>(row) * kQ + i];
+    dr += v; jx += cx(i) * v; jy += cy(i) * v; jz += cz(i) * v;
+  }
+  const double r = 1.0 + dr;
+  const long long s = cells[row].slot;
+  rho[s] = r;
+  u[3 * s] = jx / r;
+  u[3 * s + 1] = jy / r;
+  u[3 * s + 2] = jz / r;
+}
+
 inline unsigned fd_grid(int n) { return static_cast<unsigned>((n + kFdThreads - 1) / kFdThreads); }
 
 }  // namespace
@@ -259,6 +292,20 @@ cudaError_t launch_fd_collide(void* state, long long qs, float scale, float inv_
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t launch_fd_rows_from_state(const void* state, long long qs, float inv_s, const FdCell* cells, int n,
+                                     float* fnew, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_fd_rows_from_state<T><<<fd_grid(n), kFdThreads, 0, s>>>(static_cast<const T*>(state), qs, inv_s, cells, n, fnew);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fd_fields(const FdCell* cells, int n, const float* fnew, double* rho, double* u, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_fd_fields<<<fd_grid(n), kFdThreads, 0, s>>>(cells, n, fnew, rho, u);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fd_tick(double* time, cudaStream_t s) {
   k_fd_tick<<<1, 1, 0, s>>>(time);
   return cudaGetLastError();
@@ -269,6 +316,10 @@ cudaError_t launch_fd_tick(double* time, cudaStream_t s) {
                                                 float*, const double*, float, cudaStream_t);                \
   template cudaError_t launch_fd_collide<T>(void*, long long, float, float, const FdCell*, int, const float*,  \
                                             const double*, double, float, cudaStream_t);
+template cudaError_t launch_fd_rows_from_state<float>(const void*, long long, float, const FdCell*, int, float*,
+                                                     cudaStream_t);
+template cudaError_t launch_fd_rows_from_state<__half>(const void*, long long, float, const FdCell*, int, float*,
+                                                      cudaStream_t);
 OCTLB_FD_INST(float)
 OCTLB_FD_INST(__half)
 

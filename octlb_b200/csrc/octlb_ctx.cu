@@ -1868,6 +1868,8 @@ int gather_impl(octlb_ctx* ctx, double* pops, double* rho, double* u) {
     StepArgs a = L.args;
     a.src = L.buf[L.cur].p;
     CK(launch_gather<T>(a, d.as<double>(), du.as<double>(), mode, ctx->stream));
+    if (mode == 1)  // the FD pass's Dirichlet cells: the fields of their rewritten rows
+      if (int rc = fd_fix_fields(ctx, L, d.as<double>(), du.as<double>())) return rc;
     const bool direct = contiguous(L);
     const long long off = static_cast<long long>(L.blocks[0]) * n3;
     std::vector<double> h0, h1;

@@ -23,6 +23,9 @@ template <typename T>
 cudaError_t launch_fd_collide(void*, long long, float, float, const FdCell*, int, const float*, const double*,
                               double, float, cudaStream_t);
 cudaError_t launch_fd_tick(double*, cudaStream_t);
+template <typename T>
+cudaError_t launch_fd_rows_from_state(const void*, long long, float, const FdCell*, int, float*, cudaStream_t);
+cudaError_t launch_fd_fields(const FdCell*, int, const float*, double*, double*, cudaStream_t);
 }  // namespace octlb_gpu
 
 using namespace octlb_gpu;
@@ -163,6 +166,14 @@ int fd_after_step(octlb_ctx* ctx, Level& L) {
 }
 template int fd_after_step<float>(octlb_ctx*, Level&);
 template int fd_after_step<__half>(octlb_ctx*, Level&);
+
+// get_fields: the Dirichlet cells' rho and u from their rows (level L's
+// staging arrays, indexed by local core slot).
+int fd_fix_fields(octlb_ctx* ctx, Level& L, double* rho, double* u) {
+  if (!ctx->fd_on || L.nblk == 0) return OCTLB_OK;
+  CK(launch_fd_fields(ctx->fd_cells.as<FdCell>(), ctx->fd_rows, ctx->fd_new.as<float>(), rho, u, ctx->stream));
+  return OCTLB_OK;
+}
 
 int fd_end_of_step(octlb_ctx* ctx) {
   if (!ctx->fd_on) return OCTLB_OK;
@@ -373,15 +384,21 @@ int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* 
   ctx->fd_rows = static_cast<int>(cells.size());
   // The first step's collide of the Dirichlet cells (at time 0): the stored
   // initial state holds them uncollided (the initial collide takes kBulk
-  // cells only).
+  // cells only); their rows keep that state (the fields before any step).
   const float omega = static_cast<float>(ctx->omega_l[0]);
-  const cudaError_t e =
-      ctx->precision == OCTLB_FP32
-          ? launch_fd_collide<float>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, ctx->fd_cells.as<FdCell>(),
-                                     ctx->fd_rows, nullptr, ctx->fd_time.as<double>(), 0.0, omega, ctx->stream)
-          : launch_fd_collide<__half>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, ctx->fd_cells.as<FdCell>(),
-                                      ctx->fd_rows, nullptr, ctx->fd_time.as<double>(), 0.0, omega, ctx->stream);
-  CK(e);
+  const FdCell* dc = ctx->fd_cells.as<FdCell>();
+  float* rows = ctx->fd_new.as<float>();
+  const double* tm = ctx->fd_time.as<double>();
+  if (ctx->precision == OCTLB_FP32) {
+    CK(launch_fd_rows_from_state<float>(L.buf[L.cur].p, L.nslots, L.inv_scale, dc, ctx->fd_rows, rows, ctx->stream));
+    CK(launch_fd_collide<float>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, dc, ctx->fd_rows, rows, tm, 0.0,
+                                omega, ctx->stream));
+  } else {
+    CK(launch_fd_rows_from_state<__half>(L.buf[L.cur].p, L.nslots, L.inv_scale, dc, ctx->fd_rows, rows,
+                                         ctx->stream));
+    CK(launch_fd_collide<__half>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, dc, ctx->fd_rows, rows, tm, 0.0,
+                                 omega, ctx->stream));
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->fd_on = true;
   clear_graphs(ctx);  // the captured launch sequence changes
