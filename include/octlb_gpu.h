@@ -170,8 +170,11 @@ int octlb_gpu_average_rho(octlb_ctx* ctx, double* out);
  * u_wall of the y+ face on the interior top-face cells (cavity3d's lid);
  * pressure cells hold rho_target[face].  The cells must carry their kinds in
  * the tables (octlb_fd_stamp_kinds), the faces no restated fill
- * (OCTLB_TB_NONE).  One context, the rotate stream rule, BGK, one level at
- * forest level 0, blocks of n >= 4; before the first advance. */
+ * (OCTLB_TB_NONE).  One context, the rotate stream rule, one level at
+ * forest level 0, blocks of n >= 4; before the first advance.  With
+ * ConstRhoBGK (octlb_gpu_set_const_rho, called first) the velocity cells'
+ * collide densities join the average's statistics, as the reference's
+ * kFluidAndBoundary scope does (cavity3d's configuration). */
 #define OCTLB_FD_VELOCITY 2
 #define OCTLB_FD_PRESSURE 4
 int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double u_wall[18],

@@ -85,6 +85,7 @@ struct FdCtx {
   const FdCell* cells;
   const float* fnew;  // [rows][19]
   float t;
+  const double* cr_avg;  // ConstRhoBGK: the average density the step's collide used, or null
 };
 
 template <typename T>
@@ -116,7 +117,13 @@ __device__ __forceinline__ float read_rho(const FdCtx<T>& c, const FdRRead& r) {
 #pragma unroll
     for (int i = 0; i < kQ; ++i) f[i] = c.fnew[r.idx * kQ + i];
   }
-  if (r.code == kFdRhoSumPre || r.code == kFdRhoSumNew) return 1.f + sum_pops(f);
+  if (r.code == kFdRhoSumPre || r.code == kFdRhoSumNew) {
+    // a kBulk cell's stored density under ConstRhoBGK carries the 1 -
+    // average_rho its collide added (urow = 1 marks a kBulk cell)
+    const float shift = (r.code == kFdRhoSumPre && r.urow == 1 && c.cr_avg) ? static_cast<float>(1.0 - *c.cr_avg)
+                                                                             : 0.f;
+    return 1.f + sum_pops(f) - shift;
+  }
   float u[3];
   prescribed(c.cells, r.urow, c.t, u);
   return bm_rho(f, r.d, r.o, u);
@@ -136,12 +143,12 @@ __device__ __forceinline__ void normal_grad(const float u0[3], const float u1[3]
 template <typename T>
 __global__ void __launch_bounds__(kFdThreads)
 k_fd_reconstruct(const T* state, long long qs, float inv_s, const FdCell* cells, const int* list, int n,
-                 float* fnew, const double* time, float omega) {
+                 float* fnew, const double* time, float omega, const double* cr_avg) {
   const int k = blockIdx.x * kFdThreads + threadIdx.x;
   if (k >= n) return;
   const int row = list[k];
   const FdCell& cell = cells[row];
-  FdCtx<T> c{state, qs, inv_s, cells, fnew, static_cast<float>(*time)};
+  FdCtx<T> c{state, qs, inv_s, cells, fnew, static_cast<float>(*time), cr_avg};
   float uu[7][3];
 #pragma unroll
   for (int j = 0; j < 7; ++j) read_u(c, cell.u[j], uu[j]);
@@ -211,9 +218,10 @@ k_fd_reconstruct(const T* state, long long qs, float inv_s, const FdCell* cells,
 template <typename T>
 __global__ void __launch_bounds__(kFdThreads)
 k_fd_collide(T* state, long long qs, float scale, float inv_s, const FdCell* cells, int n, const float* fnew,
-             const double* time, double time_shift, float omega) {
+             const double* time, double time_shift, float omega, double* cr_part) {
   const int row = blockIdx.x * kFdThreads + threadIdx.x;
-  if (row >= n) return;
+  double stat = 0.0;  // ConstRhoBGK statistics: the velocity cell's collide density
+  if (row < n) {
   const FdCell& cell = cells[row];
   float f[kQ];
   if (fnew) {
@@ -226,12 +234,25 @@ k_fd_collide(T* state, long long qs, float scale, float inv_s, const FdCell* cel
     float u[3];
     prescribed(cells, row, static_cast<float>(*time + time_shift), u);
     const float rho = cell.role == 1 ? bm_rho(f, cell.d, cell.o, u) : 1.f + sum_pops(f);
+    stat = rho;
     const float usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
 #pragma unroll
     for (int i = 0; i < kQ; ++i) f[i] = f[i] * (1.f - omega) + omega * feq_i(i, rho, u, usq);
   }
 #pragma unroll
   for (int i = 0; i < kQ; ++i) Store<T>::st(state + i * qs + cell.slot, f[i], scale);
+  }
+  if (cr_part) {  // this CTA's sum, in a fixed order
+    for (int o = 16; o > 0; o >>= 1) stat += __shfl_down_sync(0xffffffffu, stat, o);
+    __shared__ double ws[kFdThreads / 32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = stat;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sum = 0.0;
+      for (int w = 0; w < kFdThreads / 32; ++w) sum += ws[w];
+      cr_part[blockIdx.x] = sum;
+    }
+  }
 }
 
 __global__ void k_fd_tick(double* time) { *time += 1.0; }
@@ -273,22 +294,29 @@ inline unsigned fd_grid(int n) { return static_cast<unsigned>((n + kFdThreads - 
 
 }  // namespace
 
+unsigned fd_collide_parts(int n) { return fd_grid(n); }
+
+namespace {
+
+}  // namespace
+
 template <typename T>
 cudaError_t launch_fd_reconstruct(const void* state, long long qs, float inv_s, const FdCell* cells, const int* list,
-                                  int n, float* fnew, const double* time, float omega, cudaStream_t s) {
+                                  int n, float* fnew, const double* time, float omega, const double* cr_avg,
+                                  cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   k_fd_reconstruct<T><<<fd_grid(n), kFdThreads, 0, s>>>(static_cast<const T*>(state), qs, inv_s, cells, list, n,
-                                                         fnew, time, omega);
+                                                         fnew, time, omega, cr_avg);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_fd_collide(void* state, long long qs, float scale, float inv_s, const FdCell* cells, int n,
-                              const float* fnew, const double* time, double time_shift, float omega,
+                              const float* fnew, const double* time, double time_shift, float omega, double* cr_part,
                               cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   k_fd_collide<T><<<fd_grid(n), kFdThreads, 0, s>>>(static_cast<T*>(state), qs, scale, inv_s, cells, n, fnew, time,
-                                                     time_shift, omega);
+                                                     time_shift, omega, cr_part);
   return cudaGetLastError();
 }
 
@@ -313,9 +341,9 @@ cudaError_t launch_fd_tick(double* time, cudaStream_t s) {
 
 #define OCTLB_FD_INST(T)                                                                                      \
   template cudaError_t launch_fd_reconstruct<T>(const void*, long long, float, const FdCell*, const int*, int, \
-                                                float*, const double*, float, cudaStream_t);                \
+                                                float*, const double*, float, const double*, cudaStream_t); \
   template cudaError_t launch_fd_collide<T>(void*, long long, float, float, const FdCell*, int, const float*,  \
-                                            const double*, double, float, cudaStream_t);
+                                            const double*, double, float, double*, cudaStream_t);
 template cudaError_t launch_fd_rows_from_state<float>(const void*, long long, float, const FdCell*, int, float*,
                                                      cudaStream_t);
 template cudaError_t launch_fd_rows_from_state<__half>(const void*, long long, float, const FdCell*, int, float*,

@@ -934,13 +934,23 @@ __global__ void __launch_bounds__(kThreads) k_cr_seed(const StepArgs a, int near
 // rho + (1 - average_rho) with the average that collide used, so the mean
 // over `count` kBulk cells is 2 - average_rho + sum(rho - 1) / count (1 when
 // there are none).  The partials are summed in a fixed order.
+// With the finite-difference boundary pass (kFluidAndBoundary scope) the
+// velocity-Dirichlet cells' collide densities join the statistics:
+// (sum(rho - 1) + count (2 - average_rho) + sum rho_b) / (count + count_b).
 __global__ void __launch_bounds__(kThreads)
-k_cr_update(double* avg, const double* part, int nparts, long long count) {
+k_cr_update(double* avg, const double* part, int nparts, long long count, const double* bpart, int nbparts,
+            long long bcount) {
   pdl_wait();
-  double v[1] = {0.0};
+  double v[2] = {0.0, 0.0};
   for (int p = threadIdx.x; p < nparts; p += kThreads) v[0] += part[p];
-  block_reduce<1>(v);
-  if (threadIdx.x == 0) *avg = count > 0 ? (2.0 - *avg) + v[0] / static_cast<double>(count) : 1.0;
+  for (int p = threadIdx.x; p < nbparts; p += kThreads) v[1] += bpart[p];
+  block_reduce<2>(v);
+  if (threadIdx.x == 0) {
+    if (bcount == 0)
+      *avg = count > 0 ? (2.0 - *avg) + v[0] / static_cast<double>(count) : 1.0;
+    else
+      *avg = (v[0] + static_cast<double>(count) * (2.0 - *avg) + v[1]) / static_cast<double>(count + bcount);
+  }
 }
 
 inline uint32_t grid_for(uint32_t items) { return (items + kThreads - 1) / kThreads; }
@@ -1138,8 +1148,10 @@ cudaError_t launch_cr_seed(const StepArgs& a, int near_parts, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_cr_update(double* avg, const double* part, int nparts, long long count, cudaStream_t s) {
-  const cudaError_t e = launch_chain(k_cr_update, dim3(1), dim3(kThreads), 0, s, avg, part, nparts, count);
+cudaError_t launch_cr_update(double* avg, const double* part, int nparts, long long count, const double* bpart,
+                             int nbparts, long long bcount, cudaStream_t s) {
+  const cudaError_t e = launch_chain(k_cr_update, dim3(1), dim3(kThreads), 0, s, avg, part, nparts, count, bpart,
+                                     nbparts, bcount);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 

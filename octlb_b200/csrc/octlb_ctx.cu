@@ -143,7 +143,7 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     // ConstRhoBGK: average_rho from the last collide's statistics
     // (time_loop.h:220-222), then the step whose collide uses it
     CK(launch_cr_update(ctx->cr_avg.as<double>(), ctx->cr_part.as<double>(), ctx->cr_nparts, ctx->cr_count,
-                        ctx->stream));
+                        ctx->fd_cr_part.as<double>(), ctx->fd_cr_parts, ctx->fd_vel, ctx->stream));
     const bool links = ctx->stream_mode == OCTLB_STREAM_LINKS;
     if (L.use_map && ctx->map_global && ctx->map_cells == (links ? 1 : 2)) {
       CK(launch_step_map_cr<T>(a, L.near, links, L.has_flags, ctx->stream));
@@ -2128,7 +2128,8 @@ int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on) {
   if (!ctx) return OCTLB_EINVAL;
   if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
   if (ctx->comm && on) return fail(ctx, OCTLB_EINVAL, "ConstRhoBGK is built for one context, not rank contexts");
-  if (ctx->fd_on && on) return fail(ctx, OCTLB_EINVAL, "ConstRhoBGK with the fd boundary pass is not built");
+  if (ctx->fd_on && on)
+    return fail(ctx, OCTLB_ESTATE, "ConstRhoBGK is chosen before octlb_gpu_set_fd_boundary");
   for (int c : ctx->counters_collide)
     if (c != 0) return fail(ctx, OCTLB_ESTATE, "ConstRhoBGK is chosen before the first advance");
   if ((on != 0) == ctx->const_rho) return OCTLB_OK;

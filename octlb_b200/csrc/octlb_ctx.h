@@ -38,7 +38,7 @@ cudaError_t launch_step_cr(const StepArgs&, const NearTables&, bool, bool, cudaS
 template <typename T> cudaError_t launch_cr_seed(const StepArgs&, int, cudaStream_t);
 template <typename T>
 cudaError_t launch_step_map_cr(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
-cudaError_t launch_cr_update(double*, const double*, int, long long, cudaStream_t);
+cudaError_t launch_cr_update(double*, const double*, int, long long, const double*, int, long long, cudaStream_t);
 uint32_t cr_core_parts(const StepArgs& a);
 uint32_t cr_near_parts(const NearTables& nt);
 template <typename T> cudaError_t launch_step_bulk(const StepArgs&, int, cudaStream_t);
@@ -339,6 +339,11 @@ struct octlb_ctx {
   bool fd_on = false;
   DevBuf fd_cells, fd_lists, fd_new, fd_time;
   int fd_rows = 0;
+  // ConstRhoBGK with the pass: per-CTA sums of the velocity cells' collide
+  // densities (the boundary part of the statistics), over fd_vel cells
+  DevBuf fd_cr_part;
+  int fd_cr_parts = 0;
+  long long fd_vel = 0;
   std::vector<int> fd_first, fd_count;
   bool owns(int b) const { return owner.empty() || owner[b] == rank; }
   // Host-only planning of a rank context (octlb_gpu_plan_part): the exchange

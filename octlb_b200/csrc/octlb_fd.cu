@@ -18,10 +18,11 @@
 namespace octlb_gpu {
 template <typename T>
 cudaError_t launch_fd_reconstruct(const void*, long long, float, const FdCell*, const int*, int, float*,
-                                  const double*, float, cudaStream_t);
+                                  const double*, float, const double*, cudaStream_t);
 template <typename T>
 cudaError_t launch_fd_collide(void*, long long, float, float, const FdCell*, int, const float*, const double*,
-                              double, float, cudaStream_t);
+                              double, float, double*, cudaStream_t);
+unsigned fd_collide_parts(int n);
 cudaError_t launch_fd_tick(double*, cudaStream_t);
 template <typename T>
 cudaError_t launch_fd_rows_from_state(const void*, long long, float, const FdCell*, int, float*, cudaStream_t);
@@ -132,7 +133,8 @@ struct Builder {
     if (k == kVelocityDirichlet && d >= 0) {
       out = {fresh ? row : slot(p), 0.f, fresh ? kFdRhoBmNew : kFdRhoBmPre, row, d, o};
     } else {
-      out = {fresh ? row : slot(p), 0.f, fresh ? kFdRhoSumNew : kFdRhoSumPre, 0, 0, 0};
+      // urow = 1 marks a kBulk cell (its stored density carries ConstRhoBGK's shift)
+      out = {fresh ? row : slot(p), 0.f, fresh ? kFdRhoSumNew : kFdRhoSumPre, k == kBulk && !fresh ? 1 : 0, 0, 0};
     }
     return OCTLB_OK;
   }
@@ -156,11 +158,12 @@ int fd_after_step(octlb_ctx* ctx, Level& L) {
     const int n = ctx->fd_count[role];
     if (n == 0) continue;
     CK(launch_fd_reconstruct<T>(state, L.nslots, L.inv_scale, cells, ctx->fd_lists.as<int>() + ctx->fd_first[role],
-                                n, fnew, time, omega, ctx->stream));
+                                n, fnew, time, omega, ctx->const_rho ? ctx->cr_avg.as<double>() : nullptr,
+                                ctx->stream));
     ++ctx->launch_count;
   }
   CK(launch_fd_collide<T>(state, L.nslots, L.scale, L.inv_scale, cells, ctx->fd_rows, fnew, time, 1.0, omega,
-                          ctx->stream));
+                          ctx->const_rho ? ctx->fd_cr_part.as<double>() : nullptr, ctx->stream));
   ++ctx->launch_count;
   return OCTLB_OK;
 }
@@ -367,8 +370,8 @@ int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* 
   if (ctx->fd_on) return fail(ctx, OCTLB_ESTATE, "fd boundary already set");
   if (ctx->max_level != 0)
     return fail(ctx, OCTLB_EINVAL, "fd boundary: single-level meshes at forest level 0 (one step per advance_one)");
-  if (ctx->stream_mode != OCTLB_STREAM_ROTATE || ctx->periodic || ctx->comm || ctx->const_rho)
-    return fail(ctx, OCTLB_EINVAL, "fd boundary: one context, rotate stream rule, BGK, not periodic");
+  if (ctx->stream_mode != OCTLB_STREAM_ROTATE || ctx->periodic || ctx->comm)
+    return fail(ctx, OCTLB_EINVAL, "fd boundary: one context, rotate stream rule, not periodic");
   Level& L = ctx->levels[0];
   if (L.n_bb > 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: the tree-boundary faces must carry no restated fill");
   std::vector<FdCell> cells;
@@ -382,6 +385,16 @@ int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* 
   CK(ctx->fd_new.alloc(cells.size() * kQ * sizeof(float)));
   CK(upload(ctx->fd_time, std::vector<double>{0.0}));
   ctx->fd_rows = static_cast<int>(cells.size());
+  // ConstRhoBGK (chosen before): the velocity cells' collide densities join
+  // its statistics (the reference's kFluidAndBoundary scope)
+  double* crp = nullptr;
+  if (ctx->const_rho) {
+    ctx->fd_vel = 0;
+    for (const FdCell& fc : cells) ctx->fd_vel += fc.kind == kVelocityDirichlet ? 1 : 0;
+    ctx->fd_cr_parts = static_cast<int>(fd_collide_parts(ctx->fd_rows));
+    CK(ctx->fd_cr_part.alloc(static_cast<size_t>(ctx->fd_cr_parts) * sizeof(double)));
+    crp = ctx->fd_cr_part.as<double>();
+  }
   // The first step's collide of the Dirichlet cells (at time 0): the stored
   // initial state holds them uncollided (the initial collide takes kBulk
   // cells only); their rows keep that state (the fields before any step).
@@ -392,12 +405,12 @@ int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* 
   if (ctx->precision == OCTLB_FP32) {
     CK(launch_fd_rows_from_state<float>(L.buf[L.cur].p, L.nslots, L.inv_scale, dc, ctx->fd_rows, rows, ctx->stream));
     CK(launch_fd_collide<float>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, dc, ctx->fd_rows, rows, tm, 0.0,
-                                omega, ctx->stream));
+                                omega, crp, ctx->stream));
   } else {
     CK(launch_fd_rows_from_state<__half>(L.buf[L.cur].p, L.nslots, L.inv_scale, dc, ctx->fd_rows, rows,
                                          ctx->stream));
     CK(launch_fd_collide<__half>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, dc, ctx->fd_rows, rows, tm, 0.0,
-                                 omega, ctx->stream));
+                                 omega, crp, ctx->stream));
   }
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->fd_on = true;

@@ -90,3 +90,41 @@ def test_rest_state_is_a_fixed_point(ob):
     lat.advance(10)
     assert np.abs(lat.get_populations()).max() == 0.0
     lat.close()
+
+
+@pytest.mark.parametrize("blocks", [1, 8])
+def test_const_rho_with_fd_walls(ob, ref, blocks):
+    """cavity3d's configuration: ConstRhoBGK in the bulk with the FD walls
+    and lid, the velocity cells' collide densities in the average's
+    statistics (kFluidAndBoundary): fields and average_rho after every few
+    steps against the reference TimeLoop built with use_const_rho_bgk around
+    the reference's handler.  Eight blocks also exercise the stencils'
+    reads of kBulk densities, which carry the collide's 1 - average_rho."""
+    from octlb_b200 import cases
+    if blocks == 1:
+        mesh, init, info = cases.cavity_forest(cells=16, n=16, lid=0.0, tau=0.6)
+        omega = info["omega"]
+    else:
+        sys.path.insert(0, HERE)
+        from test_const_rho import brick_cavity
+        mesh, info = brick_cavity(lid=0.0, n=8)
+        init = np.zeros((mesh.n_blocks, 8, 8, 8, 19))
+        omega = info["omega"]
+    types = [S.INTERPOLATED_VELOCITY] * 6
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    lat = ob.GpuLattice(ob.stamp_fd_kinds(mesh, types), omega, init_pops=init)
+    lat.set_const_rho(True)
+    lat.set_fd_boundary(types, u)
+    sim = S(ref, mesh, omega, init)
+    sim.set_fd_boundary(types, u, const_rho=True)
+    for _ in range(4):
+        lat.advance(10)
+        sim.advance(10)
+        rho_g, u_g = lat.get_fields()
+        rho_r, u_r = oracle.rho_u(sim.core())
+        eu, er = rel(u_g, u_r), rel(rho_g, rho_r)
+        da = abs(lat.average_rho() - sim.average_rho())
+        print(f"fd const rho ({blocks} blocks): u {eu:.2e} rho {er:.2e} average_rho {da:.2e}")
+        assert eu <= 1e-5 and er <= 1e-5 and da <= 1e-6
+    lat.close()
