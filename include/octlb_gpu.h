@@ -158,8 +158,10 @@ int octlb_gpu_average_rho(octlb_ctx* ctx, double* out);
  * The reference's ConcreteDomainBoundaryHandler (domain_boundary_handler.cpp:
  * 55-89) on the tree-boundary faces, types as DomainBcType
  * (domain_boundary_handler.h:16-22): 2 InterpolatedVelocity, 4
- * InterpolatedPressure (the two finite-difference conditions; the other
- * types are not built on the device).  Every step, after the pull and the
+ * InterpolatedPressure (the finite-difference conditions), 0 no-slip (its
+ * kBounceBack cells take the dispatcher's full-way swap at collide,
+ * bc_dispatcher.h:55-67), 1 moving lid and 3 outflow (kinds with no
+ * collide-time action there, streamed as they are).  Every step, after the pull and the
  * collide of the fluid cells, the velocity- and pressure-Dirichlet cells are
  * rebuilt from the finite-difference stencil of Skordos' method (plane, edge
  * and corner cells by their block's extents, in the reference's walk order,
@@ -175,7 +177,10 @@ int octlb_gpu_average_rho(octlb_ctx* ctx, double* out);
  * ConstRhoBGK (octlb_gpu_set_const_rho, called first) the velocity cells'
  * collide densities join the average's statistics, as the reference's
  * kFluidAndBoundary scope does (cavity3d's configuration). */
+#define OCTLB_FD_NO_SLIP 0
+#define OCTLB_FD_MOVING_LID 1
 #define OCTLB_FD_VELOCITY 2
+#define OCTLB_FD_OUTFLOW 3
 #define OCTLB_FD_PRESSURE 4
 int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double u_wall[18],
                               const double rho_target[6], const double* inlet_u /* [18] or NULL */,

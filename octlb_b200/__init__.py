@@ -226,7 +226,7 @@ def vtk_write_index(output_dir, base_name, step, vts_relative_paths):
         raise OctlbError(rc, "vtk_write_index failed")
 
 
-FD_VELOCITY, FD_PRESSURE = 2, 4
+FD_NO_SLIP, FD_MOVING_LID, FD_VELOCITY, FD_OUTFLOW, FD_PRESSURE = 0, 1, 2, 3, 4
 
 
 def stamp_fd_kinds(mesh, types):

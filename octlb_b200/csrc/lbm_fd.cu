@@ -210,21 +210,35 @@ k_fd_reconstruct(const T* state, long long qs, float inv_s, const FdCell* cells,
   }
 }
 
-// The Dirichlet collide of the boundary cells into the state buffer: velocity
-// cells f (1 - omega) + omega feq(rho, u_presc(t)), rho = velocityBMRho on
-// plane cells and 1 + sum f on edges and corners; pressure cells unchanged.
+// The collide of the boundary cells into the state buffer: velocity cells
+// f (1 - omega) + omega feq(rho, u_presc(t)), rho = velocityBMRho on plane
+// cells and 1 + sum f on edges and corners; bounce-back cells the full-way
+// swap; pressure cells unchanged.
 // Source: the rewritten rows (after the pass) or the state itself (the
 // initial state, before the first step).
 template <typename T>
 __global__ void __launch_bounds__(kFdThreads)
-k_fd_collide(T* state, long long qs, float scale, float inv_s, const FdCell* cells, int n, const float* fnew,
+k_fd_collide(T* state, long long qs, float scale, float inv_s, const FdCell* cells, int n, float* fnew,
              const double* time, double time_shift, float omega, double* cr_part) {
   const int row = blockIdx.x * kFdThreads + threadIdx.x;
   double stat = 0.0;  // ConstRhoBGK statistics: the velocity cell's collide density
   if (row < n) {
   const FdCell& cell = cells[row];
   float f[kQ];
-  if (fnew) {
+  if (cell.role == 0) {
+    // a bounce-back cell (the dispatcher's kBounceBack arm, bc_dispatcher.h:
+    // 55-67): its streamed populations are its row (the state after the
+    // step), then the full-way swap f_i <- f_opp(i)
+    load_pops(state, qs, cell.slot, inv_s, f);
+    float g[kQ];
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      if (fnew) fnew[static_cast<long long>(row) * kQ + i] = f[i];
+      g[i] = f[i];
+    }
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) f[i] = g[opp(i)];
+  } else if (fnew) {
 #pragma unroll
     for (int i = 0; i < kQ; ++i) f[i] = fnew[static_cast<long long>(row) * kQ + i];
   } else {
@@ -312,7 +326,7 @@ cudaError_t launch_fd_reconstruct(const void* state, long long qs, float inv_s, 
 
 template <typename T>
 cudaError_t launch_fd_collide(void* state, long long qs, float scale, float inv_s, const FdCell* cells, int n,
-                              const float* fnew, const double* time, double time_shift, float omega, double* cr_part,
+                              float* fnew, const double* time, double time_shift, float omega, double* cr_part,
                               cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   k_fd_collide<T><<<fd_grid(n), kFdThreads, 0, s>>>(static_cast<T*>(state), qs, scale, inv_s, cells, n, fnew, time,
@@ -342,7 +356,7 @@ cudaError_t launch_fd_tick(double* time, cudaStream_t s) {
 #define OCTLB_FD_INST(T)                                                                                      \
   template cudaError_t launch_fd_reconstruct<T>(const void*, long long, float, const FdCell*, const int*, int, \
                                                 float*, const double*, float, const double*, cudaStream_t); \
-  template cudaError_t launch_fd_collide<T>(void*, long long, float, float, const FdCell*, int, const float*,  \
+  template cudaError_t launch_fd_collide<T>(void*, long long, float, float, const FdCell*, int, float*,        \
                                             const double*, double, float, double*, cudaStream_t);
 template cudaError_t launch_fd_rows_from_state<float>(const void*, long long, float, const FdCell*, int, float*,
                                                      cudaStream_t);

@@ -20,7 +20,7 @@ template <typename T>
 cudaError_t launch_fd_reconstruct(const void*, long long, float, const FdCell*, const int*, int, float*,
                                   const double*, float, const double*, cudaStream_t);
 template <typename T>
-cudaError_t launch_fd_collide(void*, long long, float, float, const FdCell*, int, const float*, const double*,
+cudaError_t launch_fd_collide(void*, long long, float, float, const FdCell*, int, float*, const double*,
                               double, float, double*, cudaStream_t);
 unsigned fd_collide_parts(int n);
 cudaError_t launch_fd_tick(double*, cudaStream_t);
@@ -125,7 +125,7 @@ struct Builder {
     }
     const int row = (*row_of)[cell(p)];
     bool fresh = false;
-    if (row >= 0 && p < reader) {
+    if (row >= 0 && (*role_of)[row] >= 1 && p < reader) {  // a cell the pass rewrites
       const int pr = (*role_of)[row];
       if (pr == reader_role) return fail(ctx, OCTLB_EINVAL, "fd boundary: blocks of n >= 4 only");
       fresh = pr < reader_role;
@@ -228,8 +228,7 @@ int fd_build(octlb_ctx* ctx, int n, const std::vector<int>& blocks, const uint8_
              const double* u_wall, const double* rho_target, const double* inlet_u, double ramp_end_t,
              std::vector<FdCell>& cells, std::vector<int>& lists, std::vector<int>& first, std::vector<int>& count) {
   for (int f = 0; f < 6; ++f)
-    if (types[f] != 2 && types[f] != 4)
-      return fail(ctx, OCTLB_EINVAL, "fd boundary: faces take InterpolatedVelocity (2) or InterpolatedPressure (4)");
+    if (types[f] < 0 || types[f] > 4) return fail(ctx, OCTLB_EINVAL, "fd boundary: face type outside 0..4");
   if (n < 4) return fail(ctx, OCTLB_EINVAL, "fd boundary: blocks of n >= 4 only");
   const long long n3 = static_cast<long long>(n) * n * n;
   const int nblk = static_cast<int>(blocks.size());
@@ -239,7 +238,7 @@ int fd_build(octlb_ctx* ctx, int n, const std::vector<int>& blocks, const uint8_
   for (int lb = 0; lb < nblk; ++lb) {
     const uint8_t* kb = kinds + static_cast<size_t>(blocks[lb]) * n3;
     for (long long c = 0; c < n3; ++c)
-      if (kb[c] == kVelocityDirichlet || kb[c] == kPressureDirichlet) {
+      if (kb[c] == kVelocityDirichlet || kb[c] == kPressureDirichlet || kb[c] == kBounceBack) {
         row_of[lb][c] = static_cast<int>(cells.size());
         FdCell fc{};
         fc.slot = lb * n3 + c;
@@ -247,7 +246,7 @@ int fd_build(octlb_ctx* ctx, int n, const std::vector<int>& blocks, const uint8_
         cells.push_back(fc);
       }
   }
-  if (cells.empty()) return fail(ctx, OCTLB_EINVAL, "fd boundary: no velocity or pressure Dirichlet cells");
+  if (cells.empty()) return fail(ctx, OCTLB_EINVAL, "fd boundary: no Dirichlet or bounce-back cells");
   std::vector<int> role(cells.size());
   for (int lb = 0; lb < nblk; ++lb)
     for (long long c = 0; c < n3; ++c) {
@@ -256,7 +255,8 @@ int fd_build(octlb_ctx* ctx, int n, const std::vector<int>& blocks, const uint8_
       const int x = static_cast<int>(c / (n * n)), y = static_cast<int>((c / n) % n), z = static_cast<int>(c % n);
       int cnt = 0;
       for (int v : {x, y, z}) cnt += (v == 0 || v == n - 1) ? 1 : 0;
-      if (cnt == 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: a Dirichlet cell off its block's faces");
+      if (cells[r].kind == kBounceBack) cnt = 0;  // no reconstruction: the collide's full-way swap only
+      else if (cnt == 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: a Dirichlet cell off its block's faces");
       role[r] = cnt;
     }
   for (int lb = 0; lb < nblk; ++lb) {
@@ -267,6 +267,7 @@ int fd_build(octlb_ctx* ctx, int n, const std::vector<int>& blocks, const uint8_
       FdCell& fc = cells[r];
       const Pos p{static_cast<int>(c / (n * n)), static_cast<int>((c / n) % n), static_cast<int>(c % n)};
       fc.role = role[r];
+      if (fc.role == 0) continue;
       // prescribed velocity
       const bool on[6] = {p.x == 0, p.x == n - 1, p.y == 0, p.y == n - 1, p.z == 0, p.z == n - 1};
       bool done = false;

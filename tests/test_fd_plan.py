@@ -185,3 +185,16 @@ def test_eight_blocks_roles_from_block_extents(ob):
     u = np.zeros((6, 3))
     u[3, 0] = 0.05
     check(ob, mesh, [ob.FD_VELOCITY] * 6, u, np.ones(6))
+
+
+def test_no_slip_walls_and_lid(ob):
+    """No-slip faces (kBounceBack: the collide's full-way swap, no
+    reconstruction) around an InterpolatedVelocity lid: the lid's edge and
+    corner cells read bounce-back neighbours as plain cells."""
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=16, n=16, lid=0.0, tau=0.6)
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    types = [ob.FD_NO_SLIP] * 3 + [ob.FD_VELOCITY] + [ob.FD_NO_SLIP] * 2
+    rec = check(ob, mesh, types, u, np.ones(6))
+    assert np.any(rec["role"] == 0) and np.any(rec["role"] >= 1)

@@ -128,3 +128,20 @@ def test_const_rho_with_fd_walls(ob, ref, blocks):
         print(f"fd const rho ({blocks} blocks): u {eu:.2e} rho {er:.2e} average_rho {da:.2e}")
         assert eu <= 1e-5 and er <= 1e-5 and da <= 1e-6
     lat.close()
+
+
+def test_no_slip_walls_and_moving_lid_types(ob, ref):
+    """The handler's other domain types: no-slip walls (kBounceBack, the
+    dispatcher's full-way swap at collide) on five faces and an
+    InterpolatedVelocity lid; then the lid as a moving-lid face (no
+    collide-time action) over outflow side faces."""
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=16, n=16, lid=0.0, tau=0.6)
+    u = np.zeros((6, 3))
+    u[3, 0] = 0.05
+    for types in ([S.NO_SLIP] * 3 + [S.INTERPOLATED_VELOCITY] + [S.NO_SLIP] * 2,
+                  [S.OUTFLOW, S.OUTFLOW, S.NO_SLIP, S.MOVING_LID, S.INTERPOLATED_VELOCITY,
+                   S.INTERPOLATED_VELOCITY]):
+        rho_g, u_g, rho_r, u_r = run_pair(ob, ref, mesh, init, info["omega"], types, u, np.ones(6), 30, ob.FP32)
+        print(f"fd types {types}: u {rel(u_g, u_r):.2e} rho {rel(rho_g, rho_r):.2e}")
+        assert rel(u_g, u_r) <= 1e-5 and rel(rho_g, rho_r) <= 1e-5
