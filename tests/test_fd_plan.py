@@ -149,7 +149,7 @@ def check(ob, mesh, types, u_wall, rho_target, inlet=None, ramp=0.0, t=0.0, seed
                               inlets=inlets, t=t)
         got = fpre[b].copy().reshape(-1, 19)
         sl = rec["slot"]
-        mine = (sl // n ** 3) == b
+        mine = ((sl // n ** 3) == b) & (rec["role"] >= 1)  # role 0: bounce-back, not rewritten
         got[sl[mine] % n ** 3] = new[mine]
         worst = max(worst, float(np.abs(got.reshape(want.shape) - want).max()))
     assert worst <= 1e-8, worst
