@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(1024) k_step_bulk(const StepArgs a) {
       const uint32_t zs = cz(i) == 1 ? zm : (cz(i) == -1 ? zp : z);
       f[i] = Store<T>::ld(S + i * n + zs, 1.0f);
     }
-    bgk(f, a.omega, a.scale, a.inv_scale);  // storage units h = s (f - w)
+    bgk<kBgkCorrect<T>>(f, a.omega, a.scale, a.inv_scale);  // storage units h = s (f - w)
     const uint32_t row = blockIdx.x + k * gridDim.x;
     T* o = dst + static_cast<long long>(row) * n + z;
 #pragma unroll

@@ -124,8 +124,39 @@ __device__ __forceinline__ void moments(const float (&f)[kQ], float& drho, float
 //   c0 = s (rho - 1) - 1.5 A |u|^2,
 // which has no cancellation against w_i and keeps the scale out of the
 // per-population work.  The relaxation is applied to the small difference,
-// f + omega fma(w_i, t, -f), never as (1 - omega) f + omega feq, whose two
+// d_i = omega fma(w_i, t, -f), never as (1 - omega) f + omega feq, whose two
 // large terms cancel.  Arithmetic is FP32.
+//
+// In exact arithmetic sum d_i = 0 and sum c_i d_i = 0 (the collide keeps mass
+// and momentum); in FP32 the rounded equilibrium leaves a defect of about
+// 1e-9 per cell and step that does not average out (it follows the smooth
+// local state) and, over a thousand steps, drifts u by ~1e-5 relative against
+// FP64.  The defect (e_0 = sum d_i, e = sum c_i d_i, summed in a fixed order)
+// is removed along the conserved directions, f_i -= w_i (e_0 + 3 c_i . e),
+// which cuts that drift by an order of magnitude at ~2 FP32 ops per
+// population.  cx/cy/cz are +-1 or 0, so every product with them is exact; the
+// explicit round-to-nearest intrinsics keep the sequence free of contraction,
+// so bgk() and the lane form bgk_lane() round identically.  FP16-shifted
+// storage rounds each population to 11 bits every step, far above this
+// defect, so its kernels skip the removal (CORRECT = false).
+struct BgkDefect {
+  float e0, ex, ey, ez;
+};
+__device__ __forceinline__ void defect_add(BgkDefect& e, float d, int ix, int iy, int iz) {
+  e.e0 = __fadd_rn(e.e0, d);
+  if (ix) e.ex = ix > 0 ? __fadd_rn(e.ex, d) : __fsub_rn(e.ex, d);
+  if (iy) e.ey = iy > 0 ? __fadd_rn(e.ey, d) : __fsub_rn(e.ey, d);
+  if (iz) e.ez = iz > 0 ? __fadd_rn(e.ez, d) : __fsub_rn(e.ez, d);
+}
+// f - w (e0 + 3 c . e) for direction (ix, iy, iz) of weight w
+__device__ __forceinline__ float defect_remove(const BgkDefect& e, float f, float w, int ix, int iy, int iz) {
+  float ce = 0.f;
+  if (ix) ce = ix > 0 ? __fadd_rn(ce, e.ex) : __fsub_rn(ce, e.ex);
+  if (iy) ce = iy > 0 ? __fadd_rn(ce, e.ey) : __fsub_rn(ce, e.ey);
+  if (iz) ce = iz > 0 ? __fadd_rn(ce, e.ez) : __fsub_rn(ce, e.ez);
+  return fmaf(-w, fmaf(3.0f, ce, e.e0), f);
+}
+template <bool CORRECT = true>
 __device__ __forceinline__ void bgk(float (&f)[kQ], float omega, float s = 1.0f, float inv_s = 1.0f) {
   float dh, jx, jy, jz;
   moments(f, dh, jx, jy, jz);
@@ -135,13 +166,27 @@ __device__ __forceinline__ void bgk(float (&f)[kQ], float omega, float s = 1.0f,
   const float A = s * rho;
   const float a3 = 3.0f * A, b45 = 4.5f * A;
   const float c0 = dh - 1.5f * A * (ux * ux + uy * uy + uz * uz);
+  BgkDefect e{0.f, 0.f, 0.f, 0.f};
 #pragma unroll
   for (int i = 0; i < kQ; ++i) {
     const float cu = (cx(i) ? cx(i) * ux : 0.f) + (cy(i) ? cy(i) * uy : 0.f) + (cz(i) ? cz(i) * uz : 0.f);
     const float t = i == 0 ? c0 : fmaf(cu, fmaf(b45, cu, a3), c0);
-    f[i] = fmaf(omega, fmaf(wf(i), t, -f[i]), f[i]);
+    if constexpr (CORRECT) {
+      const float d = __fmul_rn(omega, fmaf(wf(i), t, -f[i]));
+      defect_add(e, d, cx(i), cy(i), cz(i));
+      f[i] = __fadd_rn(f[i], d);
+    } else {
+      f[i] = fmaf(omega, fmaf(wf(i), t, -f[i]), f[i]);
+    }
+  }
+  if constexpr (CORRECT) {
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) f[i] = defect_remove(e, f[i], wf(i), cx(i), cy(i), cz(i));
   }
 }
+// The removal for FP32 storage, not for FP16-shifted.
+template <typename T> constexpr bool kBgkCorrect = true;
+template <> constexpr bool kBgkCorrect<__half> = false;
 
 // ConstRhoBGK (OpenLB collision::ConstRhoBGK as block_lattice.h:134-151
 // restates it, unit scale):

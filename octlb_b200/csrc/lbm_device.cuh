@@ -144,6 +144,7 @@ __device__ __forceinline__ void gather_lanes(float v, float (&all)[kQ]) {
 
 // BGK (unit scale) of population i = lane from the gathered pre-collision
 // populations: the same operations and rounding as bgk() for direction i.
+template <bool CORRECT = true>
 __device__ __forceinline__ float bgk_lane(const LaneDir& d, int lane, const float (&fa)[kQ], float f, float omega) {
   float dh, jx, jy, jz;
   moments(fa, dh, jx, jy, jz);
@@ -155,7 +156,20 @@ __device__ __forceinline__ float bgk_lane(const LaneDir& d, int lane, const floa
   const float c0 = dh - 1.5f * A * (ux * ux + uy * uy + uz * uz);
   const float cu = (d.cx != 0.f ? d.cx * ux : 0.f) + (d.cy != 0.f ? d.cy * uy : 0.f) + (d.cz != 0.f ? d.cz * uz : 0.f);
   const float t = lane == 0 ? c0 : fmaf(cu, fmaf(b45, cu, a3), c0);
-  return fmaf(omega, fmaf(d.w, t, -f), f);
+  if constexpr (!CORRECT) return fmaf(omega, fmaf(d.w, t, -f), f);
+  // the collide's defect over all 19 directions, in bgk()'s order (every lane
+  // holds the cell's populations fa), so the lane's result is bgk()'s
+  BgkDefect e{0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const float cui = (cx(i) ? cx(i) * ux : 0.f) + (cy(i) ? cy(i) * uy : 0.f) + (cz(i) ? cz(i) * uz : 0.f);
+    const float ti = i == 0 ? c0 : fmaf(cui, fmaf(b45, cui, a3), c0);
+    defect_add(e, __fmul_rn(omega, fmaf(wf(i), ti, -fa[i])), cx(i), cy(i), cz(i));
+  }
+  const float g = __fadd_rn(f, __fmul_rn(omega, fmaf(d.w, t, -f)));
+  const int ix = d.cx > 0.f ? 1 : (d.cx < 0.f ? -1 : 0), iy = d.cy > 0.f ? 1 : (d.cy < 0.f ? -1 : 0),
+            iz = d.cz > 0.f ? 1 : (d.cz < 0.f ? -1 : 0);
+  return defect_remove(e, g, d.w, ix, iy, iz);
 }
 
 // ConstRhoBGK of population i = lane (the arithmetic of bgk_const_rho for
@@ -200,6 +214,7 @@ __device__ inline void read_macro(const float* f, Macro& m) {
 // feq(rho,u) + scale * f_neq (WriteProlongation, level_coupler.cpp:191-201),
 // then BGK if the target cell is kBulk: the written state is collided by the
 // next step of its level before it is streamed.
+template <bool CORRECT = true>
 __device__ inline void write_macro_cell(const Macro& m, float s, int kind, float omega, float (&f)[kQ]) {
   const float rho = 1.0f + m.drho;
   const float usq15 = 1.5f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
@@ -208,7 +223,7 @@ __device__ inline void write_macro_cell(const Macro& m, float s, int kind, float
     const float cu = cx(i) * m.ux + cy(i) * m.uy + cz(i) * m.uz;
     f[i] = wf(i) * (m.drho + rho * (3.0f * cu + 4.5f * cu * cu - usq15)) + s * m.fneq[i];
   }
-  if (kind == kBulk) bgk(f, omega);
+  if (kind == kBulk) bgk<CORRECT>(f, omega);
 }
 
 // FP64 block reduction of N doubles: warp shuffles, then one warp over the

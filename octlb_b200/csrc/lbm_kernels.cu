@@ -139,7 +139,7 @@ __device__ __forceinline__ float core_cell(const StepArgs& a, uint32_t t, const 
   }
   if (bulk) {
     if constexpr (CR) dh = bgk_const_rho(f, a.omega, dr);
-    else bgk(f, a.omega);
+    else bgk<kBgkCorrect<T>>(f, a.omega);
   }
 #pragma unroll
   for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + t, f[i], a.scale);
@@ -227,7 +227,7 @@ __device__ __forceinline__ float near_cell(const StepArgs& a, const NearTables& 
     float fa[kQ];
     gather_lanes(f, fa);
     if constexpr (CR) f = bgk_lane_const_rho(d, lane, fa, f, a.omega, dr, dh);
-    else f = bgk_lane(d, lane, fa, f, a.omega);
+    else f = bgk_lane<kBgkCorrect<T>>(d, lane, fa, f, a.omega);
   }
   if (d.act) Store<T>::st(dst + lane * a.qs + t, f, a.scale);
   return dh;
@@ -313,7 +313,7 @@ __device__ __forceinline__ float map_cell_finish(const StepArgs& a, uint32_t t, 
   }
   if (bulk) {
     if constexpr (CR) dh = bgk_const_rho(f, a.omega, dr);
-    else bgk(f, a.omega);
+    else bgk<kBgkCorrect<T>>(f, a.omega);
   }
   const uint32_t qs = static_cast<uint32_t>(a.qs);
 #pragma unroll
@@ -462,8 +462,8 @@ __global__ void __launch_bounds__(kThreads) k_step_pair(const StepArgs a) {
     }
   }
   // populations stay in storage units h = s (f - w); the scale lives in bgk
-  bgk(f0, a.omega, a.scale, a.inv_scale);
-  bgk(f1, a.omega, a.scale, a.inv_scale);
+  bgk<kBgkCorrect<T>>(f0, a.omega, a.scale, a.inv_scale);
+  bgk<kBgkCorrect<T>>(f1, a.omega, a.scale, a.inv_scale);
   T* o = dst + static_cast<long long>(row) * n + z;
 #pragma unroll
   for (int i = 0; i < kQ; ++i) Pair<T>::st(o + i * a.qs, f0[i], f1[i], a.scale);
@@ -522,10 +522,10 @@ __global__ void __launch_bounds__(kThreads) k_step_quad_h(const StepArgs a) {
       f3[i] = __half2float(r[zp4]);
     }
   }
-  bgk(f0, a.omega, a.scale, a.inv_scale);
-  bgk(f1, a.omega, a.scale, a.inv_scale);
-  bgk(f2, a.omega, a.scale, a.inv_scale);
-  bgk(f3, a.omega, a.scale, a.inv_scale);
+  bgk<false>(f0, a.omega, a.scale, a.inv_scale);
+  bgk<false>(f1, a.omega, a.scale, a.inv_scale);
+  bgk<false>(f2, a.omega, a.scale, a.inv_scale);
+  bgk<false>(f3, a.omega, a.scale, a.inv_scale);
   __half* o = dst + static_cast<long long>(row) * n + z;
 #pragma unroll
   for (int i = 0; i < kQ; ++i) st4h(o + i * a.qs, f0[i], f1[i], f2[i], f3[i]);
@@ -612,7 +612,7 @@ __device__ __forceinline__ void prolong_warp(const ProlongOp& op, int w, int lan
   float f = d.w * (wd + wrho * (3.0f * wcu + 4.5f * wcu * wcu - wusq15)) + scale * wn;
   if (it.fine_kind == kBulk) {
     gather_lanes(f, fa);
-    f = bgk_lane(d, lane, fa, f, omega);
+    f = bgk_lane<kBgkCorrect<T>>(d, lane, fa, f, omega);
   }
   if (d.act) Store<T>::st(static_cast<T*>(op.fine) + lane * op.fine_qs + it.fine_slot, f, op.fscale);
 }
@@ -652,7 +652,7 @@ __device__ __forceinline__ void restrict_warp(const RestrictOp& op, int w, int l
   if (it.coarse_kind == kBulk) {
     float fa[kQ];
     gather_lanes(f, fa);
-    f = bgk_lane(d, lane, fa, f, omega);
+    f = bgk_lane<kBgkCorrect<T>>(d, lane, fa, f, omega);
   }
   if (d.act) Store<T>::st(static_cast<T*>(op.coarse) + lane * op.coarse_qs + it.coarse_slot, f, op.cscale);
 }
@@ -845,7 +845,7 @@ k_scatter(const StepArgs a, const double* in, int near_parts) {
     const int kind = a.flags ? (a.flags[slot] & kKindMask) : kBulk;
     if (kind == kBulk) {
       if (a.cr_avg) v[0] = bgk_const_rho(f, a.omega, static_cast<float>(1.0 - *a.cr_avg));
-      else bgk(f, a.omega);
+      else bgk<kBgkCorrect<T>>(f, a.omega);
     }
     T* dst = static_cast<T*>(a.dst);
 #pragma unroll
@@ -893,7 +893,7 @@ k_scatter_eq(const StepArgs a, const double* in, int near_parts) {
     const int kind = a.flags ? (a.flags[slot] & kKindMask) : kBulk;
     if (kind == kBulk) {
       if (a.cr_avg) v[0] = bgk_const_rho(f, a.omega, static_cast<float>(1.0 - *a.cr_avg));
-      else bgk(f, a.omega);
+      else bgk<kBgkCorrect<T>>(f, a.omega);
     }
     T* dst = static_cast<T*>(a.dst);
 #pragma unroll
