@@ -348,6 +348,9 @@ def forest_measurements(ob, cases, torch, peak):
         # per-launch latency
         "cylinder_512x128x128": (lambda: cases.cylinder_forest(length=512, height=128, diameter=32.0,
                                                                center=(128.0, 64.0)), ob.STREAM_LINKS, True),
+        # the 256x64x64 channel on 16^3 blocks: an eighth of the blocks, fewer
+        # shell cells per block, a finest level that covers more of the box
+        "cylinder_256x64x64_n16": (lambda: cases.cylinder_forest(n=16), ob.STREAM_LINKS, True),
         # single-level 128^3 cavity (the reference's cavity3d collision),
         # ConstRhoBGK; BGK on the same mesh beside it
         "const_rho_cavity_128": (lambda: cases.cavity_forest(cells=128, n=8, lid=0.05, tau=0.56),
@@ -374,8 +377,12 @@ def forest_measurements(ob, cases, torch, peak):
             ms = e0.elapsed_time(e1) / K
             launches, lups = lat.step_stats()
             bpl = 76 if pn == "fp16" else 152
+            # both population buffers of every block core (halo pages aside):
+            # below the 126 MB L2 the step's bytes need not reach HBM at all
+            cells = int(mesh.n_blocks) * int(mesh.n) ** 3
             r[pn] = {"mlups": lups / ms / 1e3, "ms_per_step": ms, "launches_per_step": int(launches),
-                     "hbm_frac": bpl * lups / (ms * 1e-3) / 1e9 / peak}
+                     "hbm_frac": bpl * lups / (ms * 1e-3) / 1e9 / peak,
+                     "lattice_mb": 2 * cells * 19 * (2 if pn == "fp16" else 4) / 1e6}
             if name == "cylinder_256x64x64":
                 g = np.load(os.path.join(here, "tests", "golden", "long_c3_cylinder.npz"))["force"]
                 lat.close()

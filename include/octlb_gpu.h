@@ -141,11 +141,13 @@ int octlb_gpu_set_body_force(octlb_ctx* ctx, const double* force);
  * block_lattice.h:134-151; statistics time_loop.h:201-222).  Every kBulk
  * cell collides with ratio_rho = 1 + (1 - average_rho) / rho, and after each
  * step average_rho becomes the mean of rho + (1 - average_rho) over the kBulk
- * cells of that collide (the reference starts at 1).  Before the first
- * advance only (OCTLB_ESTATE after it), on single-level meshes (OCTLB_EINVAL
- * otherwise: the stored state is one collide ahead of the reference's, so a
- * coarse level would need the average of finest steps that have not run).
- * The adjoint refuses a ConstRhoBGK context.  get_fields returns the
+ * cells of that collide (the reference starts at 1).  On a multi-level mesh
+ * the statistics are the finest level's and every level collides at the
+ * average: the levels above the finest then stream in their step and collide
+ * after their coupling (one launch more per level step; a prolongation into
+ * the finest level takes its target's collide and statistic).  Before the
+ * first advance only (OCTLB_ESTATE after it); one context, not rank contexts
+ * (OCTLB_EINVAL).  The adjoint refuses a ConstRhoBGK context.  get_fields returns the
  * reference's post-stream rho (the stored post-collision state minus the
  * 1 - average_rho the collide added to each kBulk cell; u is unchanged). */
 int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on);

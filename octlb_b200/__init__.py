@@ -484,7 +484,8 @@ class GpuLattice:
 
     def set_const_rho(self, on=True):
         """ConstRhoBGK (TimeLoop's use_const_rho_bgk): before the first
-        advance, on a single-level mesh."""
+        advance; on a multi-level mesh the finest level's statistics set the
+        average density every level collides at."""
         self._check(self._L.octlb_gpu_set_const_rho(self._h, 1 if on else 0))
 
     def average_rho(self):

@@ -46,7 +46,13 @@ enum : uint8_t {
                         // with a halo source, or a link record)
   kFlagLink = 0x10,     // core cell with a link record (q / moving-wall term)
   kFlagSave = 0x20,     // save pre-collision populations (coupler source)
+  kFlagProlong = 0x40,  // written by a prolongation before it is next read: the
+                        // collide a step gives it is replaced, so its ConstRhoBGK
+                        // statistic is the prolongation's
 };
+// Collide of a step launch: BGK, ConstRhoBGK at *cr_avg with per-CTA
+// statistics, or none (the populations stored as pulled).
+enum : int { kCollBgk = 0, kCollConstRho = 1, kCollNone = 2 };
 
 __host__ __device__ inline bool reflects_on_pull(int k) {
   // BcKindReflectsOnPull (bc_kind.h:30-33)
@@ -133,12 +139,17 @@ __device__ __forceinline__ void moments(const float (&f)[kQ], float& drho, float
 // local state) and, over a thousand steps, drifts u by ~1e-5 relative against
 // FP64.  The defect (e_0 = sum d_i, e = sum c_i d_i, summed in a fixed order)
 // is removed along the conserved directions, f_i -= w_i (e_0 + 3 c_i . e),
-// which cuts that drift by an order of magnitude at ~2 FP32 ops per
-// population.  cx/cy/cz are +-1 or 0, so every product with them is exact; the
-// explicit round-to-nearest intrinsics keep the sequence free of contraction,
-// so bgk() and the lane form bgk_lane() round identically.  FP16-shifted
-// storage rounds each population to 11 bits every step, far above this
-// defect, so its kernels skip the removal (CORRECT = false).
+// which cuts that drift by two orders of magnitude (TGV 64^3, 1,000 steps:
+// u 2.1e-5 -> 2.4e-7) at ~7 FP32 ops per population.  cx/cy/cz are +-1 or 0,
+// so every product with them is exact; the explicit round-to-nearest
+// intrinsics keep the sequence free of contraction, so bgk() and the lane
+// form bgk_lane() round identically.  The kernels of the uniform periodic box
+// (k_step_pair, k_step_bulk, k_step on a flag-free periodic level) and the
+// set-populations collides remove it: HBM-bound, they hide the work (1.7 %
+// of the 256^3 step).  The forest kernels (slot map, near cells, coupler)
+// are issue-bound, where it costs 13 % of the cylinder's step, and skip it
+// (CORRECT = false), as do FP16-shifted kernels, whose 11-bit rounding of
+// every population each step lies far above this defect.
 struct BgkDefect {
   float e0, ex, ey, ez;
 };
@@ -184,7 +195,7 @@ __device__ __forceinline__ void bgk(float (&f)[kQ], float omega, float s = 1.0f,
     for (int i = 0; i < kQ; ++i) f[i] = defect_remove(e, f[i], wf(i), cx(i), cy(i), cz(i));
   }
 }
-// The removal for FP32 storage, not for FP16-shifted.
+// The removal where a kernel applies it: FP32 storage, not FP16-shifted.
 template <typename T> constexpr bool kBgkCorrect = true;
 template <> constexpr bool kBgkCorrect<__half> = false;
 

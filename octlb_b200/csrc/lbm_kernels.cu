@@ -100,9 +100,12 @@ __device__ __forceinline__ void cr_store_partial(const StepArgs& a, double v0, u
 }
 
 // One core cell of k_step / k_step_cr: pull, save, collide (kBulk cells:
-// BGK, or ConstRhoBGK with dr = 1 - average_rho when CR), store.  Returns
-// rho - 1 before the collision for a cell the ConstRhoBGK collided, else 0.
-template <typename T, bool LINKS, bool FLAGS, bool CR>
+// BGK, ConstRhoBGK with dr = 1 - average_rho, or none, by CM), store.
+// Returns rho - 1 before the collision for a cell the ConstRhoBGK collided
+// and a later prolongation does not overwrite, else 0.  CORR: the BGK
+// collide removes its own mass / momentum rounding defect (FP32 storage of
+// the uniform periodic box, as k_step_pair).
+template <typename T, bool LINKS, bool FLAGS, int CM, bool CORR = false>
 __device__ __forceinline__ float core_cell(const StepArgs& a, uint32_t t, const long long* sb, float dr) {
   const T* src = static_cast<const T*>(a.src);
   T* dst = static_cast<T*>(a.dst);
@@ -138,15 +141,21 @@ __device__ __forceinline__ float core_cell(const StepArgs& a, uint32_t t, const 
     bulk = (fl & kKindMask) == kBulk;
   }
   if (bulk) {
-    if constexpr (CR) dh = bgk_const_rho(f, a.omega, dr);
-    else bgk<kBgkCorrect<T>>(f, a.omega);
+    if constexpr (CM == kCollConstRho) {
+      dh = bgk_const_rho(f, a.omega, dr);
+      if (fl & kFlagProlong) dh = 0.f;
+    } else if constexpr (CM == kCollBgk) {
+      bgk<CORR && kBgkCorrect<T>>(f, a.omega);
+    }
   }
 #pragma unroll
   for (int i = 0; i < kQ; ++i) Store<T>::st(dst + i * a.qs + t, f[i], a.scale);
   return dh;
 }
 
-template <typename T, bool LINKS, bool FLAGS, bool BLOCKED>
+// CM: kCollBgk, or kCollNone for a level whose collide runs after its
+// coupling (k_collide_cr).
+template <typename T, bool LINKS, bool FLAGS, bool BLOCKED, int CM = kCollBgk, bool CORR = false>
 __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
   pdl_wait();
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
@@ -161,7 +170,7 @@ __global__ void __launch_bounds__(kThreads) k_step(const StepArgs a) {
       __syncthreads();
     }
     if (t >= a.ncore) return;
-    core_cell<T, LINKS, FLAGS, false>(a, t, BLOCKED ? sb : nullptr, 0.f);
+    core_cell<T, LINKS, FLAGS, CM, CORR>(a, t, BLOCKED ? sb : nullptr, 0.f);
     return;
   }
   // Halo items start at the first CTA after the core CTAs.
@@ -187,7 +196,7 @@ __global__ void __launch_bounds__(kThreads) k_step_cr(const StepArgs a) {
     }
     const float dr = static_cast<float>(1.0 - *a.cr_avg);
     float dh = 0.f;
-    if (t < a.ncore) dh = core_cell<T, LINKS, FLAGS, true>(a, t, BLOCKED ? sb : nullptr, dr);
+    if (t < a.ncore) dh = core_cell<T, LINKS, FLAGS, kCollConstRho>(a, t, BLOCKED ? sb : nullptr, dr);
     // the near-cell CTAs of k_step_near_cr write the partials after these
     cr_store_partial(a, static_cast<double>(dh), static_cast<uint32_t>(a.cr_total));
     return;
@@ -204,7 +213,7 @@ __global__ void __launch_bounds__(kThreads) k_step_cr(const StepArgs a) {
 // moving-wall term.  Then the same save / collide / store as k_step.  One
 // warp per cell, lane i on direction i; the collision gathers the 19 values
 // so every lane computes the moments exactly as bgk() does.
-template <typename T, bool CR = false>
+template <typename T, int CM = kCollBgk>
 __device__ __forceinline__ float near_cell(const StepArgs& a, const NearTables& nt, int k, int lane, float dr = 0.f) {
   if (k >= nt.n) return 0.f;
   const T* src = static_cast<const T*>(a.src);
@@ -223,19 +232,25 @@ __device__ __forceinline__ float near_cell(const StepArgs& a, const NearTables& 
   if (d.act && ((mask >> lane) & 1u)) f = (q < 1.0f ? bouzidi(own_opp, val, own, q) : own_opp) + add;
   if ((fl & kFlagSave) && d.act) a.save_buf[static_cast<long long>(a.save_idx[t]) * kQ + lane] = f;
   float dh = 0.f;
-  if ((fl & kKindMask) == kBulk) {
-    float fa[kQ];
-    gather_lanes(f, fa);
-    if constexpr (CR) f = bgk_lane_const_rho(d, lane, fa, f, a.omega, dr, dh);
-    else f = bgk_lane<kBgkCorrect<T>>(d, lane, fa, f, a.omega);
+  if constexpr (CM != kCollNone) {
+    if ((fl & kKindMask) == kBulk) {
+      float fa[kQ];
+      gather_lanes(f, fa);
+      if constexpr (CM == kCollConstRho) {
+        f = bgk_lane_const_rho(d, lane, fa, f, a.omega, dr, dh);
+        if (fl & kFlagProlong) dh = 0.f;
+      } else {
+        f = bgk_lane<false>(d, lane, fa, f, a.omega);
+      }
+    }
   }
   if (d.act) Store<T>::st(dst + lane * a.qs + t, f, a.scale);
   return dh;
 }
 
-template <typename T>
+template <typename T, int CM = kCollBgk>
 __global__ void __launch_bounds__(kThreads) k_step_near(const StepArgs a, const NearTables nt) {
-  near_cell<T>(a, nt, (blockIdx.x * kThreads + threadIdx.x) >> 5, threadIdx.x & 31);
+  near_cell<T, CM>(a, nt, (blockIdx.x * kThreads + threadIdx.x) >> 5, threadIdx.x & 31);
 }
 
 // Near-wall cells under ConstRhoBGK: one warp per cell as k_step_near; each
@@ -246,7 +261,7 @@ __global__ void __launch_bounds__(kThreads) k_step_near_cr(const StepArgs a, con
   pdl_wait();
   const float dr = static_cast<float>(1.0 - *a.cr_avg);
   const int lane = threadIdx.x & 31;
-  const float dh = near_cell<T, true>(a, nt, (blockIdx.x * kThreads + threadIdx.x) >> 5, lane, dr);
+  const float dh = near_cell<T, kCollConstRho>(a, nt, (blockIdx.x * kThreads + threadIdx.x) >> 5, lane, dr);
   double v[1] = {lane == 0 ? static_cast<double>(dh) : 0.0};
   block_reduce<1>(v);
   if (threadIdx.x == 0) a.cr_part[part_off + blockIdx.x] = v[0];
@@ -298,7 +313,7 @@ __device__ __forceinline__ bool map_cell_prologue(const StepArgs& a, uint32_t t,
   return true;
 }
 
-template <typename T, bool FLAGS, bool CR = false>
+template <typename T, bool FLAGS, int CM = kCollBgk>
 __device__ __forceinline__ float map_cell_finish(const StepArgs& a, uint32_t t, uint8_t fl, float (&f)[kQ], T* dst,
                                                  float dr = 0.f) {
   float dh = 0.f;
@@ -312,8 +327,12 @@ __device__ __forceinline__ float map_cell_finish(const StepArgs& a, uint32_t t, 
     bulk = (fl & kKindMask) == kBulk;
   }
   if (bulk) {
-    if constexpr (CR) dh = bgk_const_rho(f, a.omega, dr);
-    else bgk<kBgkCorrect<T>>(f, a.omega);
+    if constexpr (CM == kCollConstRho) {
+      dh = bgk_const_rho(f, a.omega, dr);
+      if (fl & kFlagProlong) dh = 0.f;
+    } else if constexpr (CM == kCollBgk) {
+      bgk<false>(f, a.omega);
+    }
   }
   const uint32_t qs = static_cast<uint32_t>(a.qs);
 #pragma unroll
@@ -326,24 +345,25 @@ __device__ __forceinline__ float map_cell_finish(const StepArgs& a, uint32_t t, 
 // the first CTAs of the launch take the near-wall cells (one warp each), so
 // they run beside the bulk instead of in a launch of their own.
 //
-// CR: the ConstRhoBGK collide at average density *cr_avg, and per near-cell
-// and block CTA the sum of rho - 1 over its collided kBulk cells in
-// cr_part[blockIdx.x] (the halo-item CTAs after them write none).
-template <typename T, bool LINKS, bool FLAGS, int CPT, bool GMAP, bool CR = false>
+// CM = kCollConstRho: the ConstRhoBGK collide at average density *cr_avg,
+// and per near-cell and block CTA the sum of rho - 1 over its collided kBulk
+// cells in cr_part[blockIdx.x] (the halo-item CTAs after them write none);
+// kCollNone: no collide.
+template <typename T, bool LINKS, bool FLAGS, int CPT, bool GMAP, int CM = kCollBgk>
 __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const StepArgs a, const NearTables nt) {
   extern __shared__ int smap_s[];  // (n+2)^3 slots of this block
   constexpr uint32_t kParts = CPT == 1 ? 2 : 1;
   const uint32_t near_ctas = LINKS ? (static_cast<uint32_t>(nt.n) + kThreads / 32 - 1) / (kThreads / 32) : 0;
   if (LINKS && blockIdx.x < near_ctas) {
-    if constexpr (CR) {
+    if constexpr (CM == kCollConstRho) {
       pdl_wait();
       const float dr = static_cast<float>(1.0 - *a.cr_avg);
-      const float dh = near_cell<T, true>(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)),
+      const float dh = near_cell<T, kCollConstRho>(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)),
                                           threadIdx.x & 31, dr);
       cr_store_partial(a, (threadIdx.x & 31) == 0 ? static_cast<double>(dh) : 0.0,
                        near_ctas + static_cast<uint32_t>(a.nblk) * kParts);
     } else {
-      near_cell<T>(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)), threadIdx.x & 31);
+      near_cell<T, CM>(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)), threadIdx.x & 31);
     }
     return;
   }
@@ -369,7 +389,7 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
   T* dst = static_cast<T*>(a.dst);
   const uint32_t n = a.n, n3 = n * n * n, qs = static_cast<uint32_t>(a.qs);
   const uint32_t span = n3 / kParts;
-  const float dr = CR ? static_cast<float>(1.0 - *a.cr_avg) : 0.f;
+  const float dr = CM == kCollConstRho ? static_cast<float>(1.0 - *a.cr_avg) : 0.f;
   float acc = 0.f;
   for (uint32_t tl0 = part * span + threadIdx.x; tl0 < (part + 1) * span; tl0 += CPT * kThreads) {
     uint32_t t[CPT];
@@ -415,11 +435,12 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
 #pragma unroll
     for (int c = 0; c < CPT; ++c)
       if (go[c]) {
-        if constexpr (CR) acc += map_cell_finish<T, FLAGS, true>(a, t[c], fl[c], f[c], dst, dr);
-        else map_cell_finish<T, FLAGS>(a, t[c], fl[c], f[c], dst);
+        if constexpr (CM == kCollConstRho) acc += map_cell_finish<T, FLAGS, CM>(a, t[c], fl[c], f[c], dst, dr);
+        else map_cell_finish<T, FLAGS, CM>(a, t[c], fl[c], f[c], dst);
       }
   }
-  if constexpr (CR) cr_store_partial(a, static_cast<double>(acc), near_ctas + static_cast<uint32_t>(a.nblk) * kParts);
+  if constexpr (CM == kCollConstRho)
+    cr_store_partial(a, static_cast<double>(acc), near_ctas + static_cast<uint32_t>(a.nblk) * kParts);
 }
 
 // One periodic all-kBulk block, two consecutive z cells per thread: every
@@ -557,8 +578,8 @@ __global__ void __launch_bounds__(kThreads) k_add_force(const StepArgs a, T* pop
 // lanes keep the item's dependent chain short: the launch is latency-bound
 // (a few thousand items).
 template <typename T>
-__device__ __forceinline__ void prolong_warp(const ProlongOp& op, int w, int lane) {
-  if (w >= op.n) return;  // whole warps
+__device__ __forceinline__ float prolong_warp(const ProlongOp& op, int w, int lane) {
+  if (w >= op.n) return 0.f;  // whole warps
   const ProlongItem it = op.items[w];
   const int half = op.half;
   float* rec_prev = op.rec_prev;
@@ -610,11 +631,16 @@ __device__ __forceinline__ void prolong_warp(const ProlongOp& op, int w, int lan
   const float wusq15 = 1.5f * (wx * wx + wy * wy + wz * wz);
   const float wcu = d.cx * wx + d.cy * wy + d.cz * wz;
   float f = d.w * (wd + wrho * (3.0f * wcu + 4.5f * wcu * wcu - wusq15)) + scale * wn;
-  if (it.fine_kind == kBulk) {
+  float dh = 0.f;
+  if (it.fine_kind == kBulk && op.cmode != kCollNone) {
     gather_lanes(f, fa);
-    f = bgk_lane<kBgkCorrect<T>>(d, lane, fa, f, omega);
+    if (op.cmode == kCollConstRho)
+      f = bgk_lane_const_rho(d, lane, fa, f, omega, static_cast<float>(1.0 - *op.cr_avg), dh);
+    else
+      f = bgk_lane<false>(d, lane, fa, f, omega);
   }
   if (d.act) Store<T>::st(static_cast<T*>(op.fine) + lane * op.fine_qs + it.fine_slot, f, op.fscale);
+  return dh;
 }
 
 // Lagrava restriction (level_coupler.cpp:613-654), one warp per item: lane
@@ -649,10 +675,10 @@ __device__ __forceinline__ void restrict_warp(const RestrictOp& op, int w, int l
   const float usq15 = 1.5f * (rx * rx + ry * ry + rz * rz);
   const float cu = d.cx * rx + d.cy * ry + d.cz * rz;
   float f = d.w * (rd + rho * (3.0f * cu + 4.5f * cu * cu - usq15)) + scale * rn;
-  if (it.coarse_kind == kBulk) {
+  if (it.coarse_kind == kBulk && op.cmode != kCollNone) {
     float fa[kQ];
     gather_lanes(f, fa);
-    f = bgk_lane<kBgkCorrect<T>>(d, lane, fa, f, omega);
+    f = bgk_lane<false>(d, lane, fa, f, omega);
   }
   if (d.act) Store<T>::st(static_cast<T*>(op.coarse) + lane * op.coarse_qs + it.coarse_slot, f, op.cscale);
 }
@@ -670,7 +696,12 @@ __global__ void __launch_bounds__(kThreads) k_couple(const ProlongOp p, const Re
   const int lane = threadIdx.x & 31;
   uint32_t b = blockIdx.x;
   if (b < gp) {
-    prolong_warp<T>(p, static_cast<int>((b * kThreads + threadIdx.x) >> 5), lane);
+    const float dh = prolong_warp<T>(p, static_cast<int>((b * kThreads + threadIdx.x) >> 5), lane);
+    if (p.cr_part) {  // ConstRhoBGK statistics of the collided targets (lane 0 of each item)
+      double v[1] = {lane == 0 ? static_cast<double>(dh) : 0.0};
+      block_reduce<1>(v);
+      if (threadIdx.x == 0) p.cr_part[b] = v[0];
+    }
     return;
   }
   b -= gp;
@@ -842,9 +873,9 @@ k_scatter(const StepArgs a, const double* in, int near_parts) {
     float f[kQ];
 #pragma unroll
     for (int i = 0; i < kQ; ++i) f[i] = static_cast<float>(in[static_cast<long long>(t) * kQ + i]);
-    const int kind = a.flags ? (a.flags[slot] & kKindMask) : kBulk;
-    if (kind == kBulk) {
-      if (a.cr_avg) v[0] = bgk_const_rho(f, a.omega, static_cast<float>(1.0 - *a.cr_avg));
+    const uint8_t fl = a.flags ? a.flags[slot] : static_cast<uint8_t>(kBulk);
+    if ((fl & kKindMask) == kBulk) {
+      if (a.cr_avg) v[0] = (fl & kFlagProlong) ? 0.0 : bgk_const_rho(f, a.omega, static_cast<float>(1.0 - *a.cr_avg));
       else bgk<kBgkCorrect<T>>(f, a.omega);
     }
     T* dst = static_cast<T*>(a.dst);
@@ -890,9 +921,9 @@ k_scatter_eq(const StepArgs a, const double* in, int near_parts) {
       const double p = __dsub_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(3.0, cu)), __dmul_rn(__dmul_rn(4.5, cu), cu)), t6);
       f[i] = static_cast<float>(__dsub_rn(__dmul_rn(__dmul_rn(rho, wd(i)), p), wd(i)));
     }
-    const int kind = a.flags ? (a.flags[slot] & kKindMask) : kBulk;
-    if (kind == kBulk) {
-      if (a.cr_avg) v[0] = bgk_const_rho(f, a.omega, static_cast<float>(1.0 - *a.cr_avg));
+    const uint8_t fl = a.flags ? a.flags[slot] : static_cast<uint8_t>(kBulk);
+    if ((fl & kKindMask) == kBulk) {
+      if (a.cr_avg) v[0] = (fl & kFlagProlong) ? 0.0 : bgk_const_rho(f, a.omega, static_cast<float>(1.0 - *a.cr_avg));
       else bgk<kBgkCorrect<T>>(f, a.omega);
     }
     T* dst = static_cast<T*>(a.dst);
@@ -908,13 +939,13 @@ k_scatter_eq(const StepArgs a, const double* in, int near_parts) {
 }
 
 // ConstRhoBGK statistics of a stored state that BGK collided (which keeps
-// each cell's density): per CTA the sum of rho - 1 over kBulk core cells, as
-// k_scatter lays them out.
+// each cell's density): per CTA the sum of rho - 1 over kBulk core cells
+// that no prolongation writes, as k_scatter lays them out.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_cr_seed(const StepArgs a, int near_parts) {
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   double v[1] = {0.0};
-  if (t < a.ncore && (a.flags ? (a.flags[t] & kKindMask) : kBulk) == kBulk) {
+  if (t < a.ncore && (a.flags ? (a.flags[t] & (kKindMask | kFlagProlong)) : kBulk) == kBulk) {
     const T* src = static_cast<const T*>(a.src);
     float f[kQ];
 #pragma unroll
@@ -927,6 +958,27 @@ __global__ void __launch_bounds__(kThreads) k_cr_seed(const StepArgs a, int near
   if (threadIdx.x == 0) a.cr_part[blockIdx.x] = v[0];
   if (blockIdx.x == 0)
     for (int p = threadIdx.x; p < near_parts; p += kThreads) a.cr_part[gridDim.x + p] = 0.0;
+}
+
+// The collide of a level above the finest under ConstRhoBGK on a multi-level
+// mesh (TimeLoop::collide_level without statistics, time_loop.h:173-187),
+// run in place on its pulled populations once its coupling is done: the
+// restriction has written its targets, and the average density is the one
+// the finest level's last collide gave, which the reference's next collide
+// of this level uses.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_collide_cr(const StepArgs a) {
+  pdl_wait();
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= a.ncore) return;
+  if (a.flags && (a.flags[t] & kKindMask) != kBulk) return;
+  T* pops = static_cast<T*>(a.dst);
+  float f[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) f[i] = LD(pops, a.qs, i, t, a.inv_scale);
+  bgk_const_rho(f, a.omega, static_cast<float>(1.0 - *a.cr_avg));
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) Store<T>::st(pops + i * a.qs + t, f[i], a.scale);
 }
 
 // average_rho <- CollideRhoStats::average() of the last collide
@@ -969,7 +1021,6 @@ bool programmatic_launch() { return g_programmatic; }
 template <typename T>
 cudaError_t launch_step(const StepArgs& a, bool periodic, bool links, bool flags, cudaStream_t s) {
   cudaError_t e = cudaSuccess;
-  (void)periodic;
   if (a.nitems == 0) return cudaSuccess;
   // CTAs aligned to blocks: core cells first (a multiple of the CTA size),
   // then the halo items in CTAs of their own.
@@ -978,13 +1029,17 @@ cudaError_t launch_step(const StepArgs& a, bool periodic, bool links, bool flags
   const uint32_t core_ctas = grid_for(a.ncore);
   const dim3 g(core_ctas + grid_for(a.nitems - a.ncore));
   StepArgs b = a;
+  // the flag-free periodic box collides as k_step_pair does (defect removal)
+  const bool box = periodic && !flags && !links;
   if (blocked) {
     if (links) e = launch_chain(k_step<T, true, true, true>, dim3(g), dim3(kThreads), 0, s, b);
     else if (flags) e = launch_chain(k_step<T, false, true, true>, dim3(g), dim3(kThreads), 0, s, b);
+    else if (box) e = launch_chain(k_step<T, false, false, true, kCollBgk, true>, dim3(g), dim3(kThreads), 0, s, b);
     else e = launch_chain(k_step<T, false, false, true>, dim3(g), dim3(kThreads), 0, s, b);
   } else {
     if (links) e = launch_chain(k_step<T, true, true, false>, dim3(g), dim3(kThreads), 0, s, b);
     else if (flags) e = launch_chain(k_step<T, false, true, false>, dim3(g), dim3(kThreads), 0, s, b);
+    else if (box) e = launch_chain(k_step<T, false, false, false, kCollBgk, true>, dim3(g), dim3(kThreads), 0, s, b);
     else e = launch_chain(k_step<T, false, false, false>, dim3(g), dim3(kThreads), 0, s, b);
   }
   return e != cudaSuccess ? e : cudaGetLastError();
@@ -1025,9 +1080,47 @@ cudaError_t launch_step_map_cr(const StepArgs& a, const NearTables& nt, bool lin
   if (a.nitems == 0) return cudaSuccess;
   const uint32_t near_ctas = links ? grid_for(static_cast<uint32_t>(nt.n) * 32) : 0;
   const dim3 g(near_ctas + static_cast<uint32_t>(a.nblk) * (links ? 2 : 1) + grid_for(static_cast<uint32_t>(a.n_open)));
-  if (links) e = launch_chain(k_step_map<T, true, true, 1, true, true>, g, dim3(kThreads), 0, s, a, nt);
-  else if (flags) e = launch_chain(k_step_map<T, false, true, 2, true, true>, g, dim3(kThreads), 0, s, a, nt);
-  else e = launch_chain(k_step_map<T, false, false, 2, true, true>, g, dim3(kThreads), 0, s, a, nt);
+  if (links) e = launch_chain(k_step_map<T, true, true, 1, true, kCollConstRho>, g, dim3(kThreads), 0, s, a, nt);
+  else if (flags) e = launch_chain(k_step_map<T, false, true, 2, true, kCollConstRho>, g, dim3(kThreads), 0, s, a, nt);
+  else e = launch_chain(k_step_map<T, false, false, 2, true, kCollConstRho>, g, dim3(kThreads), 0, s, a, nt);
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+// Stream-only steps (no collide) of the levels above the finest under
+// ConstRhoBGK on a multi-level mesh: the slot-map form in the variants of
+// launch_step_map_cr, else the core / halo-item launch and the near cells.
+template <typename T>
+cudaError_t launch_step_map_nc(const StepArgs& a, const NearTables& nt, bool links, bool flags, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
+  if (a.nitems == 0) return cudaSuccess;
+  const uint32_t near_ctas = links ? grid_for(static_cast<uint32_t>(nt.n) * 32) : 0;
+  const dim3 g(near_ctas + static_cast<uint32_t>(a.nblk) * (links ? 2 : 1) + grid_for(static_cast<uint32_t>(a.n_open)));
+  if (links) e = launch_chain(k_step_map<T, true, true, 1, true, kCollNone>, g, dim3(kThreads), 0, s, a, nt);
+  else if (flags) e = launch_chain(k_step_map<T, false, true, 2, true, kCollNone>, g, dim3(kThreads), 0, s, a, nt);
+  else e = launch_chain(k_step_map<T, false, false, 2, true, kCollNone>, g, dim3(kThreads), 0, s, a, nt);
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_step_nc(const StepArgs& a, const NearTables& nt, bool links, bool flags, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
+  if (a.nitems == 0) return cudaSuccess;
+  const uint32_t n3 = static_cast<uint32_t>(a.n) * a.n * a.n;
+  const bool blocked = n3 % kThreads == 0;
+  const uint32_t core_ctas = grid_for(a.ncore);
+  const dim3 g(core_ctas + grid_for(a.nitems - a.ncore));
+  const StepArgs& b = a;
+  if (blocked) {
+    if (links) e = launch_chain(k_step<T, true, true, true, kCollNone>, g, dim3(kThreads), 0, s, b);
+    else if (flags) e = launch_chain(k_step<T, false, true, true, kCollNone>, g, dim3(kThreads), 0, s, b);
+    else e = launch_chain(k_step<T, false, false, true, kCollNone>, g, dim3(kThreads), 0, s, b);
+  } else {
+    if (links) e = launch_chain(k_step<T, true, true, false, kCollNone>, g, dim3(kThreads), 0, s, b);
+    else if (flags) e = launch_chain(k_step<T, false, true, false, kCollNone>, g, dim3(kThreads), 0, s, b);
+    else e = launch_chain(k_step<T, false, false, false, kCollNone>, g, dim3(kThreads), 0, s, b);
+  }
+  if (e == cudaSuccess && nt.n > 0)
+    e = launch_chain(k_step_near<T, kCollNone>, dim3(grid_for(static_cast<uint32_t>(nt.n) * 32)), dim3(kThreads), 0,
+                     s, a, nt);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -1114,6 +1207,9 @@ cudaError_t launch_scatter_eq(const StepArgs& a, const double* in, int near_part
   return cudaGetLastError();
 }
 
+// CTAs of a k_couple launch's prolongation of n items (one warp per item).
+uint32_t couple_prolong_ctas(int n) { return grid_for(static_cast<uint32_t>(n) * 32); }
+
 // ConstRhoBGK partials of a level: one per core CTA of k_step_cr (the CTAs of
 // k_scatter / k_cr_seed), then one per CTA of k_step_near_cr.
 uint32_t cr_core_parts(const StepArgs& a) { return grid_for(a.ncore); }
@@ -1139,6 +1235,13 @@ cudaError_t launch_step_cr(const StepArgs& a, const NearTables& nt, bool links, 
   if (e == cudaSuccess && nt.n > 0)
     e = launch_chain(k_step_near_cr<T>, dim3(cr_near_parts(nt)), dim3(kThreads), 0, s, a, nt,
                      static_cast<int>(core_ctas));
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_collide_cr(const StepArgs& a, cudaStream_t s) {
+  if (a.ncore == 0) return cudaSuccess;
+  const cudaError_t e = launch_chain(k_collide_cr<T>, dim3(grid_for(a.ncore)), dim3(kThreads), 0, s, a);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -1171,6 +1274,9 @@ cudaError_t launch_cr_update(double* avg, const double* part, int nparts, long l
   template cudaError_t launch_scatter_eq<T>(const StepArgs&, const double*, int, cudaStream_t);  \
   template cudaError_t launch_step_cr<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
   template cudaError_t launch_step_map_cr<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
+  template cudaError_t launch_step_map_nc<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
+  template cudaError_t launch_step_nc<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
+  template cudaError_t launch_collide_cr<T>(const StepArgs&, cudaStream_t);                        \
   template cudaError_t launch_cr_seed<T>(const StepArgs&, int, cudaStream_t);
 
 OCTLB_INST(float)

@@ -139,11 +139,24 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     ctx->side_busy = true;
     ++ctx->launch_count;
   }
-  if (ctx->const_rho) {
+  if (ctx->const_rho && L.lvl != ctx->cr_level) {
+    // ConstRhoBGK, a level above the finest: the step only streams (and
+    // saves the coupler's rows); the level collides in do_advance_level once
+    // its coupling is done, at the average density the finest level's last
+    // collide gives (the stored state of every level is again one collide
+    // ahead after advance_one)
+    const bool links = ctx->stream_mode == OCTLB_STREAM_LINKS;
+    if (L.use_map && ctx->map_global && ctx->map_cells == (links ? 1 : 2)) {
+      CK(launch_step_map_nc<T>(a, L.near, links, L.has_flags, ctx->stream));
+    } else {
+      CK(launch_step_nc<T>(a, L.near, links, L.has_flags, ctx->stream));
+      if (L.near.n > 0) ++ctx->launch_count;
+    }
+  } else if (ctx->const_rho) {
     // ConstRhoBGK: average_rho from the last collide's statistics
     // (time_loop.h:220-222), then the step whose collide uses it
-    CK(launch_cr_update(ctx->cr_avg.as<double>(), ctx->cr_part.as<double>(), ctx->cr_nparts, ctx->cr_count,
-                        ctx->fd_cr_part.as<double>(), ctx->fd_cr_parts, ctx->fd_vel, ctx->stream));
+    CK(launch_cr_update(ctx->cr_avg.as<double>(), ctx->cr_part.as<double>(), ctx->cr_nparts + ctx->cr_pparts,
+                        ctx->cr_count, ctx->fd_cr_part.as<double>(), ctx->fd_cr_parts, ctx->fd_vel, ctx->stream));
     const bool links = ctx->stream_mode == OCTLB_STREAM_LINKS;
     if (L.use_map && ctx->map_global && ctx->map_cells == (links ? 1 : 2)) {
       CK(launch_step_map_cr<T>(a, L.near, links, L.has_flags, ctx->stream));
@@ -210,6 +223,18 @@ int do_advance_level(octlb_ctx* ctx, int l) {
       p.scale = ctx->pscale_l[l];
       p.omega = static_cast<float>(ctx->omega_l[l + 1]);  // the written fine cell collides with its level's rate
       p.fscale = F.scale;
+      if (ctx->cr_multi) {
+        // ConstRhoBGK: a target on the finest level takes that level's
+        // collide (the step's of the cell is replaced) and its statistic;
+        // a target above it collides with its level
+        if (l + 1 == ctx->cr_level) {
+          p.cmode = kCollConstRho;
+          p.cr_avg = ctx->cr_avg.as<double>();
+          p.cr_part = ctx->cr_part.as<double>() + ctx->cr_nparts;
+        } else {
+          p.cmode = kCollNone;
+        }
+      }
       bool share = pend.size() <= 2;
       for (const auto& q : pend)
         if (q.level == l + 1 && !F.fuse_restrict) share = false;
@@ -235,7 +260,19 @@ int do_advance_level(octlb_ctx* ctx, int l) {
     r.scale = ctx->rscale_l[l];
     r.omega = static_cast<float>(ctx->omega_l[l]);
     r.cscale = L.scale;
+    r.cmode = ctx->cr_multi ? kCollNone : kCollBgk;  // under ConstRhoBGK the level collides below
     pend.push_back({r, l});
+  }
+  if (ctx->cr_multi && L.nblk > 0) {
+    // ConstRhoBGK on a multi-level mesh: this level's collide (the
+    // reference's next collide_level(l), time_loop.h:201-205), after the
+    // restriction wrote its targets
+    rc = flush_restricts<T>(ctx);
+    if (rc) return rc;
+    StepArgs a = L.args;
+    a.dst = cur_buf(L);
+    CK(launch_collide_cr<T>(a, ctx->stream));
+    ++ctx->launch_count;
   }
   return OCTLB_OK;
 }
@@ -628,7 +665,7 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       L.args.err = ctx->dev_err.as<int>();
       continue;
     }
-    L.has_flags = !ctx->periodic || !save_rows[l].empty();
+    L.has_flags = !ctx->periodic || !save_rows[l].empty() || (l >= 1 && !prolong[l - 1].empty());
     if (ctx->periodic) {
       for (long long k = 0; k < n3; ++k) if (t->kinds[k] != kBulk) L.has_flags = true;
     }
@@ -685,6 +722,8 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
         flags[kv.first] |= kFlagSave;
       }
     }
+    if (l >= 1)
+      for (const ProlongItem& it : prolong[l - 1]) flags[static_cast<size_t>(it.fine_slot)] |= kFlagProlong;
     L.n_save = n_save_all[l];
 
     // Same-level neighbour of each of the 27 halo directions (faces and edges
@@ -2139,26 +2178,36 @@ int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on) {
   for (size_t l = 0; l < ctx->levels.size(); ++l)
     if (ctx->levels[l].nblk > 0) { lev = static_cast<int>(l); ++used; }
   if (!on) {
-    if (ctx->cr_level >= 0) {
-      ctx->levels[ctx->cr_level].args.cr_avg = nullptr;
-      ctx->levels[ctx->cr_level].args.cr_part = nullptr;
+    for (auto& L : ctx->levels) {
+      L.args.cr_avg = nullptr;
+      L.args.cr_part = nullptr;
     }
-    ctx->const_rho = false;
+    ctx->const_rho = ctx->cr_multi = false;
     ctx->cr_level = -1;
+    ctx->cr_pparts = 0;
     return OCTLB_OK;
   }
-  // The stored state is one collide ahead of the reference's, so a coarse
-  // level would collide before the finest steps that set its average density
-  // have run: ConstRhoBGK is built for one level, as the reference uses it.
-  if (used != 1) return fail(ctx, OCTLB_EINVAL, "ConstRhoBGK needs a single-level mesh");
+  // The statistics are the finest level's (TimeLoop::advance collects them
+  // when level >= max_level_, time_loop.h:201-222) and every level collides
+  // at the average density.  The stored state is one collide ahead of the
+  // reference's; a coarser level's collide needs the average of finest
+  // steps that come after its step, so with more than one level the coarser
+  // levels' steps only stream and each collides after its coupling
+  // (do_advance_level).  On the finest level a prolongation's target takes
+  // the collide and statistic the step gave it.
   Level& L = ctx->levels[lev];
   CK(upload(ctx->cr_avg, std::vector<double>{1.0}));  // TimeLoop starts at average_rho_ = 1
   const uint32_t core = cr_core_parts(L.args), near = cr_near_parts(L.near);
+  ctx->cr_multi = used > 1;
   ctx->cr_nparts = static_cast<int>(core + near);
   ctx->cr_near = static_cast<int>(near);
+  ctx->cr_pparts = ctx->cr_multi && lev >= 1 ? static_cast<int>(couple_prolong_ctas(ctx->levels[lev - 1].n_prolong)) : 0;
   ctx->cr_count = L.n_bulk;
-  CK(ctx->cr_part.alloc(static_cast<size_t>(std::max(ctx->cr_nparts, 1)) * sizeof(double)));
-  L.args.cr_avg = ctx->cr_avg.as<double>();
+  const size_t nparts = static_cast<size_t>(std::max(ctx->cr_nparts + ctx->cr_pparts, 1));
+  CK(ctx->cr_part.alloc(nparts * sizeof(double)));
+  CK(cudaMemsetAsync(ctx->cr_part.p, 0, nparts * sizeof(double), ctx->stream));
+  for (auto& C : ctx->levels)
+    if (C.nblk > 0) C.args.cr_avg = ctx->cr_avg.as<double>();  // every level collides at the average
   L.args.cr_part = ctx->cr_part.as<double>();
   L.args.cr_total = ctx->cr_nparts;
   // The stored state was collided by BGK, which is ConstRhoBGK at

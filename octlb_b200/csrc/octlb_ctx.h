@@ -38,9 +38,15 @@ cudaError_t launch_step_cr(const StepArgs&, const NearTables&, bool, bool, cudaS
 template <typename T> cudaError_t launch_cr_seed(const StepArgs&, int, cudaStream_t);
 template <typename T>
 cudaError_t launch_step_map_cr(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
+template <typename T>
+cudaError_t launch_step_map_nc(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
+template <typename T>
+cudaError_t launch_step_nc(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
+template <typename T> cudaError_t launch_collide_cr(const StepArgs&, cudaStream_t);
 cudaError_t launch_cr_update(double*, const double*, int, long long, const double*, int, long long, cudaStream_t);
 uint32_t cr_core_parts(const StepArgs& a);
 uint32_t cr_near_parts(const NearTables& nt);
+uint32_t couple_prolong_ctas(int n);
 template <typename T> cudaError_t launch_step_bulk(const StepArgs&, int, cudaStream_t);
 template <typename T> int bulk_prepare(int n);
 template <typename T> cudaError_t launch_step_pair(const StepArgs&, cudaStream_t);
@@ -315,12 +321,15 @@ struct octlb_ctx {
   std::vector<float> pscale_l, rscale_l;
   double wall_vscale = 0.0;         // largest moving-wall speed (adjoint velocity parameter)
   std::unique_ptr<AdjointState> adj;
-  // ConstRhoBGK (TimeLoop's use_const_rho_bgk, single-level meshes): the
-  // average density on the device (TimeLoop::average_rho_) and the partial
-  // sums of the last collide's statistics, over cr_count kBulk cells
-  bool const_rho = false;
+  // ConstRhoBGK (TimeLoop's use_const_rho_bgk): the average density on the
+  // device (TimeLoop::average_rho_) and the partial sums of the last collide
+  // of the finest level cr_level, over its cr_count kBulk cells: cr_nparts
+  // from its step, then cr_pparts from the prolongation into it.  cr_multi:
+  // levels above cr_level exist; their steps only stream, and each collides
+  // (k_collide_cr) once its coupling is done.
+  bool const_rho = false, cr_multi = false;
   DevBuf cr_avg, cr_part;
-  int cr_level = -1, cr_nparts = 0, cr_near = 0;
+  int cr_level = -1, cr_nparts = 0, cr_near = 0, cr_pparts = 0;
   long long cr_count = 0;
   // Ranks (octlb_gpu_create_part): this context steps the blocks with
   // owner[b] == rank and exchanges with the other ranks' contexts through

@@ -125,6 +125,11 @@ struct ProlongOp {
   void* fine;
   long long fine_qs;
   float scale, omega, fscale;
+  // collide of a kBulk target (kCollBgk, kCollNone, or kCollConstRho at
+  // *cr_avg with each prolongation CTA's sum of rho - 1 in cr_part[CTA])
+  int cmode;
+  const double* cr_avg;
+  double* cr_part;
 };
 struct RestrictOp {
   const RestrictItem* items;
@@ -133,6 +138,7 @@ struct RestrictOp {
   void* coarse;
   long long coarse_qs;
   float scale, omega, cscale;
+  int cmode;                // collide of a kBulk target: kCollBgk or kCollNone
 };
 // MEM drag cell: kBulk core cell with at least one obstacle link; bit i of
 // mask set when x + c_i is an in-block solid / Bouzidi obstacle cell

@@ -4,9 +4,11 @@ of the previous collide's statistics (time_loop.h:201-222).
 
 CPU: the reference build's statistics against their definition.  GPU (through
 the C ABI): fields and average_rho against the reference TimeLoop run with
-use_const_rho_bgk, on single-level meshes under both stream rules; FP32
-tolerance 1e-5, FP16-shifted 2e-3 (max-abs over max-abs), average_rho within
-1e-6 (FP32; the GPU sums FP32 densities in FP64)."""
+use_const_rho_bgk, on single-level meshes under both stream rules and on two-
+and three-level meshes (statistics of the finest level, every level colliding
+at the average); FP32 tolerance 1e-5, FP16-shifted 2e-3 (max-abs over
+max-abs), average_rho within 1e-6 (FP32; the GPU sums FP32 densities in
+FP64)."""
 import numpy as np
 import pytest
 
@@ -144,13 +146,87 @@ def test_const_rho_cylinder_links_matches_reference(ob, ref, kernel, monkeypatch
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol,kernel", [("fp32", TOL32, "map"), ("fp16", TOL16, "map"), ("fp32", TOL32, "plain")])
+def test_const_rho_amr_cavity_matches_reference(ob, ref, prec, tol, kernel, monkeypatch):
+    """Two-level moving-lid cavity (16^3 base, refined band under the lid)
+    from a perturbed rest state at mean density 1.02: the statistics are the
+    finest level's collides (prolongation targets included, with the
+    densities the prolongation wrote), the coarse level collides at the same
+    average (time_loop.h:201-222); average_rho after every call and the fields
+    of both levels after 1 and 12 calls against the reference TimeLoop."""
+    if kernel == "plain":
+        monkeypatch.setenv("OCTLB_STEP_KERNEL", "plain")
+    from octlb_b200 import cases
+    mesh, _, info = cases.cavity_forest(cells=16, n=8, lid=0.1, tau=0.6, band_cells=8)
+    assert len(set(mesh.levels.tolist())) == 2
+    init = rest_state(mesh, perturbed_density(mesh, 1.02, 17))
+    lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP32 if prec == "fp32" else ob.FP16_SHIFTED,
+                        init_pops=init)
+    lat.set_const_rho(True)
+    sim = oracle.Sim(ref, mesh, info["omega"], init)
+    sim.set_const_rho(True)
+    bgk = oracle.Sim(ref, mesh, info["omega"], init)
+    atol = 1e-6 if prec == "fp32" else 2e-4
+    for call in range(12):
+        lat.advance(1)
+        sim.advance(1)
+        bgk.advance(1)
+        assert abs(lat.average_rho() - sim.average_rho()) <= atol, call
+        if call in (0, 11):
+            rho_g, u_g = lat.get_fields()
+            rho_r, u_r = oracle.rho_u(sim.core())
+            assert rel(rho_g, rho_r) <= tol, call
+            assert rel(u_g, u_r) <= tol, call
+    rho_b, _ = oracle.rho_u(bgk.core())
+    assert rel(rho_b, rho_r) > 100 * TOL32
+    c, s = lat.counters()
+    cr, sr, _ = sim.counters()
+    assert c == cr and s == sr
+    lat.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", ["map", "plain"])
+def test_const_rho_three_level_cylinder_matches_reference(ob, ref, kernel, monkeypatch):
+    """Three-level channel with a Bouzidi cylinder (links stream rule, near-wall
+    cells, parabolic inlet, outflow copy) from a perturbed rest state at mean
+    density 1.01: two levels above the finest stream, couple and then collide
+    at the average of the finest level's statistics."""
+    if kernel == "plain":
+        monkeypatch.setenv("OCTLB_STEP_KERNEL", "plain")
+    from octlb_b200 import cases
+    mesh, _, info = cases.cylinder_forest(length=128, height=32, n=8, diameter=8.0, center=(16.0, 16.0), levels=3,
+                                          refine_dist=8.0)
+    assert len(set(mesh.levels.tolist())) == 3
+    init = rest_state(mesh, perturbed_density(mesh, 1.01, 23))
+    init[mesh.kinds == ob.SOLID] = 0.0
+    lat = ob.GpuLattice(mesh, info["omega"], stream_mode=ob.STREAM_LINKS, init_pops=init)
+    lat.set_const_rho(True)
+    sim = oracle.Sim(ref, mesh, info["omega"], init, link_mode=True)
+    sim.set_const_rho(True)
+    for call in range(4):
+        lat.advance(1)
+        sim.advance(1)
+        assert abs(lat.average_rho() - sim.average_rho()) <= 1e-6, call
+    rho_g, u_g = lat.get_fields()
+    rho_r, u_r = oracle.rho_u(sim.core())
+    fl = mesh.kinds != ob.SOLID
+    assert rel(rho_g[fl], rho_r[fl]) <= TOL32
+    assert rel(u_g[fl], u_r[fl]) <= TOL32
+    lat.close()
+
+
+@pytest.mark.gpu
 def test_const_rho_argument_checks(ob):
     from octlb_b200 import cases
-    mesh, init, info = cases.cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=8)
+    mesh, init, info = cases.cavity_forest(cells=16, n=8, lid=0.1, tau=0.6, band_cells=8)
     two = ob.GpuLattice(mesh, info["omega"], init_pops=init)
     assert two.average_rho() == 1.0
+    two.set_const_rho(True)                  # two levels: the finest level's statistics
+    two.advance(1)
+    assert two.average_rho() != 1.0
     with pytest.raises(ob.OctlbError):
-        two.set_const_rho(True)              # two levels
+        two.adjoint(4, 2)                    # the adjoint differentiates BGK
     two.close()
     mesh, info = brick_cavity()
     lat = ob.GpuLattice(mesh, info["omega"])
