@@ -46,7 +46,8 @@ def measured_peak():
 
 def committed_traffic(kernel_key):
     """Per-launch DRAM bytes of a kernel from the committed ncu summary
-    (profiles/ncu_traffic.txt lines: '<key> <bytes_per_launch>'), or None."""
+    (profiles/ncu_traffic.txt lines: '<key> <bytes_per_launch>', each one
+    256^3 launch captured on its own), or None."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if not os.path.exists(path):
         return None

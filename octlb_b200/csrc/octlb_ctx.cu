@@ -224,16 +224,14 @@ int do_advance_level(octlb_ctx* ctx, int l) {
       p.omega = static_cast<float>(ctx->omega_l[l + 1]);  // the written fine cell collides with its level's rate
       p.fscale = F.scale;
       if (ctx->cr_multi) {
-        // ConstRhoBGK: a target on the finest level takes that level's
-        // collide (the step's of the cell is replaced) and its statistic;
-        // a target above it collides with its level
-        if (l + 1 == ctx->cr_level) {
-          p.cmode = kCollConstRho;
-          p.cr_avg = ctx->cr_avg.as<double>();
-          p.cr_part = ctx->cr_part.as<double>() + ctx->cr_nparts;
-        } else {
-          p.cmode = kCollNone;
-        }
+        // ConstRhoBGK: the target takes the collide the reference's next
+        // collide_level(l + 1) gives it, at the average now in effect (no
+        // finest step runs in between).  On the finest level the step's
+        // collide of the cell is replaced and the statistic is this one; on
+        // a level above it, the level's own collide pass has already run.
+        p.cmode = kCollConstRho;
+        p.cr_avg = ctx->cr_avg.as<double>();
+        if (l + 1 == ctx->cr_level) p.cr_part = ctx->cr_part.as<double>() + ctx->cr_nparts;
       }
       bool share = pend.size() <= 2;
       for (const auto& q : pend)
