@@ -327,6 +327,38 @@ def accuracy_vs_fp64(ob, cases, n, steps, fields_fp32, threads=None):
     return out
 
 
+def aa_measurements(ob, cases, torch, n, steps, warmup, peak):
+    """The same periodic box in the one-buffer AA stream order (in-place
+    steps alternating between a neighbour pull / push-back and a step on the
+    cell's own slots; bitwise equal results, tests/test_gpu_tgv.py): MLUPS,
+    the fraction of the measured copy peak at the same algorithmic bytes per
+    update, and the device bytes of the population state (half the AB
+    order's)."""
+    out = {}
+    for pn, prec in (("fp32", ob.FP32), ("fp16", ob.FP16_SHIFTED)):
+        mesh, init, info = cases.tgv_periodic(n, u0=0.05, tau=0.55)
+        lat = ob.GpuLattice(mesh, info["omega"], precision=prec, init_pops=init, stream_order=ob.ORDER_AA)
+        st = torch.cuda.Stream()
+        lat.set_stream(st.cuda_stream)
+        lat.advance(warmup + (warmup % 2))  # an even count: the natural layout
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        lat.advance(steps)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        _, lups = lat.step_stats()
+        bpl = 152 if pn == "fp32" else 76
+        out[pn] = {"mlups": lups / ms / 1e3, "ms_per_step": ms, "bytes_per_lu": bpl,
+                   "frac": bpl * lups / (ms * 1e-3) / 1e9 / peak,
+                   "state_bytes": n ** 3 * 19 * (4 if pn == "fp32" else 2)}
+        lat.close()
+        del lat
+        torch.cuda.empty_cache()
+    return out
+
+
 def forest_measurements(ob, cases, torch, peak):
     """The forest configurations beside the headline line: MLUPS of the
     two-level AMR cavity (64^3 + band under the lid) and of the three-level
@@ -501,6 +533,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-forest", action="store_true", help="skip the forest / adjoint measurements")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the errors against the FP64 runs")
+    ap.add_argument("--no-aa", action="store_true", help="skip the one-buffer (AA order) measurement")
     ap.add_argument("--case", default="tgv", choices=["tgv", "amr_cavity_64", "cylinder", "cylinder_512", "adjoint",
                                                       "const_rho_cavity_128"],
                     help="tgv: the headline line; otherwise run only that case for --steps advance_one "
@@ -620,6 +653,8 @@ def main():
         m = min(args.steps, 20)
         out["accuracy_vs_fp64"] = accuracy_vs_fp64(ob, cases, n, m,
                                                    results.get("e2e_fields") if m == args.steps else None)
+    if rank == 0 and world == 1 and not args.no_aa:
+        out["aa_one_buffer"] = aa_measurements(ob, cases, torch, n, args.steps, args.warmup, peak)
     if rank == 0 and world == 1 and not args.no_forest:
         out["forest"] = forest_measurements(ob, cases, torch, peak)
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -100,6 +100,12 @@ typedef struct octlb_tables {
 #define OCTLB_COUPLER_REFERENCE 0
 #define OCTLB_COUPLER_PHYSICAL 1
 
+/* Stream order (the storage pattern of the pull; the results do not depend on
+ * it): AB keeps two population buffers, AA one (Bailey et al., "Accelerating
+ * lattice Boltzmann fluid flow simulations using graphics processors", 2009). */
+#define OCTLB_ORDER_AB 0
+#define OCTLB_ORDER_AA 1
+
 typedef struct octlb_params {
   double omega;                   /* REFERENCE: the global BGK rate; PHYSICAL: the
                                      rate of the coarsest level with blocks */
@@ -110,6 +116,15 @@ typedef struct octlb_params {
   int coupler_mode;               /* OCTLB_COUPLER_REFERENCE (0) or _PHYSICAL */
   double omega_level[32];         /* PHYSICAL: explicit rate of level l, or 0 for
                                      the rescaled one */
+  int stream_order;               /* OCTLB_ORDER_AB (0): two population buffers,
+                                     pull from one into the other; OCTLB_ORDER_AA:
+                                     one buffer updated in place, alternating a
+                                     step that pulls from and writes back to the
+                                     neighbours with one that reads and writes the
+                                     cell's own slots (uniform periodic box only:
+                                     one level, every cell kBulk, one context, no
+                                     body force, ConstRhoBGK, drag or adjoint);
+                                     half the memory, the same results bitwise */
 } octlb_params;
 
 typedef struct octlb_ctx octlb_ctx;

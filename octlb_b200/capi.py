@@ -27,6 +27,8 @@ STREAM_ROTATE = 0
 STREAM_LINKS = 1
 COUPLER_REFERENCE = 0
 COUPLER_PHYSICAL = 1
+ORDER_AB = 0
+ORDER_AA = 1
 TB_NONE = 0
 TB_WALL = 1
 TB_OUTFLOW = 2
@@ -73,6 +75,7 @@ class Params(ctypes.Structure):
         ("omega", ctypes.c_double), ("precision", ctypes.c_int), ("stream_mode", ctypes.c_int),
         ("drag", ctypes.c_int), ("fp16_scale", ctypes.c_double * 32),
         ("coupler_mode", ctypes.c_int), ("omega_level", ctypes.c_double * 32),
+        ("stream_order", ctypes.c_int),
     ]
 
 

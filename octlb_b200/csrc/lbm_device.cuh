@@ -34,6 +34,15 @@ __device__ __forceinline__ Cell cell_of(const StepArgs& a, uint32_t t) {
   return c;
 }
 
+// Population i of core slot t as a reader sees it: plane i at t, or, in an
+// AA-order box after an odd number of steps (a.aa_rev), plane opp(i) at the
+// periodic neighbour t + c_i of the single block.
+template <typename T>
+__device__ __forceinline__ float LDR(const StepArgs& a, const T* base, int i, uint32_t t) {
+  if (!a.aa_rev) return LD(base, a.qs, i, t, a.inv_scale);
+  return Store<T>::ld(base + aa_rev_slot(a, i, t), a.inv_scale);
+}
+
 // Own halo-page slot of padded position (X, Y, Z) of block b; positions that
 // no table covers are excluded by construction, the check keeps the access in
 // bounds and records an error if that ever fails.

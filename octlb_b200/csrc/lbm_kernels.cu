@@ -552,6 +552,62 @@ __global__ void __launch_bounds__(kThreads) k_step_quad_h(const StepArgs a) {
   for (int i = 0; i < kQ; ++i) st4h(o + i * a.qs, f0[i], f1[i], f2[i], f3[i]);
 }
 
+// AA stream order on a uniform periodic box: one population buffer, updated
+// in place by two alternating steps (Bailey et al. 2009).  Both pull the
+// same values as k_step_pair and collide with the same bgk() call, so the
+// results equal the two-buffer order's bitwise.
+//
+// From the natural layout (plane i at cell x): each cell pulls population i
+// from x - c_i in plane i, collides, and writes each result back into a slot
+// it read -- the slot read for direction k receives g_opp(k).  Every slot is
+// read and written by exactly one cell (x - c_k, plane k belongs to x), so
+// the update is race-free in place and leaves the reversed layout: g_i of
+// cell x in plane opp(i) at x + c_i.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_step_aa_pull(const StepArgs a) {
+  pdl_wait();
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= a.ncore) return;
+  const uint32_t n = a.n;
+  const uint32_t x = a.div_n2.div(t), r = t - x * n * n, y = a.div_n.div(r), z = r - y * n;
+  const uint32_t xm = x == 0 ? n - 1 : x - 1, xp = x == n - 1 ? 0 : x + 1;
+  const uint32_t ym = y == 0 ? n - 1 : y - 1, yp = y == n - 1 ? 0 : y + 1;
+  const uint32_t zm = z == 0 ? n - 1 : z - 1, zp = z == n - 1 ? 0 : z + 1;
+  T* pops = static_cast<T*>(a.dst);  // == a.src
+  long long at[kQ];
+  float f[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const uint32_t sx = cx(i) == 1 ? xm : (cx(i) == -1 ? xp : x);
+    const uint32_t sy = cy(i) == 1 ? ym : (cy(i) == -1 ? yp : y);
+    const uint32_t sz = cz(i) == 1 ? zm : (cz(i) == -1 ? zp : z);
+    at[i] = i * a.qs + (static_cast<long long>(sx) * n + sy) * n + sz;
+    f[i] = Store<T>::ld(pops + at[i], 1.0f);  // storage units, as k_step_pair
+  }
+  bgk<kBgkCorrect<T>>(f, a.omega, a.scale, a.inv_scale);
+#pragma unroll
+  for (int k = 0; k < kQ; ++k) Store<T>::st(pops + at[k], f[opp(k)], 1.0f);
+}
+
+// From the reversed layout: population i of cell x (streamed) is the value
+// in plane opp(i) at x itself; collide, and write plane i at x -- the
+// natural layout again.  Two z cells per thread with 2-element accesses.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_step_aa_local(const StepArgs a) {
+  pdl_wait();
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= a.ncore / 2) return;
+  T* pops = static_cast<T*>(a.dst);  // == a.src
+  const long long s = 2ll * t;
+  float f0[kQ], f1[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) Pair<T>::ld(pops + opp(i) * a.qs + s, a.inv_scale, f0[i], f1[i]);
+  bgk<kBgkCorrect<T>>(f0, a.omega, a.scale, a.inv_scale);
+  bgk<kBgkCorrect<T>>(f1, a.omega, a.scale, a.inv_scale);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) Pair<T>::st(pops + i * a.qs + s, f0[i], f1[i], a.scale);
+}
+
 // Body force: the forcing term 3 w_i (c_i . F) added to the stored
 // (post-collision) populations of kBulk core cells at the start of each level
 // step, before the boundary fills read them.  F is SoA [3][ncore].
@@ -810,7 +866,7 @@ k_audit(const StepArgs a, double* partial) {
     bool finite = true;
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
-      f[i] = LD(src, a.qs, i, slot, a.inv_scale);
+      f[i] = LDR(a, src, i, t);
       finite = finite && isfinite(f[i]);
     }
     const int kind = a.flags ? (a.flags[slot] & kKindMask) : kBulk;
@@ -840,12 +896,12 @@ k_gather(const StepArgs a, double* out, double* out_u, int mode /*0 pops, 1 fiel
   const T* src = static_cast<const T*>(a.src);
   if (mode == 0) {
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) out[static_cast<long long>(t) * kQ + i] = LD(src, a.qs, i, slot, a.inv_scale);
+    for (int i = 0; i < kQ; ++i) out[static_cast<long long>(t) * kQ + i] = LDR(a, src, i, t);
   } else {
     double drho = 0, jx = 0, jy = 0, jz = 0;
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
-      const double v = LD(src, a.qs, i, slot, a.inv_scale);
+      const double v = LDR(a, src, i, t);
       drho += v; jx += cx(i) * v; jy += cy(i) * v; jz += cz(i) * v;
     }
     const double rho = 1.0 + drho;
@@ -1144,6 +1200,15 @@ cudaError_t launch_step_pair(const StepArgs& a, cudaStream_t s) {
     e = launch_chain(k_step_pair<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
+// AA order: the step from the natural layout (reversed = false), or the one
+// from the reversed layout.
+template <typename T>
+cudaError_t launch_step_aa(const StepArgs& a, bool reversed, cudaStream_t s) {
+  const cudaError_t e = reversed
+      ? launch_chain(k_step_aa_local<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a)
+      : launch_chain(k_step_aa_pull<T>, dim3(grid_for(a.ncore)), dim3(kThreads), 0, s, a);
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
 // Paired kernel: even n (aligned pairs), n^3 < 2^31.
 bool pair_step_eligible(int n) { return n >= 4 && (n % 2) == 0 && n <= 1024; }
 
@@ -1261,6 +1326,7 @@ cudaError_t launch_cr_update(double* avg, const double* part, int nparts, long l
 #define OCTLB_INST(T)                                                                              \
   template cudaError_t launch_step<T>(const StepArgs&, bool, bool, bool, cudaStream_t);            \
   template cudaError_t launch_step_pair<T>(const StepArgs&, cudaStream_t);                         \
+  template cudaError_t launch_step_aa<T>(const StepArgs&, bool, cudaStream_t);                     \
   template cudaError_t launch_step_near<T>(const StepArgs&, const NearTables&, cudaStream_t);       \
   template cudaError_t launch_add_force<T>(const StepArgs&, T*, const float*, cudaStream_t);         \
   template cudaError_t launch_step_map<T>(const StepArgs&, const NearTables&, bool, bool, int, bool, cudaStream_t); \

@@ -165,6 +165,9 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
       CK(launch_step_cr<T>(a, L.near, links, L.has_flags, ctx->stream));
       ctx->launch_count += 1 + (L.near.n > 0 ? 1 : 0);
     }
+  } else if (L.aa) {
+    // AA order: cur is the layout (1: reversed), both buffers the same memory
+    CK(launch_step_aa<T>(a, L.cur == 1, ctx->stream));
   } else if (L.use_bulk) {
     CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
   } else if (L.use_pair) {
@@ -286,6 +289,10 @@ int validate(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p) {
   if (!(p->omega > 0.0 && p->omega < 2.0)) return fail(ctx, OCTLB_EINVAL, "omega must lie in (0, 2)");
   if (p->coupler_mode != OCTLB_COUPLER_REFERENCE && p->coupler_mode != OCTLB_COUPLER_PHYSICAL)
     return fail(ctx, OCTLB_EINVAL, "unknown coupler mode");
+  if (p->stream_order != OCTLB_ORDER_AB && p->stream_order != OCTLB_ORDER_AA)
+    return fail(ctx, OCTLB_EINVAL, "unknown stream order");
+  if (p->stream_order == OCTLB_ORDER_AA && (!t->periodic || p->drag))
+    return fail(ctx, OCTLB_EINVAL, "AA stream order needs a uniform periodic box without drag");
   for (int l = 0; l < 32 && p->coupler_mode == OCTLB_COUPLER_PHYSICAL; ++l)
     if (p->omega_level[l] != 0.0 && !(p->omega_level[l] > 0.0 && p->omega_level[l] < 2.0))
       return fail(ctx, OCTLB_EINVAL, "omega_level must be 0 or lie in (0, 2)");
@@ -1112,8 +1119,15 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
         return fail(ctx, OCTLB_EINVAL, "internal: flags required");
     }
 
-    // allocations and uploads
-    for (int k = 0; k < 2; ++k) CK(L.buf[k].alloc(static_cast<size_t>(L.nslots) * kQ * sizeof(T)));
+    // allocations and uploads; AA order: one population buffer, the second
+    // an alias of it (the step kernels update it in place)
+    L.aa = ctx->stream_order == OCTLB_ORDER_AA;
+    if (L.aa && !(ctx->periodic && !L.has_flags && L.nblk == 1 && n % 2 == 0 && !ctx->comm))
+      return fail(ctx, OCTLB_EINVAL,
+                  "AA stream order needs a uniform periodic box (one all-kBulk block, even n) in one context");
+    CK(L.buf[0].alloc(static_cast<size_t>(L.nslots) * kQ * sizeof(T)));
+    if (L.aa) L.buf[1].alias(L.buf[0]);
+    else CK(L.buf[1].alloc(static_cast<size_t>(L.nslots) * kQ * sizeof(T)));
     if (L.has_flags) CK(upload(L.flags, flags));
     CK(upload(L.link_idx, lidx));
     CK(upload(L.link_rec, lrec));
@@ -1904,6 +1918,7 @@ int gather_impl(octlb_ctx* ctx, double* pops, double* rho, double* u) {
     if (mode == 1) CK(du.reserve(bytes1));
     StepArgs a = L.args;
     a.src = L.buf[L.cur].p;
+    a.aa_rev = L.aa && L.cur;
     CK(launch_gather<T>(a, d.as<double>(), du.as<double>(), mode, ctx->stream));
     if (mode == 1)  // the FD pass's Dirichlet cells: the fields of their rewritten rows
       if (int rc = fd_fix_fields(ctx, L, d.as<double>(), du.as<double>())) return rc;
@@ -1956,6 +1971,7 @@ int scatter_impl(octlb_ctx* ctx, const double* in) {
     a.dst = L.buf[L.cur].p;
     CK(launch_scatter<T>(a, d.as<double>(), a.cr_part ? ctx->cr_near : 0, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (L.aa) L.cur = 0;  // the natural layout again
   }
   return OCTLB_OK;
 }
@@ -1991,6 +2007,7 @@ int scatter_eq_impl(octlb_ctx* ctx, const double* rho, const double* u) {
     a.dst = L.buf[L.cur].p;
     CK(launch_scatter_eq<T>(a, dr, a.cr_part ? ctx->cr_near : 0, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (L.aa) L.cur = 0;  // the natural layout again
   }
   return OCTLB_OK;
 }
@@ -2002,6 +2019,7 @@ int audit_impl(octlb_ctx* ctx, double out[4]) {
     if (L.nblk == 0) continue;
     StepArgs a = L.args;
     a.src = L.buf[L.cur].p;
+    a.aa_rev = L.aa && L.cur;
     DevBuf part;
     CK(part.alloc(audit_partials(a) * 5 * sizeof(double)));
     CK(launch_audit<T>(a, part.as<double>(), ctx->audit_out.as<double>(), ctx->stream));
@@ -2058,6 +2076,7 @@ static int create_common(const octlb_tables* t, const octlb_params* p, const dou
   if (t->bounds) ctx->bounds.assign(t->bounds, t->bounds + 6 * static_cast<size_t>(t->n_blocks));
   ctx->precision = p->precision;
   ctx->stream_mode = p->stream_mode;
+  ctx->stream_order = p->stream_order;
   ctx->periodic = t->periodic;
   ctx->drag = p->drag;
   ctx->omega = p->omega;
@@ -2158,6 +2177,7 @@ int octlb_gpu_adjoint(octlb_ctx* ctx, const octlb_adj_params* p, double* objecti
     return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates the reference coupler mode (one global tau)");
   if (ctx->fd_on) return fail(ctx, OCTLB_EINVAL, "the adjoint does not differentiate the fd boundary pass");
   if (ctx->const_rho) return fail(ctx, OCTLB_EINVAL, "the adjoint differentiates the BGK collide, not ConstRhoBGK");
+  if (ctx->stream_order != OCTLB_ORDER_AB) return fail(ctx, OCTLB_EINVAL, "the adjoint records two-buffer (AB) steps");
   return adjoint_impl<float>(ctx, p, objective, grad, grad_force);
 }
 
@@ -2165,6 +2185,8 @@ int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on) {
   if (!ctx) return OCTLB_EINVAL;
   if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
   if (ctx->comm && on) return fail(ctx, OCTLB_EINVAL, "ConstRhoBGK is built for one context, not rank contexts");
+  if (ctx->stream_order != OCTLB_ORDER_AB && on)
+    return fail(ctx, OCTLB_EINVAL, "ConstRhoBGK runs with the two-buffer (AB) stream order");
   if (ctx->fd_on && on)
     return fail(ctx, OCTLB_ESTATE, "ConstRhoBGK is chosen before octlb_gpu_set_fd_boundary");
   for (int c : ctx->counters_collide)
@@ -2240,6 +2262,8 @@ int octlb_gpu_synchronize(octlb_ctx* ctx) {
 
 int octlb_gpu_set_body_force(octlb_ctx* ctx, const double* force) {
   if (!ctx) return OCTLB_EINVAL;
+  if (force && ctx->stream_order != OCTLB_ORDER_AB)
+    return fail(ctx, OCTLB_EINVAL, "a body force needs the two-buffer (AB) stream order");
   CK(cudaStreamSynchronize(ctx->stream));
   clear_graphs(ctx);  // the captured launch sequence changes
   const long long n3 = static_cast<long long>(ctx->n) * ctx->n * ctx->n;
@@ -2518,7 +2542,7 @@ __global__ void __launch_bounds__(256) k_audit_noalloc(const StepArgs a, double*
     bool finite = true;
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
-      const float v = Store<T>::ld(src + i * a.qs + slot, a.inv_scale);
+      const float v = Store<T>::ld(src + (a.aa_rev ? aa_rev_slot(a, i, t) : i * a.qs + slot), a.inv_scale);
       finite = finite && isfinite(v);
       drho += v; jx += cx(i) * static_cast<double>(v);
       jy += cy(i) * static_cast<double>(v); jz += cz(i) * static_cast<double>(v);
@@ -2568,6 +2592,7 @@ int audit_noalloc_impl(octlb_ctx* ctx, double* scratch, double out[4]) {
     if (L.nblk == 0) continue;
     StepArgs a = L.args;
     a.src = L.buf[L.cur].p;
+    a.aa_rev = L.aa && L.cur;
     const int nrows = static_cast<int>((a.ncore + kNoAllocCellsPerCta - 1) / kNoAllocCellsPerCta);
     k_audit_noalloc<T><<<nrows, 256, 0, ctx->stream>>>(a, scratch);
     CK(cudaGetLastError());

@@ -43,6 +43,7 @@ cudaError_t launch_step_map_nc(const StepArgs&, const NearTables&, bool, bool, c
 template <typename T>
 cudaError_t launch_step_nc(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
 template <typename T> cudaError_t launch_collide_cr(const StepArgs&, cudaStream_t);
+template <typename T> cudaError_t launch_step_aa(const StepArgs&, bool, cudaStream_t);
 cudaError_t launch_cr_update(double*, const double*, int, long long, const double*, int, long long, cudaStream_t);
 uint32_t cr_core_parts(const StepArgs& a);
 uint32_t cr_near_parts(const NearTables& nt);
@@ -75,13 +76,23 @@ inline thread_local bool g_dry_run = false;
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  bool owned = true;        // false: an alias of another buffer (not freed here)
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
-  ~DevBuf() { if (p) cudaFree(p); }
+  DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes), owned(o.owned) { o.p = nullptr; o.bytes = 0; }
+  ~DevBuf() { if (p && owned) cudaFree(p); }
+  // The same memory as o, which keeps it.
+  void alias(const DevBuf& o) {
+    if (p && owned) cudaFree(p);
+    p = o.p;
+    bytes = o.bytes;
+    owned = false;
+  }
   cudaError_t alloc(size_t b) {
-    if (p) { cudaFree(p); p = nullptr; }
+    if (p && owned) cudaFree(p);
+    p = nullptr;
+    owned = true;
     bytes = b;
     if (g_dry_run) return cudaSuccess;
     if (b == 0) return cudaSuccess;
@@ -96,8 +107,10 @@ struct DevBuf {
   // Capacity of at least b bytes, kept across calls and not zero-filled:
   // staging that every use overwrites before it is read.
   cudaError_t reserve(size_t b) {
-    if (p && bytes >= b) return cudaSuccess;
-    if (p) { cudaFree(p); p = nullptr; }
+    if (p && owned && bytes >= b) return cudaSuccess;
+    if (p && owned) cudaFree(p);
+    p = nullptr;
+    owned = true;
     bytes = b;
     if (g_dry_run || b == 0) return cudaSuccess;
     return cudaMalloc(&p, b);
@@ -158,6 +171,7 @@ struct Level {
   bool use_bulk = false;            // pipelined bulk-copy step (periodic block)
   bool use_pair = false;            // two-cells-per-thread step (periodic block)
   bool use_map = false;             // slot-map step (forest level)
+  bool aa = false;                  // AA stream order: buf[1] aliases buf[0], cur = layout parity
   int bulk_grid = 0;
   DevBuf body_force;                // [3][ncore] float, or empty
   bool has_force = false;
@@ -327,6 +341,7 @@ struct octlb_ctx {
   // from its step, then cr_pparts from the prolongation into it.  cr_multi:
   // levels above cr_level exist; their steps only stream, and each collides
   // (k_collide_cr) once its coupling is done.
+  int stream_order = 0;             // OCTLB_ORDER_AB or OCTLB_ORDER_AA
   bool const_rho = false, cr_multi = false;
   DevBuf cr_avg, cr_part;
   int cr_level = -1, cr_nparts = 0, cr_near = 0, cr_pparts = 0;

@@ -62,7 +62,22 @@ struct StepArgs {
   int wrap_lo, wrap_hi;
   unsigned long long wait_ns; // limit of every bounded device wait
   int stall_first_row;      // test of the bounded wait: CTA 0 never issues its first row
+  // Readers of an AA-order box after an odd number of steps: population i of
+  // cell x sits in plane opp(i) at the periodic neighbour x + c_i.
+  int aa_rev;
 };
+
+// AA-order box after an odd number of steps: the slot holding population i
+// of core slot t, in plane opp(i) -- the periodic neighbour t + c_i of the
+// single block.
+__device__ __forceinline__ long long aa_rev_slot(const StepArgs& a, int i, uint32_t t) {
+  const uint32_t n = a.n;
+  const uint32_t x = a.div_n2.div(t), r = t - x * n * n, y = a.div_n.div(r), z = r - y * n;
+  const uint32_t xs = cx(i) > 0 ? (x + 1 == n ? 0 : x + 1) : (cx(i) < 0 ? (x == 0 ? n - 1 : x - 1) : x);
+  const uint32_t ys = cy(i) > 0 ? (y + 1 == n ? 0 : y + 1) : (cy(i) < 0 ? (y == 0 ? n - 1 : y - 1) : y);
+  const uint32_t zs = cz(i) > 0 ? (z + 1 == n ? 0 : z + 1) : (cz(i) < 0 ? (z == 0 ? n - 1 : z - 1) : z);
+  return static_cast<long long>(opp(i)) * a.qs + (static_cast<long long>(xs) * n + ys) * n + zs;
+}
 
 // Cells flagged kFlagNear with the link rule resolved on the host: for near
 // cell k and direction i (arrays [kQ][n]), the slot whose population i the

@@ -134,3 +134,79 @@ def test_fp16_four_cell_step_equals_paired_step(ob, monkeypatch):
         out.append(lat.get_populations())
         lat.close()
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("prec,launch", [("fp32", "graph"), ("fp16", "graph"), ("fp32", "direct")])
+def test_aa_order_equals_ab_order(ob, prec, launch, monkeypatch):
+    """The one-buffer AA stream order (a step that pulls from and writes back
+    to the neighbours, then one on the cell's own slots, alternating) and the
+    two-buffer AB order give bitwise equal populations, fields and audits
+    after odd step counts (reversed layout) and even ones (natural layout),
+    through captured graphs and direct launches, and after set_populations
+    while the AA buffer is in the reversed layout."""
+    from octlb_b200 import cases
+    if launch == "direct":
+        monkeypatch.setenv("OCTLB_NO_GRAPH", "1")
+    mesh, init, info = cases.tgv_periodic(64, u0=0.05, tau=0.55)
+    ab = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec), init_pops=init)
+    aa = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec), init_pops=init, stream_order=ob.ORDER_AA)
+    for k in (1, 6, 3):          # after 1, 7 and 10 steps
+        ab.advance(k)
+        aa.advance(k)
+        assert np.array_equal(aa.get_populations(), ab.get_populations()), k
+        ra, ua = aa.get_fields()
+        rb, ub = ab.get_fields()
+        assert np.array_equal(ra, rb) and np.array_equal(ua, ub), k
+        assert np.array_equal(aa.audit(), ab.audit()), k
+    aa.advance(1)
+    ab.advance(1)                # 11 steps: reversed layout
+    p = ab.get_populations()
+    aa.set_populations(p)
+    ab.set_populations(p)
+    aa.advance(5)
+    ab.advance(5)
+    assert np.array_equal(aa.get_populations(), ab.get_populations())
+    c_aa, s_aa = aa.counters()
+    c_ab, s_ab = ab.counters()
+    assert c_aa == c_ab and s_aa == s_ab
+    ab.close()
+    aa.close()
+
+
+def test_aa_order_holds_one_buffer(ob):
+    """AA keeps one population buffer: creating the 128^3 FP32 box takes about
+    half the device memory of the AB order (2 x 159 MB)."""
+    import torch
+    from octlb_b200 import cases
+    mesh, init, info = cases.tgv_periodic(128, u0=0.05, tau=0.55)
+    used = {}
+    for order in (ob.ORDER_AB, ob.ORDER_AA):
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        lat = ob.GpuLattice(mesh, info["omega"], stream_order=order)
+        torch.cuda.synchronize()
+        used[order] = free0 - torch.cuda.mem_get_info()[0]
+        lat.close()
+    one = 128 ** 3 * 19 * 4
+    assert used[ob.ORDER_AB] >= 2 * one
+    assert used[ob.ORDER_AA] < used[ob.ORDER_AB] - 0.9 * one
+
+
+def test_aa_order_refusals(ob):
+    """AA runs the uniform periodic box only, without body force or
+    ConstRhoBGK (OCTLB_EINVAL)."""
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=16, n=8, lid=0.1, tau=0.6)
+    with pytest.raises(ob.OctlbError):
+        ob.GpuLattice(mesh, info["omega"], stream_order=ob.ORDER_AA)
+    mesh, init, info = cases.tgv_periodic(32, u0=0.05, tau=0.55)
+    with pytest.raises(ob.OctlbError):
+        ob.GpuLattice(mesh, info["omega"], stream_order=7)
+    lat = ob.GpuLattice(mesh, info["omega"], init_pops=init, stream_order=ob.ORDER_AA)
+    with pytest.raises(ob.OctlbError):
+        lat.set_body_force(np.zeros((1, 32 ** 3, 3)))
+    with pytest.raises(ob.OctlbError):
+        lat.set_const_rho(True)
+    lat.advance(3)
+    assert np.all(np.isfinite(lat.get_populations()))
+    lat.close()

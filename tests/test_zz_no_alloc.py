@@ -30,13 +30,14 @@ def close(a, b):
     return np.all(np.abs(a - b) <= TOL * max(1.0, np.max(np.abs(b))))
 
 
-@pytest.mark.parametrize("case", ["tgv_fp32", "tgv_fp16", "amr_cavity"])
+@pytest.mark.parametrize("case", ["tgv_fp32", "tgv_fp16", "tgv_fp32_aa", "amr_cavity"])
 def test_audit_noalloc_matches_audit_twice(ob, case):
     from octlb_b200 import cases
     if case.startswith("tgv"):
         mesh, init, info = cases.tgv_periodic(64, u0=0.05, tau=0.55)
-        prec = ob.FP32 if case == "tgv_fp32" else ob.FP16_SHIFTED
-        lat = ob.GpuLattice(mesh, info["omega"], precision=prec, init_pops=init)
+        prec = ob.FP16_SHIFTED if case == "tgv_fp16" else ob.FP32
+        order = ob.ORDER_AA if case.endswith("_aa") else ob.ORDER_AB   # AA: 7 steps leave the reversed layout
+        lat = ob.GpuLattice(mesh, info["omega"], precision=prec, init_pops=init, stream_order=order)
     else:
         mesh, init, info = cases.cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=8)
         lat = ob.GpuLattice(mesh, info["omega"], init_pops=init)
