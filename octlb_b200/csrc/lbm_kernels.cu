@@ -589,6 +589,73 @@ __global__ void __launch_bounds__(kThreads) k_step_aa_pull(const StepArgs a) {
   for (int k = 0; k < kQ; ++k) Store<T>::st(pops + at[k], f[opp(k)], 1.0f);
 }
 
+// The same step with two z cells per thread and 2-element accesses (n a
+// multiple of 64: a warp's 32 threads cover 64 cells of one z row).  The
+// slots a thread owns for a direction with c_z != 0 sit one cell off its
+// aligned pair, so each thread stores the aligned pair of its second slot and
+// the next lane's first (a warp shuffle); the warp's edge slots, whose
+// partner lies in another warp, take scalar stores.  Every slot is still
+// written once, by the thread that read it or by its warp neighbour after
+// the shuffle that depends on that read.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_step_aa_pull2(const StepArgs a) {
+  pdl_wait();
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  const uint32_t n = a.n, half = n >> 1;
+  if (t >= a.ncore / 2) return;  // whole warps (n^3 / 2 is a multiple of 32)
+  const int lane = threadIdx.x & 31;
+  const uint32_t row = a.div_n.div(2 * t);
+  const uint32_t z = (t - row * half) * 2;
+  const uint32_t x = a.div_n.div(row), y = row - x * n;
+  const uint32_t xm = x == 0 ? n - 1 : x - 1, xp = x == n - 1 ? 0 : x + 1;
+  const uint32_t ym = y == 0 ? n - 1 : y - 1, yp = y == n - 1 ? 0 : y + 1;
+  const uint32_t zm2 = z == 0 ? n - 2 : z - 2, zp2 = z + 2 == n ? 0 : z + 2;
+  T* pops = static_cast<T*>(a.dst);  // == a.src
+  float f0[kQ], f1[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const uint32_t sx = cx(i) == 1 ? xm : (cx(i) == -1 ? xp : x);
+    const uint32_t sy = cy(i) == 1 ? ym : (cy(i) == -1 ? yp : y);
+    const T* r = pops + i * a.qs + (static_cast<long long>(sx) * n + sy) * n;
+    if (cz(i) == 0) {
+      Pair<T>::ld(r + z, a.inv_scale, f0[i], f1[i]);
+    } else if (cz(i) == 1) {  // cells z, z+1 pull z-1, z
+      float u, v, w;
+      Pair<T>::ld(r + zm2, a.inv_scale, u, v);
+      Pair<T>::ld(r + z, a.inv_scale, f1[i], w);
+      f0[i] = v;
+    } else {                  // cells z, z+1 pull z+1, z+2
+      float u, w;
+      Pair<T>::ld(r + z, a.inv_scale, u, f0[i]);
+      Pair<T>::ld(r + zp2, a.inv_scale, f1[i], w);
+    }
+  }
+  bgk<kBgkCorrect<T>>(f0, a.omega, a.scale, a.inv_scale);
+  bgk<kBgkCorrect<T>>(f1, a.omega, a.scale, a.inv_scale);
+  // slot k read by cell z (own[0]) gets g_opp(k) of cell z, the one read by
+  // cell z+1 (own[1]) that of cell z+1
+#pragma unroll
+  for (int k = 0; k < kQ; ++k) {
+    const uint32_t sx = cx(k) == 1 ? xm : (cx(k) == -1 ? xp : x);
+    const uint32_t sy = cy(k) == 1 ? ym : (cy(k) == -1 ? yp : y);
+    T* r = pops + k * a.qs + (static_cast<long long>(sx) * n + sy) * n;
+    const float o0 = f0[opp(k)], o1 = f1[opp(k)];
+    if (cz(k) == 0) {         // own slots z, z+1: the aligned pair
+      Pair<T>::st(r + z, o0, o1, a.scale);
+    } else if (cz(k) == 1) {  // own slots z-1, z: pair (z, z+1) = (own[1], next lane's own[0])
+      const float nx = __shfl_down_sync(0xffffffffu, o0, 1);
+      if (lane < 31) Pair<T>::st(r + z, o1, nx, a.scale);
+      else Store<T>::st(r + z, o1, 1.0f);
+      if (lane == 0) Store<T>::st(r + (zm2 + 1), o0, 1.0f);
+    } else {                  // own slots z+1, z+2: pair (z, z+1) = (previous lane's own[1], own[0])
+      const float pv = __shfl_up_sync(0xffffffffu, o1, 1);
+      if (lane > 0) Pair<T>::st(r + z, pv, o0, a.scale);
+      else Store<T>::st(r + (z + 1), o0, 1.0f);
+      if (lane == 31) Store<T>::st(r + zp2, o1, 1.0f);
+    }
+  }
+}
+
 // From the reversed layout: population i of cell x (streamed) is the value
 // in plane opp(i) at x itself; collide, and write plane i at x -- the
 // natural layout again.  Two z cells per thread with 2-element accesses.
@@ -1204,9 +1271,11 @@ cudaError_t launch_step_pair(const StepArgs& a, cudaStream_t s) {
 // from the reversed layout.
 template <typename T>
 cudaError_t launch_step_aa(const StepArgs& a, bool reversed, cudaStream_t s) {
-  const cudaError_t e = reversed
-      ? launch_chain(k_step_aa_local<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a)
-      : launch_chain(k_step_aa_pull<T>, dim3(grid_for(a.ncore)), dim3(kThreads), 0, s, a);
+  // pull step: two cells per thread where a warp covers 64 cells of a row
+  const cudaError_t e = reversed ? launch_chain(k_step_aa_local<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a)
+                        : a.n % 64 == 0 && std::getenv("OCTLB_AA_SCALAR") == nullptr
+                            ? launch_chain(k_step_aa_pull2<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a)
+                            : launch_chain(k_step_aa_pull<T>, dim3(grid_for(a.ncore)), dim3(kThreads), 0, s, a);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 // Paired kernel: even n (aligned pairs), n^3 < 2^31.
