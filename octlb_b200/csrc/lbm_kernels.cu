@@ -552,6 +552,98 @@ __global__ void __launch_bounds__(kThreads) k_step_quad_h(const StepArgs a) {
   for (int i = 0; i < kQ; ++i) st4h(o + i * a.qs, f0[i], f1[i], f2[i], f3[i]);
 }
 
+// FP16-shifted AA steps with four z cells per thread and 8-byte accesses,
+// as k_step_quad_h (n a multiple of 128 for the pull step: a warp's 32
+// threads cover 128 cells of one z row; the local step needs n % 4 == 0).
+// The pull step's write-back follows k_step_aa_pull2 with quads: for a
+// direction with c_z != 0 the thread's four slots sit one cell off its
+// aligned quad, which takes three of them and one of the neighbour lane's.
+template <int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) k_step_aa_pull_h(const StepArgs a) {
+  pdl_wait();
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  const uint32_t n = a.n, q4 = n >> 2;
+  if (t >= a.ncore / 4) return;  // whole warps
+  const int lane = threadIdx.x & 31;
+  const uint32_t row = a.div_n.div(4 * t);
+  const uint32_t z = (t - row * q4) * 4;
+  const uint32_t x = a.div_n.div(row), y = row - x * n;
+  const uint32_t xm = x == 0 ? n - 1 : x - 1, xp = x == n - 1 ? 0 : x + 1;
+  const uint32_t ym = y == 0 ? n - 1 : y - 1, yp = y == n - 1 ? 0 : y + 1;
+  const uint32_t zm1 = z == 0 ? n - 1 : z - 1, zp4 = z + 4 == n ? 0 : z + 4;
+  __half* pops = static_cast<__half*>(a.dst);  // == a.src
+  float f0[kQ], f1[kQ], f2[kQ], f3[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) {
+    const uint32_t sx = cx(i) == 1 ? xm : (cx(i) == -1 ? xp : x);
+    const uint32_t sy = cy(i) == 1 ? ym : (cy(i) == -1 ? yp : y);
+    const __half* r = pops + i * a.qs + (static_cast<long long>(sx) * n + sy) * n;
+    if (cz(i) == 0) {
+      ld4h(r + z, f0[i], f1[i], f2[i], f3[i]);
+    } else if (cz(i) == 1) {  // cells z..z+3 pull z-1..z+2
+      float w;
+      ld4h(r + z, f1[i], f2[i], f3[i], w);
+      f0[i] = __half2float(r[zm1]);
+    } else {                  // cells z..z+3 pull z+1..z+4
+      float w;
+      ld4h(r + z, w, f0[i], f1[i], f2[i]);
+      f3[i] = __half2float(r[zp4]);
+    }
+  }
+  bgk<false>(f0, a.omega, a.scale, a.inv_scale);
+  bgk<false>(f1, a.omega, a.scale, a.inv_scale);
+  bgk<false>(f2, a.omega, a.scale, a.inv_scale);
+  bgk<false>(f3, a.omega, a.scale, a.inv_scale);
+#pragma unroll
+  for (int k = 0; k < kQ; ++k) {
+    const uint32_t sx = cx(k) == 1 ? xm : (cx(k) == -1 ? xp : x);
+    const uint32_t sy = cy(k) == 1 ? ym : (cy(k) == -1 ? yp : y);
+    __half* r = pops + k * a.qs + (static_cast<long long>(sx) * n + sy) * n;
+    const int o = opp(k);
+    const float o0 = f0[o], o1 = f1[o], o2 = f2[o], o3 = f3[o];
+    if (cz(k) == 0) {         // own slots z..z+3: the aligned quad
+      st4h(r + z, o0, o1, o2, o3);
+    } else if (cz(k) == 1) {  // own z-1..z+2: quad (z..z+3) = (own[1..3], next lane's own[0])
+      const float nx = __shfl_down_sync(0xffffffffu, o0, 1);
+      if (lane < 31) {
+        st4h(r + z, o1, o2, o3, nx);
+      } else {
+        r[z] = __float2half_rn(o1);
+        r[z + 1] = __float2half_rn(o2);
+        r[z + 2] = __float2half_rn(o3);
+      }
+      if (lane == 0) r[zm1] = __float2half_rn(o0);
+    } else {                  // own z+1..z+4: quad (z..z+3) = (previous lane's own[3], own[0..2])
+      const float pv = __shfl_up_sync(0xffffffffu, o3, 1);
+      if (lane > 0) {
+        st4h(r + z, pv, o0, o1, o2);
+      } else {
+        r[z + 1] = __float2half_rn(o0);
+        r[z + 2] = __float2half_rn(o1);
+        r[z + 3] = __float2half_rn(o2);
+      }
+      if (lane == 31) r[zp4] = __float2half_rn(o3);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_step_aa_local_h(const StepArgs a) {
+  pdl_wait();
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  if (t >= a.ncore / 4) return;
+  __half* pops = static_cast<__half*>(a.dst);  // == a.src
+  const long long s = 4ll * t;
+  float f0[kQ], f1[kQ], f2[kQ], f3[kQ];
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) ld4h(pops + opp(i) * a.qs + s, f0[i], f1[i], f2[i], f3[i]);
+  bgk<false>(f0, a.omega, a.scale, a.inv_scale);
+  bgk<false>(f1, a.omega, a.scale, a.inv_scale);
+  bgk<false>(f2, a.omega, a.scale, a.inv_scale);
+  bgk<false>(f3, a.omega, a.scale, a.inv_scale);
+#pragma unroll
+  for (int i = 0; i < kQ; ++i) st4h(pops + i * a.qs + s, f0[i], f1[i], f2[i], f3[i]);
+}
+
 // AA stream order on a uniform periodic box: one population buffer, updated
 // in place by two alternating steps (Bailey et al. 2009).  Both pull the
 // same values as k_step_pair and collide with the same bgk() call, so the
@@ -1271,11 +1363,24 @@ cudaError_t launch_step_pair(const StepArgs& a, cudaStream_t s) {
 // from the reversed layout.
 template <typename T>
 cudaError_t launch_step_aa(const StepArgs& a, bool reversed, cudaStream_t s) {
-  // pull step: two cells per thread where a warp covers 64 cells of a row
-  const cudaError_t e = reversed ? launch_chain(k_step_aa_local<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a)
-                        : a.n % 64 == 0 && std::getenv("OCTLB_AA_SCALAR") == nullptr
-                            ? launch_chain(k_step_aa_pull2<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a)
-                            : launch_chain(k_step_aa_pull<T>, dim3(grid_for(a.ncore)), dim3(kThreads), 0, s, a);
+  // FP16: four cells per thread (the pull step where a warp covers 128 cells
+  // of a row); otherwise the pull step takes two cells per thread where a
+  // warp covers 64 cells of a row, one elsewhere (or with OCTLB_AA_SCALAR=1)
+  const bool scalar = std::getenv("OCTLB_AA_SCALAR") != nullptr;
+  const bool h = std::is_same<T, __half>::value && !scalar;
+  cudaError_t e;
+  if (reversed) {
+    e = h && a.n % 4 == 0 ? launch_chain(k_step_aa_local_h, dim3(grid_for(a.ncore / 4)), dim3(kThreads), 0, s, a)
+                          : launch_chain(k_step_aa_local<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a);
+  } else if (h && a.n % 128 == 0) {
+    const char* mb = std::getenv("OCTLB_AA_H_MINB");
+    e = mb && mb[0] == '2' ? launch_chain(k_step_aa_pull_h<2>, dim3(grid_for(a.ncore / 4)), dim3(kThreads), 0, s, a)
+                           : launch_chain(k_step_aa_pull_h<1>, dim3(grid_for(a.ncore / 4)), dim3(kThreads), 0, s, a);
+  } else if (a.n % 64 == 0 && !scalar) {
+    e = launch_chain(k_step_aa_pull2<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a);
+  } else {
+    e = launch_chain(k_step_aa_pull<T>, dim3(grid_for(a.ncore)), dim3(kThreads), 0, s, a);
+  }
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 // Paired kernel: even n (aligned pairs), n^3 < 2^31.

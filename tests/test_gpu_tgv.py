@@ -136,22 +136,23 @@ def test_fp16_four_cell_step_equals_paired_step(ob, monkeypatch):
     assert np.array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("prec,launch", [("fp32", "graph"), ("fp16", "graph"), ("fp32", "direct"),
-                                         ("fp16", "scalar")])
-def test_aa_order_equals_ab_order(ob, prec, launch, monkeypatch):
+@pytest.mark.parametrize("prec,launch,n", [("fp32", "graph", 64), ("fp16", "graph", 64), ("fp32", "direct", 64),
+                                           ("fp16", "scalar", 64), ("fp16", "graph", 128)])
+def test_aa_order_equals_ab_order(ob, prec, launch, n, monkeypatch):
     """The one-buffer AA stream order (a step that pulls from and writes back
     to the neighbours, then one on the cell's own slots, alternating) and the
     two-buffer AB order give bitwise equal populations, fields and audits
     after odd step counts (reversed layout) and even ones (natural layout),
     through captured graphs and direct launches, with the two-cell pull step
     and the one-cell one (OCTLB_AA_SCALAR=1), and after set_populations while
-    the AA buffer is in the reversed layout."""
+    the AA buffer is in the reversed layout.  FP16 at 128^3 takes the
+    four-cell pull step (a warp per 128-cell row)."""
     from octlb_b200 import cases
     if launch in ("direct", "scalar"):
         monkeypatch.setenv("OCTLB_NO_GRAPH", "1")
     if launch == "scalar":
         monkeypatch.setenv("OCTLB_AA_SCALAR", "1")
-    mesh, init, info = cases.tgv_periodic(64, u0=0.05, tau=0.55)
+    mesh, init, info = cases.tgv_periodic(n, u0=0.05, tau=0.55)
     ab = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec), init_pops=init)
     aa = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec), init_pops=init, stream_order=ob.ORDER_AA)
     for k in (1, 6, 3):          # after 1, 7 and 10 steps
