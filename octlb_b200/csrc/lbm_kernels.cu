@@ -18,6 +18,7 @@
 // stream (time_loop.h:201-217) is therefore a ghost fill followed by k_step.
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <type_traits>
 
 #include "lbm_device.cuh"
@@ -689,8 +690,8 @@ __global__ void __launch_bounds__(kThreads) k_step_aa_pull(const StepArgs a) {
 // partner lies in another warp, take scalar stores.  Every slot is still
 // written once, by the thread that read it or by its warp neighbour after
 // the shuffle that depends on that read.
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_step_aa_pull2(const StepArgs a) {
+template <typename T, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) k_step_aa_pull2(const StepArgs a) {
   pdl_wait();
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   const uint32_t n = a.n, half = n >> 1;
@@ -1363,23 +1364,26 @@ cudaError_t launch_step_pair(const StepArgs& a, cudaStream_t s) {
 // from the reversed layout.
 template <typename T>
 cudaError_t launch_step_aa(const StepArgs& a, bool reversed, cudaStream_t s) {
-  // FP16: four cells per thread (the pull step where a warp covers 128 cells
-  // of a row); otherwise the pull step takes two cells per thread where a
-  // warp covers 64 cells of a row, one elsewhere (or with OCTLB_AA_SCALAR=1)
-  const bool scalar = std::getenv("OCTLB_AA_SCALAR") != nullptr;
-  const bool h = std::is_same<T, __half>::value && !scalar;
+  // The pull step's form: OCTLB_AA_PULL = scalar (one cell per thread), pair
+  // (two, n % 64 == 0) or quad (four, FP16, n % 128 == 0), with an optional
+  // CTAs-per-SM bound digit (pair2, pair3, quad1, quad2); the local step
+  // takes four FP16 cells per thread where n % 4 == 0, else two.
+  const char* env = std::getenv("OCTLB_AA_PULL");
+  const std::string v = env ? env : "scalar";
+  const bool half = std::is_same<T, __half>::value;
+  const uint32_t gq = grid_for(a.ncore / 4), gp = grid_for(a.ncore / 2), g1 = grid_for(a.ncore);
   cudaError_t e;
   if (reversed) {
-    e = h && a.n % 4 == 0 ? launch_chain(k_step_aa_local_h, dim3(grid_for(a.ncore / 4)), dim3(kThreads), 0, s, a)
-                          : launch_chain(k_step_aa_local<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a);
-  } else if (h && a.n % 128 == 0) {
-    const char* mb = std::getenv("OCTLB_AA_H_MINB");
-    e = mb && mb[0] == '2' ? launch_chain(k_step_aa_pull_h<2>, dim3(grid_for(a.ncore / 4)), dim3(kThreads), 0, s, a)
-                           : launch_chain(k_step_aa_pull_h<1>, dim3(grid_for(a.ncore / 4)), dim3(kThreads), 0, s, a);
-  } else if (a.n % 64 == 0 && !scalar) {
-    e = launch_chain(k_step_aa_pull2<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a);
+    e = half && a.n % 4 == 0 ? launch_chain(k_step_aa_local_h, dim3(gq), dim3(kThreads), 0, s, a)
+                             : launch_chain(k_step_aa_local<T>, dim3(gp), dim3(kThreads), 0, s, a);
+  } else if (half && a.n % 128 == 0 && v.rfind("quad", 0) == 0) {
+    e = v == "quad2" ? launch_chain(k_step_aa_pull_h<2>, dim3(gq), dim3(kThreads), 0, s, a)
+                     : launch_chain(k_step_aa_pull_h<1>, dim3(gq), dim3(kThreads), 0, s, a);
+  } else if (a.n % 64 == 0 && v.rfind("pair", 0) == 0) {
+    e = v == "pair3" ? launch_chain(k_step_aa_pull2<T, 3>, dim3(gp), dim3(kThreads), 0, s, a)
+                     : launch_chain(k_step_aa_pull2<T, 2>, dim3(gp), dim3(kThreads), 0, s, a);
   } else {
-    e = launch_chain(k_step_aa_pull<T>, dim3(grid_for(a.ncore)), dim3(kThreads), 0, s, a);
+    e = launch_chain(k_step_aa_pull<T>, dim3(g1), dim3(kThreads), 0, s, a);
   }
   return e != cudaSuccess ? e : cudaGetLastError();
 }

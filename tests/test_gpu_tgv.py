@@ -136,22 +136,23 @@ def test_fp16_four_cell_step_equals_paired_step(ob, monkeypatch):
     assert np.array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("prec,launch,n", [("fp32", "graph", 64), ("fp16", "graph", 64), ("fp32", "direct", 64),
-                                           ("fp16", "scalar", 64), ("fp16", "graph", 128)])
-def test_aa_order_equals_ab_order(ob, prec, launch, n, monkeypatch):
+@pytest.mark.parametrize("prec,launch,n,pull", [("fp32", "graph", 64, None), ("fp16", "graph", 64, None),
+                                                ("fp32", "direct", 64, "pair"), ("fp16", "direct", 64, "pair3"),
+                                                ("fp16", "graph", 128, "quad"), ("fp16", "graph", 128, "quad2")])
+def test_aa_order_equals_ab_order(ob, prec, launch, n, pull, monkeypatch):
     """The one-buffer AA stream order (a step that pulls from and writes back
     to the neighbours, then one on the cell's own slots, alternating) and the
     two-buffer AB order give bitwise equal populations, fields and audits
     after odd step counts (reversed layout) and even ones (natural layout),
-    through captured graphs and direct launches, with the two-cell pull step
-    and the one-cell one (OCTLB_AA_SCALAR=1), and after set_populations while
-    the AA buffer is in the reversed layout.  FP16 at 128^3 takes the
-    four-cell pull step (a warp per 128-cell row)."""
+    through captured graphs and direct launches, with each form of the pull
+    step (OCTLB_AA_PULL: one cell per thread, two with shuffled aligned
+    stores, four in FP16 where a warp covers a 128-cell row), and after
+    set_populations while the AA buffer is in the reversed layout."""
     from octlb_b200 import cases
-    if launch in ("direct", "scalar"):
+    if launch == "direct":
         monkeypatch.setenv("OCTLB_NO_GRAPH", "1")
-    if launch == "scalar":
-        monkeypatch.setenv("OCTLB_AA_SCALAR", "1")
+    if pull:
+        monkeypatch.setenv("OCTLB_AA_PULL", pull)
     mesh, init, info = cases.tgv_periodic(n, u0=0.05, tau=0.55)
     ab = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec), init_pops=init)
     aa = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec), init_pops=init, stream_order=ob.ORDER_AA)
