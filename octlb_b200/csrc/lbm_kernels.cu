@@ -556,11 +556,12 @@ __global__ void __launch_bounds__(kThreads) k_step_quad_h(const StepArgs a) {
 // FP16-shifted AA steps with four z cells per thread and 8-byte accesses,
 // as k_step_quad_h (n a multiple of 128 for the pull step: a warp's 32
 // threads cover 128 cells of one z row; the local step needs n % 4 == 0).
-// The pull step's write-back follows k_step_aa_pull2 with quads: for a
-// direction with c_z != 0 the thread's four slots sit one cell off its
-// aligned quad, which takes three of them and one of the neighbour lane's.
-template <int MINB>
-__global__ void __launch_bounds__(kThreads, MINB) k_step_aa_pull_h(const StepArgs a) {
+// The pull step writes back with aligned 8-byte stores: for a direction with
+// c_z != 0 the thread's four slots sit one cell off its aligned quad, which
+// takes three of them and one of the neighbour lane's (a warp shuffle that
+// depends on that lane's reads); the warp's edge slots, whose partner lies in
+// another warp, take 2-byte stores.  Every slot is still written once.
+__global__ void __launch_bounds__(kThreads, 2) k_step_aa_pull_h(const StepArgs a) {
   pdl_wait();
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
   const uint32_t n = a.n, q4 = n >> 2;
@@ -680,73 +681,6 @@ __global__ void __launch_bounds__(kThreads) k_step_aa_pull(const StepArgs a) {
   bgk<kBgkCorrect<T>>(f, a.omega, a.scale, a.inv_scale);
 #pragma unroll
   for (int k = 0; k < kQ; ++k) Store<T>::st(pops + at[k], f[opp(k)], 1.0f);
-}
-
-// The same step with two z cells per thread and 2-element accesses (n a
-// multiple of 64: a warp's 32 threads cover 64 cells of one z row).  The
-// slots a thread owns for a direction with c_z != 0 sit one cell off its
-// aligned pair, so each thread stores the aligned pair of its second slot and
-// the next lane's first (a warp shuffle); the warp's edge slots, whose
-// partner lies in another warp, take scalar stores.  Every slot is still
-// written once, by the thread that read it or by its warp neighbour after
-// the shuffle that depends on that read.
-template <typename T, int MINB>
-__global__ void __launch_bounds__(kThreads, MINB) k_step_aa_pull2(const StepArgs a) {
-  pdl_wait();
-  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
-  const uint32_t n = a.n, half = n >> 1;
-  if (t >= a.ncore / 2) return;  // whole warps (n^3 / 2 is a multiple of 32)
-  const int lane = threadIdx.x & 31;
-  const uint32_t row = a.div_n.div(2 * t);
-  const uint32_t z = (t - row * half) * 2;
-  const uint32_t x = a.div_n.div(row), y = row - x * n;
-  const uint32_t xm = x == 0 ? n - 1 : x - 1, xp = x == n - 1 ? 0 : x + 1;
-  const uint32_t ym = y == 0 ? n - 1 : y - 1, yp = y == n - 1 ? 0 : y + 1;
-  const uint32_t zm2 = z == 0 ? n - 2 : z - 2, zp2 = z + 2 == n ? 0 : z + 2;
-  T* pops = static_cast<T*>(a.dst);  // == a.src
-  float f0[kQ], f1[kQ];
-#pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    const uint32_t sx = cx(i) == 1 ? xm : (cx(i) == -1 ? xp : x);
-    const uint32_t sy = cy(i) == 1 ? ym : (cy(i) == -1 ? yp : y);
-    const T* r = pops + i * a.qs + (static_cast<long long>(sx) * n + sy) * n;
-    if (cz(i) == 0) {
-      Pair<T>::ld(r + z, a.inv_scale, f0[i], f1[i]);
-    } else if (cz(i) == 1) {  // cells z, z+1 pull z-1, z
-      float u, v, w;
-      Pair<T>::ld(r + zm2, a.inv_scale, u, v);
-      Pair<T>::ld(r + z, a.inv_scale, f1[i], w);
-      f0[i] = v;
-    } else {                  // cells z, z+1 pull z+1, z+2
-      float u, w;
-      Pair<T>::ld(r + z, a.inv_scale, u, f0[i]);
-      Pair<T>::ld(r + zp2, a.inv_scale, f1[i], w);
-    }
-  }
-  bgk<kBgkCorrect<T>>(f0, a.omega, a.scale, a.inv_scale);
-  bgk<kBgkCorrect<T>>(f1, a.omega, a.scale, a.inv_scale);
-  // slot k read by cell z (own[0]) gets g_opp(k) of cell z, the one read by
-  // cell z+1 (own[1]) that of cell z+1
-#pragma unroll
-  for (int k = 0; k < kQ; ++k) {
-    const uint32_t sx = cx(k) == 1 ? xm : (cx(k) == -1 ? xp : x);
-    const uint32_t sy = cy(k) == 1 ? ym : (cy(k) == -1 ? yp : y);
-    T* r = pops + k * a.qs + (static_cast<long long>(sx) * n + sy) * n;
-    const float o0 = f0[opp(k)], o1 = f1[opp(k)];
-    if (cz(k) == 0) {         // own slots z, z+1: the aligned pair
-      Pair<T>::st(r + z, o0, o1, a.scale);
-    } else if (cz(k) == 1) {  // own slots z-1, z: pair (z, z+1) = (own[1], next lane's own[0])
-      const float nx = __shfl_down_sync(0xffffffffu, o0, 1);
-      if (lane < 31) Pair<T>::st(r + z, o1, nx, a.scale);
-      else Store<T>::st(r + z, o1, 1.0f);
-      if (lane == 0) Store<T>::st(r + (zm2 + 1), o0, 1.0f);
-    } else {                  // own slots z+1, z+2: pair (z, z+1) = (previous lane's own[1], own[0])
-      const float pv = __shfl_up_sync(0xffffffffu, o1, 1);
-      if (lane > 0) Pair<T>::st(r + z, pv, o0, a.scale);
-      else Store<T>::st(r + (z + 1), o0, 1.0f);
-      if (lane == 31) Store<T>::st(r + zp2, o1, 1.0f);
-    }
-  }
 }
 
 // From the reversed layout: population i of cell x (streamed) is the value
@@ -1364,26 +1298,23 @@ cudaError_t launch_step_pair(const StepArgs& a, cudaStream_t s) {
 // from the reversed layout.
 template <typename T>
 cudaError_t launch_step_aa(const StepArgs& a, bool reversed, cudaStream_t s) {
-  // The pull step's form: OCTLB_AA_PULL = scalar (one cell per thread), pair
-  // (two, n % 64 == 0) or quad (four, FP16, n % 128 == 0), with an optional
-  // CTAs-per-SM bound digit (pair2, pair3, quad1, quad2); the local step
-  // takes four FP16 cells per thread where n % 4 == 0, else two.
+  // The local step takes four FP16 cells per thread where n % 4 == 0, else
+  // two.  The pull step takes four FP16 cells per thread where a warp covers
+  // a 128-cell row (n % 128 == 0; OCTLB_AA_PULL=scalar keeps one), else one:
+  // measured on the 256^3 box, one FP32 cell per thread (80 registers)
+  // beats two with shuffled aligned stores (128 registers), and four FP16
+  // cells bounded to two CTAs per SM beat one.
   const char* env = std::getenv("OCTLB_AA_PULL");
-  const std::string v = env ? env : "scalar";
+  const bool scalar = env && std::string(env) == "scalar";
   const bool half = std::is_same<T, __half>::value;
-  const uint32_t gq = grid_for(a.ncore / 4), gp = grid_for(a.ncore / 2), g1 = grid_for(a.ncore);
   cudaError_t e;
   if (reversed) {
-    e = half && a.n % 4 == 0 ? launch_chain(k_step_aa_local_h, dim3(gq), dim3(kThreads), 0, s, a)
-                             : launch_chain(k_step_aa_local<T>, dim3(gp), dim3(kThreads), 0, s, a);
-  } else if (half && a.n % 128 == 0 && v.rfind("quad", 0) == 0) {
-    e = v == "quad2" ? launch_chain(k_step_aa_pull_h<2>, dim3(gq), dim3(kThreads), 0, s, a)
-                     : launch_chain(k_step_aa_pull_h<1>, dim3(gq), dim3(kThreads), 0, s, a);
-  } else if (a.n % 64 == 0 && v.rfind("pair", 0) == 0) {
-    e = v == "pair3" ? launch_chain(k_step_aa_pull2<T, 3>, dim3(gp), dim3(kThreads), 0, s, a)
-                     : launch_chain(k_step_aa_pull2<T, 2>, dim3(gp), dim3(kThreads), 0, s, a);
+    e = half && a.n % 4 == 0 ? launch_chain(k_step_aa_local_h, dim3(grid_for(a.ncore / 4)), dim3(kThreads), 0, s, a)
+                             : launch_chain(k_step_aa_local<T>, dim3(grid_for(a.ncore / 2)), dim3(kThreads), 0, s, a);
+  } else if (half && a.n % 128 == 0 && !scalar) {
+    e = launch_chain(k_step_aa_pull_h, dim3(grid_for(a.ncore / 4)), dim3(kThreads), 0, s, a);
   } else {
-    e = launch_chain(k_step_aa_pull<T>, dim3(g1), dim3(kThreads), 0, s, a);
+    e = launch_chain(k_step_aa_pull<T>, dim3(grid_for(a.ncore)), dim3(kThreads), 0, s, a);
   }
   return e != cudaSuccess ? e : cudaGetLastError();
 }

@@ -137,17 +137,17 @@ def test_fp16_four_cell_step_equals_paired_step(ob, monkeypatch):
 
 
 @pytest.mark.parametrize("prec,launch,n,pull", [("fp32", "graph", 64, None), ("fp16", "graph", 64, None),
-                                                ("fp32", "direct", 64, "pair"), ("fp16", "direct", 64, "pair3"),
-                                                ("fp16", "graph", 128, "quad"), ("fp16", "graph", 128, "quad2")])
+                                                ("fp32", "direct", 64, None), ("fp16", "graph", 128, None),
+                                                ("fp16", "direct", 128, "scalar")])
 def test_aa_order_equals_ab_order(ob, prec, launch, n, pull, monkeypatch):
     """The one-buffer AA stream order (a step that pulls from and writes back
     to the neighbours, then one on the cell's own slots, alternating) and the
     two-buffer AB order give bitwise equal populations, fields and audits
     after odd step counts (reversed layout) and even ones (natural layout),
     through captured graphs and direct launches, with each form of the pull
-    step (OCTLB_AA_PULL: one cell per thread, two with shuffled aligned
-    stores, four in FP16 where a warp covers a 128-cell row), and after
-    set_populations while the AA buffer is in the reversed layout."""
+    step (one cell per thread; four in FP16 where a warp covers a 128-cell
+    row, with shuffled aligned stores; OCTLB_AA_PULL=scalar keeps one), and
+    after set_populations while the AA buffer is in the reversed layout."""
     from octlb_b200 import cases
     if launch == "direct":
         monkeypatch.setenv("OCTLB_NO_GRAPH", "1")
