@@ -369,14 +369,12 @@ __global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const S
     return;
   }
   const uint32_t bid = blockIdx.x - near_ctas;
-  const uint32_t nrun = a.blk_list ? static_cast<uint32_t>(a.nblk_run) : static_cast<uint32_t>(a.nblk);
-  const uint32_t bi = bid / kParts, part = bid % kParts;
-  if (bi >= nrun) {
+  const uint32_t b = bid / kParts, part = bid % kParts;
+  if (b >= static_cast<uint32_t>(a.nblk)) {
     pdl_wait();
-    rotate_item<T>(a, (bid - nrun * kParts) * kThreads + threadIdx.x);
+    rotate_item<T>(a, (bid - a.nblk * kParts) * kThreads + threadIdx.x);
     return;
   }
-  const uint32_t b = a.blk_list ? static_cast<uint32_t>(a.blk_list[bi]) : bi;
   const int np = a.np, np3 = np * np * np;
   const int* gm = a.slot_map + static_cast<long long>(b) * np3;
   if constexpr (!GMAP) {
@@ -1209,9 +1207,7 @@ cudaError_t launch_step_map(const StepArgs& a, const NearTables& nt, bool links,
   cudaError_t e = cudaSuccess;
   if (a.nitems == 0) return cudaSuccess;
   const uint32_t near_ctas = links ? grid_for(static_cast<uint32_t>(nt.n) * 32) : 0;
-  const uint32_t nrun = a.blk_list ? static_cast<uint32_t>(a.nblk_run) : static_cast<uint32_t>(a.nblk);
-  const dim3 g(near_ctas + nrun * (cpt == 2 ? 1 : 2) + grid_for(static_cast<uint32_t>(a.n_open)));
-  if (g.x == 0) return cudaSuccess;
+  const dim3 g(near_ctas + static_cast<uint32_t>(a.nblk) * (cpt == 2 ? 1 : 2) + grid_for(static_cast<uint32_t>(a.n_open)));
   const size_t smem = gmap ? 0 : static_cast<size_t>(a.np) * a.np * a.np * sizeof(int);
 #define OCTLB_MAP_LAUNCH(C, G)                                                                              \
   if (links) e = launch_chain(k_step_map<T, true, true, C, G>, g, dim3(kThreads), smem, s, a, nt);          \

@@ -80,95 +80,15 @@ int flush_restricts(octlb_ctx* ctx) {
   return OCTLB_OK;
 }
 
-// A level step that may run beside a coupler launch: a slot-map step, with
-// no exchange, force, ConstRhoBGK, boundary pass or adjoint record around it.
-bool split_step(const octlb_ctx* ctx, const Level& L) {
-  return ctx->split && L.split_ok && L.nblk > 0 && !L.has_force && !ctx->const_rho && !ctx->comm && !ctx->fd_on &&
-         !(ctx->adj && ctx->adj->recording);
-}
-
-// The held coupler launch, in stream order (a step that cannot take it beside).
-template <typename T>
-int launch_pending_couple(octlb_ctx* ctx) {
-  if (!ctx->pcpl.set) return OCTLB_OK;
-  ctx->pcpl.set = false;
-  CK(launch_couple<T>(ctx->pcpl.p, ctx->pcpl.r0, ctx->pcpl.r1, ctx->stream));
-  ++ctx->launch_count;
-  return OCTLB_OK;
-}
-
-// The slot-map step beside the held coupler launch: the coupler on cstream;
-// on the context's stream the blocks whose map reads none of its targets,
-// then (after the coupler) the others with the near-wall cells and the halo
-// items.  fork_drag runs once the coupler is done (the force reads its
-// targets' level).
-template <typename T, typename F>
-int split_map_step(octlb_ctx* ctx, Level& L, const StepArgs& a, F&& fork_drag) {
-  const octlb_ctx::PendingCouple pc = ctx->pcpl;
-  ctx->pcpl.set = false;
-  CK(cudaEventRecord(ctx->ev_cfork, ctx->stream));
-  CK(cudaStreamWaitEvent(ctx->cstream, ctx->ev_cfork, 0));
-  CK(launch_couple<T>(pc.p, pc.r0, pc.r1, ctx->cstream));
-  CK(cudaEventRecord(ctx->ev_cjoin, ctx->cstream));
-  ++ctx->launch_count;
-  const bool links = ctx->stream_mode == OCTLB_STREAM_LINKS;
-  const int m = (pc.p.n > 0 && pc.plevel == L.lvl ? 1 : 0) |
-                ((pc.r0.n > 0 && pc.rlevel0 == L.lvl) || (pc.r1.n > 0 && pc.rlevel1 == L.lvl) ? 2 : 0);
-  if (m == 0) {  // the coupler writes other levels: the whole step beside it
-    if (int rc = fork_drag()) return rc;
-    CK(launch_step_map<T>(a, L.near, links, L.has_flags, ctx->map_cells, ctx->map_global, ctx->stream));
-    ++ctx->launch_count;
-    CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_cjoin, 0));
-    return OCTLB_OK;
-  }
-  const int k = 2 * (m - 1);
-  StepArgs ai = a;
-  ai.blk_list = L.split_list.as<int>() + L.split_off[k];
-  ai.nblk_run = L.split_n[k];
-  ai.n_open = 0;
-  NearTables none = L.near;
-  none.n = 0;
-  if (ai.nblk_run > 0) {
-    CK(launch_step_map<T>(ai, none, links, L.has_flags, ctx->map_cells, ctx->map_global, ctx->stream));
-    ++ctx->launch_count;
-  }
-  CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_cjoin, 0));
-  if (int rc = fork_drag()) return rc;
-  StepArgs ad = a;
-  ad.blk_list = L.split_list.as<int>() + L.split_off[k + 1];
-  ad.nblk_run = L.split_n[k + 1];
-  if (ad.nblk_run > 0 || L.near.n > 0 || a.n_open > 0) {
-    CK(launch_step_map<T>(ad, L.near, links, L.has_flags, ctx->map_cells, ctx->map_global, ctx->stream));
-    ++ctx->launch_count;
-  }
-  return OCTLB_OK;
-}
-
 template <typename T>
 int launch_level_step(octlb_ctx* ctx, Level& L) {
   if (L.nblk == 0) {
-    if (int rc = launch_pending_couple<T>(ctx)) return rc;
     // A rank context with no block on this level still takes part in the
     // level's two exchanges (it may receive save rows for its coupler items).
     if (int rc = exchange_cells<T>(ctx, L)) return rc;
     return exchange_rows(ctx, L);  // (slab contexts own every level's block)
   }
-  const bool split = split_step(ctx, L);
-  if (split && !ctx->pcpl.set && !ctx->pending_restrict.empty() && ctx->pending_restrict.size() <= 2) {
-    // the pending restrictions beside the step's blocks that do not read them
-    auto& P = ctx->pending_restrict;
-    ctx->pcpl = octlb_ctx::PendingCouple{};
-    ctx->pcpl.set = true;
-    ctx->pcpl.r0 = P[0].op;
-    ctx->pcpl.rlevel0 = P[0].level;
-    if (P.size() > 1) {
-      ctx->pcpl.r1 = P[1].op;
-      ctx->pcpl.rlevel1 = P[1].level;
-    }
-    P.clear();
-  }
   { const int rc = flush_restricts<T>(ctx); if (rc) return rc; }  // the step reads what they write
-  if (!split) { const int rc = launch_pending_couple<T>(ctx); if (rc) return rc; }
   // Body force on the stored post-collision state (the reference's apply()
   // hook after collide, time_loop.h:207-211).  The boundary fills and the
   // same-level exchange that follow there need no launch: the step reads
@@ -211,19 +131,14 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
   // launched on the side stream before that step, so it overlaps the step
   // and what follows it.  (The adjoint's recomputation needs no force: it
   // records the inputs.)
-  auto fork_drag = [&]() -> int {
-    if (!(ctx->drag && L.n_drag > 0 && L.substep + 1 == (1 << L.lvl) && !rec)) return OCTLB_OK;
+  if (ctx->drag && L.n_drag > 0 && L.substep + 1 == (1 << L.lvl) && !rec) {
     CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
     CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
     CK(launch_drag<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.drag_items.as<DragItem>(), L.n_drag,
                       ctx->drag_partial.as<double>() + 3 * L.drag_off, ctx->side));
     ctx->side_busy = true;
     ++ctx->launch_count;
-    return OCTLB_OK;
-  };
-  const bool beside = split && ctx->pcpl.set;  // the held coupler runs beside this step
-  if (!beside)
-    if (int rc = fork_drag()) return rc;
+  }
   if (ctx->const_rho && L.lvl != ctx->cr_level) {
     // ConstRhoBGK, a level above the finest: the step only streams (and
     // saves the coupler's rows); the level collides in do_advance_level once
@@ -257,9 +172,6 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
   } else if (L.use_pair) {
     CK(launch_step_pair<T>(a, ctx->stream));
-  } else if (L.use_map && beside) {
-    if (int rc = split_map_step<T>(ctx, L, a, fork_drag)) return rc;
-    --ctx->launch_count;  // counted there (the one below counts the plain step)
   } else if (L.use_map) {
     CK(launch_step_map<T>(a, L.near, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags, ctx->map_cells,
                           ctx->map_global, ctx->stream));
@@ -329,24 +241,11 @@ int do_advance_level(octlb_ctx* ctx, int l) {
         if (q.level == l + 1 && !F.fuse_restrict) share = false;
       if (!share) { rc = flush_restricts<T>(ctx); if (rc) return rc; }
       RestrictOp r0{}, r1{};
-      int rl0 = -1, rl1 = -1;
-      if (!pend.empty()) { r0 = pend[0].op; rl0 = pend[0].level; }
-      if (pend.size() > 1) { r1 = pend[1].op; rl1 = pend[1].level; }
+      if (!pend.empty()) r0 = pend[0].op;
+      if (pend.size() > 1) r1 = pend[1].op;
       pend.clear();
-      if (split_step(ctx, F)) {
-        // held for the fine level's step, which runs it beside its blocks
-        // that read none of its targets
-        ctx->pcpl.set = true;
-        ctx->pcpl.p = p;
-        ctx->pcpl.r0 = r0;
-        ctx->pcpl.r1 = r1;
-        ctx->pcpl.plevel = l + 1;
-        ctx->pcpl.rlevel0 = rl0;
-        ctx->pcpl.rlevel1 = rl1;
-      } else {
-        CK(launch_couple<T>(p, r0, r1, ctx->stream));
-        ++ctx->launch_count;
-      }
+      CK(launch_couple<T>(p, r0, r1, ctx->stream));
+      ++ctx->launch_count;
     }
     rc = do_advance_level<T>(ctx, l + 1);
     if (rc) return rc;
@@ -1326,33 +1225,6 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       CK(upload(L.blk_moving, moving));
       A.blk_moving = L.blk_moving.as<uint8_t>();
       A.slot_map = L.slot_map.as<int>();
-      // Blocks whose map reads a coupler target: of the prolongation into this
-      // level (bit 0) or of the restriction into it (bit 1).  With a coupler
-      // launch of mask m beside the step, the others run at once.
-      {
-        std::vector<uint8_t> tgt(static_cast<size_t>(L.nslots), 0);
-        if (l >= 1)
-          for (const ProlongItem& it : prolong[l - 1]) tgt[static_cast<size_t>(it.fine_slot)] |= 1;
-        if (l + 1 < nlev)
-          for (const RestrictItem& it : restrict_items[l + 1]) tgt[static_cast<size_t>(it.coarse_slot)] |= 2;
-        std::vector<uint8_t> reads(static_cast<size_t>(L.nblk), 0);
-        for (int lb = 0; lb < L.nblk; ++lb)
-          for (int k = 0; k < np3; ++k) {
-            const int sl = slot_map[static_cast<size_t>(lb) * np3 + k];
-            if (sl >= 0) reads[lb] |= tgt[static_cast<size_t>(sl)];
-          }
-        std::vector<int> lists;
-        for (int m = 1; m <= 3; ++m)
-          for (int part = 0; part < 2; ++part) {
-            const int k = 2 * (m - 1) + part;
-            L.split_off[k] = static_cast<int>(lists.size());
-            for (int lb = 0; lb < L.nblk; ++lb)
-              if (((reads[lb] & m) != 0) == (part == 1)) lists.push_back(lb);
-            L.split_n[k] = static_cast<int>(lists.size()) - L.split_off[k];
-          }
-        CK(upload(L.split_list, lists));
-        L.split_ok = true;
-      }
       A.wall_add = L.wall_add.as<float>();
       A.wall_dadd = L.wall_dadd.as<float>();
     }
@@ -1524,8 +1396,6 @@ int advance_one_launches(octlb_ctx* ctx) {
   for (auto& L : ctx->levels) L.substep = 0;
   ctx->launch_count = 0;
   int rc = do_advance_level<T>(ctx, 0);
-  if (rc) return rc;
-  rc = launch_pending_couple<T>(ctx);
   if (rc) return rc;
   rc = flush_restricts<T>(ctx);
   if (rc) return rc;
@@ -2224,16 +2094,12 @@ static int create_common(const octlb_tables* t, const octlb_params* p, const dou
     if (ms >= 1 && ms <= 60000) ctx->wait_ns = static_cast<unsigned long long>(ms) * 1000000ull;
   }
   if (const char* st = std::getenv("OCTLB_TEST_BULK_STALL")) ctx->stall_first_row = st[0] == '1' ? 1 : 0;
-  if (const char* sp = std::getenv("OCTLB_NO_SPLIT")) ctx->split = sp[0] != '1';
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "cudaStreamCreate"); *out = ctx.release(); return rc; }
   ctx->own_stream = true;
   e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_cfork, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_cjoin, cudaEventDisableTiming);
   if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "side stream"); *out = ctx.release(); return rc; }
   if (ctx->comm) {
     // The exchanges sit between the launches of a level step and the local
@@ -2272,14 +2138,8 @@ void octlb_gpu_destroy(octlb_ctx* ctx) {
     cudaStreamSynchronize(ctx->side);
     cudaStreamDestroy(ctx->side);
   }
-  if (ctx->cstream) {
-    cudaStreamSynchronize(ctx->cstream);
-    cudaStreamDestroy(ctx->cstream);
-  }
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
-  if (ctx->ev_cfork) cudaEventDestroy(ctx->ev_cfork);
-  if (ctx->ev_cjoin) cudaEventDestroy(ctx->ev_cjoin);
   delete ctx;
 }
 

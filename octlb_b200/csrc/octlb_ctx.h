@@ -172,13 +172,6 @@ struct Level {
   bool use_pair = false;            // two-cells-per-thread step (periodic block)
   bool use_map = false;             // slot-map step (forest level)
   bool aa = false;                  // AA stream order: buf[1] aliases buf[0], cur = layout parity
-  // Slot-map step beside a coupler launch: for mask m (bit 0: a prolongation
-  // into this level, bit 1: a restriction into it), the blocks whose map
-  // reads none of those targets (run beside the coupler) and the others (run
-  // after it): list k = 2 (m - 1) + {0, 1} at split_off[k], split_n[k].
-  DevBuf split_list;
-  int split_off[6] = {0, 0, 0, 0, 0, 0}, split_n[6] = {0, 0, 0, 0, 0, 0};
-  bool split_ok = false;
   int bulk_grid = 0;
   DevBuf body_force;                // [3][ncore] float, or empty
   bool has_force = false;
@@ -304,18 +297,6 @@ struct octlb_ctx {
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool side_busy = false;
-  // A coupler launch held for the next level step, which runs it on cstream
-  // beside the blocks that do not read its targets (OCTLB_NO_SPLIT=1: in
-  // stream order before the step).
-  struct PendingCouple {
-    bool set = false;
-    ProlongOp p{};
-    RestrictOp r0{}, r1{};
-    int plevel = -1, rlevel0 = -1, rlevel1 = -1;  // the levels written
-  } pcpl;
-  bool split = true;
-  cudaStream_t cstream = nullptr;
-  cudaEvent_t ev_cfork = nullptr, ev_cjoin = nullptr;
   DevBuf drag_partial, force, force_sum, audit_out, audit_partial, host_tmp, dev_err;
   // FP64 host-layout staging of set/get_populations and get_fields (grown on
   // demand, kept until destroy: no allocation per call)

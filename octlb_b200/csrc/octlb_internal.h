@@ -65,10 +65,6 @@ struct StepArgs {
   // Readers of an AA-order box after an odd number of steps: population i of
   // cell x sits in plane opp(i) at the periodic neighbour x + c_i.
   int aa_rev;
-  // Slot-map step over part of the level's blocks (the part that runs beside
-  // a coupler launch): CTA block index -> block, nblk_run of them; null: all.
-  const int* blk_list;
-  int nblk_run;
 };
 
 // AA-order box after an odd number of steps: the slot holding population i

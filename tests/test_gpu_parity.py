@@ -290,43 +290,6 @@ def test_graph_and_programmatic_launch_bitwise_equal(ob, case, monkeypatch):
         assert np.array_equal(s0[0], s1[0]) and s0[1] == s1[1] == 9
 
 
-@pytest.mark.parametrize("case", ["cylinder3_fp32", "cylinder3_fp16", "cavity_band_fp32", "cylinder2_direct"])
-def test_coupler_beside_step_bitwise_equals_stream_order(ob, case, monkeypatch):
-    """Each coupler launch runs on its own stream beside the next step's
-    blocks that read none of its targets, the other blocks after it
-    (default), or in plain stream order before the step (OCTLB_NO_SPLIT=1):
-    the same populations, forces, force sums and counters, through graphs
-    and direct launches, on three- and two-level meshes."""
-    from octlb_b200 import cases
-    if case.startswith("cylinder3"):
-        mesh, init, info = cases.cylinder_forest(length=128, height=32, n=8, diameter=8.0, center=(16.0, 16.0),
-                                                 levels=3, refine_dist=8.0)
-        kw = dict(stream_mode=ob.STREAM_LINKS, drag=True)
-    elif case.startswith("cylinder2"):
-        mesh, init, info = small_cylinder(ob)
-        kw = dict(stream_mode=ob.STREAM_LINKS, drag=True)
-        monkeypatch.setenv("OCTLB_NO_GRAPH", "1")
-    else:
-        mesh, init, info = cases.cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=8)
-        kw = {}
-    prec = ob.FP16_SHIFTED if case.endswith("fp16") else ob.FP32
-    res = []
-    for nosplit in ("1", "0"):
-        monkeypatch.setenv("OCTLB_NO_SPLIT", nosplit)
-        lat = ob.GpuLattice(mesh, info["omega"], precision=prec, init_pops=init, **kw)
-        forces = []
-        for _ in range(4):
-            lat.advance(1)
-            forces.append(lat.force() if kw else np.zeros(3))
-        lat.advance(5)
-        res.append((lat.get_populations(), np.array(forces), lat.counters(),
-                    lat.force_sum() if kw else (np.zeros(3), 9)))
-        lat.close()
-    (p0, f0, c0, s0), (p1, f1, c1, s1) = res
-    assert np.array_equal(p0, p1) and np.array_equal(f0, f1) and c0 == c1
-    assert np.array_equal(s0[0], s1[0]) and s0[1] == s1[1]
-
-
 def test_body_force_matches_reference(ob, ref):
     """A nonzero per-cell body force: GPU fields and MEM force per coarse step
     against the reference TimeLoop with the same forcing term added at its
