@@ -350,36 +350,25 @@ __device__ __forceinline__ float map_cell_finish(const StepArgs& a, uint32_t t, 
 // and per near-cell and block CTA the sum of rho - 1 over its collided kBulk
 // cells in cr_part[blockIdx.x] (the halo-item CTAs after them write none);
 // kCollNone: no collide.
-template <typename T, bool LINKS, int CPT>
-__device__ __forceinline__ bool cpl_prologue(const StepArgs& a, const NearTables& nt, const CplFuse& f);
-
-// CPL: a coupler launch folded in front of the step (its CTAs before the
-// step's; cpl_prologue); the CTA numbers below count the step's.
-template <typename T, bool LINKS, bool FLAGS, int CPT, bool GMAP, int CM = kCollBgk, bool CPL = false>
-__global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5)
-k_step_map(const StepArgs a, const NearTables nt, const CplFuse f) {
+template <typename T, bool LINKS, bool FLAGS, int CPT, bool GMAP, int CM = kCollBgk>
+__global__ void __launch_bounds__(kThreads, CPT == 2 ? 4 : 5) k_step_map(const StepArgs a, const NearTables nt) {
   extern __shared__ int smap_s[];  // (n+2)^3 slots of this block
   constexpr uint32_t kParts = CPT == 1 ? 2 : 1;
-  uint32_t cta = blockIdx.x;
-  if constexpr (CPL) {
-    if (cpl_prologue<T, LINKS, CPT>(a, nt, f)) return;
-    cta -= f.ctas;
-  }
   const uint32_t near_ctas = LINKS ? (static_cast<uint32_t>(nt.n) + kThreads / 32 - 1) / (kThreads / 32) : 0;
-  if (LINKS && cta < near_ctas) {
+  if (LINKS && blockIdx.x < near_ctas) {
     if constexpr (CM == kCollConstRho) {
       pdl_wait();
       const float dr = static_cast<float>(1.0 - *a.cr_avg);
-      const float dh = near_cell<T, kCollConstRho>(a, nt, static_cast<int>(cta * (kThreads / 32) + (threadIdx.x >> 5)),
+      const float dh = near_cell<T, kCollConstRho>(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)),
                                           threadIdx.x & 31, dr);
       cr_store_partial(a, (threadIdx.x & 31) == 0 ? static_cast<double>(dh) : 0.0,
                        near_ctas + static_cast<uint32_t>(a.nblk) * kParts);
     } else {
-      near_cell<T, CM>(a, nt, static_cast<int>(cta * (kThreads / 32) + (threadIdx.x >> 5)), threadIdx.x & 31);
+      near_cell<T, CM>(a, nt, static_cast<int>(blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)), threadIdx.x & 31);
     }
     return;
   }
-  const uint32_t bid = cta - near_ctas;
+  const uint32_t bid = blockIdx.x - near_ctas;
   const uint32_t b = bid / kParts, part = bid % kParts;
   if (b >= static_cast<uint32_t>(a.nblk)) {
     pdl_wait();
@@ -454,7 +443,6 @@ k_step_map(const StepArgs a, const NearTables nt, const CplFuse f) {
   if constexpr (CM == kCollConstRho)
     cr_store_partial(a, static_cast<double>(acc), near_ctas + static_cast<uint32_t>(a.nblk) * kParts);
 }
-
 
 // One periodic all-kBulk block, two consecutive z cells per thread: every
 // population row is read and written with 2-element vector accesses; a z-shift
@@ -850,14 +838,13 @@ __device__ __forceinline__ void restrict_warp(const RestrictOp& op, int w, int l
 // between them orders (a restriction into level l and the full-time
 // prolongation into level l with disjoint targets; two restrictions) share a
 // launch this way.
-// CTA b of a coupler launch (k_couple, or the first CTAs of k_step_map_cpl);
-// fneq_s: the restriction's [warp][row][population] staging.
 template <typename T>
-__device__ __forceinline__ void couple_cta(const ProlongOp& p, const RestrictOp& r0, const RestrictOp& r1, uint32_t b,
-                                           float (*fneq_s)[kQ][kQ + 1]) {
+__global__ void __launch_bounds__(kThreads) k_couple(const ProlongOp p, const RestrictOp r0, const RestrictOp r1) {
+  __shared__ float fneq_s[kThreads / 32][kQ][kQ + 1];  // restriction: [warp][row][population]
   const uint32_t gp = (static_cast<uint32_t>(p.n) * 32 + kThreads - 1) / kThreads;
   const uint32_t g0 = (static_cast<uint32_t>(r0.n) * 32 + kThreads - 1) / kThreads;
   const int lane = threadIdx.x & 31;
+  uint32_t b = blockIdx.x;
   if (b < gp) {
     const float dh = prolong_warp<T>(p, static_cast<int>((b * kThreads + threadIdx.x) >> 5), lane);
     if (p.cr_part) {  // ConstRhoBGK statistics of the collided targets (lane 0 of each item)
@@ -875,73 +862,6 @@ __device__ __forceinline__ void couple_cta(const ProlongOp& p, const RestrictOp&
   }
   b -= g0;
   restrict_warp<T>(r1, static_cast<int>((b * kThreads + threadIdx.x) >> 5), lane, fs);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_couple(const ProlongOp p, const RestrictOp r0, const RestrictOp r1) {
-  __shared__ float fneq_s[kThreads / 32][kQ][kQ + 1];  // restriction: [warp][row][population]
-  couple_cta<T>(p, r0, r1, blockIdx.x, fneq_s);
-}
-
-__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ unsigned long long cpl_now_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// A coupler launch and the slot-map step that follows it, as one launch
-// (k_step_map with CPL): the coupler's CTAs first (their work as k_couple's),
-// then the step's.  A step CTA whose cells read one of the coupler's targets
-// waits for the coupler CTAs (thread 0 polls a device counter with acquire
-// loads, bounded by wait_ns, then the CTA barrier); the others start at
-// once.  The coupler CTAs have the lowest indices, so they are placed on the
-// SMs before any step CTA that could wait on them.  Returns true for a
-// coupler CTA (done).
-template <typename T, bool LINKS, int CPT>
-__device__ __forceinline__ bool cpl_prologue(const StepArgs& a, const NearTables& nt, const CplFuse& f) {
-  if (blockIdx.x < f.ctas) {
-    __shared__ float fneq_s[kThreads / 32][kQ][kQ + 1];
-    couple_cta<T>(f.p, f.r0, f.r1, blockIdx.x, fneq_s);
-    if (f.n_wait > 0 && !f.stall) {
-      __syncthreads();  // every thread's stores before the release
-      if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(f.sync, 1);
-      }
-    }
-    return true;
-  }
-  if (f.n_wait == 0) return false;
-  constexpr uint32_t kParts = CPT == 1 ? 2 : 1;
-  const uint32_t cta = blockIdx.x - f.ctas;
-  const uint32_t near_ctas = LINKS ? (static_cast<uint32_t>(nt.n) + kThreads / 32 - 1) / (kThreads / 32) : 0;
-  bool wait = true;  // near-wall and halo-item CTAs always wait
-  if (cta >= near_ctas) {
-    const uint32_t bi = (cta - near_ctas) / kParts;
-    if (bi < static_cast<uint32_t>(a.nblk)) wait = f.wait_blk[bi] != 0;
-  }
-  if (!wait) return false;
-  if (threadIdx.x == 0) {
-    const int target = static_cast<int>(f.ctas);
-    if (ld_acquire_gpu(f.sync) < target) {
-      const unsigned long long t0 = cpl_now_ns();
-      while (ld_acquire_gpu(f.sync) < target) {
-        if (cpl_now_ns() - t0 > a.wait_ns) {
-          atomicMax(a.err, kErrCoupleTimeout);
-          break;
-        }
-        __nanosleep(128);
-      }
-    }
-  }
-  __syncthreads();
-  __threadfence();
-  return false;
 }
 
 // Momentum-exchange force (drag_postprocessor.h:67-115) from the buffer the
@@ -1290,9 +1210,9 @@ cudaError_t launch_step_map(const StepArgs& a, const NearTables& nt, bool links,
   const dim3 g(near_ctas + static_cast<uint32_t>(a.nblk) * (cpt == 2 ? 1 : 2) + grid_for(static_cast<uint32_t>(a.n_open)));
   const size_t smem = gmap ? 0 : static_cast<size_t>(a.np) * a.np * a.np * sizeof(int);
 #define OCTLB_MAP_LAUNCH(C, G)                                                                              \
-  if (links) e = launch_chain(k_step_map<T, true, true, C, G>, g, dim3(kThreads), smem, s, a, nt, CplFuse{});          \
-  else if (flags) e = launch_chain(k_step_map<T, false, true, C, G>, g, dim3(kThreads), smem, s, a, nt, CplFuse{});    \
-  else e = launch_chain(k_step_map<T, false, false, C, G>, g, dim3(kThreads), smem, s, a, nt, CplFuse{});
+  if (links) e = launch_chain(k_step_map<T, true, true, C, G>, g, dim3(kThreads), smem, s, a, nt);          \
+  else if (flags) e = launch_chain(k_step_map<T, false, true, C, G>, g, dim3(kThreads), smem, s, a, nt);    \
+  else e = launch_chain(k_step_map<T, false, false, C, G>, g, dim3(kThreads), smem, s, a, nt);
   if (cpt == 2) {
     if (gmap) { OCTLB_MAP_LAUNCH(2, true) } else { OCTLB_MAP_LAUNCH(2, false) }
   } else {
@@ -1300,26 +1220,6 @@ cudaError_t launch_step_map(const StepArgs& a, const NearTables& nt, bool links,
   }
 #undef OCTLB_MAP_LAUNCH
   return e != cudaSuccess ? e : cudaGetLastError();
-}
-
-// A coupler launch folded into the following slot-map step (default
-// variants: map read through L1, one cell per thread under the links rule,
-// two otherwise).
-template <typename T>
-cudaError_t launch_step_map_cpl(const StepArgs& a, const NearTables& nt, bool links, bool flags, const CplFuse& f,
-                                cudaStream_t s) {
-  const uint32_t near_ctas = links ? grid_for(static_cast<uint32_t>(nt.n) * 32) : 0;
-  const dim3 g(f.ctas + near_ctas + static_cast<uint32_t>(a.nblk) * (links ? 2 : 1) +
-               grid_for(static_cast<uint32_t>(a.n_open)));
-  cudaError_t e;
-  if (links) e = launch_chain(k_step_map<T, true, true, 1, true, kCollBgk, true>, g, dim3(kThreads), 0, s, a, nt, f);
-  else if (flags) e = launch_chain(k_step_map<T, false, true, 2, true, kCollBgk, true>, g, dim3(kThreads), 0, s, a, nt, f);
-  else e = launch_chain(k_step_map<T, false, false, 2, true, kCollBgk, true>, g, dim3(kThreads), 0, s, a, nt, f);
-  return e != cudaSuccess ? e : cudaGetLastError();
-}
-uint32_t couple_ctas(const ProlongOp& p, const RestrictOp& r0, const RestrictOp& r1) {
-  return grid_for(static_cast<uint32_t>(p.n) * 32) + grid_for(static_cast<uint32_t>(r0.n) * 32) +
-         grid_for(static_cast<uint32_t>(r1.n) * 32);
 }
 
 // ConstRhoBGK slot-map step: the default variants only (one cell per thread
@@ -1330,9 +1230,9 @@ cudaError_t launch_step_map_cr(const StepArgs& a, const NearTables& nt, bool lin
   if (a.nitems == 0) return cudaSuccess;
   const uint32_t near_ctas = links ? grid_for(static_cast<uint32_t>(nt.n) * 32) : 0;
   const dim3 g(near_ctas + static_cast<uint32_t>(a.nblk) * (links ? 2 : 1) + grid_for(static_cast<uint32_t>(a.n_open)));
-  if (links) e = launch_chain(k_step_map<T, true, true, 1, true, kCollConstRho>, g, dim3(kThreads), 0, s, a, nt, CplFuse{});
-  else if (flags) e = launch_chain(k_step_map<T, false, true, 2, true, kCollConstRho>, g, dim3(kThreads), 0, s, a, nt, CplFuse{});
-  else e = launch_chain(k_step_map<T, false, false, 2, true, kCollConstRho>, g, dim3(kThreads), 0, s, a, nt, CplFuse{});
+  if (links) e = launch_chain(k_step_map<T, true, true, 1, true, kCollConstRho>, g, dim3(kThreads), 0, s, a, nt);
+  else if (flags) e = launch_chain(k_step_map<T, false, true, 2, true, kCollConstRho>, g, dim3(kThreads), 0, s, a, nt);
+  else e = launch_chain(k_step_map<T, false, false, 2, true, kCollConstRho>, g, dim3(kThreads), 0, s, a, nt);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -1345,9 +1245,9 @@ cudaError_t launch_step_map_nc(const StepArgs& a, const NearTables& nt, bool lin
   if (a.nitems == 0) return cudaSuccess;
   const uint32_t near_ctas = links ? grid_for(static_cast<uint32_t>(nt.n) * 32) : 0;
   const dim3 g(near_ctas + static_cast<uint32_t>(a.nblk) * (links ? 2 : 1) + grid_for(static_cast<uint32_t>(a.n_open)));
-  if (links) e = launch_chain(k_step_map<T, true, true, 1, true, kCollNone>, g, dim3(kThreads), 0, s, a, nt, CplFuse{});
-  else if (flags) e = launch_chain(k_step_map<T, false, true, 2, true, kCollNone>, g, dim3(kThreads), 0, s, a, nt, CplFuse{});
-  else e = launch_chain(k_step_map<T, false, false, 2, true, kCollNone>, g, dim3(kThreads), 0, s, a, nt, CplFuse{});
+  if (links) e = launch_chain(k_step_map<T, true, true, 1, true, kCollNone>, g, dim3(kThreads), 0, s, a, nt);
+  else if (flags) e = launch_chain(k_step_map<T, false, true, 2, true, kCollNone>, g, dim3(kThreads), 0, s, a, nt);
+  else e = launch_chain(k_step_map<T, false, false, 2, true, kCollNone>, g, dim3(kThreads), 0, s, a, nt);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 template <typename T>
@@ -1550,8 +1450,6 @@ cudaError_t launch_cr_update(double* avg, const double* part, int nparts, long l
   template cudaError_t launch_step_cr<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
   template cudaError_t launch_step_map_cr<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
   template cudaError_t launch_step_map_nc<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
-  template cudaError_t launch_step_map_cpl<T>(const StepArgs&, const NearTables&, bool, bool, const CplFuse&,  \
-                                              cudaStream_t);                                                   \
   template cudaError_t launch_step_nc<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
   template cudaError_t launch_collide_cr<T>(const StepArgs&, cudaStream_t);                        \
   template cudaError_t launch_cr_seed<T>(const StepArgs&, int, cudaStream_t);

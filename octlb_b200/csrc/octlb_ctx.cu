@@ -80,53 +80,15 @@ int flush_restricts(octlb_ctx* ctx) {
   return OCTLB_OK;
 }
 
-// A level step that can take the held coupler launch into its own launch: a
-// slot-map step in its default form, with no force, exchange, ConstRhoBGK,
-// boundary pass or adjoint record around it.
-bool fuse_step(const octlb_ctx* ctx, const Level& L) {
-  const bool links = ctx->stream_mode == OCTLB_STREAM_LINKS;
-  return ctx->fuse && L.cpl_ok && L.nblk > 0 && ctx->map_global && ctx->map_cells == (links ? 1 : 2) &&
-         !L.has_force && !ctx->const_rho && !ctx->comm && !ctx->fd_on && !(ctx->adj && ctx->adj->recording);
-}
-
-// The held coupler launch, in stream order.
-template <typename T>
-int launch_pending_couple(octlb_ctx* ctx) {
-  if (!ctx->pcpl.set) return OCTLB_OK;
-  ctx->pcpl.set = false;
-  CK(launch_couple<T>(ctx->pcpl.p, ctx->pcpl.r0, ctx->pcpl.r1, ctx->stream));
-  ++ctx->launch_count;
-  return OCTLB_OK;
-}
-
 template <typename T>
 int launch_level_step(octlb_ctx* ctx, Level& L) {
   if (L.nblk == 0) {
-    if (int rc = launch_pending_couple<T>(ctx)) return rc;
     // A rank context with no block on this level still takes part in the
     // level's two exchanges (it may receive save rows for its coupler items).
     if (int rc = exchange_cells<T>(ctx, L)) return rc;
     return exchange_rows(ctx, L);  // (slab contexts own every level's block)
   }
-  const bool fuse = fuse_step(ctx, L);
-  if (fuse && !ctx->pcpl.set && !ctx->pending_restrict.empty() && ctx->pending_restrict.size() <= 2) {
-    // the pending restrictions, folded into the step's launch
-    auto& P = ctx->pending_restrict;
-    ctx->pcpl = octlb_ctx::PendingCouple{};
-    ctx->pcpl.set = true;
-    ctx->pcpl.r0 = P[0].op;
-    ctx->pcpl.rlevel0 = P[0].level;
-    if (P.size() > 1) {
-      ctx->pcpl.r1 = P[1].op;
-      ctx->pcpl.rlevel1 = P[1].level;
-    }
-    P.clear();
-  }
   { const int rc = flush_restricts<T>(ctx); if (rc) return rc; }  // the step reads what they write
-  if (!fuse || ctx->cpl_site >= octlb_ctx::kCplSites) {
-    const int rc = launch_pending_couple<T>(ctx);
-    if (rc) return rc;
-  }
   // Body force on the stored post-collision state (the reference's apply()
   // hook after collide, time_loop.h:207-211).  The boundary fills and the
   // same-level exchange that follow there need no launch: the step reads
@@ -169,22 +131,14 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
   // launched on the side stream before that step, so it overlaps the step
   // and what follows it.  (The adjoint's recomputation needs no force: it
   // records the inputs.)
-  // (With a coupler folded into the step, after the step: the coupler's
-  // targets are part of the input the force reads, and the step does not
-  // write its input.)
-  const bool folded = fuse && ctx->pcpl.set;
-  auto fork_drag = [&]() -> int {
-    if (!(ctx->drag && L.n_drag > 0 && L.substep + 1 == (1 << L.lvl) && !rec)) return OCTLB_OK;
+  if (ctx->drag && L.n_drag > 0 && L.substep + 1 == (1 << L.lvl) && !rec) {
     CK(cudaEventRecord(ctx->ev_fork, ctx->stream));
     CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
     CK(launch_drag<T>(a, ctx->stream_mode == OCTLB_STREAM_LINKS, L.drag_items.as<DragItem>(), L.n_drag,
                       ctx->drag_partial.as<double>() + 3 * L.drag_off, ctx->side));
     ctx->side_busy = true;
     ++ctx->launch_count;
-    return OCTLB_OK;
-  };
-  if (!folded)
-    if (int rc = fork_drag()) return rc;
+  }
   if (ctx->const_rho && L.lvl != ctx->cr_level) {
     // ConstRhoBGK, a level above the finest: the step only streams (and
     // saves the coupler's rows); the level collides in do_advance_level once
@@ -218,32 +172,6 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
   } else if (L.use_pair) {
     CK(launch_step_pair<T>(a, ctx->stream));
-  } else if (L.use_map && folded) {
-    // the held coupler launch folded in front of the step: step CTAs whose
-    // cells read its targets wait for its CTAs, the others start at once
-    const octlb_ctx::PendingCouple pc = ctx->pcpl;
-    ctx->pcpl.set = false;
-    const bool links = ctx->stream_mode == OCTLB_STREAM_LINKS;
-    const int m = (pc.p.n > 0 && pc.plevel == L.lvl ? 1 : 0) |
-                  ((pc.r0.n > 0 && pc.rlevel0 == L.lvl) || (pc.r1.n > 0 && pc.rlevel1 == L.lvl) ? 2 : 0);
-    CplFuse f{};
-    f.p = pc.p;
-    f.r0 = pc.r0;
-    f.r1 = pc.r1;
-    f.ctas = couple_ctas(pc.p, pc.r0, pc.r1);
-    if (m != 0 && f.ctas > 0) {
-      const int site = ctx->cpl_site++;
-      const int near_ctas = links ? static_cast<int>(cr_near_parts(L.near)) : 0;
-      const int halo_ctas = (L.n_open + 255) / 256;
-      f.sync = ctx->cpl_sync.as<int>() + site;
-      f.wait_blk = L.cpl_wait.as<uint8_t>() + static_cast<size_t>(m - 1) * L.nblk;
-      f.n_wait = L.cpl_nwait[m - 1] * (links ? 2 : 1) + near_ctas + halo_ctas;
-      f.stall = ctx->cpl_stall;
-    }
-    CK(launch_step_map_cpl<T>(a, L.near, links, L.has_flags, f, ctx->stream));
-    if (f.ctas > 0) ++ctx->launch_count;  // counted as the coupler launch it replaces: one launch less
-    --ctx->launch_count;
-    if (int rc = fork_drag()) return rc;
   } else if (L.use_map) {
     CK(launch_step_map<T>(a, L.near, ctx->stream_mode == OCTLB_STREAM_LINKS, L.has_flags, ctx->map_cells,
                           ctx->map_global, ctx->stream));
@@ -313,23 +241,11 @@ int do_advance_level(octlb_ctx* ctx, int l) {
         if (q.level == l + 1 && !F.fuse_restrict) share = false;
       if (!share) { rc = flush_restricts<T>(ctx); if (rc) return rc; }
       RestrictOp r0{}, r1{};
-      int rl0 = -1, rl1 = -1;
-      if (!pend.empty()) { r0 = pend[0].op; rl0 = pend[0].level; }
-      if (pend.size() > 1) { r1 = pend[1].op; rl1 = pend[1].level; }
+      if (!pend.empty()) r0 = pend[0].op;
+      if (pend.size() > 1) r1 = pend[1].op;
       pend.clear();
-      if (fuse_step(ctx, F)) {
-        // held for the fine level's step, which folds it into its launch
-        ctx->pcpl.set = true;
-        ctx->pcpl.p = p;
-        ctx->pcpl.r0 = r0;
-        ctx->pcpl.r1 = r1;
-        ctx->pcpl.plevel = l + 1;
-        ctx->pcpl.rlevel0 = rl0;
-        ctx->pcpl.rlevel1 = rl1;
-      } else {
-        CK(launch_couple<T>(p, r0, r1, ctx->stream));
-        ++ctx->launch_count;
-      }
+      CK(launch_couple<T>(p, r0, r1, ctx->stream));
+      ++ctx->launch_count;
     }
     rc = do_advance_level<T>(ctx, l + 1);
     if (rc) return rc;
@@ -436,7 +352,6 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
   const bool links = p->stream_mode == OCTLB_STREAM_LINKS;
   ctx->kinds.assign(t->kinds, t->kinds + n3 * nb);
   CK(ctx->dev_err.alloc(sizeof(int)));
-  CK(ctx->cpl_sync.alloc(sizeof(int) * octlb_ctx::kCplSites));
   for (int b = 0; b < nb; ++b) ctx->max_level = std::max(ctx->max_level, t->levels[b]);
   const int nlev = ctx->max_level + 1;
   ctx->levels.resize(nlev);
@@ -1310,33 +1225,6 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       CK(upload(L.blk_moving, moving));
       A.blk_moving = L.blk_moving.as<uint8_t>();
       A.slot_map = L.slot_map.as<int>();
-      // Blocks whose map reads a coupler target: of the prolongation into this
-      // level (bit 0) or of the restriction into it (bit 1) -- the step CTAs
-      // that wait when a coupler launch is folded into the step's.
-      {
-        std::vector<uint8_t> tgt(static_cast<size_t>(L.nslots), 0);
-        if (l >= 1)
-          for (const ProlongItem& it : prolong[l - 1]) tgt[static_cast<size_t>(it.fine_slot)] |= 1;
-        if (l + 1 < nlev)
-          for (const RestrictItem& it : restrict_items[l + 1]) tgt[static_cast<size_t>(it.coarse_slot)] |= 2;
-        std::vector<uint8_t> reads(static_cast<size_t>(L.nblk), 0);
-        for (int lb = 0; lb < L.nblk; ++lb)
-          for (int k = 0; k < np3; ++k) {
-            const int sl = slot_map[static_cast<size_t>(lb) * np3 + k];
-            if (sl >= 0) reads[lb] |= tgt[static_cast<size_t>(sl)];
-          }
-        std::vector<uint8_t> wait(static_cast<size_t>(3 * L.nblk), 0);
-        for (int m = 1; m <= 3; ++m) {
-          L.cpl_nwait[m - 1] = 0;
-          for (int lb = 0; lb < L.nblk; ++lb)
-            if (reads[lb] & m) {
-              wait[static_cast<size_t>(m - 1) * L.nblk + lb] = 1;
-              ++L.cpl_nwait[m - 1];
-            }
-        }
-        CK(upload(L.cpl_wait, wait));
-        L.cpl_ok = true;
-      }
       A.wall_add = L.wall_add.as<float>();
       A.wall_dadd = L.wall_dadd.as<float>();
     }
@@ -1493,10 +1381,6 @@ int check_device_error(octlb_ctx* ctx) {
   if (h == kErrBulkTimeout)
     return fail(ctx, OCTLB_ETIMEOUT,
                 "bulk-copy wait gave up after " + std::to_string(ctx->wait_ns / 1000000ull) + " ms");
-  if (h == kErrCoupleTimeout)
-    return fail(ctx, OCTLB_ETIMEOUT,
-                "a step CTA gave up waiting for the coupler CTAs of its launch after " +
-                    std::to_string(ctx->wait_ns / 1000000ull) + " ms");
   if (h == kErrBulkDrainTimeout) {
     ctx->unusable = true;
     return fail(ctx, OCTLB_ECUDA,
@@ -1511,14 +1395,7 @@ template <typename T>
 int advance_one_launches(octlb_ctx* ctx) {
   for (auto& L : ctx->levels) L.substep = 0;
   ctx->launch_count = 0;
-  ctx->cpl_site = 0;
-  // the counters of the coupler launches folded into steps (one per launch)
-  bool couplers = false;
-  for (const auto& L : ctx->levels) couplers = couplers || (L.cpl_ok && (L.n_prolong > 0 || L.n_restrict > 0));
-  if (ctx->fuse && couplers) CK(cudaMemsetAsync(ctx->cpl_sync.p, 0, ctx->cpl_sync.bytes, ctx->stream));
   int rc = do_advance_level<T>(ctx, 0);
-  if (rc) return rc;
-  rc = launch_pending_couple<T>(ctx);
   if (rc) return rc;
   rc = flush_restricts<T>(ctx);
   if (rc) return rc;
@@ -2217,8 +2094,6 @@ static int create_common(const octlb_tables* t, const octlb_params* p, const dou
     if (ms >= 1 && ms <= 60000) ctx->wait_ns = static_cast<unsigned long long>(ms) * 1000000ull;
   }
   if (const char* st = std::getenv("OCTLB_TEST_BULK_STALL")) ctx->stall_first_row = st[0] == '1' ? 1 : 0;
-  if (const char* nf = std::getenv("OCTLB_NO_FUSE")) ctx->fuse = nf[0] != '1';
-  if (const char* cs = std::getenv("OCTLB_TEST_COUPLE_STALL")) ctx->cpl_stall = cs[0] == '1' ? 1 : 0;
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "cudaStreamCreate"); *out = ctx.release(); return rc; }
   ctx->own_stream = true;

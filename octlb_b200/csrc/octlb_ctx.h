@@ -44,9 +44,6 @@ template <typename T>
 cudaError_t launch_step_nc(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
 template <typename T> cudaError_t launch_collide_cr(const StepArgs&, cudaStream_t);
 template <typename T> cudaError_t launch_step_aa(const StepArgs&, bool, cudaStream_t);
-template <typename T>
-cudaError_t launch_step_map_cpl(const StepArgs&, const NearTables&, bool, bool, const CplFuse&, cudaStream_t);
-uint32_t couple_ctas(const ProlongOp&, const RestrictOp&, const RestrictOp&);
 cudaError_t launch_cr_update(double*, const double*, int, long long, const double*, int, long long, cudaStream_t);
 uint32_t cr_core_parts(const StepArgs& a);
 uint32_t cr_near_parts(const NearTables& nt);
@@ -175,13 +172,6 @@ struct Level {
   bool use_pair = false;            // two-cells-per-thread step (periodic block)
   bool use_map = false;             // slot-map step (forest level)
   bool aa = false;                  // AA stream order: buf[1] aliases buf[0], cur = layout parity
-  // Slot-map step with a coupler launch folded in front (k_step_map with
-  // CPL): for mask m (bit 0: a prolongation into this level, bit 1: a
-  // restriction into it), per block 1 where its map reads one of those
-  // targets ([3][nblk] at (m - 1) * nblk), and how many blocks do.
-  DevBuf cpl_wait;
-  int cpl_nwait[3] = {0, 0, 0};
-  bool cpl_ok = false;
   int bulk_grid = 0;
   DevBuf body_force;                // [3][ncore] float, or empty
   bool has_force = false;
@@ -307,20 +297,6 @@ struct octlb_ctx {
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool side_busy = false;
-  // A coupler launch held for the next level step, which folds it into its
-  // own launch (OCTLB_NO_FUSE=1: in stream order before the step).  Each
-  // folded launch of an advance_one has its own pair of counters.
-  struct PendingCouple {
-    bool set = false;
-    ProlongOp p{};
-    RestrictOp r0{}, r1{};
-    int plevel = -1, rlevel0 = -1, rlevel1 = -1;  // the levels written
-  } pcpl;
-  bool fuse = true;
-  static constexpr int kCplSites = 256;
-  DevBuf cpl_sync;                  // [kCplSites] ints, zeroed at the start of each advance_one
-  int cpl_site = 0;
-  int cpl_stall = 0;                // test of the bounded wait (OCTLB_TEST_COUPLE_STALL=1)
   DevBuf drag_partial, force, force_sum, audit_out, audit_partial, host_tmp, dev_err;
   // FP64 host-layout staging of set/get_populations and get_fields (grown on
   // demand, kept until destroy: no allocation per call)

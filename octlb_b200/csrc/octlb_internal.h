@@ -96,12 +96,10 @@ struct NearTables {
 
 constexpr long long kOwnPage = -(1LL << 62);
 
-// Device error codes written to StepArgs::err (atomicMax: the most severe
-// stays).  kErrCoupleTimeout: a step CTA gave up waiting for the coupler CTAs
-// of its launch.  kErrBulkDrainTimeout: a CTA that gave up could not see its
-// own copies in flight land either, so shared memory may still be written
-// after it exited.
-enum : int { kErrNone = 0, kErrBulkTimeout = 1, kErrHalo = 2, kErrCoupleTimeout = 3, kErrBulkDrainTimeout = 4 };
+// Device error codes written to StepArgs::err.
+// kErrBulkDrainTimeout: a CTA that gave up could not see its own copies in
+// flight land either, so shared memory may still be written after it exited.
+enum : int { kErrNone = 0, kErrBulkTimeout = 1, kErrHalo = 2, kErrBulkDrainTimeout = 3 };
 
 // Tree-boundary fill of one halo-page population: value(dst, pop) =
 // g_src_pop(src) + add (bounce-back wall: src_pop = opp(pop); outflow ghost
@@ -157,22 +155,6 @@ struct RestrictOp {
   float scale, omega, cscale;
   int cmode;                // collide of a kBulk target: kCollBgk or kCollNone
 };
-// A coupler launch folded into the next slot-map step launch (k_step_map with
-// CPL): its CTAs come first and count themselves done in *sync; a step CTA
-// whose cells read one of its targets (flag wait_blk[block]; near-wall and
-// halo-item CTAs always) waits until *sync reaches ctas (bounded).  Each
-// folded launch of an advance_one has its own counter, zeroed at the start
-// of the advance_one.
-struct CplFuse {
-  ProlongOp p;
-  RestrictOp r0, r1;
-  uint32_t ctas;            // coupler CTAs: the prolongation's, then each restriction's
-  int n_wait;               // > 0: some step CTAs wait (0: none, and no counting)
-  int* sync;                // the counter of coupler CTAs done
-  const uint8_t* wait_blk;  // [nblk] 1: the block reads a target
-  int stall;                // test of the bounded wait: the coupler CTAs never count themselves
-};
-
 // MEM drag cell: kBulk core cell with at least one obstacle link; bit i of
 // mask set when x + c_i is an in-block solid / Bouzidi obstacle cell
 // (drag_postprocessor.h:86-110).

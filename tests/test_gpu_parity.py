@@ -290,50 +290,6 @@ def test_graph_and_programmatic_launch_bitwise_equal(ob, case, monkeypatch):
         assert np.array_equal(s0[0], s1[0]) and s0[1] == s1[1] == 9
 
 
-@pytest.mark.parametrize("case", ["cylinder3_fp32", "cylinder3_fp16", "cavity_band_fp32", "cylinder2_direct",
-                                  "physical3"])
-def test_folded_coupler_bitwise_equals_stream_order(ob, case, monkeypatch):
-    """Each coupler launch folded into the next slot-map step's launch (its
-    CTAs first; step CTAs whose cells read its targets wait for them), or
-    launched on its own before the step (OCTLB_NO_FUSE=1): the same
-    populations, forces, force sums and counters, through graphs and direct
-    launches, on three- and two-level meshes and in the physical coupler
-    mode."""
-    from octlb_b200 import cases
-    kw = {}
-    if case.startswith("cylinder3") or case == "physical3":
-        mesh, init, info = cases.cylinder_forest(length=128, height=32, n=8, diameter=8.0, center=(16.0, 16.0),
-                                                 levels=3, refine_dist=8.0)
-        kw = dict(stream_mode=ob.STREAM_LINKS, drag=True)
-        if case == "physical3":
-            kw["coupler_mode"] = ob.COUPLER_PHYSICAL
-    elif case.startswith("cylinder2"):
-        mesh, init, info = small_cylinder(ob)
-        kw = dict(stream_mode=ob.STREAM_LINKS, drag=True)
-        monkeypatch.setenv("OCTLB_NO_GRAPH", "1")
-    else:
-        mesh, init, info = cases.cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=8)
-    prec = ob.FP16_SHIFTED if case.endswith("fp16") else ob.FP32
-    drag = kw.get("drag", False)
-    res = []
-    for nofuse in ("1", "0"):
-        monkeypatch.setenv("OCTLB_NO_FUSE", nofuse)
-        lat = ob.GpuLattice(mesh, info["omega"], precision=prec, init_pops=init, **kw)
-        forces = []
-        for _ in range(4):
-            lat.advance(1)
-            forces.append(lat.force() if drag else np.zeros(3))
-        lat.advance(5)
-        launches, _ = lat.step_stats()
-        res.append((lat.get_populations(), np.array(forces), lat.counters(),
-                    lat.force_sum() if drag else (np.zeros(3), 9), launches))
-        lat.close()
-    (p0, f0, c0, s0, l0), (p1, f1, c1, s1, l1) = res
-    assert np.array_equal(p0, p1) and np.array_equal(f0, f1) and c0 == c1
-    assert np.array_equal(s0[0], s1[0]) and s0[1] == s1[1]
-    assert l1 < l0  # the coupler launches are gone
-
-
 def test_body_force_matches_reference(ob, ref):
     """A nonzero per-cell body force: GPU fields and MEM force per coarse step
     against the reference TimeLoop with the same forcing term added at its
