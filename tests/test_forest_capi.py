@@ -147,6 +147,17 @@ def test_create_rejects_bad_tables_without_device(ob):
         ob.GpuLattice(make_tables_mesh(ob), 2.5)                              # omega outside (0, 2)
     with pytest.raises(ob.OctlbError):
         ob.GpuLattice(ob.Mesh(3, [0], [0, 0, 0, 1, 1, 1]), 1.5)               # odd block edge
+    # parameters out of their sets (the ABI's enumerations)
+    for kw in (dict(precision=7), dict(stream_mode=5), dict(coupler_mode=3), dict(stream_order=2),
+               dict(coupler_mode=ob.COUPLER_PHYSICAL, omega_level=[2.5]),
+               dict(stream_order=ob.ORDER_AA),                                  # AA needs a periodic box
+               dict(stream_order=ob.ORDER_AA, drag=True)):
+        with pytest.raises(ob.OctlbError) as e:
+            ob.GpuLattice(make_tables_mesh(ob), 1.5, **kw)
+        assert e.value.code == ob.capi.OCTLB_EINVAL, kw
+    with pytest.raises(ob.OctlbError) as e:
+        ob.GpuLattice(make_tables_mesh(ob, periodic=1), 1.5, stream_order=ob.ORDER_AA, drag=True)
+    assert e.value.code == ob.capi.OCTLB_EINVAL
 
 
 def test_lattice_updates_per_coarse_step(ob):
