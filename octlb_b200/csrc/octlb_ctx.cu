@@ -558,6 +558,15 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       }
     }
   }
+  for (int l = 0; l < nlev; ++l) {
+    for (const PSrc& it : pall[l])
+      if (t->kinds[it.fine_g] != kBulk || t->kinds[it.coarse_g] != kBulk) ctx->cpl_cells_bulk = false;
+    for (const RSrc& it : rall[l]) {
+      if (t->kinds[it.fine_g] != kBulk || t->kinds[it.coarse_g] != kBulk) ctx->cpl_cells_bulk = false;
+      for (int j = 0; j < it.nnb; ++j)
+        if (t->kinds[it.nb_g[j]] != kBulk) ctx->cpl_cells_bulk = false;
+    }
+  }
   // Save rows per source level, keyed by global cell: first every owned cell
   // some item (on any rank) reads, sorted; then the cells of other ranks that
   // this rank's items read, grouped by owner rank and sorted -- each peer's

@@ -172,6 +172,12 @@ struct Level {
   bool use_pair = false;            // two-cells-per-thread step (periodic block)
   bool use_map = false;             // slot-map step (forest level)
   bool aa = false;                  // AA stream order: buf[1] aliases buf[0], cur = layout parity
+  // The finite-difference pass on this level's tree-boundary blocks: one
+  // record per Dirichlet cell, the cells of each role (plane, edge, corner)
+  // as runs of fd_lists, and their rewritten rows.
+  DevBuf fd_cells, fd_lists, fd_new;
+  int fd_rows = 0;
+  std::vector<int> fd_first, fd_count;
   int bulk_grid = 0;
   DevBuf body_force;                // [3][ncore] float, or empty
   bool has_force = false;
@@ -357,18 +363,18 @@ struct octlb_ctx {
   // that the neighbouring slabs fill before every step.
   bool slab = false;
   // Finite-difference domain boundary conditions (octlb_gpu_set_fd_boundary):
-  // one record per Dirichlet cell, the cells of each role (plane, edge,
-  // corner) as runs of fd_lists, the rewritten rows, and the time of the
-  // current advance_one (the inlet ramp's clock).
+  // the records per level (Level::fd_*) and the time of the current
+  // advance_one (the inlet ramp's clock).  cpl_cells_bulk: every coupler
+  // source and target cell is kBulk (the pass on multi-level meshes needs
+  // its interfaces away from the domain faces).
   bool fd_on = false;
-  DevBuf fd_cells, fd_lists, fd_new, fd_time;
-  int fd_rows = 0;
+  DevBuf fd_time;
+  bool cpl_cells_bulk = true;
   // ConstRhoBGK with the pass: per-CTA sums of the velocity cells' collide
   // densities (the boundary part of the statistics), over fd_vel cells
   DevBuf fd_cr_part;
   int fd_cr_parts = 0;
   long long fd_vel = 0;
-  std::vector<int> fd_first, fd_count;
   bool owns(int b) const { return owner.empty() || owner[b] == rank; }
   // Host-only planning of a rank context (octlb_gpu_plan_part): the exchange
   // lists as (level, kind, peer, global cell) records, kind 0 / 1 cells sent /

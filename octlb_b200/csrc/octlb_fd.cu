@@ -144,27 +144,37 @@ struct Builder {
 
 namespace octlb_host {
 
-// The pass after a step of level L: planes, edges, corners, then the
-// Dirichlet collide of the rewritten cells at the next step's time.
+// The pass after a step of level S: the reference's apply_post_stream()
+// after each level's stream runs it on every tree-boundary block of every
+// level (domain_boundary_handler.cpp:81-93), so every level's records run:
+// planes, edges, corners, then the Dirichlet collide of the rewritten cells
+// at the time of that level's next collide -- this advance_one's if the
+// level steps again in it, else the next one's.  (A level that has not
+// stepped since its last pass reads the same state again unless a coupler
+// wrote some of it.)
 template <typename T>
-int fd_after_step(octlb_ctx* ctx, Level& L) {
-  if (!ctx->fd_on || L.nblk == 0) return OCTLB_OK;
-  void* state = cur_buf(L);
-  const FdCell* cells = ctx->fd_cells.as<FdCell>();
-  float* fnew = ctx->fd_new.as<float>();
+int fd_after_step(octlb_ctx* ctx, Level& S) {
+  if (!ctx->fd_on || S.nblk == 0) return OCTLB_OK;
   const double* time = ctx->fd_time.as<double>();
-  const float omega = static_cast<float>(ctx->omega_l[L.lvl]);
-  for (int role = 1; role <= 3; ++role) {
-    const int n = ctx->fd_count[role];
-    if (n == 0) continue;
-    CK(launch_fd_reconstruct<T>(state, L.nslots, L.inv_scale, cells, ctx->fd_lists.as<int>() + ctx->fd_first[role],
-                                n, fnew, time, omega, ctx->const_rho ? ctx->cr_avg.as<double>() : nullptr,
-                                ctx->stream));
+  for (Level& L : ctx->levels) {
+    if (L.nblk == 0 || L.fd_rows == 0) continue;
+    void* state = cur_buf(L);
+    const FdCell* cells = L.fd_cells.as<FdCell>();
+    float* fnew = L.fd_new.as<float>();
+    const float omega = static_cast<float>(ctx->omega_l[L.lvl]);
+    for (int role = 1; role <= 3; ++role) {
+      const int n = L.fd_count[role];
+      if (n == 0) continue;
+      CK(launch_fd_reconstruct<T>(state, L.nslots, L.inv_scale, cells, L.fd_lists.as<int>() + L.fd_first[role], n,
+                                  fnew, time, omega, ctx->const_rho ? ctx->cr_avg.as<double>() : nullptr,
+                                  ctx->stream));
+      ++ctx->launch_count;
+    }
+    const double shift = L.substep < (1 << L.lvl) ? 0.0 : 1.0;
+    CK(launch_fd_collide<T>(state, L.nslots, L.scale, L.inv_scale, cells, L.fd_rows, fnew, time, shift, omega,
+                            ctx->const_rho ? ctx->fd_cr_part.as<double>() : nullptr, ctx->stream));
     ++ctx->launch_count;
   }
-  CK(launch_fd_collide<T>(state, L.nslots, L.scale, L.inv_scale, cells, ctx->fd_rows, fnew, time, 1.0, omega,
-                          ctx->const_rho ? ctx->fd_cr_part.as<double>() : nullptr, ctx->stream));
-  ++ctx->launch_count;
   return OCTLB_OK;
 }
 template int fd_after_step<float>(octlb_ctx*, Level&);
@@ -173,8 +183,8 @@ template int fd_after_step<__half>(octlb_ctx*, Level&);
 // get_fields: the Dirichlet cells' rho and u from their rows (level L's
 // staging arrays, indexed by local core slot).
 int fd_fix_fields(octlb_ctx* ctx, Level& L, double* rho, double* u) {
-  if (!ctx->fd_on || L.nblk == 0) return OCTLB_OK;
-  CK(launch_fd_fields(ctx->fd_cells.as<FdCell>(), ctx->fd_rows, ctx->fd_new.as<float>(), rho, u, ctx->stream));
+  if (!ctx->fd_on || L.nblk == 0 || L.fd_rows == 0) return OCTLB_OK;
+  CK(launch_fd_fields(L.fd_cells.as<FdCell>(), L.fd_rows, L.fd_new.as<float>(), rho, u, ctx->stream));
   return OCTLB_OK;
 }
 
@@ -369,49 +379,69 @@ int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* 
   for (int c : ctx->counters_collide)
     if (c != 0) return fail(ctx, OCTLB_ESTATE, "set_fd_boundary comes before the first advance");
   if (ctx->fd_on) return fail(ctx, OCTLB_ESTATE, "fd boundary already set");
-  if (ctx->max_level != 0)
-    return fail(ctx, OCTLB_EINVAL, "fd boundary: single-level meshes at forest level 0 (one step per advance_one)");
   if (ctx->stream_mode != OCTLB_STREAM_ROTATE || ctx->periodic || ctx->comm)
     return fail(ctx, OCTLB_EINVAL, "fd boundary: one context, rotate stream rule, not periodic");
-  Level& L = ctx->levels[0];
-  if (L.n_bb > 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: the tree-boundary faces must carry no restated fill");
-  std::vector<FdCell> cells;
-  std::vector<int> lists;
-  if (int rc = fd_build(ctx, ctx->n, L.blocks, ctx->kinds.data(), types, u_wall, rho_target, inlet_u, ramp_end_t,
-                        cells, lists, ctx->fd_first, ctx->fd_count))
-    return rc;
-  CK(cudaStreamSynchronize(ctx->stream));
-  CK(upload(ctx->fd_cells, cells));
-  CK(upload(ctx->fd_lists, lists));
-  CK(ctx->fd_new.alloc(cells.size() * kQ * sizeof(float)));
+  int used = 0;
+  for (const Level& L : ctx->levels) {
+    if (L.nblk == 0) continue;
+    ++used;
+    if (L.n_bb > 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: the tree-boundary faces must carry no restated fill");
+  }
+  if (used > 1 && ctx->const_rho)
+    return fail(ctx, OCTLB_EINVAL, "fd boundary with ConstRhoBGK: single-level meshes");
+  if (used > 1 && !ctx->cpl_cells_bulk)
+    return fail(ctx, OCTLB_EINVAL,
+                "fd boundary on a multi-level mesh: every coupler source and target must be a kBulk cell "
+                "(the coarse-fine interfaces away from the domain faces)");
+  std::vector<std::vector<FdCell>> cells(ctx->levels.size());
+  for (size_t l = 0; l < ctx->levels.size(); ++l) {
+    Level& L = ctx->levels[l];
+    if (L.nblk == 0) continue;
+    std::vector<int> lists;
+    if (int rc = fd_build(ctx, ctx->n, L.blocks, ctx->kinds.data(), types, u_wall, rho_target, inlet_u, ramp_end_t,
+                          cells[l], lists, L.fd_first, L.fd_count))
+      return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(upload(L.fd_cells, cells[l]));
+    CK(upload(L.fd_lists, lists));
+    CK(L.fd_new.alloc(cells[l].size() * kQ * sizeof(float)));
+    L.fd_rows = static_cast<int>(cells[l].size());
+  }
   CK(upload(ctx->fd_time, std::vector<double>{0.0}));
-  ctx->fd_rows = static_cast<int>(cells.size());
-  // ConstRhoBGK (chosen before): the velocity cells' collide densities join
-  // its statistics (the reference's kFluidAndBoundary scope)
+  // ConstRhoBGK (chosen before, one level): the velocity cells' collide
+  // densities join its statistics (the reference's kFluidAndBoundary scope)
   double* crp = nullptr;
   if (ctx->const_rho) {
     ctx->fd_vel = 0;
-    for (const FdCell& fc : cells) ctx->fd_vel += fc.kind == kVelocityDirichlet ? 1 : 0;
-    ctx->fd_cr_parts = static_cast<int>(fd_collide_parts(ctx->fd_rows));
+    int rows = 0;
+    for (size_t l = 0; l < cells.size(); ++l) {
+      rows += static_cast<int>(cells[l].size());
+      for (const FdCell& fc : cells[l]) ctx->fd_vel += fc.kind == kVelocityDirichlet ? 1 : 0;
+    }
+    ctx->fd_cr_parts = static_cast<int>(fd_collide_parts(rows));
     CK(ctx->fd_cr_part.alloc(static_cast<size_t>(ctx->fd_cr_parts) * sizeof(double)));
     crp = ctx->fd_cr_part.as<double>();
   }
-  // The first step's collide of the Dirichlet cells (at time 0): the stored
-  // initial state holds them uncollided (the initial collide takes kBulk
-  // cells only); their rows keep that state (the fields before any step).
-  const float omega = static_cast<float>(ctx->omega_l[0]);
-  const FdCell* dc = ctx->fd_cells.as<FdCell>();
-  float* rows = ctx->fd_new.as<float>();
+  // The first step's collide of the Dirichlet cells (at time 0) on every
+  // level: the stored initial state holds them uncollided (the initial
+  // collide takes kBulk cells only); their rows keep that state (the fields
+  // before any step).
   const double* tm = ctx->fd_time.as<double>();
-  if (ctx->precision == OCTLB_FP32) {
-    CK(launch_fd_rows_from_state<float>(L.buf[L.cur].p, L.nslots, L.inv_scale, dc, ctx->fd_rows, rows, ctx->stream));
-    CK(launch_fd_collide<float>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, dc, ctx->fd_rows, rows, tm, 0.0,
-                                omega, crp, ctx->stream));
-  } else {
-    CK(launch_fd_rows_from_state<__half>(L.buf[L.cur].p, L.nslots, L.inv_scale, dc, ctx->fd_rows, rows,
-                                         ctx->stream));
-    CK(launch_fd_collide<__half>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, dc, ctx->fd_rows, rows, tm, 0.0,
-                                 omega, crp, ctx->stream));
+  for (Level& L : ctx->levels) {
+    if (L.nblk == 0 || L.fd_rows == 0) continue;
+    const float omega = static_cast<float>(ctx->omega_l[L.lvl]);
+    const FdCell* dc = L.fd_cells.as<FdCell>();
+    float* rows = L.fd_new.as<float>();
+    if (ctx->precision == OCTLB_FP32) {
+      CK(launch_fd_rows_from_state<float>(L.buf[L.cur].p, L.nslots, L.inv_scale, dc, L.fd_rows, rows, ctx->stream));
+      CK(launch_fd_collide<float>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, dc, L.fd_rows, rows, tm, 0.0,
+                                  omega, crp, ctx->stream));
+    } else {
+      CK(launch_fd_rows_from_state<__half>(L.buf[L.cur].p, L.nslots, L.inv_scale, dc, L.fd_rows, rows,
+                                           ctx->stream));
+      CK(launch_fd_collide<__half>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, dc, L.fd_rows, rows, tm, 0.0,
+                                   omega, crp, ctx->stream));
+    }
   }
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->fd_on = true;

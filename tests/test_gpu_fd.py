@@ -145,3 +145,63 @@ def test_no_slip_walls_and_moving_lid_types(ob, ref):
         rho_g, u_g, rho_r, u_r = run_pair(ob, ref, mesh, init, info["omega"], types, u, np.ones(6), 30, ob.FP32)
         print(f"fd types {types}: u {rel(u_g, u_r):.2e} rho {rel(rho_g, rho_r):.2e}")
         assert rel(u_g, u_r) <= 1e-5 and rel(rho_g, rho_r) <= 1e-5
+
+
+def interior_refined_cavity(ob):
+    """32^3 cavity in 8^3 blocks (forest level 2) with its central 2 x 2 x 2
+    blocks refined one level: the coarse-fine interfaces lie inside, away
+    from every domain face."""
+    from octlb_b200 import Forest, Mesh, TB_WALL, cases
+    f = Forest((1, 1, 1), (0, 0, 0), (0, 0, 0, 1, 1, 1)).refine_uniform(2)
+    f.refine_box((0.3, 0.3, 0.3, 0.7, 0.7, 0.7), 3)
+    f.balance().build()
+    mesh = Mesh.from_forest(f, 8, tree_boundary_spec=cases._tb_spec(f, lambda b, d: [TB_WALL, 0, 0, 0, -1, 0, 0, 0]))
+    assert sorted(set(mesh.levels.tolist())) == [2, 3]
+    return mesh, np.zeros((mesh.n_blocks, 8, 8, 8, 19))
+
+
+@pytest.mark.parametrize("case", ["cavity3d", "inlet_ramp"])
+def test_two_level_mesh(ob, ref, case):
+    """The pass on a two-level mesh: after every level step on every level's
+    tree-boundary blocks, as the reference's apply_post_stream does, and
+    each level's Dirichlet cells collide at that level's next collide (the
+    inlet ramp's clock shows it): cavity3d's walls with the moving lid, and a
+    channel with an inlet ramped over 20 steps and a pressure outlet."""
+    mesh, init = interior_refined_cavity(ob)
+    omega = 1.0 / 0.6
+    if case == "cavity3d":
+        types = [S.INTERPOLATED_VELOCITY] * 6
+        u = np.zeros((6, 3))
+        u[3, 0] = 0.05
+        args = (types, u, np.ones(6), 24, ob.FP32)
+        kw = {}
+    else:
+        types = [S.INTERPOLATED_VELOCITY, S.INTERPOLATED_PRESSURE] + [S.INTERPOLATED_VELOCITY] * 4
+        inlet = np.zeros((6, 3))
+        inlet[0, 0] = 0.02
+        args = (types, np.zeros((6, 3)), np.ones(6), 24, ob.FP32)
+        kw = dict(inlet=inlet, ramp=20.0)
+    rho_g, u_g, rho_r, u_r = run_pair(ob, ref, mesh, init, omega, *args, **kw)
+    print(f"fd two levels {case}: u {rel(u_g, u_r):.2e} rho {rel(rho_g, rho_r):.2e}")
+    assert np.abs(u_r).max() > 0.004
+    assert rel(u_g, u_r) <= 1e-5 and rel(rho_g, rho_r) <= 1e-5
+
+
+def test_two_level_mesh_refusals(ob):
+    """A coarse-fine interface that meets a domain face (the cavity's band
+    under the lid) and ConstRhoBGK on a multi-level mesh are refused."""
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=32, n=8, lid=0.0, tau=0.6, band_cells=8)
+    types = [S.INTERPOLATED_VELOCITY] * 6
+    lat = ob.GpuLattice(ob.stamp_fd_kinds(mesh, types), info["omega"], init_pops=init)
+    with pytest.raises(ob.OctlbError) as e:
+        lat.set_fd_boundary(types)
+    assert e.value.code == ob.capi.OCTLB_EINVAL and "coupler" in str(e.value)
+    lat.close()
+    mesh, init = interior_refined_cavity(ob)
+    lat = ob.GpuLattice(ob.stamp_fd_kinds(mesh, types), 1.0 / 0.6, init_pops=init)
+    lat.set_const_rho(True)
+    with pytest.raises(ob.OctlbError) as e:
+        lat.set_fd_boundary(types)
+    assert e.value.code == ob.capi.OCTLB_EINVAL
+    lat.close()
