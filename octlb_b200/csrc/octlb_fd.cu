@@ -256,7 +256,6 @@ int fd_build(octlb_ctx* ctx, int n, const std::vector<int>& blocks, const uint8_
         cells.push_back(fc);
       }
   }
-  if (cells.empty()) return fail(ctx, OCTLB_EINVAL, "fd boundary: no Dirichlet or bounce-back cells");
   std::vector<int> role(cells.size());
   for (int lb = 0; lb < nblk; ++lb)
     for (long long c = 0; c < n3; ++c) {
@@ -407,6 +406,9 @@ int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* 
     CK(L.fd_new.alloc(cells[l].size() * kQ * sizeof(float)));
     L.fd_rows = static_cast<int>(cells[l].size());
   }
+  size_t total = 0;
+  for (const auto& c : cells) total += c.size();
+  if (total == 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: no Dirichlet or bounce-back cells");
   CK(upload(ctx->fd_time, std::vector<double>{0.0}));
   // ConstRhoBGK (chosen before, one level): the velocity cells' collide
   // densities join its statistics (the reference's kFluidAndBoundary scope)
@@ -463,6 +465,7 @@ int octlb_fd_plan(const octlb_tables* t, const int types[6], const double* u_wal
   if (int rc = fd_build(&ctx, t->n, blocks, t->kinds, types, u_wall, rho_target, inlet_u, ramp_end_t, cells, lists,
                         first, count))
     return rc;
+  if (cells.empty()) return OCTLB_EINVAL;  // no Dirichlet or bounce-back cells
   if (records)
     std::memcpy(records, cells.data(), sizeof(FdCell) * std::min<size_t>(cells.size(), max_records));
   return static_cast<int>(cells.size());
