@@ -189,11 +189,17 @@ int octlb_gpu_average_rho(octlb_ctx* ctx, double* out);
  * u_wall of the y+ face on the interior top-face cells (cavity3d's lid);
  * pressure cells hold rho_target[face].  The cells must carry their kinds in
  * the tables (octlb_fd_stamp_kinds), the faces no restated fill
- * (OCTLB_TB_NONE).  One context, the rotate stream rule, one level at
- * forest level 0, blocks of n >= 4; before the first advance.  With
- * ConstRhoBGK (octlb_gpu_set_const_rho, called first) the velocity cells'
- * collide densities join the average's statistics, as the reference's
- * kFluidAndBoundary scope does (cavity3d's configuration). */
+ * (OCTLB_TB_NONE).  One context, the rotate stream rule, blocks of
+ * n >= 4; before the first advance.  Any number of levels, as the reference
+ * runs it: after every level's stream (an empty level's included) the pass
+ * rewrites the Dirichlet cells of every level's tree-boundary blocks, and
+ * each level's boundary cells collide at the start of its step; on a
+ * multi-level mesh the coarse-fine interfaces must stay away from the
+ * domain faces (every coupler source and target a kBulk cell; OCTLB_EINVAL
+ * otherwise).  With ConstRhoBGK (octlb_gpu_set_const_rho, called first; one
+ * level) the velocity cells' collide densities join the average's
+ * statistics, as the reference's kFluidAndBoundary scope does (cavity3d's
+ * configuration). */
 #define OCTLB_FD_NO_SLIP 0
 #define OCTLB_FD_MOVING_LID 1
 #define OCTLB_FD_VELOCITY 2

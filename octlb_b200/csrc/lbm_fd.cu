@@ -210,12 +210,12 @@ k_fd_reconstruct(const T* state, long long qs, float inv_s, const FdCell* cells,
   }
 }
 
-// The collide of the boundary cells into the state buffer: velocity cells
-// f (1 - omega) + omega feq(rho, u_presc(t)), rho = velocityBMRho on plane
-// cells and 1 + sum f on edges and corners; bounce-back cells the full-way
-// swap; pressure cells unchanged.
-// Source: the rewritten rows (after the pass) or the state itself (the
-// initial state, before the first step).
+// The collide of the boundary cells into the state buffer, at the start of
+// their level's step: velocity cells f (1 - omega) + omega feq(rho,
+// u_presc(t)), rho = velocityBMRho on plane cells and 1 + sum f on edges and
+// corners; bounce-back cells the full-way swap of their streamed state (kept
+// in their row); pressure cells unchanged.  Source: the rows (the last
+// pass's, or the initial state's), or the state itself when fnew is null.
 template <typename T>
 __global__ void __launch_bounds__(kFdThreads)
 k_fd_collide(T* state, long long qs, float scale, float inv_s, const FdCell* cells, int n, float* fnew,
@@ -271,6 +271,18 @@ k_fd_collide(T* state, long long qs, float scale, float inv_s, const FdCell* cel
 
 __global__ void k_fd_tick(double* time) { *time += 1.0; }
 
+// The pass's rewritten rows into the state (velocity and pressure cells; the
+// bounce-back cells keep their streamed populations until their collide).
+template <typename T>
+__global__ void __launch_bounds__(kFdThreads)
+k_fd_store(T* state, long long qs, float scale, const FdCell* cells, int n, const float* fnew) {
+  const int row = blockIdx.x * kFdThreads + threadIdx.x;
+  if (row >= n || cells[row].role == 0) return;
+#pragma unroll
+  for (int i = 0; i < kQ; ++i)
+    Store<T>::st(state + i * qs + cells[row].slot, fnew[static_cast<long long>(row) * kQ + i], scale);
+}
+
 // The Dirichlet cells' populations before their collide (the initial state)
 // into their rows: what the reference holds for them after a step.
 template <typename T>
@@ -285,11 +297,12 @@ k_fd_rows_from_state(const T* state, long long qs, float inv_s, const FdCell* ce
 
 // rho and u of the Dirichlet cells from their rows (the populations after the
 // pass, before the next collide -- the reference's state after the step),
-// over the fields the gather wrote from the stored (collided) state.
+// over the fields the gather wrote; the bounce-back cells' fields are the
+// gathered ones (their streamed state).
 __global__ void __launch_bounds__(kFdThreads)
 k_fd_fields(const FdCell* cells, int n, const float* fnew, double* rho, double* u) {
   const int row = blockIdx.x * kFdThreads + threadIdx.x;
-  if (row >= n) return;
+  if (row >= n || cells[row].role == 0) return;
   double dr = 0, jx = 0, jy = 0, jz = 0;
 #pragma unroll
   for (int i = 0; i < kQ; ++i) {
@@ -347,6 +360,16 @@ cudaError_t launch_fd_fields(const FdCell* cells, int n, const float* fnew, doub
   k_fd_fields<<<fd_grid(n), kFdThreads, 0, s>>>(cells, n, fnew, rho, u);
   return cudaGetLastError();
 }
+
+template <typename T>
+cudaError_t launch_fd_store(void* state, long long qs, float scale, const FdCell* cells, int n, const float* fnew,
+                            cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_fd_store<T><<<fd_grid(n), kFdThreads, 0, s>>>(static_cast<T*>(state), qs, scale, cells, n, fnew);
+  return cudaGetLastError();
+}
+template cudaError_t launch_fd_store<float>(void*, long long, float, const FdCell*, int, const float*, cudaStream_t);
+template cudaError_t launch_fd_store<__half>(void*, long long, float, const FdCell*, int, const float*, cudaStream_t);
 
 cudaError_t launch_fd_tick(double* time, cudaStream_t s) {
   k_fd_tick<<<1, 1, 0, s>>>(time);

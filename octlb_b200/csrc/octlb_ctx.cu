@@ -85,7 +85,9 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
   if (L.nblk == 0) {
     // A rank context with no block on this level still takes part in the
     // level's two exchanges (it may receive save rows for its coupler items).
+    // The finite-difference pass runs after an empty level's step too.
     if (int rc = exchange_cells<T>(ctx, L)) return rc;
+    if (int rc = fd_after_step<T>(ctx, L)) return rc;
     return exchange_rows(ctx, L);  // (slab contexts own every level's block)
   }
   { const int rc = flush_restricts<T>(ctx); if (rc) return rc; }  // the step reads what they write
@@ -101,6 +103,8 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     ++ctx->launch_count;
   }
   if (int rc = ctx->slab ? exchange_slab<T>(ctx, L) : exchange_cells<T>(ctx, L)) return rc;
+  // the finite-difference boundary cells' collide (the step pulls from them)
+  if (int rc = fd_before_step<T>(ctx, L)) return rc;
 
   StepArgs a = L.args;
   a.src = cur;

@@ -405,6 +405,7 @@ int comm_attach(octlb_ctx* ctx);
 int comm_nranks(const octlb_comm* comm);
 // Finite-difference domain boundary pass (octlb_fd.cu).
 template <typename T> int fd_after_step(octlb_ctx* ctx, Level& L);
+template <typename T> int fd_before_step(octlb_ctx* ctx, Level& L);
 int fd_end_of_step(octlb_ctx* ctx);
 int fd_fix_fields(octlb_ctx* ctx, Level& L, double* rho, double* u);
 void clear_graphs(octlb_ctx* ctx);

@@ -27,6 +27,8 @@ cudaError_t launch_fd_tick(double*, cudaStream_t);
 template <typename T>
 cudaError_t launch_fd_rows_from_state(const void*, long long, float, const FdCell*, int, float*, cudaStream_t);
 cudaError_t launch_fd_fields(const FdCell*, int, const float*, double*, double*, cudaStream_t);
+template <typename T>
+cudaError_t launch_fd_store(void*, long long, float, const FdCell*, int, const float*, cudaStream_t);
 }  // namespace octlb_gpu
 
 using namespace octlb_gpu;
@@ -145,16 +147,16 @@ struct Builder {
 namespace octlb_host {
 
 // The pass after a step of level S: the reference's apply_post_stream()
-// after each level's stream runs it on every tree-boundary block of every
-// level (domain_boundary_handler.cpp:81-93), so every level's records run:
-// planes, edges, corners, then the Dirichlet collide of the rewritten cells
-// at the time of that level's next collide -- this advance_one's if the
-// level steps again in it, else the next one's.  (A level that has not
-// stepped since its last pass reads the same state again unless a coupler
-// wrote some of it.)
+// after each level's stream -- an empty level's too -- runs it on every
+// tree-boundary block of every level (domain_boundary_handler.cpp:81-93,
+// time_loop.h:201-214), so every level's records run:
+// planes, edges, corners into the rows, then the rows into the state,
+// uncollided, as the reference rewrites the cells in place -- a later pass
+// on a level that has not stepped since reads them as its "pre" values.
 template <typename T>
 int fd_after_step(octlb_ctx* ctx, Level& S) {
-  if (!ctx->fd_on || S.nblk == 0) return OCTLB_OK;
+  (void)S;
+  if (!ctx->fd_on) return OCTLB_OK;
   const double* time = ctx->fd_time.as<double>();
   for (Level& L : ctx->levels) {
     if (L.nblk == 0 || L.fd_rows == 0) continue;
@@ -170,13 +172,29 @@ int fd_after_step(octlb_ctx* ctx, Level& S) {
                                   ctx->stream));
       ++ctx->launch_count;
     }
-    const double shift = L.substep < (1 << L.lvl) ? 0.0 : 1.0;
-    CK(launch_fd_collide<T>(state, L.nslots, L.scale, L.inv_scale, cells, L.fd_rows, fnew, time, shift, omega,
-                            ctx->const_rho ? ctx->fd_cr_part.as<double>() : nullptr, ctx->stream));
+    CK(launch_fd_store<T>(state, L.nslots, L.scale, cells, L.fd_rows, fnew, ctx->stream));
     ++ctx->launch_count;
   }
   return OCTLB_OK;
 }
+
+// The collide of level L's boundary cells at the start of its step
+// (collide_level's per-cell dispatch, domain_boundary_handler.cpp:60-79), at
+// this advance_one's time, from the rows the last pass left.  Under
+// ConstRhoBGK the velocity cells' collide densities go to the partials the
+// average update then reads.
+template <typename T>
+int fd_before_step(octlb_ctx* ctx, Level& L) {
+  if (!ctx->fd_on || L.nblk == 0 || L.fd_rows == 0) return OCTLB_OK;
+  CK(launch_fd_collide<T>(cur_buf(L), L.nslots, L.scale, L.inv_scale, L.fd_cells.as<FdCell>(), L.fd_rows,
+                          L.fd_new.as<float>(), ctx->fd_time.as<double>(), 0.0,
+                          static_cast<float>(ctx->omega_l[L.lvl]),
+                          ctx->const_rho ? ctx->fd_cr_part.as<double>() : nullptr, ctx->stream));
+  ++ctx->launch_count;
+  return OCTLB_OK;
+}
+template int fd_before_step<float>(octlb_ctx*, Level&);
+template int fd_before_step<__half>(octlb_ctx*, Level&);
 template int fd_after_step<float>(octlb_ctx*, Level&);
 template int fd_after_step<__half>(octlb_ctx*, Level&);
 
@@ -412,7 +430,6 @@ int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* 
   CK(upload(ctx->fd_time, std::vector<double>{0.0}));
   // ConstRhoBGK (chosen before, one level): the velocity cells' collide
   // densities join its statistics (the reference's kFluidAndBoundary scope)
-  double* crp = nullptr;
   if (ctx->const_rho) {
     ctx->fd_vel = 0;
     int rows = 0;
@@ -422,28 +439,20 @@ int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* 
     }
     ctx->fd_cr_parts = static_cast<int>(fd_collide_parts(rows));
     CK(ctx->fd_cr_part.alloc(static_cast<size_t>(ctx->fd_cr_parts) * sizeof(double)));
-    crp = ctx->fd_cr_part.as<double>();
   }
-  // The first step's collide of the Dirichlet cells (at time 0) on every
-  // level: the stored initial state holds them uncollided (the initial
-  // collide takes kBulk cells only); their rows keep that state (the fields
-  // before any step).
-  const double* tm = ctx->fd_time.as<double>();
+  // The rows start as the stored initial state of the boundary cells,
+  // which the initial collide left uncollided (it takes kBulk cells only):
+  // the first step's collide starts from them (and the fields before any
+  // step read them).
   for (Level& L : ctx->levels) {
     if (L.nblk == 0 || L.fd_rows == 0) continue;
-    const float omega = static_cast<float>(ctx->omega_l[L.lvl]);
     const FdCell* dc = L.fd_cells.as<FdCell>();
     float* rows = L.fd_new.as<float>();
-    if (ctx->precision == OCTLB_FP32) {
+    if (ctx->precision == OCTLB_FP32)
       CK(launch_fd_rows_from_state<float>(L.buf[L.cur].p, L.nslots, L.inv_scale, dc, L.fd_rows, rows, ctx->stream));
-      CK(launch_fd_collide<float>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, dc, L.fd_rows, rows, tm, 0.0,
-                                  omega, crp, ctx->stream));
-    } else {
+    else
       CK(launch_fd_rows_from_state<__half>(L.buf[L.cur].p, L.nslots, L.inv_scale, dc, L.fd_rows, rows,
                                            ctx->stream));
-      CK(launch_fd_collide<__half>(L.buf[L.cur].p, L.nslots, L.scale, L.inv_scale, dc, L.fd_rows, rows, tm, 0.0,
-                                   omega, crp, ctx->stream));
-    }
   }
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->fd_on = true;
