@@ -100,7 +100,10 @@ struct Builder {
     if (k == kPressureDirichlet) {  // ExtrapolatedU: the inward neighbour's velocity
       int d, o;
       flat(p, d, o);
-      if (d < 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: a pressure cell off the faces' planes");
+      if (d < 0) {  // a block-rim cell (an edge or corner of its block): u = 0 (interpolated_velocity.h:297-305)
+        out = {0, kFdZero, flips};
+        return OCTLB_OK;
+      }
       p[d] -= o;
       return resolve_u(p, flips, out, depth + 1);
     }
@@ -120,9 +123,8 @@ struct Builder {
     const int k = kind(p);
     int d, o;
     flat(p, d, o);
-    if (k == kPressureDirichlet) {
-      if (d < 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: a pressure cell off the faces' planes");
-      out = {0, static_cast<float>(rho_target[2 * d + (o > 0)]), kFdRhoConst, 0, 0, 0};
+    if (k == kPressureDirichlet) {  // PrescribedRho (interpolated_velocity.h:320-330): 1 off a flat face
+      out = {0, d < 0 ? 1.f : static_cast<float>(rho_target[2 * d + (o > 0)]), kFdRhoConst, 0, 0, 0};
       return OCTLB_OK;
     }
     const int row = (*row_of)[cell(p)];

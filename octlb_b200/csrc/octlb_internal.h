@@ -167,10 +167,11 @@ struct DragItem {
 // Finite-difference domain boundary pass (lbm_fd.cu): one record per
 // velocity- or pressure-Dirichlet cell (its row), with every read of its
 // stencil resolved on the host.  Velocity reads: kFdZero (the overlap padding
-// at rest), kFdFluid (idx = slot: the velocity of the populations there),
+// at rest, or a pressure cell on an edge or corner of its block), kFdFluid (idx = slot: the velocity of the populations there),
 // kFdPrescribed (idx = row: that boundary cell's prescribed velocity); flip
 // bit a negates component a (a mirror image across face a).  Density reads:
-// kFdRhoConst (val), 1 + sum f of the populations before the pass (idx =
+// kFdRhoConst (val: a pressure cell's target density, 1 on its block's edges
+// and corners and in the padding), 1 + sum f of the populations before the pass (idx =
 // slot) or of a rewritten row (idx = row), or velocityBMRho of either with
 // face (d, o) and the prescribed velocity of row urow.
 enum : int { kFdZero = 0, kFdFluid = 1, kFdPrescribed = 2 };

@@ -150,7 +150,10 @@ class Block:
         if k == VELOCITY:
             return self.prescribed_u(*cell)
         if k == PRESSURE:  # ExtrapolatedU: the inward neighbour's velocity
-            d, o = self.flat(*cell)
+            fl = self.flat(*cell)
+            if fl is None:  # a block-rim cell: u = 0 (interpolated_velocity.h:297-305)
+                return np.zeros(3)
+            d, o = fl
             nb = list(cell)
             nb[d] -= o
             return self.compute_u(tuple(nb))
@@ -160,9 +163,9 @@ class Block:
         if not self.inside(cell):
             return 1.0 if self.padding(cell) else self.compute_rho(self.mirror(cell), reader)
         k = self.kinds[cell]
-        if k == PRESSURE:
-            d, o = self.flat(*cell)
-            return self.rho_target[2 * d + (o > 0)]
+        if k == PRESSURE:  # PrescribedRho (interpolated_velocity.h:320-330): 1 off a flat face
+            fl = self.flat(*cell)
+            return 1.0 if fl is None else self.rho_target[2 * fl[0] + (fl[1] > 0)]
         f = self.pops(cell, reader)
         if k == VELOCITY:
             fl = self.flat(*cell)

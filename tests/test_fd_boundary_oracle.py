@@ -2,14 +2,16 @@
 ConcreteDomainBoundaryHandler (Skordos InterpolatedVelocity and pressure
 Dirichlet, interpolated_velocity.h:571-1037, domain_boundary_handler.cpp:
 60-89) installed in the reference TimeLoop by oracle.Sim.set_fd_boundary.
-The GPU path does not have these conditions yet. These CPU tests pin the
-oracle it will be checked against, on properties of the reconstruction:
+These CPU tests pin that oracle, and the restatement of the pass in
+oracle/fd_boundary.py, which the GPU path is checked against, on properties
+of the reconstruction and against the reference's own states:
 * a rest state is a fixed point, as in the reference's
   test_interpolated_velocity_compute_rho.cpp equilibrium cases;
 * after the post-stream reconstruction every boundary cell carries its
   prescribed velocity, and every plane pressure cell its target density;
 * ConstRhoBGK's statistics include the boundary cells."""
 import numpy as np
+import pytest
 
 from oracle import oracle
 
@@ -198,12 +200,16 @@ def test_fd_step_restated_phase_by_phase(ref):
     assert np.abs(p - P[4]).max() <= 1e-14
 
 
-def test_restated_pass_matches_the_reference_per_block(ref):
+@pytest.mark.parametrize("outlet", [False, True])
+def test_restated_pass_matches_the_reference_per_block(ref, outlet):
     """Eight blocks (2 x 2 x 2 level-0 bricks of 8^3): the reference applies
     the reconstruction per block with face, edge and corner roles from the
     block's own extents, so block rims on a domain face are edges and the
-    lid moves only on each block's interior top-face cells.  The restatement
-    does the same and matches block by block."""
+    lid moves only on each block's interior top-face cells.  With a pressure
+    outlet on x+ (target density 1.002) the outlet spans four blocks: its
+    cells on a block rim read u = 0 and density 1 (ExtrapolatedU and
+    PrescribedRho off a flat face).  The restatement does the same and
+    matches block by block."""
     import os
     import sys
     sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
@@ -213,14 +219,21 @@ def test_restated_pass_matches_the_reference_per_block(ref):
     init = np.zeros((mesh.n_blocks, 8, 8, 8, 19))
     u = np.zeros((6, 3))
     u[3, 0] = 0.05
+    types = [S.INTERPOLATED_VELOCITY] * 6
+    rho_t = np.ones(6)
+    if outlet:
+        types[1] = S.INTERPOLATED_PRESSURE
+        rho_t[1] = 1.002
     sim = S(ref, mesh, info["omega"], init)
-    sim.set_fd_boundary([S.INTERPOLATED_VELOCITY] * 6, u)
+    sim.set_fd_boundary(types, u, rho_target=rho_t)
     sim.advance(15)
     before, after = sim.advance_phases()
     kinds = sim.kinds()
     assert np.abs(after - before).max() > 1e-3
+    if outlet:
+        assert np.count_nonzero(kinds == fb.PRESSURE) > 0
     for b in range(mesh.n_blocks):
-        got = fb.reconstruct(before[b], kinds[b], info["omega"], u_lid=u[3])
+        got = fb.reconstruct(before[b], kinds[b], info["omega"], u_lid=u[3], rho_target=rho_t)
         assert np.abs(got - after[b]).max() <= 1e-14, b
 
 

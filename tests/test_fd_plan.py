@@ -187,6 +187,25 @@ def test_eight_blocks_roles_from_block_extents(ob):
     check(ob, mesh, [ob.FD_VELOCITY] * 6, u, np.ones(6))
 
 
+def test_pressure_outlet_across_blocks(ob):
+    """A pressure outlet on x+ spanning four 8^3 blocks: its cells on a
+    block's rim are edges and corners of that block, whose velocity reads
+    give 0 and density reads 1 (the reference's ExtrapolatedU and
+    PrescribedRho off a flat face), beside an inlet on x-."""
+    sys.path.insert(0, HERE)
+    from test_const_rho import brick_cavity
+    mesh, info = brick_cavity(lid=0.0, n=8)
+    types = [ob.FD_VELOCITY, ob.FD_PRESSURE] + [ob.FD_VELOCITY] * 4
+    inlet = np.zeros((6, 3))
+    inlet[0, 0] = 0.02
+    rho = np.ones(6)
+    rho[1] = 1.002
+    rec = check(ob, mesh, types, np.zeros((6, 3)), rho, inlet, ramp=20.0, t=9.0)
+    p = rec[rec["kind"] == 6]
+    assert set(np.unique(p["role"])) == {1, 2, 3}
+    assert np.any(p["u"]["code"][p["role"] >= 2][:, 0] == 0)
+
+
 def test_no_slip_walls_and_lid(ob):
     """No-slip faces (kBounceBack: the collide's full-way swap, no
     reconstruction) around an InterpolatedVelocity lid: the lid's edge and

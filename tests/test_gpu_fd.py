@@ -9,7 +9,9 @@ oracle.Sim.set_fd_boundary): the fields after N steps, FP32 <= 1e-5 relative
 * a channel: a uniform inlet on x- ramped over 20 steps, a pressure outlet
   on x+ (target density 1), velocity walls elsewhere;
 * eight 8^3 blocks (the roles of a block's rim cells come from its own
-  extents, as in the reference);
+  extents, as in the reference), with the lid or with a pressure outlet
+  spanning four blocks;
+* two-level meshes (the pass after every level's step);
 * a rest state stays exactly at rest."""
 import os
 import sys
@@ -68,16 +70,30 @@ def test_inlet_and_pressure_outlet(ob, ref):
     assert rel(u_g, u_r) <= 1e-5 and rel(rho_g, rho_r) <= 1e-5
 
 
-def test_eight_blocks(ob, ref):
+@pytest.mark.parametrize("outlet", [False, True])
+def test_eight_blocks(ob, ref, outlet):
+    """Eight 8^3 blocks: the lid, or an inlet on x- against a pressure outlet
+    on x+ that spans four blocks (its block-rim cells read u = 0 and
+    density 1, as the reference's view does off a flat face)."""
     sys.path.insert(0, HERE)
     from test_const_rho import brick_cavity
     mesh, info = brick_cavity(lid=0.0, n=8)
     init = np.zeros((mesh.n_blocks, 8, 8, 8, 19))
+    types = [S.INTERPOLATED_VELOCITY] * 6
     u = np.zeros((6, 3))
-    u[3, 0] = 0.05
-    rho_g, u_g, rho_r, u_r = run_pair(ob, ref, mesh, init, info["omega"], [S.INTERPOLATED_VELOCITY] * 6, u,
-                                      np.ones(6), 30, ob.FP32)
-    print(f"fd 8 blocks: u {rel(u_g, u_r):.2e} rho {rel(rho_g, rho_r):.2e}")
+    rho_t = np.ones(6)
+    kw = {}
+    if outlet:
+        types[1] = S.INTERPOLATED_PRESSURE
+        rho_t[1] = 1.002
+        inlet = np.zeros((6, 3))
+        inlet[0, 0] = 0.02
+        kw = dict(inlet=inlet, ramp=10.0)
+    else:
+        u[3, 0] = 0.05
+    rho_g, u_g, rho_r, u_r = run_pair(ob, ref, mesh, init, info["omega"], types, u, rho_t, 30, ob.FP32, **kw)
+    print(f"fd 8 blocks (outlet {outlet}): u {rel(u_g, u_r):.2e} rho {rel(rho_g, rho_r):.2e}")
+    assert np.abs(u_r).max() > 0.004
     assert rel(u_g, u_r) <= 1e-5 and rel(rho_g, rho_r) <= 1e-5
 
 
@@ -166,7 +182,8 @@ def test_two_level_mesh(ob, ref, case):
     tree-boundary blocks, as the reference's apply_post_stream does, and
     each level's Dirichlet cells collide at that level's next collide (the
     inlet ramp's clock shows it): cavity3d's walls with the moving lid, and a
-    box with an inlet on x- ramped over 20 steps."""
+    box with an inlet on x- ramped over 20 steps against a pressure outlet
+    on x+ spanning sixteen blocks."""
     mesh, init = interior_refined_cavity(ob)
     omega = 1.0 / 0.6
     if case == "cavity3d":
@@ -175,8 +192,8 @@ def test_two_level_mesh(ob, ref, case):
         u[3, 0] = 0.05
         args = (types, u, np.ones(6), 24, ob.FP32)
         kw = {}
-    else:  # (a pressure face spanning several blocks is not built: its block-rim cells)
-        types = [S.INTERPOLATED_VELOCITY] * 6
+    else:
+        types = [S.INTERPOLATED_VELOCITY, S.INTERPOLATED_PRESSURE] + [S.INTERPOLATED_VELOCITY] * 4
         inlet = np.zeros((6, 3))
         inlet[0, 0] = 0.02
         args = (types, np.zeros((6, 3)), np.ones(6), 24, ob.FP32)
