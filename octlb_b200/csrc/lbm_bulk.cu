@@ -1,4 +1,8 @@
-// Pipelined fused step for one periodic block (the throughput path).
+// Pipelined fused steps for one periodic block fed by bulk async copies:
+// k_step_bulk (one cell per thread, FP32 or FP16, an option),
+// k_step_rows_h (four FP16 cells per thread: the FP16 default, and the AA
+// order's local step) and k_step_aa_rows_h (the AA order's FP16 pull step,
+// drained by bulk stores too).
 //
 // A persistent CTA of n threads walks z-rows (x, y).  For each row it needs
 // the 19 source rows (x - cx_i, y - cy_i) of the 19 population planes; an
@@ -17,7 +21,7 @@
 // the host reports OCTLB_ETIMEOUT (OCTLB_ECUDA after a failed drain).
 // StepArgs::stall_first_row makes CTA 0 skip issuing its first row, so its
 // first wait runs out: the test of this path (no fault, no hang).
-#include "octlb_internal.h"
+#include "lbm_device.cuh"
 
 namespace octlb_gpu {
 namespace {
@@ -66,6 +70,20 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
+
+// Bulk async stores (shared -> global) of this thread's bulk group, and the
+// proxy fence that orders a CTA's generic shared-memory writes before them.
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// this thread's committed stores have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// ... and are complete in global memory
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_smem_to_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 template <typename T>
 __device__ __forceinline__ void issue_row(const StepArgs& a, const T* src, T* stage, uint64_t* bar,
@@ -154,6 +172,290 @@ __global__ void __launch_bounds__(1024) k_step_bulk(const StepArgs a) {
   }
 }
 
+// FP16-shifted step of one periodic all-kBulk block, four z cells per
+// thread, fed by bulk async copies.  A CTA of THREADS threads computes
+// stages of 4 THREADS consecutive cells: R = 4 THREADS / n whole z rows
+// (x, y0 .. y0 + R - 1) of one x plane.  For each population a lane of warp
+// 0 copies the R source rows (x - cx_i, y0 - cy_i ..), one contiguous run or
+// two at the y wrap, into the stage's shared-memory buffer, STAGES - 1
+// stages ahead of the compute, so the loads stay in flight through the
+// arithmetic without the occupancy the register-heavy four-cell collide
+// lacks.  Per cell the values read, the arithmetic and the 8-byte stores
+// are k_step_quad_h's, so the results are bitwise equal.  Waits are bounded
+// as in k_step_bulk.  n a power of two dividing 4 THREADS, n >= 8; the
+// population stride qs a multiple of 8 (16-byte aligned rows).
+// Direction components as bit masks, for a population index known only at
+// run time (one lane per population).
+__host__ __device__ constexpr uint32_t dir_mask(int axis, int sign) {
+  uint32_t m = 0;
+  for (int i = 0; i < kQ; ++i)
+    if ((axis == 0 ? cx(i) : axis == 1 ? cy(i) : cz(i)) == sign) m |= 1u << i;
+  return m;
+}
+constexpr uint32_t kXPos = dir_mask(0, 1), kXNeg = dir_mask(0, -1);
+constexpr uint32_t kYPos = dir_mask(1, 1), kYNeg = dir_mask(1, -1);
+__device__ __forceinline__ int dir_rt(int axis, int i) {
+  const uint32_t pos = axis == 0 ? kXPos : kYPos, neg = axis == 0 ? kXNeg : kYNeg;
+  return static_cast<int>((pos >> i) & 1u) - static_cast<int>((neg >> i) & 1u);
+}
+
+// The R source rows of population i of a stage -- rows (x - cx_i, y0 - cy_i
+// .. y0 - cy_i + R - 1) of plane i, one contiguous run or two at the y wrap --
+// as (global, shared, bytes) runs handed to f.
+// Unshifted (the AA order's local step): rows (x, y0 .. y0 + R - 1) of
+// plane i, one run.
+template <typename F>
+__device__ __forceinline__ void pop_runs_h(const StepArgs& a, __half* pops, __half* stage, uint32_t row0, uint32_t R,
+                                           uint32_t cells, int i, F&& f, bool shifted = true) {
+  const uint32_t n = a.n;
+  const int ci = shifted ? dir_rt(0, i) : 0, cj = shifted ? dir_rt(1, i) : 0;
+  const uint32_t x = a.div_n.div(row0), y0 = row0 - x * n;
+  const uint32_t xs = ci == 1 ? (x == 0 ? static_cast<uint32_t>(a.wrap_lo) : x - 1)
+                              : (ci == -1 ? (x == n - 1 ? static_cast<uint32_t>(a.wrap_hi) : x + 1) : x);
+  __half* plane = pops + i * a.qs + static_cast<long long>(xs) * n * n;
+  __half* d = stage + i * cells;
+  const int ys = static_cast<int>(y0) - cj;
+  const uint32_t rb = n * sizeof(__half);
+  if (ys >= 0 && ys + static_cast<int>(R) <= static_cast<int>(n)) {
+    f(plane + static_cast<long long>(ys) * n, d, R * rb);
+  } else if (ys < 0) {  // rows n - 1, 0 .. R - 2
+    f(plane + static_cast<long long>(n - 1) * n, d, rb);
+    if (R > 1) f(plane, d + n, (R - 1) * rb);
+  } else {              // rows y0 + 1 .. n - 1, 0
+    if (R > 1) f(plane + static_cast<long long>(ys) * n, d, (R - 1) * rb);
+    f(plane, d + (R - 1) * n, rb);
+  }
+}
+__device__ __forceinline__ void issue_pop_h(const StepArgs& a, const __half* src, __half* stage, uint64_t* bar,
+                                            uint32_t row0, uint32_t R, uint32_t cells, int i, bool shifted) {
+  pop_runs_h(
+      a, const_cast<__half*>(src), stage, row0, R, cells, i,
+      [&](__half* g, __half* sm, uint32_t bytes) { bulk_g2s(sm, g, bytes, bar); }, shifted);
+}
+
+// Warp 0 requests a stage: lane 0 arms the barrier with the stage's bytes,
+// then lanes 0..18 copy one population each.  (Measured on the 256^3 box:
+// one lane issuing all 19 made the step 0.2385 ms instead of 0.2077.)
+__device__ __forceinline__ void issue_stage_h(const StepArgs& a, const __half* src, __half* stage, uint64_t* bar,
+                                              uint32_t row0, uint32_t R, uint32_t cells, uint32_t lane,
+                                              bool shifted = true) {
+  if (lane == 0) mbar_expect_tx(bar, static_cast<uint32_t>(kQ * cells * sizeof(__half)));
+  __syncwarp();
+  if (lane < static_cast<uint32_t>(kQ))
+    issue_pop_h(a, src, stage, bar, row0, R, cells, static_cast<int>(lane), shifted);
+}
+
+// LOCAL: the AA order's step from the reversed layout -- each cell's own
+// slots, population i from plane opp(i), written to plane i; no shifts, the
+// same values and arithmetic as k_step_aa_local_h (in place: every stage
+// reads and writes only its own cells' slots).
+template <int THREADS, int STAGES, int MINB, bool LOCAL>
+__global__ void __launch_bounds__(THREADS, MINB) k_step_rows_h(const StepArgs a) {
+  constexpr uint32_t kCells = 4 * THREADS;
+  constexpr uint32_t kStageElems = kQ * kCells;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __half* stages = reinterpret_cast<__half*>(smem_raw);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + static_cast<size_t>(STAGES) * kStageElems * sizeof(__half));
+  const __half* src = static_cast<const __half*>(a.src);
+  __half* dst = static_cast<__half*>(a.dst);
+  const uint32_t n = a.n;
+  const uint32_t R = kCells / n;
+  const uint32_t nst = static_cast<uint32_t>(a.ncore / kCells);
+  // this thread's four cells within a stage: row r, z .. z + 3
+  const uint32_t c = 4 * threadIdx.x;
+  const uint32_t lg = static_cast<uint32_t>(__ffs(static_cast<int>(n)) - 1);
+  const uint32_t r = c >> lg, z = c & (n - 1);
+  const uint32_t zm1 = z == 0 ? n - 1 : z - 1, zp4 = z + 4 == n ? 0 : z + 4;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  pdl_wait();
+
+  const uint32_t mine = blockIdx.x < nst ? (nst - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint32_t lane = threadIdx.x;  // < 32: warp 0, the requesting warp
+  uint32_t issued = 0;                // warp 0: stages in flight, bit k % STAGES
+  if (threadIdx.x < 32) {
+    for (uint32_t k = 0; k < mine && k < STAGES - 1; ++k) {
+      if (k == 0 && a.stall_first_row && blockIdx.x == 0) continue;
+      issue_stage_h(a, src, stages + k * kStageElems, &bars[k], (blockIdx.x + k * gridDim.x) * R, R, kCells, lane,
+                    !LOCAL);
+      issued |= 1u << k;
+    }
+  }
+  for (uint32_t k = 0; k < mine; ++k) {
+    const uint32_t s = k % STAGES;
+    bool ok = mbar_wait_bounded(&bars[s], (k / STAGES) & 1, a.wait_ns);
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok) {
+      if (threadIdx.x == 0) {
+        int code = kErrBulkTimeout;
+        for (uint32_t j = k; j < mine && j < k + STAGES - 1; ++j)
+          if ((issued >> (j % STAGES)) & 1u)
+            if (!mbar_wait_bounded(&bars[j % STAGES], (j / STAGES) & 1, a.wait_ns)) code = kErrBulkDrainTimeout;
+        atomicMax(a.err, code);
+      }
+      return;
+    }
+    if (threadIdx.x < 32) {
+      issued &= ~(1u << s);
+      // every thread has finished reading stage (k - 1) % STAGES: refill it
+      if (k + STAGES - 1 < mine) {
+        const uint32_t kk = k + STAGES - 1;
+        issue_stage_h(a, src, stages + (kk % STAGES) * kStageElems, &bars[kk % STAGES],
+                      (blockIdx.x + kk * gridDim.x) * R, R, kCells, lane, !LOCAL);
+        issued |= 1u << (kk % STAGES);
+      }
+    }
+    const __half* S = stages + s * kStageElems + r * n;
+    float f0[kQ], f1[kQ], f2[kQ], f3[kQ];
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      if constexpr (LOCAL) {
+        ld4h(S + opp(i) * kCells + z, f0[i], f1[i], f2[i], f3[i]);
+        continue;
+      }
+      const __half* p = S + i * kCells;
+      if (cz(i) == 0) {
+        ld4h(p + z, f0[i], f1[i], f2[i], f3[i]);
+      } else if (cz(i) == 1) {  // cells z..z+3 pull z-1..z+2
+        float w;
+        ld4h(p + z, f1[i], f2[i], f3[i], w);
+        f0[i] = __half2float(p[zm1]);
+      } else {                  // cells z..z+3 pull z+1..z+4
+        float w;
+        ld4h(p + z, w, f0[i], f1[i], f2[i]);
+        f3[i] = __half2float(p[zp4]);
+      }
+    }
+    bgk<false>(f0, a.omega, a.scale, a.inv_scale);
+    bgk<false>(f1, a.omega, a.scale, a.inv_scale);
+    bgk<false>(f2, a.omega, a.scale, a.inv_scale);
+    bgk<false>(f3, a.omega, a.scale, a.inv_scale);
+    __half* o = dst + static_cast<long long>(blockIdx.x + k * gridDim.x) * kCells + c;
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) st4h(o + i * a.qs, f0[i], f1[i], f2[i], f3[i]);
+  }
+}
+
+// The AA order's pull step (natural -> reversed layout) in FP16, staged the
+// same way: the 19 source rows of a stage come in by bulk copies; each cell
+// collides its pulled values and writes g_opp(k) back into the shared-memory
+// slot it read for direction k; the stage's rows then go back by bulk stores
+// to the global rows they came from.  Every slot belongs to one cell (a
+// thread's 8-byte read may include a neighbour's slot, whose value it does
+// not use), and a population's source rows of different stages are disjoint,
+// so the in-place update needs no ordering between threads before the
+// write-back or between CTAs.  Per cell the values and the arithmetic are
+// k_step_aa_pull_h's: bitwise equal.  A buffer is refilled once the lane that
+// stored a population's rows from it has seen its stores read out.
+template <int THREADS, int STAGES, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) k_step_aa_rows_h(const StepArgs a) {
+  constexpr uint32_t kCells = 4 * THREADS;
+  constexpr uint32_t kStageElems = kQ * kCells;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __half* stages = reinterpret_cast<__half*>(smem_raw);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + static_cast<size_t>(STAGES) * kStageElems * sizeof(__half));
+  __half* pops = static_cast<__half*>(a.dst);  // == a.src
+  const uint32_t n = a.n;
+  const uint32_t R = kCells / n;
+  const uint32_t nst = static_cast<uint32_t>(a.ncore / kCells);
+  const uint32_t c = 4 * threadIdx.x;
+  const uint32_t lg = static_cast<uint32_t>(__ffs(static_cast<int>(n)) - 1);
+  const uint32_t r = c >> lg, z = c & (n - 1);
+  const uint32_t zm1 = z == 0 ? n - 1 : z - 1, zp4 = z + 4 == n ? 0 : z + 4;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  pdl_wait();
+
+  const uint32_t mine = blockIdx.x < nst ? (nst - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint32_t lane = threadIdx.x;  // < 32: warp 0, the copying warp
+  uint32_t issued = 0;                // warp 0: loads in flight, bit k % STAGES
+  if (threadIdx.x < 32) {
+    for (uint32_t k = 0; k < mine && k < STAGES - 1; ++k) {
+      if (k == 0 && a.stall_first_row && blockIdx.x == 0) continue;
+      issue_stage_h(a, pops, stages + k * kStageElems, &bars[k], (blockIdx.x + k * gridDim.x) * R, R, kCells, lane);
+      issued |= 1u << k;
+    }
+  }
+  for (uint32_t k = 0; k < mine; ++k) {
+    const uint32_t s = k % STAGES;
+    if (threadIdx.x < 32 && k + STAGES - 1 < mine) {
+      // the buffer of stage k - 1: every thread wrote it before that stage's
+      // stores were issued; refill it once they have read it out
+      const uint32_t kk = k + STAGES - 1, b = kk % STAGES;
+      bulk_wait_read_all();
+      issue_stage_h(a, pops, stages + b * kStageElems, &bars[b], (blockIdx.x + kk * gridDim.x) * R, R, kCells, lane);
+      issued |= 1u << b;
+    }
+    bool ok = mbar_wait_bounded(&bars[s], (k / STAGES) & 1, a.wait_ns);
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok) {
+      if (threadIdx.x < 32) bulk_wait_all();
+      if (threadIdx.x == 0) {
+        int code = kErrBulkTimeout;
+        for (uint32_t j = k; j < mine && j < k + STAGES; ++j)
+          if ((issued >> (j % STAGES)) & 1u)
+            if (!mbar_wait_bounded(&bars[j % STAGES], (j / STAGES) & 1, a.wait_ns)) code = kErrBulkDrainTimeout;
+        atomicMax(a.err, code);
+      }
+      return;
+    }
+    if (threadIdx.x < 32) issued &= ~(1u << s);
+    __half* S = stages + s * kStageElems + r * n;
+    float f0[kQ], f1[kQ], f2[kQ], f3[kQ];
+#pragma unroll
+    for (int i = 0; i < kQ; ++i) {
+      const __half* p = S + i * kCells;
+      if (cz(i) == 0) {
+        ld4h(p + z, f0[i], f1[i], f2[i], f3[i]);
+      } else if (cz(i) == 1) {  // cells z..z+3 pull z-1..z+2
+        float w;
+        ld4h(p + z, f1[i], f2[i], f3[i], w);
+        f0[i] = __half2float(p[zm1]);
+      } else {                  // cells z..z+3 pull z+1..z+4
+        float w;
+        ld4h(p + z, w, f0[i], f1[i], f2[i]);
+        f3[i] = __half2float(p[zp4]);
+      }
+    }
+    bgk<false>(f0, a.omega, a.scale, a.inv_scale);
+    bgk<false>(f1, a.omega, a.scale, a.inv_scale);
+    bgk<false>(f2, a.omega, a.scale, a.inv_scale);
+    bgk<false>(f3, a.omega, a.scale, a.inv_scale);
+#pragma unroll
+    for (int k2 = 0; k2 < kQ; ++k2) {
+      __half* p = S + k2 * kCells;
+      const int o = opp(k2);
+      if (cz(k2) == 0) {          // slots z..z+3
+        st4h(p + z, f0[o], f1[o], f2[o], f3[o]);
+      } else if (cz(k2) == 1) {   // slots z-1, z..z+1, z+2
+        p[zm1] = __float2half_rn(f0[o]);
+        *reinterpret_cast<__half2*>(p + z) = __floats2half2_rn(f1[o], f2[o]);
+        p[z + 2] = __float2half_rn(f3[o]);
+      } else {                    // slots z+1, z+2..z+3, z+4
+        p[z + 1] = __float2half_rn(f0[o]);
+        *reinterpret_cast<__half2*>(p + z + 2) = __floats2half2_rn(f1[o], f2[o]);
+        p[zp4] = __float2half_rn(f3[o]);
+      }
+    }
+    fence_smem_to_async();
+    __syncthreads();
+    if (threadIdx.x < static_cast<uint32_t>(kQ)) {
+      pop_runs_h(a, pops, stages + s * kStageElems, (blockIdx.x + k * gridDim.x) * R, R, kCells,
+                 static_cast<int>(lane), [](__half* g, __half* sm, uint32_t bytes) { bulk_s2g(g, sm, bytes); });
+      bulk_commit();
+    }
+  }
+  if (threadIdx.x < 32) bulk_wait_all();
+}
+
 }  // namespace
 
 // Eligible: one periodic all-kBulk block, n threads per CTA, rows of 16-byte
@@ -182,6 +484,117 @@ template <typename T>
 cudaError_t launch_step_bulk(const StepArgs& a, int grid, cudaStream_t s) {
   k_step_bulk<T><<<grid, a.n, bulk_step_smem(a.n, sizeof(T)), s>>>(a);
   return cudaGetLastError();
+}
+
+// The staged FP16 step's launch shapes: threads, stages, and the CTAs per
+// SM the register budget is set for.  Per step on the 256^3 box, two boxes:
+// 0 (256 x 2) 0.2077 / 0.2058 ms, 1 (128 x 2) 0.2070 / 0.2169, 2 (128 x 3)
+// 0.2129 / 0.2306, 3 (64 x 2) 0.2130, 4 (64 x 3) 0.2521; k_step_quad_h
+// 0.2210 / 0.2213.
+namespace {
+constexpr int kRowsVariants = 5;
+constexpr int kRowsThreads[kRowsVariants] = {256, 128, 128, 64, 64};
+constexpr int kRowsStages[kRowsVariants] = {2, 2, 3, 2, 3};
+constexpr int rows_threads(int v) { return kRowsThreads[v]; }
+constexpr int rows_stages(int v) { return kRowsStages[v]; }
+size_t rows_smem(int v) {
+  return static_cast<size_t>(rows_stages(v)) * kQ * 4 * rows_threads(v) * sizeof(__half) +
+         rows_stages(v) * sizeof(uint64_t);
+}
+template <bool LOCAL, typename F>
+auto with_rows_kernel_t(int v, F&& f) {
+  switch (v) {
+    case 1: return f(k_step_rows_h<128, 2, 4, LOCAL>);
+    case 2: return f(k_step_rows_h<128, 3, 3, LOCAL>);
+    case 3: return f(k_step_rows_h<64, 2, 8, LOCAL>);
+    case 4: return f(k_step_rows_h<64, 3, 7, LOCAL>);
+    default: return f(k_step_rows_h<256, 2, 2, LOCAL>);
+  }
+}
+template <typename F>
+auto with_rows_kernel(int v, bool local, F&& f) {
+  return local ? with_rows_kernel_t<true>(v, f) : with_rows_kernel_t<false>(v, f);
+}
+}  // namespace
+
+long long rows_stage_cells(int variant) { return 4LL * rows_threads(variant); }
+
+bool rows_step_eligible(int n, long long ncore, long long qs, int variant) {
+  if (variant < 0 || variant >= kRowsVariants) return false;
+  const long long cells = rows_stage_cells(variant);
+  return n >= 32 && (n & (n - 1)) == 0 && cells % n == 0 &&
+         static_cast<long long>(n) * n >= cells && ncore % cells == 0 && qs % 8 == 0;
+}
+
+// Raises the shared-memory limit of the variant and returns its resident
+// CTAs per SM (0: it cannot run).
+int rows_prepare(int variant, bool local) {
+  const size_t smem = rows_smem(variant);
+  const int th = rows_threads(variant);
+  return with_rows_kernel(variant, local, [&](void (*k)(StepArgs)) {
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess)
+      return 0;
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, th, smem) != cudaSuccess) return 0;
+    return b;
+  });
+}
+
+// The staged AA pull step's launch shapes: 0 = 128 threads x 2 stages, 1 =
+// 256 x 2, 2 = 128 x 3.  AA steps (pull + local) on the 256^3 box, two
+// boxes: 0.2240 / 0.2167 ms, 0.2314 / 0.2224, 0.2339 / 0.2288; with the
+// unstaged pull (k_step_aa_pull_h) 0.2763 / 0.2677.
+namespace {
+constexpr int kAaVariants = 3;
+constexpr int kAaThreads[kAaVariants] = {128, 256, 128};
+constexpr int kAaStages[kAaVariants] = {2, 2, 3};
+size_t aa_rows_smem(int v) {
+  return static_cast<size_t>(kAaStages[v]) * kQ * 4 * kAaThreads[v] * sizeof(__half) + kAaStages[v] * sizeof(uint64_t);
+}
+template <typename F>
+auto with_aa_rows_kernel(int v, F&& f) {
+  switch (v) {
+    case 1: return f(k_step_aa_rows_h<256, 2, 2>);
+    case 2: return f(k_step_aa_rows_h<128, 3, 3>);
+    default: return f(k_step_aa_rows_h<128, 2, 4>);
+  }
+}
+}  // namespace
+
+bool aa_rows_eligible(int n, long long ncore, long long qs, int variant) {
+  if (variant < 0 || variant >= kAaVariants) return false;
+  const long long cells = 4LL * kAaThreads[variant];
+  return n >= 32 && (n & (n - 1)) == 0 && cells % n == 0 && static_cast<long long>(n) * n >= cells &&
+         ncore % cells == 0 && qs % 8 == 0;
+}
+long long aa_rows_stage_cells(int variant) { return 4LL * kAaThreads[variant]; }
+int aa_rows_prepare(int variant) {
+  const size_t smem = aa_rows_smem(variant);
+  const int th = kAaThreads[variant];
+  return with_aa_rows_kernel(variant, [&](void (*k)(StepArgs)) {
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess)
+      return 0;
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, th, smem) != cudaSuccess) return 0;
+    return b;
+  });
+}
+cudaError_t launch_step_aa_rows_h(const StepArgs& a, int variant, int grid, cudaStream_t s) {
+  const size_t smem = aa_rows_smem(variant);
+  const int th = kAaThreads[variant];
+  const cudaError_t e = with_aa_rows_kernel(variant, [&](void (*k)(StepArgs)) {
+    return launch_chain(k, dim3(grid), dim3(th), smem, s, a);
+  });
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+cudaError_t launch_step_rows_h(const StepArgs& a, int variant, int grid, bool local, cudaStream_t s) {
+  const size_t smem = rows_smem(variant);
+  const int th = rows_threads(variant);
+  const cudaError_t e = with_rows_kernel(variant, local, [&](void (*k)(StepArgs)) {
+    return launch_chain(k, dim3(grid), dim3(th), smem, s, a);
+  });
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template cudaError_t launch_step_bulk<float>(const StepArgs&, int, cudaStream_t);

@@ -258,6 +258,22 @@ __device__ inline void block_reduce(double (&v)[N]) {
   __syncthreads();  // sm is reused by the next reduction of the same width
 }
 
+// Four consecutive halves (8-byte aligned) to floats, and back with
+// round-to-nearest.
+__device__ __forceinline__ void ld4h(const __half* p, float& a, float& b, float& c, float& d) {
+  const uint2 u = *reinterpret_cast<const uint2*>(p);
+  const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+  const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+  a = lo.x; b = lo.y; c = hi.x; d = hi.y;
+}
+__device__ __forceinline__ void st4h(__half* p, float a, float b, float c, float d) {
+  const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
+  uint2 u;
+  u.x = *reinterpret_cast<const uint32_t*>(&lo);
+  u.y = *reinterpret_cast<const uint32_t*>(&hi);
+  *reinterpret_cast<uint2*>(p) = u;
+}
+
 // Launches of the time-step chain: with the programmatic stream-serialisation
 // attribute when enabled, so each kernel is launched as its predecessor's
 // CTAs exit and runs its constant-table prologue before pdl_wait (every such

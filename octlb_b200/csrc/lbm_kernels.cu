@@ -498,19 +498,6 @@ __global__ void __launch_bounds__(kThreads) k_step_pair(const StepArgs a) {
 // them.  Per cell the arithmetic is the paired kernel's (conversions to and
 // from half are exact / round-to-nearest alike), so the results are bitwise
 // equal.  n % 4 == 0 (rows and population planes on 8-byte boundaries).
-__device__ __forceinline__ void ld4h(const __half* p, float& a, float& b, float& c, float& d) {
-  const uint2 u = *reinterpret_cast<const uint2*>(p);
-  const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
-  const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
-  a = lo.x; b = lo.y; c = hi.x; d = hi.y;
-}
-__device__ __forceinline__ void st4h(__half* p, float a, float b, float c, float d) {
-  const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
-  uint2 u;
-  u.x = *reinterpret_cast<const uint32_t*>(&lo);
-  u.y = *reinterpret_cast<const uint32_t*>(&hi);
-  *reinterpret_cast<uint2*>(p) = u;
-}
 
 __global__ void __launch_bounds__(kThreads) k_step_quad_h(const StepArgs a) {
   pdl_wait();
@@ -1303,7 +1290,9 @@ cudaError_t launch_step_aa(const StepArgs& a, bool reversed, cudaStream_t s) {
   // a 128-cell row (n % 128 == 0; OCTLB_AA_PULL=scalar keeps one), else one:
   // measured on the 256^3 box, one FP32 cell per thread (80 registers)
   // beats two with shuffled aligned stores (128 registers), and four FP16
-  // cells bounded to two CTAs per SM beat one.
+  // cells bounded to two CTAs per SM beat one.  (The FP16 pull step the
+  // context launches by default is the staged k_step_aa_rows_h; setting
+  // OCTLB_AA_PULL selects one of these instead.)
   const char* env = std::getenv("OCTLB_AA_PULL");
   const bool scalar = env && std::string(env) == "scalar";
   const bool half = std::is_same<T, __half>::value;

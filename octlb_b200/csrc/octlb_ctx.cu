@@ -171,9 +171,14 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     }
   } else if (L.aa) {
     // AA order: cur is the layout (1: reversed), both buffers the same memory
-    CK(launch_step_aa<T>(a, L.cur == 1, ctx->stream));
+    if (L.cur == 0 && L.use_aa_rows) CK(launch_step_aa_rows_h(a, ctx->aa_rows, L.aa_rows_grid, ctx->stream));
+    else if (L.cur == 1 && L.use_aa_local_rows)
+      CK(launch_step_rows_h(a, ctx->fp16_rows, L.aa_local_grid, true, ctx->stream));
+    else CK(launch_step_aa<T>(a, L.cur == 1, ctx->stream));
   } else if (L.use_bulk) {
     CK(launch_step_bulk<T>(a, L.bulk_grid, ctx->stream));
+  } else if (L.use_rows) {
+    CK(launch_step_rows_h(a, ctx->fp16_rows, L.rows_grid, false, ctx->stream));
   } else if (L.use_pair) {
     CK(launch_step_pair<T>(a, ctx->stream));
   } else if (L.use_map) {
@@ -1241,6 +1246,47 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
       A.wall_add = L.wall_add.as<float>();
       A.wall_dadd = L.wall_dadd.as<float>();
     }
+    // FP16: the four-cell step fed by bulk async copies where its shape
+    // fits (OCTLB_FP16_ROWS=off keeps k_step_quad_h; bitwise equal)
+    if (L.use_pair && sizeof(T) == 2 && ctx->fp16_rows >= 0 &&
+        rows_step_eligible(n, L.ncore, L.nslots, ctx->fp16_rows) && !g_dry_run) {
+      const int per_sm = rows_prepare(ctx->fp16_rows, false);
+      int dev = 0, sms = 0;
+      CK(cudaGetDevice(&dev));
+      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      if (per_sm > 0) {
+        L.use_rows = true;
+        L.rows_grid = static_cast<int>(std::min<long long>(static_cast<long long>(per_sm) * sms,
+                                                           L.ncore / rows_stage_cells(ctx->fp16_rows)));
+      }
+    }
+    // FP16 AA order: the pull step fed and drained by bulk async copies where
+    // its shape fits (OCTLB_AA_ROWS=off keeps k_step_aa_pull_h; bitwise equal)
+    if (L.aa && sizeof(T) == 2 && ctx->aa_rows >= 0 && aa_rows_eligible(n, L.ncore, L.nslots, ctx->aa_rows) &&
+        !g_dry_run) {
+      const int per_sm = aa_rows_prepare(ctx->aa_rows);
+      int dev = 0, sms = 0;
+      CK(cudaGetDevice(&dev));
+      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      if (per_sm > 0) {
+        L.use_aa_rows = true;
+        L.aa_rows_grid = static_cast<int>(std::min<long long>(static_cast<long long>(per_sm) * sms,
+                                                              L.ncore / aa_rows_stage_cells(ctx->aa_rows)));
+      }
+    }
+    // ... and its local step (from the reversed layout) staged as the AB step
+    if (L.aa && sizeof(T) == 2 && ctx->fp16_rows >= 0 && rows_step_eligible(n, L.ncore, L.nslots, ctx->fp16_rows) &&
+        !g_dry_run) {
+      const int per_sm = rows_prepare(ctx->fp16_rows, true);
+      int dev = 0, sms = 0;
+      CK(cudaGetDevice(&dev));
+      CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      if (per_sm > 0) {
+        L.use_aa_local_rows = true;
+        L.aa_local_grid = static_cast<int>(std::min<long long>(static_cast<long long>(per_sm) * sms,
+                                                               L.ncore / rows_stage_cells(ctx->fp16_rows)));
+      }
+    }
     if (uniform && ctx->step_kernel == 1 && bulk_step_eligible(n, sizeof(T)) && !g_dry_run) {
       const int per_sm = bulk_prepare<T>(n);
       int dev = 0, sms = 0;
@@ -2107,6 +2153,16 @@ static int create_common(const octlb_tables* t, const octlb_params* p, const dou
     if (ms >= 1 && ms <= 60000) ctx->wait_ns = static_cast<unsigned long long>(ms) * 1000000ull;
   }
   if (const char* st = std::getenv("OCTLB_TEST_BULK_STALL")) ctx->stall_first_row = st[0] == '1' ? 1 : 0;
+  if (const char* fr = std::getenv("OCTLB_FP16_ROWS")) {
+    const std::string v(fr);
+    ctx->fp16_rows = v == "off" ? -1 : (v.size() == 1 && v[0] >= '0' && v[0] <= '4' ? v[0] - '0' : ctx->fp16_rows);
+  }
+  if (const char* ar = std::getenv("OCTLB_AA_ROWS")) {
+    const std::string v(ar);
+    ctx->aa_rows = v == "off" ? -1 : (v.size() == 1 && v[0] >= '0' && v[0] <= '2' ? v[0] - '0' : ctx->aa_rows);
+  }
+  // OCTLB_AA_PULL picks one of the unstaged pull steps (scalar, quad)
+  if (const char* ap = std::getenv("OCTLB_AA_PULL")) ctx->aa_rows = ap[0] ? -1 : ctx->aa_rows;
   cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { rc = cuda_fail(ctx.get(), e, "cudaStreamCreate"); *out = ctx.release(); return rc; }
   ctx->own_stream = true;

@@ -171,6 +171,25 @@ def test_periodic_slabs_equal_one_box(ob, P):
         assert np.array_equal(rho, rho1) and np.array_equal(u, u1)
 
 
+@pytest.mark.parametrize("rows", ["0", "2"])
+def test_fp16_staged_step_on_slabs(ob, monkeypatch, rows):
+    """The staged FP16 step on x slabs (its source rows at x - 1 and x + 1
+    of the slab's first and last planes come from the ghost planes): two
+    slabs holding the same box equal the single box stepped by the
+    four-cell step with 8-byte global loads, bit for bit."""
+    from octlb_b200 import cases
+    n, steps = 32, 11
+    mesh, init, info = cases.tgv_periodic(n, u0=0.05, tau=0.55)
+    monkeypatch.setenv("OCTLB_FP16_ROWS", "off")
+    one = ob.GpuLattice(mesh, info["omega"], precision=ob.FP16_SHIFTED, init_pops=init)
+    one.advance(steps)
+    rho1, u1 = one.get_fields()
+    one.close()
+    monkeypatch.setenv("OCTLB_FP16_ROWS", rows)
+    for rho, u in run_slabs(ob, n, [init] * 2, info["omega"], steps, ob.FP16_SHIFTED):
+        assert np.array_equal(rho, rho1) and np.array_equal(u, u1)
+
+
 @pytest.mark.parametrize("prec,tol", [("fp32", 1e-5), ("fp16", 2e-3)])
 def test_periodic_slabs_match_the_restated_box(ob, orc, prec, tol):
     """Two slabs of a 64 x 32 x 32 periodic box (one Taylor-Green period over

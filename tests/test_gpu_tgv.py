@@ -119,40 +119,53 @@ def test_set_equilibrium_equals_set_populations(ob, prec):
     b.close()
 
 
-def test_fp16_four_cell_step_equals_paired_step(ob, monkeypatch):
-    """The four-cells-per-thread FP16 periodic step (8-byte accesses) and the
-    paired one (OCTLB_FP16_PAIR=1) give bitwise equal states, on a plain
-    periodic box and on x slabs (ghost planes)."""
+@pytest.mark.parametrize("n", [32, 64, 128])
+def test_fp16_four_cell_step_equals_paired_step(ob, monkeypatch, n):
+    """The four-cells-per-thread FP16 periodic steps -- the one fed by bulk
+    async copies through shared-memory stages in each of its launch shapes
+    (OCTLB_FP16_ROWS, 128 or 256 threads, 2 to 4 stages; R = 512 / n or
+    1024 / n z rows per stage, two copies per population at the y wrap), and
+    the one with 8-byte global loads (OCTLB_FP16_ROWS=off) -- and the paired
+    step (OCTLB_FP16_PAIR=1) give bitwise equal states."""
     from octlb_b200 import cases
-    n = 64
     mesh, init, info = cases.tgv_periodic(n, u0=0.05, tau=0.55)
     out = []
-    for pair in ("0", "1"):
+    for pair, rows in (("1", "off"), ("0", "off"), ("0", "0"), ("0", "1"), ("0", "2"), ("0", "3"), ("0", "4")):
         monkeypatch.setenv("OCTLB_FP16_PAIR", pair)
+        monkeypatch.setenv("OCTLB_FP16_ROWS", rows)
         lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP16_SHIFTED, init_pops=init)
         lat.advance(7)
         out.append(lat.get_populations())
         lat.close()
-    assert np.array_equal(out[0], out[1])
+    for k in range(1, len(out)):
+        assert np.array_equal(out[0], out[k]), k
 
 
 @pytest.mark.parametrize("prec,launch,n,pull", [("fp32", "graph", 64, None), ("fp16", "graph", 64, None),
                                                 ("fp32", "direct", 64, None), ("fp16", "graph", 128, None),
-                                                ("fp16", "direct", 128, "scalar")])
+                                                ("fp16", "direct", 128, "scalar"), ("fp16", "graph", 128, "quad"),
+                                                ("fp16", "graph", 32, "rows1"), ("fp16", "direct", 64, "rows2")])
 def test_aa_order_equals_ab_order(ob, prec, launch, n, pull, monkeypatch):
     """The one-buffer AA stream order (a step that pulls from and writes back
     to the neighbours, then one on the cell's own slots, alternating) and the
     two-buffer AB order give bitwise equal populations, fields and audits
     after odd step counts (reversed layout) and even ones (natural layout),
     through captured graphs and direct launches, with each form of the pull
-    step (one cell per thread; four in FP16 where a warp covers a 128-cell
-    row, with shuffled aligned stores; OCTLB_AA_PULL=scalar keeps one), and
-    after set_populations while the AA buffer is in the reversed layout."""
+    step (one cell per thread; in FP16 by default four, staged through shared
+    memory by bulk copies and stores in each launch shape, OCTLB_AA_ROWS;
+    four with shuffled aligned stores where a warp covers a 128-cell row,
+    OCTLB_AA_PULL=quad, there with the unstaged local step too; one,
+    OCTLB_AA_PULL=scalar), and after set_populations while the AA buffer is
+    in the reversed layout."""
     from octlb_b200 import cases
     if launch == "direct":
         monkeypatch.setenv("OCTLB_NO_GRAPH", "1")
-    if pull:
+    if pull and pull.startswith("rows"):
+        monkeypatch.setenv("OCTLB_AA_ROWS", pull[4:])
+    elif pull:
         monkeypatch.setenv("OCTLB_AA_PULL", pull)
+        if pull == "quad":  # and the unstaged local step
+            monkeypatch.setenv("OCTLB_FP16_ROWS", "off")
     mesh, init, info = cases.tgv_periodic(n, u0=0.05, tau=0.55)
     ab = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec), init_pops=init)
     aa = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec), init_pops=init, stream_order=ob.ORDER_AA)

@@ -1,7 +1,7 @@
 """Bounded device waits give up with an error status, never a hang.
 
-The bulk-copy periodic step waits on shared-memory barriers for the rows it
-requested.  With OCTLB_TEST_BULK_STALL=1 one CTA skips requesting its first
+The bulk-copy periodic steps (one cell per thread, and the staged FP16 step
+with four) wait on shared-memory barriers for the rows they requested.  With OCTLB_TEST_BULK_STALL=1 one CTA skips requesting its first
 row, so nothing ever completes that barrier: the wait runs out after
 OCTLB_WAIT_MS, the CTA records the error word, drains the copies it did
 request and returns, and the host reports OCTLB_ETIMEOUT.  The CUDA context
@@ -44,3 +44,34 @@ def test_bulk_step_wait_gives_up_with_etimeout(ob, orc, monkeypatch):
     blk.run_periodic(info["omega"], 5)
     rho_o, u_o = oracle.rho_u(blk.core())
     assert np.max(np.abs(u_g[0] - u_o)) <= 1e-5 * np.max(np.abs(u_o))
+
+
+@pytest.mark.parametrize("order", ["AB", "AA"])
+def test_staged_fp16_step_wait_gives_up_with_etimeout(ob, orc, monkeypatch, order):
+    """The same bounded wait in the staged FP16 periodic steps (four cells per
+    thread: the AB step, and the AA order's pull step with its bulk stores):
+    the stalled CTA gives up, the host reports OCTLB_ETIMEOUT, and a fresh
+    lattice afterwards steps correctly."""
+    from octlb_b200 import cases
+    from oracle import oracle
+    mesh, init, info = cases.tgv_periodic(64, u0=0.05, tau=0.55)
+    monkeypatch.setenv("OCTLB_TEST_BULK_STALL", "1")
+    monkeypatch.setenv("OCTLB_WAIT_MS", "50")
+    so = ob.ORDER_AA if order == "AA" else ob.ORDER_AB
+    lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP16_SHIFTED, init_pops=init, stream_order=so)
+    lat.advance(2)
+    with pytest.raises(ob.OctlbError) as e:
+        lat.synchronize()
+    assert e.value.code == ob.capi.OCTLB_ETIMEOUT, e.value
+    lat.close()
+
+    monkeypatch.delenv("OCTLB_TEST_BULK_STALL")
+    lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP16_SHIFTED, init_pops=init, stream_order=so)
+    lat.advance(5)
+    rho_g, u_g = lat.get_fields()
+    lat.close()
+    blk = oracle.Block(orc, 64)
+    blk.set_core(init[0])
+    blk.run_periodic(info["omega"], 5)
+    rho_o, u_o = oracle.rho_u(blk.core())
+    assert np.max(np.abs(u_g[0] - u_o)) <= 2e-3 * np.max(np.abs(u_o))
