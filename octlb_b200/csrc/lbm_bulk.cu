@@ -1,7 +1,7 @@
 // Pipelined fused steps for one periodic block fed by bulk async copies:
 // k_step_bulk (one cell per thread, FP32 or FP16, an option),
 // k_step_rows_h (four FP16 cells per thread: the FP16 default, and the AA
-// order's local step) and k_step_aa_rows_h (the AA order's FP16 pull step,
+// order's local step) and k_step_aa_rows<T> (the AA order's pull step,
 // drained by bulk stores too).
 //
 // A persistent CTA of n threads walks z-rows (x, y).  For each row it needs
@@ -204,18 +204,18 @@ __device__ __forceinline__ int dir_rt(int axis, int i) {
 // as (global, shared, bytes) runs handed to f.
 // Unshifted (the AA order's local step): rows (x, y0 .. y0 + R - 1) of
 // plane i, one run.
-template <typename F>
-__device__ __forceinline__ void pop_runs_h(const StepArgs& a, __half* pops, __half* stage, uint32_t row0, uint32_t R,
+template <typename E, typename F>
+__device__ __forceinline__ void pop_runs_h(const StepArgs& a, E* pops, E* stage, uint32_t row0, uint32_t R,
                                            uint32_t cells, int i, F&& f, bool shifted = true) {
   const uint32_t n = a.n;
   const int ci = shifted ? dir_rt(0, i) : 0, cj = shifted ? dir_rt(1, i) : 0;
   const uint32_t x = a.div_n.div(row0), y0 = row0 - x * n;
   const uint32_t xs = ci == 1 ? (x == 0 ? static_cast<uint32_t>(a.wrap_lo) : x - 1)
                               : (ci == -1 ? (x == n - 1 ? static_cast<uint32_t>(a.wrap_hi) : x + 1) : x);
-  __half* plane = pops + i * a.qs + static_cast<long long>(xs) * n * n;
-  __half* d = stage + i * cells;
+  E* plane = pops + i * a.qs + static_cast<long long>(xs) * n * n;
+  E* d = stage + i * cells;
   const int ys = static_cast<int>(y0) - cj;
-  const uint32_t rb = n * sizeof(__half);
+  const uint32_t rb = n * sizeof(E);
   if (ys >= 0 && ys + static_cast<int>(R) <= static_cast<int>(n)) {
     f(plane + static_cast<long long>(ys) * n, d, R * rb);
   } else if (ys < 0) {  // rows n - 1, 0 .. R - 2
@@ -226,20 +226,21 @@ __device__ __forceinline__ void pop_runs_h(const StepArgs& a, __half* pops, __ha
     f(plane, d + (R - 1) * n, rb);
   }
 }
-__device__ __forceinline__ void issue_pop_h(const StepArgs& a, const __half* src, __half* stage, uint64_t* bar,
-                                            uint32_t row0, uint32_t R, uint32_t cells, int i, bool shifted) {
+template <typename E>
+__device__ __forceinline__ void issue_pop_h(const StepArgs& a, const E* src, E* stage, uint64_t* bar, uint32_t row0,
+                                            uint32_t R, uint32_t cells, int i, bool shifted) {
   pop_runs_h(
-      a, const_cast<__half*>(src), stage, row0, R, cells, i,
-      [&](__half* g, __half* sm, uint32_t bytes) { bulk_g2s(sm, g, bytes, bar); }, shifted);
+      a, const_cast<E*>(src), stage, row0, R, cells, i,
+      [&](E* g, E* sm, uint32_t bytes) { bulk_g2s(sm, g, bytes, bar); }, shifted);
 }
 
 // Warp 0 requests a stage: lane 0 arms the barrier with the stage's bytes,
 // then lanes 0..18 copy one population each.  (Measured on the 256^3 box:
 // one lane issuing all 19 made the step 0.2385 ms instead of 0.2077.)
-__device__ __forceinline__ void issue_stage_h(const StepArgs& a, const __half* src, __half* stage, uint64_t* bar,
-                                              uint32_t row0, uint32_t R, uint32_t cells, uint32_t lane,
-                                              bool shifted = true) {
-  if (lane == 0) mbar_expect_tx(bar, static_cast<uint32_t>(kQ * cells * sizeof(__half)));
+template <typename E>
+__device__ __forceinline__ void issue_stage_h(const StepArgs& a, const E* src, E* stage, uint64_t* bar, uint32_t row0,
+                                              uint32_t R, uint32_t cells, uint32_t lane, bool shifted = true) {
+  if (lane == 0) mbar_expect_tx(bar, static_cast<uint32_t>(kQ * cells * sizeof(E)));
   __syncwarp();
   if (lane < static_cast<uint32_t>(kQ))
     issue_pop_h(a, src, stage, bar, row0, R, cells, static_cast<int>(lane), shifted);
@@ -340,32 +341,58 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_rows_h(const StepArgs a)
   }
 }
 
-// The AA order's pull step (natural -> reversed layout) in FP16, staged the
-// same way: the 19 source rows of a stage come in by bulk copies; each cell
-// collides its pulled values and writes g_opp(k) back into the shared-memory
-// slot it read for direction k; the stage's rows then go back by bulk stores
-// to the global rows they came from.  Every slot belongs to one cell (a
-// thread's 8-byte read may include a neighbour's slot, whose value it does
-// not use), and a population's source rows of different stages are disjoint,
-// so the in-place update needs no ordering between threads before the
-// write-back or between CTAs.  Per cell the values and the arithmetic are
-// k_step_aa_pull_h's: bitwise equal.  A buffer is refilled once the lane that
-// stored a population's rows from it has seen its stores read out.
-template <int THREADS, int STAGES, int MINB>
-__global__ void __launch_bounds__(THREADS, MINB) k_step_aa_rows_h(const StepArgs a) {
-  constexpr uint32_t kCells = 4 * THREADS;
+// Vector access of a thread's CPT consecutive cells (8 bytes: four halves
+// or two floats), as k_step_aa_pull_h and k_step_pair read them.
+template <typename T> struct Cells8;
+template <> struct Cells8<__half> {
+  static constexpr int kCpt = 4;
+  __device__ static void ld(const __half* p, float (&v)[4]) { ld4h(p, v[0], v[1], v[2], v[3]); }
+  __device__ static float ld1(const __half* p) { return __half2float(*p); }
+  __device__ static void st1(__half* p, float v) { *p = __float2half_rn(v); }
+  __device__ static void st(__half* p, const float (&v)[4]) { st4h(p, v[0], v[1], v[2], v[3]); }
+};
+template <> struct Cells8<float> {
+  static constexpr int kCpt = 2;
+  __device__ static void ld(const float* p, float (&v)[2]) {
+    const float2 u = *reinterpret_cast<const float2*>(p);
+    v[0] = u.x;
+    v[1] = u.y;
+  }
+  __device__ static float ld1(const float* p) { return *p; }
+  __device__ static void st1(float* p, float v) { *p = v; }
+  __device__ static void st(float* p, const float (&v)[2]) { *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]); }
+};
+
+// The AA order's pull step (natural -> reversed layout), staged the same
+// way: the 19 source rows of a stage come in by bulk copies; each cell
+// collides its pulled values and writes g_opp(k) back into the
+// shared-memory slot it read for direction k; the stage's rows then go back
+// by bulk stores to the global rows they came from.  Every slot belongs to
+// one cell (a thread's 8-byte read may include a neighbour's slot, whose
+// value it does not use), and a population's source rows of different
+// stages are disjoint, so the in-place update needs no ordering between
+// threads before the write-back or between CTAs.  Per cell the values and
+// the arithmetic are the unstaged pull steps' (k_step_aa_pull_h,
+// k_step_aa_pull<float>): bitwise equal.  A buffer is refilled once the lane
+// that stored a population's rows from it has seen its stores read out.
+// CPT = 4 FP16 or 2 FP32 cells per thread.
+template <typename T, int THREADS, int STAGES, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) k_step_aa_rows(const StepArgs a) {
+  using V = Cells8<T>;
+  constexpr int CPT = V::kCpt;
+  constexpr uint32_t kCells = CPT * THREADS;
   constexpr uint32_t kStageElems = kQ * kCells;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __half* stages = reinterpret_cast<__half*>(smem_raw);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + static_cast<size_t>(STAGES) * kStageElems * sizeof(__half));
-  __half* pops = static_cast<__half*>(a.dst);  // == a.src
+  T* stages = reinterpret_cast<T*>(smem_raw);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + static_cast<size_t>(STAGES) * kStageElems * sizeof(T));
+  T* pops = static_cast<T*>(a.dst);  // == a.src
   const uint32_t n = a.n;
   const uint32_t R = kCells / n;
   const uint32_t nst = static_cast<uint32_t>(a.ncore / kCells);
-  const uint32_t c = 4 * threadIdx.x;
+  const uint32_t c = CPT * threadIdx.x;
   const uint32_t lg = static_cast<uint32_t>(__ffs(static_cast<int>(n)) - 1);
   const uint32_t r = c >> lg, z = c & (n - 1);
-  const uint32_t zm1 = z == 0 ? n - 1 : z - 1, zp4 = z + 4 == n ? 0 : z + 4;
+  const uint32_t zm1 = z == 0 ? n - 1 : z - 1, zpc = z + CPT == n ? 0 : z + CPT;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
@@ -408,48 +435,54 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_aa_rows_h(const StepArgs
       return;
     }
     if (threadIdx.x < 32) issued &= ~(1u << s);
-    __half* S = stages + s * kStageElems + r * n;
-    float f0[kQ], f1[kQ], f2[kQ], f3[kQ];
+    T* S = stages + s * kStageElems + r * n;
+    float f[CPT][kQ];
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
-      const __half* p = S + i * kCells;
-      if (cz(i) == 0) {
-        ld4h(p + z, f0[i], f1[i], f2[i], f3[i]);
-      } else if (cz(i) == 1) {  // cells z..z+3 pull z-1..z+2
-        float w;
-        ld4h(p + z, f1[i], f2[i], f3[i], w);
-        f0[i] = __half2float(p[zm1]);
-      } else {                  // cells z..z+3 pull z+1..z+4
-        float w;
-        ld4h(p + z, w, f0[i], f1[i], f2[i]);
-        f3[i] = __half2float(p[zp4]);
+      const T* p = S + i * kCells;
+      float v[CPT];
+      V::ld(p + z, v);
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        if (cz(i) == 0) f[j][i] = v[j];
+        else if (cz(i) == 1) f[j][i] = j == 0 ? V::ld1(p + zm1) : v[j - 1];  // cells pull z-1 ..
+        else f[j][i] = j == CPT - 1 ? V::ld1(p + zpc) : v[j + 1];             // cells pull z+1 ..
       }
     }
-    bgk<false>(f0, a.omega, a.scale, a.inv_scale);
-    bgk<false>(f1, a.omega, a.scale, a.inv_scale);
-    bgk<false>(f2, a.omega, a.scale, a.inv_scale);
-    bgk<false>(f3, a.omega, a.scale, a.inv_scale);
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) bgk<kBgkCorrect<T>>(f[j], a.omega, a.scale, a.inv_scale);
 #pragma unroll
     for (int k2 = 0; k2 < kQ; ++k2) {
-      __half* p = S + k2 * kCells;
+      T* p = S + k2 * kCells;
       const int o = opp(k2);
-      if (cz(k2) == 0) {          // slots z..z+3
-        st4h(p + z, f0[o], f1[o], f2[o], f3[o]);
-      } else if (cz(k2) == 1) {   // slots z-1, z..z+1, z+2
-        p[zm1] = __float2half_rn(f0[o]);
-        *reinterpret_cast<__half2*>(p + z) = __floats2half2_rn(f1[o], f2[o]);
-        p[z + 2] = __float2half_rn(f3[o]);
-      } else {                    // slots z+1, z+2..z+3, z+4
-        p[z + 1] = __float2half_rn(f0[o]);
-        *reinterpret_cast<__half2*>(p + z + 2) = __floats2half2_rn(f1[o], f2[o]);
-        p[zp4] = __float2half_rn(f3[o]);
+      if (cz(k2) == 0) {  // slots z .. z + CPT - 1
+        float v[CPT];
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) v[j] = f[j][o];
+        V::st(p + z, v);
+      } else if (cz(k2) == 1) {  // slots z - 1, z .. z + CPT - 2
+        V::st1(p + zm1, f[0][o]);
+        if constexpr (CPT == 4) {
+          *reinterpret_cast<__half2*>(p + z) = __floats2half2_rn(f[1][o], f[2][o]);
+          V::st1(p + z + 2, f[3][o]);
+        } else {
+          V::st1(p + z, f[1][o]);
+        }
+      } else {  // slots z + 1 .. z + CPT - 1, z + CPT
+        if constexpr (CPT == 4) {
+          V::st1(p + z + 1, f[0][o]);
+          *reinterpret_cast<__half2*>(p + z + 2) = __floats2half2_rn(f[1][o], f[2][o]);
+        } else {
+          V::st1(p + z + 1, f[0][o]);
+        }
+        V::st1(p + zpc, f[CPT - 1][o]);
       }
     }
     fence_smem_to_async();
     __syncthreads();
     if (threadIdx.x < static_cast<uint32_t>(kQ)) {
       pop_runs_h(a, pops, stages + s * kStageElems, (blockIdx.x + k * gridDim.x) * R, R, kCells,
-                 static_cast<int>(lane), [](__half* g, __half* sm, uint32_t bytes) { bulk_s2g(g, sm, bytes); });
+                 static_cast<int>(lane), [](T* g, T* sm, uint32_t bytes) { bulk_s2g(g, sm, bytes); });
       bulk_commit();
     }
   }
@@ -541,37 +574,40 @@ int rows_prepare(int variant, bool local) {
 }
 
 // The staged AA pull step's launch shapes: 0 = 128 threads x 2 stages, 1 =
-// 256 x 2, 2 = 128 x 3.  AA steps (pull + local) on the 256^3 box, two
-// boxes: 0.2240 / 0.2167 ms, 0.2314 / 0.2224, 0.2339 / 0.2288; with the
-// unstaged pull (k_step_aa_pull_h) 0.2763 / 0.2677.
+// 256 x 2, 2 = 128 x 3 (stages of 8 bytes x threads per population, either
+// precision).  AA steps (pull + local) on the 256^3 box: FP16 on two boxes
+// 0.2240 / 0.2167 ms, 0.2314 / 0.2224, 0.2339 / 0.2288, with the unstaged
+// pull (k_step_aa_pull_h) 0.2763 / 0.2677; FP32 0.3933, 0.4061, 0.4215, with
+// the unstaged one-cell pull 0.4224 (AB step 0.3813).
 namespace {
 constexpr int kAaVariants = 3;
 constexpr int kAaThreads[kAaVariants] = {128, 256, 128};
 constexpr int kAaStages[kAaVariants] = {2, 2, 3};
 size_t aa_rows_smem(int v) {
-  return static_cast<size_t>(kAaStages[v]) * kQ * 4 * kAaThreads[v] * sizeof(__half) + kAaStages[v] * sizeof(uint64_t);
+  return static_cast<size_t>(kAaStages[v]) * kQ * 8 * kAaThreads[v] + kAaStages[v] * sizeof(uint64_t);
 }
-template <typename F>
+template <typename T, typename F>
 auto with_aa_rows_kernel(int v, F&& f) {
   switch (v) {
-    case 1: return f(k_step_aa_rows_h<256, 2, 2>);
-    case 2: return f(k_step_aa_rows_h<128, 3, 3>);
-    default: return f(k_step_aa_rows_h<128, 2, 4>);
+    case 1: return f(k_step_aa_rows<T, 256, 2, 2>);
+    case 2: return f(k_step_aa_rows<T, 128, 3, 3>);
+    default: return f(k_step_aa_rows<T, 128, 2, 4>);
   }
 }
 }  // namespace
 
-bool aa_rows_eligible(int n, long long ncore, long long qs, int variant) {
-  if (variant < 0 || variant >= kAaVariants) return false;
-  const long long cells = 4LL * kAaThreads[variant];
+long long aa_rows_stage_cells(int variant, int elem_bytes) { return 8LL / elem_bytes * kAaThreads[variant]; }
+bool aa_rows_eligible(int n, long long ncore, long long qs, int elem_bytes, int variant) {
+  if (variant < 0 || variant >= kAaVariants || (elem_bytes != 2 && elem_bytes != 4)) return false;
+  const long long cells = aa_rows_stage_cells(variant, elem_bytes);
   return n >= 32 && (n & (n - 1)) == 0 && cells % n == 0 && static_cast<long long>(n) * n >= cells &&
-         ncore % cells == 0 && qs % 8 == 0;
+         ncore % cells == 0 && (qs * elem_bytes) % 16 == 0;
 }
-long long aa_rows_stage_cells(int variant) { return 4LL * kAaThreads[variant]; }
+template <typename T>
 int aa_rows_prepare(int variant) {
   const size_t smem = aa_rows_smem(variant);
   const int th = kAaThreads[variant];
-  return with_aa_rows_kernel(variant, [&](void (*k)(StepArgs)) {
+  return with_aa_rows_kernel<T>(variant, [&](void (*k)(StepArgs)) {
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess)
       return 0;
     int b = 0;
@@ -579,14 +615,19 @@ int aa_rows_prepare(int variant) {
     return b;
   });
 }
-cudaError_t launch_step_aa_rows_h(const StepArgs& a, int variant, int grid, cudaStream_t s) {
+template <typename T>
+cudaError_t launch_step_aa_rows(const StepArgs& a, int variant, int grid, cudaStream_t s) {
   const size_t smem = aa_rows_smem(variant);
   const int th = kAaThreads[variant];
-  const cudaError_t e = with_aa_rows_kernel(variant, [&](void (*k)(StepArgs)) {
+  const cudaError_t e = with_aa_rows_kernel<T>(variant, [&](void (*k)(StepArgs)) {
     return launch_chain(k, dim3(grid), dim3(th), smem, s, a);
   });
   return e != cudaSuccess ? e : cudaGetLastError();
 }
+template int aa_rows_prepare<float>(int);
+template int aa_rows_prepare<__half>(int);
+template cudaError_t launch_step_aa_rows<float>(const StepArgs&, int, int, cudaStream_t);
+template cudaError_t launch_step_aa_rows<__half>(const StepArgs&, int, int, cudaStream_t);
 
 cudaError_t launch_step_rows_h(const StepArgs& a, int variant, int grid, bool local, cudaStream_t s) {
   const size_t smem = rows_smem(variant);

@@ -1290,8 +1290,8 @@ cudaError_t launch_step_aa(const StepArgs& a, bool reversed, cudaStream_t s) {
   // a 128-cell row (n % 128 == 0; OCTLB_AA_PULL=scalar keeps one), else one:
   // measured on the 256^3 box, one FP32 cell per thread (80 registers)
   // beats two with shuffled aligned stores (128 registers), and four FP16
-  // cells bounded to two CTAs per SM beat one.  (The FP16 pull step the
-  // context launches by default is the staged k_step_aa_rows_h; setting
+  // cells bounded to two CTAs per SM beat one.  (The pull step the context
+  // launches by default is the staged k_step_aa_rows<T>; setting
   // OCTLB_AA_PULL selects one of these instead.)
   const char* env = std::getenv("OCTLB_AA_PULL");
   const bool scalar = env && std::string(env) == "scalar";

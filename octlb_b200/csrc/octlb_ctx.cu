@@ -171,7 +171,7 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
     }
   } else if (L.aa) {
     // AA order: cur is the layout (1: reversed), both buffers the same memory
-    if (L.cur == 0 && L.use_aa_rows) CK(launch_step_aa_rows_h(a, ctx->aa_rows, L.aa_rows_grid, ctx->stream));
+    if (L.cur == 0 && L.use_aa_rows) CK(launch_step_aa_rows<T>(a, ctx->aa_rows, L.aa_rows_grid, ctx->stream));
     else if (L.cur == 1 && L.use_aa_local_rows)
       CK(launch_step_rows_h(a, ctx->fp16_rows, L.aa_local_grid, true, ctx->stream));
     else CK(launch_step_aa<T>(a, L.cur == 1, ctx->stream));
@@ -1260,18 +1260,18 @@ int create_impl(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p, co
                                                            L.ncore / rows_stage_cells(ctx->fp16_rows)));
       }
     }
-    // FP16 AA order: the pull step fed and drained by bulk async copies where
-    // its shape fits (OCTLB_AA_ROWS=off keeps k_step_aa_pull_h; bitwise equal)
-    if (L.aa && sizeof(T) == 2 && ctx->aa_rows >= 0 && aa_rows_eligible(n, L.ncore, L.nslots, ctx->aa_rows) &&
+    // AA order: the pull step fed and drained by bulk async copies where its
+    // shape fits (OCTLB_AA_ROWS=off keeps the unstaged ones; bitwise equal)
+    if (L.aa && ctx->aa_rows >= 0 && aa_rows_eligible(n, L.ncore, L.nslots, sizeof(T), ctx->aa_rows) &&
         !g_dry_run) {
-      const int per_sm = aa_rows_prepare(ctx->aa_rows);
+      const int per_sm = aa_rows_prepare<T>(ctx->aa_rows);
       int dev = 0, sms = 0;
       CK(cudaGetDevice(&dev));
       CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
       if (per_sm > 0) {
         L.use_aa_rows = true;
         L.aa_rows_grid = static_cast<int>(std::min<long long>(static_cast<long long>(per_sm) * sms,
-                                                              L.ncore / aa_rows_stage_cells(ctx->aa_rows)));
+                                                              L.ncore / aa_rows_stage_cells(ctx->aa_rows, sizeof(T))));
       }
     }
     // ... and its local step (from the reversed layout) staged as the AB step

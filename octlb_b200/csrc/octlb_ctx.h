@@ -54,10 +54,10 @@ bool rows_step_eligible(int n, long long ncore, long long qs, int variant);
 long long rows_stage_cells(int variant);
 int rows_prepare(int variant, bool local);
 cudaError_t launch_step_rows_h(const StepArgs&, int variant, int grid, bool local, cudaStream_t);
-bool aa_rows_eligible(int n, long long ncore, long long qs, int variant);
-long long aa_rows_stage_cells(int variant);
-int aa_rows_prepare(int variant);
-cudaError_t launch_step_aa_rows_h(const StepArgs&, int variant, int grid, cudaStream_t);
+bool aa_rows_eligible(int n, long long ncore, long long qs, int elem_bytes, int variant);
+long long aa_rows_stage_cells(int variant, int elem_bytes);
+template <typename T> int aa_rows_prepare(int variant);
+template <typename T> cudaError_t launch_step_aa_rows(const StepArgs&, int variant, int grid, cudaStream_t);
 template <typename T> cudaError_t launch_step_pair(const StepArgs&, cudaStream_t);
 template <typename T> cudaError_t launch_step_near(const StepArgs&, const NearTables&, cudaStream_t);
 template <typename T> cudaError_t launch_add_force(const StepArgs&, T*, const float*, cudaStream_t);
@@ -189,7 +189,7 @@ struct Level {
   int bulk_grid = 0;
   bool use_rows = false;            // staged FP16 four-cell step (periodic block)
   int rows_grid = 0;
-  bool use_aa_rows = false;         // staged FP16 AA pull step
+  bool use_aa_rows = false;         // staged AA pull step
   int aa_rows_grid = 0;
   bool use_aa_local_rows = false;   // staged FP16 AA local step
   int aa_local_grid = 0;
@@ -328,7 +328,7 @@ struct octlb_ctx {
   long long launch_count = 0;       // kernels issued by the advance_one being built
   int step_kernel = 0;              // OCTLB_STEP_KERNEL: 0 pair (default), 1 bulk, 2 plain
   int fp16_rows = 0;                // OCTLB_FP16_ROWS: the staged FP16 step's launch shape (off: -1)
-  int aa_rows = 0;                  // OCTLB_AA_ROWS: the staged FP16 AA pull step's launch shape (off: -1)
+  int aa_rows = 0;                  // OCTLB_AA_ROWS: the staged AA pull step's launch shape (off: -1)
   bool map_global = true;           // slot map read through L1 (OCTLB_MAP_SMEM=1: staged in shared memory)
   // Bounded device waits: their limit (OCTLB_WAIT_MS, default 1 s) and the
   // test of the give-up path (OCTLB_TEST_BULK_STALL=1: one CTA of the bulk

@@ -144,19 +144,21 @@ def test_fp16_four_cell_step_equals_paired_step(ob, monkeypatch, n):
 @pytest.mark.parametrize("prec,launch,n,pull", [("fp32", "graph", 64, None), ("fp16", "graph", 64, None),
                                                 ("fp32", "direct", 64, None), ("fp16", "graph", 128, None),
                                                 ("fp16", "direct", 128, "scalar"), ("fp16", "graph", 128, "quad"),
-                                                ("fp16", "graph", 32, "rows1"), ("fp16", "direct", 64, "rows2")])
+                                                ("fp16", "graph", 32, "rows1"), ("fp16", "direct", 64, "rows2"),
+                                                ("fp32", "graph", 64, "scalar"), ("fp32", "graph", 32, "rows1"),
+                                                ("fp32", "direct", 128, "rows2")])
 def test_aa_order_equals_ab_order(ob, prec, launch, n, pull, monkeypatch):
     """The one-buffer AA stream order (a step that pulls from and writes back
     to the neighbours, then one on the cell's own slots, alternating) and the
     two-buffer AB order give bitwise equal populations, fields and audits
     after odd step counts (reversed layout) and even ones (natural layout),
     through captured graphs and direct launches, with each form of the pull
-    step (one cell per thread; in FP16 by default four, staged through shared
-    memory by bulk copies and stores in each launch shape, OCTLB_AA_ROWS;
-    four with shuffled aligned stores where a warp covers a 128-cell row,
-    OCTLB_AA_PULL=quad, there with the unstaged local step too; one,
-    OCTLB_AA_PULL=scalar), and after set_populations while the AA buffer is
-    in the reversed layout."""
+    step (by default staged through shared memory by bulk copies and stores,
+    four FP16 or two FP32 cells per thread, in each launch shape,
+    OCTLB_AA_ROWS; in FP16 four with shuffled aligned stores where a warp
+    covers a 128-cell row, OCTLB_AA_PULL=quad, there with the unstaged local
+    step too; one cell per thread, OCTLB_AA_PULL=scalar), and after
+    set_populations while the AA buffer is in the reversed layout."""
     from octlb_b200 import cases
     if launch == "direct":
         monkeypatch.setenv("OCTLB_NO_GRAPH", "1")

@@ -46,19 +46,20 @@ def test_bulk_step_wait_gives_up_with_etimeout(ob, orc, monkeypatch):
     assert np.max(np.abs(u_g[0] - u_o)) <= 1e-5 * np.max(np.abs(u_o))
 
 
-@pytest.mark.parametrize("order", ["AB", "AA"])
-def test_staged_fp16_step_wait_gives_up_with_etimeout(ob, orc, monkeypatch, order):
-    """The same bounded wait in the staged FP16 periodic steps (four cells per
-    thread: the AB step, and the AA order's pull step with its bulk stores):
-    the stalled CTA gives up, the host reports OCTLB_ETIMEOUT, and a fresh
-    lattice afterwards steps correctly."""
+@pytest.mark.parametrize("order,prec", [("AB", "fp16"), ("AA", "fp16"), ("AA", "fp32")])
+def test_staged_step_wait_gives_up_with_etimeout(ob, orc, monkeypatch, order, prec):
+    """The same bounded wait in the staged periodic steps (the FP16 AB step
+    with four cells per thread, and the AA order's pull step with its bulk
+    stores in FP16 and FP32): the stalled CTA gives up, the host reports
+    OCTLB_ETIMEOUT, and a fresh lattice afterwards steps correctly."""
     from octlb_b200 import cases
     from oracle import oracle
     mesh, init, info = cases.tgv_periodic(64, u0=0.05, tau=0.55)
     monkeypatch.setenv("OCTLB_TEST_BULK_STALL", "1")
     monkeypatch.setenv("OCTLB_WAIT_MS", "50")
     so = ob.ORDER_AA if order == "AA" else ob.ORDER_AB
-    lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP16_SHIFTED, init_pops=init, stream_order=so)
+    p = ob.FP16_SHIFTED if prec == "fp16" else ob.FP32
+    lat = ob.GpuLattice(mesh, info["omega"], precision=p, init_pops=init, stream_order=so)
     lat.advance(2)
     with pytest.raises(ob.OctlbError) as e:
         lat.synchronize()
@@ -66,7 +67,7 @@ def test_staged_fp16_step_wait_gives_up_with_etimeout(ob, orc, monkeypatch, orde
     lat.close()
 
     monkeypatch.delenv("OCTLB_TEST_BULK_STALL")
-    lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP16_SHIFTED, init_pops=init, stream_order=so)
+    lat = ob.GpuLattice(mesh, info["omega"], precision=p, init_pops=init, stream_order=so)
     lat.advance(5)
     rho_g, u_g = lat.get_fields()
     lat.close()
