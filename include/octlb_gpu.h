@@ -66,7 +66,7 @@ extern "C" {
  * caller and copied at create.  Cell order inside a block is the reference's
  * (ix * n + iy) * n + iz (block_lattice.h:290-296). */
 typedef struct octlb_tables {
-  int n;                          /* cells per block edge (even) */
+  int n;                          /* cells per block edge: even, or odd (>= 3) on a mesh without coarse-fine faces */
   int n_blocks;                   /* leaves (OctantId 0..n_blocks-1) */
   const int* levels;              /* [n_blocks] quadrant level */
   const double* bounds;           /* [n_blocks][6] xmin,ymin,zmin,xmax,ymax,zmax */

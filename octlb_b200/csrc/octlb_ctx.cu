@@ -289,7 +289,12 @@ int do_advance_level(octlb_ctx* ctx, int l) {
 
 int validate(octlb_ctx* ctx, const octlb_tables* t, const octlb_params* p) {
   if (!t || !p) return fail(ctx, OCTLB_EINVAL, "null tables or params");
-  if (t->n < 2 || (t->n % 2) != 0) return fail(ctx, OCTLB_EINVAL, "block edge n must be even and >= 2");
+  if (t->n < 2) return fail(ctx, OCTLB_EINVAL, "block edge n must be >= 2");
+  // 2:1 coupling pairs n / 2 coarse face cells with each fine block's
+  // (level_coupler.cpp:70-139): an odd n serves single-level meshes (the
+  // reference's cavity3d runs one 31^3 block)
+  if (t->n % 2 != 0 && (t->n < 3 || t->n_coarse_fine > 0))
+    return fail(ctx, OCTLB_EINVAL, "odd block edge n: n >= 3 and a mesh without coarse-fine faces only");
   if (t->n_blocks < 1 || !t->levels || !t->kinds) return fail(ctx, OCTLB_EINVAL, "no blocks / levels / kinds");
   if (p->precision != OCTLB_FP32 && p->precision != OCTLB_FP16_SHIFTED)
     return fail(ctx, OCTLB_EINVAL, "unknown precision");

@@ -146,7 +146,12 @@ def test_create_rejects_bad_tables_without_device(ob):
     with pytest.raises(ob.OctlbError):
         ob.GpuLattice(make_tables_mesh(ob), 2.5)                              # omega outside (0, 2)
     with pytest.raises(ob.OctlbError):
-        ob.GpuLattice(ob.Mesh(3, [0], [0, 0, 0, 1, 1, 1]), 1.5)               # odd block edge
+        ob.GpuLattice(ob.Mesh(1, [0], [0, 0, 0, 1, 1, 1]), 1.5)               # block edge below 2
+    from octlb_b200 import cases
+    odd_cf, _, _ = cases.cavity_forest(cells=6, n=3, band_cells=3)
+    with pytest.raises(ob.OctlbError) as e:                                     # odd block edge with 2:1
+        ob.GpuLattice(odd_cf, 1.5)                                              # coupling
+    assert e.value.code == ob.capi.OCTLB_EINVAL and "coarse-fine" in str(e.value)
     # parameters out of their sets (the ABI's enumerations)
     for kw in (dict(precision=7), dict(stream_mode=5), dict(coupler_mode=3), dict(stream_order=2),
                dict(coupler_mode=ob.COUPLER_PHYSICAL, omega_level=[2.5]),
@@ -186,9 +191,9 @@ double use(octlb::GpuTimeLoop& loop) {
 int main() {
   octlb_tables t{};
   octlb_params p{};
-  t.n = 3;  // odd block edge: rejected by validation
+  t.n = 1;  // block edge below 2: rejected by validation
   t.n_blocks = 1;
-  int lv = 0; double bd[6] = {0,0,0,1,1,1}; unsigned char k[27] = {0};
+  int lv = 0; double bd[6] = {0,0,0,1,1,1}; unsigned char k[1] = {0};
   t.levels = &lv; t.bounds = bd; t.kinds = k;
   p.omega = 1.5;
   try {
@@ -205,7 +210,7 @@ int main() {
     subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
                     "-L", lib_dir, "-loctlb_b200", f"-Wl,-rpath,{lib_dir}"], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
-    assert r.returncode == 0 and "even" in r.stdout
+    assert r.returncode == 0 and ">= 2" in r.stdout
 
 
 @pytest.mark.parametrize("name", ["tgv", "shell", "c1", "c2", "cyl", "c3"])

@@ -5,7 +5,8 @@ oracle.Sim.set_fd_boundary): the fields after N steps, FP32 <= 1e-5 relative
 (max |gpu - ref| / max |ref| over all cells), FP16-shifted <= 2e-3.
 
 * cavity3d's boundary: InterpolatedVelocity on every face, the y+ face's
-  wall velocity on the interior lid cells (one 16^3 block);
+  wall velocity on the interior lid cells (one 16^3 block, and one 31^3
+  block as the example runs it);
 * a channel: a uniform inlet on x- ramped over 20 steps, a pressure outlet
   on x+ (target density 1), velocity walls elsewhere;
 * eight 8^3 blocks (the roles of a block's rim cells come from its own
@@ -44,10 +45,13 @@ def run_pair(ob, ref, mesh, init, omega, types, u, rho_t, steps, prec, inlet=Non
     return rho_g, u_g, rho_r, u_r
 
 
-@pytest.mark.parametrize("prec,tol", [("fp32", 1e-5), ("fp16", 2e-3)])
-def test_cavity3d_boundary(ob, ref, prec, tol):
+@pytest.mark.parametrize("prec,tol,n", [("fp32", 1e-5, 16), ("fp16", 2e-3, 16), ("fp32", 1e-5, 31),
+                                        ("fp16", 2e-3, 31)])
+def test_cavity3d_boundary(ob, ref, prec, tol, n):
+    """cavity3d's walls and lid on one block: 16^3, and the example's own
+    31^3 lattice (an odd block edge: the one-cell-per-thread step)."""
     from octlb_b200 import cases
-    mesh, init, info = cases.cavity_forest(cells=16, n=16, lid=0.0, tau=0.6)
+    mesh, init, info = cases.cavity_forest(cells=n, n=n, lid=0.0, tau=0.6)
     u = np.zeros((6, 3))
     u[3, 0] = 0.05
     rho_g, u_g, rho_r, u_r = run_pair(ob, ref, mesh, init, info["omega"], [S.INTERPOLATED_VELOCITY] * 6, u,
@@ -108,17 +112,20 @@ def test_rest_state_is_a_fixed_point(ob):
     lat.close()
 
 
-@pytest.mark.parametrize("blocks", [1, 8])
+@pytest.mark.parametrize("blocks", [1, 8, "31"])
 def test_const_rho_with_fd_walls(ob, ref, blocks):
     """cavity3d's configuration: ConstRhoBGK in the bulk with the FD walls
     and lid, the velocity cells' collide densities in the average's
     statistics (kFluidAndBoundary): fields and average_rho after every few
     steps against the reference TimeLoop built with use_const_rho_bgk around
     the reference's handler.  Eight blocks also exercise the stencils'
-    reads of kBulk densities, which carry the collide's 1 - average_rho."""
+    reads of kBulk densities, which carry the collide's 1 - average_rho;
+    "31" is cavity3d's own lattice, one 31^3 block (RESOLUTION = 30, an odd
+    block edge)."""
     from octlb_b200 import cases
-    if blocks == 1:
-        mesh, init, info = cases.cavity_forest(cells=16, n=16, lid=0.0, tau=0.6)
+    if blocks in (1, "31"):
+        c = 16 if blocks == 1 else 31
+        mesh, init, info = cases.cavity_forest(cells=c, n=c, lid=0.0, tau=0.6)
         omega = info["omega"]
     else:
         sys.path.insert(0, HERE)

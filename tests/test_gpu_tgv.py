@@ -88,6 +88,28 @@ def test_tgv256_headline_size_against_restatement(ob, orc, prec):
     assert eu <= TOL[prec] and er <= TOL[prec]
 
 
+@pytest.mark.parametrize("prec,n", [("fp32", 33), ("fp16", 33), ("fp32", 31)])
+def test_odd_periodic_box_against_restatement(ob, orc, prec, n):
+    """An odd block edge (no cell pairs: the one-cell-per-thread step on the
+    periodic box) against the oracle's restatement of BlockLattice<double>,
+    40 steps: every cell's rho and u."""
+    from octlb_b200 import cases
+    mesh, init, info = cases.tgv_periodic(n, u0=0.05, tau=0.55)
+    lat = ob.GpuLattice(mesh, info["omega"], precision=prec_of(ob, prec), init_pops=init)
+    lat.advance(40)
+    rho_g, u_g = lat.get_fields()
+    a = lat.audit()
+    lat.close()
+    blk = oracle.Block(orc, n)
+    blk.set_core(init[0])
+    blk.run_periodic(info["omega"], 40)
+    rho_r, u_r = blk.fields()
+    eu, er = rel(u_g[0], u_r), rel(rho_g[0], rho_r)
+    print(f"periodic {n}^3 {prec}: u {eu:.2e} rho {er:.2e}")
+    assert eu <= TOL[prec] and er <= TOL[prec]
+    assert abs(a[0] - float(np.sum(rho_r))) <= TOL[prec] * n ** 3
+
+
 @pytest.mark.parametrize("prec", ["fp32", "fp16"])
 def test_set_equilibrium_equals_set_populations(ob, prec):
     from octlb_b200 import cases
