@@ -359,6 +359,43 @@ def aa_measurements(ob, cases, torch, n, steps, warmup, peak):
     return out
 
 
+def cavity3d_gate(ob, cases, torch):
+    """The reference's cavity3d example and its accuracy gate
+    (tests/integration/test_cavity3d_serial.cpp:56-82): one 31^3 block,
+    tau = 0.509, lid 0.1, InterpolatedVelocity walls, ConstRhoBGK, 5,269
+    steps; the centerline u / u_lid against OpenLB's values (relative L2,
+    gate 0.02) and against the reference TimeLoop's FP64 profile
+    (tests/golden/cavity3d_centerline.json), with the steps' MLUPS (CUDA
+    events; a small, launch-bound case)."""
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "tests", "golden", "cavity3d_centerline.json")) as f:
+        g = json.load(f)
+    mesh, init, info = cases.cavity3d(g["resolution"], g["tau"], g["phys_length"], g["phys_velocity"],
+                                      g["phys_viscosity"])
+    out = {"steps": g["steps"], "cells": mesh.n ** 3, "gate": 0.02,
+           "reference_fp64_l2_vs_openlb": g["reference_fp64_l2"]}
+    for pn, prec in (("fp32", ob.FP32), ("fp16", ob.FP16_SHIFTED)):
+        lat = ob.GpuLattice(ob.stamp_fd_kinds(mesh, info["types"]), info["omega"], precision=prec, init_pops=init)
+        lat.set_const_rho(True)
+        lat.set_fd_boundary(info["types"], info["u_wall"])
+        st = torch.cuda.Stream()
+        lat.set_stream(st.cuda_stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        lat.advance(g["steps"])
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / g["steps"]
+        _, u = lat.get_fields()
+        lat.close()
+        prof = cases.cavity3d_centerline(u[0][..., 0], info, g["y_over_h"])
+        out[pn] = {"l2_vs_openlb": cases.relative_l2(prof, g["openlb_u_over_lid"]),
+                   "max_dev_vs_fp64_profile": float(np.max(np.abs(prof - np.array(g["reference_fp64_u_over_lid"])))),
+                   "ms_per_step": ms, "mlups": mesh.n ** 3 / ms / 1e3}
+    return out
+
+
 def forest_measurements(ob, cases, torch, peak):
     """The forest configurations beside the headline line: MLUPS of the
     two-level AMR cavity (64^3 + band under the lid) and of the three-level
@@ -657,6 +694,7 @@ def main():
         out["aa_one_buffer"] = aa_measurements(ob, cases, torch, n, args.steps, args.warmup, peak)
     if rank == 0 and world == 1 and not args.no_forest:
         out["forest"] = forest_measurements(ob, cases, torch, peak)
+        out["cavity3d_gate"] = cavity3d_gate(ob, cases, torch)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_reference_mlups(n, steps_budget_s=args.ref_seconds)
     if rank == 0:

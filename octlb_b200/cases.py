@@ -12,12 +12,16 @@ the shapes the benchmark configurations name:
 * ``cylinder_forest`` channel flow past a cylinder: exact-circle Bouzidi q,
                      parabolic inlet, zero-gradient outlet, refinement near the
                      cylinder
+* ``cavity3d``       the reference's cavity3d example itself: one block of
+                     resolution + 1 lattice nodes per axis, InterpolatedVelocity
+                     on every face with the lid on y+, ConstRhoBGK, parameters
+                     from the reference's UnitConverter
 """
 import math
 
 import numpy as np
 
-from . import (Forest, Mesh, Q, C, feq, BULK, SOLID, BOUZIDI, TB_WALL, TB_OUTFLOW)
+from . import (Forest, Mesh, Q, C, feq, BULK, SOLID, BOUZIDI, TB_WALL, TB_OUTFLOW, FD_VELOCITY)
 
 
 def tgv_fields(nx, ny, nz, u0):
@@ -84,6 +88,64 @@ def cavity_forest(cells=32, n=8, lid=0.1, tau=0.6, band_cells=0):
     mesh = Mesh.from_forest(f, n, tree_boundary_spec=_tb_spec(f, spec))
     init = np.zeros((mesh.n_blocks, n, n, n, Q))
     return mesh, init, {"omega": 1.0 / tau, "tau": tau, "forest": f}
+
+
+def cavity3d(resolution=30, tau=0.509, phys_length=1.0, phys_velocity=1.0, phys_viscosity=0.001):
+    """The reference's cavity3d case (examples/cavity3d/cavity3d_case.h:
+    41-106, 148-197): one block of resolution + 1 nodes per axis at rest,
+    every face InterpolatedVelocity, the y+ face moving with the lid's
+    lattice velocity along x; ConstRhoBGK with the boundary cells in the
+    statistics.  The lattice velocity and omega follow the reference's
+    UnitConverter (unit_converter.cpp:8-26): dx = L / resolution,
+    dt = (tau - 1/2) / 3 dx^2 / nu, u_lid = U dt / dx, omega = 1 / tau.
+    Returns (mesh, init_pops, info); info holds the face types and wall
+    velocities for GpuLattice.set_fd_boundary (the mesh still needs
+    stamp_fd_kinds)."""
+    n = resolution + 1
+    dx = phys_length / resolution
+    dt = (tau - 0.5) / 3.0 * dx * dx / phys_viscosity
+    u_lid = phys_velocity * dt / dx
+    mesh, init, _ = cavity_forest(cells=n, n=n, lid=0.0, tau=tau)
+    u_wall = np.zeros((6, 3))
+    u_wall[3, 0] = u_lid
+    return mesh, init, {"omega": 1.0 / tau, "tau": tau, "u_lid": u_lid, "dx": dx, "resolution": resolution,
+                        "phys_length": phys_length, "types": [FD_VELOCITY] * 6, "u_wall": u_wall}
+
+
+def cavity3d_centerline(ux, info, y_over_h):
+    """u / u_lid on the cavity's vertical centerline x = z = L / 2 at the
+    heights y_over_h, sampled as the reference samples it
+    (cavity3d_case.h:232-300, 323-337): trilinear interpolation between
+    lattice nodes i dx, base node floor(coord / dx) clamped to [0, n - 2];
+    the Dirichlet cells carry their prescribed velocity (the lid's on the
+    interior top-face cells, 0 elsewhere on the faces).  ux: [n, n, n] x
+    velocity of the block's cells."""
+    n = ux.shape[0]
+    dx, lid, L = info["dx"], info["u_lid"], info["phys_length"]
+    u = np.array(ux, dtype=np.float64)
+    face = np.zeros((n, n, n), bool)
+    face[[0, -1], :, :] = face[:, [0, -1], :] = face[:, :, [0, -1]] = True
+    u[face] = 0.0
+    u[1:-1, -1, 1:-1] = lid
+
+    def base(c):
+        return min(max(int(math.floor(c / dx)), 0), n - 2)
+
+    def sample(x, y, z):
+        i, j, k = base(x), base(y), base(z)
+        wx, wy, wz = (x - i * dx) / dx, (y - j * dx) / dx, (z - k * dx) / dx
+        c = u[i:i + 2, j:j + 2, k:k + 2]
+        cx_ = c[0] * (1 - wx) + c[1] * wx
+        cy_ = cx_[0] * (1 - wy) + cx_[1] * wy
+        return cy_[0] * (1 - wz) + cy_[1] * wz
+
+    return np.array([sample(0.5 * L, yh * L, 0.5 * L) / lid for yh in y_over_h])
+
+
+def relative_l2(sim, ref):
+    """sqrt(sum (sim - ref)^2 / sum ref^2) (cavity3d_case.h:128-139)."""
+    sim, ref = np.asarray(sim, np.float64), np.asarray(ref, np.float64)
+    return float(np.sqrt(np.sum((sim - ref) ** 2) / np.sum(ref * ref)))
 
 
 def circle_links(mesh, center, radius, axis_free=2):
