@@ -246,13 +246,32 @@ __device__ __forceinline__ void issue_stage_h(const StepArgs& a, const E* src, E
     issue_pop_h(a, src, stage, bar, row0, R, cells, static_cast<int>(lane), shifted);
 }
 
+// A thread's CPT consecutive FP16 cells: four (8-byte accesses) or two
+// (4-byte accesses), converted to and from float as ld4h / st4h do.
+template <int CPT> struct HalfCells;
+template <> struct HalfCells<4> {
+  __device__ static void ld(const __half* p, float (&v)[4]) { ld4h(p, v[0], v[1], v[2], v[3]); }
+  __device__ static void st(__half* p, const float (&v)[4]) { st4h(p, v[0], v[1], v[2], v[3]); }
+};
+template <> struct HalfCells<2> {
+  __device__ static void ld(const __half* p, float (&v)[2]) {
+    const float2 u = __half22float2(*reinterpret_cast<const __half2*>(p));
+    v[0] = u.x;
+    v[1] = u.y;
+  }
+  __device__ static void st(__half* p, const float (&v)[2]) {
+    *reinterpret_cast<__half2*>(p) = __floats2half2_rn(v[0], v[1]);
+  }
+};
+
 // LOCAL: the AA order's step from the reversed layout -- each cell's own
 // slots, population i from plane opp(i), written to plane i; no shifts, the
 // same values and arithmetic as k_step_aa_local_h (in place: every stage
-// reads and writes only its own cells' slots).
-template <int THREADS, int STAGES, int MINB, bool LOCAL>
+// reads and writes only its own cells' slots).  CPT: cells per thread.
+template <int THREADS, int STAGES, int MINB, bool LOCAL, int CPT>
 __global__ void __launch_bounds__(THREADS, MINB) k_step_rows_h(const StepArgs a) {
-  constexpr uint32_t kCells = 4 * THREADS;
+  using V = HalfCells<CPT>;
+  constexpr uint32_t kCells = CPT * THREADS;
   constexpr uint32_t kStageElems = kQ * kCells;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __half* stages = reinterpret_cast<__half*>(smem_raw);
@@ -262,11 +281,11 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_rows_h(const StepArgs a)
   const uint32_t n = a.n;
   const uint32_t R = kCells / n;
   const uint32_t nst = static_cast<uint32_t>(a.ncore / kCells);
-  // this thread's four cells within a stage: row r, z .. z + 3
-  const uint32_t c = 4 * threadIdx.x;
+  // this thread's cells within a stage: row r, z .. z + CPT - 1
+  const uint32_t c = CPT * threadIdx.x;
   const uint32_t lg = static_cast<uint32_t>(__ffs(static_cast<int>(n)) - 1);
   const uint32_t r = c >> lg, z = c & (n - 1);
-  const uint32_t zm1 = z == 0 ? n - 1 : z - 1, zp4 = z + 4 == n ? 0 : z + 4;
+  const uint32_t zm1 = z == 0 ? n - 1 : z - 1, zpc = z + CPT == n ? 0 : z + CPT;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
@@ -311,33 +330,35 @@ __global__ void __launch_bounds__(THREADS, MINB) k_step_rows_h(const StepArgs a)
       }
     }
     const __half* S = stages + s * kStageElems + r * n;
-    float f0[kQ], f1[kQ], f2[kQ], f3[kQ];
+    float f[CPT][kQ];
 #pragma unroll
     for (int i = 0; i < kQ; ++i) {
+      float v[CPT];
       if constexpr (LOCAL) {
-        ld4h(S + opp(i) * kCells + z, f0[i], f1[i], f2[i], f3[i]);
+        V::ld(S + opp(i) * kCells + z, v);
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) f[j][i] = v[j];
         continue;
       }
       const __half* p = S + i * kCells;
-      if (cz(i) == 0) {
-        ld4h(p + z, f0[i], f1[i], f2[i], f3[i]);
-      } else if (cz(i) == 1) {  // cells z..z+3 pull z-1..z+2
-        float w;
-        ld4h(p + z, f1[i], f2[i], f3[i], w);
-        f0[i] = __half2float(p[zm1]);
-      } else {                  // cells z..z+3 pull z+1..z+4
-        float w;
-        ld4h(p + z, w, f0[i], f1[i], f2[i]);
-        f3[i] = __half2float(p[zp4]);
+      V::ld(p + z, v);
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        if (cz(i) == 0) f[j][i] = v[j];
+        else if (cz(i) == 1) f[j][i] = j == 0 ? __half2float(p[zm1]) : v[j - 1];  // cells pull z-1 ..
+        else f[j][i] = j == CPT - 1 ? __half2float(p[zpc]) : v[j + 1];             // cells pull z+1 ..
       }
     }
-    bgk<false>(f0, a.omega, a.scale, a.inv_scale);
-    bgk<false>(f1, a.omega, a.scale, a.inv_scale);
-    bgk<false>(f2, a.omega, a.scale, a.inv_scale);
-    bgk<false>(f3, a.omega, a.scale, a.inv_scale);
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) bgk<false>(f[j], a.omega, a.scale, a.inv_scale);
     __half* o = dst + static_cast<long long>(blockIdx.x + k * gridDim.x) * kCells + c;
 #pragma unroll
-    for (int i = 0; i < kQ; ++i) st4h(o + i * a.qs, f0[i], f1[i], f2[i], f3[i]);
+    for (int i = 0; i < kQ; ++i) {
+      float v[CPT];
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) v[j] = f[j][i];
+      V::st(o + i * a.qs, v);
+    }
   }
 }
 
@@ -519,29 +540,35 @@ cudaError_t launch_step_bulk(const StepArgs& a, int grid, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-// The staged FP16 step's launch shapes: threads, stages, and the CTAs per
-// SM the register budget is set for.  Per step on the 256^3 box, two boxes:
-// 0 (256 x 2) 0.2077 / 0.2058 ms, 1 (128 x 2) 0.2070 / 0.2169, 2 (128 x 3)
-// 0.2129 / 0.2306, 3 (64 x 2) 0.2130, 4 (64 x 3) 0.2521; k_step_quad_h
-// 0.2210 / 0.2213.
+// The staged FP16 step's launch shapes: threads, stages, the CTAs per SM
+// the register budget is set for, cells per thread.  Per step on the 256^3
+// box, two boxes: 0 (256 x 2, four cells) 0.2077 / 0.2058 ms, 1 (128 x 2)
+// 0.2070 / 0.2169, 2 (128 x 3) 0.2129 / 0.2306, 3 (64 x 2) 0.2130, 4 (64 x 3)
+// 0.2521; k_step_quad_h 0.2210 / 0.2213.  5-7 take two cells per thread
+// (79 registers, more warps): on a third box, where 0 took 0.2053 ms, 5
+// (256 x 3) took 0.2265, 6 (256 x 2) 0.2475 and 7 (128 x 3) 0.2231.
 namespace {
-constexpr int kRowsVariants = 5;
-constexpr int kRowsThreads[kRowsVariants] = {256, 128, 128, 64, 64};
-constexpr int kRowsStages[kRowsVariants] = {2, 2, 3, 2, 3};
+constexpr int kRowsVariants = 8;
+constexpr int kRowsThreads[kRowsVariants] = {256, 128, 128, 64, 64, 256, 256, 128};
+constexpr int kRowsStages[kRowsVariants] = {2, 2, 3, 2, 3, 3, 2, 3};
+constexpr int kRowsCpt[kRowsVariants] = {4, 4, 4, 4, 4, 2, 2, 2};
 constexpr int rows_threads(int v) { return kRowsThreads[v]; }
 constexpr int rows_stages(int v) { return kRowsStages[v]; }
 size_t rows_smem(int v) {
-  return static_cast<size_t>(rows_stages(v)) * kQ * 4 * rows_threads(v) * sizeof(__half) +
+  return static_cast<size_t>(rows_stages(v)) * kQ * kRowsCpt[v] * rows_threads(v) * sizeof(__half) +
          rows_stages(v) * sizeof(uint64_t);
 }
 template <bool LOCAL, typename F>
 auto with_rows_kernel_t(int v, F&& f) {
   switch (v) {
-    case 1: return f(k_step_rows_h<128, 2, 4, LOCAL>);
-    case 2: return f(k_step_rows_h<128, 3, 3, LOCAL>);
-    case 3: return f(k_step_rows_h<64, 2, 8, LOCAL>);
-    case 4: return f(k_step_rows_h<64, 3, 7, LOCAL>);
-    default: return f(k_step_rows_h<256, 2, 2, LOCAL>);
+    case 1: return f(k_step_rows_h<128, 2, 4, LOCAL, 4>);
+    case 2: return f(k_step_rows_h<128, 3, 3, LOCAL, 4>);
+    case 3: return f(k_step_rows_h<64, 2, 8, LOCAL, 4>);
+    case 4: return f(k_step_rows_h<64, 3, 7, LOCAL, 4>);
+    case 5: return f(k_step_rows_h<256, 3, 3, LOCAL, 2>);
+    case 6: return f(k_step_rows_h<256, 2, 3, LOCAL, 2>);
+    case 7: return f(k_step_rows_h<128, 3, 6, LOCAL, 2>);
+    default: return f(k_step_rows_h<256, 2, 2, LOCAL, 4>);
   }
 }
 template <typename F>
@@ -550,7 +577,7 @@ auto with_rows_kernel(int v, bool local, F&& f) {
 }
 }  // namespace
 
-long long rows_stage_cells(int variant) { return 4LL * rows_threads(variant); }
+long long rows_stage_cells(int variant) { return static_cast<long long>(kRowsCpt[variant]) * rows_threads(variant); }
 
 bool rows_step_eligible(int n, long long ncore, long long qs, int variant) {
   if (variant < 0 || variant >= kRowsVariants) return false;

@@ -2160,7 +2160,7 @@ static int create_common(const octlb_tables* t, const octlb_params* p, const dou
   if (const char* st = std::getenv("OCTLB_TEST_BULK_STALL")) ctx->stall_first_row = st[0] == '1' ? 1 : 0;
   if (const char* fr = std::getenv("OCTLB_FP16_ROWS")) {
     const std::string v(fr);
-    ctx->fp16_rows = v == "off" ? -1 : (v.size() == 1 && v[0] >= '0' && v[0] <= '4' ? v[0] - '0' : ctx->fp16_rows);
+    ctx->fp16_rows = v == "off" ? -1 : (v.size() == 1 && v[0] >= '0' && v[0] <= '7' ? v[0] - '0' : ctx->fp16_rows);
   }
   if (const char* ar = std::getenv("OCTLB_AA_ROWS")) {
     const std::string v(ar);

@@ -145,14 +145,16 @@ def test_set_equilibrium_equals_set_populations(ob, prec):
 def test_fp16_four_cell_step_equals_paired_step(ob, monkeypatch, n):
     """The four-cells-per-thread FP16 periodic steps -- the one fed by bulk
     async copies through shared-memory stages in each of its launch shapes
-    (OCTLB_FP16_ROWS, 128 or 256 threads, 2 to 4 stages; R = 512 / n or
-    1024 / n z rows per stage, two copies per population at the y wrap), and
+    (OCTLB_FP16_ROWS: 64 to 256 threads, 2 or 3 stages, four or two cells per
+    thread; whole z rows per stage, two copies per population at the y
+    wrap), and
     the one with 8-byte global loads (OCTLB_FP16_ROWS=off) -- and the paired
     step (OCTLB_FP16_PAIR=1) give bitwise equal states."""
     from octlb_b200 import cases
     mesh, init, info = cases.tgv_periodic(n, u0=0.05, tau=0.55)
     out = []
-    for pair, rows in (("1", "off"), ("0", "off"), ("0", "0"), ("0", "1"), ("0", "2"), ("0", "3"), ("0", "4")):
+    for pair, rows in (("1", "off"), ("0", "off"), ("0", "0"), ("0", "1"), ("0", "2"), ("0", "3"), ("0", "4"),
+                       ("0", "5"), ("0", "6"), ("0", "7")):
         monkeypatch.setenv("OCTLB_FP16_PAIR", pair)
         monkeypatch.setenv("OCTLB_FP16_ROWS", rows)
         lat = ob.GpuLattice(mesh, info["omega"], precision=ob.FP16_SHIFTED, init_pops=init)
