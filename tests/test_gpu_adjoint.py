@@ -113,26 +113,31 @@ def test_adjoint_c5_matches_fp64_fd_and_cost(ob):
     """The full adjoint configuration against FP64 finite differences and the
     tangent-linear reference; then its cost: (forward + adjoint sweep) of the
     1,000 calls against the forward alone, both in steady state (the forward
-    after a warm-up call, the sweep on its second call, after the first
-    captured its graphs), must stay within the north star's 3x."""
+    after a warm-up call, the sweep after a first call that captured its
+    graphs; each the best of three timings), must stay within the north
+    star's 3x."""
     check(ob, "adjoint_c5.npz", 16)
     g = np.load(os.path.join(HERE, "golden", "adjoint_c5.npz"))
     steps, window = int(g["steps"]), int(g["window"])
     _, lat = lattice(ob)
     lat.advance(3)  # warm-up (graph capture)
     lat.synchronize()
-    t0 = time.perf_counter()
-    lat.advance(steps)
-    lat.synchronize()
-    t_fwd = time.perf_counter() - t0
+    t_fwd = float("inf")
+    for _ in range(3):
+        t0 = time.perf_counter()
+        lat.advance(steps)
+        lat.synchronize()
+        t_fwd = min(t_fwd, time.perf_counter() - t0)
     lat.close()
     _, lat = lattice(ob)
     lat.adjoint(steps, window, 16)
     lat.synchronize()
-    t0 = time.perf_counter()
-    lat.adjoint(steps, window, 16)
-    lat.synchronize()
-    t_all = time.perf_counter() - t0
+    t_all = float("inf")
+    for _ in range(3):
+        t0 = time.perf_counter()
+        lat.adjoint(steps, window, 16)
+        lat.synchronize()
+        t_all = min(t_all, time.perf_counter() - t0)
     lat.close()
     ratio = (t_all - t_fwd) / t_fwd
     print(f"adjoint cost: forward {t_fwd:.3f} s, forward + adjoint {t_all:.3f} s, adjoint / forward {ratio:.2f}")
