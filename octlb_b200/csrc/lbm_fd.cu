@@ -15,7 +15,8 @@
 // that order.  Edge cells read plane cells and corners read edge cells, so the
 // pass runs as three launches -- planes, edges, corners -- each writing the
 // rewritten populations to its own rows and reading an earlier phase's row
-// where the reference's walk would have rewritten the cell already.  A fourth
+// where the reference's walk would have rewritten the cell already (one warp
+// per cell, lane = population, every read of the stencil loaded at once).  A fourth
 // launch collides the rewritten cells (velocity cells at the prescribed
 // velocity, the next step's time; pressure cells are not collided) into the
 // state buffer.  Every read a cell makes is resolved on the host into a table
@@ -77,58 +78,6 @@ __device__ __forceinline__ float feq_i(int i, float rho, const float u[3], float
   return rho * wf(i) * (1.f + 3.f * cu + 4.5f * cu * cu - 1.5f * usq) - wf(i);
 }
 
-template <typename T>
-struct FdCtx {
-  const T* state;
-  long long qs;
-  float inv_s;
-  const FdCell* cells;
-  const float* fnew;  // [rows][19]
-  float t;
-  const double* cr_avg;  // ConstRhoBGK: the average density the step's collide used, or null
-};
-
-template <typename T>
-__device__ __forceinline__ void read_u(const FdCtx<T>& c, const FdURead& r, float u[3]) {
-  if (r.code == kFdZero) {
-    u[0] = u[1] = u[2] = 0.f;
-  } else if (r.code == kFdFluid) {
-    float f[kQ];
-    load_pops(c.state, c.qs, r.idx, c.inv_s, f);
-    float dh, jx, jy, jz;
-    moments(f, dh, jx, jy, jz);
-    const float k = 1.f / (1.f + dh);
-    u[0] = jx * k; u[1] = jy * k; u[2] = jz * k;
-  } else {
-    prescribed(c.cells, static_cast<int>(r.idx), c.t, u);
-  }
-  if (r.flip & 1) u[0] = -u[0];
-  if (r.flip & 2) u[1] = -u[1];
-  if (r.flip & 4) u[2] = -u[2];
-}
-
-template <typename T>
-__device__ __forceinline__ float read_rho(const FdCtx<T>& c, const FdRRead& r) {
-  if (r.code == kFdRhoConst) return r.val;
-  float f[kQ];
-  if (r.code == kFdRhoSumPre || r.code == kFdRhoBmPre) {
-    load_pops(c.state, c.qs, r.idx, c.inv_s, f);
-  } else {
-#pragma unroll
-    for (int i = 0; i < kQ; ++i) f[i] = c.fnew[r.idx * kQ + i];
-  }
-  if (r.code == kFdRhoSumPre || r.code == kFdRhoSumNew) {
-    // a kBulk cell's stored density under ConstRhoBGK carries the 1 -
-    // average_rho its collide added (urow = 1 marks a kBulk cell)
-    const float shift = (r.code == kFdRhoSumPre && r.urow == 1 && c.cr_avg) ? static_cast<float>(1.0 - *c.cr_avg)
-                                                                             : 0.f;
-    return 1.f + sum_pops(f) - shift;
-  }
-  float u[3];
-  prescribed(c.cells, r.urow, c.t, u);
-  return bm_rho(f, r.d, r.o, u);
-}
-
 // Gradient along `axis` by the one-sided second-order stencil
 // -n (-3 u0 + 4 u1 - u2) / 2 (u1, u2 one and two cells inward).
 __device__ __forceinline__ void normal_grad(const float u0[3], const float u1[3], const float u2[3], int n,
@@ -137,32 +86,117 @@ __device__ __forceinline__ void normal_grad(const float u0[3], const float u1[3]
   for (int b = 0; b < 3; ++b) g[b] = -n * (-3.f * u0[b] + 4.f * u1[b] - u2[b]) * 0.5f;
 }
 
-// One boundary cell of role `role` (1 plane, 2 edge, 3 corner): rewritten
-// populations feq(rho, u) + f_neq(Pi), Pi = -rho / (3 omega) (du + du^T), into
-// its row of fnew.
+// Direction components and weight of a population index known only at run
+// time (one lane per population), from bit masks of the D3Q19 table.
+__host__ __device__ constexpr uint32_t fd_mask(int axis, int sign) {
+  uint32_t m = 0;
+  for (int i = 0; i < kQ; ++i)
+    if ((axis == 0 ? cx(i) : axis == 1 ? cy(i) : cz(i)) == sign) m |= 1u << i;
+  return m;
+}
+constexpr uint32_t kFdPx = fd_mask(0, 1), kFdNx = fd_mask(0, -1), kFdPy = fd_mask(1, 1), kFdNy = fd_mask(1, -1),
+                   kFdPz = fd_mask(2, 1), kFdNz = fd_mask(2, -1);
+__device__ __forceinline__ int c_rt(int axis, int i) {
+  const uint32_t pos = axis == 0 ? kFdPx : (axis == 1 ? kFdPy : kFdPz);
+  const uint32_t neg = axis == 0 ? kFdNx : (axis == 1 ? kFdNy : kFdNz);
+  return static_cast<int>((pos >> i) & 1u) - static_cast<int>((neg >> i) & 1u);
+}
+__device__ __forceinline__ float w_rt(const int c[3]) {
+  const int m = (c[0] != 0) + (c[1] != 0) + (c[2] != 0);
+  return m == 0 ? 1.0f / 3.0f : (m == 1 ? 1.0f / 18.0f : 1.0f / 36.0f);
+}
+// Sum over the warp, every lane receiving it.
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// One boundary cell of role `role` (1 plane, 2 edge, 3 corner) per warp,
+// lane i holding population i of every cell the stencil reads: all of them
+// are loaded up front (independent loads, one memory latency), the moments
+// and densities summed over the warp.  Rewritten populations feq(rho, u) +
+// f_neq(Pi), Pi = -rho / (3 omega) (du + du^T), into the cell's row of fnew.
 template <typename T>
 __global__ void __launch_bounds__(kFdThreads)
 k_fd_reconstruct(const T* state, long long qs, float inv_s, const FdCell* cells, const int* list, int n,
                  float* fnew, const double* time, float omega, const double* cr_avg) {
-  const int k = blockIdx.x * kFdThreads + threadIdx.x;
-  if (k >= n) return;
-  const int row = list[k];
+  const int w = static_cast<int>((blockIdx.x * kFdThreads + threadIdx.x) >> 5);
+  if (w >= n) return;  // whole warps
+  const int lane = threadIdx.x & 31;
+  const bool act = lane < kQ;
+  const int i = act ? lane : 0;
+  const int ci[3] = {c_rt(0, i), c_rt(1, i), c_rt(2, i)};
+  const int row = list[w];
   const FdCell& cell = cells[row];
-  FdCtx<T> c{state, qs, inv_s, cells, fnew, static_cast<float>(*time), cr_avg};
+  const float t = static_cast<float>(*time);
+  const int nr = cell.role == 2 ? 4 : (cell.role == 3 ? 6 : 0);
+  const bool own = cell.role == 1 && cell.kind != kPressureDirichlet;
+  float fu[7], fr[6];
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    const FdURead& r = cell.u[j];
+    fu[j] = act && r.code == kFdFluid ? Store<T>::ld(state + i * qs + r.idx, inv_s) : 0.f;
+  }
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const FdRRead& r = cell.r[j];
+    float v = 0.f;
+    if (act && j < nr && r.code != kFdRhoConst)
+      v = r.code == kFdRhoSumPre || r.code == kFdRhoBmPre ? Store<T>::ld(state + i * qs + r.idx, inv_s)
+                                                          : fnew[r.idx * kQ + i];
+    fr[j] = v;
+  }
+  const float fo = act && own ? Store<T>::ld(state + i * qs + cell.slot, inv_s) : 0.f;
+  // the seven velocities
   float uu[7][3];
 #pragma unroll
-  for (int j = 0; j < 7; ++j) read_u(c, cell.u[j], uu[j]);
+  for (int j = 0; j < 7; ++j) {
+    const FdURead& r = cell.u[j];
+    if (r.code == kFdZero) {
+      uu[j][0] = uu[j][1] = uu[j][2] = 0.f;
+    } else if (r.code == kFdFluid) {
+      const float dh = warp_sum(fu[j]);
+      const float k = 1.f / (1.f + dh);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) uu[j][a] = warp_sum(ci[a] * fu[j]) * k;
+    } else {
+      prescribed(cells, static_cast<int>(r.idx), t, uu[j]);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      if (r.flip >> a & 1) uu[j][a] = -uu[j][a];
+  }
+  // velocityBMRho of values v held one population per lane
+  auto bm = [&](float v, int d, int o, const float u[3]) {
+    const float out = warp_sum(ci[d] == o ? v : 0.f), wall = warp_sum(ci[d] == 0 ? v : 0.f);
+    return (2.f * out + wall + 1.f) / (1.f + o * u[d]);
+  };
+  float rr[6];
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    rr[j] = 0.f;
+    if (j >= nr) continue;
+    const FdRRead& r = cell.r[j];
+    if (r.code == kFdRhoConst) {
+      rr[j] = r.val;
+    } else if (r.code == kFdRhoSumPre || r.code == kFdRhoSumNew) {
+      // a kBulk cell's stored density under ConstRhoBGK carries the 1 -
+      // average_rho its collide added (urow = 1 marks a kBulk cell)
+      const float shift =
+          (r.code == kFdRhoSumPre && r.urow == 1 && cr_avg) ? static_cast<float>(1.0 - *cr_avg) : 0.f;
+      rr[j] = 1.f + warp_sum(fr[j]) - shift;
+    } else {
+      float u[3];
+      prescribed(cells, r.urow, t, u);
+      rr[j] = bm(fr[j], r.d, r.o, u);
+    }
+  }
   float du[3][3];
   float rho;
   if (cell.role == 1) {
     const int d = cell.d, o = cell.o;
-    if (cell.kind == kPressureDirichlet) {
-      rho = cell.rho_target;
-    } else {
-      float f[kQ];
-      load_pops(state, qs, cell.slot, inv_s, f);
-      rho = bm_rho(f, d, o, uu[0]);
-    }
+    rho = cell.kind == kPressureDirichlet ? cell.rho_target : bm(fo, d, o, uu[0]);
     normal_grad(uu[0], uu[1], uu[2], o, du[d]);
     const int t0 = (d + 1) % 3 < (d + 2) % 3 ? (d + 1) % 3 : (d + 2) % 3;
     const int t1 = 3 - d - t0;
@@ -177,37 +211,35 @@ k_fd_reconstruct(const T* state, long long qs, float inv_s, const FdCell* cells,
     for (int b = 0; b < 3; ++b) du[p][b] = (uu[1][b] - uu[2][b]) * 0.5f;
     normal_grad(uu[0], uu[3], uu[4], cell.nrm[0], du[d1]);
     normal_grad(uu[0], uu[5], uu[6], cell.nrm[1], du[d2]);
-    rho = 2.f / 3.f * (read_rho(c, cell.r[0]) + read_rho(c, cell.r[1])) -
-          1.f / 6.f * (read_rho(c, cell.r[2]) + read_rho(c, cell.r[3]));
+    rho = 2.f / 3.f * (rr[0] + rr[1]) - 1.f / 6.f * (rr[2] + rr[3]);
   } else {
 #pragma unroll
     for (int a = 0; a < 3; ++a) normal_grad(uu[0], uu[1 + 2 * a], uu[2 + 2 * a], cell.nrm[a], du[a]);
-    rho = 4.f / 9.f * (read_rho(c, cell.r[0]) + read_rho(c, cell.r[1]) + read_rho(c, cell.r[2])) -
-          1.f / 9.f * (read_rho(c, cell.r[3]) + read_rho(c, cell.r[4]) + read_rho(c, cell.r[5]));
+    rho = 4.f / 9.f * (rr[0] + rr[1] + rr[2]) - 1.f / 9.f * (rr[3] + rr[4] + rr[5]);
   }
+  if (!act) return;
   const float s = -rho / 3.f / omega;
   const float pi[6] = {2.f * du[0][0] * s, (du[0][1] + du[1][0]) * s, (du[0][2] + du[2][0]) * s,
                        2.f * du[1][1] * s, (du[1][2] + du[2][1]) * s, 2.f * du[2][2] * s};
   const float* u = uu[0];
   const float usq = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-  float* out = fnew + static_cast<long long>(row) * kQ;
+  const float c3[3] = {static_cast<float>(ci[0]), static_cast<float>(ci[1]), static_cast<float>(ci[2])};
+  // f_neq from the symmetric stress (lbm.h:248-270): sum over a <= b of
+  // (c_a c_b - delta_ab / 3) (x2 off the diagonal) Pi_ab, times w 9 / 2
+  float q = 0.f;
+  int m = 0;
 #pragma unroll
-  for (int i = 0; i < kQ; ++i) {
-    const float c3[3] = {static_cast<float>(cx(i)), static_cast<float>(cy(i)), static_cast<float>(cz(i))};
-    // f_neq from the symmetric stress (lbm.h:248-270): sum over a <= b of
-    // (c_a c_b - delta_ab / 3) (x2 off the diagonal) Pi_ab, times w 9 / 2
-    float q = 0.f;
-    int m = 0;
+  for (int a = 0; a < 3; ++a)
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int b = a; b < 3; ++b, ++m) {
-        float qq = c3[a] * c3[b] - (a == b ? 1.f / 3.f : 0.f);
-        if (a != b) qq *= 2.f;
-        q += qq * pi[m];
-      }
-    out[i] = feq_i(i, rho, u, usq) + q * wf(i) * 4.5f;
-  }
+    for (int b = a; b < 3; ++b, ++m) {
+      float qq = c3[a] * c3[b] - (a == b ? 1.f / 3.f : 0.f);
+      if (a != b) qq *= 2.f;
+      q += qq * pi[m];
+    }
+  const float wi = w_rt(ci);
+  const float cu = c3[0] * u[0] + c3[1] * u[1] + c3[2] * u[2];
+  const float feq = rho * wi * (1.f + 3.f * cu + 4.5f * cu * cu - 1.5f * usq) - wi;
+  fnew[static_cast<long long>(row) * kQ + i] = feq + q * wi * 4.5f;
 }
 
 // The collide of the boundary cells into the state buffer, at the start of
@@ -332,8 +364,9 @@ cudaError_t launch_fd_reconstruct(const void* state, long long qs, float inv_s, 
                                   int n, float* fnew, const double* time, float omega, const double* cr_avg,
                                   cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_fd_reconstruct<T><<<fd_grid(n), kFdThreads, 0, s>>>(static_cast<const T*>(state), qs, inv_s, cells, list, n,
-                                                         fnew, time, omega, cr_avg);
+  const unsigned grid = static_cast<unsigned>((static_cast<long long>(n) * 32 + kFdThreads - 1) / kFdThreads);
+  k_fd_reconstruct<T><<<grid, kFdThreads, 0, s>>>(static_cast<const T*>(state), qs, inv_s, cells, list, n, fnew,
+                                                  time, omega, cr_avg);
   return cudaGetLastError();
 }
 
