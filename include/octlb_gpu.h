@@ -224,6 +224,42 @@ int octlb_fd_plan(const octlb_tables* tables, const int types[6], const double u
                   int max_records);
 int octlb_fd_record_bytes(void);
 
+/* Inlet velocity fields of the velocity faces, the reference's
+ * InletVelocityField kinds (inlet_velocity_field.h), each ramped by
+ * 10x^3 - 15x^4 + 6x^5, x = t / ramp_end_t (none for ramp_end_t <= 0):
+ *   UNIFORM             u = u (UniformInletProfile, :131-159);
+ *   POISEUILLE          u = u_peak p(i0, n_inplane[0]) p(i1, n_inplane[1]) u,
+ *                       p(i, n) = 4 c (1 - c), c = (i + 1/2) / n, i0 / i1 the
+ *                       cell's block-local in-plane indices (y, z on x faces;
+ *                       x, z on y faces; x, y on z faces) (PoiseuilleInletProfile,
+ *                       :38-129);
+ *   CHANNEL_POISEUILLE  the same from the cell's physical position, block
+ *                       origin + (index + 1/2) cell width, on the patch
+ *                       [patch[0], patch[1]] x [patch[2], patch[3]] of the in-plane
+ *                       coordinates, c clamped to [0, 1]
+ *                       (ChannelPoiseuilleInletProfile, :163-269).
+ * u is the flow direction for the Poiseuille kinds. */
+#define OCTLB_INLET_NONE 0
+#define OCTLB_INLET_UNIFORM 1
+#define OCTLB_INLET_POISEUILLE 2
+#define OCTLB_INLET_CHANNEL_POISEUILLE 3
+typedef struct octlb_fd_inlet {
+  int kind;
+  int n_inplane[2];
+  double u[3];
+  double u_peak;
+  double patch[4];
+  double ramp_end_t;
+} octlb_fd_inlet;
+/* octlb_gpu_set_fd_boundary with an inlet field per face (inlets[6], NULL:
+ * none), in place of the uniform inlet_u; the cell's prescribed velocity is
+ * the field of the first face it touches that has one. */
+int octlb_gpu_set_fd_boundary_inlets(octlb_ctx* ctx, const int types[6], const double u_wall[18],
+                                     const double rho_target[6], const octlb_fd_inlet* inlets);
+/* octlb_fd_plan with inlet fields. */
+int octlb_fd_plan_inlets(const octlb_tables* tables, const int types[6], const double u_wall[18],
+                         const double rho_target[6], const octlb_fd_inlet* inlets, void* records, int max_records);
+
 /* ---- VTK output (src/solver/io/vtk_writer/) ------------------------------
  * The files of the reference's writer, byte for byte for the same values: an
  * XML StructuredGrid .vts per block with binary (base64, UInt32 header)

@@ -23,7 +23,7 @@ from . import capi
 from .capi import (BULK, SOLID, BOUNCE_BACK, MOVING_BOUNCE_BACK, BOUZIDI, VELOCITY_DIRICHLET,
                    PRESSURE_DIRICHLET, OUTFLOW, FP32, FP16_SHIFTED, STREAM_ROTATE, STREAM_LINKS,
                    TB_NONE, TB_WALL, TB_OUTFLOW, COUPLER_REFERENCE, COUPLER_PHYSICAL, ORDER_AB, ORDER_AA,
-                   OctlbError)
+                   INLET_NONE, INLET_UNIFORM, INLET_POISEUILLE, INLET_CHANNEL_POISEUILLE, OctlbError)
 
 capi.lib()  # fail loudly at import when the library is missing
 
@@ -228,6 +228,30 @@ def vtk_write_index(output_dir, base_name, step, vts_relative_paths):
 
 
 FD_NO_SLIP, FD_MOVING_LID, FD_VELOCITY, FD_OUTFLOW, FD_PRESSURE = 0, 1, 2, 3, 4
+
+
+def fd_inlet(kind, u=(0.0, 0.0, 0.0), u_peak=0.0, n_inplane=(1, 1), patch=(0.0, 1.0, 0.0, 1.0), ramp_end_t=0.0):
+    """One face's inlet velocity field (octlb_fd_inlet): kind INLET_UNIFORM
+    (velocity u), INLET_POISEUILLE (peak u_peak along direction u over
+    n_inplane cells of the block's in-plane axes) or INLET_CHANNEL_POISEUILLE
+    (the same over the physical patch (in0_lo, in0_hi, in1_lo, in1_hi))."""
+    return {"kind": kind, "u": u, "u_peak": u_peak, "n_inplane": n_inplane, "patch": patch,
+            "ramp_end_t": ramp_end_t}
+
+
+def fd_inlets(inlets):
+    """Six faces' inlet fields (dicts of fd_inlet, or None) as the C array."""
+    arr = (capi.FdInlet * 6)()
+    for f, d in enumerate(inlets):
+        if d is None:
+            continue
+        arr[f].kind = int(d["kind"])
+        arr[f].n_inplane[:] = [int(v) for v in d["n_inplane"]]
+        arr[f].u[:] = [float(v) for v in d["u"]]
+        arr[f].u_peak = float(d["u_peak"])
+        arr[f].patch[:] = [float(v) for v in d["patch"]]
+        arr[f].ramp_end_t = float(d["ramp_end_t"])
+    return arr
 
 
 def stamp_fd_kinds(mesh, types):
@@ -471,15 +495,22 @@ class GpuLattice:
         self._check(self._L.octlb_gpu_write_vtk(self._h, str(output_dir).encode(), str(base_name).encode(),
                                                 int(step), int(rank), mask, 1 if write_index else 0))
 
-    def set_fd_boundary(self, types, u_wall=None, rho_target=None, inlet_u=None, ramp_end_t=0.0):
+    def set_fd_boundary(self, types, u_wall=None, rho_target=None, inlet_u=None, ramp_end_t=0.0, inlets=None):
         """The finite-difference domain conditions (octlb_gpu_set_fd_boundary):
         types per face (x-, x+, y-, y+, z-, z+), FD_VELOCITY or FD_PRESSURE;
         u_wall [6][3] (the y+ row is the lid), rho_target [6], inlet_u [6][3]
         (a nonzero row: that face's uniform inlet, ramped over ramp_end_t
-        steps).  The mesh's kinds must be stamped (stamp_fd_kinds)."""
+        steps) -- or inlets, six inlet fields (fd_inlet(); None for a face
+        without one; octlb_gpu_set_fd_boundary_inlets).  The mesh's kinds must
+        be stamped (stamp_fd_kinds)."""
         t = np.ascontiguousarray(types, np.int32).reshape(6)
         u = np.zeros((6, 3)) if u_wall is None else np.ascontiguousarray(u_wall, np.float64).reshape(6, 3)
         r = np.ones(6) if rho_target is None else np.ascontiguousarray(rho_target, np.float64).reshape(6)
+        if inlets is not None:
+            arr = fd_inlets(inlets)
+            self._check(self._L.octlb_gpu_set_fd_boundary_inlets(
+                self._h, capi.ptr(t, ctypes.c_int), capi.ptr(u, ctypes.c_double), capi.ptr(r, ctypes.c_double), arr))
+            return
         iu = None if inlet_u is None else np.ascontiguousarray(inlet_u, np.float64).reshape(6, 3)
         self._check(self._L.octlb_gpu_set_fd_boundary(self._h, capi.ptr(t, ctypes.c_int), capi.ptr(u, ctypes.c_double),
                                                       capi.ptr(r, ctypes.c_double),

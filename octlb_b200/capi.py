@@ -63,6 +63,14 @@ class AdjParams(ctypes.Structure):
 
 VTK_VELOCITY, VTK_DENSITY, VTK_PRESSURE = 1, 2, 4
 
+INLET_NONE, INLET_UNIFORM, INLET_POISEUILLE, INLET_CHANNEL_POISEUILLE = 0, 1, 2, 3
+
+
+class FdInlet(ctypes.Structure):
+    """octlb_fd_inlet: one face's inlet velocity field."""
+    _fields_ = [("kind", ctypes.c_int), ("n_inplane", ctypes.c_int * 2), ("u", ctypes.c_double * 3),
+                ("u_peak", ctypes.c_double), ("patch", ctypes.c_double * 4), ("ramp_end_t", ctypes.c_double)]
+
 
 class Partition(ctypes.Structure):
     """octlb_partition."""
@@ -118,6 +126,9 @@ def lib():
         "octlb_fd_plan": (ctypes.c_int, [ctypes.POINTER(Tables), I32P, F64P, F64P, F64P, ctypes.c_double, P,
                                          ctypes.c_int]),
         "octlb_fd_record_bytes": (ctypes.c_int, []),
+        "octlb_gpu_set_fd_boundary_inlets": (ctypes.c_int, [P, I32P, F64P, F64P, ctypes.POINTER(FdInlet)]),
+        "octlb_fd_plan_inlets": (ctypes.c_int, [ctypes.POINTER(Tables), I32P, F64P, F64P, ctypes.POINTER(FdInlet),
+                                                P, ctypes.c_int]),
         "octlb_gpu_write_vtk": (ctypes.c_int, [P, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_int, ctypes.c_int]),
         "octlb_vtk_write_block": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, F64P,

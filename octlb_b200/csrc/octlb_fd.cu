@@ -251,14 +251,78 @@ int octlb_fd_stamp_kinds(const octlb_tables* t, const int types[6], uint8_t* kin
 
 namespace octlb_host {
 
+int check_inlets(octlb_ctx* ctx, const octlb_fd_inlet* inlets) {
+  if (!inlets) return OCTLB_OK;
+  for (int f = 0; f < 6; ++f) {
+    const octlb_fd_inlet& in = inlets[f];
+    if (in.kind < OCTLB_INLET_NONE || in.kind > OCTLB_INLET_CHANNEL_POISEUILLE)
+      return fail(ctx, OCTLB_EINVAL, "fd boundary: inlet kind outside 0..3");
+    if (in.kind == OCTLB_INLET_POISEUILLE && (in.n_inplane[0] < 1 || in.n_inplane[1] < 1))
+      return fail(ctx, OCTLB_EINVAL, "fd boundary: a Poiseuille inlet needs n_inplane >= 1");
+    if (in.kind == OCTLB_INLET_CHANNEL_POISEUILLE && !(in.patch[1] > in.patch[0] && in.patch[3] > in.patch[2]))
+      return fail(ctx, OCTLB_EINVAL, "fd boundary: a channel inlet patch needs hi > lo");
+  }
+  return OCTLB_OK;
+}
+
+// The inlet field of face `face` at cell p of a block with bounds bd (x0, y0,
+// z0, x1, y1, z1), before the ramp (inlet_velocity_field.h: UniformInletProfile
+// :131-159, PoiseuilleInletProfile :38-129 from block-local indices,
+// ChannelPoiseuilleInletProfile :163-269 from the physical position origin +
+// (index + 1/2) cell width, as PrescribedBoundaryU supplies it,
+// interpolated_velocity.h:69-117).  In-plane axes: y, z on x faces; x, z on y
+// faces; x, y on z faces.
+void inlet_velocity(const octlb_fd_inlet& in, int face, const Pos& p, int n, const double* bd, double u[3]) {
+  if (in.kind == OCTLB_INLET_UNIFORM) {
+    for (int d = 0; d < 3; ++d) u[d] = in.u[d];
+    return;
+  }
+  const int ax = face / 2, a0 = ax == 0 ? 1 : 0, a1 = ax == 2 ? 1 : 2;
+  double p0, p1;
+  if (in.kind == OCTLB_INLET_POISEUILLE) {
+    const double c0 = (p[a0] + 0.5) / in.n_inplane[0], c1 = (p[a1] + 0.5) / in.n_inplane[1];
+    p0 = 4.0 * c0 * (1.0 - c0);
+    p1 = 4.0 * c1 * (1.0 - c1);
+  } else {
+    const double cw = (bd[3] - bd[0]) / n;
+    auto clamp01 = [](double c) { return c < 0.0 ? 0.0 : (c > 1.0 ? 1.0 : c); };
+    const double c0 = clamp01((bd[a0] + (p[a0] + 0.5) * cw - in.patch[0]) / (in.patch[1] - in.patch[0]));
+    const double c1 = clamp01((bd[a1] + (p[a1] + 0.5) * cw - in.patch[2]) / (in.patch[3] - in.patch[2]));
+    p0 = 4.0 * c0 * (1.0 - c0);
+    p1 = 4.0 * c1 * (1.0 - c1);
+  }
+  const double mag = in.u_peak * p0 * p1;
+  for (int d = 0; d < 3; ++d) u[d] = mag * in.u[d];
+}
+
+// The uniform inlets of octlb_gpu_set_fd_boundary / octlb_fd_plan: face f
+// has one where inlet_u[3 f ..] is nonzero.
+std::vector<octlb_fd_inlet> uniform_inlets(const double* inlet_u, double ramp_end_t) {
+  std::vector<octlb_fd_inlet> v(6);
+  for (int f = 0; f < 6; ++f) {
+    v[f] = octlb_fd_inlet{};
+    if (!inlet_u) continue;
+    const double* iu = inlet_u + 3 * f;
+    if (iu[0] == 0.0 && iu[1] == 0.0 && iu[2] == 0.0) continue;
+    v[f].kind = OCTLB_INLET_UNIFORM;
+    for (int d = 0; d < 3; ++d) v[f].u[d] = iu[d];
+    v[f].ramp_end_t = ramp_end_t;
+  }
+  return v;
+}
+
 // The records of the pass for the blocks `blocks` (global ids, all of forest
 // level 0, in local order) with the given kinds: cells in (block, x, y, z)
 // order, and per role the rows of that role.  Host only.
-int fd_build(octlb_ctx* ctx, int n, const std::vector<int>& blocks, const uint8_t* kinds, const int types[6],
-             const double* u_wall, const double* rho_target, const double* inlet_u, double ramp_end_t,
+int fd_build(octlb_ctx* ctx, int n, const std::vector<int>& blocks, const uint8_t* kinds, const double* bounds,
+             const int types[6], const double* u_wall, const double* rho_target, const octlb_fd_inlet* inlets,
              std::vector<FdCell>& cells, std::vector<int>& lists, std::vector<int>& first, std::vector<int>& count) {
   for (int f = 0; f < 6; ++f)
     if (types[f] < 0 || types[f] > 4) return fail(ctx, OCTLB_EINVAL, "fd boundary: face type outside 0..4");
+  if (int rc = check_inlets(ctx, inlets)) return rc;
+  for (int f = 0; f < 6 && inlets; ++f)
+    if (inlets[f].kind == OCTLB_INLET_CHANNEL_POISEUILLE && !bounds)
+      return fail(ctx, OCTLB_EINVAL, "fd boundary: a channel inlet needs the blocks' bounds in the tables");
   if (n < 4) return fail(ctx, OCTLB_EINVAL, "fd boundary: blocks of n >= 4 only");
   const long long n3 = static_cast<long long>(n) * n * n;
   const int nblk = static_cast<int>(blocks.size());
@@ -301,11 +365,11 @@ int fd_build(octlb_ctx* ctx, int n, const std::vector<int>& blocks, const uint8_
       const bool on[6] = {p.x == 0, p.x == n - 1, p.y == 0, p.y == n - 1, p.z == 0, p.z == n - 1};
       bool done = false;
       for (int f = 0; f < 6 && !done; ++f) {
-        if (!on[f] || !inlet_u) continue;
-        const double* iu = inlet_u + 3 * f;
-        if (iu[0] == 0.0 && iu[1] == 0.0 && iu[2] == 0.0) continue;
+        if (!on[f] || !inlets || inlets[f].kind == OCTLB_INLET_NONE) continue;
+        double iu[3];
+        inlet_velocity(inlets[f], f, p, n, bounds + 6LL * blocks[lb], iu);
         for (int a = 0; a < 3; ++a) fc.u_base[a] = static_cast<float>(iu[a]);
-        fc.ramp_end = static_cast<float>(ramp_end_t);
+        fc.ramp_end = static_cast<float>(inlets[f].ramp_end_t);
         done = true;
       }
       if (!done && p.y == n - 1 && p.x > 0 && p.x < n - 1 && p.z > 0 && p.z < n - 1)
@@ -393,6 +457,12 @@ extern "C" {
 
 int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* u_wall, const double* rho_target,
                               const double* inlet_u, double ramp_end_t) {
+  const std::vector<octlb_fd_inlet> inlets = uniform_inlets(inlet_u, ramp_end_t);
+  return octlb_gpu_set_fd_boundary_inlets(ctx, types, u_wall, rho_target, inlets.data());
+}
+
+int octlb_gpu_set_fd_boundary_inlets(octlb_ctx* ctx, const int types[6], const double* u_wall,
+                                     const double* rho_target, const octlb_fd_inlet* inlets) {
   if (!ctx || !types || !u_wall || !rho_target) return OCTLB_EINVAL;
   if (ctx->levels.empty()) return fail(ctx, OCTLB_ESTATE, "context not initialised");
   for (int c : ctx->counters_collide)
@@ -417,8 +487,9 @@ int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* 
     Level& L = ctx->levels[l];
     if (L.nblk == 0) continue;
     std::vector<int> lists;
-    if (int rc = fd_build(ctx, ctx->n, L.blocks, ctx->kinds.data(), types, u_wall, rho_target, inlet_u, ramp_end_t,
-                          cells[l], lists, L.fd_first, L.fd_count))
+    const double* bounds = ctx->bounds.size() == 6 * static_cast<size_t>(ctx->n_blocks) ? ctx->bounds.data() : nullptr;
+    if (int rc = fd_build(ctx, ctx->n, L.blocks, ctx->kinds.data(), bounds, types, u_wall, rho_target,
+                          inlets, cells[l], lists, L.fd_first, L.fd_count))
       return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     CK(upload(L.fd_cells, cells[l]));
@@ -464,6 +535,12 @@ int octlb_gpu_set_fd_boundary(octlb_ctx* ctx, const int types[6], const double* 
 
 int octlb_fd_plan(const octlb_tables* t, const int types[6], const double* u_wall, const double* rho_target,
                   const double* inlet_u, double ramp_end_t, void* records, int max_records) {
+  const std::vector<octlb_fd_inlet> inlets = uniform_inlets(inlet_u, ramp_end_t);
+  return octlb_fd_plan_inlets(t, types, u_wall, rho_target, inlets.data(), records, max_records);
+}
+
+int octlb_fd_plan_inlets(const octlb_tables* t, const int types[6], const double* u_wall, const double* rho_target,
+                         const octlb_fd_inlet* inlets, void* records, int max_records) {
   if (!t || !types || !u_wall || !rho_target || t->n_blocks < 1) return OCTLB_EINVAL;
   std::vector<int> blocks(t->n_blocks);
   for (int b = 0; b < t->n_blocks; ++b) {
@@ -473,7 +550,7 @@ int octlb_fd_plan(const octlb_tables* t, const int types[6], const double* u_wal
   octlb_ctx ctx;
   std::vector<FdCell> cells;
   std::vector<int> lists, first, count;
-  if (int rc = fd_build(&ctx, t->n, blocks, t->kinds, types, u_wall, rho_target, inlet_u, ramp_end_t, cells, lists,
+  if (int rc = fd_build(&ctx, t->n, blocks, t->kinds, t->bounds, types, u_wall, rho_target, inlets, cells, lists,
                         first, count))
     return rc;
   if (cells.empty()) return OCTLB_EINVAL;  // no Dirichlet or bounce-back cells

@@ -70,7 +70,8 @@ def _velocity_bm_rho(f, direction, orientation, u):
 class Block:
     """One block's kinds, prescribed boundary data and state for the pass."""
 
-    def __init__(self, f_pre, kinds, omega, u_lid=(0.0, 0.0, 0.0), rho_target=None, halo=1, inlets=None, t=0.0):
+    def __init__(self, f_pre, kinds, omega, u_lid=(0.0, 0.0, 0.0), rho_target=None, halo=1, inlets=None, t=0.0,
+                 origin=(0.0, 0.0, 0.0), cell_width=0.0):
         self.f_pre = np.asarray(f_pre, np.float64)
         self.kinds = np.asarray(kinds)
         self.n = self.kinds.shape[0]
@@ -79,9 +80,13 @@ class Block:
         self.u_lid = np.asarray(u_lid, np.float64)
         self.rho_target = np.ones(6) if rho_target is None else np.asarray(rho_target, np.float64)
         self.stencil = min(int(halo), 2)  # kInterpolatedVelocityOverlap = 2
-        # face index (x-, x+, y-, y+, z-, z+) -> (u_const, ramp_end_t) of a uniform inlet
+        # face index (x-, x+, y-, y+, z-, z+) -> (u_const, ramp_end_t) of a
+        # uniform inlet, or a dict (kind, u, u_peak, n_inplane, patch,
+        # ramp_end_t) of any of the reference's inlet fields
         self.inlets = dict(inlets or {})
         self.t = float(t)
+        self.origin = np.asarray(origin, np.float64)  # BlockLattice::phys_origin, phys_cell_width
+        self.cell_width = float(cell_width)
         self.new = {}
 
     def inside(self, cell):
@@ -122,12 +127,37 @@ class Block:
         n1 = self.n - 1
         for face, on in enumerate((x == 0, x == n1, y == 0, y == n1, z == 0, z == n1)):
             if on and face in self.inlets:
-                u_const, t_end = self.inlets[face]
-                r = self.ramp(self.t, t_end)
-                return np.array([r * u_const[d] for d in range(3)])
+                spec = self.inlets[face]
+                if isinstance(spec, tuple):
+                    spec = {"kind": 1, "u": spec[0], "ramp_end_t": spec[1]}
+                return self.inlet_velocity(spec, face, (x, y, z))
         if y == n1 and 0 < x < n1 and 0 < z < n1:
             return self.u_lid.copy()
         return np.zeros(3)
+
+    def inlet_velocity(self, spec, face, cell):
+        """The reference's inlet fields (inlet_velocity_field.h):
+        UniformInletProfile (kind 1, :131-159), PoiseuilleInletProfile (2,
+        block-local in-plane indices, :38-129) and ChannelPoiseuilleInletProfile
+        (3, the physical position origin + (i + 1/2) cell_width on a patch,
+        :163-269); in-plane axes y, z on x faces, x, z on y faces, x, y on z
+        faces."""
+        r = self.ramp(self.t, spec["ramp_end_t"])
+        u = np.asarray(spec["u"], np.float64)
+        if spec["kind"] == 1:
+            return np.array([r * u[d] for d in range(3)])
+        ax = face // 2
+        a0, a1 = (1, 2) if ax == 0 else ((0, 2) if ax == 1 else (0, 1))
+        if spec["kind"] == 2:
+            c0 = (cell[a0] + 0.5) / spec["n_inplane"][0]
+            c1 = (cell[a1] + 0.5) / spec["n_inplane"][1]
+        else:
+            lo0, hi0, lo1, hi1 = spec["patch"]
+            pos = self.origin + (np.asarray(cell, np.float64) + 0.5) * self.cell_width
+            c0 = min(max((pos[a0] - lo0) / (hi0 - lo0), 0.0), 1.0)
+            c1 = min(max((pos[a1] - lo1) / (hi1 - lo1), 0.0), 1.0)
+        mag = r * spec["u_peak"] * (4.0 * c0 * (1.0 - c0)) * (4.0 * c1 * (1.0 - c1))
+        return np.array([mag * u[d] for d in range(3)])
 
     def pops(self, cell, reader):
         """The populations of cell as reader sees them in the in-place walk."""
@@ -244,11 +274,12 @@ class Block:
         self.write(cell, rho, self.compute_u(cell), du)
 
 
-def reconstruct(f_pre, kinds, omega, u_lid=(0.0, 0.0, 0.0), rho_target=None, halo=1, inlets=None, t=0.0):
+def reconstruct(f_pre, kinds, omega, u_lid=(0.0, 0.0, 0.0), rho_target=None, halo=1, inlets=None, t=0.0,
+                origin=(0.0, 0.0, 0.0), cell_width=0.0):
     """The block's populations after the pass: boundary cells (velocity or
     pressure Dirichlet on the block's faces) rewritten in three phases, the
     others unchanged."""
-    b = Block(f_pre, kinds, omega, u_lid, rho_target, halo, inlets, t)
+    b = Block(f_pre, kinds, omega, u_lid, rho_target, halo, inlets, t, origin, cell_width)
     cells = [tuple(c) for c in np.argwhere(np.isin(b.kinds, (VELOCITY, PRESSURE)))]
     count = {c: sum(1 for f in b.faces(*c) if f) for c in cells}
     for want, fn in ((1, b.plane), (2, b.edge), (3, b.corner)):

@@ -258,17 +258,37 @@ class Sim:
     PADDING_POST_STREAM, PADDING_MIRROR, PADDING_HYBRID = range(3)
 
     def set_fd_boundary(self, types, u_wall=None, rho_target=None, padding_mode=2, const_rho=False, inlet_u=None,
-                        ramp_end_t=0.0):
+                        ramp_end_t=0.0, inlets=None):
         """The reference's ConcreteDomainBoundaryHandler on every tree-boundary
         face (faces in FaceDir order x-, x+, y-, y+, z-, z+): spec types,
         wall velocities [6][3], target densities [6]; the face cells stamped
         with the spec's BcKind and the TimeLoop rebuilt around the handler
         (optionally with ConstRhoBGK); faces with a nonzero inlet_u row [6][3]
-        take a uniform inlet of that velocity ramped over ramp_end_t steps.
-        Before the first advance."""
+        take a uniform inlet of that velocity ramped over ramp_end_t steps --
+        or, with inlets (six dicts of kind, u, u_peak, n_inplane, patch,
+        ramp_end_t, or None), the reference's inlet field of that kind
+        (1 uniform, 2 Poiseuille, 3 channel Poiseuille).  Before the first
+        advance."""
         t = np.ascontiguousarray(types, np.int32).reshape(6)
         u = np.zeros((6, 3)) if u_wall is None else np.ascontiguousarray(u_wall, np.float64).reshape(6, 3)
         r = np.ones(6) if rho_target is None else np.ascontiguousarray(rho_target, np.float64).reshape(6)
+        if inlets is not None:
+            kind = np.zeros(6, np.int32)
+            par = np.zeros((6, 11))
+            for f, d in enumerate(inlets):
+                if d is None:
+                    continue
+                kind[f] = int(d["kind"])
+                par[f, 0:3] = d["u"]
+                par[f, 3] = d["u_peak"]
+                par[f, 4:6] = d["n_inplane"]
+                par[f, 6:10] = d["patch"]
+                par[f, 10] = d["ramp_end_t"]
+            self._keep += [t, u, r, kind, par]
+            self.L.ref_sim_set_fd_boundary_inlets(self.h, _p(t, ctypes.c_int), _p(u), _p(r),
+                                                  ctypes.c_int(padding_mode), ctypes.c_int(1 if const_rho else 0),
+                                                  _p(kind, ctypes.c_int), _p(par))
+            return
         iu = None if inlet_u is None else np.ascontiguousarray(inlet_u, np.float64).reshape(6, 3)
         self._keep += [t, u, r, iu]
         self.L.ref_sim_set_fd_boundary(self.h, _p(t, ctypes.c_int), _p(u), _p(r), ctypes.c_int(padding_mode),

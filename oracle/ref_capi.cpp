@@ -443,6 +443,11 @@ void* ref_sim_new(int n_oct, const int* levels, const f64* bounds, int n_sl,
     }
     lat.set_octant_id(id);
     lat.set_bouzidi_links(lp);
+#ifndef OCTLB_REF_TLM
+    // the block's physical origin and cell width, as cylinder3d sets them
+    // (cylinder3d_case.h:405-415): physical inlet fields read them
+    lat.set_phys_origin({bx[id].x_min, bx[id].y_min, bx[id].z_min}, (bx[id].x_max - bx[id].x_min) / n);
+#endif
     return lat;
   });
   s->ghosts = std::make_unique<GhostSchedule<Lat>>(MPI_COMM_WORLD, *s->faces, *s->blocks, n, n, n);
@@ -479,6 +484,8 @@ f64 ref_sim_average_rho(void* h) { return to_f64(static_cast<Sim*>(h)->loop->ave
 // inlet_u (null: none): faces with a nonzero row take a UniformInletProfile
 // of that velocity ramped over ramp_end_t steps (inlet_velocity_field.h:
 // 128-162).  Before the first advance.
+static void install_fd(Sim* s, const std::vector<DomainBcSpec>& specs, int padding_mode, int const_rho);
+
 void ref_sim_set_fd_boundary(void* h, const int* types, const f64* u_wall, const f64* rho_target,
                              int padding_mode, int const_rho, const f64* inlet_u, f64 ramp_end_t) {
   auto* s = static_cast<Sim*>(h);
@@ -492,6 +499,38 @@ void ref_sim_set_fd_boundary(void* h, const int* types, const f64* u_wall, const
       specs[f].inlet_field = std::make_shared<boundary::UniformInletProfile>(
           std::array<double, 3>{inlet_u[3 * f], inlet_u[3 * f + 1], inlet_u[3 * f + 2]}, ramp_end_t);
   }
+  install_fd(s, specs, padding_mode, const_rho);
+}
+
+// The same with one of the reference's inlet fields per face: kind[f] 0
+// none, 1 UniformInletProfile(u), 2 PoiseuilleInletProfile(face, n0, n1,
+// u_peak, u), 3 ChannelPoiseuilleInletProfile(face, patch, u_peak, u);
+// par[11 f ..] = u[3], u_peak, n0, n1, patch[4], ramp_end_t.
+void ref_sim_set_fd_boundary_inlets(void* h, const int* types, const f64* u_wall, const f64* rho_target,
+                                    int padding_mode, int const_rho, const int* kind, const f64* par) {
+  auto* s = static_cast<Sim*>(h);
+  std::vector<DomainBcSpec> specs(6);
+  for (int f = 0; f < 6; ++f) {
+    specs[f].face = static_cast<FaceDir>(f);
+    specs[f].type = static_cast<DomainBcType>(types[f]);
+    specs[f].u_wall = {u_wall[3 * f], u_wall[3 * f + 1], u_wall[3 * f + 2]};
+    specs[f].rho_target = rho_target[f];
+    const f64* p = par + 11 * f;
+    const std::array<double, 3> u{p[0], p[1], p[2]};
+    const FaceDir dir = static_cast<FaceDir>(f);
+    if (kind[f] == 1)
+      specs[f].inlet_field = std::make_shared<boundary::UniformInletProfile>(u, p[10]);
+    else if (kind[f] == 2)
+      specs[f].inlet_field = std::make_shared<boundary::PoiseuilleInletProfile>(
+          dir, static_cast<int>(p[4]), static_cast<int>(p[5]), p[3], u, p[10]);
+    else if (kind[f] == 3)
+      specs[f].inlet_field =
+          std::make_shared<boundary::ChannelPoiseuilleInletProfile>(dir, p[6], p[7], p[8], p[9], p[3], u, p[10]);
+  }
+  install_fd(s, specs, padding_mode, const_rho);
+}
+
+static void install_fd(Sim* s, const std::vector<DomainBcSpec>& specs, int padding_mode, int const_rho) {
   bc::StampTreeBoundaryCells(*s->blocks, s->tree_faces, specs, s->n, s->n, s->n);
   s->loop.reset();
   s->bc = std::make_unique<ConcreteDomainBoundaryHandler>(*s->blocks, s->tree_faces, specs, s->n, s->n, s->n,

@@ -17,6 +17,7 @@ STRUCTS = {
     "octlb_tables": capi.Tables,
     "octlb_adj_params": capi.AdjParams,
     "octlb_partition": capi.Partition,
+    "octlb_fd_inlet": capi.FdInlet,
 }
 
 

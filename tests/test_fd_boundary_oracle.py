@@ -265,6 +265,51 @@ def test_uniform_inlet_with_ramp(ref):
         assert (r == 1.0) == (ramp_end == 0.0)
 
 
+@pytest.mark.parametrize("kind", [2, 3])
+def test_poiseuille_inlets_restated(ref, kind):
+    """The reference's duct inlet fields on x- of eight 8^3 blocks, ramped
+    over 30 steps, against a pressure outlet on x+:
+    PoiseuilleInletProfile (kind 2, inlet_velocity_field.h:38-129: the
+    parabolas over each block's own in-plane indices, 8 x 8 cells) and
+    ChannelPoiseuilleInletProfile (kind 3, :163-269: over the physical
+    patch [0.1, 0.9] x [0.2, 0.8] of the face, each block's origin and cell
+    width set as cylinder3d sets them).  The restated pass matches the
+    reference block by block, and every interior x- cell carries the
+    ramped profile."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_const_rho import brick_cavity
+    from oracle import fd_boundary as fb
+    mesh, info = brick_cavity(lid=0.0, n=8)
+    init = np.zeros((mesh.n_blocks, 8, 8, 8, 19))
+    types = [S.INTERPOLATED_VELOCITY, S.INTERPOLATED_PRESSURE] + [S.INTERPOLATED_VELOCITY] * 4
+    inlet = {"kind": kind, "u": (1.0, 0.0, 0.0), "u_peak": 0.03, "n_inplane": (8, 8),
+             "patch": (0.1, 0.9, 0.2, 0.8), "ramp_end_t": 30.0}
+    sim = S(ref, mesh, info["omega"], init)
+    sim.set_fd_boundary(types, rho_target=np.ones(6), inlets=[inlet, None, None, None, None, None])
+    sim.advance(12)
+    before, after = sim.advance_phases()
+    kinds = sim.kinds()
+    t = 11.0
+    _, vel = oracle.rho_u(after)
+    hit = 0
+    for b in range(mesh.n_blocks):
+        bd = mesh.bounds[b]
+        got = fb.reconstruct(before[b], kinds[b], info["omega"], inlets={0: inlet}, t=t,
+                             origin=bd[:3], cell_width=(bd[3] - bd[0]) / 8)
+        assert np.abs(got - after[b]).max() <= 1e-14, b
+        if bd[0] == 0.0:
+            blk = fb.Block(before[b], kinds[b], info["omega"], inlets={0: inlet}, t=t, origin=bd[:3],
+                           cell_width=(bd[3] - bd[0]) / 8)
+            for y in range(1, 7):
+                for z in range(1, 7):
+                    want = blk.prescribed_u(0, y, z)
+                    assert np.abs(vel[b][0, y, z] - want).max() <= 1e-14
+                    hit += want[0] > 0
+    assert hit > 0
+
+
 def test_const_rho_collide_with_fd_conditions_restated(ref):
     """cavity3d's collision: ConstRhoBGK on kBulk cells and the Dirichlet BGK
     on the boundary cells, with the average density from both

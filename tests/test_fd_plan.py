@@ -33,7 +33,7 @@ CELL = np.dtype({"names": ["slot", "kind", "role", "d", "o", "ax", "nrm", "u_bas
                  "offsets": [0, 8, 12, 16, 20, 24, 36, 48, 60, 64, 72, 184], "itemsize": 376})
 
 
-def plan(ob, mesh, types, u_wall, rho_target, inlet=None, ramp=0.0):
+def plan(ob, mesh, types, u_wall, rho_target, inlet=None, ramp=0.0, inlets=None):
     L = ob.capi.lib()
     assert L.octlb_fd_record_bytes() == CELL.itemsize
     t = np.ascontiguousarray(types, np.int32)
@@ -41,6 +41,15 @@ def plan(ob, mesh, types, u_wall, rho_target, inlet=None, ramp=0.0):
     r = np.ascontiguousarray(rho_target, np.float64)
     iu = None if inlet is None else np.ascontiguousarray(inlet, np.float64)
     P = ctypes.POINTER
+    if inlets is not None:
+        arr = ob.fd_inlets(inlets)
+        args = (ctypes.byref(mesh.c_tables()), t.ctypes.data_as(P(ctypes.c_int)), u.ctypes.data_as(P(ctypes.c_double)),
+                r.ctypes.data_as(P(ctypes.c_double)), arr)
+        n = L.octlb_fd_plan_inlets(*args, None, 0)
+        assert n > 0, n
+        rec = np.zeros(n, CELL)
+        L.octlb_fd_plan_inlets(*args, rec.ctypes.data_as(ctypes.c_void_p), n)
+        return rec
     n = L.octlb_fd_plan(ctypes.byref(mesh.c_tables()), t.ctypes.data_as(P(ctypes.c_int)),
                         u.ctypes.data_as(P(ctypes.c_double)), r.ctypes.data_as(P(ctypes.c_double)),
                         None if iu is None else iu.ctypes.data_as(P(ctypes.c_double)), float(ramp), None, 0)
@@ -132,21 +141,24 @@ def emulate(rec, state, omega, t):
     return new
 
 
-def check(ob, mesh, types, u_wall, rho_target, inlet=None, ramp=0.0, t=0.0, seed=3):
+def check(ob, mesh, types, u_wall, rho_target, inlet=None, ramp=0.0, t=0.0, seed=3, inlets=None):
     stamped = ob.stamp_fd_kinds(mesh, types)
-    rec = plan(ob, stamped, types, u_wall, rho_target, inlet, ramp)
+    rec = plan(ob, stamped, types, u_wall, rho_target, inlet, ramp, inlets)
     n = mesh.n
     rng = np.random.default_rng(seed)
     fpre = 0.01 * rng.standard_normal((mesh.n_blocks, n, n, n, 19))
     omega = 1.0 / 0.6
     new = emulate(rec, fpre.reshape(-1, 19), omega, t)
-    inlets = None
-    if inlet is not None:
-        inlets = {f: (inlet[f], ramp) for f in range(6) if np.any(inlet[f] != 0)}
+    specs = None
+    if inlets is not None:
+        specs = {f: d for f, d in enumerate(inlets) if d is not None}
+    elif inlet is not None:
+        specs = {f: (inlet[f], ramp) for f in range(6) if np.any(inlet[f] != 0)}
     worst = 0.0
     for b in range(mesh.n_blocks):
+        bd = np.asarray(mesh.bounds[b], np.float64)
         want = fb.reconstruct(fpre[b], stamped.kinds[b], omega, u_lid=u_wall[3], rho_target=rho_target,
-                              inlets=inlets, t=t)
+                              inlets=specs, t=t, origin=bd[:3], cell_width=(bd[3] - bd[0]) / n)
         got = fpre[b].copy().reshape(-1, 19)
         sl = rec["slot"]
         mine = ((sl // n ** 3) == b) & (rec["role"] >= 1)  # role 0: bounce-back, not rewritten
@@ -204,6 +216,32 @@ def test_pressure_outlet_across_blocks(ob):
     p = rec[rec["kind"] == 6]
     assert set(np.unique(p["role"])) == {1, 2, 3}
     assert np.any(p["u"]["code"][p["role"] >= 2][:, 0] == 0)
+
+
+@pytest.mark.parametrize("kind", [2, 3])
+def test_poiseuille_inlets(ob, kind):
+    """The duct inlet fields (octlb_fd_plan_inlets): per-block parabolas
+    (Poiseuille) and a physical channel patch (channel Poiseuille) on x- of
+    eight 8^3 blocks, with their ramp, at three times."""
+    sys.path.insert(0, HERE)
+    from test_const_rho import brick_cavity
+    mesh, info = brick_cavity(lid=0.0, n=8)
+    types = [ob.FD_VELOCITY, ob.FD_PRESSURE] + [ob.FD_VELOCITY] * 4
+    inlet = ob.fd_inlet(kind, (1.0, 0.0, 0.0), 0.03, (8, 8), (0.1, 0.9, 0.2, 0.8), 20.0)
+    for t in (0.0, 7.0, 40.0):
+        rec = check(ob, mesh, types, np.zeros((6, 3)), np.ones(6), t=t, inlets=[inlet] + [None] * 5)
+    assert np.count_nonzero(rec["u_base"][:, 0] > 0) > 0 and np.all(rec["ramp_end"][rec["u_base"][:, 0] > 0] == 20.0)
+
+
+def test_inlet_validation(ob):
+    """Out-of-range inlet kinds and degenerate profiles are refused."""
+    from octlb_b200 import cases
+    mesh, init, info = cases.cavity_forest(cells=16, n=16, lid=0.0, tau=0.6)
+    types = [ob.FD_VELOCITY] * 6
+    for bad in (ob.fd_inlet(4), ob.fd_inlet(ob.INLET_POISEUILLE, n_inplane=(0, 8)),
+                ob.fd_inlet(ob.INLET_CHANNEL_POISEUILLE, patch=(0.5, 0.5, 0.0, 1.0))):
+        with pytest.raises(AssertionError):
+            plan(ob, ob.stamp_fd_kinds(mesh, types), types, np.zeros((6, 3)), np.ones(6), inlets=[bad] + [None] * 5)
 
 
 def test_no_slip_walls_and_lid(ob):

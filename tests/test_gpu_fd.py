@@ -74,11 +74,14 @@ def test_inlet_and_pressure_outlet(ob, ref):
     assert rel(u_g, u_r) <= 1e-5 and rel(rho_g, rho_r) <= 1e-5
 
 
-@pytest.mark.parametrize("outlet", [False, True])
-def test_eight_blocks(ob, ref, outlet):
+@pytest.mark.parametrize("inlet", [None, "uniform", "poiseuille", "channel"])
+def test_eight_blocks(ob, ref, inlet):
     """Eight 8^3 blocks: the lid, or an inlet on x- against a pressure outlet
     on x+ that spans four blocks (its block-rim cells read u = 0 and
-    density 1, as the reference's view does off a flat face)."""
+    density 1, as the reference's view does off a flat face).  The inlet is
+    uniform, or one of the reference's duct fields: parabolas over each
+    block's in-plane indices (PoiseuilleInletProfile) or over a physical
+    patch of the face (ChannelPoiseuilleInletProfile, cylinder3d's inlet)."""
     sys.path.insert(0, HERE)
     from test_const_rho import brick_cavity
     mesh, info = brick_cavity(lid=0.0, n=8)
@@ -86,17 +89,28 @@ def test_eight_blocks(ob, ref, outlet):
     types = [S.INTERPOLATED_VELOCITY] * 6
     u = np.zeros((6, 3))
     rho_t = np.ones(6)
-    kw = {}
-    if outlet:
+    if inlet is None:
+        u[3, 0] = 0.05
+        rho_g, u_g, rho_r, u_r = run_pair(ob, ref, mesh, init, info["omega"], types, u, rho_t, 30, ob.FP32)
+    else:
         types[1] = S.INTERPOLATED_PRESSURE
         rho_t[1] = 1.002
-        inlet = np.zeros((6, 3))
-        inlet[0, 0] = 0.02
-        kw = dict(inlet=inlet, ramp=10.0)
-    else:
-        u[3, 0] = 0.05
-    rho_g, u_g, rho_r, u_r = run_pair(ob, ref, mesh, init, info["omega"], types, u, rho_t, 30, ob.FP32, **kw)
-    print(f"fd 8 blocks (outlet {outlet}): u {rel(u_g, u_r):.2e} rho {rel(rho_g, rho_r):.2e}")
+        if inlet == "uniform":
+            spec = ob.fd_inlet(ob.INLET_UNIFORM, (0.02, 0.0, 0.0), ramp_end_t=10.0)
+        else:
+            kind = ob.INLET_POISEUILLE if inlet == "poiseuille" else ob.INLET_CHANNEL_POISEUILLE
+            spec = ob.fd_inlet(kind, (1.0, 0.0, 0.0), 0.04, (8, 8), (0.1, 0.9, 0.2, 0.8), 10.0)
+        inlets = [spec] + [None] * 5
+        lat = ob.GpuLattice(ob.stamp_fd_kinds(mesh, types), info["omega"], init_pops=init)
+        lat.set_fd_boundary(types, u, rho_t, inlets=inlets)
+        lat.advance(30)
+        rho_g, u_g = lat.get_fields()
+        lat.close()
+        sim = S(ref, mesh, info["omega"], init)
+        sim.set_fd_boundary(types, u, rho_target=rho_t, inlets=inlets)
+        sim.advance(30)
+        rho_r, u_r = oracle.rho_u(sim.core())
+    print(f"fd 8 blocks (inlet {inlet}): u {rel(u_g, u_r):.2e} rho {rel(rho_g, rho_r):.2e}")
     assert np.abs(u_r).max() > 0.004
     assert rel(u_g, u_r) <= 1e-5 and rel(rho_g, rho_r) <= 1e-5
 
