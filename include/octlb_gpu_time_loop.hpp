@@ -11,6 +11,14 @@
 //   auto f = loop.force_on_fluid();     // MomentumExchangeDrag::force_on_fluid_if
 //   octlb::GpuTimeLoop cav(tables, params, init_pops, true);   // use_const_rho_bgk
 //   cav.average_rho();                  // TimeLoop::average_rho
+//
+// cavity3d's TimeLoop around a ConcreteDomainBoundaryHandler
+// (cavity3d_case.h:148-197) takes the handler's face specs:
+//
+//   octlb::GpuDomainBc bc;              // CavityBoundarySpecs
+//   for (int f = 0; f < 6; ++f) bc.types[f] = OCTLB_FD_VELOCITY;
+//   bc.u_wall[3 * 3 + 0] = u_lid;       // y+ face
+//   octlb::GpuTimeLoop cav(tables, params, nullptr, true, &bc);
 //   loop.write_vtk("out", "cylinder3d", it);   // AmrVtkWriter::WriteTimestep + WriteVtmAndPvd
 //
 // Errors surface as std::runtime_error, the reference's convention
@@ -19,6 +27,7 @@
 #define OCTLB_GPU_TIME_LOOP_HPP_
 
 #include <array>
+#include <cstdint>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -27,6 +36,17 @@
 
 namespace octlb {
 
+// The DomainBcSpec list of a ConcreteDomainBoundaryHandler, one entry per
+// face in FaceDir order (x-, x+, y-, y+, z-, z+): type (OCTLB_FD_*), wall
+// velocity, target density, inlet field.
+struct GpuDomainBc {
+  int types[6] = {OCTLB_FD_NO_SLIP, OCTLB_FD_NO_SLIP, OCTLB_FD_NO_SLIP,
+                  OCTLB_FD_NO_SLIP, OCTLB_FD_NO_SLIP, OCTLB_FD_NO_SLIP};
+  double u_wall[18] = {};
+  double rho_target[6] = {1.0, 1.0, 1.0, 1.0, 1.0, 1.0};
+  octlb_fd_inlet inlets[6] = {};
+};
+
 struct GpuTimeLoopCounters {
   std::vector<int> collide;
   std::vector<int> stream;
@@ -34,14 +54,28 @@ struct GpuTimeLoopCounters {
 
 class GpuTimeLoop {
  public:
-  // use_const_rho_bgk: the TimeLoop constructor argument (time_loop.h:47-54),
-  // single-level meshes
+  // use_const_rho_bgk: the TimeLoop constructor argument (time_loop.h:47-54).
+  // domain_bc: the finite-difference domain conditions of a
+  // ConcreteDomainBoundaryHandler; the face cells of the tables' kinds are
+  // stamped with the faces' kinds first (bc::StampTreeBoundaryCells).
   GpuTimeLoop(const octlb_tables& tables, const octlb_params& params,
-              const double* init_pops = nullptr, bool use_const_rho_bgk = false) {
-    int rc = octlb_gpu_create(&tables, &params, init_pops, &ctx_);
+              const double* init_pops = nullptr, bool use_const_rho_bgk = false,
+              const GpuDomainBc* domain_bc = nullptr) {
+    octlb_tables t = tables;
+    std::vector<uint8_t> kinds;
+    int rc = OCTLB_OK;
+    if (domain_bc) {
+      kinds.resize(static_cast<size_t>(tables.n_blocks) * tables.n * tables.n * tables.n);
+      rc = octlb_fd_stamp_kinds(&tables, domain_bc->types, kinds.data());
+      t.kinds = kinds.data();
+    }
+    if (rc == OCTLB_OK) rc = octlb_gpu_create(&t, &params, init_pops, &ctx_);
     if (rc == OCTLB_OK && use_const_rho_bgk) rc = octlb_gpu_set_const_rho(ctx_, 1);
+    if (rc == OCTLB_OK && domain_bc)
+      rc = octlb_gpu_set_fd_boundary_inlets(ctx_, domain_bc->types, domain_bc->u_wall, domain_bc->rho_target,
+                                            domain_bc->inlets);
     if (rc != OCTLB_OK) {
-      const std::string msg = ctx_ ? octlb_gpu_last_error(ctx_) : "octlb_gpu_create failed";
+      const std::string msg = ctx_ ? octlb_gpu_last_error(ctx_) : "invalid tables or face specs";
       octlb_gpu_destroy(ctx_);
       ctx_ = nullptr;
       throw std::runtime_error("GpuTimeLoop: " + msg);

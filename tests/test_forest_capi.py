@@ -188,6 +188,14 @@ double use(octlb::GpuTimeLoop& loop) {
   loop.write_vtk("out", "case", 1);
   return loop.average_rho() + loop.total_mass() + loop.force_on_fluid()[0] + loop.counters().collide.size();
 }
+// cavity3d's construction: ConstRhoBGK and the domain handler's face specs
+void cavity(const octlb_tables& t, const octlb_params& p) {
+  octlb::GpuDomainBc bc;
+  for (int f = 0; f < 6; ++f) bc.types[f] = OCTLB_FD_VELOCITY;
+  bc.u_wall[3 * 3] = 0.1;
+  octlb::GpuTimeLoop cav(t, p, nullptr, true, &bc);
+  cav.advance(5269);
+}
 int main() {
   octlb_tables t{};
   octlb_params p{};
@@ -199,6 +207,13 @@ int main() {
   try {
     octlb::GpuTimeLoop loop(t, p);
     return 2;
+  } catch (const std::runtime_error& e) {
+    std::printf("%s\n", e.what());
+  }
+  try {  // face specs on invalid tables: refused before any device work
+    octlb::GpuDomainBc bc;
+    octlb::GpuTimeLoop loop(t, p, nullptr, false, &bc);
+    return 3;
   } catch (const std::runtime_error& e) {
     std::printf("%s\n", e.what());
     return 0;
