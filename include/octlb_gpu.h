@@ -196,10 +196,10 @@ int octlb_gpu_average_rho(octlb_ctx* ctx, double* out);
  * each level's boundary cells collide at the start of its step; on a
  * multi-level mesh the coarse-fine interfaces must stay away from the
  * domain faces (every coupler source and target a kBulk cell; OCTLB_EINVAL
- * otherwise).  With ConstRhoBGK (octlb_gpu_set_const_rho, called first; one
- * level) the velocity cells' collide densities join the average's
- * statistics, as the reference's kFluidAndBoundary scope does (cavity3d's
- * configuration). */
+ * otherwise).  With ConstRhoBGK (octlb_gpu_set_const_rho, called first; any
+ * number of levels) the finest level's velocity cells' collide densities join
+ * the average's statistics, as the reference's kFluidAndBoundary scope does
+ * (cavity3d's configuration). */
 #define OCTLB_FD_NO_SLIP 0
 #define OCTLB_FD_MOVING_LID 1
 #define OCTLB_FD_VELOCITY 2

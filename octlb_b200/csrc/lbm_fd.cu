@@ -120,7 +120,7 @@ __device__ __forceinline__ float warp_sum(float v) {
 template <typename T>
 __global__ void __launch_bounds__(kFdThreads)
 k_fd_reconstruct(const T* state, long long qs, float inv_s, const FdCell* cells, const int* list, int n,
-                 float* fnew, const double* time, float omega, const double* cr_avg) {
+                 float* fnew, const double* time, float omega, const float* cr_shift) {
   const int w = static_cast<int>((blockIdx.x * kFdThreads + threadIdx.x) >> 5);
   if (w >= n) return;  // whole warps
   const int lane = threadIdx.x & 31;
@@ -182,9 +182,9 @@ k_fd_reconstruct(const T* state, long long qs, float inv_s, const FdCell* cells,
       rr[j] = r.val;
     } else if (r.code == kFdRhoSumPre || r.code == kFdRhoSumNew) {
       // a kBulk cell's stored density under ConstRhoBGK carries the 1 -
-      // average_rho its collide added (urow = 1 marks a kBulk cell)
-      const float shift =
-          (r.code == kFdRhoSumPre && r.urow == 1 && cr_avg) ? static_cast<float>(1.0 - *cr_avg) : 0.f;
+      // average_rho its level's last collide added, if that collide came
+      // after the level's stream (urow = 1 marks a kBulk cell)
+      const float shift = (r.code == kFdRhoSumPre && r.urow == 1 && cr_shift) ? *cr_shift : 0.f;
       rr[j] = 1.f + warp_sum(fr[j]) - shift;
     } else {
       float u[3];
@@ -361,12 +361,12 @@ namespace {
 
 template <typename T>
 cudaError_t launch_fd_reconstruct(const void* state, long long qs, float inv_s, const FdCell* cells, const int* list,
-                                  int n, float* fnew, const double* time, float omega, const double* cr_avg,
+                                  int n, float* fnew, const double* time, float omega, const float* cr_shift,
                                   cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   const unsigned grid = static_cast<unsigned>((static_cast<long long>(n) * 32 + kFdThreads - 1) / kFdThreads);
   k_fd_reconstruct<T><<<grid, kFdThreads, 0, s>>>(static_cast<const T*>(state), qs, inv_s, cells, list, n, fnew,
-                                                  time, omega, cr_avg);
+                                                  time, omega, cr_shift);
   return cudaGetLastError();
 }
 
@@ -411,7 +411,7 @@ cudaError_t launch_fd_tick(double* time, cudaStream_t s) {
 
 #define OCTLB_FD_INST(T)                                                                                      \
   template cudaError_t launch_fd_reconstruct<T>(const void*, long long, float, const FdCell*, const int*, int, \
-                                                float*, const double*, float, const double*, cudaStream_t); \
+                                                float*, const double*, float, const float*, cudaStream_t);  \
   template cudaError_t launch_fd_collide<T>(void*, long long, float, float, const FdCell*, int, float*,        \
                                             const double*, double, float, double*, cudaStream_t);
 template cudaError_t launch_fd_rows_from_state<float>(const void*, long long, float, const FdCell*, int, float*,

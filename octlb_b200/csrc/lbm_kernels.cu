@@ -1103,10 +1103,15 @@ __global__ void __launch_bounds__(kThreads) k_cr_seed(const StepArgs a, int near
 // restriction has written its targets, and the average density is the one
 // the finest level's last collide gave, which the reference's next collide
 // of this level uses.
+//
+// shift (when not null): the density shift 1 - average_rho the collide puts
+// on the level's kBulk cells, which the finite-difference pass removes from
+// the densities it reads there.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_collide_cr(const StepArgs a) {
+__global__ void __launch_bounds__(kThreads) k_collide_cr(const StepArgs a, float* shift) {
   pdl_wait();
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  if (shift && t == 0) *shift = static_cast<float>(1.0 - *a.cr_avg);
   if (t >= a.ncore) return;
   if (a.flags && (a.flags[t] & kKindMask) != kBulk) return;
   T* pops = static_cast<T*>(a.dst);
@@ -1126,9 +1131,12 @@ __global__ void __launch_bounds__(kThreads) k_collide_cr(const StepArgs a) {
 // With the finite-difference boundary pass (kFluidAndBoundary scope) the
 // velocity-Dirichlet cells' collide densities join the statistics:
 // (sum(rho - 1) + count (2 - average_rho) + sum rho_b) / (count + count_b).
+//
+// shift (when not null): 1 - average_rho, the density shift the finest
+// level's collide now puts on its kBulk cells.
 __global__ void __launch_bounds__(kThreads)
 k_cr_update(double* avg, const double* part, int nparts, long long count, const double* bpart, int nbparts,
-            long long bcount) {
+            long long bcount, float* shift) {
   pdl_wait();
   double v[2] = {0.0, 0.0};
   for (int p = threadIdx.x; p < nparts; p += kThreads) v[0] += part[p];
@@ -1139,6 +1147,7 @@ k_cr_update(double* avg, const double* part, int nparts, long long count, const 
       *avg = count > 0 ? (2.0 - *avg) + v[0] / static_cast<double>(count) : 1.0;
     else
       *avg = (v[0] + static_cast<double>(count) * (2.0 - *avg) + v[1]) / static_cast<double>(count + bcount);
+    if (shift) *shift = static_cast<float>(1.0 - *avg);
   }
 }
 
@@ -1402,9 +1411,9 @@ cudaError_t launch_step_cr(const StepArgs& a, const NearTables& nt, bool links, 
 }
 
 template <typename T>
-cudaError_t launch_collide_cr(const StepArgs& a, cudaStream_t s) {
+cudaError_t launch_collide_cr(const StepArgs& a, float* shift, cudaStream_t s) {
   if (a.ncore == 0) return cudaSuccess;
-  const cudaError_t e = launch_chain(k_collide_cr<T>, dim3(grid_for(a.ncore)), dim3(kThreads), 0, s, a);
+  const cudaError_t e = launch_chain(k_collide_cr<T>, dim3(grid_for(a.ncore)), dim3(kThreads), 0, s, a, shift);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -1415,9 +1424,9 @@ cudaError_t launch_cr_seed(const StepArgs& a, int near_parts, cudaStream_t s) {
 }
 
 cudaError_t launch_cr_update(double* avg, const double* part, int nparts, long long count, const double* bpart,
-                             int nbparts, long long bcount, cudaStream_t s) {
+                             int nbparts, long long bcount, float* shift, cudaStream_t s) {
   const cudaError_t e = launch_chain(k_cr_update, dim3(1), dim3(kThreads), 0, s, avg, part, nparts, count, bpart,
-                                     nbparts, bcount);
+                                     nbparts, bcount, shift);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -1440,7 +1449,7 @@ cudaError_t launch_cr_update(double* avg, const double* part, int nparts, long l
   template cudaError_t launch_step_map_cr<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
   template cudaError_t launch_step_map_nc<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
   template cudaError_t launch_step_nc<T>(const StepArgs&, const NearTables&, bool, bool, cudaStream_t); \
-  template cudaError_t launch_collide_cr<T>(const StepArgs&, cudaStream_t);                        \
+  template cudaError_t launch_collide_cr<T>(const StepArgs&, float*, cudaStream_t);                \
   template cudaError_t launch_cr_seed<T>(const StepArgs&, int, cudaStream_t);
 
 OCTLB_INST(float)

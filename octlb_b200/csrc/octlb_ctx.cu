@@ -156,11 +156,14 @@ int launch_level_step(octlb_ctx* ctx, Level& L) {
       CK(launch_step_nc<T>(a, L.near, links, L.has_flags, ctx->stream));
       if (L.near.n > 0) ++ctx->launch_count;
     }
+    // the level's kBulk cells are post-stream now: no density shift
+    if (ctx->fd_on) CK(cudaMemsetAsync(ctx->cr_shift.as<float>() + L.lvl, 0, sizeof(float), ctx->stream));
   } else if (ctx->const_rho) {
     // ConstRhoBGK: average_rho from the last collide's statistics
     // (time_loop.h:220-222), then the step whose collide uses it
     CK(launch_cr_update(ctx->cr_avg.as<double>(), ctx->cr_part.as<double>(), ctx->cr_nparts + ctx->cr_pparts,
-                        ctx->cr_count, ctx->fd_cr_part.as<double>(), ctx->fd_cr_parts, ctx->fd_vel, ctx->stream));
+                        ctx->cr_count, ctx->fd_cr_part.as<double>(), ctx->fd_cr_parts, ctx->fd_vel,
+                        ctx->cr_shift.as<float>() + L.lvl, ctx->stream));
     const bool links = ctx->stream_mode == OCTLB_STREAM_LINKS;
     if (L.use_map && ctx->map_global && ctx->map_cells == (links ? 1 : 2)) {
       CK(launch_step_map_cr<T>(a, L.near, links, L.has_flags, ctx->stream));
@@ -281,7 +284,7 @@ int do_advance_level(octlb_ctx* ctx, int l) {
     if (rc) return rc;
     StepArgs a = L.args;
     a.dst = cur_buf(L);
-    CK(launch_collide_cr<T>(a, ctx->stream));
+    CK(launch_collide_cr<T>(a, ctx->cr_shift.as<float>() + L.lvl, ctx->stream));
     ++ctx->launch_count;
   }
   return OCTLB_OK;
@@ -2291,6 +2294,7 @@ int octlb_gpu_set_const_rho(octlb_ctx* ctx, int on) {
   // the collide and statistic the step gave it.
   Level& L = ctx->levels[lev];
   CK(upload(ctx->cr_avg, std::vector<double>{1.0}));  // TimeLoop starts at average_rho_ = 1
+  CK(upload(ctx->cr_shift, std::vector<float>(ctx->levels.size(), 0.f)));  // BGK-collided: no shift
   const uint32_t core = cr_core_parts(L.args), near = cr_near_parts(L.near);
   ctx->cr_multi = used > 1;
   ctx->cr_nparts = static_cast<int>(core + near);

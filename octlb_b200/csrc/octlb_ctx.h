@@ -42,9 +42,10 @@ template <typename T>
 cudaError_t launch_step_map_nc(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
 template <typename T>
 cudaError_t launch_step_nc(const StepArgs&, const NearTables&, bool, bool, cudaStream_t);
-template <typename T> cudaError_t launch_collide_cr(const StepArgs&, cudaStream_t);
+template <typename T> cudaError_t launch_collide_cr(const StepArgs&, float*, cudaStream_t);
 template <typename T> cudaError_t launch_step_aa(const StepArgs&, bool, cudaStream_t);
-cudaError_t launch_cr_update(double*, const double*, int, long long, const double*, int, long long, cudaStream_t);
+cudaError_t launch_cr_update(double*, const double*, int, long long, const double*, int, long long, float*,
+                             cudaStream_t);
 uint32_t cr_core_parts(const StepArgs& a);
 uint32_t cr_near_parts(const NearTables& nt);
 uint32_t couple_prolong_ctas(int n);
@@ -389,6 +390,10 @@ struct octlb_ctx {
   // ConstRhoBGK with the pass: per-CTA sums of the velocity cells' collide
   // densities (the boundary part of the statistics), over fd_vel cells
   DevBuf fd_cr_part;
+  // ConstRhoBGK: per level the density shift 1 - average_rho its kBulk
+  // cells' stored state carries (0 after a stream-only step), which the
+  // finite-difference pass removes from the densities it reads
+  DevBuf cr_shift;
   int fd_cr_parts = 0;
   long long fd_vel = 0;
   bool owns(int b) const { return owner.empty() || owner[b] == rank; }

@@ -18,7 +18,7 @@
 namespace octlb_gpu {
 template <typename T>
 cudaError_t launch_fd_reconstruct(const void*, long long, float, const FdCell*, const int*, int, float*,
-                                  const double*, float, const double*, cudaStream_t);
+                                  const double*, float, const float*, cudaStream_t);
 template <typename T>
 cudaError_t launch_fd_collide(void*, long long, float, float, const FdCell*, int, float*, const double*,
                               double, float, double*, cudaStream_t);
@@ -170,7 +170,7 @@ int fd_after_step(octlb_ctx* ctx, Level& S) {
       const int n = L.fd_count[role];
       if (n == 0) continue;
       CK(launch_fd_reconstruct<T>(state, L.nslots, L.inv_scale, cells, L.fd_lists.as<int>() + L.fd_first[role], n,
-                                  fnew, time, omega, ctx->const_rho ? ctx->cr_avg.as<double>() : nullptr,
+                                  fnew, time, omega, ctx->const_rho ? ctx->cr_shift.as<float>() + L.lvl : nullptr,
                                   ctx->stream));
       ++ctx->launch_count;
     }
@@ -191,7 +191,8 @@ int fd_before_step(octlb_ctx* ctx, Level& L) {
   CK(launch_fd_collide<T>(cur_buf(L), L.nslots, L.scale, L.inv_scale, L.fd_cells.as<FdCell>(), L.fd_rows,
                           L.fd_new.as<float>(), ctx->fd_time.as<double>(), 0.0,
                           static_cast<float>(ctx->omega_l[L.lvl]),
-                          ctx->const_rho ? ctx->fd_cr_part.as<double>() : nullptr, ctx->stream));
+                          ctx->const_rho && L.lvl == ctx->cr_level ? ctx->fd_cr_part.as<double>() : nullptr,
+                          ctx->stream));
   ++ctx->launch_count;
   return OCTLB_OK;
 }
@@ -476,8 +477,6 @@ int octlb_gpu_set_fd_boundary_inlets(octlb_ctx* ctx, const int types[6], const d
     ++used;
     if (L.n_bb > 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: the tree-boundary faces must carry no restated fill");
   }
-  if (used > 1 && ctx->const_rho)
-    return fail(ctx, OCTLB_EINVAL, "fd boundary with ConstRhoBGK: single-level meshes");
   if (used > 1 && !ctx->cpl_cells_bulk)
     return fail(ctx, OCTLB_EINVAL,
                 "fd boundary on a multi-level mesh: every coupler source and target must be a kBulk cell "
@@ -501,17 +500,20 @@ int octlb_gpu_set_fd_boundary_inlets(octlb_ctx* ctx, const int types[6], const d
   for (const auto& c : cells) total += c.size();
   if (total == 0) return fail(ctx, OCTLB_EINVAL, "fd boundary: no Dirichlet or bounce-back cells");
   CK(upload(ctx->fd_time, std::vector<double>{0.0}));
-  // ConstRhoBGK (chosen before, one level): the velocity cells' collide
-  // densities join its statistics (the reference's kFluidAndBoundary scope)
+  // ConstRhoBGK (chosen before): the finest level's velocity cells'
+  // collide densities join its statistics (the reference's
+  // kFluidAndBoundary scope, collected where level >= max_level_,
+  // time_loop.h:201-222)
   if (ctx->const_rho) {
     ctx->fd_vel = 0;
     int rows = 0;
-    for (size_t l = 0; l < cells.size(); ++l) {
-      rows += static_cast<int>(cells[l].size());
-      for (const FdCell& fc : cells[l]) ctx->fd_vel += fc.kind == kVelocityDirichlet ? 1 : 0;
+    if (ctx->cr_level >= 0 && ctx->cr_level < static_cast<int>(cells.size())) {
+      rows = static_cast<int>(cells[ctx->cr_level].size());
+      for (const FdCell& fc : cells[ctx->cr_level]) ctx->fd_vel += fc.kind == kVelocityDirichlet ? 1 : 0;
     }
-    ctx->fd_cr_parts = static_cast<int>(fd_collide_parts(rows));
+    ctx->fd_cr_parts = static_cast<int>(fd_collide_parts(std::max(rows, 1)));
     CK(ctx->fd_cr_part.alloc(static_cast<size_t>(ctx->fd_cr_parts) * sizeof(double)));
+    CK(cudaMemsetAsync(ctx->fd_cr_part.p, 0, static_cast<size_t>(ctx->fd_cr_parts) * sizeof(double), ctx->stream));
   }
   // The rows start as the stored initial state of the boundary cells,
   // which the initial collide left uncollided (it takes kBulk cells only):
