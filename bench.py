@@ -304,7 +304,7 @@ def run_reference_arm(args, world, rank, pg):
 
 def accuracy_vs_fp64(ob, cases, n, steps, fields_fp32, threads=None):
     """Errors of the headline workload against FP64 runs of the reference's
-    algorithm (north star: each result states its error against FP64):
+    algorithm (each result states its error against an FP64 run):
 
     * the 256^3 box after `steps` steps (the e2e run's fields for FP32, a
       separate run for FP16) against the oracle's C restatement of the
