@@ -307,8 +307,11 @@ __global__ void k_fd_tick(double* time) { *time += 1.0; }
 // bounce-back cells keep their streamed populations until their collide).
 template <typename T>
 __global__ void __launch_bounds__(kFdThreads)
-k_fd_store(T* state, long long qs, float scale, const FdCell* cells, int n, const float* fnew) {
+k_fd_store(T* state, long long qs, float scale, const FdCell* cells, int n, const float* fnew, double* tick) {
   const int row = blockIdx.x * kFdThreads + threadIdx.x;
+  // the boundary clock's tick, where this is the step's last pass (no kernel
+  // of the pass reads the clock after the reconstruction)
+  if (tick && row == 0) *tick += 1.0;
   if (row >= n || cells[row].role == 0) return;
 #pragma unroll
   for (int i = 0; i < kQ; ++i)
@@ -396,13 +399,15 @@ cudaError_t launch_fd_fields(const FdCell* cells, int n, const float* fnew, doub
 
 template <typename T>
 cudaError_t launch_fd_store(void* state, long long qs, float scale, const FdCell* cells, int n, const float* fnew,
-                            cudaStream_t s) {
+                            double* tick, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_fd_store<T><<<fd_grid(n), kFdThreads, 0, s>>>(static_cast<T*>(state), qs, scale, cells, n, fnew);
+  k_fd_store<T><<<fd_grid(n), kFdThreads, 0, s>>>(static_cast<T*>(state), qs, scale, cells, n, fnew, tick);
   return cudaGetLastError();
 }
-template cudaError_t launch_fd_store<float>(void*, long long, float, const FdCell*, int, const float*, cudaStream_t);
-template cudaError_t launch_fd_store<__half>(void*, long long, float, const FdCell*, int, const float*, cudaStream_t);
+template cudaError_t launch_fd_store<float>(void*, long long, float, const FdCell*, int, const float*, double*,
+                                           cudaStream_t);
+template cudaError_t launch_fd_store<__half>(void*, long long, float, const FdCell*, int, const float*, double*,
+                                            cudaStream_t);
 
 cudaError_t launch_fd_tick(double* time, cudaStream_t s) {
   k_fd_tick<<<1, 1, 0, s>>>(time);

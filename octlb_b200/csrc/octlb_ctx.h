@@ -389,6 +389,7 @@ struct octlb_ctx {
   bool cpl_cells_bulk = true;
   // ConstRhoBGK with the pass: per-CTA sums of the velocity cells' collide
   // densities (the boundary part of the statistics), over fd_vel cells
+  bool fd_single = false;           // the pass on one level: its store ticks the clock
   DevBuf fd_cr_part;
   // ConstRhoBGK: per level the density shift 1 - average_rho its kBulk
   // cells' stored state carries (0 after a stream-only step), which the

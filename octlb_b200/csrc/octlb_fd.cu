@@ -28,7 +28,7 @@ template <typename T>
 cudaError_t launch_fd_rows_from_state(const void*, long long, float, const FdCell*, int, float*, cudaStream_t);
 cudaError_t launch_fd_fields(const FdCell*, int, const float*, double*, double*, cudaStream_t);
 template <typename T>
-cudaError_t launch_fd_store(void*, long long, float, const FdCell*, int, const float*, cudaStream_t);
+cudaError_t launch_fd_store(void*, long long, float, const FdCell*, int, const float*, double*, cudaStream_t);
 }  // namespace octlb_gpu
 
 using namespace octlb_gpu;
@@ -174,7 +174,10 @@ int fd_after_step(octlb_ctx* ctx, Level& S) {
                                   ctx->stream));
       ++ctx->launch_count;
     }
-    CK(launch_fd_store<T>(state, L.nslots, L.scale, cells, L.fd_rows, fnew, ctx->stream));
+    // on a single-level mesh this is the step's only pass: the store ticks
+    // the boundary clock in place of a launch of its own
+    CK(launch_fd_store<T>(state, L.nslots, L.scale, cells, L.fd_rows, fnew,
+                          ctx->fd_single ? ctx->fd_time.as<double>() : nullptr, ctx->stream));
     ++ctx->launch_count;
   }
   return OCTLB_OK;
@@ -210,7 +213,7 @@ int fd_fix_fields(octlb_ctx* ctx, Level& L, double* rho, double* u) {
 }
 
 int fd_end_of_step(octlb_ctx* ctx) {
-  if (!ctx->fd_on) return OCTLB_OK;
+  if (!ctx->fd_on || ctx->fd_single) return OCTLB_OK;  // (a single level's store ticked it)
   CK(launch_fd_tick(ctx->fd_time.as<double>(), ctx->stream));
   ++ctx->launch_count;
   return OCTLB_OK;
@@ -531,6 +534,10 @@ int octlb_gpu_set_fd_boundary_inlets(octlb_ctx* ctx, const int types[6], const d
   }
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->fd_on = true;
+  // one level in the recursion: one pass per advance_one (a mesh whose
+  // blocks sit on a finer forest level also steps its empty coarser levels,
+  // each with a pass)
+  ctx->fd_single = ctx->levels.size() == 1;
   clear_graphs(ctx);  // the captured launch sequence changes
   return OCTLB_OK;
 }
